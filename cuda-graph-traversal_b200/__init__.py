@@ -1,0 +1,368 @@
+"""Python host mirror of the reference's Graph500 API over libg500b.so.
+
+The functions keep the names, argument meaning and error behaviour of the
+reference's C++ API (src/graph_generation.h, src/traversal.h and the
+runner's helpers in examples/graph500_runner.cu); the work runs in the CUDA
+kernels of libg500b.so through its C ABI (include/g500b.h).  PyTorch only
+provides device memory and the current stream.  There is no CPU path: if the
+shared library is missing, importing this module raises.
+
+Layout on the device (one graph):
+  rowstarts  uint64[N+1]   stored as torch.int64
+  col        int32[E]      neighbour ids, light entries (w < delta) first in each row
+  w          float32[E]
+  light_deg  int32[N]      light entries per row (uint32 on the C side)
+  column     int64[E]      optional u64 copy of col (the reference's Oned_Graph.column)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libg500b.so")
+
+G5_OK = 0
+_ERRORS = {-1: ValueError, -2: MemoryError, -3: RuntimeError, -4: TimeoutError, -5: RuntimeError}
+
+
+class G5Error(RuntimeError):
+    pass
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libg500b.so not built at {LIB_PATH}; run `make -C {_HERE}` "
+                          "(or __graft_entry__.build())")
+    L = C.CDLL(LIB_PATH)
+    p, u64, i64, u32, i32, f32 = C.c_void_p, C.c_uint64, C.c_int64, C.c_uint32, C.c_int32, C.c_float
+    sig = {
+        "g5_last_error": ([], C.c_char_p),
+        "g5_version": ([], C.c_char_p),
+        "g5_make_mrg_seed": ([u64, u64, p], C.c_int),
+        "g5_make_random_numbers": ([i64, u64, u64, i64, p], C.c_int),
+        "g5_scramble_keys": ([p, p, p], C.c_int),
+        "g5_generate_kronecker_range": ([p, u32, i64, i64, p, p, p], C.c_int),
+        "g5_csr_workspace_size": ([u64, u64, p], C.c_int),
+        "g5_csr_count": ([p, u64, u64, p, p, u64, p, p], C.c_int),
+        "g5_csr_fill": ([p, p, u64, u64, p, f32, p, u64, p, p, p, p, p], C.c_int),
+        "g5_bfs_workspace_size": ([u64, p], C.c_int),
+        "g5_bfs_run": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
+        "g5_bfs_last_stats": ([p, u64, p, p], C.c_int),
+        "g5_bfs_dist_from_pred": ([p, p, u64, p, u64, p, p, u64, p], C.c_int),
+        "g5_sssp_workspace_size": ([u64, p], C.c_int),
+        "g5_sssp_run": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
+        "g5_sssp_last_status": ([p, u64, p, p, p], C.c_int),
+        "g5_validate_workspace_size": ([u64, p], C.c_int),
+        "g5_edge_count": ([p, p, u64, p, p, u64, p, p], C.c_int),
+        "g5_bfs_validate": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
+        "g5_sssp_validate": ([p, p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
+        "g5_selftest_wait_timeout": ([u32, p, u64, p], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    return L
+
+
+lib = _load()
+
+
+def _check(rc: int) -> None:
+    if rc != G5_OK:
+        msg = lib.g5_last_error().decode()
+        raise _ERRORS.get(rc, G5Error)(f"libg500b error {rc}: {msg}")
+
+
+class BfsParams(C.Structure):
+    _fields_ = [("alpha", C.c_float), ("beta", C.c_float), ("mode", C.c_int32), ("blocks", C.c_int32)]
+
+
+class BfsStats(C.Structure):
+    _fields_ = [("levels", C.c_int32), ("bottom_up_levels", C.c_int32), ("reached", C.c_uint64)]
+
+
+class SsspParams(C.Structure):
+    _fields_ = [("delta", C.c_float), ("blocks", C.c_int32)]
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _stream(stream=None) -> int | None:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream or None
+
+
+def _workspace(nbytes: int, device) -> torch.Tensor:
+    return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+
+
+def version() -> str:
+    return lib.g5_version().decode()
+
+
+def selftest_wait_timeout(limit_ms: int = 50, device="cuda") -> None:
+    """Runs the bounded-wait self test; raises TimeoutError as designed."""
+    work = torch.zeros(64, dtype=torch.uint8, device=device)
+    _check(lib.g5_selftest_wait_timeout(limit_ms, _ptr(work), work.numel(), _stream()))
+
+
+# ----------------------------------------------------------------- MRG ----
+
+def make_mrg_seed(userseed1: int, userseed2: int) -> list[int]:
+    """make_mrg_seed (src/graph_generation.h:39)."""
+    seed = (C.c_uint32 * 5)()
+    _check(lib.g5_make_mrg_seed(userseed1, userseed2, seed))
+    return list(seed)
+
+
+def make_random_numbers(nvalues: int, userseed1: int, userseed2: int, position: int) -> np.ndarray:
+    """make_random_numbers (src/graph_generation.h:40)."""
+    out = np.zeros(max(nvalues, 0), np.float64)
+    _check(lib.g5_make_random_numbers(nvalues, userseed1, userseed2, position,
+                                      out.ctypes.data if nvalues else None))
+    return out
+
+
+def scramble_keys(seed) -> tuple[int, int]:
+    s = (C.c_uint32 * 5)(*seed)
+    a, b = C.c_uint64(), C.c_uint64()
+    _check(lib.g5_scramble_keys(s, C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+# ----------------------------------------------------------- generator ----
+
+@dataclass
+class TupleGraph:
+    """Tuple_Graph (src/graph_generation.h:12-19): edges (M, 2) as int64
+    holding the u64 vertex ids, weights float32[M]."""
+    edges: torch.Tensor
+    weights: torch.Tensor
+    nglobaledges: int
+
+    @property
+    def edges_size(self) -> int:
+        return self.edges.shape[0]
+
+
+def generate_kronecker_range(seed, log_n: int, start_edge: int, end_edge: int,
+                             device="cuda", out: TupleGraph | None = None, stream=None) -> TupleGraph:
+    """generate_kronecker_range (src/graph_generation.h:33-37)."""
+    m = max(end_edge - start_edge, 0)
+    if out is None:
+        out = TupleGraph(torch.empty((m, 2), dtype=torch.int64, device=device),
+                         torch.empty(m, dtype=torch.float32, device=device), m)
+    s = (C.c_uint32 * 5)(*seed)
+    _check(lib.g5_generate_kronecker_range(s, log_n, start_edge, end_edge, _ptr(out.edges),
+                                           _ptr(out.weights), _stream(stream)))
+    return out
+
+
+# ----------------------------------------------------------------- CSR ----
+
+@dataclass
+class OnedGraph:
+    """Oned_Graph (src/traversal.h:8-16) at one rank, plus the int32 column
+    and per-row light counts the kernels use."""
+    nglobalverts: int
+    nlocaledges: int
+    rowstarts: torch.Tensor
+    col: torch.Tensor
+    w: torch.Tensor
+    light_deg: torch.Tensor
+    light_delta: float
+    column: torch.Tensor | None = None
+
+    @property
+    def nlocalverts(self) -> int:
+        return self.nglobalverts
+
+    @property
+    def device(self):
+        return self.rowstarts.device
+
+
+def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: float = 0.1,
+                                with_column64: bool = False, stream=None) -> OnedGraph:
+    """oned_graph_from_tuple_graph (src/traversal.h:43)."""
+    dev = tg.edges.device
+    n, m = int(nglobalverts), tg.edges_size
+    nb = C.c_uint64()
+    _check(lib.g5_csr_workspace_size(n, m, C.byref(nb)))
+    work = _workspace(nb.value, dev)
+    rowstarts = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    nent = C.c_uint64()
+    st = _stream(stream)
+    _check(lib.g5_csr_count(_ptr(tg.edges), m, n, _ptr(rowstarts), _ptr(work), work.numel(),
+                            C.byref(nent), st))
+    e = nent.value
+    col = torch.empty(max(e, 1), dtype=torch.int32, device=dev)
+    w = torch.empty(max(e, 1), dtype=torch.float32, device=dev)
+    light = torch.empty(n, dtype=torch.int32, device=dev)
+    col64 = torch.empty(max(e, 1), dtype=torch.int64, device=dev) if with_column64 else None
+    _check(lib.g5_csr_fill(_ptr(tg.edges), _ptr(tg.weights), m, n, _ptr(rowstarts), light_delta,
+                           _ptr(work), work.numel(), _ptr(col), _ptr(w), _ptr(col64), _ptr(light), st))
+    return OnedGraph(n, e, rowstarts, col[:e], w[:e], light, light_delta,
+                     None if col64 is None else col64[:e])
+
+
+def oned_graph_is_vertex_isolated(g: OnedGraph, global_vertex: int) -> bool:
+    """oned_graph_is_vertex_isolated (src/traversal.h:44); raises on a vertex
+    outside [0, N) where the reference aborts."""
+    if not 0 <= global_vertex < g.nglobalverts:
+        raise ValueError(f"Vertex {global_vertex} is outside graph vertex range [0, {g.nglobalverts})")
+    r = g.rowstarts[global_vertex:global_vertex + 2].cpu()
+    return bool(r[0] == r[1])
+
+
+def generate_bfs_roots(g: OnedGraph, seed1: int = 2, seed2: int = 3, max_roots: int = 64) -> list[int]:
+    """Root choice of the runner's generate_bfs_roots
+    (examples/graph500_runner.cu:43-74): up to max_roots distinct vertices of
+    nonzero degree from the seeded MRG doubles."""
+    n = g.nglobalverts
+    deg0 = (g.rowstarts[1:] == g.rowstarts[:-1]).cpu().numpy()
+    roots: list[int] = []
+    counter = 0
+    while len(roots) < max_roots:
+        found = False
+        while True:
+            d = make_random_numbers(2, seed1, seed2, counter)
+            root = int(np.uint64((d[0] + d[1]) * float(n))) % n
+            counter += 2
+            if counter > 2 * n:
+                break
+            if root in roots or deg0[root]:
+                continue
+            found = True
+            break
+        if not found:
+            break
+        roots.append(root)
+    return roots
+
+
+# ----------------------------------------------------------------- BFS ----
+
+class BfsState:
+    """Bfs_State (src/traversal.h:18-28): pred int64[N], depth int32[N],
+    dist int64[N] (filled by bfs_compute_dist_from_pred) and the kernel's
+    workspace."""
+
+    def __init__(self, g: OnedGraph):
+        n = g.nglobalverts
+        dev = g.device
+        nb = C.c_uint64()
+        _check(lib.g5_bfs_workspace_size(n, C.byref(nb)))
+        self.work = _workspace(nb.value, dev)
+        self.pred = torch.empty(n, dtype=torch.int64, device=dev)
+        self.depth = torch.empty(n, dtype=torch.int32, device=dev)
+        self.dist: torch.Tensor | None = None
+        self.max_nlocalverts = n
+
+
+def oned_graph_bfs_create(g: OnedGraph) -> BfsState:
+    return BfsState(g)
+
+
+def oned_graph_bfs_run(g: OnedGraph, bfs: BfsState, root: int, params: BfsParams | None = None,
+                       with_depth: bool = True, stream=None) -> None:
+    """oned_graph_bfs_run (src/traversal.h:47): enqueues the whole BFS."""
+    _check(lib.g5_bfs_run(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, root, _ptr(bfs.pred),
+                          _ptr(bfs.depth) if with_depth else None, _ptr(bfs.work), bfs.work.numel(),
+                          C.byref(params) if params is not None else None, _stream(stream)))
+
+
+def bfs_stats(bfs: BfsState, stream=None) -> BfsStats:
+    s = BfsStats()
+    _check(lib.g5_bfs_last_stats(_ptr(bfs.work), bfs.work.numel(), C.byref(s), _stream(stream)))
+    return s
+
+
+def bfs_compute_dist_from_pred(g: OnedGraph, bfs: BfsState, root: int, stream=None) -> torch.Tensor:
+    """bfs_compute_dist_from_pred (src/traversal.h:48)."""
+    if bfs.dist is None:
+        bfs.dist = torch.empty(g.nglobalverts, dtype=torch.int64, device=g.device)
+    _check(lib.g5_bfs_dist_from_pred(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, _ptr(bfs.pred), root,
+                                     _ptr(bfs.dist), _ptr(bfs.work), bfs.work.numel(), _stream(stream)))
+    return bfs.dist
+
+
+# ---------------------------------------------------------------- SSSP ----
+
+class SsspState:
+    """Sssp_State (src/traversal.h:30-41): pred int64[N], dist float32[N]."""
+
+    def __init__(self, g: OnedGraph):
+        n = g.nglobalverts
+        dev = g.device
+        nb = C.c_uint64()
+        _check(lib.g5_sssp_workspace_size(n, C.byref(nb)))
+        self.work = _workspace(nb.value, dev)
+        self.pred = torch.empty(n, dtype=torch.int64, device=dev)
+        self.dist = torch.empty(n, dtype=torch.float32, device=dev)
+        self.max_nlocalverts = n
+
+
+def oned_graph_sssp_create(g: OnedGraph) -> SsspState:
+    return SsspState(g)
+
+
+def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,
+                        stream=None) -> None:
+    """oned_graph_sssp_run (src/traversal.h:52), delta 0.1 as the reference."""
+    p = SsspParams(delta, blocks)
+    _check(lib.g5_sssp_run(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
+                           g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
+                           sssp.work.numel(), C.byref(p), _stream(stream)))
+
+
+def sssp_status(sssp: SsspState, stream=None) -> tuple[int, int]:
+    b, ph = C.c_uint64(), C.c_uint64()
+    _check(lib.g5_sssp_last_status(_ptr(sssp.work), sssp.work.numel(), C.byref(b), C.byref(ph),
+                                   _stream(stream)))
+    return b.value, ph.value
+
+
+# ---------------------------------------------------------- validation ----
+
+def _val_work(g: OnedGraph) -> torch.Tensor:
+    nb = C.c_uint64()
+    _check(lib.g5_validate_workspace_size(g.nglobalverts, C.byref(nb)))
+    return _workspace(nb.value, g.device)
+
+
+def edge_count(g: OnedGraph, pred: torch.Tensor, work: torch.Tensor | None = None, stream=None) -> int:
+    """oned_graph_edge_count (examples/graph500_runner.cu:184-201)."""
+    work = _val_work(g) if work is None else work
+    out = C.c_uint64()
+    _check(lib.g5_edge_count(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, _ptr(pred), _ptr(work),
+                             work.numel(), C.byref(out), _stream(stream)))
+    return out.value
+
+
+def bfs_validate(g: OnedGraph, root: int, pred: torch.Tensor, dist: torch.Tensor,
+                 work: torch.Tensor | None = None, stream=None) -> int:
+    """Error count of oned_graph_bfs_validate (examples/graph500_runner.cu:203-255)."""
+    work = _val_work(g) if work is None else work
+    out = C.c_uint64()
+    _check(lib.g5_bfs_validate(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, root, _ptr(pred), _ptr(dist),
+                               _ptr(work), work.numel(), C.byref(out), _stream(stream)))
+    return out.value
+
+
+def sssp_validate(g: OnedGraph, root: int, dist: torch.Tensor, pred: torch.Tensor,
+                  work: torch.Tensor | None = None, stream=None) -> int:
+    """Error count of the SSSP rules (no counterpart in the reference)."""
+    work = _val_work(g) if work is None else work
+    out = C.c_uint64()
+    _check(lib.g5_sssp_validate(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), g.nglobalverts, root, _ptr(dist),
+                                _ptr(pred), _ptr(work), work.numel(), C.byref(out), _stream(stream)))
+    return out.value

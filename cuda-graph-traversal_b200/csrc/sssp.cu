@@ -1,0 +1,498 @@
+// sssp.cu -- K4: delta-stepping SSSP in one persistent cooperative kernel
+// (replaces the reference's host-driven oned_graph_sssp_run,
+// src/traversal.cu:638-711, and its kernels :211-340).
+//
+// Semantics kept from the reference: float32 relaxations cand = d[u] + w,
+// a distance is replaced only by a strictly smaller one, buckets
+// [b_k, b_{k+1}) with b_0 = 0 and b_{k+1} = b_k + delta accumulated in
+// float32 exactly as the reference's `bucket_max += delta`, light edges
+// (w < delta) relaxed to a fixed point inside a bucket before its heavy
+// edges.  With non-negative weights the float fixed point is unique, so the
+// distances equal the reference's bit for bit.
+//
+// Device-side structure:
+//   * dist and parent packed in one u64 (float bits << 32 | parent); a
+//     relaxation is one 64-bit atomicMin, which keeps the smallest distance
+//     and, among equal distances, the smallest parent -- no locks (the
+//     reference spins on a per-vertex lock, :224).
+//   * a ring of K bucket queues for the next K-1 buckets; a vertex enters a
+//     queue once per bucket (stamp per vertex), stale entries are dropped
+//     when the bucket opens.  No O(N) bucket scans (the reference scans all
+//     vertices per bucket, :297-331).
+//   * generation stamps for "already in this frontier" / "already in this
+//     bucket's heavy set", so nothing is cleared per iteration (the
+//     reference clears N visited flags per light iteration, :270-275).
+//   * a settled bitmap (N/8 bytes, L2 resident): edges into vertices of
+//     finished buckets are skipped without touching their distance.
+//   * frontiers are processed with the warp-gather / big-vertex sharing of
+//     the BFS kernel, over the light or the heavy part of each row.
+//
+// Algorithmic bytes per search: 2 m_c * (4 col + 4 w) + n_c * (8 rowstarts
+// + 8 packed dist/parent), plus 4 + 8 bytes per export.
+#include <algorithm>
+
+#include "g5_common.cuh"
+
+namespace g5 {
+
+constexpr int SSSP_THREADS = 256;
+constexpr int RING = 16;  // bucket queues; a relaxation may land at most RING-1 buckets ahead
+constexpr unsigned SBIG_DEG = 4096;
+constexpr unsigned SBIG_CHUNK = 1024;
+constexpr unsigned long long UNREACHED = ~0ull;
+
+struct SsspCtl {
+    unsigned bar;
+    unsigned error;
+    unsigned grab[3];    // per phase slot: cursor over the input list's small part
+    unsigned f_small[3]; // per phase slot: frontier produced for the next phase
+    unsigned f_big[3];
+    unsigned s_small[2]; // per bucket parity: heavy set
+    unsigned s_big[2];
+    unsigned ring_len[RING];
+    unsigned long long buckets;
+    unsigned long long phases;
+};
+
+struct SsspArgs {
+    const uint64_t *rowptr;
+    const int *col;
+    const float *w;
+    const unsigned *ld;  // light degree per vertex (partitioned rows) or nullptr
+    uint64_t n;
+    unsigned root;
+    float delta;
+    unsigned long long *pack;
+    unsigned *fstamp, *sstamp, *qstamp;
+    unsigned *settled;
+    unsigned *F[2], *FB[2];
+    unsigned *S[2], *SB[2];
+    unsigned *ring;
+    SsspCtl *ctl;
+    unsigned nblocks;
+    unsigned long long limit_ns;
+};
+
+__device__ __forceinline__ float pack_dist(unsigned long long p) { return __uint_as_float((unsigned)(p >> 32)); }
+
+// Row range [b, e) of u's light (heavy = false) or heavy part.  Without
+// partition data the whole row is returned and the caller filters by weight.
+__device__ __forceinline__ void part_range(const SsspArgs &a, unsigned u, bool heavy, uint64_t &b, uint64_t &e) {
+    b = __ldg(&a.rowptr[u]);
+    e = __ldg(&a.rowptr[u + 1]);
+    if (a.ld) {
+        const uint64_t mid = b + __ldg(&a.ld[u]);
+        if (heavy) b = mid;
+        else e = mid;
+    }
+}
+
+struct PushCtx {
+    unsigned pid;        // id of the producing phase (frontier stamp)
+    unsigned bucket;     // current bucket index (heavy-set stamp)
+    int f_slot;          // counter slot of the produced frontier
+    unsigned *Fout, *FBout;
+    unsigned *Sl, *SBl;  // heavy set of the current bucket
+    int s_par;
+    const float *bnd;    // shared: b_B .. b_{B+RING}
+};
+
+// Appends v to the produced frontier and to the bucket's heavy set (each at
+// most once).  All 32 lanes call it.
+__device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCtx &x, bool want, unsigned v) {
+    SsspCtl *c = a.ctl;
+    bool f = want && atomicExch(&a.fstamp[v], x.pid) != x.pid;
+    bool s = want && atomicExch(&a.sstamp[v], x.bucket) != x.bucket;
+    uint64_t lb = 0, le = 0, hb = 0, he = 0;
+    if (f) part_range(a, v, false, lb, le);
+    if (s) part_range(a, v, true, hb, he);
+    const bool fs = f && le - lb <= SBIG_DEG, fb = f && le - lb > SBIG_DEG;
+    const bool ss = s && he - hb <= SBIG_DEG, sb = s && he - hb > SBIG_DEG;
+    // Each vertex enters a frontier once per phase and a heavy set once per
+    // bucket, so no list exceeds n entries; the guards only keep a broken
+    // invariant from writing outside the lists.
+    unsigned p = warp_append(&c->f_small[x.f_slot], fs);
+    if (fs && p < a.n) x.Fout[p] = v;
+    p = warp_append(&c->f_big[x.f_slot], fb);
+    if (fb && p < a.n) {
+        x.Fout[a.n - 1 - p] = v;
+        x.FBout[p] = 0;
+    }
+    p = warp_append(&c->s_small[x.s_par], ss);
+    if (ss && p < a.n) x.Sl[p] = v;
+    p = warp_append(&c->s_big[x.s_par], sb);
+    if (sb && p < a.n) {
+        x.Sl[a.n - 1 - p] = v;
+        x.SBl[p] = 0;
+    }
+}
+
+// Relaxes u -> v with float weight wt from distance du; queues v when its
+// distance dropped.  All 32 lanes call it (want = lane has an edge).
+__device__ __forceinline__ void relax(const SsspArgs &a, const PushCtx &x, bool want, unsigned u, float du, unsigned v,
+                                      float wt, bool heavy_phase) {
+    bool same = false;
+    int target = -1;
+    if (want && v >= a.n) {  // not a vertex: report it, touch nothing
+        atomicOr(&a.ctl->error, DEVERR_RANGE);
+        want = false;
+    }
+    if (want && !((__ldcg(&a.settled[v >> 5]) >> (v & 31)) & 1u)) {
+        const float cand = __fadd_rn(du, wt);
+        const unsigned long long np = ((unsigned long long)__float_as_uint(cand) << 32) | u;
+        if (np < __ldcg(&a.pack[v])) {
+            const unsigned long long old = atomicMin(&a.pack[v], np);
+            if (np < old && (old >> 32) != (np >> 32)) {
+                if (cand < x.bnd[1]) {
+                    same = true;
+                    if (heavy_phase) atomicOr(&a.ctl->error, DEVERR_CAPACITY);  // cannot happen: w >= delta
+                } else {
+                    // Largest j with b_{B+j} <= cand; the ring holds B+1 .. B+RING-1.
+                    int j = 1;
+                    while (j < RING && x.bnd[j + 1] <= cand) ++j;
+                    if (j >= RING) atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+                    else target = (int)x.bucket + j;
+                }
+            }
+        }
+    }
+    push_same_bucket(a, x, same && !heavy_phase, v);
+    // Ring queue of the target bucket, once per (vertex, bucket).
+    const bool r = target >= 0 && atomicExch(&a.qstamp[v], (unsigned)target) != (unsigned)target;
+    const int slot = r ? target % RING : RING;
+    const unsigned grp = __match_any_sync(FULL, slot);
+    if (r) {
+        const unsigned leader = __ffs(grp) - 1;
+        unsigned base = 0;
+        if (lane_id() == leader) base = atomicAdd(&a.ctl->ring_len[slot], (unsigned)__popc(grp));
+        base = __shfl_sync(grp, base, leader);
+        const uint64_t at = (uint64_t)base + __popc(grp & lanemask_lt());
+        if (at < a.n) a.ring[(uint64_t)slot * a.n + at] = v;
+        else atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+    }
+}
+
+// Relaxes the light (heavy = false) or heavy edges of every vertex of list L
+// (small part [0, ns), big part at the back [n-nb, n)).
+__device__ void expand_list(const SsspArgs &a, const PushCtx &x, const unsigned *L, unsigned ns, unsigned nb,
+                            unsigned *bigcur, unsigned *grab, bool heavy) {
+    const unsigned lane = lane_id();
+    const bool filtered = a.ld == nullptr;
+    for (;;) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(grab, 32u);
+        base = __shfl_sync(FULL, base, 0);
+        if (base >= ns) break;
+        const unsigned i = base + lane;
+        const bool valid = i < ns;
+        const unsigned u = valid ? __ldcg(&L[i]) : 0u;
+        uint64_t rb = 0, re = 0;
+        float du = 0.0f;
+        if (valid) {
+            part_range(a, u, heavy, rb, re);
+            du = pack_dist(__ldcg(&a.pack[u]));
+            if (heavy) atomicOr(&a.settled[u >> 5], 1u << (u & 31));
+        }
+        const unsigned deg = (unsigned)(re - rb);
+        const unsigned incl = warp_incl_scan(deg);
+        const unsigned total = __shfl_sync(FULL, incl, 31);
+        const unsigned excl = incl - deg;
+        for (unsigned e0 = 0; e0 < total; e0 += 32) {
+            const unsigned e = e0 + lane;
+            bool has = e < total;
+            const int j = warp_owner(excl, has ? e : total - 1);
+            const unsigned uj = __shfl_sync(FULL, u, j);
+            const uint64_t rbj = __shfl_sync(FULL, rb, j);
+            const unsigned exj = __shfl_sync(FULL, excl, j);
+            const float duj = __shfl_sync(FULL, du, j);
+            unsigned v = 0;
+            float wt = 0.0f;
+            if (has) {
+                const uint64_t at = rbj + (e - exj);
+                v = (unsigned)__ldg(&a.col[at]);
+                wt = __ldg(&a.w[at]);
+                if (filtered) has = heavy ? !(wt < a.delta) : wt < a.delta;
+            }
+            relax(a, x, has, uj, duj, v, wt, heavy);
+        }
+    }
+    for (unsigned j = 0; j < nb; ++j) {
+        const unsigned u = __ldcg(&L[a.n - 1 - j]);
+        uint64_t rb, re;
+        part_range(a, u, heavy, rb, re);
+        const float du = pack_dist(__ldcg(&a.pack[u]));
+        const uint64_t deg = re - rb;
+        for (;;) {
+            unsigned cs = 0;
+            if (lane == 0) cs = atomicAdd(&bigcur[j], SBIG_CHUNK);
+            cs = __shfl_sync(FULL, cs, 0);
+            if (cs >= deg) break;
+            if (heavy && cs == 0 && lane == 0) atomicOr(&a.settled[u >> 5], 1u << (u & 31));
+            const uint64_t ce = min((uint64_t)cs + SBIG_CHUNK, deg);
+            for (uint64_t e = cs + lane; e < (uint64_t)cs + SBIG_CHUNK; e += 32) {
+                bool has = e < ce;
+                unsigned v = 0;
+                float wt = 0.0f;
+                if (has) {
+                    v = (unsigned)__ldg(&a.col[rb + e]);
+                    wt = __ldg(&a.w[rb + e]);
+                    if (filtered) has = heavy ? !(wt < a.delta) : wt < a.delta;
+                }
+                relax(a, x, has, u, du, v, wt, heavy);
+            }
+        }
+        // A big vertex without heavy edges is still settled.
+        if (heavy && deg == 0 && lane == 0) atomicOr(&a.settled[u >> 5], 1u << (u & 31));
+    }
+}
+
+__global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspArgs a) {
+    SsspCtl *c = a.ctl;
+    __shared__ float s_bnd[RING + 1];
+    unsigned epoch = 0;
+    const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+
+    if (gtid == 0) {
+        a.pack[a.root] = (unsigned long long)a.root;  // distance 0.0f, parent = root
+        a.ring[0] = a.root;
+        a.qstamp[a.root] = 0;
+        c->ring_len[0] = 1;
+    }
+    if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+
+    unsigned bucket = 0, phase = 0;
+    float blo = 0.0f;
+    unsigned long long nbuckets = 0;
+    for (;;) {
+        // ---- open the bucket: its ring queue becomes the first frontier.
+        if (threadIdx.x == 0) {
+            float b = blo;
+            for (int j = 0; j <= RING; ++j) {
+                s_bnd[j] = b;
+                b = __fadd_rn(b, a.delta);
+            }
+        }
+        __syncthreads();
+        PushCtx x;
+        x.bucket = bucket;
+        x.bnd = s_bnd;
+        x.s_par = bucket & 1;
+        x.Sl = a.S[bucket & 1];
+        x.SBl = a.SB[bucket & 1];
+        {
+            const int s_nxt = (phase + 1) % 3, s_clr = (phase + 2) % 3;
+            if (gtid == 0) {
+                c->grab[s_clr] = c->f_small[s_clr] = c->f_big[s_clr] = 0;
+                c->s_small[(bucket + 1) & 1] = c->s_big[(bucket + 1) & 1] = 0;
+            }
+            x.pid = phase;
+            x.f_slot = s_nxt;
+            x.Fout = a.F[(phase + 1) & 1];
+            x.FBout = a.FB[(phase + 1) & 1];
+            const unsigned slot = bucket % RING;
+            const unsigned len = ld_volatile(&c->ring_len[slot]);
+            const unsigned *R = a.ring + (uint64_t)slot * a.n;
+            for (uint64_t base = gtid - lane_id(); base < len; base += nthreads) {
+                const uint64_t i = base + lane_id();
+                bool ok = false;
+                unsigned v = 0;
+                if (i < len) {
+                    v = __ldcg(&R[i]);
+                    const float d = pack_dist(__ldcg(&a.pack[v]));
+                    ok = d >= s_bnd[0] && d < s_bnd[1] && !((__ldcg(&a.settled[v >> 5]) >> (v & 31)) & 1u);
+                }
+                push_same_bucket(a, x, ok, v);
+            }
+            if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+            // The queue is consumed; nothing can target this slot again before
+            // bucket + RING, which lies beyond every push of this bucket.
+            if (gtid == 0) c->ring_len[slot] = 0;
+            ++phase;
+        }
+        // ---- light iterations until the bucket's frontier is empty.
+        for (;;) {
+            const int s_cur = phase % 3, s_nxt = (phase + 1) % 3, s_clr = (phase + 2) % 3;
+            const unsigned ns = ld_volatile(&c->f_small[s_cur]), nb = ld_volatile(&c->f_big[s_cur]);
+            if (ns + nb == 0) break;
+            if (gtid == 0) c->grab[s_clr] = c->f_small[s_clr] = c->f_big[s_clr] = 0;
+            x.pid = phase;
+            x.f_slot = s_nxt;
+            x.Fout = a.F[(phase + 1) & 1];
+            x.FBout = a.FB[(phase + 1) & 1];
+            expand_list(a, x, a.F[phase & 1], ns, nb, a.FB[phase & 1], &c->grab[s_cur], false);
+            if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+            ++phase;
+        }
+        // ---- heavy edges of every vertex settled in this bucket.
+        {
+            const int s_cur = phase % 3, s_nxt = (phase + 1) % 3, s_clr = (phase + 2) % 3;
+            if (gtid == 0) c->grab[s_clr] = c->f_small[s_clr] = c->f_big[s_clr] = 0;
+            x.pid = phase;
+            x.f_slot = s_nxt;
+            x.Fout = a.F[(phase + 1) & 1];
+            x.FBout = a.FB[(phase + 1) & 1];
+            const unsigned ns = ld_volatile(&c->s_small[bucket & 1]), nb = ld_volatile(&c->s_big[bucket & 1]);
+            expand_list(a, x, a.S[bucket & 1], ns, nb, a.SB[bucket & 1], &c->grab[s_cur], true);
+            if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+            ++phase;
+        }
+        ++nbuckets;
+        // ---- next non-empty bucket within the ring window.
+        int step = 0;
+        for (int j = 1; j < RING; ++j)
+            if (ld_volatile(&c->ring_len[(bucket + j) % RING])) {
+                step = j;
+                break;
+            }
+        if (!step) break;
+        for (int j = 0; j < step; ++j) blo = __fadd_rn(blo, a.delta);
+        bucket += step;
+        __syncthreads();  // s_bnd is rewritten at the top of the loop
+    }
+    if (gtid == 0) {
+        c->buckets = nbuckets;
+        c->phases = phase;
+    }
+}
+
+__global__ void sssp_export_kernel(const unsigned long long *__restrict__ pack, uint64_t n, float *__restrict__ dist,
+                                   int64_t *__restrict__ pred) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        const unsigned long long p = pack[v];
+        dist[v] = p == UNREACHED ? -1.0f : pack_dist(p);
+        pred[v] = p == UNREACHED ? -1 : (int64_t)(unsigned)p;
+    }
+}
+
+struct SsspWork {
+    SsspCtl *ctl;
+    unsigned long long *pack;
+    unsigned *fstamp, *sstamp, *qstamp, *settled;
+    unsigned *F[2], *FB[2], *S[2], *SB[2];
+    unsigned *ring;
+    uint64_t bytes;
+};
+
+static SsspWork carve_sssp(void *base, uint64_t n) {
+    Carver c(base);
+    SsspWork w;
+    w.ctl = c.take<SsspCtl>(1);
+    w.pack = c.take<unsigned long long>(n);
+    w.fstamp = c.take<unsigned>(n);
+    w.sstamp = c.take<unsigned>(n);
+    w.qstamp = c.take<unsigned>(n);
+    w.settled = c.take<unsigned>((n + 31) / 32);
+    for (int i = 0; i < 2; ++i) {
+        w.F[i] = c.take<unsigned>(n);
+        w.FB[i] = c.take<unsigned>(n);
+        w.S[i] = c.take<unsigned>(n);
+        w.SB[i] = c.take<unsigned>(n);
+    }
+    w.ring = c.take<unsigned>((uint64_t)RING * n);
+    w.bytes = c.used;
+    return w;
+}
+
+static int sssp_max_blocks(int *out) {
+    static int cached[64] = {};
+    DeviceInfo di;
+    int rc = device_info(&di);
+    if (rc) return rc;
+    if (!cached[di.device]) {
+        int per_sm = 0;
+        G5_CUDA_TRY(
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_persistent_kernel, SSSP_THREADS, 0));
+        cached[di.device] = std::max(1, per_sm) * di.sms;
+    }
+    *out = cached[di.device];
+    return G5_OK;
+}
+
+}  // namespace g5
+
+using namespace g5;
+
+extern "C" int g5_sssp_workspace_size(uint64_t nverts, uint64_t *bytes) {
+    G5_CHECK_ARG(bytes, "g5_sssp_workspace_size: bytes is NULL");
+    *bytes = carve_sssp(nullptr, nverts).bytes;
+    return G5_OK;
+}
+
+extern "C" int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
+                           const uint32_t *d_light_deg, float light_delta, uint64_t nverts, uint64_t root,
+                           float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes,
+                           const g5_sssp_params *params, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_sssp_run: nverts outside [1, 2^31]");
+    G5_CHECK_ARG(root < nverts, "g5_sssp_run: root %llu outside [0, %llu)", (unsigned long long)root,
+                 (unsigned long long)nverts);
+    G5_CHECK_ARG(d_rowstarts && d_col && d_w && d_dist && d_pred && d_work, "g5_sssp_run: NULL argument");
+    SsspWork w = carve_sssp(d_work, nverts);
+    if (work_bytes < w.bytes)
+        return set_error(G5_ERR_WORKSPACE, "g5_sssp_run: workspace %llu < %llu bytes", (unsigned long long)work_bytes,
+                         (unsigned long long)w.bytes);
+    g5_sssp_params p = {0.1f, 0};
+    if (params) p = *params;
+    G5_CHECK_ARG(p.delta > 0.0f, "g5_sssp_run: delta must be positive");
+
+    int max_blocks = 0;
+    int rc = sssp_max_blocks(&max_blocks);
+    if (rc) return rc;
+    int blocks = p.blocks > 0 ? std::min(p.blocks, max_blocks)
+                              : (int)std::min<uint64_t>(max_blocks, std::max<uint64_t>(1, nverts / 2048));
+
+    cudaStream_t st = (cudaStream_t)stream;
+    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(SsspCtl), st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.pack, 0xff, nverts * sizeof(unsigned long long), st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.fstamp, 0xff, nverts * sizeof(unsigned), st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.sstamp, 0xff, nverts * sizeof(unsigned), st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.qstamp, 0xff, nverts * sizeof(unsigned), st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.settled, 0, (nverts + 31) / 32 * sizeof(unsigned), st));
+
+    SsspArgs a;
+    a.rowptr = d_rowstarts;
+    a.col = d_col;
+    a.w = d_w;
+    a.ld = (d_light_deg && p.delta == light_delta) ? d_light_deg : nullptr;
+    a.n = nverts;
+    a.root = (unsigned)root;
+    a.delta = p.delta;
+    a.pack = w.pack;
+    a.fstamp = w.fstamp;
+    a.sstamp = w.sstamp;
+    a.qstamp = w.qstamp;
+    a.settled = w.settled;
+    for (int i = 0; i < 2; ++i) {
+        a.F[i] = w.F[i];
+        a.FB[i] = w.FB[i];
+        a.S[i] = w.S[i];
+        a.SB[i] = w.SB[i];
+    }
+    a.ring = w.ring;
+    a.ctl = w.ctl;
+    a.nblocks = (unsigned)blocks;
+    a.limit_ns = wait_limit_ns();
+    void *args[] = {&a};
+    G5_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)sssp_persistent_kernel, dim3(blocks), dim3(SSSP_THREADS),
+                                            args, 0, st));
+    DeviceInfo di;
+    if ((rc = device_info(&di))) return rc;
+    sssp_export_kernel<<<di.sms * 8, 256, 0, st>>>(w.pack, nverts, d_dist, d_pred);
+    G5_CUDA_TRY(cudaGetLastError());
+    return G5_OK;
+}
+
+extern "C" int g5_sssp_last_status(const void *d_work, uint64_t work_bytes, uint64_t *buckets, uint64_t *phases,
+                                   void *stream) {
+    clear_error();
+    G5_CHECK_ARG(d_work && work_bytes >= sizeof(SsspCtl), "g5_sssp_last_status: bad workspace");
+    SsspCtl c;
+    cudaStream_t st = (cudaStream_t)stream;
+    G5_CUDA_TRY(cudaMemcpyAsync(&c, d_work, sizeof c, cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    if (buckets) *buckets = c.buckets;
+    if (phases) *phases = c.phases;
+    return deverr_to_status(c.error, "g5_sssp_run");
+}

@@ -1,0 +1,189 @@
+/*
+ * g500b.h -- C ABI of the B200 Graph500 hot path (libg500b.so).
+ *
+ * Plain pointers and sizes only.  Arrays named d_* live in device memory of
+ * the calling thread's current CUDA device; `stream` is a cudaStream_t (NULL
+ * = legacy default stream).  Every call is stream-ordered: it enqueues its
+ * work and returns, except where it hands a value back through a host
+ * pointer (those synchronise `stream` first).  Scratch memory is supplied
+ * by the caller as (d_work, work_bytes); the matching *_workspace_size call
+ * says how much, and nothing here calls cudaMalloc on the hot path.
+ *
+ * Every function returns G5_OK (0) or a negative G5_ERR_* code; the message
+ * of the last failure on this host thread is g5_last_error().
+ *
+ * Each entry point names the function of RuanPetrus/cuda-graph-traversal it
+ * replaces.  The reference's own C++ API (the src/ headers) is provided on top of
+ * these calls by the compatibility layer (include/compat/).
+ */
+#ifndef G500B_H
+#define G500B_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    G5_OK = 0,
+    G5_ERR_INVALID = -1,   /* bad argument: range, null pointer, size        */
+    G5_ERR_WORKSPACE = -2, /* work_bytes below the *_workspace_size answer   */
+    G5_ERR_CUDA = -3,      /* a CUDA runtime call failed                     */
+    G5_ERR_TIMEOUT = -4,   /* a bounded device-side wait gave up             */
+    G5_ERR_DEVICE = -5,    /* a kernel reported an internal consistency error */
+};
+
+/* Message of the last error on this host thread ("" if none). */
+const char *g5_last_error(void);
+/* Library version string. */
+const char *g5_version(void);
+
+/* ---------------------------------------------------------------- MRG ---- */
+
+/* make_mrg_seed, src/graph_generation.h:39 (src/graph_generation.cu:248-254). */
+int g5_make_mrg_seed(uint64_t userseed1, uint64_t userseed2, uint32_t seed[5]);
+
+/* make_random_numbers, src/graph_generation.h:40 (src/graph_generation.cu:256-266). */
+int g5_make_random_numbers(int64_t nvalues, uint64_t userseed1, uint64_t userseed2, int64_t position,
+                           double *result);
+
+/* The two vertex-scrambling keys generate_kronecker_range derives from the
+ * seed (src/graph_generation.cu:290-300). */
+int g5_scramble_keys(const uint32_t seed[5], uint64_t *val0, uint64_t *val1);
+
+/* ----------------------------------------------------------- generator --- */
+
+/* generate_kronecker_range, src/graph_generation.h:33-37
+ * (src/graph_generation.cu:269-310): Graph500 Kronecker edges
+ * [start_edge, end_edge) of a 2^log_n-vertex graph.  d_edges receives
+ * (v0, v1) u64 pairs (the Packed_Edge layout, 16 bytes per edge), d_weights
+ * one float per edge.  Any sub-range reproduces the same edges. */
+int g5_generate_kronecker_range(const uint32_t seed[5], uint32_t log_n, int64_t start_edge, int64_t end_edge,
+                                uint64_t *d_edges, float *d_weights, void *stream);
+
+/* ----------------------------------------------------------------- CSR --- */
+
+/* Scratch bytes for g5_csr_count + g5_csr_fill on nverts vertices. */
+int g5_csr_workspace_size(uint64_t nverts, uint64_t nedges, uint64_t *bytes);
+
+/* First half of oned_graph_from_tuple_graph, src/traversal.h:43
+ * (src/traversal.cu:342-368: compute_degrees_kernel + rowstarts scan):
+ * d_rowstarts[0..nverts] = exclusive prefix of the non-self-loop degree of
+ * every vertex.  *nentries (host) = d_rowstarts[nverts], the number of
+ * directed CSR entries; the call synchronises `stream`. */
+int g5_csr_count(const uint64_t *d_edges, uint64_t nedges, uint64_t nverts, uint64_t *d_rowstarts,
+                 void *d_work, uint64_t work_bytes, uint64_t *nentries, void *stream);
+
+/* Second half (src/traversal.cu:369-389, fill_csr_kernel): both directions
+ * of every non-self-loop edge into its row, duplicates kept.  Within a row,
+ * entries with weight < light_delta come first (their count per vertex goes
+ * to d_light_deg, optional) and the rest after; d_col receives int32 vertex
+ * ids, d_w the weights and d_col64 (optional) the same ids as u64, the
+ * reference's Oned_Graph.column type.  Uses the workspace state left by
+ * g5_csr_count. */
+int g5_csr_fill(const uint64_t *d_edges, const float *d_weights, uint64_t nedges, uint64_t nverts,
+                const uint64_t *d_rowstarts, float light_delta, void *d_work, uint64_t work_bytes,
+                int32_t *d_col, float *d_w, uint64_t *d_col64, uint32_t *d_light_deg, void *stream);
+
+/* ----------------------------------------------------------------- BFS --- */
+
+typedef struct g5_bfs_params {
+    float alpha;    /* top-down -> bottom-up when frontier edges > unvisited edges / alpha (default 14)  */
+    float beta;     /* bottom-up -> top-down when frontier vertices < nverts / beta (default 24)         */
+    int32_t mode;   /* 0 = direction-optimizing, 1 = top-down only, 2 = bottom-up after level 0         */
+    int32_t blocks; /* persistent grid size; 0 = fill the device                                          */
+} g5_bfs_params;
+
+typedef struct g5_bfs_stats {
+    int32_t levels;           /* BFS levels expanded                           */
+    int32_t bottom_up_levels; /* of which bottom-up                            */
+    uint64_t reached;         /* vertices with a parent (root included)        */
+} g5_bfs_stats;
+
+int g5_bfs_workspace_size(uint64_t nverts, uint64_t *bytes);
+
+/* oned_graph_bfs_run, src/traversal.h:47 (src/traversal.cu:479-503): BFS
+ * from root over the CSR (d_rowstarts u64[nverts+1], d_col int32).
+ * d_pred[v] = parent (int64), -1 when unreached, root for the root;
+ * d_depth[v] (optional, int32) = level, -1 when unreached.  One persistent
+ * cooperative kernel runs every level; nothing returns to the host.
+ * params NULL = defaults. */
+int g5_bfs_run(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
+               int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
+               const g5_bfs_params *params, void *stream);
+
+/* Statistics of the last g5_bfs_run that used this workspace (synchronises). */
+int g5_bfs_last_stats(const void *d_work, uint64_t work_bytes, g5_bfs_stats *stats, void *stream);
+
+/* bfs_compute_dist_from_pred, src/traversal.h:48 (src/traversal.cu:505-563):
+ * d_dist[v] = -1 where pred is -1, 0 at the root, the tree depth where the
+ * parent chain reaches the root through CSR edges, INT64_MAX otherwise. */
+int g5_bfs_dist_from_pred(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
+                          const int64_t *d_pred, uint64_t root, int64_t *d_dist, void *d_work,
+                          uint64_t work_bytes, void *stream);
+
+/* ---------------------------------------------------------------- SSSP --- */
+
+typedef struct g5_sssp_params {
+    float delta;    /* bucket width (default 0.1, the reference's fixed value) */
+    int32_t blocks; /* persistent grid size; 0 = fill the device              */
+} g5_sssp_params;
+
+int g5_sssp_workspace_size(uint64_t nverts, uint64_t *bytes);
+
+/* oned_graph_sssp_run, src/traversal.h:52 (src/traversal.cu:638-711):
+ * delta-stepping with float32 relaxations.  d_dist[v] = distance, -1.0f when
+ * unreached; d_pred[v] = a parent on a shortest path, -1 when unreached.
+ * d_light_deg (optional) = per-vertex count of leading row entries lighter
+ * than `light_delta` as produced by g5_csr_fill; it is used only when
+ * params->delta == light_delta. */
+int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, const uint32_t *d_light_deg,
+                float light_delta, uint64_t nverts, uint64_t root, float *d_dist, int64_t *d_pred, void *d_work,
+                uint64_t work_bytes, const g5_sssp_params *params, void *stream);
+
+/* Buckets and phases of the last g5_sssp_run that used this workspace, and
+ * its device status (synchronises). */
+int g5_sssp_last_status(const void *d_work, uint64_t work_bytes, uint64_t *buckets, uint64_t *phases, void *stream);
+
+/* ---------------------------------------------------------- validation --- */
+
+int g5_validate_workspace_size(uint64_t nverts, uint64_t *bytes);
+
+/* oned_graph_edge_count, examples/graph500_runner.cu:171-201: number of CSR
+ * entries col[e] <= v over rows of vertices with pred[v] != -1 (the TEPS
+ * edge count).  Synchronises. */
+int g5_edge_count(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, const int64_t *d_pred,
+                  void *d_work, uint64_t work_bytes, uint64_t *count, void *stream);
+
+/* oned_graph_bfs_validate, examples/graph500_runner.cu:203-255 (rules 1-7 of
+ * :84-169): *errors = number of violations; 0 means the parent tree and the
+ * depths (from g5_bfs_dist_from_pred) are a valid BFS.  Synchronises. */
+int g5_bfs_validate(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
+                    const int64_t *d_pred, const int64_t *d_dist, void *d_work, uint64_t work_bytes,
+                    uint64_t *errors, void *stream);
+
+/* SSSP validation (the reference has none): root at 0 with itself as parent;
+ * pred = -1 exactly where dist = -1; no edge from a reached vertex leads to
+ * an unreached one or can still be relaxed (dist[u] + w < dist[v] in float);
+ * every reached non-root v has an edge (pred[v], v, w) with
+ * dist[pred[v]] + w == dist[v].  Synchronises. */
+int g5_sssp_validate(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, uint64_t nverts,
+                     uint64_t root, const float *d_dist, const int64_t *d_pred, void *d_work, uint64_t work_bytes,
+                     uint64_t *errors, void *stream);
+
+/* ------------------------------------------------------------- testing --- */
+
+/* Launches a two-block cooperative kernel whose grid barrier can never
+ * complete, so each block's bounded wait gives up after limit_ms: returns
+ * G5_ERR_TIMEOUT and leaves the context usable.  It exercises the failure
+ * path every persistent kernel here shares (no counterpart in the reference,
+ * whose grid barrier spins without a bound, src/traversal.cu:126).
+ * d_work needs 8 bytes. */
+int g5_selftest_wait_timeout(unsigned limit_ms, void *d_work, uint64_t work_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* G500B_H */
