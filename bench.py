@@ -1,0 +1,394 @@
+#!/usr/bin/env python3
+"""Graph500 BFS / SSSP benchmark on B200 (harmonic-mean GTEPS).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--scale S] [--impl ours|reference]
+
+A step is one BFS from one Graph500 root (the runner's root choice,
+examples/graph500_runner.cu:43-74) over the SCALE-S, edgefactor-16 Kronecker
+graph generated and built into a CSR on the GPU beforehand.  `value` is the
+harmonic-mean GTEPS of the K timed roots (nedge / time per root, nedge as the
+reference's runner counts it), timed on the device with CUDA events;
+between steps the working set (an 8.6 GB column array at SCALE 26) is far
+larger than L2.  SSSP is timed the same way and reported under "sssp".
+
+With N > 1 (torchrun, one rank per GPU) every rank holds its own copy of the
+graph and takes every N-th root: weak scaling with no data-path collective;
+`value` is all edges traversed / the slowest rank's time.
+
+--impl reference times the reference algorithm's CPU implementation (the
+reference has no CPU path of its own, so this is the oracle restatement in
+oracle/) on all host cores, on the same workload, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+PEAKS = os.path.join(REPO, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def load_package():
+    if "cgt_b200" in sys.modules:
+        return sys.modules["cgt_b200"]
+    spec = importlib.util.spec_from_file_location("cgt_b200", os.path.join(REPO, "cuda-graph-traversal_b200", "__init__.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["cgt_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def metric_name(scale, ef):
+    return f"harmonic-mean BFS GTEPS at SCALE {scale} ef{ef} (1 B200)"
+
+
+def hmean_gteps(nedge, secs):
+    nedge = np.asarray(nedge, np.float64)
+    secs = np.asarray(secs, np.float64)
+    return float(1.0 / np.mean(secs / nedge) / 1e9)
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"g5_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(rows[0][1]) if rows[0][1].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+        pg = dist
+    G = load_package()
+    scale, ef = args.scale, args.edgefactor
+    n, m = 1 << scale, ef << scale
+    stream = torch.cuda.current_stream()
+
+    # ---- setup (untimed): generation + CSR build on the GPU, as the runner.
+    t0 = time.time()
+    seed = G.make_mrg_seed(2, 3)
+    ev0, ev1, ev2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    ev0.record()
+    tg = G.generate_kronecker_range(seed, scale, 0, m, device=dev)
+    ev1.record()
+    g = G.oned_graph_from_tuple_graph(tg, n)
+    ev2.record()
+    torch.cuda.synchronize()
+    gen_s, csr_s = ev0.elapsed_time(ev1) / 1e3, ev1.elapsed_time(ev2) / 1e3
+    del tg
+    torch.cuda.empty_cache()
+    roots_all = G.generate_bfs_roots(g, 2, 3, 64)
+    my_roots = roots_all[rank::world] or roots_all
+    K, W = args.steps, args.warmup
+    seq = [my_roots[i % len(my_roots)] for i in range(W + K)]
+    bfs = G.BfsState(g)
+    vw = G._val_work(g)
+    nedge, reached = {}, {}
+    for r in set(seq):
+        G.oned_graph_bfs_run(g, bfs, r, with_depth=False)
+        st = G.bfs_stats(bfs)
+        reached[r] = st.reached
+        nedge[r] = G.edge_count(g, bfs.pred, vw)
+    # Validate one tree per root set (untimed).
+    r0 = seq[0]
+    G.oned_graph_bfs_run(g, bfs, r0)
+    dist = G.bfs_compute_dist_from_pred(g, bfs, r0)
+    assert G.bfs_validate(g, r0, bfs.pred, dist, vw) == 0, "BFS validation failed"
+    setup_s = time.time() - t0
+
+    # ---- timed BFS: K roots back to back on one stream, events per step.
+    for r in seq[:W]:
+        G.oned_graph_bfs_reset(bfs, with_depth=False)
+        G.oned_graph_bfs_traverse(g, bfs, r, with_depth=False)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+            torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    with clocks:
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record()
+        for i, r in enumerate(seq[W:]):
+            a, b, c = evs[i]
+            a.record()
+            G.oned_graph_bfs_reset(bfs, with_depth=False)
+            b.record()
+            G.oned_graph_bfs_traverse(g, bfs, r, with_depth=False)
+            c.record()
+        stop.record()
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+    total_ms = start.elapsed_time(stop)
+    step_s = [a.elapsed_time(c) / 1e3 for a, _, c in evs]
+    kern_s = [b.elapsed_time(c) / 1e3 for _, b, c in evs]
+    timed = seq[W:]
+    t_nedge = [nedge[r] for r in timed]
+    hm = hmean_gteps(t_nedge, step_s)
+    st = G.bfs_stats(bfs)
+    assert st.reached == reached[timed[-1]]
+
+    # Roofline of the persistent BFS kernel: algorithmic bytes per search =
+    # 2*nedge*4 (int32 col) + reached*(8 rowstarts + 8 pred) (no depth array).
+    alg_bytes = [2 * nedge[r] * 4 + reached[r] * 16 for r in timed]
+    achieved_gbs = float(np.sum(alg_bytes) / np.sum(kern_s) / 1e9)
+    peak, peak_kind = hbm_peak()
+
+    # ---- SSSP, same roots.
+    sssp = G.SsspState(g)
+    for r in seq[:W]:
+        G.oned_graph_sssp_run(g, sssp, r)
+    sev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    torch.cuda.synchronize()
+    for i, r in enumerate(timed):
+        sev[i][0].record()
+        G.oned_graph_sssp_run(g, sssp, r)
+        sev[i][1].record()
+    torch.cuda.synchronize()
+    G.sssp_status(sssp)
+    s_secs = [a.elapsed_time(b) / 1e3 for a, b in sev]
+    s_hm = hmean_gteps(t_nedge, s_secs)
+    r_last = timed[-1]
+    assert G.sssp_validate(g, r_last, sssp.dist, sssp.pred, vw) == 0, "SSSP validation failed"
+
+    # ---- end to end through the C ABI with host buffers: per step the root
+    # goes host->device from pinned memory, the BFS runs, and the step's
+    # result (its statistics: levels and reached count) comes back.
+    root_host = torch.empty(1, dtype=torch.int64, pin_memory=True)
+    root_dev = torch.empty(1, dtype=torch.int64, device=dev)
+    e2e_s = []
+    torch.cuda.synchronize()
+    for r in timed:
+        t = time.perf_counter()
+        root_host[0] = r
+        root_dev.copy_(root_host, non_blocking=True)
+        G.oned_graph_bfs_run(g, bfs, int(r), with_depth=False)
+        res = G.bfs_stats(bfs)  # device -> host read of the result, synchronises
+        e2e_s.append(time.perf_counter() - t)
+        assert res.reached == reached[r]
+    e2e_hm = hmean_gteps(t_nedge, e2e_s)
+
+    # Whole-job numbers across ranks: slowest rank's time, all ranks' edges.
+    tot_edges = float(np.sum(t_nedge))
+    max_ms = total_ms
+    if pg:
+        t = torch.tensor([total_ms, tot_edges], dtype=torch.float64, device=dev)
+        mx = t.clone()
+        pg.all_reduce(mx, op=pg.ReduceOp.MAX)
+        sm = t.clone()
+        pg.all_reduce(sm, op=pg.ReduceOp.SUM)
+        max_ms, tot_edges = float(mx[0]), float(sm[1])
+    value = hm if world == 1 else tot_edges / (max_ms / 1e3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(g, timed[:args.cpu_roots], nedge)
+    if rank == 0:
+        line = {
+            "metric": metric_name(scale, ef),
+            "value": round(value, 3),
+            "unit": "GTEPS",
+            "n_gpus": world,
+            "steps": K,
+            "warmup": W,
+            "ms_per_step": round(max_ms / K, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "int32",
+            "data": "synthetic: Graph500 Kronecker generator (A,B,C,D = .57,.19,.19,.05), seeds (2,3), bit-identical to the reference's",
+            "config": {"workload": f"graph500 bfs scale{scale} ef{ef}", "scale": scale, "edgefactor": ef,
+                       "nverts": n, "nedges": m, "csr_entries": g.nlocaledges, "roots_per_rank": K,
+                       "roots": "runner root choice, seeds (2,3)", "l2": "inputs larger than L2 (int32 column "
+                       f"{g.nlocaledges * 4 / 1e9:.1f} GB)", "parallelism": f"replicas x{world}, roots sharded"},
+            "aggregate_gteps": round(tot_edges / (max_ms / 1e3) / 1e9, 3),
+            "roofline": {"bound": "hbm", "kernel": "bfs_persistent_kernel",
+                         "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved_gbs / peak, 4), "peak_kind": f"{peak_kind} copy bandwidth",
+                         "bytes_per_launch": int(np.mean(alg_bytes)),
+                         "bytes_model": "2*nedge*4 (col) + reached*(8 rowstarts + 8 pred)",
+                         "kernel_ms_mean": round(float(np.mean(kern_s)) * 1e3, 4),
+                         "traffic": args.traffic},
+            "e2e": {"value": round(e2e_hm if world == 1 else e2e_hm * world, 3), "unit": "GTEPS",
+                    "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 24,
+                    "path": "C ABI g5_bfs_run + g5_bfs_last_stats, pinned host root, host wall clock"},
+            "sssp": {"value": round(s_hm, 3), "unit": "GTEPS (harmonic mean)",
+                     "ms_per_root": round(float(np.mean(s_secs)) * 1e3, 3), "delta": 0.1},
+            "construction": {"generation_s": round(gen_s, 4), "csr_build_s": round(csr_s, 4),
+                             "setup_total_s": round(setup_s, 2)},
+            "nedge_per_root": int(np.median(t_nedge)),
+            "clocks": clocks.summary(),
+            "gpu_launches": K,
+            "gpu_launches_note": "one bfs_persistent_kernel per step (+3 cudaMemsetAsync); SSSP timed separately",
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def cpu_baseline_sample(g, roots, nedge):
+    """Oracle BFS (the reference's top-down algorithm, OpenMP on all host
+    cores) on the same CSR, copied to the host, for a few roots."""
+    from oracle import oracle as O
+    rs = g.rowstarts.cpu().numpy().view(np.uint64)
+    col = g.col.cpu().numpy().view(np.uint32)
+    n = g.nglobalverts
+    secs = []
+    for r in roots:
+        t = time.perf_counter()
+        O.bfs(rs, col, n, r)
+        secs.append(time.perf_counter() - t)
+    return {"value": round(hmean_gteps([nedge[r] for r in roots], secs), 4), "unit": "GTEPS",
+            "cores": O.num_threads(), "kind": "port",
+            "sample": f"{len(roots)} BFS roots of the same SCALE graph, oracle top-down BFS (OpenMP)"}
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    scale, ef = args.scale, args.edgefactor
+    n, m = 1 << scale, ef << scale
+    t0 = time.time()
+    seed = O.make_mrg_seed(2, 3)
+    e, w = O.generate_kronecker_range(seed, scale, 0, m)
+    gen_s = time.time() - t0
+    t1 = time.time()
+    rs, col, cw = O.csr_build(e, w, n, canonical=False)
+    csr_s = time.time() - t1
+    del e, w
+    roots = O.generate_bfs_roots(rs, n, 2, 3, 64).tolist()
+    K, W = args.steps, args.warmup
+    seq = [roots[i % len(roots)] for i in range(W + K)]
+    nedge = {}
+    for r in seq[:W]:
+        pred, _ = O.bfs(rs, col, n, r)
+        nedge[r] = O.edge_count(rs, col, n, pred)
+    secs = []
+    t_start = time.perf_counter()
+    for r in seq[W:]:
+        t = time.perf_counter()
+        pred, _ = O.bfs(rs, col, n, r)
+        secs.append(time.perf_counter() - t)
+        if r not in nedge:
+            nedge[r] = O.edge_count(rs, col, n, pred)
+    total = time.perf_counter() - t_start
+    timed = seq[W:]
+    v = hmean_gteps([nedge[r] for r in timed], secs)
+    line = {
+        "metric": metric_name(scale, ef), "value": round(v, 4), "unit": "GTEPS", "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": round(total / K * 1e3, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic: Graph500 Kronecker generator, seeds (2,3)",
+        "config": {"workload": f"graph500 bfs scale{scale} ef{ef}", "scale": scale, "edgefactor": ef,
+                   "roots_per_rank": K, "parallelism": "host cores"},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(v, 4), "unit": "GTEPS", "cores": O.num_threads(), "kind": "port",
+                         "sample": f"{K} BFS roots; the reference has no CPU path, so this is its top-down "
+                                   "algorithm as restated in oracle/ (OpenMP)"},
+        "e2e": {"value": round(v, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "setup": {"generation_s": round(gen_s, 1), "csr_build_s": round(csr_s, 1)},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--scale", type=int, default=26)
+    ap.add_argument("--edgefactor", type=int, default=16)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-roots", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="ncu dram bytes per BFS launch (read+write) to report beside the roofline")
+    args = ap.parse_args()
+    if args.warmup < 1 or args.steps < 1:
+        ap.error("steps and warmup must be positive")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

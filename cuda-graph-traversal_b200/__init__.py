@@ -52,6 +52,8 @@ def _load() -> C.CDLL:
         "g5_csr_fill": ([p, p, u64, u64, p, f32, p, u64, p, p, p, p, p], C.c_int),
         "g5_bfs_workspace_size": ([u64, p], C.c_int),
         "g5_bfs_run": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
+        "g5_bfs_reset": ([u64, p, p, p, u64, p], C.c_int),
+        "g5_bfs_traverse": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_bfs_last_stats": ([p, u64, p, p], C.c_int),
         "g5_bfs_dist_from_pred": ([p, p, u64, p, u64, p, p, u64, p], C.c_int),
         "g5_sssp_workspace_size": ([u64, p], C.c_int),
@@ -265,6 +267,7 @@ class BfsState:
         self.pred = torch.empty(n, dtype=torch.int64, device=dev)
         self.depth = torch.empty(n, dtype=torch.int32, device=dev)
         self.dist: torch.Tensor | None = None
+        self.val_work: torch.Tensor | None = None
         self.max_nlocalverts = n
 
 
@@ -280,6 +283,20 @@ def oned_graph_bfs_run(g: OnedGraph, bfs: BfsState, root: int, params: BfsParams
                           C.byref(params) if params is not None else None, _stream(stream)))
 
 
+def oned_graph_bfs_reset(bfs: BfsState, with_depth: bool = True, stream=None) -> None:
+    """First half of oned_graph_bfs_run: clear pred/depth and the workspace."""
+    _check(lib.g5_bfs_reset(bfs.max_nlocalverts, _ptr(bfs.pred), _ptr(bfs.depth) if with_depth else None,
+                            _ptr(bfs.work), bfs.work.numel(), _stream(stream)))
+
+
+def oned_graph_bfs_traverse(g: OnedGraph, bfs: BfsState, root: int, params: BfsParams | None = None,
+                            with_depth: bool = True, stream=None) -> None:
+    """Second half of oned_graph_bfs_run: the persistent BFS kernel alone."""
+    _check(lib.g5_bfs_traverse(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, root, _ptr(bfs.pred),
+                               _ptr(bfs.depth) if with_depth else None, _ptr(bfs.work), bfs.work.numel(),
+                               C.byref(params) if params is not None else None, _stream(stream)))
+
+
 def bfs_stats(bfs: BfsState, stream=None) -> BfsStats:
     s = BfsStats()
     _check(lib.g5_bfs_last_stats(_ptr(bfs.work), bfs.work.numel(), C.byref(s), _stream(stream)))
@@ -290,8 +307,10 @@ def bfs_compute_dist_from_pred(g: OnedGraph, bfs: BfsState, root: int, stream=No
     """bfs_compute_dist_from_pred (src/traversal.h:48)."""
     if bfs.dist is None:
         bfs.dist = torch.empty(g.nglobalverts, dtype=torch.int64, device=g.device)
+    if bfs.val_work is None:
+        bfs.val_work = _val_work(g)
     _check(lib.g5_bfs_dist_from_pred(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, _ptr(bfs.pred), root,
-                                     _ptr(bfs.dist), _ptr(bfs.work), bfs.work.numel(), _stream(stream)))
+                                     _ptr(bfs.dist), _ptr(bfs.val_work), bfs.val_work.numel(), _stream(stream)))
     return bfs.dist
 
 

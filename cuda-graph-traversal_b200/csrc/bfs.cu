@@ -428,40 +428,53 @@ extern "C" int g5_bfs_workspace_size(uint64_t nverts, uint64_t *bytes) {
     return G5_OK;
 }
 
-extern "C" int g5_bfs_run(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
-                          int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
-                          const g5_bfs_params *params, void *stream) {
-    clear_error();
-    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_bfs_run: nverts outside [1, 2^31]");
-    G5_CHECK_ARG(root < nverts, "g5_bfs_run: root %llu outside [0, %llu)", (unsigned long long)root,
+static int bfs_check(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
+                     int64_t *d_pred, void *d_work, uint64_t work_bytes, BfsWork *w, const char *who) {
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "%s: nverts outside [1, 2^31]", who);
+    G5_CHECK_ARG(root < nverts, "%s: root %llu outside [0, %llu)", who, (unsigned long long)root,
                  (unsigned long long)nverts);
-    G5_CHECK_ARG(d_rowstarts && d_col && d_pred && d_work, "g5_bfs_run: NULL argument");
+    G5_CHECK_ARG(d_rowstarts && d_col && d_pred && d_work, "%s: NULL argument", who);
+    *w = carve_bfs(d_work, nverts);
+    if (work_bytes < w->bytes)
+        return set_error(G5_ERR_WORKSPACE, "%s: workspace %llu < %llu bytes", who, (unsigned long long)work_bytes,
+                         (unsigned long long)w->bytes);
+    return G5_OK;
+}
+
+extern "C" int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
+                            void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31) && d_pred && d_work, "g5_bfs_reset: bad argument");
     BfsWork w = carve_bfs(d_work, nverts);
-    if (work_bytes < w.bytes)
-        return set_error(G5_ERR_WORKSPACE, "g5_bfs_run: workspace %llu < %llu bytes", (unsigned long long)work_bytes,
-                         (unsigned long long)w.bytes);
-    g5_bfs_params p = {14.0f, 24.0f, 0, 0};
-    if (params) p = *params;
-    G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= 2, "g5_bfs_run: bad params");
-
-    int max_blocks = 0;
-    int rc = bfs_max_blocks(&max_blocks);
-    if (rc) return rc;
-    int blocks = p.blocks > 0 ? std::min(p.blocks, max_blocks)
-                              : (int)std::min<uint64_t>(max_blocks, std::max<uint64_t>(1, nverts / 2048));
-
+    if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "g5_bfs_reset: workspace too small");
     cudaStream_t st = (cudaStream_t)stream;
-    const uint64_t words = (nverts + 31) / 32;
     G5_CUDA_TRY(cudaMemsetAsync(d_pred, 0xff, nverts * sizeof(int64_t), st));
     if (d_depth) G5_CUDA_TRY(cudaMemsetAsync(d_depth, 0xff, nverts * sizeof(int32_t), st));
-    G5_CUDA_TRY(cudaMemsetAsync(w.visited, 0, words * sizeof(unsigned), st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.visited, 0, (nverts + 31) / 32 * sizeof(unsigned), st));
     G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(BfsCtl), st));
+    return G5_OK;
+}
 
+extern "C" int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
+                               int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
+                               const g5_bfs_params *params, void *stream) {
+    clear_error();
+    BfsWork w;
+    int rc = bfs_check(d_rowstarts, d_col, nverts, root, d_pred, d_work, work_bytes, &w, "g5_bfs_traverse");
+    if (rc) return rc;
+    g5_bfs_params p = {14.0f, 24.0f, 0, 0};
+    if (params) p = *params;
+    G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= 2, "g5_bfs_traverse: bad params");
+
+    int max_blocks = 0;
+    if ((rc = bfs_max_blocks(&max_blocks))) return rc;
+    int blocks = p.blocks > 0 ? std::min(p.blocks, max_blocks)
+                              : (int)std::min<uint64_t>(max_blocks, std::max<uint64_t>(1, nverts / 2048));
     BfsArgs a;
     a.rowptr = d_rowstarts;
     a.col = d_col;
     a.n = nverts;
-    a.nwords = words;
+    a.nwords = (nverts + 31) / 32;
     a.root = (unsigned)root;
     a.pred = d_pred;
     a.depth = d_depth;
@@ -480,8 +493,19 @@ extern "C" int g5_bfs_run(const uint64_t *d_rowstarts, const int32_t *d_col, uin
     a.limit_ns = wait_limit_ns();
     void *args[] = {&a};
     G5_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)bfs_persistent_kernel, dim3(blocks), dim3(BFS_THREADS), args,
-                                            0, st));
+                                            0, (cudaStream_t)stream));
     return G5_OK;
+}
+
+extern "C" int g5_bfs_run(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
+                          int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
+                          const g5_bfs_params *params, void *stream) {
+    clear_error();
+    BfsWork w;
+    int rc = bfs_check(d_rowstarts, d_col, nverts, root, d_pred, d_work, work_bytes, &w, "g5_bfs_run");
+    if (rc) return rc;
+    if ((rc = g5_bfs_reset(nverts, d_pred, d_depth, d_work, work_bytes, stream))) return rc;
+    return g5_bfs_traverse(d_rowstarts, d_col, nverts, root, d_pred, d_depth, d_work, work_bytes, params, stream);
 }
 
 extern "C" int g5_bfs_last_stats(const void *d_work, uint64_t work_bytes, g5_bfs_stats *stats, void *stream) {

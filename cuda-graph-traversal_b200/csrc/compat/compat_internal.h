@@ -1,0 +1,56 @@
+// compat_internal.h -- private state of the reference-compatible C++ API.
+//
+// The reference's structs cannot grow (code written against them touches
+// their fields), so the library's extra per-object state -- the int32
+// column and light counts of a graph, the workspaces of a BFS or SSSP
+// state -- lives in side tables keyed by the object's first device pointer.
+#pragma once
+
+#include <stdint.h>
+
+#include "g500b.h"
+#include "traversal.h"
+
+namespace g5compat {
+
+struct GraphExt {
+    int32_t *col;        // int32 neighbour ids, light-first rows
+    uint32_t *light_deg; // light entries per row
+    float light_delta;
+};
+
+struct BfsExt {
+    int32_t *depth;
+    void *work;  // BFS kernel workspace (its statistics live at the front)
+    uint64_t work_bytes;
+    void *val_work;  // depth-from-parents scratch
+    uint64_t val_bytes;
+};
+
+struct SsspExt {
+    void *work;
+    uint64_t work_bytes;
+};
+
+void put_graph(const u64 *rowstarts, const GraphExt &x);
+const GraphExt *get_graph(const Oned_Graph *g, Worker_State *ws);
+void drop_graph(const u64 *rowstarts);
+void put_bfs(const i64 *pred, const BfsExt &x);
+const BfsExt *get_bfs(const i64 *pred);
+void drop_bfs(const i64 *pred);
+void put_sssp(const i64 *pred, const SsspExt &x);
+const SsspExt *get_sssp(const i64 *pred);
+void drop_sssp(const i64 *pred);
+
+// Prints the library error and aborts the worker, the reference's
+// convention for failed calls (src/base.h:48-54, src/worker.cu:64-67).
+void die(Worker_State *ws, int rc, const char *what);
+inline void check(Worker_State *ws, int rc, const char *what) {
+    if (rc != G5_OK) die(ws, rc, what);
+}
+
+// Device memory for the library's private arrays, from the worker's GPU
+// arena like everything else the reference allocates.
+void *gpu_push(Worker_State *ws, uint64_t bytes, const char *what);
+
+}  // namespace g5compat

@@ -1,0 +1,180 @@
+// traversal.cu -- the reference's src/traversal.h API over libg500b
+// (replaces src/traversal.cu:342-721).  Same inputs, outputs and error
+// behaviour; every call synchronises before returning, as the reference's
+// do, so wall-clock timing around a call measures its work.
+#include <cstring>
+
+#include "compat_internal.h"
+#include "traversal.h"
+
+using namespace g5compat;
+
+static const float kLightDelta = 0.1f;  // the reference's SSSP delta (src/traversal.cu:645)
+
+__global__ static void fill_minus_one(f32 *x, u64 n) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) x[i] = -1.0f;
+}
+
+Oned_Graph oned_graph_from_tuple_graph(Worker_State *ws, Tuple_Graph *tg, u64 nglobalverts) {
+    Oned_Graph g;
+    memset(&g, 0, sizeof g);
+    g.nglobalverts = nglobalverts;
+    g.nlocalverts = nglobalverts;  // one rank owns every vertex
+    u64 count = 0;
+    g.rowstarts = worker_arena_push_array(ws, g.nlocalverts + 1, u64, &count);
+    uint64_t wbytes = 0;
+    check(ws, g5_csr_workspace_size(nglobalverts, tg->edges_size, &wbytes), "oned_graph_from_tuple_graph");
+    void *work = gpu_push(ws, wbytes, "CSR workspace");
+    check(ws,
+          g5_csr_count((const uint64_t *)tg->edges, tg->edges_size, nglobalverts, g.rowstarts, work, wbytes,
+                       &g.nlocaledges, 0),
+          "oned_graph_from_tuple_graph");
+    g.column = worker_arena_push_array(ws, g.nlocaledges, u64, &count);
+    g.weights = worker_arena_push_array(ws, g.nlocaledges, f32, &count);
+    GraphExt x;
+    x.col = (int32_t *)gpu_push(ws, g.nlocaledges * sizeof(int32_t), "int32 column");
+    x.light_deg = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "light degrees");
+    x.light_delta = kLightDelta;
+    check(ws,
+          g5_csr_fill((const uint64_t *)tg->edges, tg->weights, tg->edges_size, nglobalverts, g.rowstarts,
+                      kLightDelta, work, wbytes, x.col, g.weights, g.column, x.light_deg, 0),
+          "oned_graph_from_tuple_graph");
+    CHECK_CUDA(cudaDeviceSynchronize());
+    put_graph(g.rowstarts, x);
+    return g;
+}
+
+b32 oned_graph_is_vertex_isolated(Worker_State *ws, const Oned_Graph *g, u64 global_vertex) {
+    if (global_vertex >= g->nglobalverts) {
+        ERROR("Vertex %llu is outside graph vertex range [0, %llu)", (unsigned long long)global_vertex,
+              (unsigned long long)g->nglobalverts);
+        worker_abort(ws, 1);
+    }
+    u64 r[2];
+    CHECK_CUDA(cudaMemcpy(r, g->rowstarts + global_vertex, sizeof r, cudaMemcpyDeviceToHost));
+    return r[0] == r[1];
+}
+
+Bfs_State oned_graph_bfs_create(Worker_State *ws, const Oned_Graph *g) {
+    Bfs_State bfs;
+    memset(&bfs, 0, sizeof bfs);
+    bfs.pred = worker_arena_push_array(ws, g->nlocalverts, i64, &bfs.max_nlocalverts);
+    BfsExt x;
+    x.depth = (int32_t *)gpu_push(ws, g->nlocalverts * sizeof(int32_t), "BFS depth");
+    check(ws, g5_bfs_workspace_size(g->nglobalverts, &x.work_bytes), "oned_graph_bfs_create");
+    x.work = gpu_push(ws, x.work_bytes, "BFS workspace");
+    check(ws, g5_validate_workspace_size(g->nglobalverts, &x.val_bytes), "oned_graph_bfs_create");
+    x.val_work = gpu_push(ws, x.val_bytes, "BFS depth scratch");
+    put_bfs(bfs.pred, x);
+    oned_graph_bfs_clear(ws, &bfs);
+    return bfs;
+}
+
+void oned_graph_bfs_clear(Worker_State *ws, Bfs_State *bfs) {
+    (void)ws;
+    CHECK_CUDA(cudaMemset(bfs->pred, 0xff, bfs->max_nlocalverts * sizeof(i64)));
+    if (bfs->dist) CHECK_CUDA(cudaMemset(bfs->dist, 0xff, bfs->max_nlocalverts * sizeof(i64)));
+    CHECK_CUDA(cudaDeviceSynchronize());
+}
+
+void oned_graph_bfs_run(Worker_State *ws, const Oned_Graph *g, Bfs_State *bfs, u64 root) {
+    if (root >= g->nglobalverts) {
+        ERROR("BFS root %llu is outside graph vertex range [0, %llu)", (unsigned long long)root,
+              (unsigned long long)g->nglobalverts);
+        worker_abort(ws, 1);
+    }
+    const GraphExt *gx = get_graph(g, ws);
+    const BfsExt *bx = get_bfs(bfs->pred);
+    if (!bx) {
+        ERROR("Bfs_State was not created by oned_graph_bfs_create of this library");
+        worker_abort(ws, 1);
+    }
+    check(ws, g5_bfs_run(g->rowstarts, gx->col, g->nglobalverts, root, bfs->pred, bx->depth, bx->work, bx->work_bytes,
+                         nullptr, 0),
+          "oned_graph_bfs_run");
+    g5_bfs_stats st;
+    check(ws, g5_bfs_last_stats(bx->work, bx->work_bytes, &st, 0), "oned_graph_bfs_run");
+}
+
+i64 *bfs_compute_dist_from_pred(Worker_State *ws, const Oned_Graph *g, Bfs_State *bfs, u64 root) {
+    if (root >= g->nglobalverts) {
+        ERROR("BFS root %llu is outside graph vertex range [0, %llu)", (unsigned long long)root,
+              (unsigned long long)g->nglobalverts);
+        worker_abort(ws, 1);
+    }
+    if (!bfs->dist) {
+        u64 count = 0;
+        bfs->dist = worker_arena_push_array(ws, g->nlocalverts, i64, &count);
+    }
+    const GraphExt *gx = get_graph(g, ws);
+    const BfsExt *bx = get_bfs(bfs->pred);
+    if (!bx) {
+        ERROR("Bfs_State was not created by oned_graph_bfs_create of this library");
+        worker_abort(ws, 1);
+    }
+    check(ws, g5_bfs_dist_from_pred(g->rowstarts, gx->col, g->nglobalverts, bfs->pred, root, bfs->dist, bx->val_work,
+                                    bx->val_bytes, 0),
+          "bfs_compute_dist_from_pred");
+    CHECK_CUDA(cudaDeviceSynchronize());
+    return bfs->dist;
+}
+
+void oned_graph_bfs_destroy(Bfs_State *bfs) {
+    if (!bfs) return;
+    drop_bfs(bfs->pred);
+    memset(bfs, 0, sizeof *bfs);
+}
+
+Sssp_State oned_graph_sssp_create(Worker_State *ws, const Oned_Graph *g) {
+    Sssp_State s;
+    memset(&s, 0, sizeof s);
+    s.pred = worker_arena_push_array(ws, g->nlocalverts, i64, &s.max_nlocalverts);
+    u64 count = 0;
+    s.dist = worker_arena_push_array(ws, g->nlocalverts, f32, &count);
+    SsspExt x;
+    check(ws, g5_sssp_workspace_size(g->nglobalverts, &x.work_bytes), "oned_graph_sssp_create");
+    x.work = gpu_push(ws, x.work_bytes, "SSSP workspace");
+    put_sssp(s.pred, x);
+    oned_graph_sssp_clear(ws, &s);
+    return s;
+}
+
+void oned_graph_sssp_clear(Worker_State *ws, Sssp_State *sssp) {
+    (void)ws;
+    CHECK_CUDA(cudaMemset(sssp->pred, 0xff, sssp->max_nlocalverts * sizeof(i64)));
+    // -1.0f everywhere, the reference's "unreached" (src/traversal.cu:250).
+    fill_minus_one<<<256, 256>>>(sssp->dist, sssp->max_nlocalverts);
+    CHECK_CUDA(cudaGetLastError());
+    CHECK_CUDA(cudaDeviceSynchronize());
+}
+
+void oned_graph_sssp_run(Worker_State *ws, const Oned_Graph *g, Sssp_State *sssp, u64 root) {
+    if (root >= g->nglobalverts) {
+        ERROR("SSSP root %llu is outside graph vertex range [0, %llu)", (unsigned long long)root,
+              (unsigned long long)g->nglobalverts);
+        worker_abort(ws, 1);
+    }
+    const GraphExt *gx = get_graph(g, ws);
+    const SsspExt *sx = get_sssp(sssp->pred);
+    if (!sx) {
+        ERROR("Sssp_State was not created by oned_graph_sssp_create of this library");
+        worker_abort(ws, 1);
+    }
+    g5_sssp_params p = {kLightDelta, 0};
+    check(ws, g5_sssp_run(g->rowstarts, gx->col, g->weights, gx->light_deg, gx->light_delta, g->nglobalverts, root,
+                          sssp->dist, sssp->pred, sx->work, sx->work_bytes, &p, 0),
+          "oned_graph_sssp_run");
+    check(ws, g5_sssp_last_status(sx->work, sx->work_bytes, nullptr, nullptr, 0), "oned_graph_sssp_run");
+}
+
+void oned_graph_sssp_destroy(Sssp_State *sssp) {
+    if (!sssp) return;
+    drop_sssp(sssp->pred);
+    memset(sssp, 0, sizeof *sssp);
+}
+
+void oned_graph_free(Oned_Graph *g) {
+    if (!g) return;
+    drop_graph(g->rowstarts);
+    memset(g, 0, sizeof *g);
+}

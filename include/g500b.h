@@ -113,12 +113,22 @@ int g5_bfs_run(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nvert
                int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
                const g5_bfs_params *params, void *stream);
 
+/* g5_bfs_run in two steps: g5_bfs_reset clears pred (-1), depth (-1) and the
+ * workspace's visited bitmap and control block; g5_bfs_traverse then runs
+ * the persistent kernel alone (on a reset state). */
+int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes, void *stream);
+int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
+                    int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
+                    const g5_bfs_params *params, void *stream);
+
 /* Statistics of the last g5_bfs_run that used this workspace (synchronises). */
 int g5_bfs_last_stats(const void *d_work, uint64_t work_bytes, g5_bfs_stats *stats, void *stream);
 
 /* bfs_compute_dist_from_pred, src/traversal.h:48 (src/traversal.cu:505-563):
  * d_dist[v] = -1 where pred is -1, 0 at the root, the tree depth where the
- * parent chain reaches the root through CSR edges, INT64_MAX otherwise. */
+ * parent chain reaches the root through CSR edges, INT64_MAX otherwise.
+ * d_work needs g5_validate_workspace_size bytes (not the BFS workspace,
+ * whose statistics it would overwrite).  Synchronises once per level. */
 int g5_bfs_dist_from_pred(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
                           const int64_t *d_pred, uint64_t root, int64_t *d_dist, void *d_work,
                           uint64_t work_bytes, void *stream);
