@@ -167,9 +167,12 @@ def run_ours(args):
     assert G.bfs_validate(g, r0, bfs.pred, dist, vw) == 0, "BFS validation failed"
     setup_s = time.time() - t0
 
-    # ---- timed BFS: K roots back to back on one stream, events per step.
+    # ---- timed BFS.  The runner's protocol (examples/graph500_runner.cu:
+    # 309-313): oned_graph_bfs_clear outside the timer, oned_graph_bfs_run
+    # inside; here both run back to back on one stream and CUDA events split
+    # them, so the reset time is reported too.
     for r in seq[:W]:
-        G.oned_graph_bfs_reset(bfs, with_depth=False)
+        G.oned_graph_bfs_reset(bfs, with_depth=False, g=g)
         G.oned_graph_bfs_traverse(g, bfs, r, with_depth=False)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
             torch.cuda.Event(enable_timing=True)) for _ in range(K)]
@@ -184,7 +187,7 @@ def run_ours(args):
         for i, r in enumerate(seq[W:]):
             a, b, c = evs[i]
             a.record()
-            G.oned_graph_bfs_reset(bfs, with_depth=False)
+            G.oned_graph_bfs_reset(bfs, with_depth=False, g=g)
             b.record()
             G.oned_graph_bfs_traverse(g, bfs, r, with_depth=False)
             c.record()
@@ -197,45 +200,58 @@ def run_ours(args):
     kern_s = [b.elapsed_time(c) / 1e3 for _, b, c in evs]
     timed = seq[W:]
     t_nedge = [nedge[r] for r in timed]
-    hm = hmean_gteps(t_nedge, step_s)
+    hm = hmean_gteps(t_nedge, kern_s)
+    hm_with_reset = hmean_gteps(t_nedge, step_s)
+    per_root_gteps = np.asarray(t_nedge, np.float64) / np.asarray(kern_s) / 1e9
     st = G.bfs_stats(bfs)
     assert st.reached == reached[timed[-1]]
+    big = [i for i, r in enumerate(timed) if nedge[r] >= 0.5 * max(t_nedge)]
+    trace = G.bfs_trace(bfs)
 
-    # Roofline of the persistent BFS kernel: algorithmic bytes per search =
-    # 2*nedge*4 (int32 col) + reached*(8 rowstarts + 8 pred) (no depth array).
-    alg_bytes = [2 * nedge[r] * 4 + reached[r] * 16 for r in timed]
-    achieved_gbs = float(np.sum(alg_bytes) / np.sum(kern_s) / 1e9)
+    # Roofline of the persistent BFS kernel over the roots in the big
+    # component: algorithmic bytes per search = 2*nedge*4 (int32 col) +
+    # reached*(8 rowstarts + 8 pred) (no depth array).
+    alg_bytes = [2 * nedge[timed[i]] * 4 + reached[timed[i]] * 16 for i in big]
+    achieved_gbs = float(np.sum(alg_bytes) / np.sum([kern_s[i] for i in big]) / 1e9)
     peak, peak_kind = hbm_peak()
 
-    # ---- SSSP, same roots.
+    # ---- SSSP, same roots and protocol.
     sssp = G.SsspState(g)
     for r in seq[:W]:
-        G.oned_graph_sssp_run(g, sssp, r)
-    sev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        G.oned_graph_sssp_reset(sssp)
+        G.oned_graph_sssp_traverse(g, sssp, r)
+    sev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+            torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     torch.cuda.synchronize()
     for i, r in enumerate(timed):
         sev[i][0].record()
-        G.oned_graph_sssp_run(g, sssp, r)
+        G.oned_graph_sssp_reset(sssp)
         sev[i][1].record()
+        G.oned_graph_sssp_traverse(g, sssp, r)
+        sev[i][2].record()
     torch.cuda.synchronize()
-    G.sssp_status(sssp)
-    s_secs = [a.elapsed_time(b) / 1e3 for a, b in sev]
+    nbuckets, nphases = G.sssp_status(sssp)
+    s_secs = [b.elapsed_time(c) / 1e3 for _, b, c in sev]
+    s_secs_reset = [a.elapsed_time(c) / 1e3 for a, _, c in sev]
     s_hm = hmean_gteps(t_nedge, s_secs)
+    s_per_root = np.asarray(t_nedge, np.float64) / np.asarray(s_secs) / 1e9
     r_last = timed[-1]
     assert G.sssp_validate(g, r_last, sssp.dist, sssp.pred, vw) == 0, "SSSP validation failed"
 
-    # ---- end to end through the C ABI with host buffers: per step the root
-    # goes host->device from pinned memory, the BFS runs, and the step's
-    # result (its statistics: levels and reached count) comes back.
+    # ---- end to end through the C ABI with host buffers, the runner's
+    # protocol: untimed clear, then per step the root goes host->device from
+    # pinned memory, the search runs, and the step's result (its statistics:
+    # levels and reached count) is read back to the host.
     root_host = torch.empty(1, dtype=torch.int64, pin_memory=True)
     root_dev = torch.empty(1, dtype=torch.int64, device=dev)
     e2e_s = []
-    torch.cuda.synchronize()
     for r in timed:
+        G.oned_graph_bfs_reset(bfs, with_depth=False, g=g)
+        torch.cuda.synchronize()
         t = time.perf_counter()
         root_host[0] = r
         root_dev.copy_(root_host, non_blocking=True)
-        G.oned_graph_bfs_run(g, bfs, int(r), with_depth=False)
+        G.oned_graph_bfs_traverse(g, bfs, int(r), with_depth=False)
         res = G.bfs_stats(bfs)  # device -> host read of the result, synchronises
         e2e_s.append(time.perf_counter() - t)
         assert res.reached == reached[r]
@@ -251,7 +267,13 @@ def run_ours(args):
         sm = t.clone()
         pg.all_reduce(sm, op=pg.ReduceOp.SUM)
         max_ms, tot_edges = float(mx[0]), float(sm[1])
-    value = hm if world == 1 else tot_edges / (max_ms / 1e3) / 1e9
+    # Per rank the Graph500 harmonic mean; across ranks (weak scaling) the
+    # ranks' harmonic means add up.
+    value = hm
+    if pg:
+        t = torch.tensor([hm], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.SUM)
+        value = float(t[0])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -259,12 +281,13 @@ def run_ours(args):
     if rank == 0:
         line = {
             "metric": metric_name(scale, ef),
-            "value": round(value, 3),
+            "value": float(f"{value:.6g}"),
             "unit": "GTEPS",
             "n_gpus": world,
             "steps": K,
             "warmup": W,
             "ms_per_step": round(max_ms / K, 4),
+            "timing": "device events per root; reset (the runner's oned_graph_bfs_clear) untimed as in the runner",
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
@@ -275,6 +298,13 @@ def run_ours(args):
                        "roots": "runner root choice, seeds (2,3)", "l2": "inputs larger than L2 (int32 column "
                        f"{g.nlocaledges * 4 / 1e9:.1f} GB)", "parallelism": f"replicas x{world}, roots sharded"},
             "aggregate_gteps": round(tot_edges / (max_ms / 1e3) / 1e9, 3),
+            "hmean_gteps_with_reset": float(f"{hm_with_reset:.6g}"),
+            "median_gteps": round(float(np.median(per_root_gteps)), 3),
+            "small_component_roots": int(sum(1 for r in timed if nedge[r] < 0.5 * max(t_nedge))),
+            "small_root_us_max": round(max([kern_s[i] for i, r in enumerate(timed) if nedge[r] < 0.5 * max(t_nedge)]
+                                           or [0.0]) * 1e6, 2),
+            "big_root_ms_mean": round(float(np.mean([kern_s[i] for i in big])) * 1e3, 4),
+            "trace_last_root": trace,
             "roofline": {"bound": "hbm", "kernel": "bfs_persistent_kernel",
                          "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved_gbs / peak, 4), "peak_kind": f"{peak_kind} copy bandwidth",
@@ -282,17 +312,21 @@ def run_ours(args):
                          "bytes_model": "2*nedge*4 (col) + reached*(8 rowstarts + 8 pred)",
                          "kernel_ms_mean": round(float(np.mean(kern_s)) * 1e3, 4),
                          "traffic": args.traffic},
-            "e2e": {"value": round(e2e_hm if world == 1 else e2e_hm * world, 3), "unit": "GTEPS",
+            "e2e": {"value": float(f"{(e2e_hm if world == 1 else e2e_hm * world):.6g}"), "unit": "GTEPS",
                     "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 24,
-                    "path": "C ABI g5_bfs_run + g5_bfs_last_stats, pinned host root, host wall clock"},
-            "sssp": {"value": round(s_hm, 3), "unit": "GTEPS (harmonic mean)",
-                     "ms_per_root": round(float(np.mean(s_secs)) * 1e3, 3), "delta": 0.1},
+                    "path": "C ABI g5_bfs_traverse + g5_bfs_last_stats after an untimed g5_bfs_reset, "
+                            "pinned host root, host wall clock"},
+            "sssp": {"value": float(f"{s_hm:.6g}"), "unit": "GTEPS (harmonic mean)",
+                     "hmean_gteps_with_reset": float(f"{hmean_gteps(t_nedge, s_secs_reset):.6g}"),
+                     "median_gteps": round(float(np.median(s_per_root)), 3),
+                     "big_root_ms_mean": round(float(np.mean([s_secs[i] for i in big])) * 1e3, 3),
+                     "buckets_last_root": nbuckets, "phases_last_root": nphases, "delta": 0.1},
             "construction": {"generation_s": round(gen_s, 4), "csr_build_s": round(csr_s, 4),
                              "setup_total_s": round(setup_s, 2)},
             "nedge_per_root": int(np.median(t_nedge)),
             "clocks": clocks.summary(),
             "gpu_launches": K,
-            "gpu_launches_note": "one bfs_persistent_kernel per step (+3 cudaMemsetAsync); SSSP timed separately",
+            "gpu_launches_note": "one bfs_persistent_kernel per step (+ memsets); SSSP timed separately",
         }
         if cpu:
             line["cpu_baseline"] = cpu
@@ -309,14 +343,19 @@ def cpu_baseline_sample(g, roots, nedge):
     rs = g.rowstarts.cpu().numpy().view(np.uint64)
     col = g.col.cpu().numpy().view(np.uint32)
     n = g.nglobalverts
+    pred = np.empty(n, np.int64)
+    depth = np.empty(n, np.int64)
     secs = []
     for r in roots:
+        O.bfs_clear(n, pred, depth)
         t = time.perf_counter()
-        O.bfs(rs, col, n, r)
+        O.bfs_search(rs, col, n, r, pred, depth)
         secs.append(time.perf_counter() - t)
-    return {"value": round(hmean_gteps([nedge[r] for r in roots], secs), 4), "unit": "GTEPS",
+    return {"value": float(f"{hmean_gteps([nedge[r] for r in roots], secs):.6g}"), "unit": "GTEPS",
             "cores": O.num_threads(), "kind": "port",
-            "sample": f"{len(roots)} BFS roots of the same SCALE graph, oracle top-down BFS (OpenMP)"}
+            "median_gteps": round(float(np.median(np.asarray([nedge[r] for r in roots]) / np.asarray(secs) / 1e9)), 4),
+            "sample": f"first {len(roots)} timed roots of the same graph, oracle top-down BFS (OpenMP), "
+                      "clear untimed as in the runner"}
 
 
 def run_reference(args):
@@ -338,14 +377,18 @@ def run_reference(args):
     K, W = args.steps, args.warmup
     seq = [roots[i % len(roots)] for i in range(W + K)]
     nedge = {}
+    pred = np.empty(n, np.int64)
+    depth = np.empty(n, np.int64)
     for r in seq[:W]:
-        pred, _ = O.bfs(rs, col, n, r)
+        O.bfs_clear(n, pred, depth)
+        O.bfs_search(rs, col, n, r, pred, depth)
         nedge[r] = O.edge_count(rs, col, n, pred)
     secs = []
     t_start = time.perf_counter()
     for r in seq[W:]:
+        O.bfs_clear(n, pred, depth)  # untimed, as the runner's oned_graph_bfs_clear
         t = time.perf_counter()
-        pred, _ = O.bfs(rs, col, n, r)
+        O.bfs_search(rs, col, n, r, pred, depth)
         secs.append(time.perf_counter() - t)
         if r not in nedge:
             nedge[r] = O.edge_count(rs, col, n, pred)
@@ -353,17 +396,18 @@ def run_reference(args):
     timed = seq[W:]
     v = hmean_gteps([nedge[r] for r in timed], secs)
     line = {
-        "metric": metric_name(scale, ef), "value": round(v, 4), "unit": "GTEPS", "n_gpus": world,
+        "metric": metric_name(scale, ef), "value": float(f"{v:.6g}"), "unit": "GTEPS", "n_gpus": world,
         "steps": K, "warmup": W, "ms_per_step": round(total / K * 1e3, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic: Graph500 Kronecker generator, seeds (2,3)",
         "config": {"workload": f"graph500 bfs scale{scale} ef{ef}", "scale": scale, "edgefactor": ef,
                    "roots_per_rank": K, "parallelism": "host cores"},
         "impl": "reference",
-        "cpu_baseline": {"value": round(v, 4), "unit": "GTEPS", "cores": O.num_threads(), "kind": "port",
+        "median_gteps": round(float(np.median(np.asarray([nedge[r] for r in timed]) / np.asarray(secs) / 1e9)), 4),
+        "cpu_baseline": {"value": float(f"{v:.6g}"), "unit": "GTEPS", "cores": O.num_threads(), "kind": "port",
                          "sample": f"{K} BFS roots; the reference has no CPU path, so this is its top-down "
                                    "algorithm as restated in oracle/ (OpenMP)"},
-        "e2e": {"value": round(v, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": float(f"{v:.6g}"), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "setup": {"generation_s": round(gen_s, 1), "csr_build_s": round(csr_s, 1)},
     }
     print(json.dumps(line), flush=True)
@@ -372,7 +416,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--steps", type=int, default=64)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--scale", type=int, default=26)
     ap.add_argument("--edgefactor", type=int, default=16)

@@ -52,13 +52,17 @@ def _load() -> C.CDLL:
         "g5_csr_fill": ([p, p, u64, u64, p, f32, p, u64, p, p, p, p, p], C.c_int),
         "g5_bfs_workspace_size": ([u64, p], C.c_int),
         "g5_bfs_run": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
-        "g5_bfs_reset": ([u64, p, p, p, u64, p], C.c_int),
+        "g5_bfs_reset": ([u64, p, p, p, p, u64, p], C.c_int),
+        "g5_graph_isolated_bitmap": ([p, u64, p, p], C.c_int),
         "g5_bfs_traverse": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_bfs_last_stats": ([p, u64, p, p], C.c_int),
+        "g5_bfs_last_trace": ([p, u64, C.c_int, p, p, p, p, p, p, p], C.c_int),
         "g5_bfs_dist_from_pred": ([p, p, u64, p, u64, p, p, u64, p], C.c_int),
         "g5_sssp_workspace_size": ([u64, p], C.c_int),
         "g5_sssp_run": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_sssp_last_status": ([p, u64, p, p, p], C.c_int),
+        "g5_sssp_reset": ([u64, p, u64, p], C.c_int),
+        "g5_sssp_traverse": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_validate_workspace_size": ([u64, p], C.c_int),
         "g5_edge_count": ([p, p, u64, p, p, u64, p, p], C.c_int),
         "g5_bfs_validate": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
@@ -182,6 +186,7 @@ class OnedGraph:
     light_deg: torch.Tensor
     light_delta: float
     column: torch.Tensor | None = None
+    isolated: torch.Tensor | None = None  # int32[ceil(N/32)] bitmap of degree-0 vertices
 
     @property
     def nlocalverts(self) -> int:
@@ -212,8 +217,10 @@ def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: 
     col64 = torch.empty(max(e, 1), dtype=torch.int64, device=dev) if with_column64 else None
     _check(lib.g5_csr_fill(_ptr(tg.edges), _ptr(tg.weights), m, n, _ptr(rowstarts), light_delta,
                            _ptr(work), work.numel(), _ptr(col), _ptr(w), _ptr(col64), _ptr(light), st))
+    iso = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
+    _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), n, _ptr(iso), st))
     return OnedGraph(n, e, rowstarts, col[:e], w[:e], light, light_delta,
-                     None if col64 is None else col64[:e])
+                     None if col64 is None else col64[:e], iso)
 
 
 def oned_graph_is_vertex_isolated(g: OnedGraph, global_vertex: int) -> bool:
@@ -277,16 +284,20 @@ def oned_graph_bfs_create(g: OnedGraph) -> BfsState:
 
 def oned_graph_bfs_run(g: OnedGraph, bfs: BfsState, root: int, params: BfsParams | None = None,
                        with_depth: bool = True, stream=None) -> None:
-    """oned_graph_bfs_run (src/traversal.h:47): enqueues the whole BFS."""
-    _check(lib.g5_bfs_run(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, root, _ptr(bfs.pred),
-                          _ptr(bfs.depth) if with_depth else None, _ptr(bfs.work), bfs.work.numel(),
-                          C.byref(params) if params is not None else None, _stream(stream)))
+    """oned_graph_bfs_run (src/traversal.h:47) with its clear: enqueues the
+    whole BFS (reset + persistent kernel)."""
+    oned_graph_bfs_reset(bfs, with_depth, g, stream)
+    oned_graph_bfs_traverse(g, bfs, root, params, with_depth, stream)
 
 
-def oned_graph_bfs_reset(bfs: BfsState, with_depth: bool = True, stream=None) -> None:
-    """First half of oned_graph_bfs_run: clear pred/depth and the workspace."""
+def oned_graph_bfs_reset(bfs: BfsState, with_depth: bool = True, g: OnedGraph | None = None,
+                         stream=None) -> None:
+    """First half of oned_graph_bfs_run (the reference's oned_graph_bfs_clear):
+    clear pred/depth and the workspace; with the graph, isolated vertices
+    start out visited."""
     _check(lib.g5_bfs_reset(bfs.max_nlocalverts, _ptr(bfs.pred), _ptr(bfs.depth) if with_depth else None,
-                            _ptr(bfs.work), bfs.work.numel(), _stream(stream)))
+                            _ptr(g.isolated) if g is not None else None, _ptr(bfs.work), bfs.work.numel(),
+                            _stream(stream)))
 
 
 def oned_graph_bfs_traverse(g: OnedGraph, bfs: BfsState, root: int, params: BfsParams | None = None,
@@ -301,6 +312,22 @@ def bfs_stats(bfs: BfsState, stream=None) -> BfsStats:
     s = BfsStats()
     _check(lib.g5_bfs_last_stats(_ptr(bfs.work), bfs.work.numel(), C.byref(s), _stream(stream)))
     return s
+
+
+def bfs_trace(bfs: BfsState, stream=None) -> dict:
+    """Per-level trace of the last BFS on this state (direction, frontier
+    size and edges, device milliseconds)."""
+    k = 64
+    mode = np.zeros(k, np.int32)
+    nv = np.zeros(k, np.uint64)
+    ne = np.zeros(k, np.uint64)
+    ms = np.zeros(k, np.float64)
+    nl, solo = C.c_int32(), C.c_int32()
+    _check(lib.g5_bfs_last_trace(_ptr(bfs.work), bfs.work.numel(), k, mode.ctypes.data, nv.ctypes.data,
+                                 ne.ctypes.data, ms.ctypes.data, C.byref(nl), C.byref(solo), _stream(stream)))
+    n = min(nl.value, k)
+    return {"levels": nl.value, "solo_levels": solo.value, "mode": mode[:n].tolist(),
+            "frontier": nv[:n].tolist(), "frontier_edges": ne[:n].tolist(), "ms": ms[:n].tolist()}
 
 
 def bfs_compute_dist_from_pred(g: OnedGraph, bfs: BfsState, root: int, stream=None) -> torch.Tensor:
@@ -341,6 +368,21 @@ def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float =
     _check(lib.g5_sssp_run(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
                            g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                            sssp.work.numel(), C.byref(p), _stream(stream)))
+
+
+def oned_graph_sssp_reset(sssp: SsspState, stream=None) -> None:
+    """The workspace reset of oned_graph_sssp_run (the reference's
+    oned_graph_sssp_clear, which its runner keeps outside the timed region)."""
+    _check(lib.g5_sssp_reset(sssp.max_nlocalverts, _ptr(sssp.work), sssp.work.numel(), _stream(stream)))
+
+
+def oned_graph_sssp_traverse(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,
+                             stream=None) -> None:
+    """The search itself, on a reset workspace."""
+    p = SsspParams(delta, blocks)
+    _check(lib.g5_sssp_traverse(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
+                                g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
+                                sssp.work.numel(), C.byref(p), _stream(stream)))
 
 
 def sssp_status(sssp: SsspState, stream=None) -> tuple[int, int]:

@@ -12,8 +12,8 @@
 // walks the combined edge list 32 edges per step (each lane finds its
 // source by a 5-step shuffle search), so low-degree vertices do not leave
 // lanes idle.  Vertices above BIG_DEG sit at the back of the queue and every
-// warp of the grid takes BIG_CHUNK-edge chunks of them from a per-vertex
-// cursor.  A neighbour is claimed with an atomicOr on the visited bitmap;
+// warp of the grid takes BIG_CHUNK-edge chunks of them from one counter
+// (g5_frontier.cuh).  A neighbour is claimed with an atomicOr on the visited bitmap;
 // the winner writes pred/depth and appends it to the next queue with one
 // atomic per warp.
 //
@@ -32,24 +32,48 @@
 #include <algorithm>
 
 #include "g5_common.cuh"
+#include "g5_frontier.cuh"
 
 namespace g5 {
 
 constexpr int BFS_THREADS = 256;
-constexpr unsigned BIG_DEG = 4096;
-constexpr unsigned BIG_CHUNK = 1024;
+constexpr unsigned long long SOLO_EDGES = 4096;  // levels at most this wide run in block 0 alone
+constexpr int BFS_TRACE = 64;                    // levels recorded in the control block
+
+// State every thread keeps identically between levels (also handed from
+// the solo prologue to the grid through the control block).
+struct LevelState {
+    int level, mode, cur, pending, levels, bu_levels;
+    unsigned n_f;
+    unsigned pad;
+    unsigned long long m_f, m_u, reached;
+};
+static_assert(sizeof(LevelState) % 8 == 0, "LevelState is copied in 8-byte words");
 
 struct BfsCtl {
     unsigned bar;  // grid barrier arrivals
     unsigned error;
     unsigned n_small[3];  // per level slot: queue entries of degree <= BIG_DEG
-    unsigned n_big[3];    //                 queue entries above BIG_DEG
+    unsigned long long big[3];  //           big entries << 40 | their chunks
     unsigned grab[3];     //                 work cursor over the small part
+    unsigned cgrab[3];    //                 work cursor over the big part's chunks
     unsigned found[3];    //                 vertices found by a bottom-up level
     unsigned long long m_next[3];  //        degree sum of the next frontier
     int levels;
     int bu_levels;
     unsigned long long reached;
+    // hand-off from the solo prologue to the grid
+    unsigned go;       // 0 wait, 1 continue on the grid, 2 finished
+    unsigned heartbeat;  // solo levels completed so far (waiters restart their clock on change)
+    unsigned hand_fb;  // 1 when the frontier bitmap is the second buffer
+    unsigned solo_levels;
+    LevelState hand;
+    // per-level trace: time at the level's end, frontier size and edges, direction
+    unsigned long long t0;
+    unsigned long long t_level[BFS_TRACE];
+    unsigned long long m_level[BFS_TRACE];
+    unsigned n_level[BFS_TRACE];
+    unsigned char mode_level[BFS_TRACE];
 };
 
 struct BfsArgs {
@@ -64,7 +88,7 @@ struct BfsArgs {
     unsigned *fbits;
     unsigned *nbits;
     unsigned *q[2];
-    unsigned *bigcur[2];
+    unsigned *base[2];  // chunk bases of each queue's big part
     BfsCtl *ctl;
     float alpha;
     float beta;
@@ -78,7 +102,7 @@ enum { TOP_DOWN = 0, BOTTOM_UP = 1 };
 // Claim v for parent u at the next level; appends it to the next queue.
 // All 32 lanes must call it (want = this lane has a candidate).
 __device__ __forceinline__ void td_visit(const BfsArgs &a, bool want, unsigned v, unsigned u, int next_level,
-                                         unsigned *qn, unsigned *bcn, unsigned *n_small, unsigned *n_big,
+                                         unsigned *qn, unsigned *basen, unsigned *n_small, unsigned long long *n_big,
                                          unsigned long long &my_m) {
     if (want && v >= a.n) {  // not a vertex: report it, touch nothing
         atomicOr(&a.ctl->error, DEVERR_RANGE);
@@ -92,15 +116,7 @@ __device__ __forceinline__ void td_visit(const BfsArgs &a, bool want, unsigned v
         deg = __ldg(&a.rowptr[v + 1]) - __ldg(&a.rowptr[v]);
         my_m += deg;
     }
-    const bool small = disc && deg <= BIG_DEG;
-    const bool big = disc && deg > BIG_DEG;
-    unsigned ps = warp_append(n_small, small);
-    if (small) qn[ps] = v;
-    unsigned pb = warp_append(n_big, big);
-    if (big) {
-        qn[a.n - 1 - pb] = v;
-        bcn[pb] = 0;
-    }
+    if (!frontier_append(qn, basen, a.n, n_small, n_big, disc, v, deg)) atomicOr(&a.ctl->error, DEVERR_CAPACITY);
 }
 
 __device__ void td_expand(const BfsArgs &a, int level, int cur, int s_cur, int s_nxt, unsigned long long &my_m) {
@@ -108,10 +124,10 @@ __device__ void td_expand(const BfsArgs &a, int level, int cur, int s_cur, int s
     const unsigned lane = lane_id();
     const unsigned *Q = a.q[cur];
     unsigned *QN = a.q[cur ^ 1];
-    unsigned *BC = a.bigcur[cur];
-    unsigned *BCN = a.bigcur[cur ^ 1];
+    const unsigned *B = a.base[cur];
+    unsigned *BN = a.base[cur ^ 1];
     const unsigned ns = ld_volatile(&c->n_small[s_cur]);
-    const unsigned nb = ld_volatile(&c->n_big[s_cur]);
+    const unsigned long long bp = ld_volatile(&c->big[s_cur]);
 
     // Small part: 32 queue entries per grab, edges gathered across the warp.
     for (;;) {
@@ -135,25 +151,27 @@ __device__ void td_expand(const BfsArgs &a, int level, int cur, int s_cur, int s
             const uint64_t rbj = __shfl_sync(FULL, rb, j);
             const unsigned exj = __shfl_sync(FULL, excl, j);
             const unsigned v = has ? (unsigned)__ldg(&a.col[rbj + (e - exj)]) : 0u;
-            td_visit(a, has, v, uj, level + 1, QN, BCN, &c->n_small[s_nxt], &c->n_big[s_nxt], my_m);
+            td_visit(a, has, v, uj, level + 1, QN, BN, &c->n_small[s_nxt], &c->big[s_nxt], my_m);
         }
     }
-    // Big part: every warp takes chunks of every big vertex.
-    for (unsigned j = 0; j < nb; ++j) {
+    // Big part: chunks of every big vertex from one grid-wide counter.
+    const unsigned nb = big_count(bp);
+    const unsigned long long nch = big_chunks(bp);
+    for (;;) {
+        unsigned ch = 0;
+        if (lane == 0) ch = atomicAdd(&c->cgrab[s_cur], 1u);
+        ch = __shfl_sync(FULL, ch, 0);
+        if (ch >= nch) break;
+        const unsigned j = chunk_owner(B, nb, ch);
         const unsigned u = __ldcg(&Q[a.n - 1 - j]);
         const uint64_t rb = __ldg(&a.rowptr[u]);
         const uint64_t deg = __ldg(&a.rowptr[u + 1]) - rb;
-        for (;;) {
-            unsigned cstart = 0;
-            if (lane == 0) cstart = atomicAdd(&BC[j], BIG_CHUNK);
-            cstart = __shfl_sync(FULL, cstart, 0);
-            if (cstart >= deg) break;
-            const uint64_t cend = min((uint64_t)cstart + BIG_CHUNK, deg);
-            for (uint64_t e = cstart + lane; e < (uint64_t)cstart + BIG_CHUNK; e += 32) {
-                const bool has = e < cend;
-                const unsigned v = has ? (unsigned)__ldg(&a.col[rb + e]) : 0u;
-                td_visit(a, has, v, u, level + 1, QN, BCN, &c->n_small[s_nxt], &c->n_big[s_nxt], my_m);
-            }
+        const uint64_t cs = (uint64_t)(ch - __ldcg(&B[j])) * BIG_CHUNK;
+        const uint64_t ce = min(cs + BIG_CHUNK, deg);
+        for (uint64_t e = cs + lane; e < cs + BIG_CHUNK; e += 32) {
+            const bool has = e < ce;
+            const unsigned v = has ? (unsigned)__ldg(&a.col[rb + e]) : 0u;
+            td_visit(a, has, v, u, level + 1, QN, BN, &c->n_small[s_nxt], &c->big[s_nxt], my_m);
         }
     }
 }
@@ -197,9 +215,9 @@ __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsig
     }
 }
 
-// Next-frontier queue from the bottom-up bitmap (small/big split by degree).
-__device__ void bits_to_queue(const BfsArgs &a, const unsigned *bits, unsigned *qn, unsigned *bcn, unsigned *n_small,
-                              unsigned *n_big) {
+// Frontier queue from a bottom-up bitmap (small/big split by degree).
+__device__ void bits_to_queue(const BfsArgs &a, const unsigned *bits, unsigned *qn, unsigned *basen, unsigned *n_small,
+                              unsigned long long *n_big) {
     const unsigned lane = lane_id();
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -218,16 +236,97 @@ __device__ void bits_to_queue(const BfsArgs &a, const unsigned *bits, unsigned *
                 m &= m - 1;
                 deg = __ldg(&a.rowptr[v + 1]) - __ldg(&a.rowptr[v]);
             }
-            const bool small = has && deg <= BIG_DEG, big = has && deg > BIG_DEG;
-            unsigned ps = warp_append(n_small, small);
-            if (small) qn[ps] = v;
-            unsigned pb = warp_append(n_big, big);
-            if (big) {
-                qn[a.n - 1 - pb] = v;
-                bcn[pb] = 0;
-            }
+            if (!frontier_append(qn, basen, a.n, n_small, n_big, has, v, deg))
+                atomicOr(&a.ctl->error, DEVERR_CAPACITY);
         }
     }
+}
+
+// Direction of the next level (Beamer's rule; a.mode forces one side).
+__device__ __forceinline__ int bfs_decide(const BfsArgs &a, int mode, unsigned n_next, unsigned long long m_next,
+                                          unsigned long long m_u, unsigned n_f, unsigned long long reached) {
+    if (a.mode == 1) return TOP_DOWN;
+    if (a.mode == 2) return BOTTOM_UP;
+    // Beamer's rule, plus: a bottom-up level touches every unvisited vertex,
+    // so it never pays when the frontier's edges are few next to them (late
+    // levels, where unexplored edges belong to other components).
+    if (mode == TOP_DOWN)
+        return ((double)m_next > (double)m_u / a.alpha && 32.0 * (double)m_next > (double)(a.n - reached))
+                   ? BOTTOM_UP
+                   : TOP_DOWN;
+    return ((double)n_next < (double)a.n / a.beta && n_next < n_f) ? TOP_DOWN : BOTTOM_UP;
+}
+
+enum { PEND_NONE = 0, PEND_TO_BITS = 1, PEND_TO_QUEUE = 2 };
+
+// Expands level st.level; adds the next frontier's degree sum and (bottom-up)
+// size into slot s_nxt.  No synchronisation.
+__device__ __forceinline__ void bfs_expand_level(const BfsArgs &a, const LevelState &st, const unsigned *fb,
+                                                 unsigned *nb) {
+    BfsCtl *c = a.ctl;
+    const int s_cur = st.level % 3, s_nxt = (st.level + 1) % 3, s_clr = (st.level + 2) % 3;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c->n_small[s_clr] = 0;
+        c->big[s_clr] = 0;
+        c->grab[s_clr] = 0;
+        c->cgrab[s_clr] = 0;
+        c->found[s_clr] = 0;
+        c->m_next[s_clr] = 0;
+    }
+    unsigned long long my_m = 0;
+    unsigned my_found = 0;
+    if (st.mode == TOP_DOWN)
+        td_expand(a, st.level, st.cur, s_cur, s_nxt, my_m);
+    else
+        bu_expand(a, st.level, fb, nb, my_m, my_found);
+    my_m = warp_sum(my_m);
+    my_found = warp_sum(my_found);
+    if (lane_id() == 0) {
+        if (my_m) atomicAdd(&c->m_next[s_nxt], my_m);
+        if (my_found) atomicAdd(&c->found[s_nxt], my_found);
+    }
+}
+
+// After the level's barrier: next frontier size/edges, trace, direction.
+// Returns false when the search is over.
+__device__ __forceinline__ bool bfs_advance(const BfsArgs &a, LevelState &st, unsigned *&fb, unsigned *&nb) {
+    BfsCtl *c = a.ctl;
+    const int s_nxt = (st.level + 1) % 3;
+    const unsigned long long m_next = ld_volatile(&c->m_next[s_nxt]);
+    const unsigned n_next = st.mode == TOP_DOWN ? ld_volatile(&c->n_small[s_nxt]) + big_count(ld_volatile(&c->big[s_nxt]))
+                                                : ld_volatile(&c->found[s_nxt]);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && st.level < BFS_TRACE) {
+        c->t_level[st.level] = globaltimer_ns();
+        c->n_level[st.level] = st.n_f;
+        c->m_level[st.level] = st.m_f;
+        c->mode_level[st.level] = (unsigned char)st.mode;
+    }
+    ++st.levels;
+    st.bu_levels += st.mode == BOTTOM_UP;
+    st.m_u -= m_next;
+    st.reached += n_next;
+    if (n_next == 0) return false;
+    const int next = bfs_decide(a, st.mode, n_next, m_next, st.m_u, st.n_f, st.reached);
+    if (st.mode == TOP_DOWN) {
+        st.cur ^= 1;  // the next frontier queue is now q[cur]
+        if (next == BOTTOM_UP) st.pending = PEND_TO_BITS;
+    } else {
+        unsigned *t = fb;  // the next frontier bitmap is now fb
+        fb = nb;
+        nb = t;
+        if (next == TOP_DOWN) st.pending = PEND_TO_QUEUE;
+    }
+    st.mode = next;
+    st.n_f = n_next;
+    st.m_f = m_next;
+    ++st.level;
+    return true;
+}
+
+__device__ __forceinline__ void bfs_write_stats(const BfsArgs &a, const LevelState &st) {
+    a.ctl->levels = st.levels;
+    a.ctl->bu_levels = st.bu_levels;
+    a.ctl->reached = st.reached;
 }
 
 __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs a) {
@@ -235,114 +334,125 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
     unsigned epoch = 0;
     const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t E = __ldg(&a.rowptr[a.n]);
-    const uint64_t root_deg = __ldg(&a.rowptr[a.root + 1]) - __ldg(&a.rowptr[a.root]);
+    unsigned *fb = a.fbits, *nb = a.nbits;
+    LevelState st;
 
-    if (gtid == 0) {
-        a.visited[a.root >> 5] |= 1u << (a.root & 31);
-        a.pred[a.root] = a.root;
-        if (a.depth) a.depth[a.root] = 0;
-        if (root_deg > BIG_DEG) {
-            a.q[0][a.n - 1] = a.root;
-            a.bigcur[0][0] = 0;
-            c->n_big[0] = 1;
-        } else {
-            a.q[0][0] = a.root;
-            c->n_small[0] = 1;
+    // ---- Solo prologue: block 0 alone runs the first levels while the
+    // frontier is small (every search starts with one vertex), syncing with
+    // __syncthreads only; the other blocks wait for the hand-off.  A search
+    // that stays small -- a root in a small component -- ends here without a
+    // single grid barrier.
+    if (blockIdx.x == 0) {
+        const uint64_t E = __ldg(&a.rowptr[a.n]);
+        const uint64_t root_deg = __ldg(&a.rowptr[a.root + 1]) - __ldg(&a.rowptr[a.root]);
+        if (threadIdx.x == 0) {
+            c->t0 = globaltimer_ns();
+            a.visited[a.root >> 5] |= 1u << (a.root & 31);
+            a.pred[a.root] = a.root;
+            if (a.depth) a.depth[a.root] = 0;
+            if (root_deg > BIG_DEG) {
+                a.q[0][a.n - 1] = a.root;
+                a.base[0][0] = 0;
+                c->big[0] = (1ull << BIG_SHIFT) | ((root_deg + BIG_CHUNK - 1) / BIG_CHUNK);
+            } else {
+                a.q[0][0] = a.root;
+                c->n_small[0] = 1;
+            }
+        }
+        st = LevelState{0, TOP_DOWN, 0, PEND_NONE, 0, 0, 1u, 0u, root_deg, E - root_deg, 1ull};
+        __syncthreads();
+        bool done = false;
+        int solo = 0;
+        while (a.nblocks == 1 || (st.mode == TOP_DOWN && st.pending == PEND_NONE && st.m_f <= SOLO_EDGES)) {
+            if (a.nblocks == 1 && st.pending != PEND_NONE) break;  // conversions run in the grid loop
+            bfs_expand_level(a, st, fb, nb);
+            __threadfence();
+            __syncthreads();
+            ++solo;
+            if (threadIdx.x == 0) atomicAdd(&c->heartbeat, 1u);
+            if (!bfs_advance(a, st, fb, nb)) {
+                done = true;
+                break;
+            }
+            __syncthreads();  // everyone has read the counters before they are reused
+        }
+        if (threadIdx.x == 0) {
+            c->hand = st;
+            c->hand_fb = fb == a.fbits ? 0 : 1;
+            c->solo_levels = solo;
+            if (done) bfs_write_stats(a, st);
+            __threadfence();
+            atomicExch(&c->go, done ? 2u : 1u);
+        }
+        if (done) return;
+    } else {
+        __shared__ unsigned s_go;
+        if (threadIdx.x == 0) {
+            // Bounded wait: the clock restarts whenever block 0 finishes a
+            // level, so only a stalled prologue times out.
+            unsigned long long t0 = globaltimer_ns();
+            unsigned beat = ld_volatile(&c->heartbeat);
+            unsigned g;
+            while ((g = ld_acquire(&c->go)) == 0) {
+                const unsigned b = ld_volatile(&c->heartbeat);
+                if (b != beat) {
+                    beat = b;
+                    t0 = globaltimer_ns();
+                }
+                if (globaltimer_ns() - t0 > a.limit_ns) {
+                    atomicOr(&c->error, DEVERR_TIMEOUT);
+                    g = 2;
+                    break;
+                }
+                __nanosleep(64);
+            }
+            s_go = g;
+        }
+        __syncthreads();
+        if (s_go == 2) return;
+        const unsigned long long *src = (const unsigned long long *)&c->hand;
+        unsigned long long *dst = (unsigned long long *)&st;
+        for (unsigned i = 0; i < sizeof(LevelState) / 8; ++i) dst[i] = __ldcg(&src[i]);
+        if (ld_volatile(&c->hand_fb)) {
+            fb = a.nbits;
+            nb = a.fbits;
         }
     }
-    if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
 
-    int mode = TOP_DOWN;
-    int cur = 0;
-    unsigned *fb = a.fbits, *nb = a.nbits;
-    uint64_t m_u = E - root_deg;
-    unsigned n_f = 1;
-    unsigned long long reached = 1;
-    int levels = 0, bu_levels = 0;
-
-    for (int level = 0;; ++level) {
-        const int s_cur = level % 3, s_nxt = (level + 1) % 3, s_clr = (level + 2) % 3;
-        if (gtid == 0) {
-            c->n_small[s_clr] = 0;
-            c->n_big[s_clr] = 0;
-            c->grab[s_clr] = 0;
-            c->found[s_clr] = 0;
-            c->m_next[s_clr] = 0;
-        }
-        unsigned long long my_m = 0;
-        unsigned my_found = 0;
-        if (mode == TOP_DOWN)
-            td_expand(a, level, cur, s_cur, s_nxt, my_m);
-        else
-            bu_expand(a, level, fb, nb, my_m, my_found);
-        my_m = warp_sum(my_m);
-        my_found = warp_sum(my_found);
-        if (lane_id() == 0) {
-            if (my_m) atomicAdd(&c->m_next[s_nxt], my_m);
-            if (my_found) atomicAdd(&c->found[s_nxt], my_found);
-        }
-        ++levels;
-        bu_levels += mode == BOTTOM_UP;
-        if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
-
-        const unsigned long long m_next = ld_volatile(&c->m_next[s_nxt]);
-        const unsigned n_next = mode == TOP_DOWN
-                                    ? ld_volatile(&c->n_small[s_nxt]) + ld_volatile(&c->n_big[s_nxt])
-                                    : ld_volatile(&c->found[s_nxt]);
-        m_u -= m_next;
-        reached += n_next;
-        if (n_next == 0) break;
-
-        int next = mode;
-        if (a.mode == 1) {
-            next = TOP_DOWN;
-        } else if (a.mode == 2) {
-            next = BOTTOM_UP;
-        } else if (mode == TOP_DOWN) {
-            if ((double)m_next > (double)m_u / a.alpha) next = BOTTOM_UP;
-        } else {
-            if ((double)n_next < (double)a.n / a.beta && n_next < n_f) next = TOP_DOWN;
-        }
-
-        if (mode == TOP_DOWN && next == BOTTOM_UP) {
-            // Frontier bitmap from the queue just built.
+    // ---- Grid loop.
+    for (;;) {
+        const int s_cur = st.level % 3;
+        if (st.pending == PEND_TO_BITS) {
+            // Frontier bitmap from the queue q[cur].
             for (uint64_t k = gtid; k < a.nwords; k += nthreads) fb[k] = 0;
             if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
-            const unsigned *QN = a.q[cur ^ 1];
-            const unsigned ns = ld_volatile(&c->n_small[s_nxt]), nbg = ld_volatile(&c->n_big[s_nxt]);
+            const unsigned *Q = a.q[st.cur];
+            const unsigned ns = ld_volatile(&c->n_small[s_cur]), nbg = big_count(ld_volatile(&c->big[s_cur]));
             for (uint64_t i = gtid; i < ns; i += nthreads) {
-                unsigned v = __ldcg(&QN[i]);
+                const unsigned v = __ldcg(&Q[i]);
                 atomicOr(&fb[v >> 5], 1u << (v & 31));
             }
             for (uint64_t i = gtid; i < nbg; i += nthreads) {
-                unsigned v = __ldcg(&QN[a.n - 1 - i]);
+                const unsigned v = __ldcg(&Q[a.n - 1 - i]);
                 atomicOr(&fb[v >> 5], 1u << (v & 31));
             }
             if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
-        } else if (mode == BOTTOM_UP && next == BOTTOM_UP) {
-            unsigned *t = fb;
-            fb = nb;
-            nb = t;
-        } else if (mode == BOTTOM_UP && next == TOP_DOWN) {
-            bits_to_queue(a, nb, a.q[cur ^ 1], a.bigcur[cur ^ 1], &c->n_small[s_nxt], &c->n_big[s_nxt]);
+        } else if (st.pending == PEND_TO_QUEUE) {
+            bits_to_queue(a, fb, a.q[st.cur], a.base[st.cur], &c->n_small[s_cur], &c->big[s_cur]);
             if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
         }
-        if (next == TOP_DOWN) cur ^= 1;
-        mode = next;
-        n_f = n_next;
+        st.pending = PEND_NONE;
+        bfs_expand_level(a, st, fb, nb);
+        if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+        if (!bfs_advance(a, st, fb, nb)) break;
     }
-    if (gtid == 0) {
-        c->levels = levels;
-        c->bu_levels = bu_levels;
-        c->reached = reached;
-    }
+    if (gtid == 0) bfs_write_stats(a, st);
 }
 
 struct BfsWork {
     BfsCtl *ctl;
     unsigned *visited, *fbits, *nbits;
-    unsigned *q[2], *bigcur[2];
+    unsigned *q[2], *base[2];
     uint64_t bytes;
 };
 
@@ -356,7 +466,7 @@ static BfsWork carve_bfs(void *base, uint64_t n) {
     w.nbits = c.take<unsigned>(words);
     for (int i = 0; i < 2; ++i) {
         w.q[i] = c.take<unsigned>(n);
-        w.bigcur[i] = c.take<unsigned>(n);
+        w.base[i] = c.take<unsigned>(n);
     }
     w.bytes = c.used;
     return w;
@@ -441,8 +551,38 @@ static int bfs_check(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t
     return G5_OK;
 }
 
-extern "C" int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
-                            void *stream) {
+// Bit v set when vertex v has no CSR entry (it can only ever be a root).
+__global__ void isolated_bits_kernel(const uint64_t *__restrict__ rowptr, uint64_t n, unsigned *__restrict__ bits) {
+    const uint64_t words = (n + 31) / 32;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < words; k += stride) {
+        unsigned m = 0;
+        const uint64_t v0 = k * 32;
+        const uint64_t vend = min(v0 + 32, n);
+        uint64_t prev = __ldg(&rowptr[v0]);
+        for (uint64_t v = v0; v < vend; ++v) {
+            const uint64_t next = __ldg(&rowptr[v + 1]);
+            if (next == prev) m |= 1u << (v - v0);
+            prev = next;
+        }
+        bits[k] = m;
+    }
+}
+
+extern "C" int g5_graph_isolated_bitmap(const uint64_t *d_rowstarts, uint64_t nverts, uint32_t *d_bits,
+                                        void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31) && d_rowstarts && d_bits, "g5_graph_isolated_bitmap: bad argument");
+    DeviceInfo di;
+    int rc = device_info(&di);
+    if (rc) return rc;
+    isolated_bits_kernel<<<di.sms * 4, 256, 0, (cudaStream_t)stream>>>(d_rowstarts, nverts, d_bits);
+    G5_CUDA_TRY(cudaGetLastError());
+    return G5_OK;
+}
+
+extern "C" int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, const uint32_t *d_visited_init,
+                            void *d_work, uint64_t work_bytes, void *stream) {
     clear_error();
     G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31) && d_pred && d_work, "g5_bfs_reset: bad argument");
     BfsWork w = carve_bfs(d_work, nverts);
@@ -450,8 +590,11 @@ extern "C" int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, 
     cudaStream_t st = (cudaStream_t)stream;
     G5_CUDA_TRY(cudaMemsetAsync(d_pred, 0xff, nverts * sizeof(int64_t), st));
     if (d_depth) G5_CUDA_TRY(cudaMemsetAsync(d_depth, 0xff, nverts * sizeof(int32_t), st));
-    G5_CUDA_TRY(cudaMemsetAsync(w.visited, 0, (nverts + 31) / 32 * sizeof(unsigned), st));
-    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(BfsCtl), st));
+    const uint64_t vbytes = (nverts + 31) / 32 * sizeof(unsigned);
+    if (d_visited_init)
+        G5_CUDA_TRY(cudaMemcpyAsync(w.visited, d_visited_init, vbytes, cudaMemcpyDeviceToDevice, st));
+    else
+        G5_CUDA_TRY(cudaMemsetAsync(w.visited, 0, vbytes, st));
     return G5_OK;
 }
 
@@ -483,8 +626,8 @@ extern "C" int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col
     a.nbits = w.nbits;
     a.q[0] = w.q[0];
     a.q[1] = w.q[1];
-    a.bigcur[0] = w.bigcur[0];
-    a.bigcur[1] = w.bigcur[1];
+    a.base[0] = w.base[0];
+    a.base[1] = w.base[1];
     a.ctl = w.ctl;
     a.alpha = p.alpha;
     a.beta = p.beta;
@@ -492,6 +635,9 @@ extern "C" int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col
     a.nblocks = (unsigned)blocks;
     a.limit_ns = wait_limit_ns();
     void *args[] = {&a};
+    // The control block (counters, hand-off, barrier) starts from zero on
+    // every search, so a traversal never sees the previous one's state.
+    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(BfsCtl), (cudaStream_t)stream));
     G5_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)bfs_persistent_kernel, dim3(blocks), dim3(BFS_THREADS), args,
                                             0, (cudaStream_t)stream));
     return G5_OK;
@@ -504,7 +650,7 @@ extern "C" int g5_bfs_run(const uint64_t *d_rowstarts, const int32_t *d_col, uin
     BfsWork w;
     int rc = bfs_check(d_rowstarts, d_col, nverts, root, d_pred, d_work, work_bytes, &w, "g5_bfs_run");
     if (rc) return rc;
-    if ((rc = g5_bfs_reset(nverts, d_pred, d_depth, d_work, work_bytes, stream))) return rc;
+    if ((rc = g5_bfs_reset(nverts, d_pred, d_depth, nullptr, d_work, work_bytes, stream))) return rc;
     return g5_bfs_traverse(d_rowstarts, d_col, nverts, root, d_pred, d_depth, d_work, work_bytes, params, stream);
 }
 
@@ -519,6 +665,29 @@ extern "C" int g5_bfs_last_stats(const void *d_work, uint64_t work_bytes, g5_bfs
     stats->levels = c.levels;
     stats->bottom_up_levels = c.bu_levels;
     stats->reached = c.reached;
+    return deverr_to_status(c.error, "g5_bfs_run");
+}
+
+extern "C" int g5_bfs_last_trace(const void *d_work, uint64_t work_bytes, int max_levels, int32_t *mode,
+                                  uint64_t *frontier_vertices, uint64_t *frontier_edges, double *level_ms,
+                                  int32_t *nlevels, int32_t *solo_levels, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(d_work && work_bytes >= sizeof(BfsCtl) && nlevels, "g5_bfs_last_trace: bad argument");
+    BfsCtl c;
+    cudaStream_t st = (cudaStream_t)stream;
+    G5_CUDA_TRY(cudaMemcpyAsync(&c, d_work, sizeof c, cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    const int n = std::min(std::min(c.levels, BFS_TRACE), std::max(max_levels, 0));
+    unsigned long long prev = c.t0;
+    for (int i = 0; i < n; ++i) {
+        if (mode) mode[i] = c.mode_level[i];
+        if (frontier_vertices) frontier_vertices[i] = c.n_level[i];
+        if (frontier_edges) frontier_edges[i] = c.m_level[i];
+        if (level_ms) level_ms[i] = (double)(c.t_level[i] - prev) * 1e-6;
+        prev = c.t_level[i];
+    }
+    *nlevels = c.levels;
+    if (solo_levels) *solo_levels = (int32_t)c.solo_levels;
     return deverr_to_status(c.error, "g5_bfs_run");
 }
 

@@ -16,10 +16,12 @@ namespace g5compat {
 struct GraphExt {
     int32_t *col;        // int32 neighbour ids, light-first rows
     uint32_t *light_deg; // light entries per row
+    uint32_t *isolated;  // bitmap of degree-0 vertices
     float light_delta;
 };
 
 struct BfsExt {
+    const uint32_t *isolated;  // the graph's isolated-vertex bitmap
     int32_t *depth;
     void *work;  // BFS kernel workspace (its statistics live at the front)
     uint64_t work_bytes;

@@ -35,10 +35,12 @@ Oned_Graph oned_graph_from_tuple_graph(Worker_State *ws, Tuple_Graph *tg, u64 ng
     x.col = (int32_t *)gpu_push(ws, g.nlocaledges * sizeof(int32_t), "int32 column");
     x.light_deg = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "light degrees");
     x.light_delta = kLightDelta;
+    x.isolated = (uint32_t *)gpu_push(ws, (nglobalverts + 31) / 32 * sizeof(uint32_t), "isolated-vertex bitmap");
     check(ws,
           g5_csr_fill((const uint64_t *)tg->edges, tg->weights, tg->edges_size, nglobalverts, g.rowstarts,
                       kLightDelta, work, wbytes, x.col, g.weights, g.column, x.light_deg, 0),
           "oned_graph_from_tuple_graph");
+    check(ws, g5_graph_isolated_bitmap(g.rowstarts, nglobalverts, x.isolated, 0), "oned_graph_from_tuple_graph");
     CHECK_CUDA(cudaDeviceSynchronize());
     put_graph(g.rowstarts, x);
     return g;
@@ -60,6 +62,7 @@ Bfs_State oned_graph_bfs_create(Worker_State *ws, const Oned_Graph *g) {
     memset(&bfs, 0, sizeof bfs);
     bfs.pred = worker_arena_push_array(ws, g->nlocalverts, i64, &bfs.max_nlocalverts);
     BfsExt x;
+    x.isolated = get_graph(g, ws)->isolated;
     x.depth = (int32_t *)gpu_push(ws, g->nlocalverts * sizeof(int32_t), "BFS depth");
     check(ws, g5_bfs_workspace_size(g->nglobalverts, &x.work_bytes), "oned_graph_bfs_create");
     x.work = gpu_push(ws, x.work_bytes, "BFS workspace");
@@ -71,8 +74,13 @@ Bfs_State oned_graph_bfs_create(Worker_State *ws, const Oned_Graph *g) {
 }
 
 void oned_graph_bfs_clear(Worker_State *ws, Bfs_State *bfs) {
-    (void)ws;
-    CHECK_CUDA(cudaMemset(bfs->pred, 0xff, bfs->max_nlocalverts * sizeof(i64)));
+    const BfsExt *bx = get_bfs(bfs->pred);
+    if (!bx) {
+        ERROR("Bfs_State was not created by oned_graph_bfs_create of this library");
+        worker_abort(ws, 1);
+    }
+    check(ws, g5_bfs_reset(bfs->max_nlocalverts, bfs->pred, bx->depth, bx->isolated, bx->work, bx->work_bytes, 0),
+          "oned_graph_bfs_clear");
     if (bfs->dist) CHECK_CUDA(cudaMemset(bfs->dist, 0xff, bfs->max_nlocalverts * sizeof(i64)));
     CHECK_CUDA(cudaDeviceSynchronize());
 }
@@ -89,8 +97,10 @@ void oned_graph_bfs_run(Worker_State *ws, const Oned_Graph *g, Bfs_State *bfs, u
         ERROR("Bfs_State was not created by oned_graph_bfs_create of this library");
         worker_abort(ws, 1);
     }
-    check(ws, g5_bfs_run(g->rowstarts, gx->col, g->nglobalverts, root, bfs->pred, bx->depth, bx->work, bx->work_bytes,
-                         nullptr, 0),
+    // The reset half ran in oned_graph_bfs_clear, which the reference's
+    // protocol calls before every search (examples/graph500_runner.cu:309).
+    check(ws, g5_bfs_traverse(g->rowstarts, gx->col, g->nglobalverts, root, bfs->pred, bx->depth, bx->work,
+                              bx->work_bytes, nullptr, 0),
           "oned_graph_bfs_run");
     g5_bfs_stats st;
     check(ws, g5_bfs_last_stats(bx->work, bx->work_bytes, &st, 0), "oned_graph_bfs_run");
@@ -140,7 +150,12 @@ Sssp_State oned_graph_sssp_create(Worker_State *ws, const Oned_Graph *g) {
 }
 
 void oned_graph_sssp_clear(Worker_State *ws, Sssp_State *sssp) {
-    (void)ws;
+    const SsspExt *sx = get_sssp(sssp->pred);
+    if (!sx) {
+        ERROR("Sssp_State was not created by oned_graph_sssp_create of this library");
+        worker_abort(ws, 1);
+    }
+    check(ws, g5_sssp_reset(sssp->max_nlocalverts, sx->work, sx->work_bytes, 0), "oned_graph_sssp_clear");
     CHECK_CUDA(cudaMemset(sssp->pred, 0xff, sssp->max_nlocalverts * sizeof(i64)));
     // -1.0f everywhere, the reference's "unreached" (src/traversal.cu:250).
     fill_minus_one<<<256, 256>>>(sssp->dist, sssp->max_nlocalverts);
@@ -161,8 +176,8 @@ void oned_graph_sssp_run(Worker_State *ws, const Oned_Graph *g, Sssp_State *sssp
         worker_abort(ws, 1);
     }
     g5_sssp_params p = {kLightDelta, 0};
-    check(ws, g5_sssp_run(g->rowstarts, gx->col, g->weights, gx->light_deg, gx->light_delta, g->nglobalverts, root,
-                          sssp->dist, sssp->pred, sx->work, sx->work_bytes, &p, 0),
+    check(ws, g5_sssp_traverse(g->rowstarts, gx->col, g->weights, gx->light_deg, gx->light_delta, g->nglobalverts,
+                               root, sssp->dist, sssp->pred, sx->work, sx->work_bytes, &p, 0),
           "oned_graph_sssp_run");
     check(ws, g5_sssp_last_status(sx->work, sx->work_bytes, nullptr, nullptr, 0), "oned_graph_sssp_run");
 }

@@ -32,23 +32,23 @@
 #include <algorithm>
 
 #include "g5_common.cuh"
+#include "g5_frontier.cuh"
 
 namespace g5 {
 
 constexpr int SSSP_THREADS = 256;
 constexpr int RING = 16;  // bucket queues; a relaxation may land at most RING-1 buckets ahead
-constexpr unsigned SBIG_DEG = 4096;
-constexpr unsigned SBIG_CHUNK = 1024;
 constexpr unsigned long long UNREACHED = ~0ull;
 
 struct SsspCtl {
     unsigned bar;
     unsigned error;
     unsigned grab[3];    // per phase slot: cursor over the input list's small part
+    unsigned cgrab[3];   //                 cursor over the input list's big-part chunks
     unsigned f_small[3]; // per phase slot: frontier produced for the next phase
-    unsigned f_big[3];
+    unsigned long long f_big[3];
     unsigned s_small[2]; // per bucket parity: heavy set
-    unsigned s_big[2];
+    unsigned long long s_big[2];
     unsigned ring_len[RING];
     unsigned long long buckets;
     unsigned long long phases;
@@ -65,8 +65,8 @@ struct SsspArgs {
     unsigned long long *pack;
     unsigned *fstamp, *sstamp, *qstamp;
     unsigned *settled;
-    unsigned *F[2], *FB[2];
-    unsigned *S[2], *SB[2];
+    unsigned *F[2], *FB[2];  // frontiers and the chunk bases of their big parts
+    unsigned *S[2], *SB[2];  // heavy sets and chunk bases
     unsigned *ring;
     SsspCtl *ctl;
     unsigned nblocks;
@@ -106,25 +106,11 @@ __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCt
     uint64_t lb = 0, le = 0, hb = 0, he = 0;
     if (f) part_range(a, v, false, lb, le);
     if (s) part_range(a, v, true, hb, he);
-    const bool fs = f && le - lb <= SBIG_DEG, fb = f && le - lb > SBIG_DEG;
-    const bool ss = s && he - hb <= SBIG_DEG, sb = s && he - hb > SBIG_DEG;
     // Each vertex enters a frontier once per phase and a heavy set once per
-    // bucket, so no list exceeds n entries; the guards only keep a broken
-    // invariant from writing outside the lists.
-    unsigned p = warp_append(&c->f_small[x.f_slot], fs);
-    if (fs && p < a.n) x.Fout[p] = v;
-    p = warp_append(&c->f_big[x.f_slot], fb);
-    if (fb && p < a.n) {
-        x.Fout[a.n - 1 - p] = v;
-        x.FBout[p] = 0;
-    }
-    p = warp_append(&c->s_small[x.s_par], ss);
-    if (ss && p < a.n) x.Sl[p] = v;
-    p = warp_append(&c->s_big[x.s_par], sb);
-    if (sb && p < a.n) {
-        x.Sl[a.n - 1 - p] = v;
-        x.SBl[p] = 0;
-    }
+    // bucket, so no list exceeds n entries.
+    bool ok = frontier_append(x.Fout, x.FBout, a.n, &c->f_small[x.f_slot], &c->f_big[x.f_slot], f, v, le - lb);
+    ok &= frontier_append(x.Sl, x.SBl, a.n, &c->s_small[x.s_par], &c->s_big[x.s_par], s, v, he - hb);
+    if (!ok) atomicOr(&c->error, DEVERR_CAPACITY);
 }
 
 // Relaxes u -> v with float weight wt from distance du; queues v when its
@@ -173,9 +159,10 @@ __device__ __forceinline__ void relax(const SsspArgs &a, const PushCtx &x, bool 
 }
 
 // Relaxes the light (heavy = false) or heavy edges of every vertex of list L
-// (small part [0, ns), big part at the back [n-nb, n)).
-__device__ void expand_list(const SsspArgs &a, const PushCtx &x, const unsigned *L, unsigned ns, unsigned nb,
-                            unsigned *bigcur, unsigned *grab, bool heavy) {
+// (small part [0, ns), big part at the back, `bp` its packed counter).  The
+// heavy pass also marks each list vertex settled.
+__device__ void expand_list(const SsspArgs &a, const PushCtx &x, const unsigned *L, unsigned ns,
+                            unsigned long long bp, const unsigned *B, unsigned *grab, unsigned *cgrab, bool heavy) {
     const unsigned lane = lane_id();
     const bool filtered = a.ld == nullptr;
     for (;;) {
@@ -216,33 +203,34 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, const unsigned 
             relax(a, x, has, uj, duj, v, wt, heavy);
         }
     }
-    for (unsigned j = 0; j < nb; ++j) {
+    const unsigned nb = big_count(bp);
+    const unsigned long long nch = big_chunks(bp);
+    for (;;) {
+        unsigned ch = 0;
+        if (lane == 0) ch = atomicAdd(cgrab, 1u);
+        ch = __shfl_sync(FULL, ch, 0);
+        if (ch >= nch) break;
+        const unsigned j = chunk_owner(B, nb, ch);
         const unsigned u = __ldcg(&L[a.n - 1 - j]);
+        const unsigned first = __ldcg(&B[j]);
         uint64_t rb, re;
         part_range(a, u, heavy, rb, re);
         const float du = pack_dist(__ldcg(&a.pack[u]));
+        if (heavy && ch == first && lane == 0) atomicOr(&a.settled[u >> 5], 1u << (u & 31));
         const uint64_t deg = re - rb;
-        for (;;) {
-            unsigned cs = 0;
-            if (lane == 0) cs = atomicAdd(&bigcur[j], SBIG_CHUNK);
-            cs = __shfl_sync(FULL, cs, 0);
-            if (cs >= deg) break;
-            if (heavy && cs == 0 && lane == 0) atomicOr(&a.settled[u >> 5], 1u << (u & 31));
-            const uint64_t ce = min((uint64_t)cs + SBIG_CHUNK, deg);
-            for (uint64_t e = cs + lane; e < (uint64_t)cs + SBIG_CHUNK; e += 32) {
-                bool has = e < ce;
-                unsigned v = 0;
-                float wt = 0.0f;
-                if (has) {
-                    v = (unsigned)__ldg(&a.col[rb + e]);
-                    wt = __ldg(&a.w[rb + e]);
-                    if (filtered) has = heavy ? !(wt < a.delta) : wt < a.delta;
-                }
-                relax(a, x, has, u, du, v, wt, heavy);
+        const uint64_t cs = (uint64_t)(ch - first) * BIG_CHUNK;
+        const uint64_t ce = min(cs + BIG_CHUNK, deg);
+        for (uint64_t e = cs + lane; e < cs + BIG_CHUNK; e += 32) {
+            bool has = e < ce;
+            unsigned v = 0;
+            float wt = 0.0f;
+            if (has) {
+                v = (unsigned)__ldg(&a.col[rb + e]);
+                wt = __ldg(&a.w[rb + e]);
+                if (filtered) has = heavy ? !(wt < a.delta) : wt < a.delta;
             }
+            relax(a, x, has, u, du, v, wt, heavy);
         }
-        // A big vertex without heavy edges is still settled.
-        if (heavy && deg == 0 && lane == 0) atomicOr(&a.settled[u >> 5], 1u << (u & 31));
     }
 }
 
@@ -283,8 +271,10 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
         {
             const int s_nxt = (phase + 1) % 3, s_clr = (phase + 2) % 3;
             if (gtid == 0) {
-                c->grab[s_clr] = c->f_small[s_clr] = c->f_big[s_clr] = 0;
-                c->s_small[(bucket + 1) & 1] = c->s_big[(bucket + 1) & 1] = 0;
+                c->grab[s_clr] = c->cgrab[s_clr] = c->f_small[s_clr] = 0;
+                c->f_big[s_clr] = 0;
+                c->s_small[(bucket + 1) & 1] = 0;
+                c->s_big[(bucket + 1) & 1] = 0;
             }
             x.pid = phase;
             x.f_slot = s_nxt;
@@ -313,27 +303,35 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
         // ---- light iterations until the bucket's frontier is empty.
         for (;;) {
             const int s_cur = phase % 3, s_nxt = (phase + 1) % 3, s_clr = (phase + 2) % 3;
-            const unsigned ns = ld_volatile(&c->f_small[s_cur]), nb = ld_volatile(&c->f_big[s_cur]);
-            if (ns + nb == 0) break;
-            if (gtid == 0) c->grab[s_clr] = c->f_small[s_clr] = c->f_big[s_clr] = 0;
+            const unsigned ns = ld_volatile(&c->f_small[s_cur]);
+            const unsigned long long bp = ld_volatile(&c->f_big[s_cur]);
+            if (ns + big_count(bp) == 0) break;
+            if (gtid == 0) {
+                c->grab[s_clr] = c->cgrab[s_clr] = c->f_small[s_clr] = 0;
+                c->f_big[s_clr] = 0;
+            }
             x.pid = phase;
             x.f_slot = s_nxt;
             x.Fout = a.F[(phase + 1) & 1];
             x.FBout = a.FB[(phase + 1) & 1];
-            expand_list(a, x, a.F[phase & 1], ns, nb, a.FB[phase & 1], &c->grab[s_cur], false);
+            expand_list(a, x, a.F[phase & 1], ns, bp, a.FB[phase & 1], &c->grab[s_cur], &c->cgrab[s_cur], false);
             if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
             ++phase;
         }
         // ---- heavy edges of every vertex settled in this bucket.
         {
             const int s_cur = phase % 3, s_nxt = (phase + 1) % 3, s_clr = (phase + 2) % 3;
-            if (gtid == 0) c->grab[s_clr] = c->f_small[s_clr] = c->f_big[s_clr] = 0;
+            if (gtid == 0) {
+                c->grab[s_clr] = c->cgrab[s_clr] = c->f_small[s_clr] = 0;
+                c->f_big[s_clr] = 0;
+            }
             x.pid = phase;
             x.f_slot = s_nxt;
             x.Fout = a.F[(phase + 1) & 1];
             x.FBout = a.FB[(phase + 1) & 1];
-            const unsigned ns = ld_volatile(&c->s_small[bucket & 1]), nb = ld_volatile(&c->s_big[bucket & 1]);
-            expand_list(a, x, a.S[bucket & 1], ns, nb, a.SB[bucket & 1], &c->grab[s_cur], true);
+            const unsigned ns = ld_volatile(&c->s_small[bucket & 1]);
+            const unsigned long long bp = ld_volatile(&c->s_big[bucket & 1]);
+            expand_list(a, x, a.S[bucket & 1], ns, bp, a.SB[bucket & 1], &c->grab[s_cur], &c->cgrab[s_cur], true);
             if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
             ++phase;
         }
@@ -420,37 +418,50 @@ extern "C" int g5_sssp_workspace_size(uint64_t nverts, uint64_t *bytes) {
     return G5_OK;
 }
 
-extern "C" int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
-                           const uint32_t *d_light_deg, float light_delta, uint64_t nverts, uint64_t root,
-                           float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes,
-                           const g5_sssp_params *params, void *stream) {
-    clear_error();
-    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_sssp_run: nverts outside [1, 2^31]");
-    G5_CHECK_ARG(root < nverts, "g5_sssp_run: root %llu outside [0, %llu)", (unsigned long long)root,
+static int sssp_check(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, uint64_t nverts,
+                      uint64_t root, float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes, SsspWork *w,
+                      const char *who) {
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "%s: nverts outside [1, 2^31]", who);
+    G5_CHECK_ARG(root < nverts, "%s: root %llu outside [0, %llu)", who, (unsigned long long)root,
                  (unsigned long long)nverts);
-    G5_CHECK_ARG(d_rowstarts && d_col && d_w && d_dist && d_pred && d_work, "g5_sssp_run: NULL argument");
+    G5_CHECK_ARG(d_rowstarts && d_col && d_w && d_dist && d_pred && d_work, "%s: NULL argument", who);
+    *w = carve_sssp(d_work, nverts);
+    if (work_bytes < w->bytes)
+        return set_error(G5_ERR_WORKSPACE, "%s: workspace %llu < %llu bytes", who, (unsigned long long)work_bytes,
+                         (unsigned long long)w->bytes);
+    return G5_OK;
+}
+
+extern "C" int g5_sssp_reset(uint64_t nverts, void *d_work, uint64_t work_bytes, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31) && d_work, "g5_sssp_reset: bad argument");
     SsspWork w = carve_sssp(d_work, nverts);
-    if (work_bytes < w.bytes)
-        return set_error(G5_ERR_WORKSPACE, "g5_sssp_run: workspace %llu < %llu bytes", (unsigned long long)work_bytes,
-                         (unsigned long long)w.bytes);
+    if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "g5_sssp_reset: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    G5_CUDA_TRY(cudaMemsetAsync(w.pack, 0xff, nverts * sizeof(unsigned long long), st));
+    // fstamp, sstamp, qstamp are consecutive carve-outs: one memset.
+    G5_CUDA_TRY(cudaMemsetAsync(w.fstamp, 0xff, (char *)(w.qstamp + nverts) - (char *)w.fstamp, st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.settled, 0, (nverts + 31) / 32 * sizeof(unsigned), st));
+    return G5_OK;
+}
+
+extern "C" int g5_sssp_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
+                                const uint32_t *d_light_deg, float light_delta, uint64_t nverts, uint64_t root,
+                                float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes,
+                                const g5_sssp_params *params, void *stream) {
+    clear_error();
+    SsspWork w;
+    int rc = sssp_check(d_rowstarts, d_col, d_w, nverts, root, d_dist, d_pred, d_work, work_bytes, &w,
+                        "g5_sssp_traverse");
+    if (rc) return rc;
     g5_sssp_params p = {0.1f, 0};
     if (params) p = *params;
-    G5_CHECK_ARG(p.delta > 0.0f, "g5_sssp_run: delta must be positive");
-
+    G5_CHECK_ARG(p.delta > 0.0f, "g5_sssp_traverse: delta must be positive");
     int max_blocks = 0;
-    int rc = sssp_max_blocks(&max_blocks);
-    if (rc) return rc;
+    if ((rc = sssp_max_blocks(&max_blocks))) return rc;
     int blocks = p.blocks > 0 ? std::min(p.blocks, max_blocks)
                               : (int)std::min<uint64_t>(max_blocks, std::max<uint64_t>(1, nverts / 2048));
-
     cudaStream_t st = (cudaStream_t)stream;
-    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(SsspCtl), st));
-    G5_CUDA_TRY(cudaMemsetAsync(w.pack, 0xff, nverts * sizeof(unsigned long long), st));
-    G5_CUDA_TRY(cudaMemsetAsync(w.fstamp, 0xff, nverts * sizeof(unsigned), st));
-    G5_CUDA_TRY(cudaMemsetAsync(w.sstamp, 0xff, nverts * sizeof(unsigned), st));
-    G5_CUDA_TRY(cudaMemsetAsync(w.qstamp, 0xff, nverts * sizeof(unsigned), st));
-    G5_CUDA_TRY(cudaMemsetAsync(w.settled, 0, (nverts + 31) / 32 * sizeof(unsigned), st));
-
     SsspArgs a;
     a.rowptr = d_rowstarts;
     a.col = d_col;
@@ -475,6 +486,7 @@ extern "C" int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, co
     a.nblocks = (unsigned)blocks;
     a.limit_ns = wait_limit_ns();
     void *args[] = {&a};
+    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(SsspCtl), st));
     G5_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)sssp_persistent_kernel, dim3(blocks), dim3(SSSP_THREADS),
                                             args, 0, st));
     DeviceInfo di;
@@ -482,6 +494,19 @@ extern "C" int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, co
     sssp_export_kernel<<<di.sms * 8, 256, 0, st>>>(w.pack, nverts, d_dist, d_pred);
     G5_CUDA_TRY(cudaGetLastError());
     return G5_OK;
+}
+
+extern "C" int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
+                           const uint32_t *d_light_deg, float light_delta, uint64_t nverts, uint64_t root,
+                           float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes,
+                           const g5_sssp_params *params, void *stream) {
+    clear_error();
+    SsspWork w;
+    int rc = sssp_check(d_rowstarts, d_col, d_w, nverts, root, d_dist, d_pred, d_work, work_bytes, &w, "g5_sssp_run");
+    if (rc) return rc;
+    if ((rc = g5_sssp_reset(nverts, d_work, work_bytes, stream))) return rc;
+    return g5_sssp_traverse(d_rowstarts, d_col, d_w, d_light_deg, light_delta, nverts, root, d_dist, d_pred, d_work,
+                            work_bytes, params, stream);
 }
 
 extern "C" int g5_sssp_last_status(const void *d_work, uint64_t work_bytes, uint64_t *buckets, uint64_t *phases,

@@ -113,16 +113,33 @@ int g5_bfs_run(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nvert
                int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
                const g5_bfs_params *params, void *stream);
 
-/* g5_bfs_run in two steps: g5_bfs_reset clears pred (-1), depth (-1) and the
- * workspace's visited bitmap and control block; g5_bfs_traverse then runs
- * the persistent kernel alone (on a reset state). */
-int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes, void *stream);
+/* d_bits[ceil(nverts/32)]: bit v set when vertex v has no CSR entry. */
+int g5_graph_isolated_bitmap(const uint64_t *d_rowstarts, uint64_t nverts, uint32_t *d_bits, void *stream);
+
+/* g5_bfs_run in two steps, like the reference's oned_graph_bfs_clear +
+ * oned_graph_bfs_run: g5_bfs_reset clears pred (-1), depth (-1) and the
+ * workspace's visited bitmap (O(N) writes) -- to a copy of d_visited_init
+ * when given (the isolated-vertex bitmap, so bottom-up levels skip vertices
+ * no search can reach); g5_bfs_traverse zeroes the small control block and
+ * runs the persistent kernel (on a reset state). */
+int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, const uint32_t *d_visited_init, void *d_work,
+                 uint64_t work_bytes, void *stream);
 int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
                     int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
                     const g5_bfs_params *params, void *stream);
 
 /* Statistics of the last g5_bfs_run that used this workspace (synchronises). */
 int g5_bfs_last_stats(const void *d_work, uint64_t work_bytes, g5_bfs_stats *stats, void *stream);
+
+/* Per-level trace of the last g5_bfs_run on this workspace (synchronises):
+ * direction (0 top-down, 1 bottom-up), frontier vertices and edges, and the
+ * level's device time from the globaltimer, for up to max_levels levels
+ * (64 recorded); *nlevels = levels expanded, *solo_levels = levels run by a
+ * single block before the grid took over.  Any output pointer may be NULL
+ * except nlevels. */
+int g5_bfs_last_trace(const void *d_work, uint64_t work_bytes, int max_levels, int32_t *mode,
+                      uint64_t *frontier_vertices, uint64_t *frontier_edges, double *level_ms, int32_t *nlevels,
+                      int32_t *solo_levels, void *stream);
 
 /* bfs_compute_dist_from_pred, src/traversal.h:48 (src/traversal.cu:505-563):
  * d_dist[v] = -1 where pred is -1, 0 at the root, the tree depth where the
@@ -151,6 +168,15 @@ int g5_sssp_workspace_size(uint64_t nverts, uint64_t *bytes);
 int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, const uint32_t *d_light_deg,
                 float light_delta, uint64_t nverts, uint64_t root, float *d_dist, int64_t *d_pred, void *d_work,
                 uint64_t work_bytes, const g5_sssp_params *params, void *stream);
+
+/* g5_sssp_run in two steps, like the reference's oned_graph_sssp_clear +
+ * oned_graph_sssp_run: g5_sssp_reset clears the workspace's O(N) arrays
+ * (distances, stamps, settled bitmap); g5_sssp_traverse zeroes the control
+ * block, runs the persistent kernel and writes d_dist / d_pred. */
+int g5_sssp_reset(uint64_t nverts, void *d_work, uint64_t work_bytes, void *stream);
+int g5_sssp_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, const uint32_t *d_light_deg,
+                     float light_delta, uint64_t nverts, uint64_t root, float *d_dist, int64_t *d_pred, void *d_work,
+                     uint64_t work_bytes, const g5_sssp_params *params, void *stream);
 
 /* Buckets and phases of the last g5_sssp_run that used this workspace, and
  * its device status (synchronises). */

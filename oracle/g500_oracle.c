@@ -353,11 +353,18 @@ int orc_generate_bfs_roots(const uint64_t *rowstarts, uint64_t nverts, uint64_t 
  * by the reference's BFS; it is what bfs_compute_dist_from_pred derives,
  * :505-563) is -1 for unreached vertices and the level otherwise.
  * Returns the number of levels. */
-int orc_bfs(const uint64_t *rowstarts, const uint32_t *col, uint64_t nverts, uint64_t root,
-            int64_t *pred, int64_t *depth, int nthreads) {
+void orc_bfs_clear(uint64_t nverts, int64_t *pred, int64_t *depth, int nthreads) {
     if (nthreads <= 0) nthreads = omp_get_max_threads();
 #pragma omp parallel for num_threads(nthreads)
     for (uint64_t v = 0; v < nverts; ++v) { pred[v] = -1; depth[v] = -1; }
+}
+
+/* The search of orc_bfs on arrays already cleared by orc_bfs_clear (the
+ * runner keeps oned_graph_bfs_clear outside its timed region,
+ * examples/graph500_runner.cu:309-313). */
+int orc_bfs_search(const uint64_t *rowstarts, const uint32_t *col, uint64_t nverts, uint64_t root,
+                   int64_t *pred, int64_t *depth, int nthreads) {
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
     uint32_t *cur = (uint32_t *)malloc(nverts * sizeof(uint32_t));
     uint32_t *nxt = (uint32_t *)malloc(nverts * sizeof(uint32_t));
     uint64_t ncur = 1, nnext = 0;
@@ -402,6 +409,12 @@ int orc_bfs(const uint64_t *rowstarts, const uint32_t *col, uint64_t nverts, uin
     free(cur);
     free(nxt);
     return level;
+}
+
+int orc_bfs(const uint64_t *rowstarts, const uint32_t *col, uint64_t nverts, uint64_t root,
+            int64_t *pred, int64_t *depth, int nthreads) {
+    orc_bfs_clear(nverts, pred, depth, nthreads);
+    return orc_bfs_search(rowstarts, col, nverts, root, pred, depth, nthreads);
 }
 
 /* bfs_compute_dist_from_pred, src/traversal.cu:505-563 with the kernels at

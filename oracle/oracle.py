@@ -49,6 +49,9 @@ def lib():
     L.orc_generate_bfs_roots.restype = C.c_int
     L.orc_bfs.argtypes = [u64p, u32p, C.c_uint64, C.c_uint64, i64p, i64p, C.c_int]
     L.orc_bfs.restype = C.c_int
+    L.orc_bfs_clear.argtypes = [C.c_uint64, i64p, i64p, C.c_int]
+    L.orc_bfs_search.argtypes = [u64p, u32p, C.c_uint64, C.c_uint64, i64p, i64p, C.c_int]
+    L.orc_bfs_search.restype = C.c_int
     L.orc_bfs_dist_from_pred.argtypes = [u64p, u32p, C.c_uint64, i64p, C.c_uint64, i64p]
     L.orc_bfs_validate.argtypes = [u64p, u32p, C.c_uint64, C.c_uint64, i64p, i64p]
     L.orc_bfs_validate.restype = C.c_uint64
@@ -135,6 +138,17 @@ def bfs(rowstarts, col, nverts: int, root: int, nthreads: int = 0):
     depth = np.zeros(nverts, np.int64)
     lib().orc_bfs(rowstarts, _col(col), nverts, root, pred, depth, nthreads)
     return pred, depth
+
+
+def bfs_clear(nverts: int, pred: np.ndarray, depth: np.ndarray, nthreads: int = 0) -> None:
+    """The clear half of bfs (the runner's untimed oned_graph_bfs_clear)."""
+    lib().orc_bfs_clear(nverts, pred, depth, nthreads)
+
+
+def bfs_search(rowstarts, col, nverts: int, root: int, pred: np.ndarray, depth: np.ndarray,
+               nthreads: int = 0) -> int:
+    """The search half of bfs on cleared arrays; returns the level count."""
+    return lib().orc_bfs_search(rowstarts, _col(col), nverts, root, pred, depth, nthreads)
 
 
 def bfs_dist_from_pred(rowstarts, col, nverts: int, pred: np.ndarray, root: int) -> np.ndarray:
