@@ -62,6 +62,7 @@ def _load() -> C.CDLL:
         "g5_sssp_run": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_sssp_last_status": ([p, u64, p, p, p], C.c_int),
         "g5_sssp_reset": ([u64, p, u64, p], C.c_int),
+        "g5_sssp_last_trace": ([p, u64, p, C.c_int, p, p, p, p, p], C.c_int),
         "g5_sssp_traverse": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_validate_workspace_size": ([u64, p], C.c_int),
         "g5_edge_count": ([p, p, u64, p, p, u64, p, p], C.c_int),
@@ -383,6 +384,22 @@ def oned_graph_sssp_traverse(g: OnedGraph, sssp: SsspState, root: int, delta: fl
     _check(lib.g5_sssp_traverse(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
                                 g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                                 sssp.work.numel(), C.byref(p), _stream(stream)))
+
+
+def sssp_trace(sssp: SsspState, stream=None) -> dict:
+    """Counters and per-phase trace of the last SSSP on this state."""
+    k = 256
+    counts = np.zeros(6, np.uint64)
+    kind = np.zeros(k, np.int32)
+    size = np.zeros(k, np.uint64)
+    ms = np.zeros(k, np.float64)
+    n = C.c_int32()
+    _check(lib.g5_sssp_last_trace(_ptr(sssp.work), sssp.work.numel(), counts.ctypes.data, k, kind.ctypes.data,
+                                  size.ctypes.data, ms.ctypes.data, C.byref(n), _stream(stream)))
+    m = min(n.value, k)
+    names = ["edges", "settled_skips", "atomics", "improved", "ring_pushes", "frontier_pushes"]
+    return {"counts": dict(zip(names, counts.tolist())), "phases": n.value, "kind": kind[:m].tolist(),
+            "size": size[:m].tolist(), "ms": ms[:m].tolist()}
 
 
 def sssp_status(sssp: SsspState, stream=None) -> tuple[int, int]:

@@ -37,6 +37,7 @@
 namespace g5 {
 
 constexpr int BFS_THREADS = 256;
+constexpr unsigned BFS_STAGE = 512;  // per-warp staging of the next queue (16 KiB shared per block)
 constexpr unsigned long long SOLO_EDGES = 4096;  // levels at most this wide run in block 0 alone
 constexpr int BFS_TRACE = 64;                    // levels recorded in the control block
 
@@ -101,14 +102,15 @@ enum { TOP_DOWN = 0, BOTTOM_UP = 1 };
 
 // Claim v for parent u at the next level; appends it to the next queue.
 // All 32 lanes must call it (want = this lane has a candidate).
-__device__ __forceinline__ void td_visit(const BfsArgs &a, bool want, unsigned v, unsigned u, int next_level,
-                                         unsigned *qn, unsigned *basen, unsigned *n_small, unsigned long long *n_big,
-                                         unsigned long long &my_m) {
+__device__ __forceinline__ void td_visit(const BfsArgs &a, const WarpStage &bq, bool want, unsigned v, unsigned u,
+                                         int next_level, unsigned *qn, unsigned *basen, unsigned *n_small,
+                                         unsigned long long *n_big, unsigned long long &my_m) {
     if (want && v >= a.n) {  // not a vertex: report it, touch nothing
         atomicOr(&a.ctl->error, DEVERR_RANGE);
         want = false;
     }
     bool disc = want && bit_claim(a.visited, v);
+    if (!__any_sync(FULL, disc)) return;  // nothing new in this warp step
     uint64_t deg = 0;
     if (disc) {
         a.pred[v] = (int64_t)u;
@@ -116,10 +118,12 @@ __device__ __forceinline__ void td_visit(const BfsArgs &a, bool want, unsigned v
         deg = __ldg(&a.rowptr[v + 1]) - __ldg(&a.rowptr[v]);
         my_m += deg;
     }
-    if (!frontier_append(qn, basen, a.n, n_small, n_big, disc, v, deg)) atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+    if (!frontier_append_staged(bq, qn, basen, a.n, n_small, n_big, disc, v, deg))
+        atomicOr(&a.ctl->error, DEVERR_CAPACITY);
 }
 
-__device__ void td_expand(const BfsArgs &a, int level, int cur, int s_cur, int s_nxt, unsigned long long &my_m) {
+__device__ void td_expand(const BfsArgs &a, const WarpStage &bq, int level, int cur, int s_cur, int s_nxt,
+                          unsigned long long &my_m) {
     BfsCtl *c = a.ctl;
     const unsigned lane = lane_id();
     const unsigned *Q = a.q[cur];
@@ -129,14 +133,15 @@ __device__ void td_expand(const BfsArgs &a, int level, int cur, int s_cur, int s
     const unsigned ns = ld_volatile(&c->n_small[s_cur]);
     const unsigned long long bp = ld_volatile(&c->big[s_cur]);
 
-    // Small part: 32 queue entries per grab, edges gathered across the warp.
+    // Small part: g queue entries per grab, edges gathered across the warp.
+    const unsigned g = grab_size(ns, ((unsigned long long)gridDim.x * blockDim.x) >> 5);
     for (;;) {
         unsigned base = 0;
-        if (lane == 0) base = atomicAdd(&c->grab[s_cur], 32u);
+        if (lane == 0) base = atomicAdd(&c->grab[s_cur], g);
         base = __shfl_sync(FULL, base, 0);
         if (base >= ns) break;
         const unsigned i = base + lane;
-        const bool valid = i < ns;
+        const bool valid = lane < g && i < ns;
         const unsigned u = valid ? __ldcg(&Q[i]) : 0u;
         const uint64_t rb = valid ? __ldg(&a.rowptr[u]) : 0;
         const unsigned deg = valid ? (unsigned)(__ldg(&a.rowptr[u + 1]) - rb) : 0u;
@@ -151,7 +156,7 @@ __device__ void td_expand(const BfsArgs &a, int level, int cur, int s_cur, int s
             const uint64_t rbj = __shfl_sync(FULL, rb, j);
             const unsigned exj = __shfl_sync(FULL, excl, j);
             const unsigned v = has ? (unsigned)__ldg(&a.col[rbj + (e - exj)]) : 0u;
-            td_visit(a, has, v, uj, level + 1, QN, BN, &c->n_small[s_nxt], &c->big[s_nxt], my_m);
+            td_visit(a, bq, has, v, uj, level + 1, QN, BN, &c->n_small[s_nxt], &c->big[s_nxt], my_m);
         }
     }
     // Big part: chunks of every big vertex from one grid-wide counter.
@@ -171,9 +176,10 @@ __device__ void td_expand(const BfsArgs &a, int level, int cur, int s_cur, int s
         for (uint64_t e = cs + lane; e < cs + BIG_CHUNK; e += 32) {
             const bool has = e < ce;
             const unsigned v = has ? (unsigned)__ldg(&a.col[rb + e]) : 0u;
-            td_visit(a, has, v, u, level + 1, QN, BN, &c->n_small[s_nxt], &c->big[s_nxt], my_m);
+            td_visit(a, bq, has, v, u, level + 1, QN, BN, &c->n_small[s_nxt], &c->big[s_nxt], my_m);
         }
     }
+    if (!stage_flush_warp(bq, QN, a.n, &c->n_small[s_nxt])) atomicOr(&c->error, DEVERR_CAPACITY);
 }
 
 __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsigned *nb, unsigned long long &my_m,
@@ -189,15 +195,18 @@ __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsig
         if (v < a.n && !((vis >> lane) & 1u)) {
             rb = __ldg(&a.rowptr[v]);
             re = __ldg(&a.rowptr[v + 1]);
-            for (uint64_t e = rb; e < re; ++e) {
-                const unsigned u = (unsigned)__ldg(&a.col[e]);
-                if (u >= a.n) {
-                    atomicOr(&a.ctl->error, DEVERR_RANGE);
-                    continue;
-                }
-                if ((__ldcg(&fb[u >> 5]) >> (u & 31)) & 1u) {
-                    found = (int)u;
-                    break;
+            // Four neighbours per step: their loads and bitmap probes are
+            // independent, so each step costs one memory round trip, not four.
+            for (uint64_t e = rb; e < re && found < 0; e += 4) {
+                unsigned u[4], word[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) u[i] = e + i < re ? (unsigned)__ldg(&a.col[e + i]) : a.n;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) word[i] = u[i] < a.n ? __ldcg(&fb[u[i] >> 5]) : 0u;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if (e + i < re && u[i] >= a.n) atomicOr(&a.ctl->error, DEVERR_RANGE);
+                    if (found < 0 && u[i] < a.n && ((word[i] >> (u[i] & 31)) & 1u)) found = (int)u[i];
                 }
             }
         }
@@ -216,8 +225,8 @@ __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsig
 }
 
 // Frontier queue from a bottom-up bitmap (small/big split by degree).
-__device__ void bits_to_queue(const BfsArgs &a, const unsigned *bits, unsigned *qn, unsigned *basen, unsigned *n_small,
-                              unsigned long long *n_big) {
+__device__ void bits_to_queue(const BfsArgs &a, const WarpStage &bq, const unsigned *bits, unsigned *qn,
+                              unsigned *basen, unsigned *n_small, unsigned long long *n_big) {
     const unsigned lane = lane_id();
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -236,10 +245,11 @@ __device__ void bits_to_queue(const BfsArgs &a, const unsigned *bits, unsigned *
                 m &= m - 1;
                 deg = __ldg(&a.rowptr[v + 1]) - __ldg(&a.rowptr[v]);
             }
-            if (!frontier_append(qn, basen, a.n, n_small, n_big, has, v, deg))
+            if (!frontier_append_staged(bq, qn, basen, a.n, n_small, n_big, has, v, deg))
                 atomicOr(&a.ctl->error, DEVERR_CAPACITY);
         }
     }
+    if (!stage_flush_warp(bq, qn, a.n, n_small)) atomicOr(&a.ctl->error, DEVERR_CAPACITY);
 }
 
 // Direction of the next level (Beamer's rule; a.mode forces one side).
@@ -261,8 +271,8 @@ enum { PEND_NONE = 0, PEND_TO_BITS = 1, PEND_TO_QUEUE = 2 };
 
 // Expands level st.level; adds the next frontier's degree sum and (bottom-up)
 // size into slot s_nxt.  No synchronisation.
-__device__ __forceinline__ void bfs_expand_level(const BfsArgs &a, const LevelState &st, const unsigned *fb,
-                                                 unsigned *nb) {
+__device__ __forceinline__ void bfs_expand_level(const BfsArgs &a, const WarpStage &bq, const LevelState &st,
+                                                 const unsigned *fb, unsigned *nb) {
     BfsCtl *c = a.ctl;
     const int s_cur = st.level % 3, s_nxt = (st.level + 1) % 3, s_clr = (st.level + 2) % 3;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -276,7 +286,7 @@ __device__ __forceinline__ void bfs_expand_level(const BfsArgs &a, const LevelSt
     unsigned long long my_m = 0;
     unsigned my_found = 0;
     if (st.mode == TOP_DOWN)
-        td_expand(a, st.level, st.cur, s_cur, s_nxt, my_m);
+        td_expand(a, bq, st.level, st.cur, s_cur, s_nxt, my_m);
     else
         bu_expand(a, st.level, fb, nb, my_m, my_found);
     my_m = warp_sum(my_m);
@@ -336,6 +346,11 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
     const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
     unsigned *fb = a.fbits, *nb = a.nbits;
     LevelState st;
+    __shared__ unsigned s_stage[BFS_THREADS / 32][BFS_STAGE];
+    __shared__ unsigned s_stage_cnt[BFS_THREADS / 32];
+    if (lane_id() == 0) s_stage_cnt[threadIdx.x >> 5] = 0;
+    __syncwarp();
+    const WarpStage bq{s_stage[threadIdx.x >> 5], &s_stage_cnt[threadIdx.x >> 5], BFS_STAGE};
 
     // ---- Solo prologue: block 0 alone runs the first levels while the
     // frontier is small (every search starts with one vertex), syncing with
@@ -365,7 +380,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
         int solo = 0;
         while (a.nblocks == 1 || (st.mode == TOP_DOWN && st.pending == PEND_NONE && st.m_f <= SOLO_EDGES)) {
             if (a.nblocks == 1 && st.pending != PEND_NONE) break;  // conversions run in the grid loop
-            bfs_expand_level(a, st, fb, nb);
+            bfs_expand_level(a, bq, st, fb, nb);
             __threadfence();
             __syncthreads();
             ++solo;
@@ -438,11 +453,11 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
             }
             if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
         } else if (st.pending == PEND_TO_QUEUE) {
-            bits_to_queue(a, fb, a.q[st.cur], a.base[st.cur], &c->n_small[s_cur], &c->big[s_cur]);
+            bits_to_queue(a, bq, fb, a.q[st.cur], a.base[st.cur], &c->n_small[s_cur], &c->big[s_cur]);
             if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
         }
         st.pending = PEND_NONE;
-        bfs_expand_level(a, st, fb, nb);
+        bfs_expand_level(a, bq, st, fb, nb);
         if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
         if (!bfs_advance(a, st, fb, nb)) break;
     }
@@ -634,12 +649,34 @@ extern "C" int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col
     a.mode = p.mode;
     a.nblocks = (unsigned)blocks;
     a.limit_ns = wait_limit_ns();
-    void *args[] = {&a};
     // The control block (counters, hand-off, barrier) starts from zero on
     // every search, so a traversal never sees the previous one's state.
     G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(BfsCtl), (cudaStream_t)stream));
-    G5_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)bfs_persistent_kernel, dim3(blocks), dim3(BFS_THREADS), args,
-                                            0, (cudaStream_t)stream));
+    // Cooperative launch; the three bitmaps (visited, frontier, next: N/8
+    // bytes each, adjacent in the workspace) get an L2 persisting window so
+    // the streaming column reads do not evict them.
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(BFS_THREADS);
+    cfg.stream = (cudaStream_t)stream;
+    cudaLaunchAttribute attrs[2];
+    attrs[0].id = cudaLaunchAttributeCooperative;
+    attrs[0].val.cooperative = 1;
+    cfg.attrs = attrs;
+    cfg.numAttrs = 1;
+    const uint64_t win = (uint64_t)((char *)(w.nbits + a.nwords) - (char *)w.visited);
+    uint64_t win_bytes = 0;
+    if ((rc = l2_persist_window(win, &win_bytes))) return rc;
+    if (win_bytes) {
+        attrs[1].id = cudaLaunchAttributeAccessPolicyWindow;
+        attrs[1].val.accessPolicyWindow.base_ptr = w.visited;
+        attrs[1].val.accessPolicyWindow.num_bytes = win_bytes;
+        attrs[1].val.accessPolicyWindow.hitRatio = 1.0f;
+        attrs[1].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        attrs[1].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        cfg.numAttrs = 2;
+    }
+    G5_CUDA_TRY(cudaLaunchKernelEx(&cfg, bfs_persistent_kernel, a));
     return G5_OK;
 }
 

@@ -1,4 +1,5 @@
 // common.cu -- host helpers shared by every entry point of libg500b.
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -45,6 +46,35 @@ int deverr_to_status(unsigned flags, const char *what) {
     if (flags & DEVERR_RANGE)
         return set_error(G5_ERR_INVALID, "%s: input value out of range (flags 0x%x)", what, flags);
     return set_error(G5_ERR_DEVICE, "%s: internal capacity exceeded (flags 0x%x)", what, flags);
+}
+
+int l2_persist_window(uint64_t want, uint64_t *bytes) {
+    static std::mutex mu;
+    static uint64_t reserved[64] = {};
+    static int max_window[64] = {}, max_persist[64] = {};
+    static bool probed[64] = {};
+    *bytes = 0;
+    const char *env = getenv("G5_L2_PERSIST");
+    if (env && env[0] == '0') return G5_OK;
+    DeviceInfo di;
+    int rc = device_info(&di);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!probed[di.device]) {
+        G5_CUDA_TRY(cudaDeviceGetAttribute(&max_window[di.device], cudaDevAttrMaxAccessPolicyWindowSize, di.device));
+        G5_CUDA_TRY(cudaDeviceGetAttribute(&max_persist[di.device], cudaDevAttrMaxPersistingL2CacheSize, di.device));
+        probed[di.device] = true;
+    }
+    uint64_t b = std::min<uint64_t>(want, (uint64_t)max_window[di.device]);
+    b = std::min<uint64_t>(b, (uint64_t)max_persist[di.device]);
+    if (!b) return G5_OK;
+    if (reserved[di.device] < b) {
+        // Context-level limit: it lasts until this process's context ends.
+        G5_CUDA_TRY(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, b));
+        reserved[di.device] = b;
+    }
+    *bytes = b;
+    return G5_OK;
 }
 
 unsigned long long wait_limit_ns() {

@@ -65,6 +65,12 @@ enum : unsigned {
 };
 int deverr_to_status(unsigned flags, const char *what);
 
+// Bytes of an L2 persisting access-policy window to use for a region of
+// `want` bytes (0 = none): min(want, the device's window limit), after
+// reserving that much persisting L2 for this process's context once per
+// device.  G5_L2_PERSIST=0 disables it.
+int l2_persist_window(uint64_t want, uint64_t *bytes);
+
 // Wait limit of the persistent kernels' grid barriers, nanoseconds
 // (G5_WAIT_LIMIT_MS overrides; default 2000 ms).
 unsigned long long wait_limit_ns();

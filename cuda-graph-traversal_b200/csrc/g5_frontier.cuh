@@ -3,21 +3,31 @@
 //
 // A list of capacity n holds vertices whose edge range has at most BIG_DEG
 // entries at the front ("small" part, counted by a u32) and the others at
-// the back ("big" part).  Small vertices are expanded 32 at a time by a
-// warp that gathers their edges across its lanes.  Big vertices are cut
-// into BIG_CHUNK-edge chunks and every warp of the grid takes chunks from
-// one counter: a big entry is appended with a single 64-bit atomicAdd on a
-// packed counter (entry count << 40 | chunk count), which hands it both its
-// slot j and the id of its first chunk, so chunk bases are sorted by slot
-// and a chunk id maps back to its vertex by binary search.
+// the back ("big" part).  Small vertices are expanded a few at a time (the
+// grab size adapts to the list length, up to 32) by a warp that gathers
+// their edges across its lanes, so a short list of heavy vertices still
+// spreads over the whole grid.  Big vertices are cut into BIG_CHUNK-edge
+// chunks and every warp of the grid takes chunks from one counter, so no
+// vertex's edges serialise on one warp.  Big entries are
+// appended with one 64-bit atomicAdd per warp on a packed counter
+// (entry count << 40 | chunk count), which hands out slots and first-chunk
+// ids in the same order, so chunk bases are sorted by slot and a chunk id
+// maps back to its vertex by binary search.
 #pragma once
 
 #include "g5_common.cuh"
 
 namespace g5 {
 
-constexpr unsigned BIG_DEG = 4096;
+constexpr unsigned BIG_DEG = 1024;
 constexpr unsigned BIG_CHUNK = 1024;
+
+// Entries per grab over a small part of ns entries: about four grabs per
+// warp, between 1 and 32.
+__host__ __device__ __forceinline__ unsigned grab_size(unsigned ns, unsigned long long nwarps) {
+    unsigned long long g = ns / (4 * nwarps);
+    return g < 1 ? 1u : g > 32 ? 32u : (unsigned)g;
+}
 constexpr int BIG_SHIFT = 40;
 constexpr unsigned long long BIG_LOW = (1ull << BIG_SHIFT) - 1;
 
@@ -40,17 +50,80 @@ __device__ __forceinline__ bool frontier_append(unsigned *L, unsigned *base, uin
         if (p < n) L[p] = v;
         else ok = false;
     }
-    if (bg) {
-        const unsigned long long nch = (deg + BIG_CHUNK - 1) / BIG_CHUNK;
-        const unsigned long long old = atomicAdd(big, (1ull << BIG_SHIFT) | nch);
-        const uint64_t j = old >> BIG_SHIFT;
-        if (j < n) {
-            L[n - 1 - j] = v;
-            base[j] = (unsigned)(old & BIG_LOW);
-        } else {
-            ok = false;
+    const unsigned bmask = __ballot_sync(FULL, bg);
+    if (bmask) {
+        const unsigned nch = bg ? (unsigned)((deg + BIG_CHUNK - 1) / BIG_CHUNK) : 0u;
+        const unsigned incl = warp_incl_scan(nch);
+        const unsigned total = __shfl_sync(FULL, incl, 31);
+        const unsigned leader = __ffs(bmask) - 1;
+        unsigned long long old = 0;
+        if (lane_id() == leader) old = atomicAdd(big, ((unsigned long long)__popc(bmask) << BIG_SHIFT) | total);
+        old = __shfl_sync(FULL, old, leader);
+        if (bg) {
+            const uint64_t j = (old >> BIG_SHIFT) + __popc(bmask & lanemask_lt());
+            if (j < n) {
+                L[n - 1 - j] = v;
+                base[j] = (unsigned)((old & BIG_LOW) + incl - nch);
+            } else {
+                ok = false;
+            }
         }
     }
+    return ok;
+}
+
+// Per-warp staging of a list's small part in shared memory.  A warp
+// appends into its own slice with ballots only, and when the slice is full
+// it reserves a range of the global list with one atomicAdd and copies the
+// slice out (coalesced).  A frontier of millions of vertices then costs one
+// global atomic per `cap` entries instead of one per warp step on a single
+// counter, and no block-wide synchronisation is needed.
+struct WarpStage {
+    unsigned *buf;  // this warp's slice (shared), cap entries, cap >= 32
+    unsigned *cnt;  // this warp's fill count (shared)
+    unsigned cap;
+};
+
+__device__ __forceinline__ bool stage_flush_warp(const WarpStage &q, unsigned *L, uint64_t n, unsigned *gcount) {
+    __syncwarp();
+    const unsigned c = *q.cnt;
+    if (!c) return true;
+    unsigned base = 0;
+    if (lane_id() == 0) base = atomicAdd(gcount, c);
+    base = __shfl_sync(FULL, base, 0);
+    const bool ok = (uint64_t)base + c <= n;
+    if (ok)
+        for (unsigned i = lane_id(); i < c; i += 32) L[base + i] = q.buf[i];
+    __syncwarp();
+    if (lane_id() == 0) *q.cnt = 0;
+    __syncwarp();
+    return ok;
+}
+
+// Appends v for every lane with `want`.  All 32 lanes call it.
+__device__ __forceinline__ bool stage_append(const WarpStage &q, bool want, unsigned v, unsigned *L, uint64_t n,
+                                             unsigned *gcount) {
+    const unsigned mask = __ballot_sync(FULL, want);
+    if (!mask) return true;
+    bool ok = true;
+    unsigned c = *q.cnt;
+    if (c + __popc(mask) > q.cap) {
+        ok = stage_flush_warp(q, L, n, gcount);
+        c = 0;
+    }
+    if (want) q.buf[c + __popc(mask & lanemask_lt())] = v;
+    __syncwarp();
+    if (lane_id() == 0) *q.cnt = c + __popc(mask);
+    __syncwarp();
+    return ok;
+}
+
+// frontier_append with the small part staged per warp.  All lanes call it.
+__device__ __forceinline__ bool frontier_append_staged(const WarpStage &q, unsigned *L, unsigned *basearr, uint64_t n,
+                                                       unsigned *n_small, unsigned long long *big, bool want,
+                                                       unsigned v, uint64_t deg) {
+    bool ok = stage_append(q, want && deg <= BIG_DEG, v, L, n, n_small);
+    ok &= frontier_append(L, basearr, n, n_small, big, want && deg > BIG_DEG, v, deg);
     return ok;
 }
 

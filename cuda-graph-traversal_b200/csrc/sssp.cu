@@ -38,6 +38,10 @@ namespace g5 {
 
 constexpr int SSSP_THREADS = 256;
 constexpr int RING = 16;  // bucket queues; a relaxation may land at most RING-1 buckets ahead
+constexpr unsigned STAGE_F = 256;    // per-warp staging: frontier
+constexpr unsigned STAGE_S = 256;    //                   heavy set
+constexpr unsigned STAGE_R = 32;     //                   each ring queue
+constexpr int SSSP_TRACE = 256;      // phases recorded in the control block
 constexpr unsigned long long UNREACHED = ~0ull;
 
 struct SsspCtl {
@@ -52,6 +56,14 @@ struct SsspCtl {
     unsigned ring_len[RING];
     unsigned long long buckets;
     unsigned long long phases;
+    // counters: edges looked at, skipped as settled, atomicMin issued,
+    // distances lowered, ring and frontier pushes
+    unsigned long long n_edges, n_settled, n_atomic, n_improved, n_ring, n_front;
+    // per-phase trace: end time, kind (0 open, 1 light, 2 heavy), input size
+    unsigned long long t0;
+    unsigned long long t_phase[SSSP_TRACE];
+    unsigned n_phase[SSSP_TRACE];
+    unsigned char kind_phase[SSSP_TRACE];
 };
 
 struct SsspArgs {
@@ -87,7 +99,20 @@ __device__ __forceinline__ void part_range(const SsspArgs &a, unsigned u, bool h
     }
 }
 
+// Per-warp shared-memory staging of every list a phase appends to.
+struct Stage {
+    WarpStage f, s;
+    unsigned *rbuf;  // RING * STAGE_R, this warp's
+    unsigned *rcnt;  // RING, this warp's
+};
+
+// Per-thread event counts, summed into the control block once per phase.
+struct Counts {
+    unsigned long long edges, settled, atomics, improved, ring, front;
+};
+
 struct PushCtx {
+    Stage st;
     unsigned pid;        // id of the producing phase (frontier stamp)
     unsigned bucket;     // current bucket index (heavy-set stamp)
     int f_slot;          // counter slot of the produced frontier
@@ -108,27 +133,33 @@ __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCt
     if (s) part_range(a, v, true, hb, he);
     // Each vertex enters a frontier once per phase and a heavy set once per
     // bucket, so no list exceeds n entries.
-    bool ok = frontier_append(x.Fout, x.FBout, a.n, &c->f_small[x.f_slot], &c->f_big[x.f_slot], f, v, le - lb);
-    ok &= frontier_append(x.Sl, x.SBl, a.n, &c->s_small[x.s_par], &c->s_big[x.s_par], s, v, he - hb);
+    bool ok = frontier_append_staged(x.st.f, x.Fout, x.FBout, a.n, &c->f_small[x.f_slot], &c->f_big[x.f_slot], f, v,
+                                     le - lb);
+    ok &= frontier_append_staged(x.st.s, x.Sl, x.SBl, a.n, &c->s_small[x.s_par], &c->s_big[x.s_par], s, v, he - hb);
     if (!ok) atomicOr(&c->error, DEVERR_CAPACITY);
 }
 
 // Relaxes u -> v with float weight wt from distance du; queues v when its
 // distance dropped.  All 32 lanes call it (want = lane has an edge).
-__device__ __forceinline__ void relax(const SsspArgs &a, const PushCtx &x, bool want, unsigned u, float du, unsigned v,
-                                      float wt, bool heavy_phase) {
+__device__ __forceinline__ void relax(const SsspArgs &a, const PushCtx &x, Counts &k, bool want, unsigned u, float du,
+                                      unsigned v, float wt, bool heavy_phase) {
     bool same = false;
     int target = -1;
+    k.edges += want;
     if (want && v >= a.n) {  // not a vertex: report it, touch nothing
         atomicOr(&a.ctl->error, DEVERR_RANGE);
         want = false;
     }
-    if (want && !((__ldcg(&a.settled[v >> 5]) >> (v & 31)) & 1u)) {
+    const bool settled = want && ((__ldcg(&a.settled[v >> 5]) >> (v & 31)) & 1u);
+    k.settled += settled;
+    if (want && !settled) {
         const float cand = __fadd_rn(du, wt);
         const unsigned long long np = ((unsigned long long)__float_as_uint(cand) << 32) | u;
         if (np < __ldcg(&a.pack[v])) {
+            ++k.atomics;
             const unsigned long long old = atomicMin(&a.pack[v], np);
             if (np < old && (old >> 32) != (np >> 32)) {
+                ++k.improved;
                 if (cand < x.bnd[1]) {
                     same = true;
                     if (heavy_phase) atomicOr(&a.ctl->error, DEVERR_CAPACITY);  // cannot happen: w >= delta
@@ -142,36 +173,67 @@ __device__ __forceinline__ void relax(const SsspArgs &a, const PushCtx &x, bool 
             }
         }
     }
+    if (!__any_sync(FULL, same || target >= 0)) return;  // nothing lowered in this warp step
     push_same_bucket(a, x, same && !heavy_phase, v);
-    // Ring queue of the target bucket, once per (vertex, bucket).
+    // Ring queue of the target bucket, once per (vertex, bucket), staged in
+    // the block's shared memory.
     const bool r = target >= 0 && atomicExch(&a.qstamp[v], (unsigned)target) != (unsigned)target;
+    k.ring += r;
+    k.front += same && !heavy_phase;
+    // Per-slot warp staging: lanes with the same target slot append
+    // together; a full slot is flushed to its global queue first.
     const int slot = r ? target % RING : RING;
-    const unsigned grp = __match_any_sync(FULL, slot);
-    if (r) {
-        const unsigned leader = __ffs(grp) - 1;
-        unsigned base = 0;
-        if (lane_id() == leader) base = atomicAdd(&a.ctl->ring_len[slot], (unsigned)__popc(grp));
-        base = __shfl_sync(grp, base, leader);
-        const uint64_t at = (uint64_t)base + __popc(grp & lanemask_lt());
-        if (at < a.n) a.ring[(uint64_t)slot * a.n + at] = v;
-        else atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+    unsigned todo = __ballot_sync(FULL, r);
+    while (todo) {
+        const int sl = __shfl_sync(FULL, slot, __ffs(todo) - 1);
+        const bool mine = r && slot == sl;
+        const unsigned m = __ballot_sync(FULL, mine);
+        WarpStage q{x.st.rbuf + sl * STAGE_R, x.st.rcnt + sl, STAGE_R};
+        if (!stage_append(q, mine, v, a.ring + (uint64_t)sl * a.n, a.n, &a.ctl->ring_len[sl]))
+            atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+        todo &= ~m;
     }
+}
+
+// Writes every staged entry of this warp to its global list and the warp's
+// counts to the control block.  Every warp calls it at the end of a phase.
+__device__ void stage_flush(const SsspArgs &a, const PushCtx &x, Counts &k) {
+    SsspCtl *c = a.ctl;
+    {
+        unsigned long long v[6] = {k.edges, k.settled, k.atomics, k.improved, k.ring, k.front};
+        unsigned long long *dst[6] = {&c->n_edges, &c->n_settled, &c->n_atomic, &c->n_improved, &c->n_ring,
+                                      &c->n_front};
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const unsigned long long t = warp_sum(v[i]);
+            if (lane_id() == 0 && t) atomicAdd(dst[i], t);
+        }
+        k = Counts{0, 0, 0, 0, 0, 0};
+    }
+    bool ok = stage_flush_warp(x.st.f, x.Fout, a.n, &c->f_small[x.f_slot]);
+    ok &= stage_flush_warp(x.st.s, x.Sl, a.n, &c->s_small[x.s_par]);
+    for (int sl = 0; sl < RING; ++sl) {
+        WarpStage q{x.st.rbuf + sl * STAGE_R, x.st.rcnt + sl, STAGE_R};
+        ok &= stage_flush_warp(q, a.ring + (uint64_t)sl * a.n, a.n, &c->ring_len[sl]);
+    }
+    if (!ok && lane_id() == 0) atomicOr(&c->error, DEVERR_CAPACITY);
 }
 
 // Relaxes the light (heavy = false) or heavy edges of every vertex of list L
 // (small part [0, ns), big part at the back, `bp` its packed counter).  The
 // heavy pass also marks each list vertex settled.
-__device__ void expand_list(const SsspArgs &a, const PushCtx &x, const unsigned *L, unsigned ns,
+__device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, const unsigned *L, unsigned ns,
                             unsigned long long bp, const unsigned *B, unsigned *grab, unsigned *cgrab, bool heavy) {
     const unsigned lane = lane_id();
     const bool filtered = a.ld == nullptr;
+    const unsigned g = grab_size(ns, ((unsigned long long)gridDim.x * blockDim.x) >> 5);
     for (;;) {
         unsigned base = 0;
-        if (lane == 0) base = atomicAdd(grab, 32u);
+        if (lane == 0) base = atomicAdd(grab, g);
         base = __shfl_sync(FULL, base, 0);
         if (base >= ns) break;
         const unsigned i = base + lane;
-        const bool valid = i < ns;
+        const bool valid = lane < g && i < ns;
         const unsigned u = valid ? __ldcg(&L[i]) : 0u;
         uint64_t rb = 0, re = 0;
         float du = 0.0f;
@@ -200,7 +262,7 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, const unsigned 
                 wt = __ldg(&a.w[at]);
                 if (filtered) has = heavy ? !(wt < a.delta) : wt < a.delta;
             }
-            relax(a, x, has, uj, duj, v, wt, heavy);
+            relax(a, x, k, has, uj, duj, v, wt, heavy);
         }
     }
     const unsigned nb = big_count(bp);
@@ -229,14 +291,31 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, const unsigned 
                 wt = __ldg(&a.w[rb + e]);
                 if (filtered) has = heavy ? !(wt < a.delta) : wt < a.delta;
             }
-            relax(a, x, has, u, du, v, wt, heavy);
+            relax(a, x, k, has, u, du, v, wt, heavy);
         }
+    }
+}
+
+__device__ __forceinline__ void trace_phase(SsspCtl *c, unsigned phase, int kind, unsigned size) {
+    if (phase < SSSP_TRACE) {
+        c->t_phase[phase] = globaltimer_ns();
+        c->kind_phase[phase] = (unsigned char)kind;
+        c->n_phase[phase] = size;
     }
 }
 
 __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspArgs a) {
     SsspCtl *c = a.ctl;
     __shared__ float s_bnd[RING + 1];
+    constexpr int WARPS = SSSP_THREADS / 32;
+    __shared__ unsigned s_fbuf[WARPS][STAGE_F], s_sbuf[WARPS][STAGE_S], s_rbuf[WARPS][RING * STAGE_R];
+    __shared__ unsigned s_fcnt[WARPS], s_scnt[WARPS], s_rcnt[WARPS][RING];
+    const unsigned wid = threadIdx.x >> 5;
+    if (lane_id() == 0) s_fcnt[wid] = s_scnt[wid] = 0;
+    if (lane_id() < RING) s_rcnt[wid][lane_id()] = 0;
+    __syncwarp();
+    const Stage stage{WarpStage{s_fbuf[wid], &s_fcnt[wid], STAGE_F}, WarpStage{s_sbuf[wid], &s_scnt[wid], STAGE_S},
+                      s_rbuf[wid], s_rcnt[wid]};
     unsigned epoch = 0;
     const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
@@ -251,6 +330,8 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
 
     unsigned bucket = 0, phase = 0;
     float blo = 0.0f;
+    Counts cnt{0, 0, 0, 0, 0, 0};
+    if (gtid == 0) c->t0 = globaltimer_ns();
     unsigned long long nbuckets = 0;
     for (;;) {
         // ---- open the bucket: its ring queue becomes the first frontier.
@@ -263,6 +344,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
         }
         __syncthreads();
         PushCtx x;
+        x.st = stage;
         x.bucket = bucket;
         x.bnd = s_bnd;
         x.s_par = bucket & 1;
@@ -294,10 +376,14 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
                 }
                 push_same_bucket(a, x, ok, v);
             }
+            stage_flush(a, x, cnt);
             if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
             // The queue is consumed; nothing can target this slot again before
             // bucket + RING, which lies beyond every push of this bucket.
-            if (gtid == 0) c->ring_len[slot] = 0;
+            if (gtid == 0) {
+                c->ring_len[slot] = 0;
+                trace_phase(c, phase, 0, len);
+            }
             ++phase;
         }
         // ---- light iterations until the bucket's frontier is empty.
@@ -314,8 +400,10 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
             x.f_slot = s_nxt;
             x.Fout = a.F[(phase + 1) & 1];
             x.FBout = a.FB[(phase + 1) & 1];
-            expand_list(a, x, a.F[phase & 1], ns, bp, a.FB[phase & 1], &c->grab[s_cur], &c->cgrab[s_cur], false);
+            expand_list(a, x, cnt, a.F[phase & 1], ns, bp, a.FB[phase & 1], &c->grab[s_cur], &c->cgrab[s_cur], false);
+            stage_flush(a, x, cnt);
             if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+            if (gtid == 0) trace_phase(c, phase, 1, ns + big_count(bp));
             ++phase;
         }
         // ---- heavy edges of every vertex settled in this bucket.
@@ -331,8 +419,10 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
             x.FBout = a.FB[(phase + 1) & 1];
             const unsigned ns = ld_volatile(&c->s_small[bucket & 1]);
             const unsigned long long bp = ld_volatile(&c->s_big[bucket & 1]);
-            expand_list(a, x, a.S[bucket & 1], ns, bp, a.SB[bucket & 1], &c->grab[s_cur], &c->cgrab[s_cur], true);
+            expand_list(a, x, cnt, a.S[bucket & 1], ns, bp, a.SB[bucket & 1], &c->grab[s_cur], &c->cgrab[s_cur], true);
+            stage_flush(a, x, cnt);
             if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+            if (gtid == 0) trace_phase(c, phase, 2, ns + big_count(bp));
             ++phase;
         }
         ++nbuckets;
@@ -507,6 +597,35 @@ extern "C" int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, co
     if ((rc = g5_sssp_reset(nverts, d_work, work_bytes, stream))) return rc;
     return g5_sssp_traverse(d_rowstarts, d_col, d_w, d_light_deg, light_delta, nverts, root, d_dist, d_pred, d_work,
                             work_bytes, params, stream);
+}
+
+extern "C" int g5_sssp_last_trace(const void *d_work, uint64_t work_bytes, uint64_t counts[6], int max_phases,
+                                   int32_t *kind, uint64_t *size, double *phase_ms, int32_t *nphases, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(d_work && work_bytes >= sizeof(SsspCtl) && nphases, "g5_sssp_last_trace: bad argument");
+    SsspCtl c;
+    cudaStream_t st = (cudaStream_t)stream;
+    G5_CUDA_TRY(cudaMemcpyAsync(&c, d_work, sizeof c, cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    if (counts) {
+        counts[0] = c.n_edges;
+        counts[1] = c.n_settled;
+        counts[2] = c.n_atomic;
+        counts[3] = c.n_improved;
+        counts[4] = c.n_ring;
+        counts[5] = c.n_front;
+    }
+    const int n = (int)std::min<unsigned long long>(std::min<unsigned long long>(c.phases, SSSP_TRACE),
+                                                     (unsigned long long)std::max(max_phases, 0));
+    unsigned long long prev = c.t0;
+    for (int i = 0; i < n; ++i) {
+        if (kind) kind[i] = c.kind_phase[i];
+        if (size) size[i] = c.n_phase[i];
+        if (phase_ms) phase_ms[i] = (double)(c.t_phase[i] - prev) * 1e-6;
+        prev = c.t_phase[i];
+    }
+    *nphases = (int32_t)c.phases;
+    return deverr_to_status(c.error, "g5_sssp_run");
 }
 
 extern "C" int g5_sssp_last_status(const void *d_work, uint64_t work_bytes, uint64_t *buckets, uint64_t *phases,

@@ -182,6 +182,14 @@ int g5_sssp_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, const fl
  * its device status (synchronises). */
 int g5_sssp_last_status(const void *d_work, uint64_t work_bytes, uint64_t *buckets, uint64_t *phases, void *stream);
 
+/* Counters and per-phase trace of the last g5_sssp_run on this workspace
+ * (synchronises): counts[6] = edges looked at, edges into settled vertices,
+ * atomicMin issued, distances lowered, bucket-queue pushes, same-bucket
+ * frontier pushes; per phase (up to 256) its kind (0 bucket open, 1 light,
+ * 2 heavy), input list size and device milliseconds. */
+int g5_sssp_last_trace(const void *d_work, uint64_t work_bytes, uint64_t counts[6], int max_phases, int32_t *kind,
+                       uint64_t *size, double *phase_ms, int32_t *nphases, void *stream);
+
 /* ---------------------------------------------------------- validation --- */
 
 int g5_validate_workspace_size(uint64_t nverts, uint64_t *bytes);
