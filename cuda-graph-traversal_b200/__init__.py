@@ -55,6 +55,8 @@ def _load() -> C.CDLL:
         "g5_bfs_reset": ([u64, p, p, p, p, u64, p], C.c_int),
         "g5_graph_isolated_bitmap": ([p, u64, p, p], C.c_int),
         "g5_bfs_traverse": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
+        "g5_bfs_query": ([p, p, u64, p, p, p, p, p, u64, p, p, p], C.c_int),
+        "g5_bfs_visited_bitmap": ([p, u64, u64, p, p], C.c_int),
         "g5_bfs_last_stats": ([p, u64, p, p], C.c_int),
         "g5_bfs_last_trace": ([p, u64, C.c_int, p, p, p, p, p, p, p], C.c_int),
         "g5_bfs_dist_from_pred": ([p, p, u64, p, u64, p, p, u64, p], C.c_int),
@@ -91,7 +93,8 @@ class BfsParams(C.Structure):
 
 
 class BfsStats(C.Structure):
-    _fields_ = [("levels", C.c_int32), ("bottom_up_levels", C.c_int32), ("reached", C.c_uint64)]
+    _fields_ = [("levels", C.c_int32), ("bottom_up_levels", C.c_int32), ("reached", C.c_uint64),
+                ("error_flags", C.c_uint32), ("solo_levels", C.c_int32)]
 
 
 class SsspParams(C.Structure):
@@ -188,6 +191,10 @@ class OnedGraph:
     light_delta: float
     column: torch.Tensor | None = None
     isolated: torch.Tensor | None = None  # int32[ceil(N/32)] bitmap of degree-0 vertices
+    main_bits: np.ndarray | None = None   # host uint32 bitmap of the largest component
+
+    def in_main_component(self, v: int) -> bool:
+        return self.main_bits is None or bool((int(self.main_bits[v >> 5]) >> (v & 31)) & 1)
 
     @property
     def nlocalverts(self) -> int:
@@ -220,8 +227,28 @@ def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: 
                            _ptr(work), work.numel(), _ptr(col), _ptr(w), _ptr(col64), _ptr(light), st))
     iso = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
     _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), n, _ptr(iso), st))
-    return OnedGraph(n, e, rowstarts, col[:e], w[:e], light, light_delta,
-                     None if col64 is None else col64[:e], iso)
+    g = OnedGraph(n, e, rowstarts, col[:e], w[:e], light, light_delta, None if col64 is None else col64[:e], iso)
+    g.main_bits = main_component_bitmap(g, stream)
+    return g
+
+
+def main_component_bitmap(g: OnedGraph, stream=None) -> np.ndarray:
+    """Host bitmap of the component of a maximum-degree vertex (the giant
+    component of a Kronecker graph): one BFS from it at build time.  Queries
+    from roots outside it run on a single block (g5_bfs_query)."""
+    if g.nlocaledges == 0:
+        return np.zeros((g.nglobalverts + 31) // 32, np.uint32)
+    hub = int(torch.argmax(g.rowstarts[1:] - g.rowstarts[:-1]))
+    bfs = BfsState(g)
+    _check(lib.g5_bfs_reset(g.nglobalverts, _ptr(bfs.pred), None, None, _ptr(bfs.work), bfs.work.numel(),
+                            _stream(stream)))
+    _check(lib.g5_bfs_traverse(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, hub, _ptr(bfs.pred), None,
+                               _ptr(bfs.work), bfs.work.numel(), None, _stream(stream)))
+    bits = torch.empty((g.nglobalverts + 31) // 32, dtype=torch.int32, device=g.device)
+    _check(lib.g5_bfs_visited_bitmap(_ptr(bfs.work), bfs.work.numel(), g.nglobalverts, _ptr(bits),
+                                     _stream(stream)))
+    bfs_stats(bfs, stream)  # surfaces any device error
+    return bits.cpu().numpy().view(np.uint32)
 
 
 def oned_graph_is_vertex_isolated(g: OnedGraph, global_vertex: int) -> bool:
@@ -277,6 +304,8 @@ class BfsState:
         self.dist: torch.Tensor | None = None
         self.val_work: torch.Tensor | None = None
         self.max_nlocalverts = n
+        self.h_root = torch.zeros(1, dtype=torch.int64).pin_memory()
+        self.h_stats = BfsStats()
 
 
 def oned_graph_bfs_create(g: OnedGraph) -> BfsState:
@@ -301,12 +330,34 @@ def oned_graph_bfs_reset(bfs: BfsState, with_depth: bool = True, g: OnedGraph | 
                             _stream(stream)))
 
 
+def _right_sized(g: OnedGraph, root: int, params: BfsParams | None) -> BfsParams | None:
+    if params is None and not g.in_main_component(root):
+        return BfsParams(14.0, 24.0, 0, 1)  # small component: one block
+    return params
+
+
 def oned_graph_bfs_traverse(g: OnedGraph, bfs: BfsState, root: int, params: BfsParams | None = None,
                             with_depth: bool = True, stream=None) -> None:
-    """Second half of oned_graph_bfs_run: the persistent BFS kernel alone."""
+    """Second half of oned_graph_bfs_run: the persistent BFS kernel alone
+    (one block for a root outside the main component)."""
+    params = _right_sized(g, root, params)
     _check(lib.g5_bfs_traverse(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, root, _ptr(bfs.pred),
                                _ptr(bfs.depth) if with_depth else None, _ptr(bfs.work), bfs.work.numel(),
                                C.byref(params) if params is not None else None, _stream(stream)))
+
+
+def oned_graph_bfs_query(g: OnedGraph, bfs: BfsState, root: int, with_depth: bool = False,
+                         stream=None) -> BfsStats:
+    """One search end to end from the host (g5_bfs_query): the root goes
+    host->device from pinned memory, the search runs on a state reset since
+    its last search, and its statistics come back; synchronises."""
+    bfs.h_root[0] = root
+    mb = g.main_bits
+    _check(lib.g5_bfs_query(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, bfs.h_root.data_ptr(),
+                            mb.ctypes.data if mb is not None else None, _ptr(bfs.pred),
+                            _ptr(bfs.depth) if with_depth else None, _ptr(bfs.work), bfs.work.numel(), None,
+                            C.byref(bfs.h_stats), _stream(stream)))
+    return bfs.h_stats
 
 
 def bfs_stats(bfs: BfsState, stream=None) -> BfsStats:

@@ -52,22 +52,19 @@ struct LevelState {
 static_assert(sizeof(LevelState) % 8 == 0, "LevelState is copied in 8-byte words");
 
 struct BfsCtl {
-    unsigned bar;  // grid barrier arrivals
-    unsigned error;
+    g5_bfs_stats res;     // the search's result (same layout as the C ABI's)
+    unsigned bar;         // grid barrier arrivals
+    unsigned long long root_in;  // root copied in by g5_bfs_query
     unsigned n_small[3];  // per level slot: queue entries of degree <= BIG_DEG
     unsigned long long big[3];  //           big entries << 40 | their chunks
     unsigned grab[3];     //                 work cursor over the small part
     unsigned cgrab[3];    //                 work cursor over the big part's chunks
     unsigned found[3];    //                 vertices found by a bottom-up level
     unsigned long long m_next[3];  //        degree sum of the next frontier
-    int levels;
-    int bu_levels;
-    unsigned long long reached;
     // hand-off from the solo prologue to the grid
     unsigned go;       // 0 wait, 1 continue on the grid, 2 finished
     unsigned heartbeat;  // solo levels completed so far (waiters restart their clock on change)
     unsigned hand_fb;  // 1 when the frontier bitmap is the second buffer
-    unsigned solo_levels;
     LevelState hand;
     // per-level trace: time at the level's end, frontier size and edges, direction
     unsigned long long t0;
@@ -96,6 +93,7 @@ struct BfsArgs {
     int mode;
     unsigned nblocks;
     unsigned long long limit_ns;
+    bool root_from_ctl;  // take the root from ctl->root_in (copied in by the caller's stream)
 };
 
 enum { TOP_DOWN = 0, BOTTOM_UP = 1 };
@@ -106,7 +104,7 @@ __device__ __forceinline__ void td_visit(const BfsArgs &a, const WarpStage &bq, 
                                          int next_level, unsigned *qn, unsigned *basen, unsigned *n_small,
                                          unsigned long long *n_big, unsigned long long &my_m) {
     if (want && v >= a.n) {  // not a vertex: report it, touch nothing
-        atomicOr(&a.ctl->error, DEVERR_RANGE);
+        atomicOr(&a.ctl->res.error_flags, DEVERR_RANGE);
         want = false;
     }
     bool disc = want && bit_claim(a.visited, v);
@@ -119,7 +117,7 @@ __device__ __forceinline__ void td_visit(const BfsArgs &a, const WarpStage &bq, 
         my_m += deg;
     }
     if (!frontier_append_staged(bq, qn, basen, a.n, n_small, n_big, disc, v, deg))
-        atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+        atomicOr(&a.ctl->res.error_flags, DEVERR_CAPACITY);
 }
 
 __device__ void td_expand(const BfsArgs &a, const WarpStage &bq, int level, int cur, int s_cur, int s_nxt,
@@ -179,7 +177,7 @@ __device__ void td_expand(const BfsArgs &a, const WarpStage &bq, int level, int 
             td_visit(a, bq, has, v, u, level + 1, QN, BN, &c->n_small[s_nxt], &c->big[s_nxt], my_m);
         }
     }
-    if (!stage_flush_warp(bq, QN, a.n, &c->n_small[s_nxt])) atomicOr(&c->error, DEVERR_CAPACITY);
+    if (!stage_flush_warp(bq, QN, a.n, &c->n_small[s_nxt])) atomicOr(&c->res.error_flags, DEVERR_CAPACITY);
 }
 
 __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsigned *nb, unsigned long long &my_m,
@@ -205,7 +203,7 @@ __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsig
                 for (int i = 0; i < 4; ++i) word[i] = u[i] < a.n ? __ldcg(&fb[u[i] >> 5]) : 0u;
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
-                    if (e + i < re && u[i] >= a.n) atomicOr(&a.ctl->error, DEVERR_RANGE);
+                    if (e + i < re && u[i] >= a.n) atomicOr(&a.ctl->res.error_flags, DEVERR_RANGE);
                     if (found < 0 && u[i] < a.n && ((word[i] >> (u[i] & 31)) & 1u)) found = (int)u[i];
                 }
             }
@@ -246,10 +244,10 @@ __device__ void bits_to_queue(const BfsArgs &a, const WarpStage &bq, const unsig
                 deg = __ldg(&a.rowptr[v + 1]) - __ldg(&a.rowptr[v]);
             }
             if (!frontier_append_staged(bq, qn, basen, a.n, n_small, n_big, has, v, deg))
-                atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+                atomicOr(&a.ctl->res.error_flags, DEVERR_CAPACITY);
         }
     }
-    if (!stage_flush_warp(bq, qn, a.n, n_small)) atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+    if (!stage_flush_warp(bq, qn, a.n, n_small)) atomicOr(&a.ctl->res.error_flags, DEVERR_CAPACITY);
 }
 
 // Direction of the next level (Beamer's rule; a.mode forces one side).
@@ -334,9 +332,9 @@ __device__ __forceinline__ bool bfs_advance(const BfsArgs &a, LevelState &st, un
 }
 
 __device__ __forceinline__ void bfs_write_stats(const BfsArgs &a, const LevelState &st) {
-    a.ctl->levels = st.levels;
-    a.ctl->bu_levels = st.bu_levels;
-    a.ctl->reached = st.reached;
+    a.ctl->res.levels = st.levels;
+    a.ctl->res.bottom_up_levels = st.bu_levels;
+    a.ctl->res.reached = st.reached;
 }
 
 __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs a) {
@@ -359,18 +357,19 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
     // single grid barrier.
     if (blockIdx.x == 0) {
         const uint64_t E = __ldg(&a.rowptr[a.n]);
-        const uint64_t root_deg = __ldg(&a.rowptr[a.root + 1]) - __ldg(&a.rowptr[a.root]);
+        const unsigned root = a.root_from_ctl ? (unsigned)ld_volatile(&c->root_in) : a.root;
+        const uint64_t root_deg = __ldg(&a.rowptr[root + 1]) - __ldg(&a.rowptr[root]);
         if (threadIdx.x == 0) {
             c->t0 = globaltimer_ns();
-            a.visited[a.root >> 5] |= 1u << (a.root & 31);
-            a.pred[a.root] = a.root;
-            if (a.depth) a.depth[a.root] = 0;
+            a.visited[root >> 5] |= 1u << (root & 31);
+            a.pred[root] = root;
+            if (a.depth) a.depth[root] = 0;
             if (root_deg > BIG_DEG) {
-                a.q[0][a.n - 1] = a.root;
+                a.q[0][a.n - 1] = root;
                 a.base[0][0] = 0;
                 c->big[0] = (1ull << BIG_SHIFT) | ((root_deg + BIG_CHUNK - 1) / BIG_CHUNK);
             } else {
-                a.q[0][0] = a.root;
+                a.q[0][0] = root;
                 c->n_small[0] = 1;
             }
         }
@@ -394,7 +393,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
         if (threadIdx.x == 0) {
             c->hand = st;
             c->hand_fb = fb == a.fbits ? 0 : 1;
-            c->solo_levels = solo;
+            c->res.solo_levels = solo;
             if (done) bfs_write_stats(a, st);
             __threadfence();
             atomicExch(&c->go, done ? 2u : 1u);
@@ -415,7 +414,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
                     t0 = globaltimer_ns();
                 }
                 if (globaltimer_ns() - t0 > a.limit_ns) {
-                    atomicOr(&c->error, DEVERR_TIMEOUT);
+                    atomicOr(&c->res.error_flags, DEVERR_TIMEOUT);
                     g = 2;
                     break;
                 }
@@ -440,7 +439,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
         if (st.pending == PEND_TO_BITS) {
             // Frontier bitmap from the queue q[cur].
             for (uint64_t k = gtid; k < a.nwords; k += nthreads) fb[k] = 0;
-            if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+            if (!grid_sync(&c->bar, &c->res.error_flags, epoch, a.nblocks, a.limit_ns)) return;
             const unsigned *Q = a.q[st.cur];
             const unsigned ns = ld_volatile(&c->n_small[s_cur]), nbg = big_count(ld_volatile(&c->big[s_cur]));
             for (uint64_t i = gtid; i < ns; i += nthreads) {
@@ -451,14 +450,14 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
                 const unsigned v = __ldcg(&Q[a.n - 1 - i]);
                 atomicOr(&fb[v >> 5], 1u << (v & 31));
             }
-            if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+            if (!grid_sync(&c->bar, &c->res.error_flags, epoch, a.nblocks, a.limit_ns)) return;
         } else if (st.pending == PEND_TO_QUEUE) {
             bits_to_queue(a, bq, fb, a.q[st.cur], a.base[st.cur], &c->n_small[s_cur], &c->big[s_cur]);
-            if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+            if (!grid_sync(&c->bar, &c->res.error_flags, epoch, a.nblocks, a.limit_ns)) return;
         }
         st.pending = PEND_NONE;
         bfs_expand_level(a, bq, st, fb, nb);
-        if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+        if (!grid_sync(&c->bar, &c->res.error_flags, epoch, a.nblocks, a.limit_ns)) return;
         if (!bfs_advance(a, st, fb, nb)) break;
     }
     if (gtid == 0) bfs_write_stats(a, st);
@@ -613,19 +612,17 @@ extern "C" int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, 
     return G5_OK;
 }
 
-extern "C" int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
-                               int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
-                               const g5_bfs_params *params, void *stream) {
-    clear_error();
-    BfsWork w;
-    int rc = bfs_check(d_rowstarts, d_col, nverts, root, d_pred, d_work, work_bytes, &w, "g5_bfs_traverse");
-    if (rc) return rc;
+// Builds the kernel arguments and launches the persistent BFS (after zeroing
+// the control block; the root comes from root_in when from_ctl).
+static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
+                      uint64_t root, int64_t *d_pred, int32_t *d_depth, const g5_bfs_params *params,
+                      const uint64_t *h_root, cudaStream_t st) {
     g5_bfs_params p = {14.0f, 24.0f, 0, 0};
     if (params) p = *params;
-    G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= 2, "g5_bfs_traverse: bad params");
-
+    G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= 2, "g5_bfs: bad params");
     int max_blocks = 0;
-    if ((rc = bfs_max_blocks(&max_blocks))) return rc;
+    int rc = bfs_max_blocks(&max_blocks);
+    if (rc) return rc;
     int blocks = p.blocks > 0 ? std::min(p.blocks, max_blocks)
                               : (int)std::min<uint64_t>(max_blocks, std::max<uint64_t>(1, nverts / 2048));
     BfsArgs a;
@@ -649,16 +646,18 @@ extern "C" int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col
     a.mode = p.mode;
     a.nblocks = (unsigned)blocks;
     a.limit_ns = wait_limit_ns();
+    a.root_from_ctl = h_root != nullptr;
     // The control block (counters, hand-off, barrier) starts from zero on
     // every search, so a traversal never sees the previous one's state.
-    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(BfsCtl), (cudaStream_t)stream));
+    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(BfsCtl), st));
+    if (h_root) G5_CUDA_TRY(cudaMemcpyAsync(&w.ctl->root_in, h_root, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     // Cooperative launch; the three bitmaps (visited, frontier, next: N/8
     // bytes each, adjacent in the workspace) get an L2 persisting window so
     // the streaming column reads do not evict them.
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(blocks);
     cfg.blockDim = dim3(BFS_THREADS);
-    cfg.stream = (cudaStream_t)stream;
+    cfg.stream = st;
     cudaLaunchAttribute attrs[2];
     attrs[0].id = cudaLaunchAttributeCooperative;
     attrs[0].val.cooperative = 1;
@@ -666,7 +665,7 @@ extern "C" int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col
     cfg.numAttrs = 1;
     const uint64_t win = (uint64_t)((char *)(w.nbits + a.nwords) - (char *)w.visited);
     uint64_t win_bytes = 0;
-    if ((rc = l2_persist_window(win, &win_bytes))) return rc;
+    if (blocks > 1 && (rc = l2_persist_window(win, &win_bytes))) return rc;
     if (win_bytes) {
         attrs[1].id = cudaLaunchAttributeAccessPolicyWindow;
         attrs[1].val.accessPolicyWindow.base_ptr = w.visited;
@@ -677,6 +676,48 @@ extern "C" int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col
         cfg.numAttrs = 2;
     }
     G5_CUDA_TRY(cudaLaunchKernelEx(&cfg, bfs_persistent_kernel, a));
+    return G5_OK;
+}
+
+extern "C" int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
+                               int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
+                               const g5_bfs_params *params, void *stream) {
+    clear_error();
+    BfsWork w;
+    int rc = bfs_check(d_rowstarts, d_col, nverts, root, d_pred, d_work, work_bytes, &w, "g5_bfs_traverse");
+    if (rc) return rc;
+    return bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, params, nullptr, (cudaStream_t)stream);
+}
+
+extern "C" int g5_bfs_query(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, const uint64_t *h_root,
+                            const uint32_t *h_main_bits, int64_t *d_pred, int32_t *d_depth, void *d_work,
+                            uint64_t work_bytes, const g5_bfs_params *params, g5_bfs_stats *h_stats, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(h_root && h_stats, "g5_bfs_query: NULL host pointer");
+    const uint64_t root = *h_root;
+    BfsWork w;
+    int rc = bfs_check(d_rowstarts, d_col, nverts, root, d_pred, d_work, work_bytes, &w, "g5_bfs_query");
+    if (rc) return rc;
+    g5_bfs_params p = {14.0f, 24.0f, 0, 0};
+    if (params) p = *params;
+    // A root outside the main component reaches a small set: one block
+    // runs the whole search, with no grid to launch or wait for.
+    if (h_main_bits && p.blocks == 0 && !((h_main_bits[root >> 5] >> (root & 31)) & 1u)) p.blocks = 1;
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, &p, h_root, st))) return rc;
+    G5_CUDA_TRY(cudaMemcpyAsync(h_stats, &w.ctl->res, sizeof(g5_bfs_stats), cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    return deverr_to_status(h_stats->error_flags, "g5_bfs_query");
+}
+
+extern "C" int g5_bfs_visited_bitmap(const void *d_work, uint64_t work_bytes, uint64_t nverts, uint32_t *d_bits,
+                                     void *stream) {
+    clear_error();
+    G5_CHECK_ARG(d_work && d_bits && nverts >= 1 && nverts <= (1ull << 31), "g5_bfs_visited_bitmap: bad argument");
+    BfsWork w = carve_bfs((void *)d_work, nverts);
+    if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "g5_bfs_visited_bitmap: workspace too small");
+    G5_CUDA_TRY(cudaMemcpyAsync(d_bits, w.visited, (nverts + 31) / 32 * sizeof(unsigned), cudaMemcpyDeviceToDevice,
+                                (cudaStream_t)stream));
     return G5_OK;
 }
 
@@ -699,10 +740,8 @@ extern "C" int g5_bfs_last_stats(const void *d_work, uint64_t work_bytes, g5_bfs
     cudaStream_t st = (cudaStream_t)stream;
     G5_CUDA_TRY(cudaMemcpyAsync(&c, d_work, sizeof c, cudaMemcpyDeviceToHost, st));
     G5_CUDA_TRY(cudaStreamSynchronize(st));
-    stats->levels = c.levels;
-    stats->bottom_up_levels = c.bu_levels;
-    stats->reached = c.reached;
-    return deverr_to_status(c.error, "g5_bfs_run");
+    *stats = c.res;
+    return deverr_to_status(c.res.error_flags, "g5_bfs_run");
 }
 
 extern "C" int g5_bfs_last_trace(const void *d_work, uint64_t work_bytes, int max_levels, int32_t *mode,
@@ -714,7 +753,7 @@ extern "C" int g5_bfs_last_trace(const void *d_work, uint64_t work_bytes, int ma
     cudaStream_t st = (cudaStream_t)stream;
     G5_CUDA_TRY(cudaMemcpyAsync(&c, d_work, sizeof c, cudaMemcpyDeviceToHost, st));
     G5_CUDA_TRY(cudaStreamSynchronize(st));
-    const int n = std::min(std::min(c.levels, BFS_TRACE), std::max(max_levels, 0));
+    const int n = std::min(std::min(c.res.levels, BFS_TRACE), std::max(max_levels, 0));
     unsigned long long prev = c.t0;
     for (int i = 0; i < n; ++i) {
         if (mode) mode[i] = c.mode_level[i];
@@ -723,9 +762,9 @@ extern "C" int g5_bfs_last_trace(const void *d_work, uint64_t work_bytes, int ma
         if (level_ms) level_ms[i] = (double)(c.t_level[i] - prev) * 1e-6;
         prev = c.t_level[i];
     }
-    *nlevels = c.levels;
-    if (solo_levels) *solo_levels = (int32_t)c.solo_levels;
-    return deverr_to_status(c.error, "g5_bfs_run");
+    *nlevels = c.res.levels;
+    if (solo_levels) *solo_levels = c.res.solo_levels;
+    return deverr_to_status(c.res.error_flags, "g5_bfs_run");
 }
 
 extern "C" int g5_bfs_dist_from_pred(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,

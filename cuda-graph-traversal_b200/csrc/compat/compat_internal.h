@@ -17,6 +17,7 @@ struct GraphExt {
     int32_t *col;        // int32 neighbour ids, light-first rows
     uint32_t *light_deg; // light entries per row
     uint32_t *isolated;  // bitmap of degree-0 vertices
+    uint32_t *main_host; // host bitmap of the largest component (set by the first BFS state)
     float light_delta;
 };
 
@@ -27,6 +28,7 @@ struct BfsExt {
     uint64_t work_bytes;
     void *val_work;  // depth-from-parents scratch
     uint64_t val_bytes;
+    uint64_t *root_host;  // pinned: the root of the next search
 };
 
 struct SsspExt {
@@ -35,7 +37,7 @@ struct SsspExt {
 };
 
 void put_graph(const u64 *rowstarts, const GraphExt &x);
-const GraphExt *get_graph(const Oned_Graph *g, Worker_State *ws);
+GraphExt *get_graph(const Oned_Graph *g, Worker_State *ws);
 void drop_graph(const u64 *rowstarts);
 void put_bfs(const i64 *pred, const BfsExt &x);
 const BfsExt *get_bfs(const i64 *pred);

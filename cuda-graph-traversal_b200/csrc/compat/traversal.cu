@@ -3,6 +3,7 @@
 // behaviour; every call synchronises before returning, as the reference's
 // do, so wall-clock timing around a call measures its work.
 #include <cstring>
+#include <vector>
 
 #include "compat_internal.h"
 #include "traversal.h"
@@ -35,6 +36,7 @@ Oned_Graph oned_graph_from_tuple_graph(Worker_State *ws, Tuple_Graph *tg, u64 ng
     x.col = (int32_t *)gpu_push(ws, g.nlocaledges * sizeof(int32_t), "int32 column");
     x.light_deg = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "light degrees");
     x.light_delta = kLightDelta;
+    x.main_host = nullptr;
     x.isolated = (uint32_t *)gpu_push(ws, (nglobalverts + 31) / 32 * sizeof(uint32_t), "isolated-vertex bitmap");
     check(ws,
           g5_csr_fill((const uint64_t *)tg->edges, tg->weights, tg->edges_size, nglobalverts, g.rowstarts,
@@ -68,7 +70,28 @@ Bfs_State oned_graph_bfs_create(Worker_State *ws, const Oned_Graph *g) {
     x.work = gpu_push(ws, x.work_bytes, "BFS workspace");
     check(ws, g5_validate_workspace_size(g->nglobalverts, &x.val_bytes), "oned_graph_bfs_create");
     x.val_work = gpu_push(ws, x.val_bytes, "BFS depth scratch");
+    CHECK_CUDA(cudaMallocHost(&x.root_host, sizeof(uint64_t)));
     put_bfs(bfs.pred, x);
+    GraphExt *gx = get_graph(g, ws);
+    if (!gx->main_host && g->nlocaledges) {
+        // The largest component: one search from a maximum-degree vertex.
+        // Later searches from roots outside it run on a single block.
+        std::vector<u64> rs(g->nglobalverts + 1);
+        CHECK_CUDA(cudaMemcpy(rs.data(), g->rowstarts, rs.size() * sizeof(u64), cudaMemcpyDeviceToHost));
+        u64 hub = 0;
+        for (u64 v = 1; v < g->nglobalverts; ++v)
+            if (rs[v + 1] - rs[v] > rs[hub + 1] - rs[hub]) hub = v;
+        const u64 words = (g->nglobalverts + 31) / 32;
+        check(ws, g5_bfs_reset(g->nglobalverts, bfs.pred, nullptr, nullptr, x.work, x.work_bytes, 0),
+              "oned_graph_bfs_create");
+        check(ws, g5_bfs_traverse(g->rowstarts, gx->col, g->nglobalverts, hub, bfs.pred, nullptr, x.work, x.work_bytes,
+                                  nullptr, 0),
+              "oned_graph_bfs_create");
+        uint32_t *bits = (uint32_t *)gpu_push(ws, words * sizeof(uint32_t), "component bitmap");
+        check(ws, g5_bfs_visited_bitmap(x.work, x.work_bytes, g->nglobalverts, bits, 0), "oned_graph_bfs_create");
+        gx->main_host = (uint32_t *)malloc(words * sizeof(uint32_t));
+        CHECK_CUDA(cudaMemcpy(gx->main_host, bits, words * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    }
     oned_graph_bfs_clear(ws, &bfs);
     return bfs;
 }
@@ -92,18 +115,18 @@ void oned_graph_bfs_run(Worker_State *ws, const Oned_Graph *g, Bfs_State *bfs, u
         worker_abort(ws, 1);
     }
     const GraphExt *gx = get_graph(g, ws);
-    const BfsExt *bx = get_bfs(bfs->pred);
+    BfsExt *bx = const_cast<BfsExt *>(get_bfs(bfs->pred));
     if (!bx) {
         ERROR("Bfs_State was not created by oned_graph_bfs_create of this library");
         worker_abort(ws, 1);
     }
     // The reset half ran in oned_graph_bfs_clear, which the reference's
     // protocol calls before every search (examples/graph500_runner.cu:309).
-    check(ws, g5_bfs_traverse(g->rowstarts, gx->col, g->nglobalverts, root, bfs->pred, bx->depth, bx->work,
-                              bx->work_bytes, nullptr, 0),
-          "oned_graph_bfs_run");
+    *bx->root_host = root;
     g5_bfs_stats st;
-    check(ws, g5_bfs_last_stats(bx->work, bx->work_bytes, &st, 0), "oned_graph_bfs_run");
+    check(ws, g5_bfs_query(g->rowstarts, gx->col, g->nglobalverts, bx->root_host, gx->main_host, bfs->pred, bx->depth,
+                           bx->work, bx->work_bytes, nullptr, &st, 0),
+          "oned_graph_bfs_run");
 }
 
 i64 *bfs_compute_dist_from_pred(Worker_State *ws, const Oned_Graph *g, Bfs_State *bfs, u64 root) {

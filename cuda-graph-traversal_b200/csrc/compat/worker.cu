@@ -92,7 +92,7 @@ void put_graph(const u64 *k, const GraphExt &x) {
     std::lock_guard<std::mutex> l(g_mu);
     g_graphs[k] = x;
 }
-const GraphExt *get_graph(const Oned_Graph *g, Worker_State *ws) {
+GraphExt *get_graph(const Oned_Graph *g, Worker_State *ws) {
     std::lock_guard<std::mutex> l(g_mu);
     auto it = g_graphs.find(g->rowstarts);
     if (it == g_graphs.end()) {
@@ -103,6 +103,8 @@ const GraphExt *get_graph(const Oned_Graph *g, Worker_State *ws) {
 }
 void drop_graph(const u64 *k) {
     std::lock_guard<std::mutex> l(g_mu);
+    auto it = g_graphs.find(k);
+    if (it != g_graphs.end() && it->second.main_host) free(it->second.main_host);
     g_graphs.erase(k);
 }
 void put_bfs(const i64 *k, const BfsExt &x) {
@@ -116,6 +118,8 @@ const BfsExt *get_bfs(const i64 *k) {
 }
 void drop_bfs(const i64 *k) {
     std::lock_guard<std::mutex> l(g_mu);
+    auto it = g_bfs.find(k);
+    if (it != g_bfs.end() && it->second.root_host) cudaFreeHost(it->second.root_host);
     g_bfs.erase(k);
 }
 void put_sssp(const i64 *k, const SsspExt &x) {

@@ -99,6 +99,8 @@ typedef struct g5_bfs_stats {
     int32_t levels;           /* BFS levels expanded                           */
     int32_t bottom_up_levels; /* of which bottom-up                            */
     uint64_t reached;         /* vertices with a parent (root included)        */
+    uint32_t error_flags;     /* device-side error bits, 0 when none           */
+    int32_t solo_levels;      /* levels run by one block before the grid       */
 } g5_bfs_stats;
 
 int g5_bfs_workspace_size(uint64_t nverts, uint64_t *bytes);
@@ -127,6 +129,23 @@ int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, const uint3
 int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
                     int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
                     const g5_bfs_params *params, void *stream);
+
+/* One search end to end from host memory, for callers that issue single
+ * queries: copies *h_root (pinned host memory) to the device, runs the
+ * traversal on a workspace reset since its last search, copies the
+ * statistics to *h_stats and synchronises.  h_main_bits (host bitmap of the
+ * main component, optional; see g5_bfs_visited_bitmap) lets a root outside
+ * it run on a single block, which a small component needs and which avoids
+ * launching and waiting for the whole grid. */
+int g5_bfs_query(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, const uint64_t *h_root,
+                 const uint32_t *h_main_bits, int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
+                 const g5_bfs_params *params, g5_bfs_stats *h_stats, void *stream);
+
+/* Copies the visited bitmap of the last search on this workspace (bit v set
+ * when v was reached; ceil(nverts/32) words).  After a search from a
+ * vertex of the largest component, reset without an initial bitmap, this
+ * is the main-component bitmap g5_bfs_query takes. */
+int g5_bfs_visited_bitmap(const void *d_work, uint64_t work_bytes, uint64_t nverts, uint32_t *d_bits, void *stream);
 
 /* Statistics of the last g5_bfs_run that used this workspace (synchronises). */
 int g5_bfs_last_stats(const void *d_work, uint64_t work_bytes, g5_bfs_stats *stats, void *stream);

