@@ -194,7 +194,11 @@ class OnedGraph:
     main_bits: np.ndarray | None = None   # host uint32 bitmap of the largest component
 
     def in_main_component(self, v: int) -> bool:
-        return self.main_bits is None or bool((int(self.main_bits[v >> 5]) >> (v & 31)) & 1)
+        """True when v is in the largest component (or unknown / out of
+        range: the library call itself then validates v)."""
+        if self.main_bits is None or not 0 <= v < self.nglobalverts:
+            return True
+        return bool((int(self.main_bits[v >> 5]) >> (v & 31)) & 1)
 
     @property
     def nlocalverts(self) -> int:
