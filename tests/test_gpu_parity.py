@@ -301,26 +301,34 @@ def test_bounded_wait_reports_timeout_and_context_survives(cgt):
 
 
 def test_bfs_query_path_and_small_components(cgt, oracle, graphs):
-    """g5_bfs_query (pinned root in, stats out) gives the same trees as the
-    plain path; roots outside the main component run on one block."""
+    """g5_bfs_query (pinned root in, stats out) gives the oracle's trees;
+    roots outside the main component run on one block with the same result."""
     d = graphs[14]
     g = d["g"]
     bfs = cgt.BfsState(g)
-    main = g.main_bits
-    roots = cgt.generate_bfs_roots(g, 2, 3, 16)
-    rs = d["ors"]
-    deg = np.diff(rs.astype(np.int64))
-    outside = [v for v in range(g.nglobalverts) if deg[v] > 0 and not g.in_main_component(v)][:6]
-    assert outside, "a Kronecker graph has small components"
-    for r in roots + outside:
+    for r in cgt.generate_bfs_roots(g, 2, 3, 8):
+        assert g.in_main_component(r)
         cgt.oned_graph_bfs_reset(bfs, g=g)
         st = cgt.oned_graph_bfs_query(g, bfs, r, with_depth=True)
-        _, od = oracle.bfs(rs, d["ocol"], d["n"], r)
+        _, od = oracle.bfs(d["ors"], d["ocol"], d["n"], r)
         assert np.array_equal(_np(bfs.depth).astype(np.int64), od)
         assert st.reached == int((od != -1).sum()) and st.error_flags == 0
-        if r in outside:
-            assert st.reached < 1000
-    # the main component is where the big searches go
-    assert all(g.in_main_component(r) for r in roots if (lambda s: s)(True)) or True
-    big = [r for r in roots if g.in_main_component(r)]
-    assert len(big) >= len(roots) - 2
+    # A graph with a 300-vertex star-and-chain component and small ones.
+    n = 1024
+    e = [(0, i) for i in range(1, 200)] + [(i, i + 1) for i in range(199, 299)]
+    e += [(500, 501), (600, 601), (601, 602), (602, 603), (700, 700)]
+    edges = torch.tensor(e, dtype=torch.int64, device="cuda")
+    tg = cgt.TupleGraph(edges, torch.full((len(e),), 0.5, device="cuda"), len(e))
+    h = cgt.oned_graph_from_tuple_graph(tg, n)
+    assert h.in_main_component(0) and h.in_main_component(299)
+    assert not h.in_main_component(500) and not h.in_main_component(603) and not h.in_main_component(700)
+    rs, col = _np(h.rowstarts).view(np.uint64), _np(h.col).view(np.uint32)
+    hb = cgt.BfsState(h)
+    for r in (0, 250, 500, 601, 603, 700, 1000):
+        cgt.oned_graph_bfs_reset(hb, g=h)
+        st = cgt.oned_graph_bfs_query(h, hb, r, with_depth=True)
+        _, od = oracle.bfs(rs, col, n, r)
+        assert np.array_equal(_np(hb.depth).astype(np.int64), od), r
+        assert st.reached == int((od != -1).sum())
+        if not h.in_main_component(r):
+            assert st.solo_levels == st.levels  # the whole search ran on one block
