@@ -310,6 +310,10 @@ class BfsState:
         self.max_nlocalverts = n
         self.h_root = torch.zeros(1, dtype=torch.int64).pin_memory()
         self.h_stats = BfsStats()
+        # Raw addresses for the single-call query path.
+        self._root_slot = C.c_uint64.from_address(self.h_root.data_ptr())
+        self._q = (self.h_root.data_ptr(), self.pred.data_ptr(), self.depth.data_ptr(), self.work.data_ptr(),
+                   self.work.numel(), C.byref(self.h_stats))
 
 
 def oned_graph_bfs_create(g: OnedGraph) -> BfsState:
@@ -355,12 +359,14 @@ def oned_graph_bfs_query(g: OnedGraph, bfs: BfsState, root: int, with_depth: boo
     """One search end to end from the host (g5_bfs_query): the root goes
     host->device from pinned memory, the search runs on a state reset since
     its last search, and its statistics come back; synchronises."""
-    bfs.h_root[0] = root
+    bfs._root_slot.value = root
+    hr, pred, depth, work, nwork, stats = bfs._q
     mb = g.main_bits
-    _check(lib.g5_bfs_query(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, bfs.h_root.data_ptr(),
-                            mb.ctypes.data if mb is not None else None, _ptr(bfs.pred),
-                            _ptr(bfs.depth) if with_depth else None, _ptr(bfs.work), bfs.work.numel(), None,
-                            C.byref(bfs.h_stats), _stream(stream)))
+    rc = lib.g5_bfs_query(g.rowstarts.data_ptr(), g.col.data_ptr(), g.nglobalverts, hr,
+                          mb.ctypes.data if mb is not None else None, pred, depth if with_depth else None, work,
+                          nwork, None, stats, _stream(stream))
+    if rc:
+        _check(rc)
     return bfs.h_stats
 
 

@@ -30,6 +30,7 @@
 // Algorithmic bytes per search (one component of n_c vertices and m_c
 // undirected edges): 2 m_c * 4 (col) + n_c * (8 rowstarts + 8 pred + 4 depth).
 #include <algorithm>
+#include <atomic>
 
 #include "g5_common.cuh"
 #include "g5_frontier.cuh"
@@ -62,8 +63,8 @@ struct BfsCtl {
     unsigned found[3];    //                 vertices found by a bottom-up level
     unsigned long long m_next[3];  //        degree sum of the next frontier
     // hand-off from the solo prologue to the grid
-    unsigned go;       // 0 wait, 1 continue on the grid, 2 finished
-    unsigned heartbeat;  // solo levels completed so far (waiters restart their clock on change)
+    unsigned long long go;  // launch sequence << 2 | 1 (continue on the grid) or 2 (finished)
+    unsigned heartbeat;     // solo levels completed so far (waiters restart their clock on change)
     unsigned hand_fb;  // 1 when the frontier bitmap is the second buffer
     LevelState hand;
     // per-level trace: time at the level's end, frontier size and edges, direction
@@ -94,6 +95,7 @@ struct BfsArgs {
     unsigned nblocks;
     unsigned long long limit_ns;
     bool root_from_ctl;  // take the root from ctl->root_in (copied in by the caller's stream)
+    unsigned long long seq;  // unique per launch: releases only this launch's waiting blocks
 };
 
 enum { TOP_DOWN = 0, BOTTOM_UP = 1 };
@@ -360,7 +362,17 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
         const unsigned root = a.root_from_ctl ? (unsigned)ld_volatile(&c->root_in) : a.root;
         const uint64_t root_deg = __ldg(&a.rowptr[root + 1]) - __ldg(&a.rowptr[root]);
         if (threadIdx.x == 0) {
+            // Fresh control state for this launch.  The other blocks read
+            // none of it before block 0 releases them below, and they wait
+            // for this launch's sequence number, so no leftover from an
+            // earlier search on the workspace can release them.
             c->t0 = globaltimer_ns();
+            c->res = g5_bfs_stats{0, 0, 0, 0, 0};
+            c->bar = 0;
+            for (int k = 0; k < 3; ++k) {
+                c->n_small[k] = c->grab[k] = c->cgrab[k] = c->found[k] = 0;
+                c->big[k] = c->m_next[k] = 0;
+            }
             a.visited[root >> 5] |= 1u << (root & 31);
             a.pred[root] = root;
             if (a.depth) a.depth[root] = 0;
@@ -396,7 +408,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
             c->res.solo_levels = solo;
             if (done) bfs_write_stats(a, st);
             __threadfence();
-            atomicExch(&c->go, done ? 2u : 1u);
+            atomicExch(&c->go, (a.seq << 2) | (done ? 2ull : 1ull));
         }
         if (done) return;
     } else {
@@ -406,8 +418,9 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
             // level, so only a stalled prologue times out.
             unsigned long long t0 = globaltimer_ns();
             unsigned beat = ld_volatile(&c->heartbeat);
-            unsigned g;
-            while ((g = ld_acquire(&c->go)) == 0) {
+            unsigned long long go;
+            unsigned g = 0;
+            while (((go = ld_acquire64(&c->go)) >> 2) != a.seq) {
                 const unsigned b = ld_volatile(&c->heartbeat);
                 if (b != beat) {
                     beat = b;
@@ -420,7 +433,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
                 }
                 __nanosleep(64);
             }
-            s_go = g;
+            s_go = g ? g : (unsigned)(go & 3);
         }
         __syncthreads();
         if (s_go == 2) return;
@@ -604,6 +617,7 @@ extern "C" int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, 
     cudaStream_t st = (cudaStream_t)stream;
     G5_CUDA_TRY(cudaMemsetAsync(d_pred, 0xff, nverts * sizeof(int64_t), st));
     if (d_depth) G5_CUDA_TRY(cudaMemsetAsync(d_depth, 0xff, nverts * sizeof(int32_t), st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(BfsCtl), st));
     const uint64_t vbytes = (nverts + 31) / 32 * sizeof(unsigned);
     if (d_visited_init)
         G5_CUDA_TRY(cudaMemcpyAsync(w.visited, d_visited_init, vbytes, cudaMemcpyDeviceToDevice, st));
@@ -647,9 +661,8 @@ static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32
     a.nblocks = (unsigned)blocks;
     a.limit_ns = wait_limit_ns();
     a.root_from_ctl = h_root != nullptr;
-    // The control block (counters, hand-off, barrier) starts from zero on
-    // every search, so a traversal never sees the previous one's state.
-    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(BfsCtl), st));
+    static std::atomic<unsigned long long> next_seq{1};
+    a.seq = next_seq.fetch_add(1);
     if (h_root) G5_CUDA_TRY(cudaMemcpyAsync(&w.ctl->root_in, h_root, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     // Cooperative launch; the three bitmaps (visited, frontier, next: N/8
     // bytes each, adjacent in the workspace) get an L2 persisting window so
