@@ -112,6 +112,23 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def rank_roots(roots, rank, world):
+    """Roots of one rank under weak scaling: every world-th root."""
+    return roots[rank::world] or list(roots)
+
+
+def combine_ranks(dist, device, total_ms, edges, hm):
+    """Whole-job numbers: the slowest rank's time, all ranks' edges, and the
+    sum of the ranks' harmonic means.  Every rank calls it (collectives)."""
+    import torch
+    t = torch.tensor([total_ms, edges, hm], dtype=torch.float64, device=device)
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = t.clone()
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(sm[1]), float(sm[2])
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -149,7 +166,7 @@ def run_ours(args):
     del tg
     torch.cuda.empty_cache()
     roots_all = G.generate_bfs_roots(g, 2, 3, 64)
-    my_roots = roots_all[rank::world] or roots_all
+    my_roots = rank_roots(roots_all, rank, world)
     K, W = args.steps, args.warmup
     seq = [my_roots[i % len(my_roots)] for i in range(W + K)]
     bfs = G.BfsState(g)
@@ -256,20 +273,11 @@ def run_ours(args):
     # Whole-job numbers across ranks: slowest rank's time, all ranks' edges.
     tot_edges = float(np.sum(t_nedge))
     max_ms = total_ms
-    if pg:
-        t = torch.tensor([total_ms, tot_edges], dtype=torch.float64, device=dev)
-        mx = t.clone()
-        pg.all_reduce(mx, op=pg.ReduceOp.MAX)
-        sm = t.clone()
-        pg.all_reduce(sm, op=pg.ReduceOp.SUM)
-        max_ms, tot_edges = float(mx[0]), float(sm[1])
     # Per rank the Graph500 harmonic mean; across ranks (weak scaling) the
     # ranks' harmonic means add up.
     value = hm
     if pg:
-        t = torch.tensor([hm], dtype=torch.float64, device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.SUM)
-        value = float(t[0])
+        max_ms, tot_edges, value = combine_ranks(pg, dev, total_ms, tot_edges, hm)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
