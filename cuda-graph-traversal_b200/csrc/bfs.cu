@@ -31,6 +31,7 @@
 // undirected edges): 2 m_c * 4 (col) + n_c * (8 rowstarts + 8 pred + 4 depth).
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 
 #include "g5_common.cuh"
 #include "g5_frontier.cuh"
@@ -743,6 +744,62 @@ extern "C" int g5_bfs_run(const uint64_t *d_rowstarts, const int32_t *d_col, uin
     if (rc) return rc;
     if ((rc = g5_bfs_reset(nverts, d_pred, d_depth, nullptr, d_work, work_bytes, stream))) return rc;
     return g5_bfs_traverse(d_rowstarts, d_col, nverts, root, d_pred, d_depth, d_work, work_bytes, params, stream);
+}
+
+// ---------------------------------------------- allocation-free variant --
+//
+// Some callers cannot allocate device memory when they search: a process
+// whose device memory is handed out entirely by another allocator (an arena
+// like the reference's symmetric heap, or a framework's caching pool) would
+// fail or fragment it, and cudaMalloc/cudaFree synchronise the device,
+// which a latency-bound query loop cannot afford.  For them the BFS scratch
+// can live in a fixed array in this library's device image instead of a
+// caller-provided workspace: STATIC_BFS_BYTES (5 MiB) on every GPU that
+// loads the library, held until the process exits, enough for graphs of up
+// to STATIC_BFS_MAX_VERTS (2^18) vertices.
+
+constexpr uint64_t STATIC_BFS_MAX_VERTS = 1ull << 18;
+constexpr uint64_t STATIC_BFS_BYTES = 5ull << 20;
+static __device__ __align__(256) unsigned char g5_bfs_static_scratch[STATIC_BFS_BYTES];
+
+// Device address of the array on the current device, looked up once per
+// device (in host code the array's name is only a stand-in).
+static int static_bfs_scratch(void **out) {
+    static std::mutex mu;
+    static void *addr[64] = {};
+    int dev = 0;
+    G5_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(G5_ERR_INVALID, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g5_bfs_static_scratch);
+        if (e != cudaSuccess || !p)
+            return set_error(G5_ERR_CUDA, "g5_bfs_run_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        addr[dev] = p;
+    }
+    *out = addr[dev];
+    return G5_OK;
+}
+
+extern "C" int g5_bfs_run_static(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
+                                 int64_t *d_pred, int32_t *d_depth, const g5_bfs_params *params, void *stream) {
+    clear_error();
+    if (nverts > STATIC_BFS_MAX_VERTS)
+        return set_error(G5_ERR_INVALID,
+                         "g5_bfs_run_static: %llu vertices exceed its fixed scratch limit of %llu; use g5_bfs_run "
+                         "with a workspace",
+                         (unsigned long long)nverts, (unsigned long long)STATIC_BFS_MAX_VERTS);
+    if (carve_bfs(nullptr, nverts).bytes > STATIC_BFS_BYTES)
+        return set_error(G5_ERR_WORKSPACE, "g5_bfs_run_static: scratch too small for %llu vertices",
+                         (unsigned long long)nverts);
+    void *scratch = nullptr;
+    int rc = static_bfs_scratch(&scratch);
+    if (rc) return rc;
+    // g5_bfs_run clears what must start at zero (pred, depth, the visited
+    // bitmap, the control block) before the search, so the previous call's
+    // contents do not matter.
+    return g5_bfs_run(d_rowstarts, d_col, nverts, root, d_pred, d_depth, scratch, STATIC_BFS_BYTES, params, stream);
 }
 
 extern "C" int g5_bfs_last_stats(const void *d_work, uint64_t work_bytes, g5_bfs_stats *stats, void *stream) {

@@ -160,6 +160,21 @@ int g5_bfs_last_trace(const void *d_work, uint64_t work_bytes, int max_levels, i
                       uint64_t *frontier_vertices, uint64_t *frontier_edges, double *level_ms, int32_t *nlevels,
                       int32_t *solo_levels, void *stream);
 
+/* g5_bfs_run without a workspace, for callers that cannot allocate device
+ * memory: a process whose device memory belongs entirely to another
+ * allocator (an arena or caching pool) has none to give, and cudaMalloc /
+ * cudaFree synchronise the whole device, which a query loop cannot stall
+ * for.  The scratch is a fixed 5 MiB array inside the library, present on
+ * every GPU that loads it until the process exits; graphs are limited to
+ * 2^18 vertices (G5_ERR_INVALID beyond).  The caller still provides the
+ * graph and the outputs.  The first call on a device looks up the array's
+ * device address, so make it before any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU (other streams, other host
+ * threads) race, so serialise them.  Each call clears what must start at
+ * zero.  No counterpart in the reference. */
+int g5_bfs_run_static(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
+                      int64_t *d_pred, int32_t *d_depth, const g5_bfs_params *params, void *stream);
+
 /* bfs_compute_dist_from_pred, src/traversal.h:48 (src/traversal.cu:505-563):
  * d_dist[v] = -1 where pred is -1, 0 at the root, the tree depth where the
  * parent chain reaches the root through CSR edges, INT64_MAX otherwise.
