@@ -50,6 +50,8 @@ def _load() -> C.CDLL:
         "g5_csr_workspace_size": ([u64, u64, p], C.c_int),
         "g5_csr_count": ([p, u64, u64, p, p, u64, p, p], C.c_int),
         "g5_csr_fill": ([p, p, u64, u64, p, f32, p, u64, p, p, p, p, p], C.c_int),
+        "g5_csr_count_kronecker": ([p, u32, u64, p, p, u64, p, p], C.c_int),
+        "g5_csr_fill_kronecker": ([p, u32, u64, p, f32, p, u64, p, p, p, p, p], C.c_int),
         "g5_bfs_workspace_size": ([u64, p], C.c_int),
         "g5_bfs_run": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_bfs_reset": ([u64, p, p, p, p, u64, p], C.c_int),
@@ -230,6 +232,33 @@ def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: 
     _check(lib.g5_csr_fill(_ptr(tg.edges), _ptr(tg.weights), m, n, _ptr(rowstarts), light_delta,
                            _ptr(work), work.numel(), _ptr(col), _ptr(w), _ptr(col64), _ptr(light), st))
     iso = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
+    _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), n, _ptr(iso), st))
+    g = OnedGraph(n, e, rowstarts, col[:e], w[:e], light, light_delta, None if col64 is None else col64[:e], iso)
+    g.main_bits = main_component_bitmap(g, stream)
+    return g
+
+
+def oned_graph_from_kronecker(seed, log_n: int, nedges: int, device="cuda", light_delta: float = 0.1,
+                              with_column64: bool = False, stream=None) -> OnedGraph:
+    """generate_kronecker_range + oned_graph_from_tuple_graph in one step,
+    with the generator fused into the CSR passes (no edge list in memory)."""
+    n = 1 << log_n
+    s = (C.c_uint32 * 5)(*seed)
+    nb = C.c_uint64()
+    _check(lib.g5_csr_workspace_size(n, nedges, C.byref(nb)))
+    work = _workspace(nb.value, device)
+    rowstarts = torch.empty(n + 1, dtype=torch.int64, device=device)
+    nent = C.c_uint64()
+    st = _stream(stream)
+    _check(lib.g5_csr_count_kronecker(s, log_n, nedges, _ptr(rowstarts), _ptr(work), work.numel(), C.byref(nent), st))
+    e = nent.value
+    col = torch.empty(max(e, 1), dtype=torch.int32, device=device)
+    w = torch.empty(max(e, 1), dtype=torch.float32, device=device)
+    light = torch.empty(n, dtype=torch.int32, device=device)
+    col64 = torch.empty(max(e, 1), dtype=torch.int64, device=device) if with_column64 else None
+    _check(lib.g5_csr_fill_kronecker(s, log_n, nedges, _ptr(rowstarts), light_delta, _ptr(work), work.numel(),
+                                     _ptr(col), _ptr(w), _ptr(col64), _ptr(light), st))
+    iso = torch.empty((n + 31) // 32, dtype=torch.int32, device=device)
     _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), n, _ptr(iso), st))
     g = OnedGraph(n, e, rowstarts, col[:e], w[:e], light, light_delta, None if col64 is None else col64[:e], iso)
     g.main_bits = main_component_bitmap(g, stream)

@@ -15,6 +15,7 @@
 // HBM bytes per edge: count reads 16; fill reads 20 and writes 2 x (4 col +
 // 4 w [+ 8 col64]) scattered.
 #include "g5_common.cuh"
+#include "g5_mrg.cuh"
 
 namespace g5 {
 
@@ -178,6 +179,50 @@ __global__ void csr_fill_kernel(const ulonglong2 *__restrict__ edges, const floa
     }
 }
 
+// Generator fused into the CSR passes: each thread walks its edges of the
+// Kronecker stream (as kron_generate_kernel) and counts (FILL = false) or
+// scatters (FILL = true) them directly, so the 20-byte-per-edge edge list is
+// never written or read.  Both passes regenerate the same edges.
+template <bool FILL>
+__global__ void __launch_bounds__(256) kron_csr_kernel(KronLaunch k, uint64_t n, const uint64_t *__restrict__ rowstarts,
+                                                       float delta, unsigned *__restrict__ lo,
+                                                       unsigned *__restrict__ hi, int *__restrict__ col,
+                                                       float *__restrict__ w, uint64_t *__restrict__ col64) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t T = (int64_t)gridDim.x * blockDim.x;
+    if (t >= k.count) return;
+    MrgState z = kron_thread_start(k, t);
+    for (int64_t i = t; i < k.count; i += T) {
+        uint64_t a, b;
+        float wt;
+        kron_edge(z, k.log_n, k.val0, k.val1, a, b, wt);
+        mrg_apply(k.stride_jump, z);
+        if (a == b) continue;  // ids are < 2^log_n = n by construction
+        if (!FILL) {
+            atomicAdd(&lo[a], 1u);
+            atomicAdd(&lo[b], 1u);
+            continue;
+        }
+        uint64_t pa, pb;
+        if (wt < delta) {
+            pa = rowstarts[a] + atomicAdd(&lo[a], 1u);
+            pb = rowstarts[b] + atomicAdd(&lo[b], 1u);
+        } else {
+            pa = rowstarts[a + 1] - 1 - atomicAdd(&hi[a], 1u);
+            pb = rowstarts[b + 1] - 1 - atomicAdd(&hi[b], 1u);
+        }
+        if (pa >= rowstarts[a + 1] || pa < rowstarts[a] || pb >= rowstarts[b + 1] || pb < rowstarts[b]) continue;
+        col[pa] = (int)b;
+        w[pa] = wt;
+        col[pb] = (int)a;
+        w[pb] = wt;
+        if (col64) {
+            col64[pa] = b;
+            col64[pb] = a;
+        }
+    }
+}
+
 struct CsrWork {
     unsigned *deg;    // degrees, then heavy cursors
     unsigned *lo;     // light cursors when the caller keeps no light degrees
@@ -263,6 +308,55 @@ extern "C" int g5_csr_fill(const uint64_t *d_edges, const float *d_weights, uint
         csr_fill_kernel<<<grid_for(nedges, 256), 256, 0, st>>>((const ulonglong2 *)d_edges, d_weights, nedges, nverts,
                                                                d_rowstarts, light_delta, lo, w.deg, d_col, d_w,
                                                                d_col64);
+        G5_CUDA_TRY(cudaGetLastError());
+    }
+    return G5_OK;
+}
+
+extern "C" int g5_csr_count_kronecker(const uint32_t seed[5], uint32_t log_n, uint64_t nedges, uint64_t *d_rowstarts,
+                                      void *d_work, uint64_t work_bytes, uint64_t *nentries, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(log_n >= 1 && log_n <= 31, "g5_csr_count_kronecker: log_n %u outside [1, 31]", log_n);
+    G5_CHECK_ARG(d_rowstarts && d_work && nentries, "g5_csr_count_kronecker: NULL argument");
+    const uint64_t n = 1ull << log_n;
+    KronLaunch k;
+    int blocks = 0;
+    int rc = kron_prepare(seed, log_n, 0, (int64_t)nedges, 256, &k, &blocks, "g5_csr_count_kronecker");
+    if (rc) return rc;
+    CsrWork w = carve_csr(d_work, n);
+    if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "g5_csr_count_kronecker: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    G5_CUDA_TRY(cudaMemsetAsync(w.deg, 0, n * sizeof(unsigned), st));
+    if (nedges) {
+        kron_csr_kernel<false><<<blocks, 256, 0, st>>>(k, n, nullptr, 0.0f, w.deg, nullptr, nullptr, nullptr, nullptr);
+        G5_CUDA_TRY(cudaGetLastError());
+    }
+    if ((rc = scan_u32_to_u64(w.deg, n, d_rowstarts, w.scan, st))) return rc;
+    G5_CUDA_TRY(cudaMemcpyAsync(nentries, d_rowstarts + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    return G5_OK;
+}
+
+extern "C" int g5_csr_fill_kronecker(const uint32_t seed[5], uint32_t log_n, uint64_t nedges,
+                                     const uint64_t *d_rowstarts, float light_delta, void *d_work, uint64_t work_bytes,
+                                     int32_t *d_col, float *d_w, uint64_t *d_col64, uint32_t *d_light_deg,
+                                     void *stream) {
+    clear_error();
+    G5_CHECK_ARG(log_n >= 1 && log_n <= 31, "g5_csr_fill_kronecker: log_n %u outside [1, 31]", log_n);
+    G5_CHECK_ARG(d_rowstarts && d_work && d_col && d_w, "g5_csr_fill_kronecker: NULL argument");
+    const uint64_t n = 1ull << log_n;
+    KronLaunch k;
+    int blocks = 0;
+    int rc = kron_prepare(seed, log_n, 0, (int64_t)nedges, 256, &k, &blocks, "g5_csr_fill_kronecker");
+    if (rc) return rc;
+    CsrWork w = carve_csr(d_work, n);
+    if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "g5_csr_fill_kronecker: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned *lo = d_light_deg ? d_light_deg : w.lo;
+    G5_CUDA_TRY(cudaMemsetAsync(lo, 0, n * sizeof(unsigned), st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.deg, 0, n * sizeof(unsigned), st));
+    if (nedges) {
+        kron_csr_kernel<true><<<blocks, 256, 0, st>>>(k, n, d_rowstarts, light_delta, lo, w.deg, d_col, d_w, d_col64);
         G5_CUDA_TRY(cudaGetLastError());
     }
     return G5_OK;

@@ -115,6 +115,51 @@ G5_HD float mrg_unit_float(uint32_t u) {
 #endif
 }
 
+// One Graph500 edge from the stream that starts at s: one quadrant per
+// level, most significant bit first, folding the lower-left quadrant onto the
+// upper-right while on the diagonal (cuda_make_one_edge,
+// src/graph_generation.cu:186-207), both endpoints scrambled, then the
+// weight drawn from the same stream (:225-238).
+G5_HD void kron_edge(MrgState s, int log_n, uint64_t val0, uint64_t val1, uint64_t &src_out, uint64_t &dst_out,
+                     float &w_out) {
+    uint64_t src = 0, dst = 0;
+    for (int lvl = log_n - 1; lvl >= 0; --lvl) {
+        const int q = kron_quadrant(s);
+        uint64_t so = (uint64_t)(q >> 1), to = (uint64_t)(q & 1);
+        if (src == dst && so > to) {
+            so = 0;
+            to = 1;
+        }
+        src |= so << lvl;
+        dst |= to << lvl;
+    }
+    src_out = kron_scramble(src, log_n, val0, val1);
+    dst_out = kron_scramble(dst, log_n, val0, val1);
+    w_out = mrg_unit_float(mrg_next(s));
+}
+
+// Everything a grid needs to walk edges [start, start + count): thread t of
+// T starts at edge start + t (jump through the mid-byte tables) and steps by
+// A^(T * 2^64).
+struct KronLaunch {
+    MrgState base;
+    MrgMatrix stride_jump;
+    int log_n;
+    int64_t start, count;
+    uint64_t val0, val1;
+    const MrgMatrix *mid_table;
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ MrgState kron_thread_start(const KronLaunch &k, int64_t t) {
+    MrgState z = k.base;
+    uint64_t e = (uint64_t)(k.start + t);
+    for (int b = 0; e; ++b, e >>= 8)
+        if (e & 0xFF) mrg_apply(k.mid_table[256 * b + (e & 0xFF)], z);
+    return z;
+}
+#endif
+
 // ------------------------------------------------------------- host only --
 
 // Host copy of A^(v * 256^b) for byte b in [0, 24) and value v.
@@ -126,5 +171,9 @@ MrgMatrix mrg_jump_mid(uint64_t n);
 // Uploads the byte tables for the 2^64-step jumps (bytes 8..15) to the
 // current device once; returns their device address.
 int mrg_device_mid_table(const MrgMatrix **out);
+// Validates the seed and range and fills a KronLaunch for a grid of
+// `threads` threads (capped by the device; *blocks gets the grid size).
+int kron_prepare(const uint32_t seed[5], uint32_t log_n, int64_t start, int64_t end, int threads_per_block,
+                 KronLaunch *k, int *blocks, const char *who);
 
 }  // namespace g5

@@ -102,38 +102,49 @@ int mrg_device_mid_table(const MrgMatrix **out) {
 
 // ---------------------------------------------------------------- kernel --
 
-__global__ void __launch_bounds__(256) kron_generate_kernel(MrgState base, MrgMatrix stride_jump, int log_n,
-                                                            int64_t start, int64_t count, uint64_t val0,
-                                                            uint64_t val1, const MrgMatrix *__restrict__ mid_table,
-                                                            ulonglong2 *__restrict__ edges,
+__global__ void __launch_bounds__(256) kron_generate_kernel(KronLaunch k, ulonglong2 *__restrict__ edges,
                                                             float *__restrict__ weights) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t T = (int64_t)gridDim.x * blockDim.x;
-    if (t >= count) return;
-
-    // Stream of the thread's first edge: seed * A^((start + t) * 2^64).
-    MrgState z = base;
-    uint64_t e = (uint64_t)(start + t);
-    for (int b = 0; e; ++b, e >>= 8)
-        if (e & 0xFF) mrg_apply(mid_table[256 * b + (e & 0xFF)], z);
-
-    for (int64_t i = t; i < count; i += T) {
-        MrgState s = z;
-        uint64_t src = 0, dst = 0;
-        // One quadrant per level, most significant bit first; on the
-        // diagonal the lower-left quadrant folds onto the upper-right
-        // (cuda_make_one_edge, src/graph_generation.cu:186-207).
-        for (int lvl = log_n - 1; lvl >= 0; --lvl) {
-            int q = kron_quadrant(s);
-            uint64_t so = (uint64_t)(q >> 1), to = (uint64_t)(q & 1);
-            if (src == dst && so > to) { so = 0; to = 1; }
-            src |= so << lvl;
-            dst |= to << lvl;
-        }
-        edges[i] = make_ulonglong2(kron_scramble(src, log_n, val0, val1), kron_scramble(dst, log_n, val0, val1));
-        weights[i] = mrg_unit_float(mrg_next(s));
-        mrg_apply(stride_jump, z);
+    if (t >= k.count) return;
+    MrgState z = kron_thread_start(k, t);
+    for (int64_t i = t; i < k.count; i += T) {
+        uint64_t src, dst;
+        float w;
+        kron_edge(z, k.log_n, k.val0, k.val1, src, dst, w);
+        edges[i] = make_ulonglong2(src, dst);
+        weights[i] = w;
+        mrg_apply(k.stride_jump, z);
     }
+}
+
+int kron_prepare(const uint32_t seed[5], uint32_t log_n, int64_t start, int64_t end, int threads_per_block,
+                 KronLaunch *k, int *blocks, const char *who) {
+    G5_CHECK_ARG(seed, "%s: seed is NULL", who);
+    G5_CHECK_ARG(log_n >= 1 && log_n <= 62, "%s: log_n %u outside [1, 62]", who, log_n);
+    G5_CHECK_ARG(start >= 0 && end >= start, "%s: bad edge range", who);
+    for (int i = 0; i < 5; ++i) G5_CHECK_ARG(seed[i] < MRG_P, "%s: seed word %d not below 2^31-1", who, i);
+    G5_CHECK_ARG(seed[0] | seed[1] | seed[2] | seed[3] | seed[4], "%s: all-zero seed", who);
+    const int64_t count = end - start;
+    *blocks = 0;
+    k->count = count;
+    if (!count) return G5_OK;  // nothing to launch; no device work either
+    DeviceInfo di;
+    int rc = device_info(&di);
+    if (rc) return rc;
+    if ((rc = mrg_device_mid_table(&k->mid_table))) return rc;
+    int64_t b = (count + threads_per_block - 1) / threads_per_block;
+    const int64_t cap = (int64_t)di.sms * (di.max_threads_per_sm / threads_per_block);
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    *blocks = (int)b;
+    k->base = MrgState{{seed[0], seed[1], seed[2], seed[3], seed[4]}};
+    k->stride_jump = mrg_jump_mid((uint64_t)b * threads_per_block);
+    k->log_n = (int)log_n;
+    k->start = start;
+    k->count = count;
+    g5_scramble_keys(seed, &k->val0, &k->val1);
+    return G5_OK;
 }
 
 }  // namespace g5
@@ -180,35 +191,15 @@ extern "C" int g5_scramble_keys(const uint32_t seed[5], uint64_t *val0, uint64_t
 extern "C" int g5_generate_kronecker_range(const uint32_t seed[5], uint32_t log_n, int64_t start_edge,
                                            int64_t end_edge, uint64_t *d_edges, float *d_weights, void *stream) {
     clear_error();
-    G5_CHECK_ARG(seed, "g5_generate_kronecker_range: seed is NULL");
-    G5_CHECK_ARG(log_n >= 1 && log_n <= 62, "g5_generate_kronecker_range: log_n %u outside [1, 62]", log_n);
-    G5_CHECK_ARG(start_edge >= 0, "g5_generate_kronecker_range: negative start edge");
-    for (int i = 0; i < 5; ++i)
-        G5_CHECK_ARG(seed[i] < MRG_P, "g5_generate_kronecker_range: seed word %d not below 2^31-1", i);
-    G5_CHECK_ARG(seed[0] | seed[1] | seed[2] | seed[3] | seed[4], "g5_generate_kronecker_range: all-zero seed");
+    KronLaunch k;
+    int blocks = 0;
+    int rc = kron_prepare(seed, log_n, start_edge, end_edge < start_edge ? start_edge : end_edge, 256, &k, &blocks,
+                          "g5_generate_kronecker_range");
+    if (rc) return rc;
     if (end_edge <= start_edge) return G5_OK;
     G5_CHECK_ARG(d_edges && d_weights, "g5_generate_kronecker_range: NULL output");
     G5_CHECK_ARG(((uintptr_t)d_edges & 15) == 0, "g5_generate_kronecker_range: edges not 16-byte aligned");
-
-    const int64_t count = end_edge - start_edge;
-    DeviceInfo di;
-    int rc = device_info(&di);
-    if (rc) return rc;
-    const MrgMatrix *table = nullptr;
-    if ((rc = mrg_device_mid_table(&table))) return rc;
-
-    const int threads = 256;
-    int64_t blocks = (count + threads - 1) / threads;
-    const int64_t cap = (int64_t)di.sms * (di.max_threads_per_sm / threads);
-    if (blocks > cap) blocks = cap;
-    const uint64_t T = (uint64_t)blocks * threads;
-
-    uint64_t val0, val1;
-    g5_scramble_keys(seed, &val0, &val1);
-    MrgState base{{seed[0], seed[1], seed[2], seed[3], seed[4]}};
-    MrgMatrix jump = mrg_jump_mid(T);
-    kron_generate_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
-        base, jump, (int)log_n, start_edge, count, val0, val1, table, (ulonglong2 *)d_edges, d_weights);
+    kron_generate_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(k, (ulonglong2 *)d_edges, d_weights);
     G5_CUDA_TRY(cudaGetLastError());
     return G5_OK;
 }

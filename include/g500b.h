@@ -86,6 +86,17 @@ int g5_csr_fill(const uint64_t *d_edges, const float *d_weights, uint64_t nedges
                 const uint64_t *d_rowstarts, float light_delta, void *d_work, uint64_t work_bytes,
                 int32_t *d_col, float *d_w, uint64_t *d_col64, uint32_t *d_light_deg, void *stream);
 
+/* The CSR of the Kronecker graph with edges [0, nedges) of seed `seed` on
+ * 2^log_n vertices, without an edge list: both passes regenerate every edge
+ * in registers (the generator fused into the build; 20 bytes per edge
+ * neither written nor read twice).  Same results and workspace as
+ * g5_csr_count + g5_csr_fill over g5_generate_kronecker_range's output. */
+int g5_csr_count_kronecker(const uint32_t seed[5], uint32_t log_n, uint64_t nedges, uint64_t *d_rowstarts,
+                           void *d_work, uint64_t work_bytes, uint64_t *nentries, void *stream);
+int g5_csr_fill_kronecker(const uint32_t seed[5], uint32_t log_n, uint64_t nedges, const uint64_t *d_rowstarts,
+                          float light_delta, void *d_work, uint64_t work_bytes, int32_t *d_col, float *d_w,
+                          uint64_t *d_col64, uint32_t *d_light_deg, void *stream);
+
 /* ----------------------------------------------------------------- BFS --- */
 
 typedef struct g5_bfs_params {

@@ -332,3 +332,19 @@ def test_bfs_query_path_and_small_components(cgt, oracle, graphs):
         assert st.reached == int((od != -1).sum())
         if not h.in_main_component(r):
             assert st.solo_levels == st.levels  # the whole search ran on one block
+
+
+def test_fused_generator_csr_matches(cgt, graphs, golden_dump):
+    """The generator fused into the CSR passes (no edge list) builds the
+    reference's CSR: same rowstarts and canonical rows as the fixtures."""
+    scale = golden_dump["scale"]
+    g = cgt.oned_graph_from_kronecker(cgt.make_mrg_seed(2, 3), scale, 16 << scale, with_column64=True)
+    d = graphs[scale]
+    h = golden_hashes(_np(d["tg"].edges).view(np.uint64), _np(d["tg"].weights),
+                      _np(g.rowstarts).view(np.uint64), _np(g.col), _np(g.w))
+    assert h["rowstarts_sha256"] == golden_dump["rowstarts_sha256"]
+    assert h["csr_canonical_sha256"] == golden_dump["csr_canonical_sha256"]
+    assert np.array_equal(_np(g.column), _np(g.col).astype(np.int64))
+    ref = d["g"]
+    assert np.array_equal(_np(g.light_deg), _np(ref.light_deg))
+    assert np.array_equal(g.main_bits, ref.main_bits)
