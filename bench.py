@@ -342,10 +342,176 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if world == 1 and not (args.no_batched and args.no_packed):
+            del g, bfs, vw, sssp  # the SCALE-26 graph is not needed any more
+            torch.cuda.empty_cache()
+        if world == 1 and not args.no_batched:
+            line["batched"] = run_batched(G, dev, args.batched_scale, args.edgefactor, args.batched_roots)
+            torch.cuda.empty_cache()
+        if world == 1 and not args.no_packed:
+            line["packed"] = run_packed(G, dev, args.packed_graphs, args.packed_min_scale, args.packed_max_scale,
+                                        args.edgefactor)
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def run_batched(G, dev, scale, ef, nroots, reps=3):
+    """Batched BFS: `nroots` Graph500 roots (the runner's root choice) in
+    one g5_msbfs search on the SCALE-`scale` Kronecker graph, against the
+    same roots searched one by one with the single-root BFS.  Aggregate
+    GTEPS = sum of the roots' TEPS edge counts / device time.  The batch's
+    depth arrays are compared with the single searches' for every 16th root."""
+    import torch
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    t0 = time.time()
+    g = G.oned_graph_from_kronecker(G.make_mrg_seed(2, 3), scale, ef << scale, device=dev)
+    roots = G.generate_bfs_roots(g, 2, 3, nroots)
+    a, b = ev(), ev()
+    a.record()
+    ms = G.MsBfsState(g)
+    b.record()
+    torch.cuda.synchronize()
+    prep_ms = a.elapsed_time(b)
+    depth8 = torch.empty((len(roots), g.nglobalverts), dtype=torch.uint8, device=dev)
+    G.msbfs_run(g, ms, roots)  # warm-up
+    search_ms, full_ms = [], []
+    for _ in range(reps):
+        a, b, c = ev(), ev(), ev()
+        a.record()
+        G.msbfs_run(g, ms, roots, sync=False)
+        b.record()
+        G.msbfs_depths_u8(ms, depth8)
+        c.record()
+        torch.cuda.synchronize()
+        search_ms.append(a.elapsed_time(b))
+        full_ms.append(a.elapsed_time(c))
+    st = G.msbfs_stats(ms)
+    trace = G.msbfs_trace(ms)
+    # The same roots one at a time (reset untimed, as the runner's clear).
+    bfs = G.BfsState(g)
+    vw = G._val_work(g)
+    plain_ms, nedge, checked = 0.0, [], 0
+    for i, r in enumerate(roots):
+        G.oned_graph_bfs_reset(bfs, True, g)
+        a, b = ev(), ev()
+        a.record()
+        G.oned_graph_bfs_traverse(g, bfs, r, None, True)
+        b.record()
+        torch.cuda.synchronize()
+        plain_ms += a.elapsed_time(b)
+        nedge.append(G.edge_count(g, bfs.pred, vw))
+        if i % 16 == 0:
+            want = bfs.depth.to(torch.int64)
+            got = depth8[i].to(torch.int64)
+            got[got == 255] = -1
+            assert torch.equal(want, got), f"batched depth of root {r} differs from the single search"
+            checked += 1
+    E = float(sum(nedge))
+    best, best_full = min(search_ms), min(full_ms)
+    return {"workload": f"multi-source bfs scale{scale} ef{ef}, {len(roots)} roots in one search",
+            "value": round(E / best / 1e6, 1), "unit": "GTEPS (aggregate over the batch)",
+            "ms_per_batch": round(best, 3), "ms_per_batch_with_depth_export": round(best_full, 3),
+            "plain_ms_total": round(plain_ms, 3), "plain_gteps": round(E / plain_ms / 1e6, 1),
+            "speedup_vs_plain": round(plain_ms / best, 2),
+            "speedup_vs_plain_with_export": round(plain_ms / best_full, 2),
+            "depth_arrays_checked_identical": checked, "levels": st.levels, "pull_levels": st.pull_levels,
+            "level_ms": [round(x, 3) for x in trace["ms"]], "level_mode": trace["mode"],
+            "prepare_ms": round(prep_ms, 2), "setup_s": round(time.time() - t0, 2),
+            "timing": "device events, min of 3 after one warm-up; plain = single-root traverse with depth, "
+                      "reset untimed"}
+
+
+def run_packed(G, dev, ngraphs, smin, smax, ef, reps=3):
+    """Many small graphs: `ngraphs` Kronecker graphs with SCALE drawn
+    uniformly from [smin, smax] (seeded), one BFS and one SSSP root each (the
+    graph's first Graph500 root), packed into one CSR and run as one CUDA
+    graph (reset, multi-root BFS, reset, multi-source SSSP).  Baseline: the
+    same graphs one at a time, each a plain g5_bfs_run + g5_sssp_run on its
+    own CSR.  Aggregate GTEPS = sum of the graphs' TEPS edge counts / time."""
+    import torch
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    rng = np.random.default_rng(2024)
+    scales = rng.integers(smin, smax + 1, size=ngraphs).tolist()
+    t0 = time.time()
+    pk = G.pack_kronecker(scales, edgefactor=ef, seed1_base=100, seed2=3, device=dev)
+    batch = G.PackedBatch(pk, delta=0.1, capture=True)
+    build_s = time.time() - t0
+    bfs_ms, all_ms = [], []
+    for _ in range(reps):
+        a, b, c = ev(), ev(), ev()
+        a.record(batch.stream)
+        batch.run()
+        c.record(batch.stream)
+        torch.cuda.synchronize()
+        all_ms.append(a.elapsed_time(c))
+    batch.check()
+    # BFS alone (eager, same stream), for the BFS share.
+    for _ in range(reps):
+        a, b = ev(), ev()
+        with torch.cuda.stream(batch.stream):
+            G.oned_graph_bfs_reset(batch.bfs, True, pk.g)
+            a.record(batch.stream)
+            G.oned_graph_bfs_traverse_multi(pk.g, batch.bfs, pk.d_roots)
+            b.record(batch.stream)
+        torch.cuda.synchronize()
+        bfs_ms.append(a.elapsed_time(b))
+    vw = G._val_work(pk.g)
+    nedge = G.edge_count(pk.g, batch.bfs.pred, vw)  # sum of every graph's TEPS edge count
+    depth = batch.bfs.depth.cpu().numpy()
+    dist = batch.sssp.dist.cpu().numpy()
+    del batch, vw
+    torch.cuda.empty_cache()
+    # One at a time: each graph rebuilt on its own, plain BFS + SSSP timed.
+    plain_bfs, plain_sssp, checked = 0.0, 0.0, 0
+    for i, s in enumerate(scales):
+        g = G.oned_graph_from_kronecker(G.make_mrg_seed(100 + i, 3), s, ef << s, device=dev, with_main=False)
+        r = int(pk.local_roots[i])
+        bfs, ss = G.BfsState(g), G.SsspState(g)
+        a, b, c = ev(), ev(), ev()
+        a.record()
+        G.oned_graph_bfs_run(g, bfs, r)
+        b.record()
+        G.oned_graph_sssp_run(g, ss, r)
+        c.record()
+        torch.cuda.synchronize()
+        plain_bfs += a.elapsed_time(b)
+        plain_sssp += b.elapsed_time(c)
+        if i % 50 == 0:
+            sl = pk.graph_slice(i)
+            assert np.array_equal(depth[sl], bfs.depth.cpu().numpy()), f"packed BFS of graph {i} differs"
+            assert np.array_equal(dist[sl].view(np.uint32), ss.dist.cpu().numpy().view(np.uint32)), \
+                f"packed SSSP of graph {i} differs"
+            checked += 1
+    best, best_bfs = min(all_ms), min(bfs_ms)
+    return {"workload": f"{ngraphs} Kronecker graphs, SCALE uniform in [{smin}, {smax}], ef{ef}, "
+                        "one BFS + one SSSP root each, packed into one CSR, one CUDA graph per batch",
+            "vertices": int(pk.g.nglobalverts), "csr_entries": int(pk.g.nlocaledges),
+            "ms_per_batch": round(best, 3), "bfs_ms": round(best_bfs, 3),
+            "bfs_gteps": round(nedge / best_bfs / 1e6, 2),
+            "bfs_plus_sssp_gteps": round(2 * nedge / best / 1e6, 2),
+            "plain_ms_total": round(plain_bfs + plain_sssp, 2), "plain_bfs_ms": round(plain_bfs, 2),
+            "plain_sssp_ms": round(plain_sssp, 2),
+            "speedup_vs_plain": round((plain_bfs + plain_sssp) / best, 2),
+            "bfs_speedup_vs_plain": round(plain_bfs / best_bfs, 2),
+            "graphs_checked_identical": checked, "build_s": round(build_s, 2),
+            "timing": "device events; batch = replay of the captured CUDA graph (BFS+SSSP resets included), "
+                      "min of 3 after a warm-up; plain = per-graph g5_bfs_run + g5_sssp_run, resets included"}
+
+
+def run_batched_only(args):
+    import torch
+    torch.cuda.set_device(0)
+    G = load_package()
+    dev = torch.device("cuda", 0)
+    out = {}
+    if args.only_batched in ("msbfs", "all"):
+        out["batched"] = run_batched(G, dev, args.batched_scale, args.edgefactor, args.batched_roots)
+    if args.only_batched in ("packed", "all"):
+        out["packed"] = run_packed(G, dev, args.packed_graphs, args.packed_min_scale, args.packed_max_scale,
+                                   args.edgefactor)
+    print(json.dumps(out), flush=True)
 
 
 def cpu_baseline_sample(g, roots, nedge):
@@ -435,6 +601,15 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-roots", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched-scale", type=int, default=24, help="SCALE of the batched (multi-source) BFS graph")
+    ap.add_argument("--batched-roots", type=int, default=256)
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched BFS measurement")
+    ap.add_argument("--only-batched", nargs="?", const="msbfs", choices=["msbfs", "packed", "all"],
+                    help="run only the batched measurements (multi-source BFS, packed graphs or both)")
+    ap.add_argument("--packed-graphs", type=int, default=2000)
+    ap.add_argument("--packed-min-scale", type=int, default=10)
+    ap.add_argument("--packed-max-scale", type=int, default=18)
+    ap.add_argument("--no-packed", action="store_true", help="skip the packed many-graph measurement")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per BFS launch (read+write) to report beside the roofline")
     args = ap.parse_args()
@@ -442,6 +617,8 @@ def main():
         ap.error("steps and warmup must be positive")
     if args.impl == "reference":
         run_reference(args)
+    elif args.only_batched:
+        run_batched_only(args)
     else:
         run_ours(args)
 

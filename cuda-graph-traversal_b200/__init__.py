@@ -52,6 +52,9 @@ def _load() -> C.CDLL:
         "g5_csr_fill": ([p, p, u64, u64, p, f32, p, u64, p, p, p, p, p], C.c_int),
         "g5_csr_count_kronecker": ([p, u32, u64, p, p, u64, p, p], C.c_int),
         "g5_csr_fill_kronecker": ([p, u32, u64, p, f32, p, u64, p, p, p, p, p], C.c_int),
+        "g5_csr_pack_append": ([p, p, p, p, u64, u64, u64, u64, p, p, p, p, p], C.c_int),
+        "g5_bfs_traverse_multi": ([p, p, u64, p, u32, p, p, p, u64, p, p], C.c_int),
+        "g5_sssp_traverse_multi": ([p, p, p, p, f32, u64, p, u32, p, p, p, u64, p, p], C.c_int),
         "g5_bfs_workspace_size": ([u64, p], C.c_int),
         "g5_bfs_run": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_bfs_reset": ([u64, p, p, p, p, u64, p], C.c_int),
@@ -73,6 +76,13 @@ def _load() -> C.CDLL:
         "g5_bfs_validate": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_sssp_validate": ([p, p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_selftest_wait_timeout": ([u32, p, u64, p], C.c_int),
+        "g5_msbfs_workspace_size": ([u64, u64, C.c_int, p], C.c_int),
+        "g5_msbfs_prepare": ([p, p, u64, u64, C.c_int, p, u64, p], C.c_int),
+        "g5_msbfs_run": ([u64, u64, C.c_int, p, u32, p, u64, p, p, p], C.c_int),
+        "g5_msbfs_depths_u8": ([p, u64, u64, u64, C.c_int, u32, p, p], C.c_int),
+        "g5_msbfs_depth": ([p, u64, u64, u64, C.c_int, u32, p, p], C.c_int),
+        "g5_msbfs_last_stats": ([p, u64, p, p], C.c_int),
+        "g5_msbfs_last_trace": ([p, u64, C.c_int, p, p, p, p, p, p], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -97,6 +107,15 @@ class BfsParams(C.Structure):
 class BfsStats(C.Structure):
     _fields_ = [("levels", C.c_int32), ("bottom_up_levels", C.c_int32), ("reached", C.c_uint64),
                 ("error_flags", C.c_uint32), ("solo_levels", C.c_int32)]
+
+
+class MsBfsParams(C.Structure):
+    _fields_ = [("alpha", C.c_float), ("mode", C.c_int32), ("check_frontier", C.c_int32), ("blocks", C.c_int32)]
+
+
+class MsBfsStats(C.Structure):
+    _fields_ = [("levels", C.c_int32), ("pull_levels", C.c_int32), ("error_flags", C.c_uint32),
+                ("nroots", C.c_uint32), ("pairs_reached", C.c_uint64), ("frontier_edges", C.c_uint64)]
 
 
 class SsspParams(C.Structure):
@@ -239,9 +258,10 @@ def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: 
 
 
 def oned_graph_from_kronecker(seed, log_n: int, nedges: int, device="cuda", light_delta: float = 0.1,
-                              with_column64: bool = False, stream=None) -> OnedGraph:
+                              with_column64: bool = False, stream=None, with_main: bool = True) -> OnedGraph:
     """generate_kronecker_range + oned_graph_from_tuple_graph in one step,
-    with the generator fused into the CSR passes (no edge list in memory)."""
+    with the generator fused into the CSR passes (no edge list in memory).
+    with_main=False skips the main-component search (g.main_bits = None)."""
     n = 1 << log_n
     s = (C.c_uint32 * 5)(*seed)
     nb = C.c_uint64()
@@ -261,8 +281,159 @@ def oned_graph_from_kronecker(seed, log_n: int, nedges: int, device="cuda", ligh
     iso = torch.empty((n + 31) // 32, dtype=torch.int32, device=device)
     _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), n, _ptr(iso), st))
     g = OnedGraph(n, e, rowstarts, col[:e], w[:e], light, light_delta, None if col64 is None else col64[:e], iso)
-    g.main_bits = main_component_bitmap(g, stream)
+    if with_main:
+        g.main_bits = main_component_bitmap(g, stream)
     return g
+
+
+# ------------------------------------------------------- packed graphs ----
+
+class PackedGraphs:
+    """Disjoint graphs packed into one CSR (g5_csr_pack_append): graph i
+    owns vertices [vbase[i], vbase[i] + nverts[i]) and the entries of their
+    rows; `g` is the union as an OnedGraph.  One root per graph then makes a
+    single g5_bfs_traverse_multi / g5_sssp_traverse_multi launch compute
+    every graph's own BFS / SSSP (no counterpart in the reference, which
+    holds one graph)."""
+
+    def __init__(self, nverts, vbase, g: OnedGraph, roots):
+        self.nverts = np.asarray(nverts, np.int64)
+        self.vbase = np.asarray(vbase, np.int64)
+        self.g = g
+        self.local_roots = np.asarray(roots, np.int64)
+        self.roots = self.vbase + self.local_roots
+        self.d_roots = torch.as_tensor(self.roots, dtype=torch.int64, device=g.device)
+
+    @property
+    def ngraphs(self) -> int:
+        return len(self.vbase)
+
+    def graph_slice(self, i: int) -> slice:
+        return slice(int(self.vbase[i]), int(self.vbase[i] + self.nverts[i]))
+
+
+def pack_graphs(graphs, roots, device="cuda", stream=None) -> PackedGraphs:
+    """Packs the OnedGraphs in `graphs`; roots[i] is graph i's root (its own
+    vertex number).  pack_kronecker builds and packs generated graphs one
+    at a time instead, without holding them all unpacked."""
+    graphs = list(graphs)
+    sizes = [(g.nglobalverts, g.nlocaledges) for g in graphs]
+    return _pack(sizes, iter(graphs), roots, device, graphs[0].light_delta if graphs else 0.1, stream)
+
+
+def pack_kronecker(scales, edgefactor: int = 16, seed1_base: int = 2, seed2: int = 3, device="cuda",
+                   light_delta: float = 0.1, stream=None) -> PackedGraphs:
+    """Generates Kronecker graph i (SCALE scales[i], seeds (seed1_base + i,
+    seed2)) with the fused generator -> CSR path and packs it at once; each
+    graph's root is its first Graph500 root (the runner's choice)."""
+    scales = [int(x) for x in scales]
+    # Entries are at most 2 per edge (self-loops store one): size for that.
+    sizes = [(1 << s, 2 * edgefactor << s) for s in scales]
+    roots: list[int] = []
+
+    def gen():
+        for i, s in enumerate(scales):
+            g = oned_graph_from_kronecker(make_mrg_seed(seed1_base + i, seed2), s, edgefactor << s, device=device,
+                                          light_delta=light_delta, stream=stream, with_main=False)
+            r = generate_bfs_roots(g, 2, 3, 1)
+            roots.append(r[0] if r else 0)
+            yield g
+
+    return _pack(sizes, gen(), roots, device, light_delta, stream)
+
+
+def _pack(sizes, graphs, roots, device, light_delta, stream) -> PackedGraphs:
+    N = sum(n for n, _ in sizes)
+    Emax = sum(e for _, e in sizes)
+    if N > (1 << 31):
+        raise ValueError(f"pack: {N} vertices exceed 2^31")
+    rowstarts = torch.empty(N + 1, dtype=torch.int64, device=device)
+    col = torch.empty(max(Emax, 1), dtype=torch.int32, device=device)
+    w = torch.empty(max(Emax, 1), dtype=torch.float32, device=device)
+    light = torch.empty(max(N, 1), dtype=torch.int32, device=device)
+    st = _stream(stream)
+    vb, eb = 0, 0
+    nverts, vbase = [], []
+    for g in graphs:
+        _check(lib.g5_csr_pack_append(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.nglobalverts,
+                                      g.nlocaledges, vb, eb, _ptr(rowstarts), _ptr(col), _ptr(w), _ptr(light), st))
+        nverts.append(g.nglobalverts)
+        vbase.append(vb)
+        vb += g.nglobalverts
+        eb += g.nlocaledges
+        del g
+    if vb == 0:
+        raise ValueError("pack: no graphs")
+    iso = torch.empty((vb + 31) // 32, dtype=torch.int32, device=device)
+    _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), vb, _ptr(iso), st))
+    u = OnedGraph(vb, eb, rowstarts[:vb + 1], col[:eb], w[:eb], light[:vb], light_delta, None, iso)
+    return PackedGraphs(nverts, vbase, u, list(roots))
+
+
+def oned_graph_bfs_traverse_multi(g: OnedGraph, bfs: "BfsState", d_roots: torch.Tensor, params=None,
+                                  with_depth: bool = True, stream=None) -> None:
+    """BFS from every root in d_roots (device int64) at once
+    (g5_bfs_traverse_multi); reset bfs first."""
+    _check(lib.g5_bfs_traverse_multi(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, _ptr(d_roots), d_roots.numel(),
+                                     _ptr(bfs.pred), _ptr(bfs.depth) if with_depth else None, _ptr(bfs.work),
+                                     bfs.work.numel(), C.byref(params) if params is not None else None,
+                                     _stream(stream)))
+
+
+def oned_graph_sssp_traverse_multi(g: OnedGraph, sssp: "SsspState", d_roots: torch.Tensor, delta: float = 0.1,
+                                   blocks: int = 0, stream=None) -> None:
+    """SSSP from every source in d_roots at once (g5_sssp_traverse_multi);
+    reset sssp first."""
+    p = SsspParams(delta, blocks)
+    _check(lib.g5_sssp_traverse_multi(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
+                                      g.nglobalverts, _ptr(d_roots), d_roots.numel(), _ptr(sssp.dist),
+                                      _ptr(sssp.pred), _ptr(sssp.work), sssp.work.numel(), C.byref(p),
+                                      _stream(stream)))
+
+
+class PackedBatch:
+    """One BFS and one SSSP from every packed graph's root: reset, the
+    multi-root BFS, reset, the multi-source SSSP -- four library calls on one
+    stream, captured once into a CUDA graph and replayed per batch (no
+    per-graph launches, no host work between them)."""
+
+    def __init__(self, pk: PackedGraphs, delta: float = 0.1, capture: bool = True, with_depth: bool = True):
+        self.pk, self.delta, self.with_depth = pk, delta, with_depth
+        self.bfs = BfsState(pk.g)
+        self.sssp = SsspState(pk.g)
+        self.stream = torch.cuda.Stream(device=pk.g.device)
+        self.graph = None
+        # One eager batch first: the library's once-per-device setup (L2
+        # window, occupancy queries) must not happen inside the capture.
+        self.run()
+        self.stream.synchronize()
+        if capture:
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph, stream=self.stream):
+                self._enqueue_bfs()
+                self._enqueue_sssp()
+
+    def _enqueue_bfs(self):
+        oned_graph_bfs_reset(self.bfs, self.with_depth, self.pk.g)
+        oned_graph_bfs_traverse_multi(self.pk.g, self.bfs, self.pk.d_roots, with_depth=self.with_depth)
+
+    def _enqueue_sssp(self):
+        oned_graph_sssp_reset(self.sssp)
+        oned_graph_sssp_traverse_multi(self.pk.g, self.sssp, self.pk.d_roots, self.delta)
+
+    def run(self) -> None:
+        """Enqueues one batch on self.stream (replaying the graph when captured)."""
+        with torch.cuda.stream(self.stream):
+            if self.graph is not None:
+                self.graph.replay()
+            else:
+                self._enqueue_bfs()
+                self._enqueue_sssp()
+
+    def check(self) -> None:
+        """Raises if either search of the last batch reported a device error."""
+        bfs_stats(self.bfs, self.stream)
+        sssp_status(self.sssp, self.stream)
 
 
 def main_component_bitmap(g: OnedGraph, stream=None) -> np.ndarray:
@@ -430,6 +601,87 @@ def bfs_compute_dist_from_pred(g: OnedGraph, bfs: BfsState, root: int, stream=No
     _check(lib.g5_bfs_dist_from_pred(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, _ptr(bfs.pred), root,
                                      _ptr(bfs.dist), _ptr(bfs.val_work), bfs.val_work.numel(), _stream(stream)))
     return bfs.dist
+
+
+# --------------------------------------------------------- batched BFS ----
+
+MSBFS_MAX_ROOTS = 256
+
+
+class MsBfsState:
+    """Workspace of the batched BFS (g5_msbfs_*) bound to one graph: up to
+    256 roots per search, one bit each.  No counterpart in the reference,
+    which runs oned_graph_bfs_run once per root (src/traversal.h:47)."""
+
+    def __init__(self, g: OnedGraph, depth_bits: int = 0, stream=None):
+        self.n = g.nglobalverts
+        self.nentries = g.nlocaledges
+        self.depth_bits = depth_bits
+        nb = C.c_uint64()
+        _check(lib.g5_msbfs_workspace_size(self.n, self.nentries, depth_bits, C.byref(nb)))
+        self.work = _workspace(nb.value, g.device)
+        self.nroots = 0
+        self.h_roots = torch.zeros(MSBFS_MAX_ROOTS, dtype=torch.int64).pin_memory()
+        _check(lib.g5_msbfs_prepare(_ptr(g.rowstarts), _ptr(g.col), self.n, self.nentries, depth_bits,
+                                    _ptr(self.work), self.work.numel(), _stream(stream)))
+
+
+def msbfs_run(g: OnedGraph, ms: MsBfsState, roots, params: MsBfsParams | None = None, sync: bool = True,
+              stream=None) -> MsBfsStats | None:
+    """Searches from every root in `roots` (1..256 vertex ids) at once on
+    the graph `ms` was prepared for (its own copy of g).  With sync, waits
+    and returns the statistics (raising on a failed search); otherwise only
+    enqueues."""
+    roots = [int(r) for r in roots]
+    if not 1 <= len(roots) <= MSBFS_MAX_ROOTS:
+        raise ValueError(f"msbfs_run: {len(roots)} roots, expected 1..{MSBFS_MAX_ROOTS}")
+    ms.h_roots[:len(roots)] = torch.tensor(roots, dtype=torch.int64)
+    ms.nroots = len(roots)
+    st = MsBfsStats() if sync else None
+    _check(lib.g5_msbfs_run(ms.n, ms.nentries, ms.depth_bits, ms.h_roots.data_ptr(), len(roots),
+                            _ptr(ms.work), ms.work.numel(),
+                            C.byref(params) if params is not None else None,
+                            C.byref(st) if st is not None else None, _stream(stream)))
+    return st
+
+
+def msbfs_depths_u8(ms: MsBfsState, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """Depths of the last search, uint8[nroots, N] (255 = not reached)."""
+    if out is None:
+        out = torch.empty((ms.nroots, ms.n), dtype=torch.uint8, device=ms.work.device)
+    _check(lib.g5_msbfs_depths_u8(_ptr(ms.work), ms.work.numel(), ms.n, ms.nentries, ms.depth_bits, ms.nroots,
+                                  _ptr(out), _stream(stream)))
+    return out
+
+
+def msbfs_depth(ms: MsBfsState, root_index: int, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """Root `root_index`'s depth array, int32[N] with -1 where unreached (the
+    layout of BfsState.depth)."""
+    if out is None:
+        out = torch.empty(ms.n, dtype=torch.int32, device=ms.work.device)
+    _check(lib.g5_msbfs_depth(_ptr(ms.work), ms.work.numel(), ms.n, ms.nentries, ms.depth_bits, root_index,
+                              _ptr(out), _stream(stream)))
+    return out
+
+
+def msbfs_stats(ms: MsBfsState, stream=None) -> MsBfsStats:
+    s = MsBfsStats()
+    _check(lib.g5_msbfs_last_stats(_ptr(ms.work), ms.work.numel(), C.byref(s), _stream(stream)))
+    return s
+
+
+def msbfs_trace(ms: MsBfsState, stream=None) -> dict:
+    k = 64
+    mode = np.zeros(k, np.int32)
+    nv = np.zeros(k, np.uint64)
+    ne = np.zeros(k, np.uint64)
+    tm = np.zeros(k, np.float64)
+    nl = C.c_int32()
+    _check(lib.g5_msbfs_last_trace(_ptr(ms.work), ms.work.numel(), k, mode.ctypes.data, nv.ctypes.data,
+                                   ne.ctypes.data, tm.ctypes.data, C.byref(nl), _stream(stream)))
+    n = min(nl.value, k)
+    return {"levels": nl.value, "mode": mode[:n].tolist(), "frontier": nv[:n].tolist(),
+            "frontier_edges": ne[:n].tolist(), "ms": tm[:n].tolist()}
 
 
 # ---------------------------------------------------------------- SSSP ----

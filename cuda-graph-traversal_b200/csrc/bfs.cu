@@ -97,6 +97,8 @@ struct BfsArgs {
     unsigned long long limit_ns;
     bool root_from_ctl;  // take the root from ctl->root_in (copied in by the caller's stream)
     unsigned long long seq;  // unique per launch: releases only this launch's waiting blocks
+    const uint64_t *roots;   // several roots at once (device array) instead of `root`, or nullptr
+    unsigned nroots;
 };
 
 enum { TOP_DOWN = 0, BOTTOM_UP = 1 };
@@ -360,8 +362,6 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
     // single grid barrier.
     if (blockIdx.x == 0) {
         const uint64_t E = __ldg(&a.rowptr[a.n]);
-        const unsigned root = a.root_from_ctl ? (unsigned)ld_volatile(&c->root_in) : a.root;
-        const uint64_t root_deg = __ldg(&a.rowptr[root + 1]) - __ldg(&a.rowptr[root]);
         if (threadIdx.x == 0) {
             // Fresh control state for this launch.  The other blocks read
             // none of it before block 0 releases them below, and they wait
@@ -374,19 +374,66 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
                 c->n_small[k] = c->grab[k] = c->cgrab[k] = c->found[k] = 0;
                 c->big[k] = c->m_next[k] = 0;
             }
-            a.visited[root >> 5] |= 1u << (root & 31);
-            a.pred[root] = root;
-            if (a.depth) a.depth[root] = 0;
-            if (root_deg > BIG_DEG) {
-                a.q[0][a.n - 1] = root;
-                a.base[0][0] = 0;
-                c->big[0] = (1ull << BIG_SHIFT) | ((root_deg + BIG_CHUNK - 1) / BIG_CHUNK);
-            } else {
-                a.q[0][0] = root;
-                c->n_small[0] = 1;
-            }
         }
-        st = LevelState{0, TOP_DOWN, 0, PEND_NONE, 0, 0, 1u, 0u, root_deg, E - root_deg, 1ull};
+        if (!a.roots) {
+            const unsigned root = a.root_from_ctl ? (unsigned)ld_volatile(&c->root_in) : a.root;
+            const uint64_t root_deg = __ldg(&a.rowptr[root + 1]) - __ldg(&a.rowptr[root]);
+            if (threadIdx.x == 0) {
+                a.visited[root >> 5] |= 1u << (root & 31);
+                a.pred[root] = root;
+                if (a.depth) a.depth[root] = 0;
+                if (root_deg > BIG_DEG) {
+                    a.q[0][a.n - 1] = root;
+                    a.base[0][0] = 0;
+                    c->big[0] = (1ull << BIG_SHIFT) | ((root_deg + BIG_CHUNK - 1) / BIG_CHUNK);
+                } else {
+                    a.q[0][0] = root;
+                    c->n_small[0] = 1;
+                }
+            }
+            st = LevelState{0, TOP_DOWN, 0, PEND_NONE, 0, 0, 1u, 0u, root_deg, E - root_deg, 1ull};
+        } else {
+            // Several roots (disjoint graphs packed into one CSR, one root
+            // each): level 0 is all of them.  A root is claimed through its
+            // parent entry, so a repeated root is queued once.
+            __shared__ unsigned long long s_m;
+            __shared__ unsigned s_n;
+            if (threadIdx.x == 0) s_m = 0, s_n = 0;
+            __syncthreads();
+            unsigned long long my_m = 0;
+            unsigned my_n = 0;
+            for (unsigned b0 = 0; b0 < a.nroots; b0 += blockDim.x) {
+                const unsigned i = b0 + threadIdx.x;
+                bool mine = false;
+                unsigned r = 0;
+                uint64_t deg = 0;
+                if (i < a.nroots) {
+                    const uint64_t rr = __ldg(&a.roots[i]);
+                    if (rr >= a.n) {
+                        atomicOr(&c->res.error_flags, DEVERR_RANGE);
+                    } else if (atomicCAS((unsigned long long *)&a.pred[rr], ~0ull, (unsigned long long)rr) == ~0ull) {
+                        mine = true;
+                        r = (unsigned)rr;
+                        atomicOr(&a.visited[r >> 5], 1u << (r & 31));
+                        if (a.depth) a.depth[r] = 0;
+                        deg = __ldg(&a.rowptr[r + 1]) - __ldg(&a.rowptr[r]);
+                        my_m += deg;
+                        ++my_n;
+                    }
+                }
+                if (!frontier_append_staged(bq, a.q[0], a.base[0], a.n, &c->n_small[0], &c->big[0], mine, r, deg))
+                    atomicOr(&c->res.error_flags, DEVERR_CAPACITY);
+            }
+            if (!stage_flush_warp(bq, a.q[0], a.n, &c->n_small[0])) atomicOr(&c->res.error_flags, DEVERR_CAPACITY);
+            my_m = warp_sum(my_m);
+            my_n = warp_sum(my_n);
+            if (lane_id() == 0) {
+                atomicAdd(&s_m, my_m);
+                atomicAdd(&s_n, my_n);
+            }
+            __syncthreads();
+            st = LevelState{0, TOP_DOWN, 0, PEND_NONE, 0, 0, s_n, 0u, s_m, E - s_m, (unsigned long long)s_n};
+        }
         __syncthreads();
         bool done = false;
         int solo = 0;
@@ -631,7 +678,8 @@ extern "C" int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, 
 // the control block; the root comes from root_in when from_ctl).
 static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
                       uint64_t root, int64_t *d_pred, int32_t *d_depth, const g5_bfs_params *params,
-                      const uint64_t *h_root, cudaStream_t st) {
+                      const uint64_t *h_root, cudaStream_t st, const uint64_t *d_roots = nullptr,
+                      unsigned nroots = 0) {
     g5_bfs_params p = {14.0f, 24.0f, 0, 0};
     if (params) p = *params;
     G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= 2, "g5_bfs: bad params");
@@ -662,6 +710,8 @@ static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32
     a.nblocks = (unsigned)blocks;
     a.limit_ns = wait_limit_ns();
     a.root_from_ctl = h_root != nullptr;
+    a.roots = d_roots;
+    a.nroots = nroots;
     static std::atomic<unsigned long long> next_seq{1};
     a.seq = next_seq.fetch_add(1);
     if (h_root) G5_CUDA_TRY(cudaMemcpyAsync(&w.ctl->root_in, h_root, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
@@ -701,6 +751,18 @@ extern "C" int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col
     int rc = bfs_check(d_rowstarts, d_col, nverts, root, d_pred, d_work, work_bytes, &w, "g5_bfs_traverse");
     if (rc) return rc;
     return bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, params, nullptr, (cudaStream_t)stream);
+}
+
+extern "C" int g5_bfs_traverse_multi(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
+                                     const uint64_t *d_roots, uint32_t nroots, int64_t *d_pred, int32_t *d_depth,
+                                     void *d_work, uint64_t work_bytes, const g5_bfs_params *params, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(d_roots && nroots >= 1, "g5_bfs_traverse_multi: no roots");
+    BfsWork w;
+    int rc = bfs_check(d_rowstarts, d_col, nverts, 0, d_pred, d_work, work_bytes, &w, "g5_bfs_traverse_multi");
+    if (rc) return rc;
+    return bfs_launch(w, d_rowstarts, d_col, nverts, 0, d_pred, d_depth, params, nullptr, (cudaStream_t)stream,
+                      d_roots, nroots);
 }
 
 extern "C" int g5_bfs_query(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, const uint64_t *h_root,

@@ -45,6 +45,11 @@ int deverr_to_status(unsigned flags, const char *what) {
         return set_error(G5_ERR_TIMEOUT, "%s: a bounded grid barrier wait expired (flags 0x%x)", what, flags);
     if (flags & DEVERR_RANGE)
         return set_error(G5_ERR_INVALID, "%s: input value out of range (flags 0x%x)", what, flags);
+    if (flags & DEVERR_DEPTH)
+        return set_error(G5_ERR_INVALID, "%s: the graph is deeper than the depth planes hold; raise depth_bits "
+                         "(flags 0x%x)", what, flags);
+    if (flags & DEVERR_UNPREPARED)
+        return set_error(G5_ERR_INVALID, "%s: workspace not prepared for this graph (flags 0x%x)", what, flags);
     return set_error(G5_ERR_DEVICE, "%s: internal capacity exceeded (flags 0x%x)", what, flags);
 }
 

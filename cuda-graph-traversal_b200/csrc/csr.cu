@@ -22,6 +22,7 @@ namespace g5 {
 constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 16;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+static_assert(SCAN_TILE == 4096, "scan_scratch_words assumes 4096-item tiles");
 
 __global__ void csr_degree_kernel(const ulonglong2 *__restrict__ edges, uint64_t m, uint64_t n,
                                   unsigned *__restrict__ deg, unsigned *__restrict__ err) {
@@ -242,6 +243,27 @@ static CsrWork carve_csr(void *base, uint64_t n) {
     return w;
 }
 
+// One graph's CSR copied into a larger one at vertex offset vbase and
+// entry offset ebase (disjoint graphs packed into one CSR).
+__global__ void csr_pack_rows_kernel(const uint64_t *__restrict__ src_rs, uint64_t n, uint64_t vbase, uint64_t ebase,
+                                     const uint32_t *__restrict__ src_ld, uint64_t *__restrict__ dst_rs,
+                                     uint32_t *__restrict__ dst_ld) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += stride) {
+        dst_rs[vbase + i] = ebase + src_rs[i];
+        if (src_ld && i < n) dst_ld[vbase + i] = src_ld[i];
+    }
+}
+
+__global__ void csr_pack_entries_kernel(const int *__restrict__ src_col, const float *__restrict__ src_w, uint64_t m,
+                                        uint64_t vbase, int *__restrict__ dst_col, float *__restrict__ dst_w) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) {
+        dst_col[e] = (int)((uint64_t)src_col[e] + vbase);
+        if (src_w) dst_w[e] = src_w[e];
+    }
+}
+
 static int grid_for(uint64_t items, int threads) {
     DeviceInfo di;
     if (device_info(&di)) return 1;
@@ -359,5 +381,26 @@ extern "C" int g5_csr_fill_kronecker(const uint32_t seed[5], uint32_t log_n, uin
         kron_csr_kernel<true><<<blocks, 256, 0, st>>>(k, n, d_rowstarts, light_delta, lo, w.deg, d_col, d_w, d_col64);
         G5_CUDA_TRY(cudaGetLastError());
     }
+    return G5_OK;
+}
+
+extern "C" int g5_csr_pack_append(const uint64_t *d_src_rowstarts, const int32_t *d_src_col, const float *d_src_w,
+                                  const uint32_t *d_src_light_deg, uint64_t src_nverts, uint64_t src_nentries,
+                                  uint64_t vbase, uint64_t ebase, uint64_t *d_dst_rowstarts, int32_t *d_dst_col,
+                                  float *d_dst_w, uint32_t *d_dst_light_deg, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(d_src_rowstarts && d_dst_rowstarts && (src_nentries == 0 || (d_src_col && d_dst_col)),
+                 "g5_csr_pack_append: NULL argument");
+    G5_CHECK_ARG(!d_src_w == !d_dst_w && !d_src_light_deg == !d_dst_light_deg,
+                 "g5_csr_pack_append: weights / light counts given on one side only");
+    G5_CHECK_ARG(vbase + src_nverts <= (1ull << 31), "g5_csr_pack_append: packed graph above 2^31 vertices");
+    cudaStream_t st = (cudaStream_t)stream;
+    csr_pack_rows_kernel<<<grid_for(src_nverts + 1, 256), 256, 0, st>>>(d_src_rowstarts, src_nverts, vbase, ebase,
+                                                                         d_src_light_deg, d_dst_rowstarts,
+                                                                         d_dst_light_deg);
+    if (src_nentries)
+        csr_pack_entries_kernel<<<grid_for(src_nentries, 256), 256, 0, st>>>(
+            d_src_col, d_src_w, src_nentries, vbase, d_dst_col + ebase, d_dst_w ? d_dst_w + ebase : nullptr);
+    G5_CUDA_TRY(cudaGetLastError());
     return G5_OK;
 }

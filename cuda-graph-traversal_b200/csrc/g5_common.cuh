@@ -62,6 +62,8 @@ enum : unsigned {
     DEVERR_TIMEOUT = 1u,    // a bounded wait gave up
     DEVERR_RANGE = 2u,      // an input value outside its documented range
     DEVERR_CAPACITY = 4u,   // an internal list would have overflowed
+    DEVERR_DEPTH = 8u,      // a batched search went deeper than its depth planes hold
+    DEVERR_UNPREPARED = 16u, // a batched-search workspace was not prepared for this graph
 };
 int deverr_to_status(unsigned flags, const char *what);
 
@@ -70,6 +72,11 @@ int deverr_to_status(unsigned flags, const char *what);
 // reserving that much persisting L2 for this process's context once per
 // device.  G5_L2_PERSIST=0 disables it.
 int l2_persist_window(uint64_t want, uint64_t *bytes);
+
+// Exclusive scan (csr.cu): out[0..n] = prefix sums of in[0..n) widened to
+// u64, out[n] = total; `scratch` holds scan_scratch_words(n) u64.
+int scan_u32_to_u64(const unsigned *in, uint64_t n, uint64_t *out, uint64_t *scratch, cudaStream_t st);
+inline uint64_t scan_scratch_words(uint64_t n) { return (n + 4095) / 4096 + 1; }
 
 // Wait limit of the persistent kernels' grid barriers, nanoseconds
 // (G5_WAIT_LIMIT_MS overrides; default 2000 ms).

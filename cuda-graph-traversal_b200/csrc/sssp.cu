@@ -73,6 +73,8 @@ struct SsspArgs {
     const unsigned *ld;  // light degree per vertex (partitioned rows) or nullptr
     uint64_t n;
     unsigned root;
+    const uint64_t *roots;  // several sources at once (device array) instead of `root`, or nullptr
+    unsigned nroots;
     float delta;
     unsigned long long *pack;
     unsigned *fstamp, *sstamp, *qstamp;
@@ -320,11 +322,25 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
     const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
 
-    if (gtid == 0) {
-        a.pack[a.root] = (unsigned long long)a.root;  // distance 0.0f, parent = root
-        a.ring[0] = a.root;
-        a.qstamp[a.root] = 0;
-        c->ring_len[0] = 1;
+    if (!a.roots) {
+        if (gtid == 0) {
+            a.pack[a.root] = (unsigned long long)a.root;  // distance 0.0f, parent = root
+            a.ring[0] = a.root;
+            a.qstamp[a.root] = 0;
+            c->ring_len[0] = 1;
+        }
+    } else {
+        // Several sources (disjoint graphs packed into one CSR, one source
+        // each) all start in bucket 0; a repeated source is queued once.
+        for (uint64_t i = gtid; i < a.nroots; i += nthreads) {
+            const uint64_t r = __ldg(&a.roots[i]);
+            if (r >= a.n) {
+                atomicOr(&c->error, DEVERR_RANGE);
+            } else if (atomicCAS(&a.qstamp[r], 0xffffffffu, 0u) == 0xffffffffu) {
+                a.pack[r] = r;
+                a.ring[atomicAdd(&c->ring_len[0], 1u)] = (unsigned)r;
+            }
+        }
     }
     if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
 
@@ -535,14 +551,12 @@ extern "C" int g5_sssp_reset(uint64_t nverts, void *d_work, uint64_t work_bytes,
     return G5_OK;
 }
 
-extern "C" int g5_sssp_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
-                                const uint32_t *d_light_deg, float light_delta, uint64_t nverts, uint64_t root,
-                                float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes,
-                                const g5_sssp_params *params, void *stream) {
-    clear_error();
+static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
+                       const uint32_t *d_light_deg, float light_delta, uint64_t nverts, uint64_t root,
+                       const uint64_t *d_roots, unsigned nroots, float *d_dist, int64_t *d_pred, void *d_work,
+                       uint64_t work_bytes, const g5_sssp_params *params, void *stream, const char *who) {
     SsspWork w;
-    int rc = sssp_check(d_rowstarts, d_col, d_w, nverts, root, d_dist, d_pred, d_work, work_bytes, &w,
-                        "g5_sssp_traverse");
+    int rc = sssp_check(d_rowstarts, d_col, d_w, nverts, root, d_dist, d_pred, d_work, work_bytes, &w, who);
     if (rc) return rc;
     g5_sssp_params p = {0.1f, 0};
     if (params) p = *params;
@@ -559,6 +573,8 @@ extern "C" int g5_sssp_traverse(const uint64_t *d_rowstarts, const int32_t *d_co
     a.ld = (d_light_deg && p.delta == light_delta) ? d_light_deg : nullptr;
     a.n = nverts;
     a.root = (unsigned)root;
+    a.roots = d_roots;
+    a.nroots = nroots;
     a.delta = p.delta;
     a.pack = w.pack;
     a.fstamp = w.fstamp;
@@ -584,6 +600,26 @@ extern "C" int g5_sssp_traverse(const uint64_t *d_rowstarts, const int32_t *d_co
     sssp_export_kernel<<<di.sms * 8, 256, 0, st>>>(w.pack, nverts, d_dist, d_pred);
     G5_CUDA_TRY(cudaGetLastError());
     return G5_OK;
+}
+
+extern "C" int g5_sssp_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
+                                const uint32_t *d_light_deg, float light_delta, uint64_t nverts, uint64_t root,
+                                float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes,
+                                const g5_sssp_params *params, void *stream) {
+    clear_error();
+    return sssp_launch(d_rowstarts, d_col, d_w, d_light_deg, light_delta, nverts, root, nullptr, 0, d_dist, d_pred,
+                       d_work, work_bytes, params, stream, "g5_sssp_traverse");
+}
+
+extern "C" int g5_sssp_traverse_multi(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
+                                      const uint32_t *d_light_deg, float light_delta, uint64_t nverts,
+                                      const uint64_t *d_roots, uint32_t nroots, float *d_dist, int64_t *d_pred,
+                                      void *d_work, uint64_t work_bytes, const g5_sssp_params *params,
+                                      void *stream) {
+    clear_error();
+    G5_CHECK_ARG(d_roots && nroots >= 1, "g5_sssp_traverse_multi: no sources");
+    return sssp_launch(d_rowstarts, d_col, d_w, d_light_deg, light_delta, nverts, 0, d_roots, nroots, d_dist, d_pred,
+                       d_work, work_bytes, params, stream, "g5_sssp_traverse_multi");
 }
 
 extern "C" int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,

@@ -97,6 +97,17 @@ int g5_csr_fill_kronecker(const uint32_t seed[5], uint32_t log_n, uint64_t nedge
                           float light_delta, void *d_work, uint64_t work_bytes, int32_t *d_col, float *d_w,
                           uint64_t *d_col64, uint32_t *d_light_deg, void *stream);
 
+/* Packs disjoint graphs into one CSR (no counterpart in the reference, which
+ * holds one graph): copies one graph's CSR into the destination at vertex
+ * offset vbase and entry offset ebase, shifting its column by vbase.  Call
+ * once per graph with increasing offsets; the last call also writes the
+ * destination's final row start.  d_src_w / d_src_light_deg are optional,
+ * together with their destinations. */
+int g5_csr_pack_append(const uint64_t *d_src_rowstarts, const int32_t *d_src_col, const float *d_src_w,
+                       const uint32_t *d_src_light_deg, uint64_t src_nverts, uint64_t src_nentries, uint64_t vbase,
+                       uint64_t ebase, uint64_t *d_dst_rowstarts, int32_t *d_dst_col, float *d_dst_w,
+                       uint32_t *d_dst_light_deg, void *stream);
+
 /* ----------------------------------------------------------------- BFS --- */
 
 typedef struct g5_bfs_params {
@@ -140,6 +151,15 @@ int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, const uint3
 int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
                     int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
                     const g5_bfs_params *params, void *stream);
+
+/* g5_bfs_traverse from several roots at once (device array): every root is
+ * at depth 0 and its own parent.  On disjoint graphs packed with
+ * g5_csr_pack_append, one root per graph, this is every graph's own BFS in
+ * one persistent launch (no counterpart in the reference).  Reset first with
+ * g5_bfs_reset as for g5_bfs_traverse. */
+int g5_bfs_traverse_multi(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, const uint64_t *d_roots,
+                          uint32_t nroots, int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
+                          const g5_bfs_params *params, void *stream);
 
 /* One search end to end from host memory, for callers that issue single
  * queries: copies *h_root (pinned host memory) to the device, runs the
@@ -223,6 +243,15 @@ int g5_sssp_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, const fl
                      float light_delta, uint64_t nverts, uint64_t root, float *d_dist, int64_t *d_pred, void *d_work,
                      uint64_t work_bytes, const g5_sssp_params *params, void *stream);
 
+/* g5_sssp_traverse from several sources at once (device array), all at
+ * distance 0: on packed disjoint graphs, one source per graph, every
+ * graph's own SSSP in one persistent launch (no counterpart in the
+ * reference). */
+int g5_sssp_traverse_multi(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
+                           const uint32_t *d_light_deg, float light_delta, uint64_t nverts, const uint64_t *d_roots,
+                           uint32_t nroots, float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes,
+                           const g5_sssp_params *params, void *stream);
+
 /* Buckets and phases of the last g5_sssp_run that used this workspace, and
  * its device status (synchronises). */
 int g5_sssp_last_status(const void *d_work, uint64_t work_bytes, uint64_t *buckets, uint64_t *phases, void *stream);
@@ -260,6 +289,74 @@ int g5_bfs_validate(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t 
 int g5_sssp_validate(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, uint64_t nverts,
                      uint64_t root, const float *d_dist, const int64_t *d_pred, void *d_work, uint64_t work_bytes,
                      uint64_t *errors, void *stream);
+
+/* ------------------------------------------------------- batched BFS --- */
+/*
+ * Multi-source BFS: up to 256 roots searched together in one persistent
+ * launch, one bit per root in a 256-bit row per vertex.  No counterpart in
+ * the reference, which searches one root per oned_graph_bfs_run call
+ * (src/traversal.cu:479-503); for every root the depth array equals that
+ * search's depth (g5_bfs_run with d_depth).  Parents are not produced.
+ *
+ * A workspace is bound to one graph: size it with g5_msbfs_workspace_size,
+ * fill its per-graph lists once with g5_msbfs_prepare, then run any number of
+ * searches.  Depths are kept as `depth_bits` bit-planes, so a search whose
+ * graph is deeper than 2^depth_bits - 1 levels fails with G5_ERR_INVALID.
+ */
+typedef struct g5_msbfs_params {
+    float alpha;    /* top-down while frontier edges * alpha < CSR entries (<= 0: 32) */
+    int mode;       /* 0 automatic, 1 top-down only, 2 pull only */
+    int check_frontier; /* pull levels test the frontier bitmap before reading a neighbour's row:
+                           0 when under half the entries lead into the frontier, 1 always, 2 never */
+    int blocks;     /* persistent grid (0 = every co-resident block) */
+} g5_msbfs_params;
+
+typedef struct g5_msbfs_stats {
+    int32_t levels;        /* levels expanded */
+    int32_t pull_levels;   /* of which pull (bottom-up) levels */
+    uint32_t error_flags;  /* nonzero: the search did not complete */
+    uint32_t nroots;
+    uint64_t pairs_reached; /* sum over roots of the vertices each reached */
+    uint64_t frontier_edges; /* sum over levels of the frontier's CSR entries */
+} g5_msbfs_stats;
+
+/* Bytes of a workspace for a graph of nverts vertices and nentries CSR
+ * entries with depth_bits planes (1..8; 0 = 6, depths up to 63). */
+int g5_msbfs_workspace_size(uint64_t nverts, uint64_t nentries, int depth_bits, uint64_t *bytes);
+
+/* Builds the workspace's copy of the graph: vertices renumbered by
+ * decreasing degree (so the rows most CSR entries point at sit together and
+ * stay in L2), the CSR in that order with its column in the new numbers,
+ * and the longer rows (above 256 entries) cut into 1024-entry chunks.  Once
+ * per graph and workspace; later searches read only the workspace.
+ * Synchronises. */
+int g5_msbfs_prepare(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t nentries,
+                     int depth_bits, void *d_work, uint64_t work_bytes, void *stream);
+
+/* Searches from h_roots[0..nroots) (host array of vertex ids, 1 <= nroots
+ * <= 256, repeats allowed) on the prepared graph.  Root i is bit i of every
+ * row.  Stream-ordered; h_stats (may be NULL) makes the call synchronise
+ * and report the search's status. */
+int g5_msbfs_run(uint64_t nverts, uint64_t nentries, int depth_bits, const uint64_t *h_roots, uint32_t nroots,
+                 void *d_work, uint64_t work_bytes, const g5_msbfs_params *params, g5_msbfs_stats *h_stats,
+                 void *stream);
+
+/* Depths of the last search as bytes, root-major: d_out[i * nverts + v] is
+ * root i's depth of v, 255 where root i did not reach v. */
+int g5_msbfs_depths_u8(const void *d_work, uint64_t work_bytes, uint64_t nverts, uint64_t nentries, int depth_bits,
+                       uint32_t nroots, uint8_t *d_out, void *stream);
+
+/* Depth array of root i of the last search, -1 where unreached (the layout
+ * of g5_bfs_run's d_depth). */
+int g5_msbfs_depth(const void *d_work, uint64_t work_bytes, uint64_t nverts, uint64_t nentries, int depth_bits,
+                   uint32_t root_index, int32_t *d_depth, void *stream);
+
+/* Status and per-level trace of the last search (synchronises).  mode[i]:
+ * 0 top-down, 1 pull. */
+int g5_msbfs_last_stats(const void *d_work, uint64_t work_bytes, g5_msbfs_stats *stats, void *stream);
+int g5_msbfs_last_trace(const void *d_work, uint64_t work_bytes, int max_levels, int32_t *mode,
+                        uint64_t *frontier_vertices, uint64_t *frontier_edges, double *level_ms, int32_t *nlevels,
+                        void *stream);
 
 /* ------------------------------------------------------------- testing --- */
 

@@ -51,6 +51,12 @@ def test_argument_errors_need_no_device(cgt):
     assert b"root" in lib.g5_last_error()
     assert lib.g5_sssp_run(None, None, None, None, 0.1, 16, 99, None, None, None, 0, None, None) == -1
     assert lib.g5_csr_count(None, 0, 0, None, None, 0, None, None) == -1
+    nb = C.c_uint64()
+    assert lib.g5_msbfs_workspace_size(1 << 10, 1 << 14, 9, C.byref(nb)) == -1
+    assert lib.g5_msbfs_workspace_size(1 << 10, 1 << 14, 0, C.byref(nb)) == 0 and nb.value > 0
+    roots = (C.c_uint64 * 2)(1, 2)
+    assert lib.g5_msbfs_run(16, 100, 0, roots, 2, None, 0, None, None, None) == -1
+    assert lib.g5_msbfs_prepare(None, None, 0, 0, 0, None, 0, None) == -1
 
 
 def test_workspace_sizes_scale_with_vertices(cgt):
