@@ -44,7 +44,9 @@ TRAFFIC_BYTES_PER_EDGE = 3.41
 def load_package():
     if "cgt_b200" in sys.modules:
         return sys.modules["cgt_b200"]
-    spec = importlib.util.spec_from_file_location("cgt_b200", os.path.join(REPO, "cuda-graph-traversal_b200", "__init__.py"))
+    pkg = os.path.join(REPO, "cuda-graph-traversal_b200")
+    spec = importlib.util.spec_from_file_location("cgt_b200", os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
     mod = importlib.util.module_from_spec(spec)
     sys.modules["cgt_b200"] = mod
     spec.loader.exec_module(mod)
@@ -342,7 +344,7 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
-        if world == 1 and not (args.no_batched and args.no_packed):
+        if world == 1 and not (args.no_batched and args.no_packed and args.no_serve):
             del g, bfs, vw, sssp  # the SCALE-26 graph is not needed any more
             torch.cuda.empty_cache()
         if world == 1 and not args.no_batched:
@@ -351,6 +353,9 @@ def run_ours(args):
         if world == 1 and not args.no_packed:
             line["packed"] = run_packed(G, dev, args.packed_graphs, args.packed_min_scale, args.packed_max_scale,
                                         args.edgefactor)
+            torch.cuda.empty_cache()
+        if world == 1 and not args.no_serve:
+            line["serving"] = run_serving(G, dev, args.serve_queries, args.serve_rate, args.edgefactor)
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
@@ -500,6 +505,46 @@ def run_packed(G, dev, ngraphs, smin, smax, ef, reps=3):
                       "min of 3 after a warm-up; plain = per-graph g5_bfs_run + g5_sssp_run, resets included"}
 
 
+SERVE_SCALES = (16, 18, 20, 22, 22, 23, 24, 24)
+
+
+def run_serving(G, dev, nqueries, rate, ef=16):
+    """Serving: 8 resident Kronecker graphs (SCALE 16, 18, 20, 22, 22, 23, 24,
+    24; seeds (2+i, 3)), a Poisson stream of queries (70% BFS, 30% SSSP,
+    uniform graph, uniform non-zero-degree root, seed 1) replayed in real
+    time through the continuous-batching server, then through plain calls
+    one query at a time.  Latency = completion seen by the host - arrival."""
+    import torch
+    import cgt_b200.serve as S
+    t0 = time.time()
+    graphs = [G.oned_graph_from_kronecker(G.make_mrg_seed(2 + i, 3), s, ef << s, device=dev, with_main=False)
+              for i, s in enumerate(SERVE_SCALES)]
+    build_s = time.time() - t0
+    trace = S.poisson_trace(graphs, nqueries, rate, bfs_share=0.7, seed=1)
+    warm = S.poisson_trace(graphs, 64, rate, bfs_share=0.5, seed=99)
+    srv = S.GraphServer(graphs, slots=4, hbm_reserve=16 << 30)
+    srv.run_trace(warm, deadline=600)  # workspaces created, batched copies prepared
+    srv.stats = S.ServerStats()
+    res = srv.run_trace(trace, deadline=3600)
+    ours = S.latency_summary(res)
+    st = srv.stats
+    del srv
+    torch.cuda.empty_cache()
+    S.serve_plain(graphs, warm)
+    plain = S.latency_summary(S.serve_plain(graphs, trace))
+    kinds = {k: S.latency_summary([r for r in res if r.kind == k]) for k in ("bfs", "sssp")}
+    return {"workload": f"{len(graphs)} resident graphs SCALE {list(SERVE_SCALES)} ef{ef}, {nqueries} Poisson "
+                        f"queries at {rate:g}/s (70% BFS, 30% SSSP)",
+            "qps": ours["qps"], "p50_ms": ours["p50_ms"], "p99_ms": ours["p99_ms"],
+            "makespan_s": ours["makespan_s"], "by_kind": kinds,
+            "plain_one_at_a_time": plain, "qps_vs_plain": round(ours["qps"] / plain["qps"], 2),
+            "bfs_batches": st.bfs_batches, "bfs_queries_batched": st.bfs_batched_queries,
+            "sssp_launches": st.sssp_launches, "max_concurrent_launches": st.max_inflight,
+            "build_s": round(build_s, 2),
+            "timing": "host clock: latency from a query's arrival time to the host seeing its launch's "
+                      "CUDA event complete; BFS results exported as depth arrays"}
+
+
 def run_batched_only(args):
     import torch
     torch.cuda.set_device(0)
@@ -511,6 +556,8 @@ def run_batched_only(args):
     if args.only_batched in ("packed", "all"):
         out["packed"] = run_packed(G, dev, args.packed_graphs, args.packed_min_scale, args.packed_max_scale,
                                    args.edgefactor)
+    if args.only_batched in ("serve", "all"):
+        out["serving"] = run_serving(G, dev, args.serve_queries, args.serve_rate, args.edgefactor)
     print(json.dumps(out), flush=True)
 
 
@@ -604,8 +651,11 @@ def main():
     ap.add_argument("--batched-scale", type=int, default=24, help="SCALE of the batched (multi-source) BFS graph")
     ap.add_argument("--batched-roots", type=int, default=256)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched BFS measurement")
-    ap.add_argument("--only-batched", nargs="?", const="msbfs", choices=["msbfs", "packed", "all"],
-                    help="run only the batched measurements (multi-source BFS, packed graphs or both)")
+    ap.add_argument("--only-batched", nargs="?", const="msbfs", choices=["msbfs", "packed", "serve", "all"],
+                    help="run only the batched measurements (multi-source BFS, packed graphs, serving or all)")
+    ap.add_argument("--serve-queries", type=int, default=2000)
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate, queries per second")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     ap.add_argument("--packed-graphs", type=int, default=2000)
     ap.add_argument("--packed-min-scale", type=int, default=10)
     ap.add_argument("--packed-max-scale", type=int, default=18)

@@ -77,6 +77,9 @@ def _load() -> C.CDLL:
         "g5_sssp_validate": ([p, p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_selftest_wait_timeout": ([u32, p, u64, p], C.c_int),
         "g5_msbfs_workspace_size": ([u64, u64, C.c_int, p], C.c_int),
+        "g5_bfs_grid": ([u64, p, p], C.c_int),
+        "g5_sssp_grid": ([u64, p, p], C.c_int),
+        "g5_msbfs_grid": ([u64, p, p], C.c_int),
         "g5_msbfs_prepare": ([p, p, u64, u64, C.c_int, p, u64, p], C.c_int),
         "g5_msbfs_run": ([u64, u64, C.c_int, p, u32, p, u64, p, p, p], C.c_int),
         "g5_msbfs_depths_u8": ([p, u64, u64, u64, C.c_int, u32, p, p], C.c_int),
@@ -133,6 +136,14 @@ def _stream(stream=None) -> int | None:
 
 def _workspace(nbytes: int, device) -> torch.Tensor:
     return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+
+
+def search_grid(kind: str, nverts: int) -> tuple[int, int]:
+    """(blocks, max co-resident blocks) of the persistent kernel of `kind`
+    ("bfs", "sssp", "msbfs") for a graph of nverts vertices."""
+    b, m = C.c_int32(), C.c_int32()
+    _check(getattr(lib, f"g5_{kind}_grid")(nverts, C.byref(b), C.byref(m)))
+    return b.value, m.value
 
 
 def version() -> str:

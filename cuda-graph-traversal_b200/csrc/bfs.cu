@@ -932,3 +932,14 @@ extern "C" int g5_bfs_dist_from_pred(const uint64_t *d_rowstarts, const int32_t 
     }
     return G5_OK;
 }
+
+extern "C" int g5_bfs_grid(uint64_t nverts, int32_t *blocks, int32_t *max_blocks) {
+    clear_error();
+    G5_CHECK_ARG(blocks && max_blocks, "g5_bfs_grid: NULL argument");
+    int mb = 0;
+    int rc = bfs_max_blocks(&mb);
+    if (rc) return rc;
+    *max_blocks = mb;
+    *blocks = (int)std::min<uint64_t>(mb, std::max<uint64_t>(1, nverts / 2048));
+    return G5_OK;
+}

@@ -1074,3 +1074,16 @@ extern "C" int g5_msbfs_last_trace(const void *d_work, uint64_t work_bytes, int 
     *nlevels = c.res.levels;
     return deverr_to_status(c.res.error_flags, "g5_msbfs_run");
 }
+
+extern "C" int g5_msbfs_grid(uint64_t nverts, int32_t *blocks, int32_t *max_blocks) {
+    clear_error();
+    G5_CHECK_ARG(blocks && max_blocks, "g5_msbfs_grid: NULL argument");
+    int mb = 0;
+    int rc = ms_max_blocks(&mb);
+    if (rc) return rc;
+    *max_blocks = mb;
+    // g5_msbfs_run launches every co-resident block by default; this is the
+    // grid a caller sharing the device should pass in params.blocks.
+    *blocks = (int)std::min<uint64_t>(mb, std::max<uint64_t>(1, nverts / 1024));
+    return G5_OK;
+}

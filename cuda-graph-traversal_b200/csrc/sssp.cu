@@ -676,3 +676,14 @@ extern "C" int g5_sssp_last_status(const void *d_work, uint64_t work_bytes, uint
     if (phases) *phases = c.phases;
     return deverr_to_status(c.error, "g5_sssp_run");
 }
+
+extern "C" int g5_sssp_grid(uint64_t nverts, int32_t *blocks, int32_t *max_blocks) {
+    clear_error();
+    G5_CHECK_ARG(blocks && max_blocks, "g5_sssp_grid: NULL argument");
+    int mb = 0;
+    int rc = sssp_max_blocks(&mb);
+    if (rc) return rc;
+    *max_blocks = mb;
+    *blocks = (int)std::min<uint64_t>(mb, std::max<uint64_t>(1, nverts / 2048));
+    return G5_OK;
+}

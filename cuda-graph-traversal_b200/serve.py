@@ -1,0 +1,349 @@
+"""Query serving over graphs resident on one GPU: continuous batching of BFS
+and SSSP queries.  No counterpart in the reference, whose runner issues one
+search per call (examples/graph500_runner.cu:303-409).
+
+A query asks for every vertex's BFS depth or SSSP distance from a root of
+one resident graph.  The server keeps per graph a pending BFS queue and a
+pending SSSP queue and a pool of CUDA streams ("slots").  Whenever a slot is
+free it launches the oldest waiting work:
+
+* all pending BFS queries of a graph (up to 256) become one batched search
+  (g5_msbfs_run + depth export) on that graph's batched-BFS workspace;
+* an SSSP query runs on its own (distances differ per source) on a pooled
+  SSSP workspace of that graph.
+
+Every search is a persistent cooperative kernel whose grid is sized to its
+graph (g5_*_grid); launches run concurrently only while the sum of their
+grids fits on the device at once, so no two grids can wait on each other
+for SMs, and small graphs' searches share the GPU.
+
+Queries that arrive while others run join the next batch of their graph, so
+batches form continuously and work on different graphs and different
+queries overlaps on the device.  Workspaces are created on first use and
+only while free device memory stays above `hbm_reserve` (admission by free
+HBM); otherwise the work waits for a workspace to come free.  Completion is
+seen by polling each launch's CUDA event.  A query's result (an int32 depth
+array, -1 unreached, or a float32 distance array, -1.0 unreached) is
+identical whether it ran alone or in a batch.
+"""
+from __future__ import annotations
+
+import collections
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import (MSBFS_MAX_ROOTS, BfsState, MsBfsParams, MsBfsState, OnedGraph, SsspState, msbfs_depths_u8,
+               msbfs_run, msbfs_stats, oned_graph_bfs_run, oned_graph_sssp_reset, oned_graph_sssp_traverse,
+               search_grid, sssp_status)
+
+
+@dataclass
+class Query:
+    qid: int
+    kind: str      # "bfs" or "sssp"
+    graph: int     # index into the server's graphs
+    root: int
+    arrival: float = 0.0  # seconds, on the trace's clock
+
+
+@dataclass
+class Result:
+    qid: int
+    kind: str
+    graph: int
+    root: int
+    arrival: float
+    done: float           # seconds, same clock as arrival
+    batch: int            # queries in the launch that answered it
+    value: torch.Tensor | None = None  # depth (int32) or distance (float32), when kept
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+
+@dataclass
+class _Launch:
+    event: torch.cuda.Event
+    queries: list
+    kind: str
+    graph: int
+    slot: int
+    resource: object
+    blocks: int
+    out: torch.Tensor | None = None
+
+
+@dataclass
+class ServerStats:
+    launches: int = 0
+    bfs_batches: int = 0
+    bfs_batched_queries: int = 0
+    sssp_launches: int = 0
+    max_inflight: int = 0
+    workspaces: dict = field(default_factory=dict)
+    refused_for_memory: int = 0
+
+
+class GraphServer:
+    def __init__(self, graphs: list[OnedGraph], slots: int = 4, hbm_reserve: int = 8 << 30,
+                 max_batch: int = MSBFS_MAX_ROOTS, keep_results: bool = False, max_sssp_per_graph: int = 4):
+        if not graphs:
+            raise ValueError("GraphServer needs at least one graph")
+        self.graphs = graphs
+        self.dev = graphs[0].device
+        self.streams = [torch.cuda.Stream(device=self.dev) for _ in range(slots)]
+        self.free_slots = list(range(slots))
+        self.hbm_reserve = int(hbm_reserve)
+        self.max_batch = int(max_batch)
+        self.keep = keep_results
+        self.max_sssp = int(max_sssp_per_graph)
+        self.pending = {k: [collections.deque() for _ in graphs] for k in ("bfs", "sssp")}
+        self.ms: list[MsBfsState | None] = [None] * len(graphs)
+        self.ms_busy = [False] * len(graphs)
+        self.sssp_free: list[list[SsspState]] = [[] for _ in graphs]
+        self.sssp_count = [0] * len(graphs)
+        self.inflight: list[_Launch] = []
+        self.grid = {k: [search_grid(k, g.nglobalverts)[0] for g in graphs] for k in ("msbfs", "sssp")}
+        self.max_blocks = min(search_grid(k, 1)[1] for k in ("msbfs", "sssp"))
+        self.blocks_in_use = 0
+        self.stats = ServerStats()
+        self.clock0 = time.perf_counter()
+
+    # ------------------------------------------------------------ admission
+    def _fits(self, nbytes: int) -> bool:
+        free, _ = torch.cuda.mem_get_info(self.dev)
+        ok = free - nbytes >= self.hbm_reserve
+        if not ok:
+            self.stats.refused_for_memory += 1
+        return ok
+
+    def _ms_state(self, gi: int) -> MsBfsState | None:
+        if self.ms[gi] is None:
+            g = self.graphs[gi]
+            need = 330 * g.nglobalverts + 12 * g.nlocaledges  # rows, planes, renumbered copy
+            if not self._fits(need):
+                return None
+            self.ms[gi] = MsBfsState(g)
+            self.stats.workspaces[f"msbfs{gi}"] = self.ms[gi].work.numel()
+        return self.ms[gi]
+
+    def _sssp_state(self, gi: int) -> SsspState | None:
+        if self.sssp_free[gi]:
+            return self.sssp_free[gi].pop()
+        if self.sssp_count[gi] >= self.max_sssp:
+            return None
+        g = self.graphs[gi]
+        if not self._fits(140 * g.nglobalverts):
+            return None
+        self.sssp_count[gi] += 1
+        self.stats.workspaces[f"sssp{gi}_{self.sssp_count[gi]}"] = 1
+        return SsspState(g)
+
+    # ------------------------------------------------------------- queueing
+    def now(self) -> float:
+        return time.perf_counter() - self.clock0
+
+    def submit(self, q: Query) -> None:
+        if q.kind not in ("bfs", "sssp"):
+            raise ValueError(f"unknown query kind {q.kind!r}")
+        if not 0 <= q.graph < len(self.graphs):
+            raise ValueError(f"query {q.qid}: no graph {q.graph}")
+        if not 0 <= q.root < self.graphs[q.graph].nglobalverts:
+            raise ValueError(f"query {q.qid}: root {q.root} out of range")
+        self.pending[q.kind][q.graph].append(q)
+
+    def idle(self) -> bool:
+        return not self.inflight and not any(any(d) for k in self.pending.values() for d in k)
+
+    def _candidates(self):
+        """(arrival, kind, graph) of every launchable queue head, oldest first."""
+        c = []
+        for kind, queues in self.pending.items():
+            for gi, d in enumerate(queues):
+                if d and not (kind == "bfs" and self.ms_busy[gi]):
+                    c.append((d[0].arrival, kind, gi))
+        c.sort()
+        return c
+
+    # --------------------------------------------------------------- launch
+    def _launch_one(self) -> bool:
+        """Launches the oldest work whose grid fits beside what runs; work
+        without a workspace (memory) is passed over.  False when nothing
+        could start."""
+        if not self.free_slots:
+            return False
+        for _, kind, gi in self._candidates():
+            blocks = self.grid["msbfs" if kind == "bfs" else "sssp"][gi]
+            if self.blocks_in_use + blocks > self.max_blocks:
+                # Oldest first: younger work may not take the SMs this
+                # launch is waiting for (a full-device search would starve).
+                return False
+            g = self.graphs[gi]
+            if kind == "bfs":
+                ms = self._ms_state(gi)
+                if ms is None:
+                    continue
+                slot = self.free_slots.pop()
+                d = self.pending["bfs"][gi]
+                qs = [d.popleft() for _ in range(min(len(d), self.max_batch))]
+                s = self.streams[slot]
+                with torch.cuda.stream(s):
+                    msbfs_run(g, ms, [q.root for q in qs], MsBfsParams(0.0, 0, 0, blocks), sync=False, stream=s)
+                    out = msbfs_depths_u8(ms, stream=s)
+                    ev = torch.cuda.Event()
+                    ev.record(s)
+                self.ms_busy[gi] = True
+                self.inflight.append(_Launch(ev, qs, "bfs", gi, slot, ms, blocks, out))
+                self.stats.bfs_batches += 1
+                self.stats.bfs_batched_queries += len(qs)
+            else:
+                st = self._sssp_state(gi)
+                if st is None:
+                    continue
+                slot = self.free_slots.pop()
+                q = self.pending["sssp"][gi].popleft()
+                s = self.streams[slot]
+                with torch.cuda.stream(s):
+                    oned_graph_sssp_reset(st, stream=s)
+                    oned_graph_sssp_traverse(g, st, q.root, blocks=blocks, stream=s)
+                    ev = torch.cuda.Event()
+                    ev.record(s)
+                self.inflight.append(_Launch(ev, [q], "sssp", gi, slot, st, blocks))
+                self.stats.sssp_launches += 1
+            self.blocks_in_use += blocks
+            self.stats.launches += 1
+            self.stats.max_inflight = max(self.stats.max_inflight, len(self.inflight))
+            return True
+        return False
+
+    def _complete(self, L: _Launch, t: float) -> list[Result]:
+        out = []
+        if L.kind == "bfs":
+            msbfs_stats(L.resource, self.streams[L.slot])  # raises on a device error
+            for i, q in enumerate(L.queries):
+                v = None
+                if self.keep:
+                    v = L.out[i].to(torch.int32)
+                    v[v == 255] = -1
+                out.append(Result(q.qid, q.kind, q.graph, q.root, q.arrival, t, len(L.queries), v))
+            self.ms_busy[L.graph] = False
+        else:
+            sssp_status(L.resource, self.streams[L.slot])
+            q = L.queries[0]
+            v = L.resource.dist.clone() if self.keep else None
+            out.append(Result(q.qid, q.kind, q.graph, q.root, q.arrival, t, 1, v))
+            self.sssp_free[L.graph].append(L.resource)
+        self.free_slots.append(L.slot)
+        self.blocks_in_use -= L.blocks
+        return out
+
+    def poll(self) -> list[Result]:
+        """Launches what it can, then collects finished launches."""
+        while self._launch_one():
+            pass
+        done, still = [], []
+        for L in self.inflight:
+            if L.event.query():
+                done.append(L)
+            else:
+                still.append(L)
+        self.inflight = still
+        t = self.now()
+        res = []
+        for L in done:
+            res.extend(self._complete(L, t))
+        if done:
+            while self._launch_one():
+                pass
+        return res
+
+    def run_trace(self, queries: list[Query], deadline: float | None = None) -> list[Result]:
+        """Replays `queries` (sorted by arrival, seconds from now) in real
+        time: each is submitted once its arrival time has passed.  Raises
+        TimeoutError when work is still waiting `deadline` seconds after the
+        start (for instance when no workspace can ever be admitted)."""
+        queries = sorted(queries, key=lambda q: q.arrival)
+        self.clock0 = time.perf_counter()
+        results: list[Result] = []
+        i = 0
+        while i < len(queries) or not self.idle():
+            t = self.now()
+            if deadline is not None and t > deadline:
+                raise TimeoutError(f"{len(queries) - len(results)} queries unanswered after {deadline} s "
+                                   f"({self.stats.refused_for_memory} workspace requests refused for memory)")
+            while i < len(queries) and queries[i].arrival <= t:
+                self.submit(queries[i])
+                i += 1
+            results.extend(self.poll())
+            if not self.inflight and i < len(queries) and not any(
+                    any(d) for k in self.pending.values() for d in k):
+                # nothing to do until the next arrival
+                wait = queries[i].arrival - self.now()
+                if wait > 0:
+                    time.sleep(min(wait, 0.001))
+        return results
+
+
+def serve_plain(graphs: list[OnedGraph], queries: list[Query], keep_results: bool = False) -> list[Result]:
+    """The same trace answered one query at a time with the plain calls
+    (g5_bfs_run with depth, g5_sssp_run), in arrival order: a query starts
+    when it has arrived and the previous one finished."""
+    queries = sorted(queries, key=lambda q: q.arrival)
+    bfs = [None] * len(graphs)
+    sssp = [None] * len(graphs)
+    t0 = time.perf_counter()
+    out = []
+    for q in queries:
+        now = time.perf_counter() - t0
+        if q.arrival > now:
+            time.sleep(q.arrival - now)
+        g = graphs[q.graph]
+        if q.kind == "bfs":
+            if bfs[q.graph] is None:
+                bfs[q.graph] = BfsState(g)
+            oned_graph_bfs_run(g, bfs[q.graph], q.root)
+            torch.cuda.synchronize()
+            v = bfs[q.graph].depth.clone() if keep_results else None
+        else:
+            if sssp[q.graph] is None:
+                sssp[q.graph] = SsspState(g)
+            oned_graph_sssp_reset(sssp[q.graph])
+            oned_graph_sssp_traverse(g, sssp[q.graph], q.root)
+            torch.cuda.synchronize()
+            v = sssp[q.graph].dist.clone() if keep_results else None
+        out.append(Result(q.qid, q.kind, q.graph, q.root, q.arrival, time.perf_counter() - t0, 1, v))
+    return out
+
+
+def poisson_trace(graphs: list[OnedGraph], nqueries: int, rate: float, bfs_share: float = 0.7,
+                  seed: int = 1) -> list[Query]:
+    """nqueries queries with exponential inter-arrival times (mean 1/rate
+    seconds), kind BFS with probability bfs_share, graph uniform, root
+    uniform over the graph's vertices of non-zero degree."""
+    rng = np.random.default_rng(seed)
+    nz = []
+    for g in graphs:
+        deg = (g.rowstarts[1:] - g.rowstarts[:-1]).cpu().numpy()
+        nz.append(np.nonzero(deg > 0)[0])
+    t = np.cumsum(rng.exponential(1.0 / rate, nqueries))
+    kinds = np.where(rng.random(nqueries) < bfs_share, "bfs", "sssp")
+    gsel = rng.integers(0, len(graphs), nqueries)
+    qs = []
+    for i in range(nqueries):
+        cand = nz[gsel[i]]
+        root = int(cand[rng.integers(0, len(cand))]) if len(cand) else 0
+        qs.append(Query(i, str(kinds[i]), int(gsel[i]), root, float(t[i])))
+    return qs
+
+
+def latency_summary(results: list[Result]) -> dict:
+    lat = np.array([r.latency for r in results])
+    span = max(r.done for r in results) - min(r.arrival for r in results)
+    return {"queries": len(results), "qps": round(len(results) / span, 1),
+            "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
+            "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
+            "mean_ms": round(float(lat.mean()) * 1e3, 3), "makespan_s": round(span, 3)}

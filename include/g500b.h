@@ -358,6 +358,17 @@ int g5_msbfs_last_trace(const void *d_work, uint64_t work_bytes, int max_levels,
                         uint64_t *frontier_vertices, uint64_t *frontier_edges, double *level_ms, int32_t *nlevels,
                         void *stream);
 
+/* ------------------------------------------------------------- grids ----- */
+/* Grid (blocks) sized for a graph of nverts vertices -- what g5_bfs_* and
+ * g5_sssp_* launch with params.blocks = 0 (g5_msbfs_run then takes every
+ * co-resident block instead) -- and the most blocks of the kernel that fit
+ * on the device at once.  A caller that runs searches on several streams at
+ * the same time passes these grids in params.blocks and keeps their sum
+ * within max_blocks, so every cooperative grid can be resident together. */
+int g5_bfs_grid(uint64_t nverts, int32_t *blocks, int32_t *max_blocks);
+int g5_sssp_grid(uint64_t nverts, int32_t *blocks, int32_t *max_blocks);
+int g5_msbfs_grid(uint64_t nverts, int32_t *blocks, int32_t *max_blocks);
+
 /* ------------------------------------------------------------- testing --- */
 
 /* Launches a two-block cooperative kernel whose grid barrier can never

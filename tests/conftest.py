@@ -30,7 +30,8 @@ def load_package():
     lib = os.path.join(PKG_DIR, "lib", "libg500b.so")
     if not os.path.exists(lib):
         subprocess.run(["make", "-s", "-C", PKG_DIR, "-j8"], check=True)
-    spec = importlib.util.spec_from_file_location("cgt_b200", os.path.join(PKG_DIR, "__init__.py"))
+    spec = importlib.util.spec_from_file_location("cgt_b200", os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
     mod = importlib.util.module_from_spec(spec)
     sys.modules["cgt_b200"] = mod
     spec.loader.exec_module(mod)
