@@ -380,12 +380,15 @@ def run_batched(G, dev, scale, ef, nroots, reps=3):
     torch.cuda.synchronize()
     prep_ms = a.elapsed_time(b)
     depth8 = torch.empty((len(roots), g.nglobalverts), dtype=torch.uint8, device=dev)
-    G.msbfs_run(g, ms, roots)  # warm-up
+    import cgt_b200.autotune as T
+    tuned = T.tune_msbfs(g, roots, alphas=(16.0, 32.0, 64.0), checks=(0, 2), ms=ms)
+    params = T.msbfs_params(tuned)
+    G.msbfs_run(g, ms, roots, params)  # warm-up
     search_ms, full_ms = [], []
     for _ in range(reps):
         a, b, c = ev(), ev(), ev()
         a.record()
-        G.msbfs_run(g, ms, roots, sync=False)
+        G.msbfs_run(g, ms, roots, params, sync=False)
         b.record()
         G.msbfs_depths_u8(ms, depth8)
         c.record()
@@ -424,6 +427,7 @@ def run_batched(G, dev, scale, ef, nroots, reps=3):
             "depth_arrays_checked_identical": checked, "levels": st.levels, "pull_levels": st.pull_levels,
             "level_ms": [round(x, 3) for x in trace["ms"]], "level_mode": trace["mode"],
             "prepare_ms": round(prep_ms, 2), "setup_s": round(time.time() - t0, 2),
+            "autotuned": {k: tuned[k] for k in ("alpha", "check_frontier", "blocks", "candidates")},
             "timing": "device events, min of 3 after one warm-up; plain = single-root traverse with depth, "
                       "reset untimed"}
 
@@ -441,7 +445,11 @@ def run_packed(G, dev, ngraphs, smin, smax, ef, reps=3):
     scales = rng.integers(smin, smax + 1, size=ngraphs).tolist()
     t0 = time.time()
     pk = G.pack_kronecker(scales, edgefactor=ef, seed1_base=100, seed2=3, device=dev)
-    batch = G.PackedBatch(pk, delta=0.1, capture=True)
+    import cgt_b200.autotune as T
+    tb = T.tune_bfs(pk.g, pk.d_roots, alphas=(10.0, 14.0, 20.0), betas=(24.0,), grids=(0,))
+    ts = T.tune_sssp(pk.g, pk.d_roots, deltas=(0.08, 0.1, 0.2, 0.4), grids=(0,))
+    batch = G.PackedBatch(pk, delta=ts["delta"], capture=True, bfs_params=T.bfs_params(tb),
+                          sssp_blocks=ts["blocks"])
     build_s = time.time() - t0
     bfs_ms, all_ms = [], []
     for _ in range(reps):
@@ -458,7 +466,7 @@ def run_packed(G, dev, ngraphs, smin, smax, ef, reps=3):
         with torch.cuda.stream(batch.stream):
             G.oned_graph_bfs_reset(batch.bfs, True, pk.g)
             a.record(batch.stream)
-            G.oned_graph_bfs_traverse_multi(pk.g, batch.bfs, pk.d_roots)
+            G.oned_graph_bfs_traverse_multi(pk.g, batch.bfs, pk.d_roots, batch.bfs_params)
             b.record(batch.stream)
         torch.cuda.synchronize()
         bfs_ms.append(a.elapsed_time(b))
@@ -478,7 +486,7 @@ def run_packed(G, dev, ngraphs, smin, smax, ef, reps=3):
         a.record()
         G.oned_graph_bfs_run(g, bfs, r)
         b.record()
-        G.oned_graph_sssp_run(g, ss, r)
+        G.oned_graph_sssp_run(g, ss, r, delta=ts["delta"])
         c.record()
         torch.cuda.synchronize()
         plain_bfs += a.elapsed_time(b)
@@ -501,6 +509,7 @@ def run_packed(G, dev, ngraphs, smin, smax, ef, reps=3):
             "speedup_vs_plain": round((plain_bfs + plain_sssp) / best, 2),
             "bfs_speedup_vs_plain": round(plain_bfs / best_bfs, 2),
             "graphs_checked_identical": checked, "build_s": round(build_s, 2),
+            "autotuned": {"bfs_alpha": tb["alpha"], "bfs_beta": tb["beta"], "sssp_delta": ts["delta"]},
             "timing": "device events; batch = replay of the captured CUDA graph (BFS+SSSP resets included), "
                       "min of 3 after a warm-up; plain = per-graph g5_bfs_run + g5_sssp_run, resets included"}
 

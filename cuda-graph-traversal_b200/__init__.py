@@ -408,8 +408,10 @@ class PackedBatch:
     stream, captured once into a CUDA graph and replayed per batch (no
     per-graph launches, no host work between them)."""
 
-    def __init__(self, pk: PackedGraphs, delta: float = 0.1, capture: bool = True, with_depth: bool = True):
+    def __init__(self, pk: PackedGraphs, delta: float = 0.1, capture: bool = True, with_depth: bool = True,
+                 bfs_params: BfsParams | None = None, sssp_blocks: int = 0):
         self.pk, self.delta, self.with_depth = pk, delta, with_depth
+        self.bfs_params, self.sssp_blocks = bfs_params, sssp_blocks
         self.bfs = BfsState(pk.g)
         self.sssp = SsspState(pk.g)
         self.stream = torch.cuda.Stream(device=pk.g.device)
@@ -426,11 +428,12 @@ class PackedBatch:
 
     def _enqueue_bfs(self):
         oned_graph_bfs_reset(self.bfs, self.with_depth, self.pk.g)
-        oned_graph_bfs_traverse_multi(self.pk.g, self.bfs, self.pk.d_roots, with_depth=self.with_depth)
+        oned_graph_bfs_traverse_multi(self.pk.g, self.bfs, self.pk.d_roots, self.bfs_params,
+                                      with_depth=self.with_depth)
 
     def _enqueue_sssp(self):
         oned_graph_sssp_reset(self.sssp)
-        oned_graph_sssp_traverse_multi(self.pk.g, self.sssp, self.pk.d_roots, self.delta)
+        oned_graph_sssp_traverse_multi(self.pk.g, self.sssp, self.pk.d_roots, self.delta, self.sssp_blocks)
 
     def run(self) -> None:
         """Enqueues one batch on self.stream (replaying the graph when captured)."""

@@ -169,7 +169,7 @@ __device__ __forceinline__ void relax(const SsspArgs &a, const PushCtx &x, Count
                     // Largest j with b_{B+j} <= cand; the ring holds B+1 .. B+RING-1.
                     int j = 1;
                     while (j < RING && x.bnd[j + 1] <= cand) ++j;
-                    if (j >= RING) atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+                    if (j >= RING) atomicOr(&a.ctl->error, DEVERR_RING);
                     else target = (int)x.bucket + j;
                 }
             }

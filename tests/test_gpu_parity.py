@@ -348,3 +348,16 @@ def test_fused_generator_csr_matches(cgt, graphs, golden_dump):
     ref = d["g"]
     assert np.array_equal(_np(g.light_deg), _np(ref.light_deg))
     assert np.array_equal(g.main_bits, ref.main_bits)
+
+
+def test_sssp_delta_too_small_is_an_error(cgt, graphs):
+    """A delta so small that a weight spans more buckets than the ring holds
+    is reported (ValueError), not answered wrongly; the next search works."""
+    g = graphs[12]["g"]
+    ss = cgt.SsspState(g)
+    r = cgt.generate_bfs_roots(g, 2, 3, 1)[0]
+    with pytest.raises(ValueError, match="larger delta"):
+        cgt.oned_graph_sssp_run(g, ss, r, delta=0.01)
+        cgt.sssp_status(ss)
+    cgt.oned_graph_sssp_run(g, ss, r)
+    assert cgt.sssp_status(ss)[0] > 0

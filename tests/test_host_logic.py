@@ -1,0 +1,42 @@
+"""Host-side logic of the batching layers, without a GPU: the autotuner's
+cache, the serving trace generator and latency summary."""
+from __future__ import annotations
+
+import types
+
+import numpy as np
+import torch
+
+
+def _fake_graph(n, rowstarts=None, nentries=30000):
+    rs = torch.as_tensor(rowstarts if rowstarts is not None else np.arange(n + 1) * 2, dtype=torch.int64)
+    return types.SimpleNamespace(device=torch.device("cpu"), nglobalverts=n, nlocaledges=nentries, rowstarts=rs)
+
+
+def test_tuning_cache_round_trip(cgt, tmp_path):
+    """Settings are keyed by device, kind and graph size and survive a reload."""
+    from cgt_b200 import autotune as T
+    fake, other = _fake_graph(1 << 10), _fake_graph(1 << 11)
+    c = T.TuningCache(str(tmp_path / "t.json"))
+    assert c.get("bfs", fake) is None
+    c.put("bfs", fake, {"alpha": 10.0, "beta": 24.0, "blocks": 0})
+    c2 = T.TuningCache(str(tmp_path / "t.json"))
+    assert c2.get("bfs", fake)["alpha"] == 10.0 and c2.get("bfs", other) is None and c2.get("sssp", fake) is None
+    assert T.bfs_params(c2.get("bfs", fake)).alpha == 10.0
+
+
+def test_poisson_trace_and_summary(cgt):
+    from cgt_b200 import serve as S
+    # graph 1 has isolated vertices 0 and 2: roots never land there
+    g0 = _fake_graph(8)
+    g1 = _fake_graph(4, rowstarts=[0, 0, 3, 3, 5])
+    tr = S.poisson_trace([g0, g1], 2000, rate=1000.0, bfs_share=0.7, seed=5)
+    assert len(tr) == 2000 and all(a.arrival < b.arrival for a, b in zip(tr, tr[1:]))
+    assert 0.65 < sum(q.kind == "bfs" for q in tr) / len(tr) < 0.75
+    assert {q.root for q in tr if q.graph == 1} <= {1, 3}
+    assert abs(tr[-1].arrival - 2.0) < 0.3  # mean gap 1 ms
+    assert tr == S.poisson_trace([g0, g1], 2000, rate=1000.0, bfs_share=0.7, seed=5)
+    res = [S.Result(q.qid, q.kind, q.graph, q.root, q.arrival, q.arrival + 0.001 * (1 + q.qid % 10), 1)
+           for q in tr]
+    s = S.latency_summary(res)
+    assert s["queries"] == 2000 and abs(s["p50_ms"] - 5.5) < 1.0 and s["p99_ms"] >= 9.9

@@ -55,3 +55,4 @@ def test_two_rank_sharding_and_reductions():
 
 def test_single_rank_takes_every_root():
     assert bench.rank_roots([5, 6, 7], 0, 1) == [5, 6, 7]
+
