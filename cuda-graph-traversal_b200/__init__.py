@@ -68,7 +68,7 @@ def _load() -> C.CDLL:
         "g5_sssp_workspace_size": ([u64, p], C.c_int),
         "g5_sssp_run": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_sssp_last_status": ([p, u64, p, p, p], C.c_int),
-        "g5_sssp_reset": ([u64, p, u64, p], C.c_int),
+        "g5_sssp_reset": ([u64, p, p, p, u64, p], C.c_int),
         "g5_sssp_last_trace": ([p, u64, p, C.c_int, p, p, p, p, p], C.c_int),
         "g5_sssp_traverse": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_validate_workspace_size": ([u64, p], C.c_int),
@@ -728,14 +728,20 @@ def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float =
 
 
 def oned_graph_sssp_reset(sssp: SsspState, stream=None) -> None:
-    """The workspace reset of oned_graph_sssp_run (the reference's
-    oned_graph_sssp_clear, which its runner keeps outside the timed region)."""
-    _check(lib.g5_sssp_reset(sssp.max_nlocalverts, _ptr(sssp.work), sssp.work.numel(), _stream(stream)))
+    """The reset half of oned_graph_sssp_run (the reference's
+    oned_graph_sssp_clear, which its runner keeps outside the timed region):
+    workspace cleared, dist = -1.0f and pred = -1 everywhere, so the search
+    writes only the vertices it reaches."""
+    _check(lib.g5_sssp_reset(sssp.max_nlocalverts, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
+                             sssp.work.numel(), _stream(stream)))
 
 
 def oned_graph_sssp_traverse(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,
                              stream=None) -> None:
-    """The search itself, on a reset workspace."""
+    """The search itself, on a reset state (one block for a root outside the
+    main component)."""
+    if blocks == 0 and not g.in_main_component(root):
+        blocks = 1
     p = SsspParams(delta, blocks)
     _check(lib.g5_sssp_traverse(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
                                 g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),

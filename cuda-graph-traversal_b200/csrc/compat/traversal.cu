@@ -12,10 +12,6 @@ using namespace g5compat;
 
 static const float kLightDelta = 0.1f;  // the reference's SSSP delta (src/traversal.cu:645)
 
-__global__ static void fill_minus_one(f32 *x, u64 n) {
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) x[i] = -1.0f;
-}
-
 Oned_Graph oned_graph_from_tuple_graph(Worker_State *ws, Tuple_Graph *tg, u64 nglobalverts) {
     Oned_Graph g;
     memset(&g, 0, sizeof g);
@@ -178,11 +174,10 @@ void oned_graph_sssp_clear(Worker_State *ws, Sssp_State *sssp) {
         ERROR("Sssp_State was not created by oned_graph_sssp_create of this library");
         worker_abort(ws, 1);
     }
-    check(ws, g5_sssp_reset(sssp->max_nlocalverts, sx->work, sx->work_bytes, 0), "oned_graph_sssp_clear");
-    CHECK_CUDA(cudaMemset(sssp->pred, 0xff, sssp->max_nlocalverts * sizeof(i64)));
-    // -1.0f everywhere, the reference's "unreached" (src/traversal.cu:250).
-    fill_minus_one<<<256, 256>>>(sssp->dist, sssp->max_nlocalverts);
-    CHECK_CUDA(cudaGetLastError());
+    // pred = -1 and dist = -1.0f everywhere, the reference's "unreached"
+    // (src/traversal.cu:248-249); the search then writes reached vertices only.
+    check(ws, g5_sssp_reset(sssp->max_nlocalverts, sssp->dist, sssp->pred, sx->work, sx->work_bytes, 0),
+          "oned_graph_sssp_clear");
     CHECK_CUDA(cudaDeviceSynchronize());
 }
 
@@ -198,7 +193,10 @@ void oned_graph_sssp_run(Worker_State *ws, const Oned_Graph *g, Sssp_State *sssp
         ERROR("Sssp_State was not created by oned_graph_sssp_create of this library");
         worker_abort(ws, 1);
     }
-    g5_sssp_params p = {kLightDelta, 0};
+    // A root outside the largest component (host bitmap from the first BFS
+    // state) runs on one block: its search touches a handful of vertices.
+    const bool small = gx->main_host && !((gx->main_host[root >> 5] >> (root & 31)) & 1u);
+    g5_sssp_params p = {kLightDelta, small ? 1 : 0};
     check(ws, g5_sssp_traverse(g->rowstarts, gx->col, g->weights, gx->light_deg, gx->light_delta, g->nglobalverts,
                                root, sssp->dist, sssp->pred, sx->work, sx->work_bytes, &p, 0),
           "oned_graph_sssp_run");

@@ -28,7 +28,7 @@
 //     the BFS kernel, over the light or the heavy part of each row.
 //
 // Algorithmic bytes per search: 2 m_c * (4 col + 4 w) + n_c * (8 rowstarts
-// + 8 packed dist/parent), plus 4 + 8 bytes per export.
+// + 8 packed dist/parent + 4 dist + 8 parent written out).
 #include <algorithm>
 
 #include "g5_common.cuh"
@@ -66,6 +66,16 @@ struct SsspCtl {
     unsigned char kind_phase[SSSP_TRACE];
 };
 
+// Output arrays that g5_sssp_reset pre-filled with -1.0f / -1.  When the
+// search writes to the same arrays, it stores each vertex's distance and
+// parent when the vertex is settled and leaves unreached ones untouched, so
+// a search costs O(reached) instead of O(N) (a search in a two-vertex
+// component must not sweep a 67M-vertex array).
+struct SsspOut {
+    float *dist;
+    int64_t *pred;
+};
+
 struct SsspArgs {
     const uint64_t *rowptr;
     const int *col;
@@ -83,6 +93,9 @@ struct SsspArgs {
     unsigned *S[2], *SB[2];  // heavy sets and chunk bases
     unsigned *ring;
     SsspCtl *ctl;
+    const SsspOut *prefilled;
+    float *dist;
+    int64_t *pred;
     unsigned nblocks;
     unsigned long long limit_ns;
 };
@@ -98,6 +111,17 @@ __device__ __forceinline__ void part_range(const SsspArgs &a, unsigned u, bool h
         const uint64_t mid = b + __ldg(&a.ld[u]);
         if (heavy) b = mid;
         else e = mid;
+    }
+}
+
+// Marks u settled; with pre-filled outputs also stores its final distance
+// and parent (p = its packed value, final once its bucket's light phases are
+// done).
+__device__ __forceinline__ void settle(const SsspArgs &a, bool sparse_out, unsigned u, unsigned long long p) {
+    atomicOr(&a.settled[u >> 5], 1u << (u & 31));
+    if (sparse_out) {
+        a.dist[u] = pack_dist(p);
+        a.pred[u] = (int64_t)(unsigned)p;
     }
 }
 
@@ -141,23 +165,53 @@ __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCt
     if (!ok) atomicOr(&c->error, DEVERR_CAPACITY);
 }
 
-// Relaxes u -> v with float weight wt from distance du; queues v when its
-// distance dropped.  All 32 lanes call it (want = lane has an edge).
+// Edges of one warp step, E per lane: their target vertices' settled bits
+// and packed distances are loaded together before any is used, so the
+// step costs one chain of memory round trips, not E.
+constexpr int SSSP_EDGES = 2;
+
+struct EdgeProbe {
+    unsigned v[SSSP_EDGES];
+    float wt[SSSP_EDGES];
+    unsigned u[SSSP_EDGES];
+    float du[SSSP_EDGES];
+    bool has[SSSP_EDGES];
+    unsigned long long cur[SSSP_EDGES];  // v's packed distance/parent, ~0 if not needed
+};
+
+// Fills p.cur for the edges in p (settled targets and non-vertices get
+// UNREACHED-free zero so relax() skips them).
+__device__ __forceinline__ void probe_edges(const SsspArgs &a, Counts &k, EdgeProbe &p) {
+    unsigned sw[SSSP_EDGES];
+#pragma unroll
+    for (int t = 0; t < SSSP_EDGES; ++t) {
+        k.edges += p.has[t];
+        if (p.has[t] && p.v[t] >= a.n) {  // not a vertex: report it, touch nothing
+            atomicOr(&a.ctl->error, DEVERR_RANGE);
+            p.has[t] = false;
+        }
+        sw[t] = p.has[t] ? __ldcg(&a.settled[p.v[t] >> 5]) : 0u;
+    }
+#pragma unroll
+    for (int t = 0; t < SSSP_EDGES; ++t) {
+        const bool settled = (sw[t] >> (p.v[t] & 31)) & 1u;
+        k.settled += p.has[t] && settled;
+        p.has[t] = p.has[t] && !settled;
+        p.cur[t] = p.has[t] ? __ldcg(&a.pack[p.v[t]]) : 0ull;
+    }
+}
+
+// Relaxes u -> v with float weight wt from distance du (cur = v's packed
+// value read by probe_edges); queues v when its distance dropped.  All 32
+// lanes call it (want = lane has an edge to a vertex not settled).
 __device__ __forceinline__ void relax(const SsspArgs &a, const PushCtx &x, Counts &k, bool want, unsigned u, float du,
-                                      unsigned v, float wt, bool heavy_phase) {
+                                      unsigned v, float wt, unsigned long long cur, bool heavy_phase) {
     bool same = false;
     int target = -1;
-    k.edges += want;
-    if (want && v >= a.n) {  // not a vertex: report it, touch nothing
-        atomicOr(&a.ctl->error, DEVERR_RANGE);
-        want = false;
-    }
-    const bool settled = want && ((__ldcg(&a.settled[v >> 5]) >> (v & 31)) & 1u);
-    k.settled += settled;
-    if (want && !settled) {
+    if (want) {
         const float cand = __fadd_rn(du, wt);
         const unsigned long long np = ((unsigned long long)__float_as_uint(cand) << 32) | u;
-        if (np < __ldcg(&a.pack[v])) {
+        if (np < cur) {
             ++k.atomics;
             const unsigned long long old = atomicMin(&a.pack[v], np);
             if (np < old && (old >> 32) != (np >> 32)) {
@@ -225,7 +279,8 @@ __device__ void stage_flush(const SsspArgs &a, const PushCtx &x, Counts &k) {
 // (small part [0, ns), big part at the back, `bp` its packed counter).  The
 // heavy pass also marks each list vertex settled.
 __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, const unsigned *L, unsigned ns,
-                            unsigned long long bp, const unsigned *B, unsigned *grab, unsigned *cgrab, bool heavy) {
+                            unsigned long long bp, const unsigned *B, unsigned *grab, unsigned *cgrab, bool heavy,
+                            bool sparse_out) {
     const unsigned lane = lane_id();
     const bool filtered = a.ld == nullptr;
     const unsigned g = grab_size(ns, ((unsigned long long)gridDim.x * blockDim.x) >> 5);
@@ -241,30 +296,38 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
         float du = 0.0f;
         if (valid) {
             part_range(a, u, heavy, rb, re);
-            du = pack_dist(__ldcg(&a.pack[u]));
-            if (heavy) atomicOr(&a.settled[u >> 5], 1u << (u & 31));
+            const unsigned long long pu = __ldcg(&a.pack[u]);
+            du = pack_dist(pu);
+            if (heavy) settle(a, sparse_out, u, pu);
         }
         const unsigned deg = (unsigned)(re - rb);
         const unsigned incl = warp_incl_scan(deg);
         const unsigned total = __shfl_sync(FULL, incl, 31);
         const unsigned excl = incl - deg;
-        for (unsigned e0 = 0; e0 < total; e0 += 32) {
-            const unsigned e = e0 + lane;
-            bool has = e < total;
-            const int j = warp_owner(excl, has ? e : total - 1);
-            const unsigned uj = __shfl_sync(FULL, u, j);
-            const uint64_t rbj = __shfl_sync(FULL, rb, j);
-            const unsigned exj = __shfl_sync(FULL, excl, j);
-            const float duj = __shfl_sync(FULL, du, j);
-            unsigned v = 0;
-            float wt = 0.0f;
-            if (has) {
-                const uint64_t at = rbj + (e - exj);
-                v = (unsigned)__ldg(&a.col[at]);
-                wt = __ldg(&a.w[at]);
-                if (filtered) has = heavy ? !(wt < a.delta) : wt < a.delta;
+        for (unsigned e0 = 0; e0 < total; e0 += 32 * SSSP_EDGES) {
+            EdgeProbe p;
+#pragma unroll
+            for (int t = 0; t < SSSP_EDGES; ++t) {
+                const unsigned e = e0 + 32 * t + lane;
+                bool has = e < total;
+                const int j = warp_owner(excl, has ? e : total - 1);
+                p.u[t] = __shfl_sync(FULL, u, j);
+                const uint64_t rbj = __shfl_sync(FULL, rb, j);
+                const unsigned exj = __shfl_sync(FULL, excl, j);
+                p.du[t] = __shfl_sync(FULL, du, j);
+                p.v[t] = 0;
+                p.wt[t] = 0.0f;
+                if (has) {
+                    const uint64_t at = rbj + (e - exj);
+                    p.v[t] = (unsigned)__ldg(&a.col[at]);
+                    p.wt[t] = __ldg(&a.w[at]);
+                    if (filtered) has = heavy ? !(p.wt[t] < a.delta) : p.wt[t] < a.delta;
+                }
+                p.has[t] = has;
             }
-            relax(a, x, k, has, uj, duj, v, wt, heavy);
+            probe_edges(a, k, p);
+#pragma unroll
+            for (int t = 0; t < SSSP_EDGES; ++t) relax(a, x, k, p.has[t], p.u[t], p.du[t], p.v[t], p.wt[t], p.cur[t], heavy);
         }
     }
     const unsigned nb = big_count(bp);
@@ -279,21 +342,32 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
         const unsigned first = __ldcg(&B[j]);
         uint64_t rb, re;
         part_range(a, u, heavy, rb, re);
-        const float du = pack_dist(__ldcg(&a.pack[u]));
-        if (heavy && ch == first && lane == 0) atomicOr(&a.settled[u >> 5], 1u << (u & 31));
+        const unsigned long long pu = __ldcg(&a.pack[u]);
+        const float du = pack_dist(pu);
+        if (heavy && ch == first && lane == 0) settle(a, sparse_out, u, pu);
         const uint64_t deg = re - rb;
         const uint64_t cs = (uint64_t)(ch - first) * BIG_CHUNK;
         const uint64_t ce = min(cs + BIG_CHUNK, deg);
-        for (uint64_t e = cs + lane; e < cs + BIG_CHUNK; e += 32) {
-            bool has = e < ce;
-            unsigned v = 0;
-            float wt = 0.0f;
-            if (has) {
-                v = (unsigned)__ldg(&a.col[rb + e]);
-                wt = __ldg(&a.w[rb + e]);
-                if (filtered) has = heavy ? !(wt < a.delta) : wt < a.delta;
+        for (uint64_t e0 = cs + lane; e0 < cs + BIG_CHUNK; e0 += 32 * SSSP_EDGES) {
+            EdgeProbe p;
+#pragma unroll
+            for (int t = 0; t < SSSP_EDGES; ++t) {
+                const uint64_t e = e0 + 32 * t;
+                bool has = e < ce;
+                p.u[t] = u;
+                p.du[t] = du;
+                p.v[t] = 0;
+                p.wt[t] = 0.0f;
+                if (has) {
+                    p.v[t] = (unsigned)__ldg(&a.col[rb + e]);
+                    p.wt[t] = __ldg(&a.w[rb + e]);
+                    if (filtered) has = heavy ? !(p.wt[t] < a.delta) : p.wt[t] < a.delta;
+                }
+                p.has[t] = has;
             }
-            relax(a, x, k, has, u, du, v, wt, heavy);
+            probe_edges(a, k, p);
+#pragma unroll
+            for (int t = 0; t < SSSP_EDGES; ++t) relax(a, x, k, p.has[t], p.u[t], p.du[t], p.v[t], p.wt[t], p.cur[t], heavy);
         }
     }
 }
@@ -321,6 +395,8 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
     unsigned epoch = 0;
     const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+    const bool sparse_out = __ldcg((const unsigned long long *)&a.prefilled->dist) == (unsigned long long)a.dist &&
+                            __ldcg((const unsigned long long *)&a.prefilled->pred) == (unsigned long long)a.pred;
 
     if (!a.roots) {
         if (gtid == 0) {
@@ -416,7 +492,8 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
             x.f_slot = s_nxt;
             x.Fout = a.F[(phase + 1) & 1];
             x.FBout = a.FB[(phase + 1) & 1];
-            expand_list(a, x, cnt, a.F[phase & 1], ns, bp, a.FB[phase & 1], &c->grab[s_cur], &c->cgrab[s_cur], false);
+            expand_list(a, x, cnt, a.F[phase & 1], ns, bp, a.FB[phase & 1], &c->grab[s_cur], &c->cgrab[s_cur], false,
+                        sparse_out);
             stage_flush(a, x, cnt);
             if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
             if (gtid == 0) trace_phase(c, phase, 1, ns + big_count(bp));
@@ -435,7 +512,8 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
             x.FBout = a.FB[(phase + 1) & 1];
             const unsigned ns = ld_volatile(&c->s_small[bucket & 1]);
             const unsigned long long bp = ld_volatile(&c->s_big[bucket & 1]);
-            expand_list(a, x, cnt, a.S[bucket & 1], ns, bp, a.SB[bucket & 1], &c->grab[s_cur], &c->cgrab[s_cur], true);
+            expand_list(a, x, cnt, a.S[bucket & 1], ns, bp, a.SB[bucket & 1], &c->grab[s_cur], &c->cgrab[s_cur], true,
+                        sparse_out);
             stage_flush(a, x, cnt);
             if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
             if (gtid == 0) trace_phase(c, phase, 2, ns + big_count(bp));
@@ -458,20 +536,31 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
         c->buckets = nbuckets;
         c->phases = phase;
     }
+    // Every distance is final (the last heavy phase ended at a grid barrier).
+    // Outputs not pre-filled by the reset are written here in full.
+    if (!sparse_out) {
+        for (uint64_t v = gtid; v < a.n; v += nthreads) {
+            const unsigned long long p = __ldcg(&a.pack[v]);
+            a.dist[v] = p == UNREACHED ? -1.0f : pack_dist(p);
+            a.pred[v] = p == UNREACHED ? -1 : (int64_t)(unsigned)p;
+        }
+    }
 }
 
-__global__ void sssp_export_kernel(const unsigned long long *__restrict__ pack, uint64_t n, float *__restrict__ dist,
-                                   int64_t *__restrict__ pred) {
+// Fills the outputs with "unreached" and records them as pre-filled.
+__global__ void sssp_prefill_kernel(float *__restrict__ dist, int64_t *__restrict__ pred, uint64_t n, SsspOut *hdr) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
-        const unsigned long long p = pack[v];
-        dist[v] = p == UNREACHED ? -1.0f : pack_dist(p);
-        pred[v] = p == UNREACHED ? -1 : (int64_t)(unsigned)p;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint64_t v = t; v < n; v += stride) {
+        dist[v] = -1.0f;
+        pred[v] = -1;
     }
+    if (t == 0) *hdr = SsspOut{dist, pred};
 }
 
 struct SsspWork {
     SsspCtl *ctl;
+    SsspOut *out;
     unsigned long long *pack;
     unsigned *fstamp, *sstamp, *qstamp, *settled;
     unsigned *F[2], *FB[2], *S[2], *SB[2];
@@ -483,6 +572,7 @@ static SsspWork carve_sssp(void *base, uint64_t n) {
     Carver c(base);
     SsspWork w;
     w.ctl = c.take<SsspCtl>(1);
+    w.out = c.take<SsspOut>(1);
     w.pack = c.take<unsigned long long>(n);
     w.fstamp = c.take<unsigned>(n);
     w.sstamp = c.take<unsigned>(n);
@@ -538,12 +628,23 @@ static int sssp_check(const uint64_t *d_rowstarts, const int32_t *d_col, const f
     return G5_OK;
 }
 
-extern "C" int g5_sssp_reset(uint64_t nverts, void *d_work, uint64_t work_bytes, void *stream) {
+extern "C" int g5_sssp_reset(uint64_t nverts, float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes,
+                             void *stream) {
     clear_error();
     G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31) && d_work, "g5_sssp_reset: bad argument");
+    G5_CHECK_ARG((d_dist == nullptr) == (d_pred == nullptr), "g5_sssp_reset: give both outputs or neither");
     SsspWork w = carve_sssp(d_work, nverts);
     if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "g5_sssp_reset: workspace too small");
     cudaStream_t st = (cudaStream_t)stream;
+    if (d_dist) {
+        DeviceInfo di;
+        int rc = device_info(&di);
+        if (rc) return rc;
+        sssp_prefill_kernel<<<di.sms * 8, 256, 0, st>>>(d_dist, d_pred, nverts, w.out);
+        G5_CUDA_TRY(cudaGetLastError());
+    } else {
+        G5_CUDA_TRY(cudaMemsetAsync(w.out, 0, sizeof(SsspOut), st));
+    }
     G5_CUDA_TRY(cudaMemsetAsync(w.pack, 0xff, nverts * sizeof(unsigned long long), st));
     // fstamp, sstamp, qstamp are consecutive carve-outs: one memset.
     G5_CUDA_TRY(cudaMemsetAsync(w.fstamp, 0xff, (char *)(w.qstamp + nverts) - (char *)w.fstamp, st));
@@ -589,16 +690,15 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     }
     a.ring = w.ring;
     a.ctl = w.ctl;
+    a.prefilled = w.out;
+    a.dist = d_dist;
+    a.pred = d_pred;
     a.nblocks = (unsigned)blocks;
     a.limit_ns = wait_limit_ns();
     void *args[] = {&a};
     G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(SsspCtl), st));
     G5_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)sssp_persistent_kernel, dim3(blocks), dim3(SSSP_THREADS),
                                             args, 0, st));
-    DeviceInfo di;
-    if ((rc = device_info(&di))) return rc;
-    sssp_export_kernel<<<di.sms * 8, 256, 0, st>>>(w.pack, nverts, d_dist, d_pred);
-    G5_CUDA_TRY(cudaGetLastError());
     return G5_OK;
 }
 
@@ -630,7 +730,7 @@ extern "C" int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, co
     SsspWork w;
     int rc = sssp_check(d_rowstarts, d_col, d_w, nverts, root, d_dist, d_pred, d_work, work_bytes, &w, "g5_sssp_run");
     if (rc) return rc;
-    if ((rc = g5_sssp_reset(nverts, d_work, work_bytes, stream))) return rc;
+    if ((rc = g5_sssp_reset(nverts, d_dist, d_pred, d_work, work_bytes, stream))) return rc;
     return g5_sssp_traverse(d_rowstarts, d_col, d_w, d_light_deg, light_delta, nverts, root, d_dist, d_pred, d_work,
                             work_bytes, params, stream);
 }

@@ -234,11 +234,17 @@ int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, const float *
                 float light_delta, uint64_t nverts, uint64_t root, float *d_dist, int64_t *d_pred, void *d_work,
                 uint64_t work_bytes, const g5_sssp_params *params, void *stream);
 
-/* g5_sssp_run in two steps, like the reference's oned_graph_sssp_clear +
+/* g5_sssp_run in two steps, like the reference's oned_graph_sssp_clear
+ * (src/traversal.cu:625-636 with sssp_clear_kernel :242-253, which also
+ * set pred to -1 and dist to -1.0f) +
  * oned_graph_sssp_run: g5_sssp_reset clears the workspace's O(N) arrays
- * (distances, stamps, settled bitmap); g5_sssp_traverse zeroes the control
- * block, runs the persistent kernel and writes d_dist / d_pred. */
-int g5_sssp_reset(uint64_t nverts, void *d_work, uint64_t work_bytes, void *stream);
+ * (distances, stamps, settled bitmap) and, when given d_dist and d_pred
+ * (both or neither), fills them with -1.0f / -1; g5_sssp_traverse zeroes
+ * the control block, runs the persistent kernel and writes d_dist / d_pred.
+ * When the traverse gets the same output arrays the reset pre-filled, it
+ * writes only the reached vertices (O(reached) work); otherwise it writes
+ * all nverts entries. */
+int g5_sssp_reset(uint64_t nverts, float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes, void *stream);
 int g5_sssp_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, const uint32_t *d_light_deg,
                      float light_delta, uint64_t nverts, uint64_t root, float *d_dist, int64_t *d_pred, void *d_work,
                      uint64_t work_bytes, const g5_sssp_params *params, void *stream);
