@@ -69,7 +69,7 @@ def _load() -> C.CDLL:
         "g5_sssp_run": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_sssp_last_status": ([p, u64, p, p, p], C.c_int),
         "g5_sssp_reset": ([u64, p, p, p, u64, p], C.c_int),
-        "g5_sssp_last_trace": ([p, u64, p, C.c_int, p, p, p, p, p], C.c_int),
+        "g5_sssp_last_trace": ([p, u64, p, C.c_int, p, p, p, p, p, p], C.c_int),
         "g5_sssp_traverse": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_validate_workspace_size": ([u64, p], C.c_int),
         "g5_edge_count": ([p, p, u64, p, p, u64, p, p], C.c_int),
@@ -122,7 +122,7 @@ class MsBfsStats(C.Structure):
 
 
 class SsspParams(C.Structure):
-    _fields_ = [("delta", C.c_float), ("blocks", C.c_int32)]
+    _fields_ = [("delta", C.c_float), ("blocks", C.c_int32), ("pull", C.c_float), ("sub_min", C.c_int32)]
 
 
 def _ptr(t: torch.Tensor | None) -> int | None:
@@ -392,10 +392,10 @@ def oned_graph_bfs_traverse_multi(g: OnedGraph, bfs: "BfsState", d_roots: torch.
 
 
 def oned_graph_sssp_traverse_multi(g: OnedGraph, sssp: "SsspState", d_roots: torch.Tensor, delta: float = 0.1,
-                                   blocks: int = 0, stream=None) -> None:
+                                   blocks: int = 0, pull: float = 0.0, sub_min: int = 0, stream=None) -> None:
     """SSSP from every source in d_roots at once (g5_sssp_traverse_multi);
     reset sssp first."""
-    p = SsspParams(delta, blocks)
+    p = SsspParams(delta, blocks, pull, sub_min)
     _check(lib.g5_sssp_traverse_multi(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
                                       g.nglobalverts, _ptr(d_roots), d_roots.numel(), _ptr(sssp.dist),
                                       _ptr(sssp.pred), _ptr(sssp.work), sssp.work.numel(), C.byref(p),
@@ -409,9 +409,11 @@ class PackedBatch:
     per-graph launches, no host work between them)."""
 
     def __init__(self, pk: PackedGraphs, delta: float = 0.1, capture: bool = True, with_depth: bool = True,
-                 bfs_params: BfsParams | None = None, sssp_blocks: int = 0):
+                 bfs_params: BfsParams | None = None, sssp_blocks: int = 0, sssp_pull: float = 0.0,
+                 sssp_sub_min: int = 0):
         self.pk, self.delta, self.with_depth = pk, delta, with_depth
         self.bfs_params, self.sssp_blocks = bfs_params, sssp_blocks
+        self.sssp_pull, self.sssp_sub_min = sssp_pull, sssp_sub_min
         self.bfs = BfsState(pk.g)
         self.sssp = SsspState(pk.g)
         self.stream = torch.cuda.Stream(device=pk.g.device)
@@ -433,7 +435,8 @@ class PackedBatch:
 
     def _enqueue_sssp(self):
         oned_graph_sssp_reset(self.sssp)
-        oned_graph_sssp_traverse_multi(self.pk.g, self.sssp, self.pk.d_roots, self.delta, self.sssp_blocks)
+        oned_graph_sssp_traverse_multi(self.pk.g, self.sssp, self.pk.d_roots, self.delta, self.sssp_blocks,
+                                       self.sssp_pull, self.sssp_sub_min)
 
     def run(self) -> None:
         """Enqueues one batch on self.stream (replaying the graph when captured)."""
@@ -719,9 +722,9 @@ def oned_graph_sssp_create(g: OnedGraph) -> SsspState:
 
 
 def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,
-                        stream=None) -> None:
+                        pull: float = 0.0, sub_min: int = 0, stream=None) -> None:
     """oned_graph_sssp_run (src/traversal.h:52), delta 0.1 as the reference."""
-    p = SsspParams(delta, blocks)
+    p = SsspParams(delta, blocks, pull, sub_min)
     _check(lib.g5_sssp_run(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
                            g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                            sssp.work.numel(), C.byref(p), _stream(stream)))
@@ -737,12 +740,12 @@ def oned_graph_sssp_reset(sssp: SsspState, stream=None) -> None:
 
 
 def oned_graph_sssp_traverse(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,
-                             stream=None) -> None:
+                             pull: float = 0.0, sub_min: int = 0, stream=None) -> None:
     """The search itself, on a reset state (one block for a root outside the
     main component)."""
     if blocks == 0 and not g.in_main_component(root):
         blocks = 1
-    p = SsspParams(delta, blocks)
+    p = SsspParams(delta, blocks, pull, sub_min)
     _check(lib.g5_sssp_traverse(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
                                 g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                                 sssp.work.numel(), C.byref(p), _stream(stream)))
@@ -751,17 +754,18 @@ def oned_graph_sssp_traverse(g: OnedGraph, sssp: SsspState, root: int, delta: fl
 def sssp_trace(sssp: SsspState, stream=None) -> dict:
     """Counters and per-phase trace of the last SSSP on this state."""
     k = 256
-    counts = np.zeros(6, np.uint64)
+    counts = np.zeros(7, np.uint64)
     kind = np.zeros(k, np.int32)
     size = np.zeros(k, np.uint64)
     ms = np.zeros(k, np.float64)
+    edges = np.zeros(k, np.uint64)
     n = C.c_int32()
     _check(lib.g5_sssp_last_trace(_ptr(sssp.work), sssp.work.numel(), counts.ctypes.data, k, kind.ctypes.data,
-                                  size.ctypes.data, ms.ctypes.data, C.byref(n), _stream(stream)))
+                                  size.ctypes.data, ms.ctypes.data, edges.ctypes.data, C.byref(n), _stream(stream)))
     m = min(n.value, k)
-    names = ["edges", "settled_skips", "atomics", "improved", "ring_pushes", "frontier_pushes"]
+    names = ["edges", "settled_skips", "atomics", "improved", "ring_pushes", "frontier_pushes", "pulls"]
     return {"counts": dict(zip(names, counts.tolist())), "phases": n.value, "kind": kind[:m].tolist(),
-            "size": size[:m].tolist(), "ms": ms[:m].tolist()}
+            "size": size[:m].tolist(), "ms": ms[:m].tolist(), "edges": edges[:m].tolist()}
 
 
 def sssp_status(sssp: SsspState, stream=None) -> tuple[int, int]:

@@ -72,24 +72,28 @@ def tune_bfs(g: OnedGraph, roots, alphas=(6.0, 10.0, 14.0, 20.0, 28.0), betas=(1
             "candidates": len(table)}
 
 
-def tune_sssp(g: OnedGraph, roots, deltas=(0.08, 0.1, 0.2, 0.4), grids=None, reps: int = 1) -> dict:
-    """Best (delta, blocks) for SSSP over `roots` (a list: one search each;
-    a device tensor: one multi-source search)."""
+def tune_sssp(g: OnedGraph, roots, deltas=(0.08, 0.1, 0.2, 0.4), grids=None, pulls=(0.0, -1.0), subs=(0, -1),
+              reps: int = 1) -> dict:
+    """Best (delta, blocks, pull, sub_min) for SSSP over `roots` (a list: one
+    search each; a device tensor: one multi-source search).  pull / sub_min
+    are g5_sssp_params' heavy-phase pull threshold and sub-bucket threshold
+    (0 = the library's default, -1 = off)."""
     st = SsspState(g)
     grids = _grids("sssp", g.nglobalverts) if grids is None else list(grids)
     table = []
-    for delta, blocks in itertools.product(deltas, grids):
+    for delta, blocks, pull, sub in itertools.product(deltas, grids, pulls, subs):
         ms = 0.0
         for _ in range(reps):
             for r in _searches(roots):
                 if isinstance(r, torch.Tensor):
-                    run = lambda: oned_graph_sssp_traverse_multi(g, st, r, delta, blocks)  # noqa: E731
+                    run = lambda: oned_graph_sssp_traverse_multi(g, st, r, delta, blocks, pull, sub)  # noqa: E731
                 else:
-                    run = lambda: oned_graph_sssp_traverse(g, st, r, delta, blocks)  # noqa: E731
+                    run = lambda: oned_graph_sssp_traverse(g, st, r, delta, blocks, pull, sub)  # noqa: E731
                 ms += _timed(run, lambda: oned_graph_sssp_reset(st))
-        table.append((ms / reps, delta, blocks))
+        table.append((ms / reps, delta, blocks, pull, sub))
     best = min(table)
-    return {"kind": "sssp", "delta": best[1], "blocks": best[2], "ms": round(best[0], 4), "candidates": len(table)}
+    return {"kind": "sssp", "delta": best[1], "blocks": best[2], "pull": best[3], "sub_min": best[4],
+            "ms": round(best[0], 4), "candidates": len(table)}
 
 
 def tune_msbfs(g: OnedGraph, roots, alphas=(8.0, 16.0, 32.0, 64.0), checks=(0, 1, 2), grids=None,

@@ -8,7 +8,10 @@
 // float32 exactly as the reference's `bucket_max += delta`, light edges
 // (w < delta) relaxed to a fixed point inside a bucket before its heavy
 // edges.  With non-negative weights the float fixed point is unique, so the
-// distances equal the reference's bit for bit.
+// distances equal the reference's bit for bit, whatever the bucket width and
+// the order of relaxations -- which lets the kernel use a light threshold
+// above the bucket width (the CSR's light/heavy split at 0.1 serves every
+// width up to 0.1) and pull instead of push in large heavy phases.
 //
 // Device-side structure:
 //   * dist and parent packed in one u64 (float bits << 32 | parent); a
@@ -37,31 +40,66 @@
 namespace g5 {
 
 constexpr int SSSP_THREADS = 256;
-constexpr int RING = 16;  // bucket queues; a relaxation may land at most RING-1 buckets ahead
-constexpr unsigned STAGE_F = 256;    // per-warp staging: frontier
-constexpr unsigned STAGE_S = 256;    //                   heavy set
-constexpr unsigned STAGE_R = 32;     //                   each ring queue
+constexpr int RING = 32;  // bucket queues; a relaxation may land at most RING-1 buckets ahead
+constexpr unsigned STAGE_F = 128;    // per-warp staging: frontier
+constexpr unsigned STAGE_S = 128;    //                   heavy set
+constexpr unsigned STAGE_R = 16;     //                   each ring queue
+constexpr unsigned STAGE_Q = 16;     //                   each sub-bucket queue
+// stage_append takes up to 32 entries at once; the ring and sub-bucket
+// slices are smaller and use stage_push, which writes through when full.
+static_assert(STAGE_F >= 32 && STAGE_S >= 32, "staging slices hold one warp step");
+static_assert(STAGE_R <= 32 && STAGE_Q <= 32, "stage_push writes a full slice with one lane per entry");
 constexpr int SSSP_TRACE = 256;      // phases recorded in the control block
+// Sub-buckets: once a bucket's light frontier holds SPLIT_MIN light entries,
+// the rest of the bucket is processed in SUB equal sub-buckets in order
+// (delta-stepping with width delta/SUB for the light edges, nested in the
+// bucket), so a vertex is expanded again only when its distance drops
+// within its sub-bucket.  On Kronecker graphs the bucket that holds the
+// hubs' neighbourhood has most vertices at nearly equal distances; without
+// this every one of them is re-expanded several times.
+constexpr int SUB = 32;
+constexpr unsigned long long SPLIT_MIN = 1ull << 25;  // default; g5_sssp_params.sub_min overrides
+constexpr float SSSP_PULL_RATIO = 1.0f;  // default heavy-phase pull threshold
 constexpr unsigned long long UNREACHED = ~0ull;
 
+// List sizes that every block reads after a grid barrier.  They lead the
+// control block, and each block copies them into shared memory once per
+// barrier (a few warps, one load per word) instead of every warp reading
+// the same words from L2.
+struct SsspSnap {
+    unsigned long long f_big[3];      // per phase slot: frontier produced for the next phase (big part)
+    // Heavy set (vertices settled by the bucket) per bucket slot: the
+    // bucket opened i-th uses slot i % 3, cleared when bucket i-1 opens.
+    unsigned long long s_big[3];
+    unsigned long long s_entries[3];  // CSR entries of the heavy set's rows
+    unsigned long long f_entries[3];  // light CSR entries of the frontier's rows
+    unsigned long long pl_big;        // heavy-phase pull: rows too long for one warp
+    unsigned f_small[3];
+    unsigned s_small[3];
+    unsigned ring_len[RING];
+    unsigned fq_len[SUB];  // sub-bucket queues of the current bucket
+};
+constexpr int SNAP_WORDS = (int)(sizeof(SsspSnap) / 4);
+
 struct SsspCtl {
+    SsspSnap sn;  // first: copied as words 0 .. SNAP_WORDS-1
     unsigned bar;
     unsigned error;
     unsigned grab[3];    // per phase slot: cursor over the input list's small part
     unsigned cgrab[3];   //                 cursor over the input list's big-part chunks
-    unsigned f_small[3]; // per phase slot: frontier produced for the next phase
-    unsigned long long f_big[3];
-    unsigned s_small[2]; // per bucket parity: heavy set
-    unsigned long long s_big[2];
-    unsigned ring_len[RING];
+    unsigned pl_small, pl_cgrab;  // heavy-phase pull: long-row list
+    unsigned long long pulls;
+    unsigned long long splits;
     unsigned long long buckets;
     unsigned long long phases;
     // counters: edges looked at, skipped as settled, atomicMin issued,
     // distances lowered, ring and frontier pushes
     unsigned long long n_edges, n_settled, n_atomic, n_improved, n_ring, n_front;
-    // per-phase trace: end time, kind (0 open, 1 light, 2 heavy), input size
+    // per-phase trace: end time, kind (0 open, 1 light, 2 heavy push, 3
+    // heavy pull), input size, edges looked at so far
     unsigned long long t0;
     unsigned long long t_phase[SSSP_TRACE];
+    unsigned long long e_phase[SSSP_TRACE];
     unsigned n_phase[SSSP_TRACE];
     unsigned char kind_phase[SSSP_TRACE];
 };
@@ -85,13 +123,18 @@ struct SsspArgs {
     unsigned root;
     const uint64_t *roots;  // several sources at once (device array) instead of `root`, or nullptr
     unsigned nroots;
-    float delta;
+    float delta;       // bucket width
+    float light;       // light edges: w < light (light >= delta)
+    float pull_ratio;  // heavy phase pulls when its rows' entries >= pull_ratio x unsettled rows' entries; <= 0 never
+    unsigned long long split_min;  // frontier light entries that start sub-buckets (~0: never)
     unsigned long long *pack;
     unsigned *fstamp, *sstamp, *qstamp;
     unsigned *settled;
+    unsigned *cur;           // bitmap of the bucket being pulled from (heavy pull only)
     unsigned *F[2], *FB[2];  // frontiers and the chunk bases of their big parts
     unsigned *S[2], *SB[2];  // heavy sets and chunk bases
     unsigned *ring;
+    unsigned *fq;  // SUB sub-bucket queues of n entries
     SsspCtl *ctl;
     const SsspOut *prefilled;
     float *dist;
@@ -130,11 +173,15 @@ struct Stage {
     WarpStage f, s;
     unsigned *rbuf;  // RING * STAGE_R, this warp's
     unsigned *rcnt;  // RING, this warp's
+    unsigned *qbuf;  // SUB * STAGE_Q, this warp's
+    unsigned *qcnt;  // SUB, this warp's
+    unsigned long long *bcnt;  // 8 event counts of the block (shared); [7] = frontier light entries
 };
 
 // Per-thread event counts, summed into the control block once per phase.
 struct Counts {
-    unsigned long long edges, settled, atomics, improved, ring, front;
+    unsigned edges, settled, atomics, improved, ring, front;  // per thread and phase: far below 2^32
+    unsigned long long s_entries;
 };
 
 struct PushCtx {
@@ -144,25 +191,111 @@ struct PushCtx {
     int f_slot;          // counter slot of the produced frontier
     unsigned *Fout, *FBout;
     unsigned *Sl, *SBl;  // heavy set of the current bucket
-    int s_par;
+    int s_slot;
     const float *bnd;    // shared: b_B .. b_{B+RING}
+    const float *sub;    // shared: sub-bucket bounds t_0 = b_B .. t_SUB = b_{B+1}
+    float sub_hi;        // upper bound of the light frontier's range (t_{j+1}, or b_{B+1})
+    bool sub_mode;       // the bucket is processed by sub-buckets
 };
+
+// Sub-bucket queue stamp of (bucket, j), kept apart from bucket-ring stamps
+// (bucket numbers) by the top bit.
+__device__ __forceinline__ unsigned fine_id(unsigned bucket, int j) {
+    return 0x80000000u | ((bucket * (unsigned)SUB + (unsigned)j) % 0x7fffffffu);
+}
+
+// Largest j in [0, SUB) with t_j <= d, for d in [t_0, t_SUB).
+__device__ __forceinline__ int sub_index(const float *t, float d) {
+    int j = 0;
+#pragma unroll
+    for (int step = SUB / 2; step > 0; step >>= 1)
+        if (t[j + step] <= d) j += step;
+    return j;
+}
 
 // Appends v to the produced frontier and to the bucket's heavy set (each at
 // most once).  All 32 lanes call it.
-__device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCtx &x, bool want, unsigned v) {
+__device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCtx &x, Counts &k, bool want_f,
+                                                 bool want_s, unsigned v) {
     SsspCtl *c = a.ctl;
-    bool f = want && atomicExch(&a.fstamp[v], x.pid) != x.pid;
-    bool s = want && atomicExch(&a.sstamp[v], x.bucket) != x.bucket;
+    bool f = want_f && atomicExch(&a.fstamp[v], x.pid) != x.pid;
+    bool s = want_s && atomicExch(&a.sstamp[v], x.bucket) != x.bucket;
     uint64_t lb = 0, le = 0, hb = 0, he = 0;
-    if (f) part_range(a, v, false, lb, le);
-    if (s) part_range(a, v, true, hb, he);
+    if (f || s) {
+        const uint64_t b = __ldg(&a.rowptr[v]), e = __ldg(&a.rowptr[v + 1]);
+        const uint64_t mid = a.ld ? b + __ldg(&a.ld[v]) : e;
+        if (f) {
+            lb = b;
+            le = mid;
+        }
+        if (s) {
+            hb = a.ld ? mid : b;
+            he = e;
+            k.s_entries += e - b;
+        }
+    }
+    // Light entries of the produced frontier, summed per block (they decide
+    // whether the bucket goes on by sub-buckets).
+    const unsigned long long fe = warp_sum((unsigned long long)(le - lb));
+    if (lane_id() == 0 && fe) atomicAdd(&x.st.bcnt[7], fe);
     // Each vertex enters a frontier once per phase and a heavy set once per
     // bucket, so no list exceeds n entries.
-    bool ok = frontier_append_staged(x.st.f, x.Fout, x.FBout, a.n, &c->f_small[x.f_slot], &c->f_big[x.f_slot], f, v,
+    bool ok = frontier_append_staged(x.st.f, x.Fout, x.FBout, a.n, &c->sn.f_small[x.f_slot], &c->sn.f_big[x.f_slot], f, v,
                                      le - lb);
-    ok &= frontier_append_staged(x.st.s, x.Sl, x.SBl, a.n, &c->s_small[x.s_par], &c->s_big[x.s_par], s, v, he - hb);
+    ok &= frontier_append_staged(x.st.s, x.Sl, x.SBl, a.n, &c->sn.s_small[x.s_slot], &c->sn.s_big[x.s_slot], s, v, he - hb);
     if (!ok) atomicOr(&c->error, DEVERR_CAPACITY);
+}
+
+// Appends v for every lane with `want` to a warp's staging slice of any
+// capacity: entries wait in the slice while they fit; otherwise the slice
+// and this step's entries go to the global list together under one
+// atomicAdd.  A hot queue (all warps pushing to the same few bucket or
+// sub-bucket queues) then costs one global atomic per slice-full, not per
+// warp step.  All 32 lanes call it.
+__device__ __forceinline__ bool stage_push(const WarpStage &q, bool want, unsigned v, unsigned *L, uint64_t n,
+                                           unsigned *gcount) {
+    const unsigned mask = __ballot_sync(FULL, want);
+    if (!mask) return true;
+    const unsigned c = *q.cnt;
+    const unsigned k = __popc(mask);
+    const unsigned rank = __popc(mask & lanemask_lt());
+    bool ok = true;
+    if (c + k <= q.cap) {
+        if (want) q.buf[c + rank] = v;
+    } else {
+        unsigned base = 0;
+        if (lane_id() == 0) base = atomicAdd(gcount, c + k);
+        base = __shfl_sync(FULL, base, 0);
+        ok = (uint64_t)base + c + k <= n;
+        if (ok) {
+            if (lane_id() < c) L[base + lane_id()] = q.buf[lane_id()];
+            if (want) L[base + c + rank] = v;
+        }
+    }
+    __syncwarp();
+    if (lane_id() == 0) *q.cnt = c + k <= q.cap ? c + k : 0u;
+    __syncwarp();
+    return ok;
+}
+
+// Appends v to sub-bucket queue j of the current bucket (lanes with j >= 0),
+// once per (vertex, sub-bucket).  Lanes with the same j append together
+// with one atomicAdd.  All 32 lanes call it.
+__device__ __forceinline__ void push_fine(const SsspArgs &a, const PushCtx &x, int j, unsigned v) {
+    const unsigned id = j >= 0 ? fine_id(x.bucket, j) : 0u;
+    const bool r = j >= 0 && atomicExch(&a.qstamp[v], id) != id;
+    unsigned todo = __ballot_sync(FULL, r);
+    while (todo) {
+        const int q = __shfl_sync(FULL, j, __ffs(todo) - 1);
+        const bool mine = r && j == q;
+        const unsigned m = __ballot_sync(FULL, mine);
+        // A vertex enters each sub-bucket queue at most once per bucket, so
+        // no queue exceeds n entries.
+        WarpStage st{x.st.qbuf + q * STAGE_Q, x.st.qcnt + q, STAGE_Q};
+        if (!stage_push(st, mine, v, a.fq + (uint64_t)q * a.n, a.n, &a.ctl->sn.fq_len[q]))
+            atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+        todo &= ~m;
+    }
 }
 
 // Edges of one warp step, E per lane: their target vertices' settled bits
@@ -180,8 +313,11 @@ struct EdgeProbe {
 };
 
 // Fills p.cur for the edges in p (settled targets and non-vertices get
-// UNREACHED-free zero so relax() skips them).
-__device__ __forceinline__ void probe_edges(const SsspArgs &a, Counts &k, EdgeProbe &p) {
+// UNREACHED-free zero so relax() skips them).  In light phases most targets
+// are not settled, so the settled bits and the distances are loaded
+// together (one memory round trip); in heavy phases most targets are
+// settled, so a distance is loaded only after its bit says it is needed.
+__device__ __forceinline__ void probe_edges(const SsspArgs &a, Counts &k, EdgeProbe &p, bool heavy) {
     unsigned sw[SSSP_EDGES];
 #pragma unroll
     for (int t = 0; t < SSSP_EDGES; ++t) {
@@ -191,34 +327,35 @@ __device__ __forceinline__ void probe_edges(const SsspArgs &a, Counts &k, EdgePr
             p.has[t] = false;
         }
         sw[t] = p.has[t] ? __ldcg(&a.settled[p.v[t] >> 5]) : 0u;
+        p.cur[t] = p.has[t] && !heavy ? __ldcg(&a.pack[p.v[t]]) : 0ull;
     }
 #pragma unroll
     for (int t = 0; t < SSSP_EDGES; ++t) {
         const bool settled = (sw[t] >> (p.v[t] & 31)) & 1u;
         k.settled += p.has[t] && settled;
         p.has[t] = p.has[t] && !settled;
-        p.cur[t] = p.has[t] ? __ldcg(&a.pack[p.v[t]]) : 0ull;
+        if (heavy) p.cur[t] = p.has[t] ? __ldcg(&a.pack[p.v[t]]) : 0ull;
     }
 }
 
-// Relaxes u -> v with float weight wt from distance du (cur = v's packed
-// value read by probe_edges); queues v when its distance dropped.  All 32
-// lanes call it (want = lane has an edge to a vertex not settled).
-__device__ __forceinline__ void relax(const SsspArgs &a, const PushCtx &x, Counts &k, bool want, unsigned u, float du,
-                                      unsigned v, float wt, unsigned long long cur, bool heavy_phase) {
+// Offers v the packed distance/parent np (cur = v's packed value as last
+// read); queues v when its distance dropped.  All 32 lanes call it (want =
+// lane has a candidate for a vertex not settled).
+__device__ __forceinline__ void lower(const SsspArgs &a, const PushCtx &x, Counts &k, bool want, unsigned v,
+                                      unsigned long long np, unsigned long long cur, bool heavy_phase) {
     bool same = false;
-    int target = -1;
+    int target = -1, fine = -1;
     if (want) {
-        const float cand = __fadd_rn(du, wt);
-        const unsigned long long np = ((unsigned long long)__float_as_uint(cand) << 32) | u;
+        const float cand = pack_dist(np);
         if (np < cur) {
             ++k.atomics;
             const unsigned long long old = atomicMin(&a.pack[v], np);
             if (np < old && (old >> 32) != (np >> 32)) {
                 ++k.improved;
                 if (cand < x.bnd[1]) {
-                    same = true;
                     if (heavy_phase) atomicOr(&a.ctl->error, DEVERR_CAPACITY);  // cannot happen: w >= delta
+                    if (cand < x.sub_hi) same = true;
+                    else fine = sub_index(x.sub, cand);  // a later sub-bucket of this bucket
                 } else {
                     // Largest j with b_{B+j} <= cand; the ring holds B+1 .. B+RING-1.
                     int j = 1;
@@ -229,8 +366,12 @@ __device__ __forceinline__ void relax(const SsspArgs &a, const PushCtx &x, Count
             }
         }
     }
-    if (!__any_sync(FULL, same || target >= 0)) return;  // nothing lowered in this warp step
-    push_same_bucket(a, x, same && !heavy_phase, v);
+    if (!__any_sync(FULL, same || target >= 0 || fine >= 0)) return;  // nothing lowered in this warp step
+    push_same_bucket(a, x, k, same && !heavy_phase, (same || fine >= 0) && !heavy_phase, v);
+    if (x.sub_mode) {
+        push_fine(a, x, heavy_phase ? -1 : fine, v);
+        k.front += fine >= 0;
+    }
     // Ring queue of the target bucket, once per (vertex, bucket), staged in
     // the block's shared memory.
     const bool r = target >= 0 && atomicExch(&a.qstamp[v], (unsigned)target) != (unsigned)target;
@@ -245,32 +386,68 @@ __device__ __forceinline__ void relax(const SsspArgs &a, const PushCtx &x, Count
         const bool mine = r && slot == sl;
         const unsigned m = __ballot_sync(FULL, mine);
         WarpStage q{x.st.rbuf + sl * STAGE_R, x.st.rcnt + sl, STAGE_R};
-        if (!stage_append(q, mine, v, a.ring + (uint64_t)sl * a.n, a.n, &a.ctl->ring_len[sl]))
+        if (!stage_push(q, mine, v, a.ring + (uint64_t)sl * a.n, a.n, &a.ctl->sn.ring_len[sl]))
             atomicOr(&a.ctl->error, DEVERR_CAPACITY);
         todo &= ~m;
     }
 }
 
+// Relaxes u -> v with float weight wt from distance du (cur = v's packed
+// value read by probe_edges).  All 32 lanes call it.
+__device__ __forceinline__ void relax(const SsspArgs &a, const PushCtx &x, Counts &k, bool want, unsigned u, float du,
+                                      unsigned v, float wt, unsigned long long cur, bool heavy_phase) {
+    const float cand = __fadd_rn(du, wt);
+    const unsigned long long np = ((unsigned long long)__float_as_uint(cand) << 32) | u;
+    lower(a, x, k, want, v, np, cur, heavy_phase);
+}
+
 // Writes every staged entry of this warp to its global list and the warp's
-// counts to the control block.  Every warp calls it at the end of a phase.
+// counts to the control block.  Every thread of the block calls it at the
+// end of a phase (it synchronises the block once).
 __device__ void stage_flush(const SsspArgs &a, const PushCtx &x, Counts &k) {
     SsspCtl *c = a.ctl;
     {
-        unsigned long long v[6] = {k.edges, k.settled, k.atomics, k.improved, k.ring, k.front};
-        unsigned long long *dst[6] = {&c->n_edges, &c->n_settled, &c->n_atomic, &c->n_improved, &c->n_ring,
-                                      &c->n_front};
+        unsigned long long v[7] = {k.edges, k.settled, k.atomics, k.improved, k.ring, k.front, k.s_entries};
+        unsigned long long *dst[8] = {&c->n_edges, &c->n_settled, &c->n_atomic, &c->n_improved, &c->n_ring,
+                                      &c->n_front, &c->sn.s_entries[x.s_slot], &c->sn.f_entries[x.f_slot]};
+        // Warp sums meet in the block's shared counters; one thread per
+        // block adds them to the control block (a few hundred global atomics
+        // per phase instead of several per warp on the same words).
 #pragma unroll
-        for (int i = 0; i < 6; ++i) {
+        for (int i = 0; i < 7; ++i) {
             const unsigned long long t = warp_sum(v[i]);
-            if (lane_id() == 0 && t) atomicAdd(dst[i], t);
+            if (lane_id() == 0 && t) atomicAdd(&x.st.bcnt[i], t);
         }
-        k = Counts{0, 0, 0, 0, 0, 0};
+        k = Counts{0, 0, 0, 0, 0, 0, 0ull};
+        __syncthreads();
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (x.st.bcnt[i]) atomicAdd(dst[i], x.st.bcnt[i]);
+                x.st.bcnt[i] = 0;  // the next phase adds after the grid barrier's __syncthreads
+            }
+        }
     }
-    bool ok = stage_flush_warp(x.st.f, x.Fout, a.n, &c->f_small[x.f_slot]);
-    ok &= stage_flush_warp(x.st.s, x.Sl, a.n, &c->s_small[x.s_par]);
-    for (int sl = 0; sl < RING; ++sl) {
+    bool ok = stage_flush_warp(x.st.f, x.Fout, a.n, &c->sn.f_small[x.f_slot]);
+    ok &= stage_flush_warp(x.st.s, x.Sl, a.n, &c->sn.s_small[x.s_slot]);
+    // Only the slices holding entries (one ballot over their counts).
+    static_assert(RING <= 32, "one lane per ring slice");
+    __syncwarp();
+    unsigned todo = __ballot_sync(FULL, lane_id() < RING && x.st.rcnt[lane_id()] != 0);
+    while (todo) {
+        const int sl = __ffs(todo) - 1;
+        todo &= todo - 1;
         WarpStage q{x.st.rbuf + sl * STAGE_R, x.st.rcnt + sl, STAGE_R};
-        ok &= stage_flush_warp(q, a.ring + (uint64_t)sl * a.n, a.n, &c->ring_len[sl]);
+        ok &= stage_flush_warp(q, a.ring + (uint64_t)sl * a.n, a.n, &c->sn.ring_len[sl]);
+    }
+    for (int j0 = 0; x.sub_mode && j0 < SUB; j0 += 32) {
+        todo = __ballot_sync(FULL, j0 + lane_id() < SUB && x.st.qcnt[j0 + lane_id()] != 0);
+        while (todo) {
+            const int j = j0 + __ffs(todo) - 1;
+            todo &= todo - 1;
+            WarpStage q{x.st.qbuf + j * STAGE_Q, x.st.qcnt + j, STAGE_Q};
+            ok &= stage_flush_warp(q, a.fq + (uint64_t)j * a.n, a.n, &c->sn.fq_len[j]);
+        }
     }
     if (!ok && lane_id() == 0) atomicOr(&c->error, DEVERR_CAPACITY);
 }
@@ -283,13 +460,25 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
                             bool sparse_out) {
     const unsigned lane = lane_id();
     const bool filtered = a.ld == nullptr;
-    const unsigned g = grab_size(ns, ((unsigned long long)gridDim.x * blockDim.x) >> 5);
+    const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+    const unsigned wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned g = grab_size(ns, nw);
+    // Each warp's first grab is static (warp wg takes [wg*g, wg*g + g)); the
+    // rest come from the counter, offset past the static range.  A short
+    // list then costs no atomics on the shared counter.
+    bool first = true;
     for (;;) {
-        unsigned base = 0;
-        if (lane == 0) base = atomicAdd(grab, g);
-        base = __shfl_sync(FULL, base, 0);
+        unsigned long long base;
+        if (first) {
+            base = (unsigned long long)wg * g;
+            first = false;
+        } else {
+            unsigned b = 0;
+            if (lane == 0) b = atomicAdd(grab, g);
+            base = (unsigned long long)nw * g + __shfl_sync(FULL, b, 0);
+        }
         if (base >= ns) break;
-        const unsigned i = base + lane;
+        const unsigned long long i = base + lane;
         const bool valid = lane < g && i < ns;
         const unsigned u = valid ? __ldcg(&L[i]) : 0u;
         uint64_t rb = 0, re = 0;
@@ -321,32 +510,39 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
                     const uint64_t at = rbj + (e - exj);
                     p.v[t] = (unsigned)__ldg(&a.col[at]);
                     p.wt[t] = __ldg(&a.w[at]);
-                    if (filtered) has = heavy ? !(p.wt[t] < a.delta) : p.wt[t] < a.delta;
+                    if (filtered) has = heavy ? !(p.wt[t] < a.light) : p.wt[t] < a.light;
                 }
                 p.has[t] = has;
             }
-            probe_edges(a, k, p);
+            probe_edges(a, k, p, heavy);
 #pragma unroll
             for (int t = 0; t < SSSP_EDGES; ++t) relax(a, x, k, p.has[t], p.u[t], p.du[t], p.v[t], p.wt[t], p.cur[t], heavy);
         }
     }
     const unsigned nb = big_count(bp);
     const unsigned long long nch = big_chunks(bp);
+    first = true;
     for (;;) {
-        unsigned ch = 0;
-        if (lane == 0) ch = atomicAdd(cgrab, 1u);
-        ch = __shfl_sync(FULL, ch, 0);
+        unsigned ch;
+        if (first) {
+            ch = wg;
+            first = false;
+        } else {
+            unsigned b = 0;
+            if (lane == 0) b = atomicAdd(cgrab, 1u);
+            ch = nw + __shfl_sync(FULL, b, 0);
+        }
         if (ch >= nch) break;
         const unsigned j = chunk_owner(B, nb, ch);
         const unsigned u = __ldcg(&L[a.n - 1 - j]);
-        const unsigned first = __ldcg(&B[j]);
+        const unsigned cfirst = __ldcg(&B[j]);
         uint64_t rb, re;
         part_range(a, u, heavy, rb, re);
         const unsigned long long pu = __ldcg(&a.pack[u]);
         const float du = pack_dist(pu);
-        if (heavy && ch == first && lane == 0) settle(a, sparse_out, u, pu);
+        if (heavy && ch == cfirst && lane == 0) settle(a, sparse_out, u, pu);
         const uint64_t deg = re - rb;
-        const uint64_t cs = (uint64_t)(ch - first) * BIG_CHUNK;
+        const uint64_t cs = (uint64_t)(ch - cfirst) * BIG_CHUNK;
         const uint64_t ce = min(cs + BIG_CHUNK, deg);
         for (uint64_t e0 = cs + lane; e0 < cs + BIG_CHUNK; e0 += 32 * SSSP_EDGES) {
             EdgeProbe p;
@@ -361,14 +557,213 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
                 if (has) {
                     p.v[t] = (unsigned)__ldg(&a.col[rb + e]);
                     p.wt[t] = __ldg(&a.w[rb + e]);
-                    if (filtered) has = heavy ? !(p.wt[t] < a.delta) : p.wt[t] < a.delta;
+                    if (filtered) has = heavy ? !(p.wt[t] < a.light) : p.wt[t] < a.light;
                 }
                 p.has[t] = has;
             }
-            probe_edges(a, k, p);
+            probe_edges(a, k, p, heavy);
 #pragma unroll
             for (int t = 0; t < SSSP_EDGES; ++t) relax(a, x, k, p.has[t], p.u[t], p.du[t], p.v[t], p.wt[t], p.cur[t], heavy);
         }
+    }
+}
+
+// Grid barrier, then a copy of the control block's list sizes into the
+// block's shared snapshot (SNAP_WORDS threads, one word each).  Every read
+// of those sizes after a barrier uses the snapshot.
+__device__ __forceinline__ bool sssp_sync(const SsspArgs &a, unsigned &epoch, SsspSnap *sp) {
+    if (!grid_sync(&a.ctl->bar, &a.ctl->error, epoch, a.nblocks, a.limit_ns)) return false;
+    static_assert(SNAP_WORDS <= SSSP_THREADS, "one word per thread");
+    if (threadIdx.x < SNAP_WORDS)
+        ((unsigned *)sp)[threadIdx.x] = ld_volatile(&((const unsigned *)&a.ctl->sn)[threadIdx.x]);
+    __syncthreads();
+    return true;
+}
+
+// ---- heavy-phase pull -------------------------------------------------------
+// When a bucket's rows hold at least pull_ratio times the CSR entries of the
+// rows of all vertices not settled yet, its heavy phase runs the other way
+// round: every unsettled vertex v scans its own heavy entries (u, w) -- the
+// same undirected edges, stored in both rows -- and keeps the smallest
+// (fl(d_u + w), u) over the u settled in this bucket.  That is the value the
+// pushes from the bucket would leave in pack[v] (their atomicMin sees the
+// same candidates), so the distances and parents are the same, but the work
+// is proportional to the unsettled vertices' rows, which after the first
+// large buckets are a small part of the graph.  Rows with more than BIG_DEG
+// heavy entries are cut into BIG_CHUNK chunks taken by warps from one
+// grid-wide counter, as in the frontier lists.
+
+constexpr int PULL_EDGES = 2;
+
+// Marks every vertex of the heavy set settled (outputs written when
+// pre-filled) and sets its bit in `cur`.
+__device__ void pull_settle(const SsspArgs &a, bool sparse_out, const unsigned *L, unsigned ns,
+                            unsigned long long bp) {
+    const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t total = (uint64_t)ns + big_count(bp);
+    for (uint64_t i = gtid; i < total; i += nthreads) {
+        const unsigned u = __ldcg(&L[i < ns ? i : a.n - 1 - (i - ns)]);
+        settle(a, sparse_out, u, __ldcg(&a.pack[u]));
+        atomicOr(&a.cur[u >> 5], 1u << (u & 31));
+    }
+}
+
+// Candidates of PULL_EDGES heavy entries (u[t], w[t]) for their row's
+// vertex: (fl(d_u + w), u) when u is in `cur`, UNREACHED otherwise.  The
+// bitmap probes, then the distance loads, are issued together.
+__device__ __forceinline__ void pull_probe(const SsspArgs &a, Counts &k, const unsigned *u, const float *w,
+                                           const bool *has, unsigned long long *cand) {
+    unsigned cw[PULL_EDGES];
+#pragma unroll
+    for (int t = 0; t < PULL_EDGES; ++t) {
+        bool ok = has[t];
+        k.edges += ok;
+        if (ok && u[t] >= a.n) {  // not a vertex: report it, touch nothing
+            atomicOr(&a.ctl->error, DEVERR_RANGE);
+            ok = false;
+        }
+        cw[t] = ok ? (__ldcg(&a.cur[u[t] >> 5]) >> (u[t] & 31)) & 1u : 0u;
+    }
+    unsigned long long pu[PULL_EDGES];
+#pragma unroll
+    for (int t = 0; t < PULL_EDGES; ++t) pu[t] = cw[t] ? __ldcg(&a.pack[u[t]]) : UNREACHED;
+#pragma unroll
+    for (int t = 0; t < PULL_EDGES; ++t) {
+        const float c = __fadd_rn(pack_dist(pu[t]), w[t]);
+        cand[t] = cw[t] ? ((unsigned long long)__float_as_uint(c) << 32) | u[t] : UNREACHED;
+    }
+}
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long x) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) x = min(x, __shfl_xor_sync(FULL, x, d));
+    return x;
+}
+
+// Pull over every 32-vertex word of the settled bitmap: rows of at most
+// BIG_DEG heavy entries are gathered by the word's warp (their entries
+// walked 32 x PULL_EDGES at a time, each lane's candidates folded into its
+// row's slot of s_best with a shared-memory atomicMin); longer rows go to
+// the list (LL, LB) for pull_long.
+__device__ void pull_words(const SsspArgs &a, const PushCtx &x, Counts &k, unsigned long long *s_best,
+                           unsigned *LL, unsigned *LB) {
+    SsspCtl *c = a.ctl;
+    const unsigned lane = lane_id();
+    const bool filtered = a.ld == nullptr;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint64_t nwords = (a.n + 31) >> 5;
+    for (uint64_t kw = warp; kw < nwords; kw += nwarps) {
+        const unsigned sw = __ldcg(&a.settled[kw]);
+        if (sw == FULL) continue;  // warp-uniform
+        const uint64_t v = kw * 32 + lane;
+        const bool live = v < a.n && !((sw >> lane) & 1u);
+        uint64_t hb = 0, he = 0;
+        if (live) part_range(a, (unsigned)v, true, hb, he);
+        const uint64_t hdeg = he - hb;
+        const bool longrow = hdeg > BIG_DEG;
+        if (!frontier_append(LL, LB, a.n, &c->pl_small, &c->sn.pl_big, longrow, (unsigned)v, hdeg))
+            atomicOr(&c->error, DEVERR_CAPACITY);
+        const unsigned deg = longrow ? 0u : (unsigned)hdeg;
+        const unsigned incl = warp_incl_scan(deg);
+        const unsigned total = __shfl_sync(FULL, incl, 31);
+        if (total == 0) continue;  // warp-uniform
+        const unsigned excl = incl - deg;
+        s_best[lane] = UNREACHED;
+        __syncwarp();
+        for (unsigned e0 = 0; e0 < total; e0 += 32 * PULL_EDGES) {
+            unsigned u[PULL_EDGES];
+            float w[PULL_EDGES];
+            bool has[PULL_EDGES];
+            int own[PULL_EDGES];
+#pragma unroll
+            for (int t = 0; t < PULL_EDGES; ++t) {
+                const unsigned e = e0 + 32 * t + lane;
+                has[t] = e < total;
+                own[t] = warp_owner(excl, has[t] ? e : total - 1);
+                const uint64_t hbj = __shfl_sync(FULL, hb, own[t]);
+                const unsigned exj = __shfl_sync(FULL, excl, own[t]);
+                u[t] = 0;
+                w[t] = 0.0f;
+                if (has[t]) {
+                    const uint64_t at = hbj + (e - exj);
+                    u[t] = (unsigned)__ldg(&a.col[at]);
+                    w[t] = __ldg(&a.w[at]);
+                    if (filtered) has[t] = !(w[t] < a.light);
+                }
+            }
+            unsigned long long cand[PULL_EDGES];
+            pull_probe(a, k, u, w, has, cand);
+#pragma unroll
+            for (int t = 0; t < PULL_EDGES; ++t)
+                if (cand[t] != UNREACHED) atomicMin(&s_best[own[t]], cand[t]);
+        }
+        __syncwarp();
+        const unsigned long long best = s_best[lane];
+        __syncwarp();  // every lane has read its slot before the next word resets it
+        const bool want = best != UNREACHED;
+        const unsigned long long curv = want ? __ldcg(&a.pack[v]) : 0ull;
+        lower(a, x, k, want, (unsigned)v, best, curv, true);
+    }
+}
+
+// Pull of the long rows listed by pull_words (big part of LL, chunk bases
+// LB): one BIG_CHUNK chunk per warp grab, the chunk's best candidate offered
+// with one atomicMin.
+__device__ void pull_long(const SsspArgs &a, const PushCtx &x, Counts &k, const unsigned *LL, const unsigned *LB,
+                          const SsspSnap *sp) {
+    SsspCtl *c = a.ctl;
+    const unsigned lane = lane_id();
+    const bool filtered = a.ld == nullptr;
+    const unsigned long long bp = sp->pl_big;
+    const unsigned nb = big_count(bp);
+    const unsigned long long nch = big_chunks(bp);
+    const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+    bool first = true;  // first chunk static (the warp's id), then from the counter
+    for (;;) {
+        unsigned ch;
+        if (first) {
+            ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+            first = false;
+        } else {
+            unsigned b = 0;
+            if (lane == 0) b = atomicAdd(&c->pl_cgrab, 1u);
+            ch = nw + __shfl_sync(FULL, b, 0);
+        }
+        if (ch >= nch) break;
+        const unsigned j = chunk_owner(LB, nb, ch);
+        const unsigned v = __ldcg(&LL[a.n - 1 - j]);
+        uint64_t hb, he;
+        part_range(a, v, true, hb, he);
+        const uint64_t cs = (uint64_t)(ch - __ldcg(&LB[j])) * BIG_CHUNK;
+        const uint64_t ce = min(cs + BIG_CHUNK, he - hb);
+        unsigned long long m = UNREACHED;
+        for (uint64_t e0 = cs + lane; e0 < cs + BIG_CHUNK; e0 += 32 * PULL_EDGES) {
+            unsigned u[PULL_EDGES];
+            float w[PULL_EDGES];
+            bool has[PULL_EDGES];
+#pragma unroll
+            for (int t = 0; t < PULL_EDGES; ++t) {
+                const uint64_t e = e0 + 32 * t;
+                has[t] = e < ce;
+                u[t] = 0;
+                w[t] = 0.0f;
+                if (has[t]) {
+                    u[t] = (unsigned)__ldg(&a.col[hb + e]);
+                    w[t] = __ldg(&a.w[hb + e]);
+                    if (filtered) has[t] = !(w[t] < a.light);
+                }
+            }
+            unsigned long long cand[PULL_EDGES];
+            pull_probe(a, k, u, w, has, cand);
+#pragma unroll
+            for (int t = 0; t < PULL_EDGES; ++t) m = min(m, cand[t]);
+        }
+        m = warp_min_u64(m);
+        const bool want = lane == 0 && m != UNREACHED;
+        const unsigned long long curv = want ? __ldcg(&a.pack[v]) : 0ull;
+        lower(a, x, k, want, v, m, curv, true);
     }
 }
 
@@ -377,33 +772,45 @@ __device__ __forceinline__ void trace_phase(SsspCtl *c, unsigned phase, int kind
         c->t_phase[phase] = globaltimer_ns();
         c->kind_phase[phase] = (unsigned char)kind;
         c->n_phase[phase] = size;
+        c->e_phase[phase] = c->n_edges;
     }
 }
 
 __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspArgs a) {
     SsspCtl *c = a.ctl;
     __shared__ float s_bnd[RING + 1];
+    __shared__ float s_sub[SUB + 1];
     constexpr int WARPS = SSSP_THREADS / 32;
     __shared__ unsigned s_fbuf[WARPS][STAGE_F], s_sbuf[WARPS][STAGE_S], s_rbuf[WARPS][RING * STAGE_R];
     __shared__ unsigned s_fcnt[WARPS], s_scnt[WARPS], s_rcnt[WARPS][RING];
+    __shared__ unsigned s_qbuf[WARPS][SUB * STAGE_Q], s_qcnt[WARPS][SUB];
+    __shared__ unsigned long long s_best[WARPS][32];
+    __shared__ unsigned long long s_bcnt[8];
+    __shared__ SsspSnap s_snap;
+    SsspSnap *const sp = &s_snap;
+    if (threadIdx.x < 8) s_bcnt[threadIdx.x] = 0;
+    __syncthreads();
     const unsigned wid = threadIdx.x >> 5;
     if (lane_id() == 0) s_fcnt[wid] = s_scnt[wid] = 0;
     if (lane_id() < RING) s_rcnt[wid][lane_id()] = 0;
+    for (int j = lane_id(); j < SUB; j += 32) s_qcnt[wid][j] = 0;
     __syncwarp();
     const Stage stage{WarpStage{s_fbuf[wid], &s_fcnt[wid], STAGE_F}, WarpStage{s_sbuf[wid], &s_scnt[wid], STAGE_S},
-                      s_rbuf[wid], s_rcnt[wid]};
+                      s_rbuf[wid], s_rcnt[wid], s_qbuf[wid], s_qcnt[wid], s_bcnt};
     unsigned epoch = 0;
     const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
     const bool sparse_out = __ldcg((const unsigned long long *)&a.prefilled->dist) == (unsigned long long)a.dist &&
                             __ldcg((const unsigned long long *)&a.prefilled->pred) == (unsigned long long)a.pred;
+    const unsigned long long e_total = __ldg(&a.rowptr[a.n]);
+    unsigned long long settled_entries = 0;  // CSR entries of the rows of settled vertices
 
     if (!a.roots) {
         if (gtid == 0) {
             a.pack[a.root] = (unsigned long long)a.root;  // distance 0.0f, parent = root
             a.ring[0] = a.root;
             a.qstamp[a.root] = 0;
-            c->ring_len[0] = 1;
+            c->sn.ring_len[0] = 1;
         }
     } else {
         // Several sources (disjoint graphs packed into one CSR, one source
@@ -414,15 +821,15 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
                 atomicOr(&c->error, DEVERR_RANGE);
             } else if (atomicCAS(&a.qstamp[r], 0xffffffffu, 0u) == 0xffffffffu) {
                 a.pack[r] = r;
-                a.ring[atomicAdd(&c->ring_len[0], 1u)] = (unsigned)r;
+                a.ring[atomicAdd(&c->sn.ring_len[0], 1u)] = (unsigned)r;
             }
         }
     }
-    if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+    if (!sssp_sync(a, epoch, sp)) return;
 
     unsigned bucket = 0, phase = 0;
     float blo = 0.0f;
-    Counts cnt{0, 0, 0, 0, 0, 0};
+    Counts cnt{0, 0, 0, 0, 0, 0, 0ull};
     if (gtid == 0) c->t0 = globaltimer_ns();
     unsigned long long nbuckets = 0;
     for (;;) {
@@ -433,29 +840,40 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
                 s_bnd[j] = b;
                 b = __fadd_rn(b, a.delta);
             }
+            // t_j = b_B + j * (delta / SUB): monotone, t_0 = b_B, t_SUB = b_{B+1}.
+            const float wf = a.delta / (float)SUB;
+            for (int j = 0; j < SUB; ++j) s_sub[j] = __fadd_rn(blo, (float)j * wf);
+            s_sub[SUB] = s_bnd[1];
         }
         __syncthreads();
         PushCtx x;
         x.st = stage;
         x.bucket = bucket;
         x.bnd = s_bnd;
-        x.s_par = bucket & 1;
-        x.Sl = a.S[bucket & 1];
-        x.SBl = a.SB[bucket & 1];
+        x.sub = s_sub;
+        x.sub_hi = s_bnd[1];
+        x.sub_mode = false;
+        int sj = -1;  // current sub-bucket in sub mode
+        const int sb = (int)(nbuckets % 3);
+        x.s_slot = sb;
+        x.Sl = a.S[nbuckets & 1];
+        x.SBl = a.SB[nbuckets & 1];
         {
             const int s_nxt = (phase + 1) % 3, s_clr = (phase + 2) % 3;
             if (gtid == 0) {
-                c->grab[s_clr] = c->cgrab[s_clr] = c->f_small[s_clr] = 0;
-                c->f_big[s_clr] = 0;
-                c->s_small[(bucket + 1) & 1] = 0;
-                c->s_big[(bucket + 1) & 1] = 0;
+                c->grab[s_clr] = c->cgrab[s_clr] = c->sn.f_small[s_clr] = 0;
+                c->sn.f_big[s_clr] = c->sn.f_entries[s_clr] = 0;
+                const int sn = (sb + 1) % 3;  // the next bucket's heavy-set slot
+                c->sn.s_small[sn] = 0;
+                c->sn.s_big[sn] = 0;
+                c->sn.s_entries[sn] = 0;
             }
             x.pid = phase;
             x.f_slot = s_nxt;
             x.Fout = a.F[(phase + 1) & 1];
             x.FBout = a.FB[(phase + 1) & 1];
             const unsigned slot = bucket % RING;
-            const unsigned len = ld_volatile(&c->ring_len[slot]);
+            const unsigned len = sp->ring_len[slot];
             const unsigned *R = a.ring + (uint64_t)slot * a.n;
             for (uint64_t base = gtid - lane_id(); base < len; base += nthreads) {
                 const uint64_t i = base + lane_id();
@@ -466,36 +884,101 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
                     const float d = pack_dist(__ldcg(&a.pack[v]));
                     ok = d >= s_bnd[0] && d < s_bnd[1] && !((__ldcg(&a.settled[v >> 5]) >> (v & 31)) & 1u);
                 }
-                push_same_bucket(a, x, ok, v);
+                push_same_bucket(a, x, cnt, ok, ok, v);
             }
             stage_flush(a, x, cnt);
-            if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+            if (!sssp_sync(a, epoch, sp)) return;
             // The queue is consumed; nothing can target this slot again before
             // bucket + RING, which lies beyond every push of this bucket.
             if (gtid == 0) {
-                c->ring_len[slot] = 0;
+                c->sn.ring_len[slot] = 0;
                 trace_phase(c, phase, 0, len);
             }
             ++phase;
         }
-        // ---- light iterations until the bucket's frontier is empty.
+        // ---- light iterations until the bucket's frontier is empty (in sub
+        // mode: until every sub-bucket's frontier is).  Every block reads the
+        // same counters after a barrier, so all take the same branches.
         for (;;) {
             const int s_cur = phase % 3, s_nxt = (phase + 1) % 3, s_clr = (phase + 2) % 3;
-            const unsigned ns = ld_volatile(&c->f_small[s_cur]);
-            const unsigned long long bp = ld_volatile(&c->f_big[s_cur]);
-            if (ns + big_count(bp) == 0) break;
+            const unsigned ns = sp->f_small[s_cur];
+            const unsigned long long bp = sp->f_big[s_cur];
+            const unsigned fsize = ns + big_count(bp);
+            int nj = -1;
+            if (fsize == 0) {
+                if (!x.sub_mode) break;
+                for (int j = sj + 1; j < SUB; ++j)
+                    if (sp->fq_len[j]) {
+                        nj = j;
+                        break;
+                    }
+                if (nj < 0) break;
+            }
             if (gtid == 0) {
-                c->grab[s_clr] = c->cgrab[s_clr] = c->f_small[s_clr] = 0;
-                c->f_big[s_clr] = 0;
+                c->grab[s_clr] = c->cgrab[s_clr] = c->sn.f_small[s_clr] = 0;
+                c->sn.f_big[s_clr] = c->sn.f_entries[s_clr] = 0;
             }
             x.pid = phase;
             x.f_slot = s_nxt;
             x.Fout = a.F[(phase + 1) & 1];
             x.FBout = a.FB[(phase + 1) & 1];
+            if (nj >= 0) {
+                // Open sub-bucket nj: its queue's entries still in its range
+                // become the frontier (they are in the heavy set already).
+                sj = nj;
+                x.sub_hi = s_sub[sj + 1];
+                const unsigned len = sp->fq_len[sj];
+                const unsigned *Q = a.fq + (uint64_t)sj * a.n;
+                for (uint64_t base = gtid - lane_id(); base < len; base += nthreads) {
+                    const uint64_t i = base + lane_id();
+                    bool ok = false;
+                    unsigned v = 0;
+                    if (i < len) {
+                        v = __ldcg(&Q[i]);
+                        const float d = pack_dist(__ldcg(&a.pack[v]));
+                        ok = d >= s_sub[sj] && d < s_sub[sj + 1];
+                    }
+                    push_same_bucket(a, x, cnt, ok, false, v);
+                }
+                stage_flush(a, x, cnt);
+                if (!sssp_sync(a, epoch, sp)) return;
+                // Nothing is queued into sub-bucket sj once it is open.
+                if (gtid == 0) {
+                    c->sn.fq_len[sj] = 0;
+                    trace_phase(c, phase, 4, len);
+                }
+                ++phase;
+                continue;
+            }
+            if (!x.sub_mode && sp->f_entries[s_cur] >= a.split_min) {
+                // Split: the frontier goes to the sub-bucket queues of its
+                // distances; the bucket continues by sub-buckets in order.
+                x.sub_mode = true;
+                const uint64_t total = (uint64_t)fsize;
+                const unsigned *L = a.F[phase & 1];
+                for (uint64_t base = gtid - lane_id(); base < total; base += nthreads) {
+                    const uint64_t i = base + lane_id();
+                    int j = -1;
+                    unsigned v = 0;
+                    if (i < total) {
+                        v = __ldcg(&L[i < ns ? i : a.n - 1 - (i - ns)]);
+                        j = sub_index(s_sub, pack_dist(__ldcg(&a.pack[v])));
+                    }
+                    push_fine(a, x, j, v);
+                }
+                stage_flush(a, x, cnt);
+                if (!sssp_sync(a, epoch, sp)) return;
+                if (gtid == 0) {
+                    ++c->splits;
+                    trace_phase(c, phase, 5, fsize);
+                }
+                ++phase;
+                continue;
+            }
             expand_list(a, x, cnt, a.F[phase & 1], ns, bp, a.FB[phase & 1], &c->grab[s_cur], &c->cgrab[s_cur], false,
                         sparse_out);
             stage_flush(a, x, cnt);
-            if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
+            if (!sssp_sync(a, epoch, sp)) return;
             if (gtid == 0) trace_phase(c, phase, 1, ns + big_count(bp));
             ++phase;
         }
@@ -503,27 +986,57 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
         {
             const int s_cur = phase % 3, s_nxt = (phase + 1) % 3, s_clr = (phase + 2) % 3;
             if (gtid == 0) {
-                c->grab[s_clr] = c->cgrab[s_clr] = c->f_small[s_clr] = 0;
-                c->f_big[s_clr] = 0;
+                c->grab[s_clr] = c->cgrab[s_clr] = c->sn.f_small[s_clr] = 0;
+                c->sn.f_big[s_clr] = c->sn.f_entries[s_clr] = 0;
             }
             x.pid = phase;
             x.f_slot = s_nxt;
             x.Fout = a.F[(phase + 1) & 1];
             x.FBout = a.FB[(phase + 1) & 1];
-            const unsigned ns = ld_volatile(&c->s_small[bucket & 1]);
-            const unsigned long long bp = ld_volatile(&c->s_big[bucket & 1]);
-            expand_list(a, x, cnt, a.S[bucket & 1], ns, bp, a.SB[bucket & 1], &c->grab[s_cur], &c->cgrab[s_cur], true,
-                        sparse_out);
-            stage_flush(a, x, cnt);
-            if (!grid_sync(&c->bar, &c->error, epoch, a.nblocks, a.limit_ns)) return;
-            if (gtid == 0) trace_phase(c, phase, 2, ns + big_count(bp));
+            const unsigned ns = sp->s_small[sb];
+            const unsigned long long bp = sp->s_big[sb];
+            const unsigned long long s_ent = sp->s_entries[sb];
+            // Every block reads the same counters after the barrier, so all
+            // take the same branch.
+            const bool pull = a.pull_ratio > 0.0f &&
+                              (double)s_ent >= (double)a.pull_ratio * (double)(e_total - settled_entries - s_ent);
+            settled_entries += s_ent;
+            if (!pull) {
+                expand_list(a, x, cnt, x.Sl, ns, bp, x.SBl, &c->grab[s_cur], &c->cgrab[s_cur], true, sparse_out);
+                stage_flush(a, x, cnt);
+                if (!sssp_sync(a, epoch, sp)) return;
+                if (gtid == 0) trace_phase(c, phase, 2, ns + big_count(bp));
+            } else {
+                // The long-row list borrows the other heavy-set array: the
+                // previous bucket is done with it and the next one starts
+                // writing it only after this phase's last barrier.
+                unsigned *LL = a.S[(nbuckets + 1) & 1], *LB = a.SB[(nbuckets + 1) & 1];
+                pull_settle(a, sparse_out, x.Sl, ns, bp);
+                if (!sssp_sync(a, epoch, sp)) return;
+                pull_words(a, x, cnt, s_best[wid], LL, LB);
+                stage_flush(a, x, cnt);
+                if (!sssp_sync(a, epoch, sp)) return;
+                pull_long(a, x, cnt, LL, LB, sp);
+                stage_flush(a, x, cnt);
+                if (!sssp_sync(a, epoch, sp)) return;
+                // `cur` and the long-row counters are next used by a later
+                // bucket's pull, several barriers from here.
+                for (uint64_t i = gtid; i < ((a.n + 31) >> 5); i += nthreads) a.cur[i] = 0;
+                if (gtid == 0) {
+                    c->pl_small = 0;
+                    c->sn.pl_big = 0;
+                    c->pl_cgrab = 0;
+                    ++c->pulls;
+                    trace_phase(c, phase, 3, ns + big_count(bp));
+                }
+            }
             ++phase;
         }
         ++nbuckets;
         // ---- next non-empty bucket within the ring window.
         int step = 0;
         for (int j = 1; j < RING; ++j)
-            if (ld_volatile(&c->ring_len[(bucket + j) % RING])) {
+            if (sp->ring_len[(bucket + j) % RING]) {
                 step = j;
                 break;
             }
@@ -562,9 +1075,10 @@ struct SsspWork {
     SsspCtl *ctl;
     SsspOut *out;
     unsigned long long *pack;
-    unsigned *fstamp, *sstamp, *qstamp, *settled;
+    unsigned *fstamp, *sstamp, *qstamp, *settled, *cur;
     unsigned *F[2], *FB[2], *S[2], *SB[2];
     unsigned *ring;
+    unsigned *fq;
     uint64_t bytes;
 };
 
@@ -578,6 +1092,7 @@ static SsspWork carve_sssp(void *base, uint64_t n) {
     w.sstamp = c.take<unsigned>(n);
     w.qstamp = c.take<unsigned>(n);
     w.settled = c.take<unsigned>((n + 31) / 32);
+    w.cur = c.take<unsigned>((n + 31) / 32);
     for (int i = 0; i < 2; ++i) {
         w.F[i] = c.take<unsigned>(n);
         w.FB[i] = c.take<unsigned>(n);
@@ -585,6 +1100,7 @@ static SsspWork carve_sssp(void *base, uint64_t n) {
         w.SB[i] = c.take<unsigned>(n);
     }
     w.ring = c.take<unsigned>((uint64_t)RING * n);
+    w.fq = c.take<unsigned>((uint64_t)SUB * n);
     w.bytes = c.used;
     return w;
 }
@@ -648,7 +1164,8 @@ extern "C" int g5_sssp_reset(uint64_t nverts, float *d_dist, int64_t *d_pred, vo
     G5_CUDA_TRY(cudaMemsetAsync(w.pack, 0xff, nverts * sizeof(unsigned long long), st));
     // fstamp, sstamp, qstamp are consecutive carve-outs: one memset.
     G5_CUDA_TRY(cudaMemsetAsync(w.fstamp, 0xff, (char *)(w.qstamp + nverts) - (char *)w.fstamp, st));
-    G5_CUDA_TRY(cudaMemsetAsync(w.settled, 0, (nverts + 31) / 32 * sizeof(unsigned), st));
+    // settled and cur are consecutive carve-outs: one memset.
+    G5_CUDA_TRY(cudaMemsetAsync(w.settled, 0, (char *)(w.cur + (nverts + 31) / 32) - (char *)w.settled, st));
     return G5_OK;
 }
 
@@ -659,7 +1176,7 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     SsspWork w;
     int rc = sssp_check(d_rowstarts, d_col, d_w, nverts, root, d_dist, d_pred, d_work, work_bytes, &w, who);
     if (rc) return rc;
-    g5_sssp_params p = {0.1f, 0};
+    g5_sssp_params p = {0.1f, 0, 0.0f, 0};
     if (params) p = *params;
     G5_CHECK_ARG(p.delta > 0.0f, "g5_sssp_traverse: delta must be positive");
     int max_blocks = 0;
@@ -671,17 +1188,25 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     a.rowptr = d_rowstarts;
     a.col = d_col;
     a.w = d_w;
-    a.ld = (d_light_deg && p.delta == light_delta) ? d_light_deg : nullptr;
+    // Rows split at light_delta serve any bucket width up to light_delta:
+    // heavy edges (w >= light_delta >= delta) still land beyond the current
+    // bucket.  A wider bucket filters every row by weight instead.
+    const bool split = d_light_deg && p.delta <= light_delta;
+    a.ld = split ? d_light_deg : nullptr;
+    a.light = split ? light_delta : p.delta;
     a.n = nverts;
     a.root = (unsigned)root;
     a.roots = d_roots;
     a.nroots = nroots;
     a.delta = p.delta;
+    a.pull_ratio = p.pull == 0.0f ? SSSP_PULL_RATIO : p.pull;
+    a.split_min = p.sub_min == 0 ? SPLIT_MIN : p.sub_min < 0 ? ~0ull : (unsigned long long)p.sub_min;
     a.pack = w.pack;
     a.fstamp = w.fstamp;
     a.sstamp = w.sstamp;
     a.qstamp = w.qstamp;
     a.settled = w.settled;
+    a.cur = w.cur;
     for (int i = 0; i < 2; ++i) {
         a.F[i] = w.F[i];
         a.FB[i] = w.FB[i];
@@ -689,6 +1214,7 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
         a.SB[i] = w.SB[i];
     }
     a.ring = w.ring;
+    a.fq = w.fq;
     a.ctl = w.ctl;
     a.prefilled = w.out;
     a.dist = d_dist;
@@ -735,8 +1261,9 @@ extern "C" int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, co
                             work_bytes, params, stream);
 }
 
-extern "C" int g5_sssp_last_trace(const void *d_work, uint64_t work_bytes, uint64_t counts[6], int max_phases,
-                                   int32_t *kind, uint64_t *size, double *phase_ms, int32_t *nphases, void *stream) {
+extern "C" int g5_sssp_last_trace(const void *d_work, uint64_t work_bytes, uint64_t counts[7], int max_phases,
+                                   int32_t *kind, uint64_t *size, double *phase_ms, uint64_t *phase_edges,
+                                   int32_t *nphases, void *stream) {
     clear_error();
     G5_CHECK_ARG(d_work && work_bytes >= sizeof(SsspCtl) && nphases, "g5_sssp_last_trace: bad argument");
     SsspCtl c;
@@ -750,15 +1277,18 @@ extern "C" int g5_sssp_last_trace(const void *d_work, uint64_t work_bytes, uint6
         counts[3] = c.n_improved;
         counts[4] = c.n_ring;
         counts[5] = c.n_front;
+        counts[6] = c.pulls;
     }
     const int n = (int)std::min<unsigned long long>(std::min<unsigned long long>(c.phases, SSSP_TRACE),
                                                      (unsigned long long)std::max(max_phases, 0));
-    unsigned long long prev = c.t0;
+    unsigned long long prev = c.t0, prev_e = 0;
     for (int i = 0; i < n; ++i) {
         if (kind) kind[i] = c.kind_phase[i];
         if (size) size[i] = c.n_phase[i];
         if (phase_ms) phase_ms[i] = (double)(c.t_phase[i] - prev) * 1e-6;
+        if (phase_edges) phase_edges[i] = c.e_phase[i] - prev_e;
         prev = c.t_phase[i];
+        prev_e = c.e_phase[i];
     }
     *nphases = (int32_t)c.phases;
     return deverr_to_status(c.error, "g5_sssp_run");

@@ -220,6 +220,14 @@ int g5_bfs_dist_from_pred(const uint64_t *d_rowstarts, const int32_t *d_col, uin
 typedef struct g5_sssp_params {
     float delta;    /* bucket width (default 0.1, the reference's fixed value) */
     int32_t blocks; /* persistent grid size; 0 = fill the device              */
+    float pull;     /* a bucket's heavy phase pulls (each unsettled vertex scans
+                       its own heavy entries) when the bucket's rows hold at
+                       least pull x the entries of all unsettled vertices'
+                       rows; 0 = default (1.0), < 0 = always push           */
+    int32_t sub_min; /* once a bucket's light frontier holds this many light
+                       CSR entries, the rest of the bucket runs in 32
+                       sub-buckets in distance order; 0 = default (2^25),
+                       < 0 = never                                           */
 } g5_sssp_params;
 
 int g5_sssp_workspace_size(uint64_t nverts, uint64_t *bytes);
@@ -228,8 +236,11 @@ int g5_sssp_workspace_size(uint64_t nverts, uint64_t *bytes);
  * delta-stepping with float32 relaxations.  d_dist[v] = distance, -1.0f when
  * unreached; d_pred[v] = a parent on a shortest path, -1 when unreached.
  * d_light_deg (optional) = per-vertex count of leading row entries lighter
- * than `light_delta` as produced by g5_csr_fill; it is used only when
- * params->delta == light_delta. */
+ * than `light_delta` as produced by g5_csr_fill; it is used when
+ * params->delta <= light_delta (light edges are then those below
+ * light_delta), otherwise rows are filtered by weight against delta.
+ * The bucket ring holds 31 buckets ahead, so delta must exceed
+ * (largest weight) / 30 (G5_ERR_INVALID from the search otherwise). */
 int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, const uint32_t *d_light_deg,
                 float light_delta, uint64_t nverts, uint64_t root, float *d_dist, int64_t *d_pred, void *d_work,
                 uint64_t work_bytes, const g5_sssp_params *params, void *stream);
@@ -263,12 +274,14 @@ int g5_sssp_traverse_multi(const uint64_t *d_rowstarts, const int32_t *d_col, co
 int g5_sssp_last_status(const void *d_work, uint64_t work_bytes, uint64_t *buckets, uint64_t *phases, void *stream);
 
 /* Counters and per-phase trace of the last g5_sssp_run on this workspace
- * (synchronises): counts[6] = edges looked at, edges into settled vertices,
+ * (synchronises): counts[7] = edges looked at, edges into settled vertices,
  * atomicMin issued, distances lowered, bucket-queue pushes, same-bucket
- * frontier pushes; per phase (up to 256) its kind (0 bucket open, 1 light,
- * 2 heavy), input list size and device milliseconds. */
-int g5_sssp_last_trace(const void *d_work, uint64_t work_bytes, uint64_t counts[6], int max_phases, int32_t *kind,
-                       uint64_t *size, double *phase_ms, int32_t *nphases, void *stream);
+ * frontier and sub-bucket pushes, heavy phases run as pulls; per phase (up
+ * to 256) its kind (0 bucket open, 1 light, 2 heavy push, 3 heavy pull,
+ * 4 sub-bucket open, 5 bucket split into sub-buckets), input list size,
+ * device milliseconds and edges looked at.  Any output pointer may be NULL. */
+int g5_sssp_last_trace(const void *d_work, uint64_t work_bytes, uint64_t counts[7], int max_phases, int32_t *kind,
+                       uint64_t *size, double *phase_ms, uint64_t *phase_edges, int32_t *nphases, void *stream);
 
 /* ---------------------------------------------------------- validation --- */
 

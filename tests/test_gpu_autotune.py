@@ -30,7 +30,8 @@ def test_tuned_settings_keep_results(cgt, g, tmp_path):
     ss = cgt.SsspState(g)
     cgt.oned_graph_sssp_run(g, ss, roots[0])
     want = ss.dist.clone()
-    cgt.oned_graph_sssp_run(g, ss, roots[0], delta=ts["delta"], blocks=ts["blocks"])
+    cgt.oned_graph_sssp_run(g, ss, roots[0], delta=ts["delta"], blocks=ts["blocks"], pull=ts["pull"],
+                            sub_min=ts["sub_min"])
     assert torch.equal(ss.dist.view(torch.int32), want.view(torch.int32))
 
     tm = T.tune_msbfs(g, roots, alphas=(8.0, 32.0), checks=(0, 2))

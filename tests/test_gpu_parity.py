@@ -235,10 +235,10 @@ def test_sssp_matches_reference(cgt, graphs, golden_dump):
         assert cgt.edge_count(g, s.pred, vw) == pr["nedge"]
 
 
-@pytest.mark.parametrize("delta", [0.1, 0.07, 0.25, 1.0, 4.0])
+@pytest.mark.parametrize("delta", [0.1, 0.07, 0.04, 0.25, 1.0, 4.0])
 def test_sssp_any_delta_same_bits(cgt, oracle, graphs, delta):
-    """The distances do not depend on delta (light/heavy split used when
-    delta matches the CSR's, weight filtering otherwise)."""
+    """The distances do not depend on delta (the CSR's light/heavy split at
+    0.1 used for every delta up to 0.1, weight filtering above)."""
     d = graphs[16]
     g = d["g"]
     s = cgt.SsspState(g)
@@ -248,6 +248,34 @@ def test_sssp_any_delta_same_bits(cgt, oracle, graphs, delta):
         od, _ = oracle.sssp(d["ors"], d["ocol"], d["ocw"], d["n"], r)
         assert np.array_equal(_np(s.dist).view(np.uint32), od.view(np.uint32))
         assert oracle.sssp_validate(d["ors"], d["ocol"], d["ocw"], d["n"], r, _np(s.dist), _np(s.pred)) == 0
+
+
+@pytest.mark.parametrize("delta", [0.1, 0.25, 0.05])
+def test_sssp_pull_push_and_sub_buckets_same_bits(cgt, oracle, graphs, delta):
+    """Heavy phases run as pulls (every unsettled vertex scans its own heavy
+    entries) and buckets split into sub-buckets give the same distances as
+    the oracle and the same parents as plain push-only buckets: the parent is
+    the smallest u on a tight edge either way.  pull=1e-9 pulls whenever a
+    bucket has rows, -1 never; sub_min=1 splits every bucket with a light
+    frontier, -1 never."""
+    d = graphs[16]
+    g = d["g"]
+    s = cgt.SsspState(g)
+    for r in cgt.generate_bfs_roots(g, 2, 3, 3):
+        cgt.oned_graph_sssp_run(g, s, r, delta=delta, pull=-1.0, sub_min=-1)
+        tr = cgt.sssp_trace(s)
+        assert tr["counts"]["pulls"] == 0 and 5 not in tr["kind"]
+        push_pred = _np(s.pred).copy()
+        od, _ = oracle.sssp(d["ors"], d["ocol"], d["ocw"], d["n"], r)
+        for pull, sub_min in ((1e-9, -1), (-1.0, 1), (1e-9, 1), (0.0, 0), (4.0, 64)):
+            cgt.oned_graph_sssp_run(g, s, r, delta=delta, pull=pull, sub_min=sub_min)
+            tr = cgt.sssp_trace(s)
+            if pull == 1e-9:
+                assert tr["counts"]["pulls"] > 0
+            if sub_min == 1:
+                assert 5 in tr["kind"] and 4 in tr["kind"]
+            assert np.array_equal(_np(s.dist).view(np.uint32), od.view(np.uint32)), (r, pull, sub_min)
+            assert np.array_equal(_np(s.pred), push_pred), (r, pull, sub_min)
 
 
 def test_sssp_validation_counts_match_oracle(cgt, oracle, graphs):
