@@ -355,7 +355,7 @@ def run_ours(args):
                                         args.edgefactor)
             torch.cuda.empty_cache()
         if world == 1 and not args.no_serve:
-            line["serving"] = run_serving(G, dev, args.serve_queries, args.serve_rate, args.edgefactor)
+            line["serving"] = run_serving(G, dev, args.serve_queries, args.serve_rate, args.edgefactor, args.serve_slots)
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
@@ -518,12 +518,14 @@ def run_packed(G, dev, ngraphs, smin, smax, ef, reps=3):
 SERVE_SCALES = (16, 18, 20, 22, 22, 23, 24, 24)
 
 
-def run_serving(G, dev, nqueries, rate, ef=16):
+def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0):
     """Serving: 8 resident Kronecker graphs (SCALE 16, 18, 20, 22, 22, 23, 24,
     24; seeds (2+i, 3)), a Poisson stream of queries (70% BFS, 30% SSSP,
     uniform graph, uniform non-zero-degree root, seed 1) replayed in real
     time through the continuous-batching server, then through plain calls
-    one query at a time.  Latency = completion seen by the host - arrival."""
+    one query at a time.  Latency = completion seen by the host - arrival.
+    `rate` saturates both (throughput); a second trace at `low_rate`, below
+    the server's capacity, shows latency when queries do not pile up."""
     import torch
     import cgt_b200.serve as S
     t0 = time.time()
@@ -532,7 +534,7 @@ def run_serving(G, dev, nqueries, rate, ef=16):
     build_s = time.time() - t0
     trace = S.poisson_trace(graphs, nqueries, rate, bfs_share=0.7, seed=1)
     warm = S.poisson_trace(graphs, 64, rate, bfs_share=0.5, seed=99)
-    srv = S.GraphServer(graphs, slots=4, hbm_reserve=16 << 30)
+    srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots)
     srv.run_trace(warm, deadline=600)  # workspaces created, batched copies prepared
     srv.stats = S.ServerStats()
     res = srv.run_trace(trace, deadline=3600)
@@ -540,8 +542,18 @@ def run_serving(G, dev, nqueries, rate, ef=16):
     st = srv.stats
     del srv
     torch.cuda.empty_cache()
+    low = None
+    if low_rate:
+        ltrace = S.poisson_trace(graphs, nqueries, low_rate, bfs_share=0.7, seed=2)
+        srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots)
+        srv.run_trace(warm, deadline=600)
+        low = {"rate_qps": low_rate, "ours": S.latency_summary(srv.run_trace(ltrace, deadline=3600))}
+        del srv
+        torch.cuda.empty_cache()
     S.serve_plain(graphs, warm)
     plain = S.latency_summary(S.serve_plain(graphs, trace))
+    if low:
+        low["plain_one_at_a_time"] = S.latency_summary(S.serve_plain(graphs, ltrace))
     kinds = {k: S.latency_summary([r for r in res if r.kind == k]) for k in ("bfs", "sssp")}
     return {"workload": f"{len(graphs)} resident graphs SCALE {list(SERVE_SCALES)} ef{ef}, {nqueries} Poisson "
                         f"queries at {rate:g}/s (70% BFS, 30% SSSP)",
@@ -550,7 +562,7 @@ def run_serving(G, dev, nqueries, rate, ef=16):
             "plain_one_at_a_time": plain, "qps_vs_plain": round(ours["qps"] / plain["qps"], 2),
             "bfs_batches": st.bfs_batches, "bfs_queries_batched": st.bfs_batched_queries,
             "sssp_launches": st.sssp_launches, "max_concurrent_launches": st.max_inflight,
-            "build_s": round(build_s, 2),
+            "slots": slots, "low_load": low, "build_s": round(build_s, 2),
             "timing": "host clock: latency from a query's arrival time to the host seeing its launch's "
                       "CUDA event complete; BFS results exported as depth arrays"}
 
@@ -567,7 +579,7 @@ def run_batched_only(args):
         out["packed"] = run_packed(G, dev, args.packed_graphs, args.packed_min_scale, args.packed_max_scale,
                                    args.edgefactor)
     if args.only_batched in ("serve", "all"):
-        out["serving"] = run_serving(G, dev, args.serve_queries, args.serve_rate, args.edgefactor)
+        out["serving"] = run_serving(G, dev, args.serve_queries, args.serve_rate, args.edgefactor, args.serve_slots)
     print(json.dumps(out), flush=True)
 
 
@@ -665,6 +677,7 @@ def main():
                     help="run only the batched measurements (multi-source BFS, packed graphs, serving or all)")
     ap.add_argument("--serve-queries", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate, queries per second")
+    ap.add_argument("--serve-slots", type=int, default=8, help="concurrent launches (streams) of the server")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     ap.add_argument("--packed-graphs", type=int, default=2000)
     ap.add_argument("--packed-min-scale", type=int, default=10)

@@ -703,6 +703,14 @@ def msbfs_trace(ms: MsBfsState, stream=None) -> dict:
 
 # ---------------------------------------------------------------- SSSP ----
 
+def sssp_workspace_bytes(nverts: int) -> int:
+    """Bytes of the SSSP workspace for a graph of nverts vertices
+    (g5_sssp_workspace_size)."""
+    nb = C.c_uint64()
+    _check(lib.g5_sssp_workspace_size(nverts, C.byref(nb)))
+    return nb.value
+
+
 class SsspState:
     """Sssp_State (src/traversal.h:30-41): pred int64[N], dist float32[N]."""
 

@@ -724,7 +724,7 @@ static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32
     cfg.stream = st;
     cudaLaunchAttribute attrs[2];
     attrs[0].id = cudaLaunchAttributeCooperative;
-    attrs[0].val.cooperative = 1;
+    attrs[0].val.cooperative = blocks > 1;  // one block has nothing to co-schedule
     cfg.attrs = attrs;
     cfg.numAttrs = 1;
     const uint64_t win = (uint64_t)((char *)(w.nbits + a.nwords) - (char *)w.visited);

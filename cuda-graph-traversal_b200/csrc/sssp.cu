@@ -572,7 +572,14 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
 // block's shared snapshot (SNAP_WORDS threads, one word each).  Every read
 // of those sizes after a barrier uses the snapshot.
 __device__ __forceinline__ bool sssp_sync(const SsspArgs &a, unsigned &epoch, SsspSnap *sp) {
-    if (!grid_sync(&a.ctl->bar, &a.ctl->error, epoch, a.nblocks, a.limit_ns)) return false;
+    if (a.nblocks == 1) {
+        // One block (a search in a small component): the block barrier
+        // orders every global write of the phase before the next phase.
+        __syncthreads();
+        if (ld_volatile(&a.ctl->error)) return false;
+    } else if (!grid_sync(&a.ctl->bar, &a.ctl->error, epoch, a.nblocks, a.limit_ns)) {
+        return false;
+    }
     static_assert(SNAP_WORDS <= SSSP_THREADS, "one word per thread");
     if (threadIdx.x < SNAP_WORDS)
         ((unsigned *)sp)[threadIdx.x] = ld_volatile(&((const unsigned *)&a.ctl->sn)[threadIdx.x]);
@@ -1223,8 +1230,12 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     a.limit_ns = wait_limit_ns();
     void *args[] = {&a};
     G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(SsspCtl), st));
-    G5_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)sssp_persistent_kernel, dim3(blocks), dim3(SSSP_THREADS),
-                                            args, 0, st));
+    if (blocks == 1)  // nothing to co-schedule: a plain launch
+        sssp_persistent_kernel<<<1, SSSP_THREADS, 0, st>>>(a);
+    else
+        G5_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)sssp_persistent_kernel, dim3(blocks),
+                                                dim3(SSSP_THREADS), args, 0, st));
+    G5_CUDA_TRY(cudaGetLastError());
     return G5_OK;
 }
 

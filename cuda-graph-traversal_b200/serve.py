@@ -15,7 +15,12 @@ free it launches the oldest waiting work:
 Every search is a persistent cooperative kernel whose grid is sized to its
 graph (g5_*_grid); launches run concurrently only while the sum of their
 grids fits on the device at once, so no two grids can wait on each other
-for SMs, and small graphs' searches share the GPU.
+for SMs, and small graphs' searches share the GPU.  A launch gets at most
+1/k of the device, k = the launches running plus the queue heads waiting
+(at most `slots`): a search on a quarter of the SMs takes well under four
+times as long (its phases are latency bound), so under load several
+searches side by side answer more queries per second, while a lone query
+still gets the whole device.
 
 Queries that arrive while others run join the next batch of their graph, so
 batches form continuously and work on different graphs and different
@@ -37,7 +42,7 @@ import torch
 
 from . import (MSBFS_MAX_ROOTS, BfsState, MsBfsParams, MsBfsState, OnedGraph, SsspState, msbfs_depths_u8,
                msbfs_run, msbfs_stats, oned_graph_bfs_run, oned_graph_sssp_reset, oned_graph_sssp_traverse,
-               search_grid, sssp_status)
+               search_grid, sssp_status, sssp_workspace_bytes)
 
 
 @dataclass
@@ -137,7 +142,7 @@ class GraphServer:
         if self.sssp_count[gi] >= self.max_sssp:
             return None
         g = self.graphs[gi]
-        if not self._fits(140 * g.nglobalverts):
+        if not self._fits(sssp_workspace_bytes(g.nglobalverts) + 12 * g.nglobalverts):  # + dist, pred
             return None
         self.sssp_count[gi] += 1
         self.stats.workspaces[f"sssp{gi}_{self.sssp_count[gi]}"] = 1
@@ -176,8 +181,11 @@ class GraphServer:
         could start."""
         if not self.free_slots:
             return False
-        for _, kind, gi in self._candidates():
-            blocks = self.grid["msbfs" if kind == "bfs" else "sssp"][gi]
+        cands = self._candidates()
+        k = min(len(self.streams), len(self.inflight) + len(cands))
+        share = max(1, self.max_blocks // max(1, k))
+        for _, kind, gi in cands:
+            blocks = min(self.grid["msbfs" if kind == "bfs" else "sssp"][gi], share)
             if self.blocks_in_use + blocks > self.max_blocks:
                 # Oldest first: younger work may not take the SMs this
                 # launch is waiting for (a full-device search would starve).
