@@ -103,6 +103,10 @@ struct BfsArgs {
 
 enum { TOP_DOWN = 0, BOTTOM_UP = 1 };
 
+// Bottom-up: entries of a row a lane scans on its own before the rest of
+// the row goes to the whole warp.
+constexpr uint64_t BU_LANE_ENTRIES = 8;
+
 // Claim v for parent u at the next level; appends it to the next queue.
 // All 32 lanes must call it (want = this lane has a candidate).
 __device__ __forceinline__ void td_visit(const BfsArgs &a, const WarpStage &bq, bool want, unsigned v, unsigned u,
@@ -190,17 +194,38 @@ __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsig
     const unsigned lane = lane_id();
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    // The visited word and the row bounds of the warp's next word are loaded
+    // while the current word is scanned (one word ahead), so a word's scan
+    // does not start with two dependent round trips.  Each word has one
+    // owner warp, which alone writes its visited word in this level.
+    unsigned vis_n = 0;
+    uint64_t rb_n = 0, re_n = 0;
+    auto fetch = [&](uint64_t kk) {
+        if (kk >= a.nwords) return;
+        vis_n = __ldcg(&a.visited[kk]);
+        const uint64_t vv = kk * 32 + lane;
+        if (vv < a.n) {
+            rb_n = __ldg(&a.rowptr[vv]);
+            re_n = __ldg(&a.rowptr[vv + 1]);
+        }
+    };
+    fetch(warp);
     for (uint64_t k = warp; k < a.nwords; k += nwarps) {
-        const unsigned vis = __ldcg(&a.visited[k]);
+        const unsigned vis = vis_n;
+        const uint64_t rb_k = rb_n, re_k = re_n;
+        fetch(k + nwarps);
         const uint64_t v = k * 32 + lane;
         int found = -1;
         uint64_t rb = 0, re = 0;
+        uint64_t e = 0;  // next entry of the row to look at
         if (v < a.n && !((vis >> lane) & 1u)) {
-            rb = __ldg(&a.rowptr[v]);
-            re = __ldg(&a.rowptr[v + 1]);
-            // Four neighbours per step: their loads and bitmap probes are
-            // independent, so each step costs one memory round trip, not four.
-            for (uint64_t e = rb; e < re && found < 0; e += 4) {
+            rb = rb_k;
+            re = re_k;
+            // Each lane scans the head of its own row, four neighbours per
+            // step: their loads and bitmap probes are independent, so a step
+            // costs one memory round trip, not four.
+            const uint64_t head = min(re, rb + BU_LANE_ENTRIES);
+            for (e = rb; e < head && found < 0; e += 4) {
                 unsigned u[4], word[4];
 #pragma unroll
                 for (int i = 0; i < 4; ++i) u[i] = e + i < re ? (unsigned)__ldg(&a.col[e + i]) : a.n;
@@ -212,6 +237,30 @@ __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsig
                     if (found < 0 && u[i] < a.n && ((word[i] >> (u[i] & 31)) & 1u)) found = (int)u[i];
                 }
             }
+        }
+        // The rest of every longer row is scanned by the whole warp, 32
+        // consecutive entries per step (coalesced), stopping at the first
+        // step with a hit; the row's first frontier neighbour is taken, as
+        // in the lane scan.  A warp no longer waits on one lane walking a
+        // long row four entries at a time.
+        unsigned longrows = __ballot_sync(FULL, found < 0 && e < re);
+        while (longrows) {
+            const int src = __ffs(longrows) - 1;
+            longrows &= longrows - 1;
+            const uint64_t b0 = __shfl_sync(FULL, e, src), end = __shfl_sync(FULL, re, src);
+            int hitv = -1;
+            for (uint64_t x0 = b0; x0 < end; x0 += 32) {
+                const uint64_t xe = x0 + lane;
+                const unsigned u = xe < end ? (unsigned)__ldg(&a.col[xe]) : a.n;
+                if (xe < end && u >= a.n) atomicOr(&a.ctl->res.error_flags, DEVERR_RANGE);
+                const bool hit = u < a.n && ((__ldcg(&fb[u >> 5]) >> (u & 31)) & 1u);
+                const unsigned m = __ballot_sync(FULL, hit);
+                if (m) {
+                    hitv = (int)__shfl_sync(FULL, u, __ffs(m) - 1);
+                    break;
+                }
+            }
+            if (lane == (unsigned)src) found = hitv;
         }
         const unsigned mask = __ballot_sync(FULL, found >= 0);
         if (found >= 0) {
