@@ -106,6 +106,7 @@ enum { TOP_DOWN = 0, BOTTOM_UP = 1 };
 // Bottom-up: entries of a row a lane scans on its own before the rest of
 // the row goes to the whole warp.
 constexpr uint64_t BU_LANE_ENTRIES = 8;
+constexpr int BU_STEP = 4;  // entries per lane step (loads issued together)
 
 // Claim v for parent u at the next level; appends it to the next queue.
 // All 32 lanes must call it (want = this lane has a candidate).
@@ -194,26 +195,30 @@ __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsig
     const unsigned lane = lane_id();
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    // The visited word and the row bounds of the warp's next word are loaded
-    // while the current word is scanned (one word ahead), so a word's scan
-    // does not start with two dependent round trips.  Each word has one
-    // owner warp, which alone writes its visited word in this level.
-    unsigned vis_n = 0;
-    uint64_t rb_n = 0, re_n = 0;
-    auto fetch = [&](uint64_t kk) {
-        if (kk >= a.nwords) return;
-        vis_n = __ldcg(&a.visited[kk]);
+    // Software pipeline over the warp's words: while word k is scanned, the
+    // row bounds of word k+1 (for its unvisited lanes, known from its
+    // visited word, loaded one step earlier) and the visited word of word
+    // k+2 are in flight, so a word's scan does not start with two dependent
+    // round trips.  Each word has one owner warp, which alone writes its
+    // visited word in this level.
+    auto vis_at = [&](uint64_t kk) -> unsigned { return kk < a.nwords ? __ldcg(&a.visited[kk]) : FULL; };
+    auto bounds = [&](uint64_t kk, unsigned vw, uint64_t &b, uint64_t &e) {
         const uint64_t vv = kk * 32 + lane;
-        if (vv < a.n) {
-            rb_n = __ldg(&a.rowptr[vv]);
-            re_n = __ldg(&a.rowptr[vv + 1]);
+        b = e = 0;
+        if (kk < a.nwords && vv < a.n && !((vw >> lane) & 1u)) {
+            b = __ldg(&a.rowptr[vv]);
+            e = __ldg(&a.rowptr[vv + 1]);
         }
     };
-    fetch(warp);
+    unsigned vis_n = vis_at(warp), vis_nn = vis_at(warp + nwarps);
+    uint64_t rb_n, re_n;
+    bounds(warp, vis_n, rb_n, re_n);
     for (uint64_t k = warp; k < a.nwords; k += nwarps) {
         const unsigned vis = vis_n;
         const uint64_t rb_k = rb_n, re_k = re_n;
-        fetch(k + nwarps);
+        vis_n = vis_nn;
+        bounds(k + nwarps, vis_n, rb_n, re_n);
+        vis_nn = vis_at(k + 2 * nwarps);
         const uint64_t v = k * 32 + lane;
         int found = -1;
         uint64_t rb = 0, re = 0;
@@ -221,18 +226,18 @@ __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsig
         if (v < a.n && !((vis >> lane) & 1u)) {
             rb = rb_k;
             re = re_k;
-            // Each lane scans the head of its own row, four neighbours per
+            // Each lane scans the head of its own row, BU_STEP neighbours per
             // step: their loads and bitmap probes are independent, so a step
-            // costs one memory round trip, not four.
+            // costs one memory round trip, not BU_STEP.
             const uint64_t head = min(re, rb + BU_LANE_ENTRIES);
-            for (e = rb; e < head && found < 0; e += 4) {
-                unsigned u[4], word[4];
+            for (e = rb; e < head && found < 0; e += BU_STEP) {
+                unsigned u[BU_STEP], word[BU_STEP];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) u[i] = e + i < re ? (unsigned)__ldg(&a.col[e + i]) : a.n;
+                for (int i = 0; i < BU_STEP; ++i) u[i] = e + i < re ? (unsigned)__ldg(&a.col[e + i]) : a.n;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) word[i] = u[i] < a.n ? __ldcg(&fb[u[i] >> 5]) : 0u;
+                for (int i = 0; i < BU_STEP; ++i) word[i] = u[i] < a.n ? __ldcg(&fb[u[i] >> 5]) : 0u;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
+                for (int i = 0; i < BU_STEP; ++i) {
                     if (e + i < re && u[i] >= a.n) atomicOr(&a.ctl->res.error_flags, DEVERR_RANGE);
                     if (found < 0 && u[i] < a.n && ((word[i] >> (u[i] & 31)) & 1u)) found = (int)u[i];
                 }
