@@ -36,8 +36,8 @@ sys.path.insert(0, REPO)
 PEAKS = os.path.join(REPO, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per traversed input edge of bfs_persistent_kernel on a
-# main-component root, from an ncu capture at SCALE 22 (228.6 MB for 67,106,224 edges,
-# profiles/bfs_persistent_kernel_scale22.md); scaled to the bench's roots by their edges.
+# main-component root, from an ncu capture at SCALE 23 (570.2 MB for 134,213,828 edges,
+# profiles/bfs_persistent_kernel_scale23.md); scaled to the bench's roots by their edges.
 TRAFFIC_BYTES_PER_EDGE = 4.25
 
 
