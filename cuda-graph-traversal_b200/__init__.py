@@ -122,7 +122,8 @@ class MsBfsStats(C.Structure):
 
 
 class SsspParams(C.Structure):
-    _fields_ = [("delta", C.c_float), ("blocks", C.c_int32), ("pull", C.c_float), ("sub_min", C.c_int32)]
+    _fields_ = [("delta", C.c_float), ("blocks", C.c_int32), ("pull", C.c_float), ("sub_min", C.c_int32),
+                ("small", C.c_int32)]
 
 
 def _ptr(t: torch.Tensor | None) -> int | None:
@@ -557,7 +558,7 @@ def oned_graph_bfs_reset(bfs: BfsState, with_depth: bool = True, g: OnedGraph | 
 
 def _right_sized(g: OnedGraph, root: int, params: BfsParams | None) -> BfsParams | None:
     if params is None and not g.in_main_component(root):
-        return BfsParams(14.0, 24.0, 0, 1)  # small component: one block
+        return BfsParams(14.0, 24.0, 3, 1)  # small component: the lean one-block search
     return params
 
 
@@ -729,10 +730,18 @@ def oned_graph_sssp_create(g: OnedGraph) -> SsspState:
     return SsspState(g)
 
 
+def _sssp_params(g: OnedGraph, root: int, delta, blocks, pull, sub_min, small) -> SsspParams:
+    # small=None: the lean one-block search for a root outside the main
+    # component (when the grid is left to the library).
+    if small is None:
+        small = blocks == 0 and not g.in_main_component(root)
+    return SsspParams(delta, 1 if small and blocks == 0 else blocks, pull, sub_min, int(bool(small)))
+
+
 def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,
-                        pull: float = 0.0, sub_min: int = 0, stream=None) -> None:
+                        pull: float = 0.0, sub_min: int = 0, small: bool | None = None, stream=None) -> None:
     """oned_graph_sssp_run (src/traversal.h:52), delta 0.1 as the reference."""
-    p = SsspParams(delta, blocks, pull, sub_min)
+    p = _sssp_params(g, root, delta, blocks, pull, sub_min, small)
     _check(lib.g5_sssp_run(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
                            g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                            sssp.work.numel(), C.byref(p), _stream(stream)))
@@ -748,12 +757,11 @@ def oned_graph_sssp_reset(sssp: SsspState, stream=None) -> None:
 
 
 def oned_graph_sssp_traverse(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,
-                             pull: float = 0.0, sub_min: int = 0, stream=None) -> None:
-    """The search itself, on a reset state (one block for a root outside the
-    main component)."""
-    if blocks == 0 and not g.in_main_component(root):
-        blocks = 1
-    p = SsspParams(delta, blocks, pull, sub_min)
+                             pull: float = 0.0, sub_min: int = 0, small: bool | None = None,
+                             stream=None) -> None:
+    """The search itself, on a reset state (the lean one-block search for a
+    root outside the main component)."""
+    p = _sssp_params(g, root, delta, blocks, pull, sub_min, small)
     _check(lib.g5_sssp_traverse(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
                                 g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                                 sssp.work.numel(), C.byref(p), _stream(stream)))

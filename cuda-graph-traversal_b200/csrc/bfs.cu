@@ -102,6 +102,7 @@ struct BfsArgs {
 };
 
 enum { TOP_DOWN = 0, BOTTOM_UP = 1 };
+constexpr int BFS_SMALL = 3;  // g5_bfs_params.mode: one lean block, for a root in a small component
 
 // Bottom-up: entries of a row a lane scans on its own before the rest of
 // the row goes to the whole warp.
@@ -578,6 +579,84 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
     if (gtid == 0) bfs_write_stats(a, st);
 }
 
+// A search from a root whose component is small (mode BFS_SMALL): one block,
+// levels top-down with the frontier queues in the workspace, claims on the
+// visited bitmap, level sizes in shared memory -- none of the grid
+// machinery (hand-off, grab counters, staging, grid barriers), so a
+// search of a few vertices costs a few memory round trips per level.
+// Correct for a component of any size, only slow when it is large.
+__global__ void __launch_bounds__(BFS_THREADS) bfs_small_kernel(BfsArgs a) {
+    BfsCtl *c = a.ctl;
+    __shared__ unsigned s_len[2];
+    __shared__ unsigned s_err;
+    __shared__ unsigned long long s_reached;
+    const unsigned root = a.root_from_ctl ? (unsigned)ld_volatile(&c->root_in) : a.root;
+    const unsigned lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) {
+        c->t0 = globaltimer_ns();
+        if (root >= a.n) {
+            s_err = DEVERR_RANGE;  // the host checks roots; a bad root_in is reported, not used
+            s_len[0] = 0;
+        } else {
+            a.visited[root >> 5] |= 1u << (root & 31);
+            a.pred[root] = root;
+            if (a.depth) a.depth[root] = 0;
+            a.q[0][0] = root;
+            s_len[0] = 1;
+            s_err = 0;
+        }
+        s_len[1] = 0;
+        s_reached = s_len[0];
+    }
+    __syncthreads();
+    int level = 0;
+    for (;; ++level) {
+        const int cur = level & 1;
+        const unsigned n = s_len[cur];
+        if (n == 0) break;
+        const unsigned *Q = a.q[cur];
+        unsigned *QN = a.q[cur ^ 1];
+        // One warp per frontier vertex, its lanes over the vertex's row.
+        for (unsigned i = wid; i < n; i += nw) {
+            const unsigned u = __ldcg(&Q[i]);
+            const uint64_t rb = __ldg(&a.rowptr[u]), re = __ldg(&a.rowptr[u + 1]);
+            for (uint64_t e = rb + lane; e < re; e += 32) {
+                const unsigned v = (unsigned)__ldg(&a.col[e]);
+                if (v >= a.n) {  // not a vertex: report it, touch nothing
+                    atomicOr(&s_err, DEVERR_RANGE);
+                    continue;
+                }
+                const unsigned bit = 1u << (v & 31);
+                if ((__ldcg(&a.visited[v >> 5]) & bit) || (atomicOr(&a.visited[v >> 5], bit) & bit)) continue;
+                a.pred[v] = u;
+                if (a.depth) a.depth[v] = level + 1;
+                const unsigned pos = atomicAdd(&s_len[cur ^ 1], 1u);  // each vertex is claimed once: pos < n
+                if (pos < a.n) QN[pos] = v;
+                else atomicOr(&s_err, DEVERR_CAPACITY);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_reached += s_len[cur ^ 1];
+            s_len[cur] = 0;
+            if (level < BFS_TRACE) {
+                c->t_level[level] = globaltimer_ns();
+                c->n_level[level] = n;
+                c->m_level[level] = 0;
+                c->mode_level[level] = TOP_DOWN;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        c->res.levels = level;
+        c->res.bottom_up_levels = 0;
+        c->res.reached = s_reached;
+        c->res.error_flags |= s_err;
+        c->res.solo_levels = level;
+    }
+}
+
 struct BfsWork {
     BfsCtl *ctl;
     unsigned *visited, *fbits, *nbits;
@@ -736,7 +815,7 @@ static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32
                       unsigned nroots = 0) {
     g5_bfs_params p = {14.0f, 24.0f, 0, 0};
     if (params) p = *params;
-    G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= 2, "g5_bfs: bad params");
+    G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= BFS_SMALL, "g5_bfs: bad params");
     int max_blocks = 0;
     int rc = bfs_max_blocks(&max_blocks);
     if (rc) return rc;
@@ -769,6 +848,11 @@ static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32
     static std::atomic<unsigned long long> next_seq{1};
     a.seq = next_seq.fetch_add(1);
     if (h_root) G5_CUDA_TRY(cudaMemcpyAsync(&w.ctl->root_in, h_root, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    if (p.mode == BFS_SMALL && !d_roots) {
+        bfs_small_kernel<<<1, BFS_THREADS, 0, st>>>(a);
+        G5_CUDA_TRY(cudaGetLastError());
+        return G5_OK;
+    }
     // Cooperative launch; the three bitmaps (visited, frontier, next: N/8
     // bytes each, adjacent in the workspace) get an L2 persisting window so
     // the streaming column reads do not evict them.
@@ -832,7 +916,10 @@ extern "C" int g5_bfs_query(const uint64_t *d_rowstarts, const int32_t *d_col, u
     if (params) p = *params;
     // A root outside the main component reaches a small set: one block
     // runs the whole search, with no grid to launch or wait for.
-    if (h_main_bits && p.blocks == 0 && !((h_main_bits[root >> 5] >> (root & 31)) & 1u)) p.blocks = 1;
+    if (h_main_bits && p.blocks == 0 && !((h_main_bits[root >> 5] >> (root & 31)) & 1u)) {
+        p.blocks = 1;
+        p.mode = BFS_SMALL;
+    }
     cudaStream_t st = (cudaStream_t)stream;
     if ((rc = bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, &p, h_root, st))) return rc;
     G5_CUDA_TRY(cudaMemcpyAsync(h_stats, &w.ctl->res, sizeof(g5_bfs_stats), cudaMemcpyDeviceToHost, st));

@@ -1067,6 +1067,104 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
     }
 }
 
+// A search from a source whose component is small (g5_sssp_params.small):
+// one block, label-correcting rounds (every vertex whose distance dropped in
+// a round relaxes all its edges in the next), lists in the workspace, list
+// sizes in shared memory -- no buckets, phases or grid machinery.  It
+// reaches the same float fixed point, hence the same distances, and the
+// same parents (the smallest u on a tight edge: every vertex relaxes its
+// edges again after its last decrease).  Correct for a component of any
+// size, only slow when it is large.
+__global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
+    SsspCtl *c = a.ctl;
+    __shared__ unsigned s_len[2];
+    __shared__ unsigned s_nreach;
+    __shared__ unsigned s_err;
+    const unsigned lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const bool sparse_out = __ldcg((const unsigned long long *)&a.prefilled->dist) == (unsigned long long)a.dist &&
+                            __ldcg((const unsigned long long *)&a.prefilled->pred) == (unsigned long long)a.pred;
+    unsigned *R = a.S[0];  // every vertex reached, once (sstamp)
+    if (threadIdx.x == 0) {
+        c->t0 = globaltimer_ns();
+        a.pack[a.root] = (unsigned long long)a.root;  // distance 0.0f, parent = root
+        a.sstamp[a.root] = 0;
+        a.F[0][0] = a.root;
+        R[0] = a.root;
+        s_len[0] = 1;
+        s_len[1] = 0;
+        s_nreach = 1;
+        s_err = 0;
+    }
+    __syncthreads();
+    unsigned round = 0;
+    for (;; ++round) {
+        const int cur = round & 1;
+        const unsigned n = s_len[cur];
+        if (n == 0) break;
+        const unsigned *L = a.F[cur];
+        unsigned *LN = a.F[cur ^ 1];
+        // One warp per listed vertex, its lanes over the vertex's row.
+        for (unsigned i = wid; i < n; i += nw) {
+            const unsigned u = __ldcg(&L[i]);
+            const float du = pack_dist(__ldcg(&a.pack[u]));
+            const uint64_t rb = __ldg(&a.rowptr[u]), re = __ldg(&a.rowptr[u + 1]);
+            for (uint64_t e = rb + lane; e < re; e += 32) {
+                const unsigned v = (unsigned)__ldg(&a.col[e]);
+                if (v >= a.n) {  // not a vertex: report it, touch nothing
+                    atomicOr(&s_err, DEVERR_RANGE);
+                    continue;
+                }
+                const float cand = __fadd_rn(du, __ldg(&a.w[e]));
+                const unsigned long long np = ((unsigned long long)__float_as_uint(cand) << 32) | u;
+                if (np >= __ldcg(&a.pack[v])) continue;
+                const unsigned long long old = atomicMin(&a.pack[v], np);
+                if (!(np < old && (old >> 32) != (np >> 32))) continue;  // distance unchanged
+                if (atomicExch(&a.fstamp[v], round) != round) {
+                    const unsigned pos = atomicAdd(&s_len[cur ^ 1], 1u);  // once per vertex and round
+                    if (pos < a.n) LN[pos] = v;
+                    else atomicOr(&s_err, DEVERR_CAPACITY);
+                }
+                if (atomicExch(&a.sstamp[v], 0u) != 0u) {
+                    const unsigned pos = atomicAdd(&s_nreach, 1u);
+                    if (pos < a.n) R[pos] = v;
+                    else atomicOr(&s_err, DEVERR_CAPACITY);
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_len[cur] = 0;
+            if (round < SSSP_TRACE) {
+                c->t_phase[round] = globaltimer_ns();
+                c->kind_phase[round] = 1;
+                c->n_phase[round] = n;
+                c->e_phase[round] = 0;
+            }
+        }
+        __syncthreads();
+    }
+    // Outputs: the reached vertices (pre-filled outputs) or every vertex.
+    if (sparse_out) {
+        for (unsigned i = threadIdx.x; i < s_nreach; i += blockDim.x) {
+            const unsigned v = __ldcg(&R[i]);
+            const unsigned long long p = __ldcg(&a.pack[v]);
+            a.dist[v] = pack_dist(p);
+            a.pred[v] = (int64_t)(unsigned)p;
+        }
+    } else {
+        for (uint64_t v = threadIdx.x; v < a.n; v += blockDim.x) {
+            const unsigned long long p = __ldcg(&a.pack[v]);
+            a.dist[v] = p == UNREACHED ? -1.0f : pack_dist(p);
+            a.pred[v] = p == UNREACHED ? -1 : (int64_t)(unsigned)p;
+        }
+    }
+    if (threadIdx.x == 0) {
+        c->buckets = 1;
+        c->phases = round;
+        c->error |= s_err;
+    }
+}
+
 // Fills the outputs with "unreached" and records them as pre-filled.
 __global__ void sssp_prefill_kernel(float *__restrict__ dist, int64_t *__restrict__ pred, uint64_t n, SsspOut *hdr) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -1183,7 +1281,7 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     SsspWork w;
     int rc = sssp_check(d_rowstarts, d_col, d_w, nverts, root, d_dist, d_pred, d_work, work_bytes, &w, who);
     if (rc) return rc;
-    g5_sssp_params p = {0.1f, 0, 0.0f, 0};
+    g5_sssp_params p = {0.1f, 0, 0.0f, 0, 0};
     if (params) p = *params;
     G5_CHECK_ARG(p.delta > 0.0f, "g5_sssp_traverse: delta must be positive");
     int max_blocks = 0;
@@ -1230,7 +1328,9 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     a.limit_ns = wait_limit_ns();
     void *args[] = {&a};
     G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(SsspCtl), st));
-    if (blocks == 1)  // nothing to co-schedule: a plain launch
+    if (p.small && !d_roots)
+        sssp_small_kernel<<<1, SSSP_THREADS, 0, st>>>(a);
+    else if (blocks == 1)  // nothing to co-schedule: a plain launch
         sssp_persistent_kernel<<<1, SSSP_THREADS, 0, st>>>(a);
     else
         G5_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)sssp_persistent_kernel, dim3(blocks),

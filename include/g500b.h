@@ -113,7 +113,9 @@ int g5_csr_pack_append(const uint64_t *d_src_rowstarts, const int32_t *d_src_col
 typedef struct g5_bfs_params {
     float alpha;    /* top-down -> bottom-up when frontier edges > unvisited edges / alpha (default 14)  */
     float beta;     /* bottom-up -> top-down when frontier vertices < nverts / beta (default 24)         */
-    int32_t mode;   /* 0 = direction-optimizing, 1 = top-down only, 2 = bottom-up after level 0         */
+    int32_t mode;   /* 0 = direction-optimizing, 1 = top-down only, 2 = bottom-up after level 0,
+                       3 = one lean block, top-down (a root in a small component; g5_bfs_query picks
+                       it from the main-component bitmap)                                             */
     int32_t blocks; /* persistent grid size; 0 = fill the device                                          */
 } g5_bfs_params;
 
@@ -228,6 +230,9 @@ typedef struct g5_sssp_params {
                        CSR entries, the rest of the bucket runs in 32
                        sub-buckets in distance order; 0 = default (2^25),
                        < 0 = never                                           */
+    int32_t small;   /* 1: the source's component is small (outside the main
+                       component): one lean block, label-correcting rounds,
+                       same distances and parents; 0 = the bucketed search  */
 } g5_sssp_params;
 
 int g5_sssp_workspace_size(uint64_t nverts, uint64_t *bytes);

@@ -138,7 +138,7 @@ def test_bfs_depth_matches_reference(cgt, graphs, golden_dump):
         assert st.reached == pr["reached"]
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
 @pytest.mark.parametrize("blocks", [0, 1, 3])
 def test_bfs_modes_and_grids_agree(cgt, oracle, graphs, mode, blocks):
     """Direction-optimizing, top-down-only and bottom-up-only BFS on any
@@ -268,7 +268,7 @@ def test_sssp_pull_push_and_sub_buckets_same_bits(cgt, oracle, graphs, delta):
         push_pred = _np(s.pred).copy()
         od, _ = oracle.sssp(d["ors"], d["ocol"], d["ocw"], d["n"], r)
         for pull, sub_min in ((1e-9, -1), (-1.0, 1), (1e-9, 1), (0.0, 0), (4.0, 64)):
-            cgt.oned_graph_sssp_run(g, s, r, delta=delta, pull=pull, sub_min=sub_min)
+            cgt.oned_graph_sssp_run(g, s, r, delta=delta, pull=pull, sub_min=sub_min, small=False)
             tr = cgt.sssp_trace(s)
             if pull == 1e-9:
                 assert tr["counts"]["pulls"] > 0
@@ -276,6 +276,35 @@ def test_sssp_pull_push_and_sub_buckets_same_bits(cgt, oracle, graphs, delta):
                 assert 5 in tr["kind"] and 4 in tr["kind"]
             assert np.array_equal(_np(s.dist).view(np.uint32), od.view(np.uint32)), (r, pull, sub_min)
             assert np.array_equal(_np(s.pred), push_pred), (r, pull, sub_min)
+
+
+def test_sssp_small_component_search_same_bits(cgt, oracle, graphs):
+    """The lean one-block search (label-correcting rounds, meant for roots
+    outside the main component) gives the oracle's distances and the bucketed
+    search's parents, from main-component roots too, with outputs pre-filled
+    by the reset and with outputs left to the search."""
+    d = graphs[16]  # 12 vertices of non-zero degree lie outside its main component
+    g = d["g"]
+    s = cgt.SsspState(g)
+    rs = _np(g.rowstarts)
+    small_roots = [v for v in range(d["n"]) if not g.in_main_component(v) and rs[v + 1] > rs[v]][:3]
+    assert small_roots
+    for r in cgt.generate_bfs_roots(g, 2, 3, 2) + small_roots:
+        cgt.oned_graph_sssp_run(g, s, r, small=False)
+        want_pred = _np(s.pred).copy()
+        od, _ = oracle.sssp(d["ors"], d["ocol"], d["ocw"], d["n"], r)
+        for prefill in (True, False):
+            if prefill:
+                cgt.oned_graph_sssp_reset(s)
+            else:  # workspace only: the search writes all N outputs itself
+                s.dist.fill_(7.0)
+                s.pred.fill_(7)
+                assert cgt.lib.g5_sssp_reset(s.max_nlocalverts, None, None, s.work.data_ptr(), s.work.numel(),
+                                             None) == 0
+            cgt.oned_graph_sssp_traverse(g, s, r, small=True)
+            cgt.sssp_status(s)
+            assert np.array_equal(_np(s.dist).view(np.uint32), od.view(np.uint32)), (r, prefill)
+            assert np.array_equal(_np(s.pred), want_pred), (r, prefill)
 
 
 def test_sssp_validation_counts_match_oracle(cgt, oracle, graphs):
