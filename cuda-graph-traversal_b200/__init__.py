@@ -527,7 +527,10 @@ class BfsState:
         self.val_work: torch.Tensor | None = None
         self.max_nlocalverts = n
         self.h_root = torch.zeros(1, dtype=torch.int64).pin_memory()
-        self.h_stats = BfsStats()
+        # Pinned too: g5_bfs_query then reads the root and writes the
+        # statistics from the device, with no copy calls.
+        self._h_stats_buf = torch.zeros(C.sizeof(BfsStats), dtype=torch.uint8).pin_memory()
+        self.h_stats = BfsStats.from_address(self._h_stats_buf.data_ptr())
         # Raw addresses for the single-call query path.
         self._root_slot = C.c_uint64.from_address(self.h_root.data_ptr())
         self._q = (self.h_root.data_ptr(), self.pred.data_ptr(), self.depth.data_ptr(), self.work.data_ptr(),
@@ -574,9 +577,10 @@ def oned_graph_bfs_traverse(g: OnedGraph, bfs: BfsState, root: int, params: BfsP
 
 def oned_graph_bfs_query(g: OnedGraph, bfs: BfsState, root: int, with_depth: bool = False,
                          stream=None) -> BfsStats:
-    """One search end to end from the host (g5_bfs_query): the root goes
-    host->device from pinned memory, the search runs on a state reset since
-    its last search, and its statistics come back; synchronises."""
+    """One search end to end from the host (g5_bfs_query): the device reads
+    the root from pinned host memory, the search runs on a state reset since
+    its last search, and the device writes its statistics back to pinned
+    host memory; synchronises."""
     bfs._root_slot.value = root
     hr, pred, depth, work, nwork, stats = bfs._q
     mb = g.main_bits

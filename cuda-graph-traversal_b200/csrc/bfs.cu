@@ -95,7 +95,10 @@ struct BfsArgs {
     int mode;
     unsigned nblocks;
     unsigned long long limit_ns;
-    bool root_from_ctl;  // take the root from ctl->root_in (copied in by the caller's stream)
+    // Root source for g5_bfs_query: ctl->root_in (copied in on the stream)
+    // or the caller's mapped pinned host word; nullptr = `root`.
+    const unsigned long long *root_src;
+    g5_bfs_stats *stats_out;  // the caller's mapped pinned host statistics, or nullptr
     unsigned long long seq;  // unique per launch: releases only this launch's waiting blocks
     const uint64_t *roots;   // several roots at once (device array) instead of `root`, or nullptr
     unsigned nroots;
@@ -391,10 +394,24 @@ __device__ __forceinline__ bool bfs_advance(const BfsArgs &a, LevelState &st, un
     return true;
 }
 
+// Copies the finished search's statistics to the caller's mapped host
+// memory (g5_bfs_query), visible to the host once the stream is synchronised.
+__device__ __forceinline__ void bfs_publish_stats(const BfsArgs &a) {
+    if (!a.stats_out) return;
+    volatile g5_bfs_stats *r = &a.ctl->res;
+    a.stats_out->levels = r->levels;
+    a.stats_out->bottom_up_levels = r->bottom_up_levels;
+    a.stats_out->reached = r->reached;
+    a.stats_out->error_flags = r->error_flags;
+    a.stats_out->solo_levels = r->solo_levels;
+    __threadfence_system();
+}
+
 __device__ __forceinline__ void bfs_write_stats(const BfsArgs &a, const LevelState &st) {
     a.ctl->res.levels = st.levels;
     a.ctl->res.bottom_up_levels = st.bu_levels;
     a.ctl->res.reached = st.reached;
+    bfs_publish_stats(a);
 }
 
 __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs a) {
@@ -431,7 +448,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
             }
         }
         if (!a.roots) {
-            const unsigned root = a.root_from_ctl ? (unsigned)ld_volatile(&c->root_in) : a.root;
+            const unsigned root = a.root_src ? (unsigned)ld_volatile(a.root_src) : a.root;
             const uint64_t root_deg = __ldg(&a.rowptr[root + 1]) - __ldg(&a.rowptr[root]);
             if (threadIdx.x == 0) {
                 a.visited[root >> 5] |= 1u << (root & 31);
@@ -590,7 +607,7 @@ __global__ void __launch_bounds__(BFS_THREADS) bfs_small_kernel(BfsArgs a) {
     __shared__ unsigned s_len[2];
     __shared__ unsigned s_err;
     __shared__ unsigned long long s_reached;
-    const unsigned root = a.root_from_ctl ? (unsigned)ld_volatile(&c->root_in) : a.root;
+    const unsigned root = a.root_src ? (unsigned)ld_volatile(a.root_src) : a.root;
     const unsigned lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (threadIdx.x == 0) {
         c->t0 = globaltimer_ns();
@@ -654,6 +671,7 @@ __global__ void __launch_bounds__(BFS_THREADS) bfs_small_kernel(BfsArgs a) {
         c->res.reached = s_reached;
         c->res.error_flags |= s_err;
         c->res.solo_levels = level;
+        bfs_publish_stats(a);
     }
 }
 
@@ -807,12 +825,15 @@ extern "C" int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, 
     return G5_OK;
 }
 
-// Builds the kernel arguments and launches the persistent BFS (after zeroing
-// the control block; the root comes from root_in when from_ctl).
+// Builds the kernel arguments and launches the persistent BFS.  With h_root
+// the root is read on the device: from h_root itself when it is mapped
+// pinned memory (d_root_map), else from ctl->root_in after a copy on the
+// stream; d_stats_map (mapped pinned memory, or nullptr) receives the
+// statistics at the end of the search.
 static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
                       uint64_t root, int64_t *d_pred, int32_t *d_depth, const g5_bfs_params *params,
                       const uint64_t *h_root, cudaStream_t st, const uint64_t *d_roots = nullptr,
-                      unsigned nroots = 0) {
+                      unsigned nroots = 0, const uint64_t *d_root_map = nullptr, g5_bfs_stats *d_stats_map = nullptr) {
     g5_bfs_params p = {14.0f, 24.0f, 0, 0};
     if (params) p = *params;
     G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= BFS_SMALL, "g5_bfs: bad params");
@@ -842,12 +863,15 @@ static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32
     a.mode = p.mode;
     a.nblocks = (unsigned)blocks;
     a.limit_ns = wait_limit_ns();
-    a.root_from_ctl = h_root != nullptr;
+    a.root_src = d_root_map ? (const unsigned long long *)d_root_map
+                            : h_root ? &w.ctl->root_in : nullptr;
+    a.stats_out = d_stats_map;
     a.roots = d_roots;
     a.nroots = nroots;
     static std::atomic<unsigned long long> next_seq{1};
     a.seq = next_seq.fetch_add(1);
-    if (h_root) G5_CUDA_TRY(cudaMemcpyAsync(&w.ctl->root_in, h_root, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    if (h_root && !d_root_map)
+        G5_CUDA_TRY(cudaMemcpyAsync(&w.ctl->root_in, h_root, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     if (p.mode == BFS_SMALL && !d_roots) {
         bfs_small_kernel<<<1, BFS_THREADS, 0, st>>>(a);
         G5_CUDA_TRY(cudaGetLastError());
@@ -903,6 +927,18 @@ extern "C" int g5_bfs_traverse_multi(const uint64_t *d_rowstarts, const int32_t 
                       d_roots, nroots);
 }
 
+// Device address of pinned host memory `h`, when the device can address it.
+static bool host_mapped(const void *h, void **d) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, h) != cudaSuccess) {
+        cudaGetLastError();  // pageable memory on older drivers: not an error here
+        return false;
+    }
+    if (at.type != cudaMemoryTypeHost || !at.devicePointer) return false;
+    *d = at.devicePointer;
+    return true;
+}
+
 extern "C" int g5_bfs_query(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, const uint64_t *h_root,
                             const uint32_t *h_main_bits, int64_t *d_pred, int32_t *d_depth, void *d_work,
                             uint64_t work_bytes, const g5_bfs_params *params, g5_bfs_stats *h_stats, void *stream) {
@@ -921,8 +957,19 @@ extern "C" int g5_bfs_query(const uint64_t *d_rowstarts, const int32_t *d_col, u
         p.mode = BFS_SMALL;
     }
     cudaStream_t st = (cudaStream_t)stream;
-    if ((rc = bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, &p, h_root, st))) return rc;
-    G5_CUDA_TRY(cudaMemcpyAsync(h_stats, &w.ctl->res, sizeof(g5_bfs_stats), cudaMemcpyDeviceToHost, st));
+    // Pinned host memory that the device can address (mapped; every pinned
+    // allocation is under unified addressing) is read and written by the
+    // kernel itself: no copy calls around the search.
+    void *d_root_map = nullptr, *d_stats_map = nullptr;
+    const bool mapped = host_mapped(h_root, &d_root_map) && host_mapped(h_stats, &d_stats_map);
+    if (mapped) {
+        if ((rc = bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, &p, h_root, st, nullptr, 0,
+                             (const uint64_t *)d_root_map, (g5_bfs_stats *)d_stats_map)))
+            return rc;
+    } else {
+        if ((rc = bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, &p, h_root, st))) return rc;
+        G5_CUDA_TRY(cudaMemcpyAsync(h_stats, &w.ctl->res, sizeof(g5_bfs_stats), cudaMemcpyDeviceToHost, st));
+    }
     G5_CUDA_TRY(cudaStreamSynchronize(st));
     return deverr_to_status(h_stats->error_flags, "g5_bfs_query");
 }

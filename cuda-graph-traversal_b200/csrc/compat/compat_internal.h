@@ -28,7 +28,7 @@ struct BfsExt {
     uint64_t work_bytes;
     void *val_work;  // depth-from-parents scratch
     uint64_t val_bytes;
-    uint64_t *root_host;  // pinned: the root of the next search
+    uint64_t *root_host;  // pinned: the root of the next search, then its g5_bfs_stats
 };
 
 struct SsspExt {

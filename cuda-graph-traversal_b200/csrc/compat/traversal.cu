@@ -66,7 +66,9 @@ Bfs_State oned_graph_bfs_create(Worker_State *ws, const Oned_Graph *g) {
     x.work = gpu_push(ws, x.work_bytes, "BFS workspace");
     check(ws, g5_validate_workspace_size(g->nglobalverts, &x.val_bytes), "oned_graph_bfs_create");
     x.val_work = gpu_push(ws, x.val_bytes, "BFS depth scratch");
-    CHECK_CUDA(cudaMallocHost(&x.root_host, sizeof(uint64_t)));
+    // Pinned root word followed by the statistics (g5_bfs_query reads and
+    // writes both from the device when they are pinned).
+    CHECK_CUDA(cudaMallocHost(&x.root_host, sizeof(uint64_t) + sizeof(g5_bfs_stats)));
     put_bfs(bfs.pred, x);
     GraphExt *gx = get_graph(g, ws);
     if (!gx->main_host && g->nlocaledges) {
@@ -119,9 +121,9 @@ void oned_graph_bfs_run(Worker_State *ws, const Oned_Graph *g, Bfs_State *bfs, u
     // The reset half ran in oned_graph_bfs_clear, which the reference's
     // protocol calls before every search (examples/graph500_runner.cu:309).
     *bx->root_host = root;
-    g5_bfs_stats st;
+    g5_bfs_stats *st = (g5_bfs_stats *)(bx->root_host + 1);
     check(ws, g5_bfs_query(g->rowstarts, gx->col, g->nglobalverts, bx->root_host, gx->main_host, bfs->pred, bx->depth,
-                           bx->work, bx->work_bytes, nullptr, &st, 0),
+                           bx->work, bx->work_bytes, nullptr, st, 0),
           "oned_graph_bfs_run");
 }
 

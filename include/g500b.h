@@ -164,9 +164,10 @@ int g5_bfs_traverse_multi(const uint64_t *d_rowstarts, const int32_t *d_col, uin
                           const g5_bfs_params *params, void *stream);
 
 /* One search end to end from host memory, for callers that issue single
- * queries: copies *h_root (pinned host memory) to the device, runs the
- * traversal on a workspace reset since its last search, copies the
- * statistics to *h_stats and synchronises.  h_main_bits (host bitmap of the
+ * queries: reads *h_root, runs the traversal on a workspace reset since its
+ * last search, stores the statistics in *h_stats and synchronises.  When
+ * both are pinned host memory the kernel itself reads the root and writes
+ * the statistics (no copy calls); otherwise they are copied on the stream.  h_main_bits (host bitmap of the
  * main component, optional; see g5_bfs_visited_bitmap) lets a root outside
  * it run on a single block, which a small component needs and which avoids
  * launching and waiting for the whole grid. */
