@@ -23,10 +23,10 @@ constexpr unsigned BIG_DEG = 1024;
 constexpr unsigned BIG_CHUNK = 1024;
 
 // Entries per grab over a small part of ns entries: about four grabs per
-// warp, between 1 and 32.
-__host__ __device__ __forceinline__ unsigned grab_size(unsigned ns, unsigned long long nwarps) {
+// warp, between 1 and `cap` (at most 32).
+__host__ __device__ __forceinline__ unsigned grab_size(unsigned ns, unsigned long long nwarps, unsigned cap = 32) {
     unsigned long long g = ns / (4 * nwarps);
-    return g < 1 ? 1u : g > 32 ? 32u : (unsigned)g;
+    return g < 1 ? 1u : g > cap ? cap : (unsigned)g;
 }
 constexpr int BIG_SHIFT = 40;
 constexpr unsigned long long BIG_LOW = (1ull << BIG_SHIFT) - 1;
@@ -37,13 +37,15 @@ __device__ __forceinline__ unsigned big_count(unsigned long long packed) { retur
 __device__ __forceinline__ unsigned long long big_chunks(unsigned long long packed) { return packed & BIG_LOW; }
 
 // Appends v, whose edge range to expand has `deg` entries, to list L of
-// capacity n (base[] = chunk bases of the big part).  All 32 lanes call it.
-// Returns false (and writes nothing) when the list would overflow, which
-// the callers' once-per-list invariants rule out.
+// capacity n (base[] = chunk bases of the big part): the small part when
+// deg <= big_deg, else the big part.  All 32 lanes call it.  Returns false
+// (and writes nothing) when the list would overflow, which the callers'
+// once-per-list invariants rule out.
 __device__ __forceinline__ bool frontier_append(unsigned *L, unsigned *base, uint64_t n, unsigned *n_small,
-                                                unsigned long long *big, bool want, unsigned v, uint64_t deg) {
-    const bool sm = want && deg <= BIG_DEG;
-    const bool bg = want && deg > BIG_DEG;
+                                                unsigned long long *big, bool want, unsigned v, uint64_t deg,
+                                                unsigned big_deg = BIG_DEG) {
+    const bool sm = want && deg <= big_deg;
+    const bool bg = want && deg > big_deg;
     bool ok = true;
     const unsigned p = warp_append(n_small, sm);
     if (sm) {
@@ -121,9 +123,9 @@ __device__ __forceinline__ bool stage_append(const WarpStage &q, bool want, unsi
 // frontier_append with the small part staged per warp.  All lanes call it.
 __device__ __forceinline__ bool frontier_append_staged(const WarpStage &q, unsigned *L, unsigned *basearr, uint64_t n,
                                                        unsigned *n_small, unsigned long long *big, bool want,
-                                                       unsigned v, uint64_t deg) {
-    bool ok = stage_append(q, want && deg <= BIG_DEG, v, L, n, n_small);
-    ok &= frontier_append(L, basearr, n, n_small, big, want && deg > BIG_DEG, v, deg);
+                                                       unsigned v, uint64_t deg, unsigned big_deg = BIG_DEG) {
+    bool ok = stage_append(q, want && deg <= big_deg, v, L, n, n_small);
+    ok &= frontier_append(L, basearr, n, n_small, big, want && deg > big_deg, v, deg, big_deg);
     return ok;
 }
 

@@ -50,6 +50,12 @@ constexpr unsigned STAGE_Q = 16;     //                   each sub-bucket queue
 static_assert(STAGE_F >= 32 && STAGE_S >= 32, "staging slices hold one warp step");
 static_assert(STAGE_R <= 32 && STAGE_Q <= 32, "stage_push writes a full slice with one lane per entry");
 constexpr int SSSP_TRACE = 256;      // phases recorded in the control block
+// List entries with more edges to expand than this go to the big part (cut
+// into BIG_CHUNK chunks across the grid), and a warp grabs at most SSSP_GRAB
+// small entries at once: a grab holds at most SSSP_GRAB x SSSP_BIG_DEG edges,
+// so no warp is left with a long tail of relaxations at the end of a phase.
+constexpr unsigned SSSP_BIG_DEG = 128;
+constexpr unsigned SSSP_GRAB = 32;
 // Sub-buckets: once a bucket's light frontier holds SPLIT_MIN light entries,
 // the rest of the bucket is processed in SUB equal sub-buckets in order
 // (delta-stepping with width delta/SUB for the light edges, nested in the
@@ -241,8 +247,9 @@ __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCt
     // Each vertex enters a frontier once per phase and a heavy set once per
     // bucket, so no list exceeds n entries.
     bool ok = frontier_append_staged(x.st.f, x.Fout, x.FBout, a.n, &c->sn.f_small[x.f_slot], &c->sn.f_big[x.f_slot], f, v,
-                                     le - lb);
-    ok &= frontier_append_staged(x.st.s, x.Sl, x.SBl, a.n, &c->sn.s_small[x.s_slot], &c->sn.s_big[x.s_slot], s, v, he - hb);
+                                     le - lb, SSSP_BIG_DEG);
+    ok &= frontier_append_staged(x.st.s, x.Sl, x.SBl, a.n, &c->sn.s_small[x.s_slot], &c->sn.s_big[x.s_slot], s, v, he - hb,
+                                 SSSP_BIG_DEG);
     if (!ok) atomicOr(&c->error, DEVERR_CAPACITY);
 }
 
@@ -462,7 +469,7 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
     const bool filtered = a.ld == nullptr;
     const unsigned nw = (gridDim.x * blockDim.x) >> 5;
     const unsigned wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const unsigned g = grab_size(ns, nw);
+    const unsigned g = grab_size(ns, nw, SSSP_GRAB);
     // Each warp's first grab is static (warp wg takes [wg*g, wg*g + g)); the
     // rest come from the counter, offset past the static range.  A short
     // list then costs no atomics on the shared counter.
