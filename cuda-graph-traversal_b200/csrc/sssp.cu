@@ -41,8 +41,8 @@ namespace g5 {
 
 constexpr int SSSP_THREADS = 256;
 constexpr int RING = 32;  // bucket queues; a relaxation may land at most RING-1 buckets ahead
-constexpr unsigned STAGE_F = 128;    // per-warp staging: frontier
-constexpr unsigned STAGE_S = 128;    //                   heavy set
+constexpr unsigned STAGE_F = 64;     // per-warp staging: frontier
+constexpr unsigned STAGE_S = 64;     //                   heavy set
 constexpr unsigned STAGE_R = 16;     //                   each ring queue
 constexpr unsigned STAGE_Q = 16;     //                   each sub-bucket queue
 // stage_append takes up to 32 entries at once; the ring and sub-bucket
@@ -182,7 +182,18 @@ struct Stage {
     unsigned *qbuf;  // SUB * STAGE_Q, this warp's
     unsigned *qcnt;  // SUB, this warp's
     unsigned long long *bcnt;  // 8 event counts of the block (shared); [7] = frontier light entries
+    unsigned *pv, *pw;         // PEND pushes waiting, this warp's: vertex and what (P_*)
+    unsigned *pcnt;            // their count, always < 32 between calls
 };
+
+// Pushes decided by relaxations wait in a per-warp list and run 32 at a
+// time, one per lane, instead of once per warp step with the few lanes that
+// lowered a distance: the dependent atomics and loads of a push then serve
+// a full warp.
+constexpr unsigned PEND = 64;
+constexpr unsigned P_SAME = 0x100u;  // this bucket's frontier (and heavy set)
+constexpr unsigned P_FINE = 0x200u;  // | j: sub-bucket j's queue (and heavy set)
+constexpr unsigned P_RING = 0x300u;  // | j: the ring queue of bucket B + j
 
 // Per-thread event counts, summed into the control block once per phase.
 struct Counts {
@@ -348,42 +359,24 @@ __device__ __forceinline__ void probe_edges(const SsspArgs &a, Counts &k, EdgePr
 // Offers v the packed distance/parent np (cur = v's packed value as last
 // read); queues v when its distance dropped.  All 32 lanes call it (want =
 // lane has a candidate for a vertex not settled).
-__device__ __forceinline__ void lower(const SsspArgs &a, const PushCtx &x, Counts &k, bool want, unsigned v,
-                                      unsigned long long np, unsigned long long cur, bool heavy_phase) {
-    bool same = false;
-    int target = -1, fine = -1;
-    if (want) {
-        const float cand = pack_dist(np);
-        if (np < cur) {
-            ++k.atomics;
-            const unsigned long long old = atomicMin(&a.pack[v], np);
-            if (np < old && (old >> 32) != (np >> 32)) {
-                ++k.improved;
-                if (cand < x.bnd[1]) {
-                    if (heavy_phase) atomicOr(&a.ctl->error, DEVERR_CAPACITY);  // cannot happen: w >= delta
-                    if (cand < x.sub_hi) same = true;
-                    else fine = sub_index(x.sub, cand);  // a later sub-bucket of this bucket
-                } else {
-                    // Largest j with b_{B+j} <= cand; the ring holds B+1 .. B+RING-1.
-                    int j = 1;
-                    while (j < RING && x.bnd[j + 1] <= cand) ++j;
-                    if (j >= RING) atomicOr(&a.ctl->error, DEVERR_RING);
-                    else target = (int)x.bucket + j;
-                }
-            }
-        }
-    }
-    if (!__any_sync(FULL, same || target >= 0 || fine >= 0)) return;  // nothing lowered in this warp step
-    push_same_bucket(a, x, k, same && !heavy_phase, (same || fine >= 0) && !heavy_phase, v);
+// Runs the pushes of up to 32 waiting entries, one per lane (have = the lane
+// holds one: vertex v, what = P_* | argument).  All 32 lanes call it.
+__device__ __forceinline__ void run_pushes(const SsspArgs &a, const PushCtx &x, Counts &k, bool have, unsigned v,
+                                        unsigned what) {
+    const unsigned cls = what & 0xf00u, arg = what & 0xffu;
+    const bool same = have && cls == P_SAME;
+    const int fine = have && cls == P_FINE ? (int)arg : -1;
+    const int target = have && cls == P_RING ? (int)(x.bucket + arg) : -1;
+    push_same_bucket(a, x, k, same, same || fine >= 0, v);
     if (x.sub_mode) {
-        push_fine(a, x, heavy_phase ? -1 : fine, v);
+        push_fine(a, x, fine, v);
         k.front += fine >= 0;
     }
     // Ring queue of the target bucket, once per (vertex, bucket), staged in
     // the block's shared memory.
     const bool r = target >= 0 && atomicExch(&a.qstamp[v], (unsigned)target) != (unsigned)target;
     k.ring += r;
-    k.front += same && !heavy_phase;
+    k.front += same;
     // Per-slot warp staging: lanes with the same target slot append
     // together; a full slot is flushed to its global queue first.
     const int slot = r ? target % RING : RING;
@@ -397,6 +390,67 @@ __device__ __forceinline__ void lower(const SsspArgs &a, const PushCtx &x, Count
             atomicOr(&a.ctl->error, DEVERR_CAPACITY);
         todo &= ~m;
     }
+}
+
+// Runs the waiting pushes of this warp (at the end of a phase).  All 32
+// lanes call it.
+__device__ __forceinline__ void drain_pushes(const SsspArgs &a, const PushCtx &x, Counts &k) {
+    __syncwarp();
+    const unsigned c = *x.st.pcnt;
+    if (!c) return;
+    const bool have = lane_id() < c;
+    run_pushes(a, x, k, have, have ? x.st.pv[lane_id()] : 0u, have ? x.st.pw[lane_id()] : 0u);
+    __syncwarp();
+    if (lane_id() == 0) *x.st.pcnt = 0;
+    __syncwarp();
+}
+
+// Offers v the packed distance/parent np (cur = v's packed value as last
+// read); when its distance drops, queues the push it needs (this bucket's
+// frontier, a later sub-bucket or a later bucket).  All 32 lanes call it
+// (want = lane has a candidate for a vertex not settled).
+__device__ __forceinline__ void lower(const SsspArgs &a, const PushCtx &x, Counts &k, bool want, unsigned v,
+                                      unsigned long long np, unsigned long long cur, bool heavy_phase) {
+    unsigned what = 0;
+    if (want) {
+        const float cand = pack_dist(np);
+        if (np < cur) {
+            ++k.atomics;
+            const unsigned long long old = atomicMin(&a.pack[v], np);
+            if (np < old && (old >> 32) != (np >> 32)) {
+                ++k.improved;
+                if (cand < x.bnd[1]) {
+                    if (heavy_phase) atomicOr(&a.ctl->error, DEVERR_CAPACITY);  // cannot happen: w >= delta
+                    else if (cand < x.sub_hi) what = P_SAME;
+                    else what = P_FINE | (unsigned)sub_index(x.sub, cand);  // a later sub-bucket of this bucket
+                } else {
+                    // Largest j with b_{B+j} <= cand; the ring holds B+1 .. B+RING-1.
+                    int j = 1;
+                    while (j < RING && x.bnd[j + 1] <= cand) ++j;
+                    if (j >= RING) atomicOr(&a.ctl->error, DEVERR_RING);
+                    else what = P_RING | (unsigned)j;
+                }
+            }
+        }
+    }
+    const unsigned m = __ballot_sync(FULL, what != 0);
+    if (!m) return;  // nothing lowered in this warp step
+    unsigned c = *x.st.pcnt;  // < 32, so c + 32 <= PEND
+    if (what) {
+        const unsigned i = c + __popc(m & lanemask_lt());
+        x.st.pv[i] = v;
+        x.st.pw[i] = what;
+    }
+    c += __popc(m);
+    __syncwarp();
+    if (c >= 32) {  // run the last 32 (one per lane); the rest stays below 32
+        c -= 32;
+        const unsigned pv = x.st.pv[c + lane_id()], pw = x.st.pw[c + lane_id()];
+        __syncwarp();
+        run_pushes(a, x, k, true, pv, pw);
+    }
+    if (lane_id() == 0) *x.st.pcnt = c;
+    __syncwarp();
 }
 
 // Relaxes u -> v with float weight wt from distance du (cur = v's packed
@@ -413,6 +467,7 @@ __device__ __forceinline__ void relax(const SsspArgs &a, const PushCtx &x, Count
 // end of a phase (it synchronises the block once).
 __device__ void stage_flush(const SsspArgs &a, const PushCtx &x, Counts &k) {
     SsspCtl *c = a.ctl;
+    drain_pushes(a, x, k);
     {
         unsigned long long v[7] = {k.edges, k.settled, k.atomics, k.improved, k.ring, k.front, k.s_entries};
         unsigned long long *dst[8] = {&c->n_edges, &c->n_settled, &c->n_atomic, &c->n_improved, &c->n_ring,
@@ -798,6 +853,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
     __shared__ unsigned s_fbuf[WARPS][STAGE_F], s_sbuf[WARPS][STAGE_S], s_rbuf[WARPS][RING * STAGE_R];
     __shared__ unsigned s_fcnt[WARPS], s_scnt[WARPS], s_rcnt[WARPS][RING];
     __shared__ unsigned s_qbuf[WARPS][SUB * STAGE_Q], s_qcnt[WARPS][SUB];
+    __shared__ unsigned s_pv[WARPS][PEND], s_pw[WARPS][PEND], s_pcnt[WARPS];
     __shared__ unsigned long long s_best[WARPS][32];
     __shared__ unsigned long long s_bcnt[8];
     __shared__ SsspSnap s_snap;
@@ -808,9 +864,11 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
     if (lane_id() == 0) s_fcnt[wid] = s_scnt[wid] = 0;
     if (lane_id() < RING) s_rcnt[wid][lane_id()] = 0;
     for (int j = lane_id(); j < SUB; j += 32) s_qcnt[wid][j] = 0;
+    if (lane_id() == 0) s_pcnt[wid] = 0;
     __syncwarp();
     const Stage stage{WarpStage{s_fbuf[wid], &s_fcnt[wid], STAGE_F}, WarpStage{s_sbuf[wid], &s_scnt[wid], STAGE_S},
-                      s_rbuf[wid], s_rcnt[wid], s_qbuf[wid], s_qcnt[wid], s_bcnt};
+                      s_rbuf[wid], s_rcnt[wid], s_qbuf[wid], s_qcnt[wid], s_bcnt, s_pv[wid], s_pw[wid],
+                      &s_pcnt[wid]};
     unsigned epoch = 0;
     const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
