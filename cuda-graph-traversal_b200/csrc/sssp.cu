@@ -66,6 +66,7 @@ constexpr unsigned SSSP_GRAB = 32;
 constexpr int SUB = 32;
 constexpr unsigned long long SPLIT_MIN = 1ull << 25;  // default; g5_sssp_params.sub_min overrides
 constexpr float SSSP_PULL_RATIO = 1.0f;  // default heavy-phase pull threshold
+constexpr double PULL_WALK = 0.25;       // cost of a pull's bitmap walk, in CSR entries per vertex
 constexpr unsigned long long UNREACHED = ~0ull;
 
 // List sizes that every block reads after a grid barrier.  They lead the
@@ -1070,8 +1071,11 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
             const unsigned long long s_ent = sp->s_entries[sb];
             // Every block reads the same counters after the barrier, so all
             // take the same branch.
+            // A pull walks every word of the settled bitmap besides the
+            // unsettled rows: that walk counts as PULL_WALK entries a vertex.
             const bool pull = a.pull_ratio > 0.0f &&
-                              (double)s_ent >= (double)a.pull_ratio * (double)(e_total - settled_entries - s_ent);
+                              (double)s_ent >= (double)a.pull_ratio * ((double)(e_total - settled_entries - s_ent) +
+                                                                       PULL_WALK * (double)a.n);
             settled_entries += s_ent;
             if (!pull) {
                 expand_list(a, x, cnt, x.Sl, ns, bp, x.SBl, &c->grab[s_cur], &c->cgrab[s_cur], true, sparse_out);
