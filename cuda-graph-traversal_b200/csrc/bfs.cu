@@ -48,7 +48,7 @@ constexpr int BFS_TRACE = 64;                    // levels recorded in the contr
 struct LevelState {
     int level, mode, cur, pending, levels, bu_levels;
     unsigned n_f;
-    unsigned pad;
+    unsigned ucur;  // bottom-up: the unvisited list is q[ucur] (q[ucur ^ 1] takes the survivors)
     unsigned long long m_f, m_u, reached;
 };
 static_assert(sizeof(LevelState) % 8 == 0, "LevelState is copied in 8-byte words");
@@ -62,6 +62,7 @@ struct BfsCtl {
     unsigned grab[3];     //                 work cursor over the small part
     unsigned cgrab[3];    //                 work cursor over the big part's chunks
     unsigned found[3];    //                 vertices found by a bottom-up level
+    unsigned ulen[3];     //                 bottom-up: entries of the unvisited list
     unsigned long long m_next[3];  //        degree sum of the next frontier
     // hand-off from the solo prologue to the grid
     unsigned long long go;  // launch sequence << 2 | 1 (continue on the grid) or 2 (finished)
@@ -87,6 +88,7 @@ struct BfsArgs {
     unsigned *visited;
     unsigned *fbits;
     unsigned *nbits;
+    unsigned *zbits;    // third frontier bitmap: bottom-up levels rotate fb -> zb -> nb
     unsigned *q[2];
     unsigned *base[2];  // chunk bases of each queue's big part
     BfsCtl *ctl;
@@ -194,42 +196,56 @@ __device__ void td_expand(const BfsArgs &a, const WarpStage &bq, int level, int 
     if (!stage_flush_warp(bq, QN, a.n, &c->n_small[s_nxt])) atomicOr(&c->res.error_flags, DEVERR_CAPACITY);
 }
 
-__device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsigned *nb, unsigned long long &my_m,
+__device__ void bu_expand(const BfsArgs &a, const WarpStage &bq, const LevelState &st, int s_cur, int s_nxt,
+                          const unsigned *fb, unsigned *nb, unsigned *zb, unsigned long long &my_m,
                           unsigned &my_found) {
+    BfsCtl *c = a.ctl;
     const unsigned lane = lane_id();
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    // Software pipeline over the warp's words: while word k is scanned, the
-    // row bounds of word k+1 (for its unvisited lanes, known from its
-    // visited word, loaded one step earlier) and the visited word of word
-    // k+2 are in flight, so a word's scan does not start with two dependent
-    // round trips.  Each word has one owner warp, which alone writes its
-    // visited word in this level.
-    auto vis_at = [&](uint64_t kk) -> unsigned { return kk < a.nwords ? __ldcg(&a.visited[kk]) : FULL; };
-    auto bounds = [&](uint64_t kk, unsigned vw, uint64_t &b, uint64_t &e) {
-        const uint64_t vv = kk * 32 + lane;
+    const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+    // The unvisited vertices are a list (built when the search turned
+    // bottom-up, then the survivors of each level), 32 per warp step, so a
+    // level costs its unvisited vertices, not N/32 bitmap words with a few
+    // live lanes each.  Found vertices set their visited and next-frontier
+    // bits with atomics (a word's vertices are spread over warps).
+    const unsigned *U = a.q[st.ucur];
+    unsigned *UN = a.q[st.ucur ^ 1];
+    const uint64_t len = ld_volatile(&c->ulen[s_cur]);
+    // zb, the frontier bitmap of the level before, becomes the clean
+    // next-frontier bitmap of the level after; nobody reads it now.
+    for (uint64_t k = gtid; k < a.nwords; k += nthreads) zb[k] = 0;
+    // Software pipeline over the warp's chunks of 32 entries: while chunk j
+    // is scanned, the row bounds of chunk j+1 and the list entries of chunk
+    // j+2 are in flight.
+    constexpr unsigned NONE = 0xffffffffu;
+    auto ent = [&](uint64_t ch) -> unsigned {
+        const uint64_t i = ch * 32 + lane;
+        return i < len ? __ldcg(&U[i]) : NONE;
+    };
+    auto bounds = [&](unsigned vv, uint64_t &b, uint64_t &e) {
         b = e = 0;
-        if (kk < a.nwords && vv < a.n && !((vw >> lane) & 1u)) {
+        if (vv < a.n) {
             b = __ldg(&a.rowptr[vv]);
             e = __ldg(&a.rowptr[vv + 1]);
         }
     };
-    unsigned vis_n = vis_at(warp), vis_nn = vis_at(warp + nwarps);
+    const uint64_t nch = (len + 31) / 32;
+    unsigned v_n = ent(warp), v_nn = ent(warp + nwarps);
     uint64_t rb_n, re_n;
-    bounds(warp, vis_n, rb_n, re_n);
-    for (uint64_t k = warp; k < a.nwords; k += nwarps) {
-        const unsigned vis = vis_n;
-        const uint64_t rb_k = rb_n, re_k = re_n;
-        vis_n = vis_nn;
-        bounds(k + nwarps, vis_n, rb_n, re_n);
-        vis_nn = vis_at(k + 2 * nwarps);
-        const uint64_t v = k * 32 + lane;
+    bounds(v_n, rb_n, re_n);
+    for (uint64_t ch = warp; ch < nch; ch += nwarps) {
+        const unsigned v = v_n;
+        const uint64_t rb = rb_n, re = re_n;
+        v_n = v_nn;
+        bounds(v_n, rb_n, re_n);
+        v_nn = ent(ch + 2 * nwarps);
+        if (v != NONE && v >= a.n) atomicOr(&c->res.error_flags, DEVERR_RANGE);
+        const bool live = v < a.n;
         int found = -1;
-        uint64_t rb = 0, re = 0;
-        uint64_t e = 0;  // next entry of the row to look at
-        if (v < a.n && !((vis >> lane) & 1u)) {
-            rb = rb_k;
-            re = re_k;
+        uint64_t e = rb;  // next entry of the row to look at
+        if (live) {
             // Each lane scans the head of its own row, BU_STEP neighbours per
             // step: their loads and bitmap probes are independent, so a step
             // costs one memory round trip, not BU_STEP.
@@ -242,7 +258,7 @@ __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsig
                 for (int i = 0; i < BU_STEP; ++i) word[i] = u[i] < a.n ? __ldcg(&fb[u[i] >> 5]) : 0u;
 #pragma unroll
                 for (int i = 0; i < BU_STEP; ++i) {
-                    if (e + i < re && u[i] >= a.n) atomicOr(&a.ctl->res.error_flags, DEVERR_RANGE);
+                    if (e + i < re && u[i] >= a.n) atomicOr(&c->res.error_flags, DEVERR_RANGE);
                     if (found < 0 && u[i] < a.n && ((word[i] >> (u[i] & 31)) & 1u)) found = (int)u[i];
                 }
             }
@@ -250,9 +266,8 @@ __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsig
         // The rest of every longer row is scanned by the whole warp, 32
         // consecutive entries per step (coalesced), stopping at the first
         // step with a hit; the row's first frontier neighbour is taken, as
-        // in the lane scan.  A warp no longer waits on one lane walking a
-        // long row four entries at a time.
-        unsigned longrows = __ballot_sync(FULL, found < 0 && e < re);
+        // in the lane scan.
+        unsigned longrows = __ballot_sync(FULL, live && found < 0 && e < re);
         while (longrows) {
             const int src = __ffs(longrows) - 1;
             longrows &= longrows - 1;
@@ -261,7 +276,7 @@ __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsig
             for (uint64_t x0 = b0; x0 < end; x0 += 32) {
                 const uint64_t xe = x0 + lane;
                 const unsigned u = xe < end ? (unsigned)__ldg(&a.col[xe]) : a.n;
-                if (xe < end && u >= a.n) atomicOr(&a.ctl->res.error_flags, DEVERR_RANGE);
+                if (xe < end && u >= a.n) atomicOr(&c->res.error_flags, DEVERR_RANGE);
                 const bool hit = u < a.n && ((__ldcg(&fb[u >> 5]) >> (u & 31)) & 1u);
                 const unsigned m = __ballot_sync(FULL, hit);
                 if (m) {
@@ -271,17 +286,52 @@ __device__ void bu_expand(const BfsArgs &a, int level, const unsigned *fb, unsig
             }
             if (lane == (unsigned)src) found = hitv;
         }
-        const unsigned mask = __ballot_sync(FULL, found >= 0);
         if (found >= 0) {
             a.pred[v] = found;
-            if (a.depth) a.depth[v] = level + 1;
+            if (a.depth) a.depth[v] = st.level + 1;
+            const unsigned bit = 1u << (v & 31);
+            atomicOr(&a.visited[v >> 5], bit);
+            atomicOr(&nb[v >> 5], bit);
             my_m += re - rb;
+            ++my_found;
         }
-        if (lane == 0) {
-            if (mask) a.visited[k] = vis | mask;
-            nb[k] = mask;
-            my_found += __popc(mask);
+        // Vertices still unvisited go on to the next level's list.
+        if (!stage_append(bq, live && found < 0, v, UN, a.n, &c->ulen[s_nxt]))
+            atomicOr(&c->res.error_flags, DEVERR_CAPACITY);
+    }
+    if (!stage_flush_warp(bq, UN, a.n, &c->ulen[s_nxt])) atomicOr(&c->res.error_flags, DEVERR_CAPACITY);
+}
+
+// The unvisited vertices (visited bit clear) as a list in L, count in
+// *count: each warp counts its words' vertices, reserves its range with one
+// atomicAdd, then writes them in a second pass over the same words.
+__device__ void build_unvisited(const BfsArgs &a, unsigned *L, unsigned *count) {
+    const unsigned lane = lane_id();
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    auto live_bits = [&](uint64_t k) -> unsigned {
+        if (k >= a.nwords) return 0u;
+        unsigned m = ~__ldcg(&a.visited[k]);
+        const uint64_t v0 = k * 32;
+        if (v0 + 32 > a.n) m &= (1u << (a.n - v0)) - 1u;
+        return m;
+    };
+    unsigned long long mine = 0;
+    for (uint64_t base = warp * 32; base < a.nwords; base += nwarps * 32) mine += __popc(live_bits(base + lane));
+    const unsigned long long total = warp_sum(mine);
+    unsigned long long off = 0;
+    if (lane == 0 && total) off = atomicAdd(count, (unsigned)total);
+    off = __shfl_sync(FULL, off, 0);
+    for (uint64_t base = warp * 32; base < a.nwords; base += nwarps * 32) {
+        unsigned m = live_bits(base + lane);
+        const unsigned p = __popc(m);
+        const unsigned incl = warp_incl_scan(p);
+        uint64_t at = off + incl - p;
+        while (m) {
+            L[at++] = (unsigned)((base + lane) * 32 + __ffs(m) - 1);
+            m &= m - 1;
         }
+        off += __shfl_sync(FULL, incl, 31);
     }
 }
 
@@ -333,7 +383,7 @@ enum { PEND_NONE = 0, PEND_TO_BITS = 1, PEND_TO_QUEUE = 2 };
 // Expands level st.level; adds the next frontier's degree sum and (bottom-up)
 // size into slot s_nxt.  No synchronisation.
 __device__ __forceinline__ void bfs_expand_level(const BfsArgs &a, const WarpStage &bq, const LevelState &st,
-                                                 const unsigned *fb, unsigned *nb) {
+                                                 const unsigned *fb, unsigned *nb, unsigned *zb) {
     BfsCtl *c = a.ctl;
     const int s_cur = st.level % 3, s_nxt = (st.level + 1) % 3, s_clr = (st.level + 2) % 3;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -342,6 +392,7 @@ __device__ __forceinline__ void bfs_expand_level(const BfsArgs &a, const WarpSta
         c->grab[s_clr] = 0;
         c->cgrab[s_clr] = 0;
         c->found[s_clr] = 0;
+        c->ulen[s_clr] = 0;
         c->m_next[s_clr] = 0;
     }
     unsigned long long my_m = 0;
@@ -349,7 +400,7 @@ __device__ __forceinline__ void bfs_expand_level(const BfsArgs &a, const WarpSta
     if (st.mode == TOP_DOWN)
         td_expand(a, bq, st.level, st.cur, s_cur, s_nxt, my_m);
     else
-        bu_expand(a, st.level, fb, nb, my_m, my_found);
+        bu_expand(a, bq, st, s_cur, s_nxt, fb, nb, zb, my_m, my_found);
     my_m = warp_sum(my_m);
     my_found = warp_sum(my_found);
     if (lane_id() == 0) {
@@ -360,7 +411,8 @@ __device__ __forceinline__ void bfs_expand_level(const BfsArgs &a, const WarpSta
 
 // After the level's barrier: next frontier size/edges, trace, direction.
 // Returns false when the search is over.
-__device__ __forceinline__ bool bfs_advance(const BfsArgs &a, LevelState &st, unsigned *&fb, unsigned *&nb) {
+__device__ __forceinline__ bool bfs_advance(const BfsArgs &a, LevelState &st, unsigned *&fb, unsigned *&nb,
+                                            unsigned *&zb) {
     BfsCtl *c = a.ctl;
     const int s_nxt = (st.level + 1) % 3;
     const unsigned long long m_next = ld_volatile(&c->m_next[s_nxt]);
@@ -382,9 +434,11 @@ __device__ __forceinline__ bool bfs_advance(const BfsArgs &a, LevelState &st, un
         st.cur ^= 1;  // the next frontier queue is now q[cur]
         if (next == BOTTOM_UP) st.pending = PEND_TO_BITS;
     } else {
-        unsigned *t = fb;  // the next frontier bitmap is now fb
+        unsigned *t = fb;  // the next frontier bitmap is now fb; zb (cleared) the next one's
         fb = nb;
-        nb = t;
+        nb = zb;
+        zb = t;
+        st.ucur ^= 1;  // the survivors are the next level's unvisited list
         if (next == TOP_DOWN) st.pending = PEND_TO_QUEUE;
     }
     st.mode = next;
@@ -419,7 +473,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
     unsigned epoch = 0;
     const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
-    unsigned *fb = a.fbits, *nb = a.nbits;
+    unsigned *fb = a.fbits, *nb = a.nbits, *zb = a.zbits;
     LevelState st;
     __shared__ unsigned s_stage[BFS_THREADS / 32][BFS_STAGE];
     __shared__ unsigned s_stage_cnt[BFS_THREADS / 32];
@@ -443,7 +497,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
             c->res = g5_bfs_stats{0, 0, 0, 0, 0};
             c->bar = 0;
             for (int k = 0; k < 3; ++k) {
-                c->n_small[k] = c->grab[k] = c->cgrab[k] = c->found[k] = 0;
+                c->n_small[k] = c->grab[k] = c->cgrab[k] = c->found[k] = c->ulen[k] = 0;
                 c->big[k] = c->m_next[k] = 0;
             }
         }
@@ -511,12 +565,12 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
         int solo = 0;
         while (a.nblocks == 1 || (st.mode == TOP_DOWN && st.pending == PEND_NONE && st.m_f <= SOLO_EDGES)) {
             if (a.nblocks == 1 && st.pending != PEND_NONE) break;  // conversions run in the grid loop
-            bfs_expand_level(a, bq, st, fb, nb);
+            bfs_expand_level(a, bq, st, fb, nb, nullptr);  // top-down only (conversions end the loop)
             __threadfence();
             __syncthreads();
             ++solo;
             if (threadIdx.x == 0) atomicAdd(&c->heartbeat, 1u);
-            if (!bfs_advance(a, st, fb, nb)) {
+            if (!bfs_advance(a, st, fb, nb, zb)) {
                 done = true;
                 break;
             }
@@ -570,8 +624,15 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
     for (;;) {
         const int s_cur = st.level % 3;
         if (st.pending == PEND_TO_BITS) {
-            // Frontier bitmap from the queue q[cur].
-            for (uint64_t k = gtid; k < a.nwords; k += nthreads) fb[k] = 0;
+            // Frontier bitmap from the queue q[cur]; a clean next-frontier
+            // bitmap; the unvisited list in q[cur ^ 1] (free: its queue was
+            // the level before's).
+            fb = a.fbits;
+            nb = a.nbits;
+            zb = a.zbits;
+            for (uint64_t k = gtid; k < a.nwords; k += nthreads) fb[k] = nb[k] = 0;
+            st.ucur = st.cur ^ 1;
+            build_unvisited(a, a.q[st.ucur], &c->ulen[s_cur]);
             if (!grid_sync(&c->bar, &c->res.error_flags, epoch, a.nblocks, a.limit_ns)) return;
             const unsigned *Q = a.q[st.cur];
             const unsigned ns = ld_volatile(&c->n_small[s_cur]), nbg = big_count(ld_volatile(&c->big[s_cur]));
@@ -589,9 +650,9 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
             if (!grid_sync(&c->bar, &c->res.error_flags, epoch, a.nblocks, a.limit_ns)) return;
         }
         st.pending = PEND_NONE;
-        bfs_expand_level(a, bq, st, fb, nb);
+        bfs_expand_level(a, bq, st, fb, nb, zb);
         if (!grid_sync(&c->bar, &c->res.error_flags, epoch, a.nblocks, a.limit_ns)) return;
-        if (!bfs_advance(a, st, fb, nb)) break;
+        if (!bfs_advance(a, st, fb, nb, zb)) break;
     }
     if (gtid == 0) bfs_write_stats(a, st);
 }
@@ -677,7 +738,7 @@ __global__ void __launch_bounds__(BFS_THREADS) bfs_small_kernel(BfsArgs a) {
 
 struct BfsWork {
     BfsCtl *ctl;
-    unsigned *visited, *fbits, *nbits;
+    unsigned *visited, *fbits, *nbits, *zbits;
     unsigned *q[2], *base[2];
     uint64_t bytes;
 };
@@ -690,6 +751,7 @@ static BfsWork carve_bfs(void *base, uint64_t n) {
     w.visited = c.take<unsigned>(words);
     w.fbits = c.take<unsigned>(words);
     w.nbits = c.take<unsigned>(words);
+    w.zbits = c.take<unsigned>(words);
     for (int i = 0; i < 2; ++i) {
         w.q[i] = c.take<unsigned>(n);
         w.base[i] = c.take<unsigned>(n);
@@ -853,6 +915,7 @@ static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32
     a.visited = w.visited;
     a.fbits = w.fbits;
     a.nbits = w.nbits;
+    a.zbits = w.zbits;
     a.q[0] = w.q[0];
     a.q[1] = w.q[1];
     a.base[0] = w.base[0];
@@ -889,7 +952,7 @@ static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32
     attrs[0].val.cooperative = blocks > 1;  // one block has nothing to co-schedule
     cfg.attrs = attrs;
     cfg.numAttrs = 1;
-    const uint64_t win = (uint64_t)((char *)(w.nbits + a.nwords) - (char *)w.visited);
+    const uint64_t win = (uint64_t)((char *)(w.zbits + a.nwords) - (char *)w.visited);
     uint64_t win_bytes = 0;
     if (blocks > 1 && (rc = l2_persist_window(win, &win_bytes))) return rc;
     if (win_bytes) {
