@@ -510,6 +510,14 @@ def generate_bfs_roots(g: OnedGraph, seed1: int = 2, seed2: int = 3, max_roots: 
 
 # ----------------------------------------------------------------- BFS ----
 
+def bfs_workspace_bytes(nverts: int) -> int:
+    """Bytes of the BFS workspace for a graph of nverts vertices
+    (g5_bfs_workspace_size)."""
+    nb = C.c_uint64()
+    _check(lib.g5_bfs_workspace_size(nverts, C.byref(nb)))
+    return nb.value
+
+
 class BfsState:
     """Bfs_State (src/traversal.h:18-28): pred int64[N], depth int32[N],
     dist int64[N] (filled by bfs_compute_dist_from_pred) and the kernel's

@@ -8,7 +8,11 @@ pending SSSP queue and a pool of CUDA streams ("slots").  Whenever a slot is
 free it launches the oldest waiting work:
 
 * all pending BFS queries of a graph (up to 256) become one batched search
-  (g5_msbfs_run + depth export) on that graph's batched-BFS workspace;
+  (g5_msbfs_run + depth export) on that graph's batched-BFS workspace --
+  when at least `bfs_batch_min` (8) are waiting; fewer are answered one at a
+  time by the plain search on a pooled BFS workspace, which costs less than
+  a batched search below about 8 roots (SCALE 16-24: a batch of one root
+  takes 4-6x a plain search, a batch of 16 about 1.1x two plain searches);
 * an SSSP query runs on its own (distances differ per source) on a pooled
   SSSP workspace of that graph.
 
@@ -40,8 +44,9 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from . import (MSBFS_MAX_ROOTS, BfsState, MsBfsParams, MsBfsState, OnedGraph, SsspState, msbfs_depths_u8,
-               msbfs_run, msbfs_stats, oned_graph_bfs_run, oned_graph_sssp_reset, oned_graph_sssp_traverse,
+from . import (MSBFS_MAX_ROOTS, BfsParams, BfsState, MsBfsParams, MsBfsState, OnedGraph, SsspState,
+               bfs_stats, bfs_workspace_bytes, msbfs_depths_u8, msbfs_run, msbfs_stats, oned_graph_bfs_reset,
+               oned_graph_bfs_run, oned_graph_bfs_traverse, oned_graph_sssp_reset, oned_graph_sssp_traverse,
                search_grid, sssp_status, sssp_workspace_bytes)
 
 
@@ -87,6 +92,7 @@ class ServerStats:
     launches: int = 0
     bfs_batches: int = 0
     bfs_batched_queries: int = 0
+    bfs_single: int = 0
     sssp_launches: int = 0
     max_inflight: int = 0
     workspaces: dict = field(default_factory=dict)
@@ -95,7 +101,8 @@ class ServerStats:
 
 class GraphServer:
     def __init__(self, graphs: list[OnedGraph], slots: int = 4, hbm_reserve: int = 8 << 30,
-                 max_batch: int = MSBFS_MAX_ROOTS, keep_results: bool = False, max_sssp_per_graph: int = 4):
+                 max_batch: int = MSBFS_MAX_ROOTS, keep_results: bool = False, max_sssp_per_graph: int = 4,
+                 bfs_batch_min: int = 8):
         if not graphs:
             raise ValueError("GraphServer needs at least one graph")
         self.graphs = graphs
@@ -106,14 +113,17 @@ class GraphServer:
         self.max_batch = int(max_batch)
         self.keep = keep_results
         self.max_sssp = int(max_sssp_per_graph)
+        self.bfs_batch_min = max(1, int(bfs_batch_min))
+        self.bfs_free: list[list[BfsState]] = [[] for _ in graphs]
+        self.bfs_count = [0] * len(graphs)
         self.pending = {k: [collections.deque() for _ in graphs] for k in ("bfs", "sssp")}
         self.ms: list[MsBfsState | None] = [None] * len(graphs)
         self.ms_busy = [False] * len(graphs)
         self.sssp_free: list[list[SsspState]] = [[] for _ in graphs]
         self.sssp_count = [0] * len(graphs)
         self.inflight: list[_Launch] = []
-        self.grid = {k: [search_grid(k, g.nglobalverts)[0] for g in graphs] for k in ("msbfs", "sssp")}
-        self.max_blocks = min(search_grid(k, 1)[1] for k in ("msbfs", "sssp"))
+        self.grid = {k: [search_grid(k, g.nglobalverts)[0] for g in graphs] for k in ("bfs", "msbfs", "sssp")}
+        self.max_blocks = min(search_grid(k, 1)[1] for k in ("bfs", "msbfs", "sssp"))
         self.blocks_in_use = 0
         self.stats = ServerStats()
         self.clock0 = time.perf_counter()
@@ -135,6 +145,18 @@ class GraphServer:
             self.ms[gi] = MsBfsState(g)
             self.stats.workspaces[f"msbfs{gi}"] = self.ms[gi].work.numel()
         return self.ms[gi]
+
+    def _bfs_state(self, gi: int) -> BfsState | None:
+        if self.bfs_free[gi]:
+            return self.bfs_free[gi].pop()
+        if self.bfs_count[gi] >= self.max_sssp:
+            return None
+        g = self.graphs[gi]
+        if not self._fits(bfs_workspace_bytes(g.nglobalverts) + 12 * g.nglobalverts):  # + pred, depth
+            return None
+        self.bfs_count[gi] += 1
+        self.stats.workspaces[f"bfs{gi}_{self.bfs_count[gi]}"] = 1
+        return BfsState(g)
 
     def _sssp_state(self, gi: int) -> SsspState | None:
         if self.sssp_free[gi]:
@@ -185,13 +207,29 @@ class GraphServer:
         k = min(len(self.streams), len(self.inflight) + len(cands))
         share = max(1, self.max_blocks // max(1, k))
         for _, kind, gi in cands:
-            blocks = min(self.grid["msbfs" if kind == "bfs" else "sssp"][gi], share)
+            single = kind == "bfs" and len(self.pending["bfs"][gi]) < self.bfs_batch_min
+            gk = ("bfs" if single else "msbfs") if kind == "bfs" else "sssp"
+            blocks = min(self.grid[gk][gi], share)
             if self.blocks_in_use + blocks > self.max_blocks:
                 # Oldest first: younger work may not take the SMs this
                 # launch is waiting for (a full-device search would starve).
                 return False
             g = self.graphs[gi]
-            if kind == "bfs":
+            if single:
+                st = self._bfs_state(gi)
+                if st is None:
+                    continue
+                slot = self.free_slots.pop()
+                q = self.pending["bfs"][gi].popleft()
+                s = self.streams[slot]
+                with torch.cuda.stream(s):
+                    oned_graph_bfs_reset(st, True, g, stream=s)
+                    oned_graph_bfs_traverse(g, st, q.root, BfsParams(14.0, 24.0, 0, blocks), True, stream=s)
+                    ev = torch.cuda.Event()
+                    ev.record(s)
+                self.inflight.append(_Launch(ev, [q], "bfs1", gi, slot, st, blocks))
+                self.stats.bfs_single += 1
+            elif kind == "bfs":
                 ms = self._ms_state(gi)
                 if ms is None:
                     continue
@@ -230,7 +268,13 @@ class GraphServer:
 
     def _complete(self, L: _Launch, t: float) -> list[Result]:
         out = []
-        if L.kind == "bfs":
+        if L.kind == "bfs1":
+            bfs_stats(L.resource, self.streams[L.slot])  # raises on a device error
+            q = L.queries[0]
+            v = L.resource.depth.clone() if self.keep else None
+            out.append(Result(q.qid, "bfs", q.graph, q.root, q.arrival, t, 1, v))
+            self.bfs_free[L.graph].append(L.resource)
+        elif L.kind == "bfs":
             msbfs_stats(L.resource, self.streams[L.slot])  # raises on a device error
             for i, q in enumerate(L.queries):
                 v = None

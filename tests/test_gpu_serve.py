@@ -34,6 +34,19 @@ def test_batched_results_equal_alone(cgt, graphs):
     assert s["queries"] == 300 and s["p99_ms"] >= s["p50_ms"] > 0
 
 
+def test_few_bfs_queries_run_single(cgt, graphs):
+    """Fewer than bfs_batch_min waiting BFS queries of a graph take the plain
+    single-root search, with the same depth arrays."""
+    from cgt_b200 import serve
+    trace = [serve.Query(i, "bfs", i % len(graphs), 1 + 7 * i, 0.002 * i) for i in range(6)]
+    srv = serve.GraphServer(graphs, slots=4, hbm_reserve=1 << 30, keep_results=True)
+    res = srv.run_trace(trace, deadline=60.0)
+    assert srv.stats.bfs_single > 0
+    alone = {r.qid: r for r in serve.serve_plain(graphs, trace, keep_results=True)}
+    for r in res:
+        assert torch.equal(r.value, alone[r.qid].value), r.qid
+
+
 def test_small_graph_searches_overlap(cgt, graphs):
     """SSSP queries on small graphs use small grids and run side by side."""
     from cgt_b200 import serve
