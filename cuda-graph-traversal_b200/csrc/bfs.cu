@@ -304,8 +304,10 @@ __device__ void bu_expand(const BfsArgs &a, const WarpStage &bq, const LevelStat
 
 // The unvisited vertices (visited bit clear) as a list in L, count in
 // *count: each warp counts its words' vertices, reserves its range with one
-// atomicAdd, then writes them in a second pass over the same words.
-__device__ void build_unvisited(const BfsArgs &a, unsigned *L, unsigned *count) {
+// atomicAdd, then writes them in a second pass over the same words -- 16
+// words at a time gathered in the warp's shared staging buffer (at most 512
+// vertices) and copied out with coalesced stores.
+__device__ void build_unvisited(const BfsArgs &a, const WarpStage &bq, unsigned *L, unsigned *count) {
     const unsigned lane = lane_id();
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -316,6 +318,7 @@ __device__ void build_unvisited(const BfsArgs &a, unsigned *L, unsigned *count) 
         if (v0 + 32 > a.n) m &= (1u << (a.n - v0)) - 1u;
         return m;
     };
+    static_assert(BFS_STAGE >= 16 * 32, "16 words of vertices fit the staging buffer");
     unsigned long long mine = 0;
     for (uint64_t base = warp * 32; base < a.nwords; base += nwarps * 32) mine += __popc(live_bits(base + lane));
     const unsigned long long total = warp_sum(mine);
@@ -323,15 +326,22 @@ __device__ void build_unvisited(const BfsArgs &a, unsigned *L, unsigned *count) 
     if (lane == 0 && total) off = atomicAdd(count, (unsigned)total);
     off = __shfl_sync(FULL, off, 0);
     for (uint64_t base = warp * 32; base < a.nwords; base += nwarps * 32) {
-        unsigned m = live_bits(base + lane);
-        const unsigned p = __popc(m);
-        const unsigned incl = warp_incl_scan(p);
-        uint64_t at = off + incl - p;
-        while (m) {
-            L[at++] = (unsigned)((base + lane) * 32 + __ffs(m) - 1);
-            m &= m - 1;
+        for (unsigned half = 0; half < 32; half += 16) {
+            const uint64_t k = base + half + lane;
+            unsigned m = lane < 16 ? live_bits(k) : 0u;
+            const unsigned p = __popc(m);
+            const unsigned incl = warp_incl_scan(p);
+            const unsigned t = __shfl_sync(FULL, incl, 31);
+            unsigned at = incl - p;
+            while (m) {
+                bq.buf[at++] = (unsigned)(k * 32 + __ffs(m) - 1);
+                m &= m - 1;
+            }
+            __syncwarp();
+            for (unsigned i = lane; i < t; i += 32) L[off + i] = bq.buf[i];
+            __syncwarp();
+            off += t;
         }
-        off += __shfl_sync(FULL, incl, 31);
     }
 }
 
@@ -632,7 +642,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
             zb = a.zbits;
             for (uint64_t k = gtid; k < a.nwords; k += nthreads) fb[k] = nb[k] = 0;
             st.ucur = st.cur ^ 1;
-            build_unvisited(a, a.q[st.ucur], &c->ulen[s_cur]);
+            build_unvisited(a, bq, a.q[st.ucur], &c->ulen[s_cur]);
             if (!grid_sync(&c->bar, &c->res.error_flags, epoch, a.nblocks, a.limit_ns)) return;
             const unsigned *Q = a.q[st.cur];
             const unsigned ns = ld_volatile(&c->n_small[s_cur]), nbg = big_count(ld_volatile(&c->big[s_cur]));
