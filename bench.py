@@ -39,6 +39,7 @@ FALLBACK_HBM_GBS = 6650.0
 # main-component root, from an ncu capture at SCALE 23 (612.2 MB for 134,213,828 edges,
 # profiles/bfs_persistent_kernel_scale23.md); scaled to the bench's roots by their edges.
 TRAFFIC_BYTES_PER_EDGE = 4.56
+E2E_REPS = 3  # end-to-end calls per root (median kept)
 
 
 def load_package():
@@ -258,6 +259,8 @@ def run_ours(args):
     s_secs_reset = [a.elapsed_time(c) / 1e3 for a, _, c in sev]
     s_hm = hmean_gteps(t_nedge, s_secs)
     s_per_root = np.asarray(t_nedge, np.float64) / np.asarray(s_secs) / 1e9
+    s_alg_bytes = [2 * nedge[timed[i]] * 8 + reached[timed[i]] * 28 for i in big]
+    s_achieved_gbs = float(np.sum(s_alg_bytes) / np.sum([s_secs[i] for i in big]) / 1e9)
     r_last = timed[-1]
     assert G.sssp_validate(g, r_last, sssp.dist, sssp.pred, vw) == 0, "SSSP validation failed"
 
@@ -265,15 +268,22 @@ def run_ours(args):
     # protocol: untimed clear, then per step the root goes host->device from
     # pinned memory, the search runs, and the step's result (its statistics:
     # levels and reached count) is read back to the host.
+    # Each root's call is timed E2E_REPS times (reset untimed before each) and
+    # its median kept: one host wall-clock sample of a ~10-50 us call is at the
+    # mercy of host scheduling noise.
     e2e_s = []
     for r in timed:
-        G.oned_graph_bfs_reset(bfs, with_depth=False, g=g)
-        torch.cuda.synchronize()
-        t = time.perf_counter()
-        # one public call: root host->device (pinned), search, stats back
-        res = G.oned_graph_bfs_query(g, bfs, int(r))
-        e2e_s.append(time.perf_counter() - t)
-        assert res.reached == reached[r]
+        reps = []
+        for _ in range(E2E_REPS):
+            G.oned_graph_bfs_reset(bfs, with_depth=False, g=g)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            # one public call: the device reads the root from pinned host
+            # memory, searches, and writes the statistics back to it
+            res = G.oned_graph_bfs_query(g, bfs, int(r))
+            reps.append(time.perf_counter() - t)
+            assert res.reached == reached[r]
+        e2e_s.append(float(np.median(reps)))
     e2e_hm = hmean_gteps(t_nedge, e2e_s)
 
     # Whole-job numbers across ranks: slowest rank's time, all ranks' edges.
@@ -328,6 +338,7 @@ def run_ours(args):
             "e2e": {"value": float(f"{(e2e_hm if world == 1 else e2e_hm * world):.6g}"), "unit": "GTEPS",
                     "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 24,
                     "small_root_us": round(min(e2e_s) * 1e6, 1) if e2e_s else None,
+                    "timing": f"median of {E2E_REPS} calls per root (reset untimed before each)",
                     "path": "oned_graph_bfs_query -> C ABI g5_bfs_query after an untimed reset: the kernel "
                             "reads the 8-byte root from pinned host memory and writes the 24-byte stats back "
                             "to pinned host memory (over PCIe, inside the timed call), host wall clock"},
@@ -335,7 +346,15 @@ def run_ours(args):
                      "hmean_gteps_with_reset": float(f"{hmean_gteps(t_nedge, s_secs_reset):.6g}"),
                      "median_gteps": round(float(np.median(s_per_root)), 3),
                      "big_root_ms_mean": round(float(np.mean([s_secs[i] for i in big])) * 1e3, 3),
-                     "buckets_last_root": nbuckets, "phases_last_root": nphases, "delta": 0.1},
+                     "buckets_last_root": nbuckets, "phases_last_root": nphases, "delta": 0.1,
+                     # The SSSP kernel against the same HBM roofline: algorithmic bytes
+                     # per search = 2*nedge*(4 col + 4 w) + reached*(8 rowstarts + 8
+                     # packed distance/parent + 12 output).
+                     "roofline": {"bound": "hbm", "kernel": "sssp_persistent_kernel",
+                                  "achieved": round(s_achieved_gbs, 1), "peak": peak, "unit": "GB/s",
+                                  "frac": round(s_achieved_gbs / peak, 4),
+                                  "bytes_per_launch": int(np.mean(s_alg_bytes)),
+                                  "bytes_model": "2*nedge*8 (col + w) + reached*(8 rowstarts + 8 packed + 12 out)"}},
             "construction": {"generation_s": round(gen_s, 4), "csr_build_s": round(csr_s, 4),
                              "setup_total_s": round(setup_s, 2)},
             "nedge_per_root": int(np.median(t_nedge)),
@@ -536,7 +555,8 @@ def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0):
     trace = S.poisson_trace(graphs, nqueries, rate, bfs_share=0.7, seed=1)
     warm = S.poisson_trace(graphs, 64, rate, bfs_share=0.5, seed=99)
     srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots)
-    srv.run_trace(warm, deadline=600)  # workspaces created, batched copies prepared
+    srv.prewarm()  # workspaces created up front (admission by free HBM)
+    srv.run_trace(warm, deadline=600)  # batched copies prepared, kernels loaded
     srv.stats = S.ServerStats()
     res = srv.run_trace(trace, deadline=3600)
     ours = S.latency_summary(res)
@@ -547,6 +567,7 @@ def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0):
     if low_rate:
         ltrace = S.poisson_trace(graphs, nqueries, low_rate, bfs_share=0.7, seed=2)
         srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots)
+        srv.prewarm()
         srv.run_trace(warm, deadline=600)
         low = {"rate_qps": low_rate, "ours": S.latency_summary(srv.run_trace(ltrace, deadline=3600))}
         del srv

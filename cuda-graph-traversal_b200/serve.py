@@ -149,6 +149,9 @@ class GraphServer:
     def _bfs_state(self, gi: int) -> BfsState | None:
         if self.bfs_free[gi]:
             return self.bfs_free[gi].pop()
+        return self._new_bfs_state(gi)
+
+    def _new_bfs_state(self, gi: int) -> BfsState | None:
         if self.bfs_count[gi] >= self.max_sssp:
             return None
         g = self.graphs[gi]
@@ -161,6 +164,9 @@ class GraphServer:
     def _sssp_state(self, gi: int) -> SsspState | None:
         if self.sssp_free[gi]:
             return self.sssp_free[gi].pop()
+        return self._new_sssp_state(gi)
+
+    def _new_sssp_state(self, gi: int) -> SsspState | None:
         if self.sssp_count[gi] >= self.max_sssp:
             return None
         g = self.graphs[gi]
@@ -169,6 +175,24 @@ class GraphServer:
         self.sssp_count[gi] += 1
         self.stats.workspaces[f"sssp{gi}_{self.sssp_count[gi]}"] = 1
         return SsspState(g)
+
+    def prewarm(self) -> None:
+        """Creates the workspaces a trace can use -- per graph the batched-BFS
+        workspace, then plain BFS and SSSP workspaces up to the per-graph cap,
+        round-robin over the graphs -- while admission by free HBM allows, so
+        that no query waits on a first-use allocation."""
+        for gi in range(len(self.graphs)):
+            self._ms_state(gi)
+        for _ in range(self.max_sssp):
+            grew = False
+            for gi in range(len(self.graphs)):
+                for make, free in ((self._new_bfs_state, self.bfs_free), (self._new_sssp_state, self.sssp_free)):
+                    st = make(gi)
+                    if st is not None:
+                        free[gi].append(st)
+                        grew = True
+            if not grew:
+                break
 
     # ------------------------------------------------------------- queueing
     def now(self) -> float:

@@ -19,6 +19,8 @@ def test_batched_results_equal_alone(cgt, graphs):
     from cgt_b200 import serve
     trace = serve.poisson_trace(graphs, 300, rate=20000.0, bfs_share=0.7, seed=3)
     srv = serve.GraphServer(graphs, slots=4, hbm_reserve=1 << 30, keep_results=True)
+    srv.prewarm()
+    assert all(srv.sssp_free[gi] and srv.bfs_free[gi] for gi in range(len(graphs)))
     res = srv.run_trace(trace, deadline=120.0)
     assert sorted(r.qid for r in res) == list(range(300))
     assert srv.stats.bfs_batches < sum(1 for q in trace if q.kind == "bfs")  # queries were batched
