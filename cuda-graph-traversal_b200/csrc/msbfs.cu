@@ -831,46 +831,134 @@ __global__ void ms_export_one_kernel(const unsigned *__restrict__ seen, const un
 // All roots: a thread takes 4 consecutive vertices, reads their rows once
 // and writes 4 bytes per root (a warp writes 128 contiguous bytes of each
 // root's array).
-__global__ void ms_export_u8_kernel(const unsigned *__restrict__ seen, const unsigned *__restrict__ planes,
-                                    const unsigned *__restrict__ pos, uint64_t n, int bits, unsigned nroots,
-                                    uint8_t *__restrict__ out) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+// Word i of b = byte i of a0, a1, a2, a3 (a 4x4 byte transpose).
+__device__ __forceinline__ void transpose_bytes4(unsigned a0, unsigned a1, unsigned a2, unsigned a3, unsigned b[4]) {
+    const unsigned u0 = __byte_perm(a0, a1, 0x5140), u1 = __byte_perm(a0, a1, 0x7362);
+    const unsigned u2 = __byte_perm(a2, a3, 0x5140), u3 = __byte_perm(a2, a3, 0x7362);
+    b[0] = __byte_perm(u0, u2, 0x5410), b[1] = __byte_perm(u0, u2, 0x7632);
+    b[2] = __byte_perm(u1, u3, 0x5410), b[3] = __byte_perm(u1, u3, 0x7632);
+}
+// Transpose of an 8x8 bit matrix stored one row per byte (bit j of byte i
+// becomes bit i of byte j): the three-stage exchange of Hacker's Delight,
+// section 7-3.
+__device__ __forceinline__ uint64_t transpose_bits8x8(uint64_t x) {
+    uint64_t t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
+    x ^= t ^ (t << 7);
+    t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
+    x ^= t ^ (t << 14);
+    t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
+    x ^= t ^ (t << 28);
+    return x;
+}
+// Byte i = 0xFF where bit i of s8 is set, else 0.
+__device__ __forceinline__ uint64_t byte_mask_of_bits(unsigned s8) {
+    const uint64_t t = ((uint64_t)s8 * 0x0101010101010101ull) & 0x8040201008040201ull;
+    return (((t + 0x7F7F7F7F7F7F7F7Full) & 0x8080808080808080ull) >> 7) * 0xFFull;
+}
+
+// Depths of every root as bytes, out[r * n + v] (255 = not reached).  A
+// block takes EX_V vertices at a time.  First the vertex's seen row and its
+// depth-plane rows are loaded whole (32-byte loads) into shared memory, laid
+// out [row kind][word][vertex]; the block's two halves take alternate rows,
+// so each thread has up to 5 loads in flight.  Then thread (w, q) turns word w
+// (32 roots) of vertices 4q..4q+3 into 32 stores of 4 bytes, one per root, a
+// warp's stores covering 128 consecutive bytes of one root's output.  The
+// bit planes become depth bytes by byte permutes and 8x8 bit transposes
+// (about 7 instructions per output byte).  Every row is read once.
+constexpr int EX_V = 128;
+static_assert(EX_V == 4 * 32, "a warp's 32 threads take the 128 vertices four each");
+
+__global__ void __launch_bounds__(256, 2) ms_export_u8_kernel(const unsigned *__restrict__ seen,
+                                                           const unsigned *__restrict__ planes,
+                                                           const unsigned *__restrict__ pos, uint64_t n, int bits,
+                                                           unsigned nroots, uint8_t *__restrict__ out) {
+    __shared__ __align__(16) unsigned s_rows[9][MS_W][EX_V];  // seen, then up to 8 depth planes
+    const unsigned t = threadIdx.x;
+    const unsigned w = t >> 5, q = t & 31;
     const bool aligned = (n & 3) == 0 && ((uintptr_t)out & 3) == 0;
-    for (uint64_t v0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4; v0 < n; v0 += stride * 4) {
-        const unsigned cnt = (unsigned)(n - v0 < 4 ? n - v0 : 4);
-        uint64_t p[4];
+    for (uint64_t base = (uint64_t)blockIdx.x * EX_V; base < n; base += (uint64_t)gridDim.x * EX_V) {
+        {  // the two halves of the block load alternate rows of the same vertex
+            const unsigned vi = t & (EX_V - 1), half = t / EX_V;
+            const uint64_t v = base + vi;
+            const uint64_t p = v < n ? __ldg(&pos[v]) : 0;
+            Row r[5];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) p[j] = (unsigned)j < cnt ? __ldg(&pos[v0 + j]) : 0;
-        for (unsigned w = 0; w * 32 < nroots; ++w) {
-            unsigned sw[4], pw[4][8];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                sw[j] = (unsigned)j < cnt ? __ldg(&seen[p[j] * MS_W + w]) : 0u;
-#pragma unroll
-                for (int k = 0; k < 8; ++k)
-                    pw[j][k] = (k < bits && (unsigned)j < cnt) ? __ldg(&planes[((uint64_t)k * n + p[j]) * MS_W + w]) : 0u;
+            for (int i = 0; i < 5; ++i) {
+                const int k = half + 2 * i;
+                r[i] = row_zero();
+                if (v < n && k <= bits) r[i] = row_ld(k == 0 ? seen : planes + (uint64_t)(k - 1) * n * MS_W, p);
             }
-            const unsigned lim = min(32u, nroots - w * 32);
-            for (unsigned b = 0; b < lim; ++b) {
-                unsigned packed = 0;
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    unsigned d = 255;
-                    if ((sw[j] >> b) & 1u) {
-                        d = 0;
+            for (int i = 0; i < 5; ++i) {
+                const int k = half + 2 * i;
+                if (k <= bits) {
 #pragma unroll
-                        for (int k = 0; k < 8; ++k) d |= ((pw[j][k] >> b) & 1u) << k;
-                    }
-                    packed |= d << (8 * j);
-                }
-                uint8_t *dst = out + (uint64_t)(w * 32 + b) * n + v0;
-                if (aligned && cnt == 4) {
-                    *(unsigned *)dst = packed;
-                } else {
-                    for (unsigned j = 0; j < cnt; ++j) dst[j] = (uint8_t)(packed >> (8 * j));
+                    for (int x = 0; x < MS_W; ++x) s_rows[k][x][vi] = row_word(r[i], x);
                 }
             }
         }
+        __syncthreads();
+        if (w * 32 < nroots) {
+            const uint4 S4 = *(const uint4 *)&s_rows[0][w][4 * q];
+            const unsigned S[4] = {S4.x, S4.y, S4.z, S4.w};
+            // L[j][g] = byte g of planes 0..3 of vertex j, H[j][g] of planes 4..7.
+            unsigned L[4][4], H[4][4];
+            {
+                uint4 P[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    P[k] = k < bits ? *(const uint4 *)&s_rows[1 + k][w][4 * q] : make_uint4(0, 0, 0, 0);
+                transpose_bytes4(P[0].x, P[1].x, P[2].x, P[3].x, L[0]);
+                transpose_bytes4(P[0].y, P[1].y, P[2].y, P[3].y, L[1]);
+                transpose_bytes4(P[0].z, P[1].z, P[2].z, P[3].z, L[2]);
+                transpose_bytes4(P[0].w, P[1].w, P[2].w, P[3].w, L[3]);
+            }
+            if (bits > 4) {
+                uint4 P[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    P[k] = 4 + k < bits ? *(const uint4 *)&s_rows[5 + k][w][4 * q] : make_uint4(0, 0, 0, 0);
+                transpose_bytes4(P[0].x, P[1].x, P[2].x, P[3].x, H[0]);
+                transpose_bytes4(P[0].y, P[1].y, P[2].y, P[3].y, H[1]);
+                transpose_bytes4(P[0].z, P[1].z, P[2].z, P[3].z, H[2]);
+                transpose_bytes4(P[0].w, P[1].w, P[2].w, P[3].w, H[3]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int g = 0; g < 4; ++g) H[j][g] = 0;
+            }
+            const uint64_t v0 = base + 4 * q;
+            const unsigned lim = min(32u, nroots - w * 32);
+            const bool whole = aligned && v0 + 4 <= n;
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+                // D[j] byte i = depth of root 32w + 8g + i at vertex j.
+                uint64_t D[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    D[j] = transpose_bits8x8(((uint64_t)H[j][g] << 32) | L[j][g]) |
+                           ~byte_mask_of_bits((S[j] >> (8 * g)) & 0xFFu);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    unsigned o[4];
+                    transpose_bytes4((unsigned)(D[0] >> (32 * h)), (unsigned)(D[1] >> (32 * h)),
+                                     (unsigned)(D[2] >> (32 * h)), (unsigned)(D[3] >> (32 * h)), o);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const unsigned b = 8 * g + 4 * h + i;
+                        if (b >= lim) continue;
+                        uint8_t *dst = out + (uint64_t)(w * 32 + b) * n + v0;
+                        if (whole) {
+                            *(unsigned *)dst = o[i];
+                        } else {
+                            for (unsigned j = 0; j < 4 && v0 + j < n; ++j) dst[j] = (uint8_t)(o[i] >> (8 * j));
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -1023,7 +1111,7 @@ extern "C" int g5_msbfs_depths_u8(const void *d_work, uint64_t work_bytes, uint6
     G5_CHECK_ARG(d_out && nroots >= 1 && nroots <= MS_MAX_ROOTS, "g5_msbfs_depths_u8: bad argument");
     DeviceInfo di;
     if ((rc = device_info(&di))) return rc;
-    ms_export_u8_kernel<<<di.sms * 8, 256, 0, (cudaStream_t)stream>>>(w.seen, w.planes, w.pos, nverts, depth_bits,
+    ms_export_u8_kernel<<<di.sms * 2, 256, 0, (cudaStream_t)stream>>>(w.seen, w.planes, w.pos, nverts, depth_bits,
                                                                        nroots, d_out);
     G5_CUDA_TRY(cudaGetLastError());
     return G5_OK;
