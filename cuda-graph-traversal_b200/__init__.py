@@ -130,9 +130,16 @@ def _ptr(t: torch.Tensor | None) -> int | None:
     return None if t is None else t.data_ptr()
 
 
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+_cur_dev = getattr(torch._C, "_cuda_getDevice", None)
+
+
 def _stream(stream=None) -> int | None:
-    s = stream if stream is not None else torch.cuda.current_stream()
-    return s.cuda_stream or None
+    if stream is not None:
+        return stream.cuda_stream or None
+    if _raw_stream is not None and _cur_dev is not None:
+        return _raw_stream(_cur_dev()) or None  # the current stream without building a Stream object
+    return torch.cuda.current_stream().cuda_stream or None
 
 
 def _workspace(nbytes: int, device) -> torch.Tensor:
@@ -583,6 +590,18 @@ def oned_graph_bfs_traverse(g: OnedGraph, bfs: BfsState, root: int, params: BfsP
                                C.byref(params) if params is not None else None, _stream(stream)))
 
 
+def _main_bits_ptr(g: OnedGraph) -> int | None:
+    """Host address of g.main_bits, looked up once per array."""
+    mb = g.main_bits
+    if mb is None:
+        return None
+    c = g.__dict__.get("_main_bits_addr")
+    if c is None or c[0] is not mb:
+        c = (mb, mb.ctypes.data)
+        g.__dict__["_main_bits_addr"] = c
+    return c[1]
+
+
 def oned_graph_bfs_query(g: OnedGraph, bfs: BfsState, root: int, with_depth: bool = False,
                          stream=None) -> BfsStats:
     """One search end to end from the host (g5_bfs_query): the device reads
@@ -591,10 +610,8 @@ def oned_graph_bfs_query(g: OnedGraph, bfs: BfsState, root: int, with_depth: boo
     host memory; synchronises."""
     bfs._root_slot.value = root
     hr, pred, depth, work, nwork, stats = bfs._q
-    mb = g.main_bits
-    rc = lib.g5_bfs_query(g.rowstarts.data_ptr(), g.col.data_ptr(), g.nglobalverts, hr,
-                          mb.ctypes.data if mb is not None else None, pred, depth if with_depth else None, work,
-                          nwork, None, stats, _stream(stream))
+    rc = lib.g5_bfs_query(g.rowstarts.data_ptr(), g.col.data_ptr(), g.nglobalverts, hr, _main_bits_ptr(g), pred,
+                          depth if with_depth else None, work, nwork, None, stats, _stream(stream))
     if rc:
         _check(rc)
     return bfs.h_stats

@@ -459,7 +459,9 @@ __device__ __forceinline__ bool bfs_advance(const BfsArgs &a, LevelState &st, un
 }
 
 // Copies the finished search's statistics to the caller's mapped host
-// memory (g5_bfs_query), visible to the host once the stream is synchronised.
+// memory (g5_bfs_query), visible to the host once the stream is synchronised
+// (the kernel's completion orders them; no fence is needed while the host
+// does not read before that).
 __device__ __forceinline__ void bfs_publish_stats(const BfsArgs &a) {
     if (!a.stats_out) return;
     volatile g5_bfs_stats *r = &a.ctl->res;
@@ -468,7 +470,6 @@ __device__ __forceinline__ void bfs_publish_stats(const BfsArgs &a) {
     a.stats_out->reached = r->reached;
     a.stats_out->error_flags = r->error_flags;
     a.stats_out->solo_levels = r->solo_levels;
-    __threadfence_system();
 }
 
 __device__ __forceinline__ void bfs_write_stats(const BfsArgs &a, const LevelState &st) {
@@ -668,28 +669,54 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
 }
 
 // A search from a root whose component is small (mode BFS_SMALL): one block,
-// levels top-down with the frontier queues in the workspace, claims on the
-// visited bitmap, level sizes in shared memory -- none of the grid
-// machinery (hand-off, grab counters, staging, grid barriers), so a
-// search of a few vertices costs a few memory round trips per level.
-// Correct for a component of any size, only slow when it is large.
+// levels top-down, claims on the visited bitmap -- none of the grid
+// machinery (hand-off, grab counters, staging, grid barriers).  The first
+// SMALL_Q entries of each frontier live in shared memory together with their
+// row bounds: the lane that claims a vertex loads its two row starts in the
+// same breath as the claim (both issued before either returns), so a level
+// costs one column load and one atomic round trip on its critical path
+// instead of queue, row-start, column and bitmap loads in a chain.  Entries
+// past SMALL_Q go to the workspace queue (vertex only).  Correct for a
+// component of any size, only slow when it is large.
+constexpr unsigned SMALL_Q = 1024;
+
+// Row starts of v and v + 1 and the claim of v's visited bit, issued in this
+// order without waiting for one another; returns the bit's old word.
+__device__ __forceinline__ unsigned claim_with_row(const uint64_t *rowptr, unsigned *visited, unsigned v,
+                                                   uint64_t &rb, uint64_t &re) {
+    const uint64_t *p = rowptr + v;
+    unsigned *w = visited + (v >> 5);
+    unsigned old;
+    asm volatile("ld.global.nc.u64 %0, [%3];\n\t"
+                 "ld.global.nc.u64 %1, [%3+8];\n\t"
+                 "atom.global.or.b32 %2, [%4], %5;"
+                 : "=l"(rb), "=l"(re), "=r"(old)
+                 : "l"(p), "l"(w), "r"(1u << (v & 31))
+                 : "memory");
+    return old;
+}
 __global__ void __launch_bounds__(BFS_THREADS) bfs_small_kernel(BfsArgs a) {
     BfsCtl *c = a.ctl;
+    __shared__ unsigned s_v[2][SMALL_Q];
+    __shared__ uint64_t s_rb[2][SMALL_Q], s_re[2][SMALL_Q];
     __shared__ unsigned s_len[2];
     __shared__ unsigned s_err;
     __shared__ unsigned long long s_reached;
-    const unsigned root = a.root_src ? (unsigned)ld_volatile(a.root_src) : a.root;
     const unsigned lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (threadIdx.x == 0) {
         c->t0 = globaltimer_ns();
+        const unsigned long long root = a.root_src ? ld_volatile(a.root_src) : a.root;
         if (root >= a.n) {
             s_err = DEVERR_RANGE;  // the host checks roots; a bad root_in is reported, not used
             s_len[0] = 0;
         } else {
-            a.visited[root >> 5] |= 1u << (root & 31);
-            a.pred[root] = root;
+            uint64_t rb, re;
+            claim_with_row(a.rowptr, a.visited, (unsigned)root, rb, re);
+            a.pred[root] = (int64_t)root;
             if (a.depth) a.depth[root] = 0;
-            a.q[0][0] = root;
+            s_v[0][0] = (unsigned)root;
+            s_rb[0][0] = rb;
+            s_re[0][0] = re;
             s_len[0] = 1;
             s_err = 0;
         }
@@ -699,33 +726,49 @@ __global__ void __launch_bounds__(BFS_THREADS) bfs_small_kernel(BfsArgs a) {
     __syncthreads();
     int level = 0;
     for (;; ++level) {
-        const int cur = level & 1;
+        const int cur = level & 1, nxt = cur ^ 1;
         const unsigned n = s_len[cur];
         if (n == 0) break;
-        const unsigned *Q = a.q[cur];
-        unsigned *QN = a.q[cur ^ 1];
         // One warp per frontier vertex, its lanes over the vertex's row.
         for (unsigned i = wid; i < n; i += nw) {
-            const unsigned u = __ldcg(&Q[i]);
-            const uint64_t rb = __ldg(&a.rowptr[u]), re = __ldg(&a.rowptr[u + 1]);
+            unsigned u;
+            uint64_t rb, re;
+            if (i < SMALL_Q) {
+                u = s_v[cur][i];
+                rb = s_rb[cur][i];
+                re = s_re[cur][i];
+            } else {
+                u = __ldcg(&a.q[cur][i]);
+                rb = __ldg(&a.rowptr[u]);
+                re = __ldg(&a.rowptr[u + 1]);
+            }
             for (uint64_t e = rb + lane; e < re; e += 32) {
                 const unsigned v = (unsigned)__ldg(&a.col[e]);
                 if (v >= a.n) {  // not a vertex: report it, touch nothing
                     atomicOr(&s_err, DEVERR_RANGE);
                     continue;
                 }
-                const unsigned bit = 1u << (v & 31);
-                if ((__ldcg(&a.visited[v >> 5]) & bit) || (atomicOr(&a.visited[v >> 5], bit) & bit)) continue;
+                uint64_t vb, ve;
+                if (claim_with_row(a.rowptr, a.visited, v, vb, ve) & (1u << (v & 31))) continue;
+                // The next level reads v's row: start bringing it into L2 now.
+                if (vb < ve) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.col + vb));
                 a.pred[v] = u;
                 if (a.depth) a.depth[v] = level + 1;
-                const unsigned pos = atomicAdd(&s_len[cur ^ 1], 1u);  // each vertex is claimed once: pos < n
-                if (pos < a.n) QN[pos] = v;
-                else atomicOr(&s_err, DEVERR_CAPACITY);
+                const unsigned pos = atomicAdd(&s_len[nxt], 1u);  // each vertex is claimed once: pos < n
+                if (pos < SMALL_Q) {
+                    s_v[nxt][pos] = v;
+                    s_rb[nxt][pos] = vb;
+                    s_re[nxt][pos] = ve;
+                } else if (pos < a.n) {
+                    a.q[nxt][pos] = v;
+                } else {
+                    atomicOr(&s_err, DEVERR_CAPACITY);
+                }
             }
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            s_reached += s_len[cur ^ 1];
+            s_reached += s_len[nxt];
             s_len[cur] = 0;
             if (level < BFS_TRACE) {
                 c->t_level[level] = globaltimer_ns();
