@@ -1138,27 +1138,49 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
 
 // A search from a source whose component is small (g5_sssp_params.small):
 // one block, label-correcting rounds (every vertex whose distance dropped in
-// a round relaxes all its edges in the next), lists in the workspace, list
-// sizes in shared memory -- no buckets, phases or grid machinery.  It
-// reaches the same float fixed point, hence the same distances, and the
-// same parents (the smallest u on a tight edge: every vertex relaxes its
-// edges again after its last decrease).  Correct for a component of any
-// size, only slow when it is large.
+// a round relaxes all its edges in the next) -- no buckets, phases or grid
+// machinery.  It reaches the same float fixed point, hence the same
+// distances, and the same parents (the smallest u on a tight edge: every
+// vertex relaxes its edges again after its last decrease).  The first
+// SMALL_L entries of each round's list and of the reached list live in
+// shared memory, list entries with their row bounds, which the relaxing
+// lane loads together with its atomicMin (issued before either returns);
+// the rest go to the workspace lists.  Correct for a component of any size,
+// only slow when it is large.
+constexpr unsigned SMALL_L = 512;
+
+// Row starts of v and v + 1 and atomicMin(pack[v], np), issued in this
+// order without waiting for one another; returns pack[v]'s old value.
+__device__ __forceinline__ unsigned long long relax_with_row(const uint64_t *rowptr, unsigned long long *pack,
+                                                             unsigned v, unsigned long long np, uint64_t &rb,
+                                                             uint64_t &re) {
+    unsigned long long old;
+    asm volatile("ld.global.nc.u64 %0, [%3];\n\t"
+                 "ld.global.nc.u64 %1, [%3+8];\n\t"
+                 "atom.global.min.u64 %2, [%4], %5;"
+                 : "=l"(rb), "=l"(re), "=l"(old)
+                 : "l"(rowptr + v), "l"(pack + v), "l"(np)
+                 : "memory");
+    return old;
+}
 __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
     SsspCtl *c = a.ctl;
+    __shared__ unsigned s_v[2][SMALL_L];
+    __shared__ uint64_t s_rb[2][SMALL_L], s_re[2][SMALL_L];
+    __shared__ unsigned s_r[SMALL_L];
     __shared__ unsigned s_len[2];
     __shared__ unsigned s_nreach;
     __shared__ unsigned s_err;
     const unsigned lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const bool sparse_out = __ldcg((const unsigned long long *)&a.prefilled->dist) == (unsigned long long)a.dist &&
-                            __ldcg((const unsigned long long *)&a.prefilled->pred) == (unsigned long long)a.pred;
-    unsigned *R = a.S[0];  // every vertex reached, once (sstamp)
+    unsigned *R = a.S[0];  // every vertex reached, once (sstamp); entries from SMALL_L on
     if (threadIdx.x == 0) {
         c->t0 = globaltimer_ns();
         a.pack[a.root] = (unsigned long long)a.root;  // distance 0.0f, parent = root
         a.sstamp[a.root] = 0;
-        a.F[0][0] = a.root;
-        R[0] = a.root;
+        s_v[0][0] = a.root;
+        s_rb[0][0] = __ldg(&a.rowptr[a.root]);
+        s_re[0][0] = __ldg(&a.rowptr[a.root + 1]);
+        s_r[0] = a.root;
         s_len[0] = 1;
         s_len[1] = 0;
         s_nreach = 1;
@@ -1167,16 +1189,23 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
     __syncthreads();
     unsigned round = 0;
     for (;; ++round) {
-        const int cur = round & 1;
+        const int cur = round & 1, nxt = cur ^ 1;
         const unsigned n = s_len[cur];
         if (n == 0) break;
-        const unsigned *L = a.F[cur];
-        unsigned *LN = a.F[cur ^ 1];
         // One warp per listed vertex, its lanes over the vertex's row.
         for (unsigned i = wid; i < n; i += nw) {
-            const unsigned u = __ldcg(&L[i]);
+            unsigned u;
+            uint64_t rb, re;
+            if (i < SMALL_L) {
+                u = s_v[cur][i];
+                rb = s_rb[cur][i];
+                re = s_re[cur][i];
+            } else {
+                u = __ldcg(&a.F[cur][i]);
+                rb = __ldg(&a.rowptr[u]);
+                re = __ldg(&a.rowptr[u + 1]);
+            }
             const float du = pack_dist(__ldcg(&a.pack[u]));
-            const uint64_t rb = __ldg(&a.rowptr[u]), re = __ldg(&a.rowptr[u + 1]);
             for (uint64_t e = rb + lane; e < re; e += 32) {
                 const unsigned v = (unsigned)__ldg(&a.col[e]);
                 if (v >= a.n) {  // not a vertex: report it, touch nothing
@@ -1185,17 +1214,27 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
                 }
                 const float cand = __fadd_rn(du, __ldg(&a.w[e]));
                 const unsigned long long np = ((unsigned long long)__float_as_uint(cand) << 32) | u;
-                if (np >= __ldcg(&a.pack[v])) continue;
-                const unsigned long long old = atomicMin(&a.pack[v], np);
+                uint64_t vb, ve;
+                const unsigned long long old = relax_with_row(a.rowptr, a.pack, v, np, vb, ve);
                 if (!(np < old && (old >> 32) != (np >> 32))) continue;  // distance unchanged
-                if (atomicExch(&a.fstamp[v], round) != round) {
-                    const unsigned pos = atomicAdd(&s_len[cur ^ 1], 1u);  // once per vertex and round
-                    if (pos < a.n) LN[pos] = v;
-                    else atomicOr(&s_err, DEVERR_CAPACITY);
+                const unsigned fold = atomicExch(&a.fstamp[v], round);
+                const unsigned sold = atomicExch(&a.sstamp[v], 0u);
+                if (fold != round) {
+                    const unsigned pos = atomicAdd(&s_len[nxt], 1u);  // once per vertex and round
+                    if (pos < SMALL_L) {
+                        s_v[nxt][pos] = v;
+                        s_rb[nxt][pos] = vb;
+                        s_re[nxt][pos] = ve;
+                    } else if (pos < a.n) {
+                        a.F[nxt][pos] = v;
+                    } else {
+                        atomicOr(&s_err, DEVERR_CAPACITY);
+                    }
                 }
-                if (atomicExch(&a.sstamp[v], 0u) != 0u) {
+                if (sold != 0u) {
                     const unsigned pos = atomicAdd(&s_nreach, 1u);
-                    if (pos < a.n) R[pos] = v;
+                    if (pos < SMALL_L) s_r[pos] = v;
+                    else if (pos < a.n) R[pos] = v;
                     else atomicOr(&s_err, DEVERR_CAPACITY);
                 }
             }
@@ -1213,9 +1252,12 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
         __syncthreads();
     }
     // Outputs: the reached vertices (pre-filled outputs) or every vertex.
+    const bool sparse_out = __ldcg((const unsigned long long *)&a.prefilled->dist) == (unsigned long long)a.dist &&
+                            __ldcg((const unsigned long long *)&a.prefilled->pred) == (unsigned long long)a.pred;
     if (sparse_out) {
-        for (unsigned i = threadIdx.x; i < s_nreach; i += blockDim.x) {
-            const unsigned v = __ldcg(&R[i]);
+        const unsigned nr = min(s_nreach, (unsigned)a.n);
+        for (unsigned i = threadIdx.x; i < nr; i += blockDim.x) {
+            const unsigned v = i < SMALL_L ? s_r[i] : __ldcg(&R[i]);
             const unsigned long long p = __ldcg(&a.pack[v]);
             a.dist[v] = pack_dist(p);
             a.pred[v] = (int64_t)(unsigned)p;
@@ -1340,6 +1382,8 @@ extern "C" int g5_sssp_reset(uint64_t nverts, float *d_dist, int64_t *d_pred, vo
     G5_CUDA_TRY(cudaMemsetAsync(w.fstamp, 0xff, (char *)(w.qstamp + nverts) - (char *)w.fstamp, st));
     // settled and cur are consecutive carve-outs: one memset.
     G5_CUDA_TRY(cudaMemsetAsync(w.settled, 0, (char *)(w.cur + (nverts + 31) / 32) - (char *)w.settled, st));
+    // Fresh control block (counters, cursors, trace) for the next search.
+    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(SsspCtl), st));
     return G5_OK;
 }
 
@@ -1396,7 +1440,6 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     a.nblocks = (unsigned)blocks;
     a.limit_ns = wait_limit_ns();
     void *args[] = {&a};
-    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(SsspCtl), st));
     if (p.small && !d_roots)
         sssp_small_kernel<<<1, SSSP_THREADS, 0, st>>>(a);
     else if (blocks == 1)  // nothing to co-schedule: a plain launch

@@ -255,9 +255,10 @@ int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, const float *
  * (src/traversal.cu:625-636 with sssp_clear_kernel :242-253, which also
  * set pred to -1 and dist to -1.0f) +
  * oned_graph_sssp_run: g5_sssp_reset clears the workspace's O(N) arrays
- * (distances, stamps, settled bitmap) and, when given d_dist and d_pred
- * (both or neither), fills them with -1.0f / -1; g5_sssp_traverse zeroes
- * the control block, runs the persistent kernel and writes d_dist / d_pred.
+ * (distances, stamps, settled bitmap) and its control block and, when given
+ * d_dist and d_pred (both or neither), fills them with -1.0f / -1;
+ * g5_sssp_traverse (on a state reset since its last search) runs the
+ * persistent kernel and writes d_dist / d_pred.
  * When the traverse gets the same output arrays the reset pre-filled, it
  * writes only the reached vertices (O(reached) work); otherwise it writes
  * all nverts entries. */
