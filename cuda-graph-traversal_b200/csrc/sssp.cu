@@ -45,6 +45,7 @@ constexpr unsigned STAGE_F = 64;     // per-warp staging: frontier
 constexpr unsigned STAGE_S = 64;     //                   heavy set
 constexpr unsigned STAGE_R = 16;     //                   each ring queue
 constexpr unsigned STAGE_Q = 16;     //                   each sub-bucket queue
+constexpr unsigned STAGE_D = 32;     //                   the sub-bucket's expanded set
 // stage_append takes up to 32 entries at once; the ring and sub-bucket
 // slices are smaller and use stage_push, which writes through when full.
 static_assert(STAGE_F >= 32 && STAGE_S >= 32, "staging slices hold one warp step");
@@ -63,6 +64,15 @@ constexpr unsigned SSSP_GRAB = 32;
 // within its sub-bucket.  On Kronecker graphs the bucket that holds the
 // hubs' neighbourhood has most vertices at nearly equal distances; without
 // this every one of them is re-expanded several times.
+//
+// Inside a sub-bucket only the relaxations that can land in the same
+// sub-bucket (fl(d_u + w) < its upper bound) are made when a vertex is
+// expanded; the others are deferred.  Every vertex expanded in the
+// sub-bucket enters its expanded set once; when the sub-bucket's frontier
+// is empty their distances are final, and a settle pass relaxes each one's
+// deferred light edges once, into later sub-buckets or buckets.  A hub whose
+// distance drops several times inside the sub-bucket then re-reads its light
+// row (weights only decide) but repeats none of its random relaxations.
 constexpr int SUB = 32;
 constexpr unsigned long long SPLIT_MIN = 1ull << 25;  // default; g5_sssp_params.sub_min overrides
 constexpr float SSSP_PULL_RATIO = 1.0f;  // default heavy-phase pull threshold
@@ -81,10 +91,12 @@ struct SsspSnap {
     unsigned long long s_entries[3];  // CSR entries of the heavy set's rows
     unsigned long long f_entries[3];  // light CSR entries of the frontier's rows
     unsigned long long pl_big;        // heavy-phase pull: rows too long for one warp
+    unsigned long long d_big[2];      // expanded set of a sub-bucket (two slots, alternating)
     unsigned f_small[3];
     unsigned s_small[3];
     unsigned ring_len[RING];
     unsigned fq_len[SUB];  // sub-bucket queues of the current bucket
+    unsigned d_small[2];
 };
 constexpr int SNAP_WORDS = (int)(sizeof(SsspSnap) / 4);
 
@@ -136,6 +148,7 @@ struct SsspArgs {
     unsigned long long split_min;  // frontier light entries that start sub-buckets (~0: never)
     unsigned long long *pack;
     unsigned *fstamp, *sstamp, *qstamp;
+    unsigned *dstamp;        // expanded-set stamp: fine_id of the sub-bucket that expanded the vertex
     unsigned *settled;
     unsigned *cur;           // bitmap of the bucket being pulled from (heavy pull only)
     unsigned *F[2], *FB[2];  // frontiers and the chunk bases of their big parts
@@ -177,7 +190,7 @@ __device__ __forceinline__ void settle(const SsspArgs &a, bool sparse_out, unsig
 
 // Per-warp shared-memory staging of every list a phase appends to.
 struct Stage {
-    WarpStage f, s;
+    WarpStage f, s, d;
     unsigned *rbuf;  // RING * STAGE_R, this warp's
     unsigned *rcnt;  // RING, this warp's
     unsigned *qbuf;  // SUB * STAGE_Q, this warp's
@@ -214,6 +227,9 @@ struct PushCtx {
     const float *sub;    // shared: sub-bucket bounds t_0 = b_B .. t_SUB = b_{B+1}
     float sub_hi;        // upper bound of the light frontier's range (t_{j+1}, or b_{B+1})
     bool sub_mode;       // the bucket is processed by sub-buckets
+    unsigned *Dl, *DBl;  // expanded set of the open sub-bucket (borrows the idle heavy-set arrays)
+    int d_slot;          // its counter slot
+    unsigned d_tag;      // its stamp: fine_id(bucket, sub-bucket)
 };
 
 // Sub-bucket queue stamp of (bucket, j), kept apart from bucket-ring stamps
@@ -238,6 +254,9 @@ __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCt
     SsspCtl *c = a.ctl;
     bool f = want_f && atomicExch(&a.fstamp[v], x.pid) != x.pid;
     bool s = want_s && atomicExch(&a.sstamp[v], x.bucket) != x.bucket;
+    // In sub mode a vertex entering the frontier joins the sub-bucket's
+    // expanded set (once per sub-bucket).
+    const bool d = f && x.sub_mode && atomicExch(&a.dstamp[v], x.d_tag) != x.d_tag;
     uint64_t lb = 0, le = 0, hb = 0, he = 0;
     if (f || s) {
         const uint64_t b = __ldg(&a.rowptr[v]), e = __ldg(&a.rowptr[v + 1]);
@@ -262,6 +281,10 @@ __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCt
                                      le - lb, SSSP_BIG_DEG);
     ok &= frontier_append_staged(x.st.s, x.Sl, x.SBl, a.n, &c->sn.s_small[x.s_slot], &c->sn.s_big[x.s_slot], s, v, he - hb,
                                  SSSP_BIG_DEG);
+    // Once per vertex and sub-bucket, so the set stays within n entries.
+    if (x.sub_mode)
+        ok &= frontier_append_staged(x.st.d, x.Dl, x.DBl, a.n, &c->sn.d_small[x.d_slot], &c->sn.d_big[x.d_slot], d, v,
+                                     le - lb, SSSP_BIG_DEG);
     if (!ok) atomicOr(&c->error, DEVERR_CAPACITY);
 }
 
@@ -493,6 +516,7 @@ __device__ void stage_flush(const SsspArgs &a, const PushCtx &x, Counts &k) {
     }
     bool ok = stage_flush_warp(x.st.f, x.Fout, a.n, &c->sn.f_small[x.f_slot]);
     ok &= stage_flush_warp(x.st.s, x.Sl, a.n, &c->sn.s_small[x.s_slot]);
+    if (x.sub_mode) ok &= stage_flush_warp(x.st.d, x.Dl, a.n, &c->sn.d_small[x.d_slot]);
     // Only the slices holding entries (one ballot over their counts).
     static_assert(RING <= 32, "one lane per ring slice");
     __syncwarp();
@@ -515,12 +539,17 @@ __device__ void stage_flush(const SsspArgs &a, const PushCtx &x, Counts &k) {
     if (!ok && lane_id() == 0) atomicOr(&c->error, DEVERR_CAPACITY);
 }
 
+// Which light edges an expansion relaxes: all, only those whose candidate
+// distance falls below x.sub_hi (a sub-bucket's frontier), or only the others
+// (its settle pass).
+enum { SEL_ALL = 0, SEL_SAME = 1, SEL_LATER = 2 };
+
 // Relaxes the light (heavy = false) or heavy edges of every vertex of list L
 // (small part [0, ns), big part at the back, `bp` its packed counter).  The
 // heavy pass also marks each list vertex settled.
 __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, const unsigned *L, unsigned ns,
                             unsigned long long bp, const unsigned *B, unsigned *grab, unsigned *cgrab, bool heavy,
-                            bool sparse_out) {
+                            bool sparse_out, int sel = SEL_ALL) {
     const unsigned lane = lane_id();
     const bool filtered = a.ld == nullptr;
     const unsigned nw = (gridDim.x * blockDim.x) >> 5;
@@ -574,6 +603,7 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
                     p.v[t] = (unsigned)__ldg(&a.col[at]);
                     p.wt[t] = __ldg(&a.w[at]);
                     if (filtered) has = heavy ? !(p.wt[t] < a.light) : p.wt[t] < a.light;
+                    if (sel != SEL_ALL) has = has && ((__fadd_rn(p.du[t], p.wt[t]) < x.sub_hi) == (sel == SEL_SAME));
                 }
                 p.has[t] = has;
             }
@@ -621,6 +651,7 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
                     p.v[t] = (unsigned)__ldg(&a.col[rb + e]);
                     p.wt[t] = __ldg(&a.w[rb + e]);
                     if (filtered) has = heavy ? !(p.wt[t] < a.light) : p.wt[t] < a.light;
+                    if (sel != SEL_ALL) has = has && ((__fadd_rn(du, p.wt[t]) < x.sub_hi) == (sel == SEL_SAME));
                 }
                 p.has[t] = has;
             }
@@ -855,6 +886,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
     __shared__ unsigned s_fcnt[WARPS], s_scnt[WARPS], s_rcnt[WARPS][RING];
     __shared__ unsigned s_qbuf[WARPS][SUB * STAGE_Q], s_qcnt[WARPS][SUB];
     __shared__ unsigned s_pv[WARPS][PEND], s_pw[WARPS][PEND], s_pcnt[WARPS];
+    __shared__ unsigned s_dbuf[WARPS][STAGE_D], s_dcnt[WARPS];
     __shared__ unsigned long long s_best[WARPS][32];
     __shared__ unsigned long long s_bcnt[8];
     __shared__ SsspSnap s_snap;
@@ -865,10 +897,10 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
     if (lane_id() == 0) s_fcnt[wid] = s_scnt[wid] = 0;
     if (lane_id() < RING) s_rcnt[wid][lane_id()] = 0;
     for (int j = lane_id(); j < SUB; j += 32) s_qcnt[wid][j] = 0;
-    if (lane_id() == 0) s_pcnt[wid] = 0;
+    if (lane_id() == 0) s_pcnt[wid] = s_dcnt[wid] = 0;
     __syncwarp();
     const Stage stage{WarpStage{s_fbuf[wid], &s_fcnt[wid], STAGE_F}, WarpStage{s_sbuf[wid], &s_scnt[wid], STAGE_S},
-                      s_rbuf[wid], s_rcnt[wid], s_qbuf[wid], s_qcnt[wid], s_bcnt, s_pv[wid], s_pw[wid],
+                      WarpStage{s_dbuf[wid], &s_dcnt[wid], STAGE_D}, s_rbuf[wid], s_rcnt[wid], s_qbuf[wid], s_qcnt[wid], s_bcnt, s_pv[wid], s_pw[wid],
                       &s_pcnt[wid]};
     unsigned epoch = 0;
     const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -905,6 +937,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
     Counts cnt{0, 0, 0, 0, 0, 0, 0ull};
     if (gtid == 0) c->t0 = globaltimer_ns();
     unsigned long long nbuckets = 0;
+    unsigned dgen = 0;  // settle passes so far: the expanded set's counter slot alternates with it
     for (;;) {
         // ---- open the bucket: its ring queue becomes the first frontier.
         if (threadIdx.x == 0) {
@@ -931,6 +964,13 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
         x.s_slot = sb;
         x.Sl = a.S[nbuckets & 1];
         x.SBl = a.SB[nbuckets & 1];
+        // The other heavy-set arrays are idle until this bucket's heavy phase
+        // (a pull borrows them there; the next bucket fills them).
+        x.Dl = a.S[(nbuckets + 1) & 1];
+        x.DBl = a.SB[(nbuckets + 1) & 1];
+        x.d_slot = (int)(dgen & 1);
+        x.d_tag = 0;
+        bool just_settled = false;  // the snapshot still shows the settled set's size
         {
             const int s_nxt = (phase + 1) % 3, s_clr = (phase + 2) % 3;
             if (gtid == 0) {
@@ -980,6 +1020,35 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
             int nj = -1;
             if (fsize == 0) {
                 if (!x.sub_mode) break;
+                const unsigned dn = sp->d_small[x.d_slot];
+                const unsigned long long dbp = sp->d_big[x.d_slot];
+                if (!just_settled && dn + big_count(dbp) > 0) {
+                    // Settle pass of sub-bucket sj: every distance in it is
+                    // final; its expanded set relaxes the deferred edges.
+                    // The other counter slot is cleared for the next set
+                    // (appends to it start after this phase's barrier).
+                    if (gtid == 0) {
+                        c->grab[s_clr] = c->cgrab[s_clr] = c->sn.f_small[s_clr] = 0;
+                        c->sn.f_big[s_clr] = c->sn.f_entries[s_clr] = 0;
+                        c->sn.d_small[x.d_slot ^ 1] = 0;
+                        c->sn.d_big[x.d_slot ^ 1] = 0;
+                    }
+                    x.pid = phase;
+                    x.f_slot = s_nxt;
+                    x.Fout = a.F[(phase + 1) & 1];
+                    x.FBout = a.FB[(phase + 1) & 1];
+                    expand_list(a, x, cnt, x.Dl, dn, dbp, x.DBl, &c->grab[s_cur], &c->cgrab[s_cur], false, sparse_out,
+                                SEL_LATER);
+                    stage_flush(a, x, cnt);
+                    if (!sssp_sync(a, epoch, sp)) return;
+                    if (gtid == 0) trace_phase(c, phase, 6, dn + big_count(dbp));
+                    ++phase;
+                    ++dgen;
+                    x.d_slot = (int)(dgen & 1);
+                    just_settled = true;
+                    continue;
+                }
+                just_settled = false;
                 for (int j = sj + 1; j < SUB; ++j)
                     if (sp->fq_len[j]) {
                         nj = j;
@@ -1000,6 +1069,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
                 // become the frontier (they are in the heavy set already).
                 sj = nj;
                 x.sub_hi = s_sub[sj + 1];
+                x.d_tag = fine_id(bucket, sj);
                 const unsigned len = sp->fq_len[sj];
                 const unsigned *Q = a.fq + (uint64_t)sj * a.n;
                 for (uint64_t base = gtid - lane_id(); base < len; base += nthreads) {
@@ -1049,7 +1119,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
                 continue;
             }
             expand_list(a, x, cnt, a.F[phase & 1], ns, bp, a.FB[phase & 1], &c->grab[s_cur], &c->cgrab[s_cur], false,
-                        sparse_out);
+                        sparse_out, x.sub_mode ? SEL_SAME : SEL_ALL);
             stage_flush(a, x, cnt);
             if (!sssp_sync(a, epoch, sp)) return;
             if (gtid == 0) trace_phase(c, phase, 1, ns + big_count(bp));
@@ -1291,7 +1361,7 @@ struct SsspWork {
     SsspCtl *ctl;
     SsspOut *out;
     unsigned long long *pack;
-    unsigned *fstamp, *sstamp, *qstamp, *settled, *cur;
+    unsigned *fstamp, *sstamp, *qstamp, *dstamp, *settled, *cur;
     unsigned *F[2], *FB[2], *S[2], *SB[2];
     unsigned *ring;
     unsigned *fq;
@@ -1307,6 +1377,7 @@ static SsspWork carve_sssp(void *base, uint64_t n) {
     w.fstamp = c.take<unsigned>(n);
     w.sstamp = c.take<unsigned>(n);
     w.qstamp = c.take<unsigned>(n);
+    w.dstamp = c.take<unsigned>(n);
     w.settled = c.take<unsigned>((n + 31) / 32);
     w.cur = c.take<unsigned>((n + 31) / 32);
     for (int i = 0; i < 2; ++i) {
@@ -1378,8 +1449,8 @@ extern "C" int g5_sssp_reset(uint64_t nverts, float *d_dist, int64_t *d_pred, vo
         G5_CUDA_TRY(cudaMemsetAsync(w.out, 0, sizeof(SsspOut), st));
     }
     G5_CUDA_TRY(cudaMemsetAsync(w.pack, 0xff, nverts * sizeof(unsigned long long), st));
-    // fstamp, sstamp, qstamp are consecutive carve-outs: one memset.
-    G5_CUDA_TRY(cudaMemsetAsync(w.fstamp, 0xff, (char *)(w.qstamp + nverts) - (char *)w.fstamp, st));
+    // fstamp, sstamp, qstamp, dstamp are consecutive carve-outs: one memset.
+    G5_CUDA_TRY(cudaMemsetAsync(w.fstamp, 0xff, (char *)(w.dstamp + nverts) - (char *)w.fstamp, st));
     // settled and cur are consecutive carve-outs: one memset.
     G5_CUDA_TRY(cudaMemsetAsync(w.settled, 0, (char *)(w.cur + (nverts + 31) / 32) - (char *)w.settled, st));
     // Fresh control block (counters, cursors, trace) for the next search.
@@ -1423,6 +1494,7 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     a.fstamp = w.fstamp;
     a.sstamp = w.sstamp;
     a.qstamp = w.qstamp;
+    a.dstamp = w.dstamp;
     a.settled = w.settled;
     a.cur = w.cur;
     for (int i = 0; i < 2; ++i) {
