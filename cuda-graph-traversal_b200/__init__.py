@@ -53,6 +53,7 @@ def _load() -> C.CDLL:
         "g5_csr_count_kronecker": ([p, u32, u64, p, p, u64, p, p], C.c_int),
         "g5_csr_fill_kronecker": ([p, u32, u64, p, f32, p, u64, p, p, p, p, p], C.c_int),
         "g5_csr_pack_append": ([p, p, p, p, u64, u64, u64, u64, p, p, p, p, p], C.c_int),
+        "g5_csr_split_tiny": ([p, p, p, p, p, u64, f32, p, p], C.c_int),
         "g5_bfs_traverse_multi": ([p, p, u64, p, u32, p, p, p, u64, p, p], C.c_int),
         "g5_sssp_traverse_multi": ([p, p, p, p, f32, u64, p, u32, p, p, p, u64, p, p], C.c_int),
         "g5_bfs_workspace_size": ([u64, p], C.c_int),
@@ -123,7 +124,7 @@ class MsBfsStats(C.Structure):
 
 class SsspParams(C.Structure):
     _fields_ = [("delta", C.c_float), ("blocks", C.c_int32), ("pull", C.c_float), ("sub_min", C.c_int32),
-                ("small", C.c_int32)]
+                ("small", C.c_int32), ("tiny_deg", C.c_void_p)]
 
 
 def _ptr(t: torch.Tensor | None) -> int | None:
@@ -232,6 +233,7 @@ class OnedGraph:
     column: torch.Tensor | None = None
     isolated: torch.Tensor | None = None  # int32[ceil(N/32)] bitmap of degree-0 vertices
     main_bits: np.ndarray | None = None   # host uint32 bitmap of the largest component
+    tiny_deg: torch.Tensor | None = None  # int32[N] leading tiny entries of each light part (g5_csr_split_tiny)
 
     def in_main_component(self, v: int) -> bool:
         """True when v is in the largest component (or unknown / out of
@@ -269,11 +271,21 @@ def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: 
     col64 = torch.empty(max(e, 1), dtype=torch.int64, device=dev) if with_column64 else None
     _check(lib.g5_csr_fill(_ptr(tg.edges), _ptr(tg.weights), m, n, _ptr(rowstarts), light_delta,
                            _ptr(work), work.numel(), _ptr(col), _ptr(w), _ptr(col64), _ptr(light), st))
+    tiny = _split_tiny(rowstarts, col, w, col64, light, n, light_delta, st)
     iso = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
     _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), n, _ptr(iso), st))
     g = OnedGraph(n, e, rowstarts, col[:e], w[:e], light, light_delta, None if col64 is None else col64[:e], iso)
+    g.tiny_deg = tiny
     g.main_bits = main_component_bitmap(g, stream)
     return g
+
+
+def _split_tiny(rowstarts, col, w, col64, light, n: int, light_delta: float, st) -> torch.Tensor:
+    """g5_csr_split_tiny: tiny-first light parts and their tiny counts."""
+    tiny = torch.empty(max(n, 1), dtype=torch.int32, device=rowstarts.device)
+    _check(lib.g5_csr_split_tiny(_ptr(rowstarts), _ptr(col), _ptr(w), _ptr(col64), _ptr(light), n, light_delta,
+                                 _ptr(tiny), st))
+    return tiny[:n]
 
 
 def oned_graph_from_kronecker(seed, log_n: int, nedges: int, device="cuda", light_delta: float = 0.1,
@@ -297,9 +309,11 @@ def oned_graph_from_kronecker(seed, log_n: int, nedges: int, device="cuda", ligh
     col64 = torch.empty(max(e, 1), dtype=torch.int64, device=device) if with_column64 else None
     _check(lib.g5_csr_fill_kronecker(s, log_n, nedges, _ptr(rowstarts), light_delta, _ptr(work), work.numel(),
                                      _ptr(col), _ptr(w), _ptr(col64), _ptr(light), st))
+    tiny = _split_tiny(rowstarts, col, w, col64, light, n, light_delta, st)
     iso = torch.empty((n + 31) // 32, dtype=torch.int32, device=device)
     _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), n, _ptr(iso), st))
     g = OnedGraph(n, e, rowstarts, col[:e], w[:e], light, light_delta, None if col64 is None else col64[:e], iso)
+    g.tiny_deg = tiny
     if with_main:
         g.main_bits = main_component_bitmap(g, stream)
     return g
@@ -386,6 +400,9 @@ def _pack(sizes, graphs, roots, device, light_delta, stream) -> PackedGraphs:
     iso = torch.empty((vb + 31) // 32, dtype=torch.int32, device=device)
     _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), vb, _ptr(iso), st))
     u = OnedGraph(vb, eb, rowstarts[:vb + 1], col[:eb], w[:eb], light[:vb], light_delta, None, iso)
+    # Packed rows keep their order; the split (a no-op on split rows) yields
+    # the packed graph's tiny counts.
+    u.tiny_deg = _split_tiny(u.rowstarts, u.col, u.w, None, u.light_deg, vb, light_delta, st)
     return PackedGraphs(nverts, vbase, u, list(roots))
 
 
@@ -403,7 +420,7 @@ def oned_graph_sssp_traverse_multi(g: OnedGraph, sssp: "SsspState", d_roots: tor
                                    blocks: int = 0, pull: float = 0.0, sub_min: int = 0, stream=None) -> None:
     """SSSP from every source in d_roots at once (g5_sssp_traverse_multi);
     reset sssp first."""
-    p = SsspParams(delta, blocks, pull, sub_min)
+    p = SsspParams(delta, blocks, pull, sub_min, 0, _ptr(g.tiny_deg))
     _check(lib.g5_sssp_traverse_multi(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
                                       g.nglobalverts, _ptr(d_roots), d_roots.numel(), _ptr(sssp.dist),
                                       _ptr(sssp.pred), _ptr(sssp.work), sssp.work.numel(), C.byref(p),
@@ -764,7 +781,8 @@ def _sssp_params(g: OnedGraph, root: int, delta, blocks, pull, sub_min, small) -
     # component (when the grid is left to the library).
     if small is None:
         small = blocks == 0 and not g.in_main_component(root)
-    return SsspParams(delta, 1 if small and blocks == 0 else blocks, pull, sub_min, int(bool(small)))
+    return SsspParams(delta, 1 if small and blocks == 0 else blocks, pull, sub_min, int(bool(small)),
+                      _ptr(g.tiny_deg))
 
 
 def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,

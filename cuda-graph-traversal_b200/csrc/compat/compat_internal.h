@@ -16,6 +16,7 @@ namespace g5compat {
 struct GraphExt {
     int32_t *col;        // int32 neighbour ids, light-first rows
     uint32_t *light_deg; // light entries per row
+    uint32_t *tiny_deg;  // leading tiny entries of each light part (g5_csr_split_tiny)
     uint32_t *isolated;  // bitmap of degree-0 vertices
     uint32_t *main_host; // host bitmap of the largest component (set by the first BFS state)
     float light_delta;

@@ -31,12 +31,17 @@ Oned_Graph oned_graph_from_tuple_graph(Worker_State *ws, Tuple_Graph *tg, u64 ng
     GraphExt x;
     x.col = (int32_t *)gpu_push(ws, g.nlocaledges * sizeof(int32_t), "int32 column");
     x.light_deg = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "light degrees");
+    x.tiny_deg = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "tiny degrees");
     x.light_delta = kLightDelta;
     x.main_host = nullptr;
     x.isolated = (uint32_t *)gpu_push(ws, (nglobalverts + 31) / 32 * sizeof(uint32_t), "isolated-vertex bitmap");
     check(ws,
           g5_csr_fill((const uint64_t *)tg->edges, tg->weights, tg->edges_size, nglobalverts, g.rowstarts,
                       kLightDelta, work, wbytes, x.col, g.weights, g.column, x.light_deg, 0),
+          "oned_graph_from_tuple_graph");
+    check(ws,
+          g5_csr_split_tiny(g.rowstarts, x.col, g.weights, g.column, x.light_deg, nglobalverts, kLightDelta,
+                            x.tiny_deg, 0),
           "oned_graph_from_tuple_graph");
     check(ws, g5_graph_isolated_bitmap(g.rowstarts, nglobalverts, x.isolated, 0), "oned_graph_from_tuple_graph");
     CHECK_CUDA(cudaDeviceSynchronize());
@@ -198,7 +203,7 @@ void oned_graph_sssp_run(Worker_State *ws, const Oned_Graph *g, Sssp_State *sssp
     // A root outside the largest component (host bitmap from the first BFS
     // state) runs on one block: its search touches a handful of vertices.
     const bool small = gx->main_host && !((gx->main_host[root >> 5] >> (root & 31)) & 1u);
-    g5_sssp_params p = {kLightDelta, small ? 1 : 0, 0.0f, 0, small ? 1 : 0};
+    g5_sssp_params p = {kLightDelta, small ? 1 : 0, 0.0f, 0, small ? 1 : 0, gx->tiny_deg};
     check(ws, g5_sssp_traverse(g->rowstarts, gx->col, g->weights, gx->light_deg, gx->light_delta, g->nglobalverts,
                                root, sssp->dist, sssp->pred, sx->work, sx->work_bytes, &p, 0),
           "oned_graph_sssp_run");

@@ -384,6 +384,119 @@ extern "C" int g5_csr_fill_kronecker(const uint32_t seed[5], uint32_t log_n, uin
     return G5_OK;
 }
 
+// Tiny-first order of each row's light part.  One warp per row.  Short
+// parts (at most 32 entries) are reordered in registers; longer ones are
+// counted (t tiny entries), then every non-tiny entry among the first t is
+// swapped with a tiny entry after them, the k-th with the k-th, both found
+// by warp-wide scans that queue up to 63 positions of each kind; each round
+// swaps up to 32 pairs (one per lane).  In place, the multiset of the row
+// unchanged.
+__global__ void __launch_bounds__(256) csr_split_tiny_kernel(const uint64_t *__restrict__ rowptr, int *col, float *w,
+                                                             uint64_t *col64, const unsigned *__restrict__ ld,
+                                                             uint64_t n, float tiny, unsigned *__restrict__ td) {
+    __shared__ unsigned s_q[8][2][64];  // per warp: queued head / tail positions (row offsets)
+    const unsigned lane = lane_id(), wib = threadIdx.x >> 5;
+    unsigned *hq = s_q[wib][0], *tq = s_q[wib][1];
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        const uint64_t rb = __ldg(&rowptr[v]);
+        const unsigned L = __ldg(&ld[v]);
+        if (L <= 32) {
+            const bool has = lane < L;
+            const float wt = has ? w[rb + lane] : 0.0f;
+            const int c = has ? col[rb + lane] : 0;
+            const uint64_t c64 = has && col64 ? col64[rb + lane] : 0;
+            const bool t = has && wt < tiny;
+            const unsigned tm = __ballot_sync(FULL, t), om = __ballot_sync(FULL, has && !t);
+            const unsigned nt = __popc(tm);
+            __syncwarp();
+            if (has) {
+                const unsigned to = t ? __popc(tm & lanemask_lt()) : nt + __popc(om & lanemask_lt());
+                w[rb + to] = wt;
+                col[rb + to] = c;
+                if (col64) col64[rb + to] = c64;
+            }
+            if (lane == 0) td[v] = nt;
+            continue;
+        }
+        unsigned t = 0;
+        for (unsigned i = lane; i < L; i += 32) t += w[rb + i] < tiny;
+        t = warp_sum(t);
+        unsigned h = 0, tc = t, nh = 0, nt = 0;
+        for (;;) {
+            // Refill both queues to at least 32 entries (or to the end of their range).
+            while (nh < 32 && h < t) {
+                const unsigned i = h + lane;
+                const bool m = i < t && !(w[rb + i] < tiny);
+                const unsigned bm = __ballot_sync(FULL, m);
+                if (m) hq[nh + __popc(bm & lanemask_lt())] = i;
+                nh += __popc(bm);
+                h += 32;
+                __syncwarp();
+            }
+            while (nt < 32 && tc < L) {
+                const unsigned i = tc + lane;
+                const bool m = i < L && w[rb + i] < tiny;
+                const unsigned bm = __ballot_sync(FULL, m);
+                if (m) tq[nt + __popc(bm & lanemask_lt())] = i;
+                nt += __popc(bm);
+                tc += 32;
+                __syncwarp();
+            }
+            const unsigned k = min(min(nh, nt), 32u);  // one pair per lane
+            if (k == 0) break;  // equal counts of misplaced entries: both queues run dry together
+            if (lane < k) {
+                const uint64_t a = rb + hq[lane], b = rb + tq[lane];
+                const float wa = w[a], wb = w[b];
+                const int ca = col[a], cb = col[b];
+                w[a] = wb;
+                w[b] = wa;
+                col[a] = cb;
+                col[b] = ca;
+                if (col64) {
+                    const uint64_t xa = col64[a], xb = col64[b];
+                    col64[a] = xb;
+                    col64[b] = xa;
+                }
+            }
+            __syncwarp();
+            // Drop the k swapped positions from the front of each queue (up
+            // to 63 entries stay: two per lane).
+            const unsigned hr = nh - k, tr = nt - k;
+            const unsigned h0 = lane < hr ? hq[k + lane] : 0u, h1 = lane + 32 < hr ? hq[k + lane + 32] : 0u;
+            const unsigned t0 = lane < tr ? tq[k + lane] : 0u, t1 = lane + 32 < tr ? tq[k + lane + 32] : 0u;
+            __syncwarp();
+            if (lane < hr) hq[lane] = h0;
+            if (lane + 32 < hr) hq[lane + 32] = h1;
+            if (lane < tr) tq[lane] = t0;
+            if (lane + 32 < tr) tq[lane + 32] = t1;
+            nh = hr;
+            nt = tr;
+            __syncwarp();
+        }
+        if (lane == 0) td[v] = t;
+    }
+}
+
+extern "C" int g5_csr_split_tiny(const uint64_t *d_rowstarts, int32_t *d_col, float *d_w, uint64_t *d_col64,
+                                 const uint32_t *d_light_deg, uint64_t nverts, float light_delta, uint32_t *d_tiny_deg,
+                                 void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_csr_split_tiny: nverts outside [1, 2^31]");
+    G5_CHECK_ARG(d_rowstarts && d_col && d_w && d_light_deg && d_tiny_deg, "g5_csr_split_tiny: NULL argument");
+    G5_CHECK_ARG(light_delta > 0.0f, "g5_csr_split_tiny: light_delta must be positive");
+    DeviceInfo di;
+    int rc = device_info(&di);
+    if (rc) return rc;
+    const float tiny = light_delta / (float)G5_TINY_DIV;
+    const uint64_t want = (nverts + 7) / 8;  // blocks of 8 warps, one row each
+    const unsigned blocks = (unsigned)std::min<uint64_t>(want, (uint64_t)di.sms * 8);
+    csr_split_tiny_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(d_rowstarts, d_col, d_w, d_col64, d_light_deg,
+                                                                    nverts, tiny, d_tiny_deg);
+    G5_CUDA_TRY(cudaGetLastError());
+    return G5_OK;
+}
+
 extern "C" int g5_csr_pack_append(const uint64_t *d_src_rowstarts, const int32_t *d_src_col, const float *d_src_w,
                                   const uint32_t *d_src_light_deg, uint64_t src_nverts, uint64_t src_nentries,
                                   uint64_t vbase, uint64_t ebase, uint64_t *d_dst_rowstarts, int32_t *d_dst_col,

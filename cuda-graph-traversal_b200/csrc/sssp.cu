@@ -138,6 +138,8 @@ struct SsspArgs {
     const int *col;
     const float *w;
     const unsigned *ld;  // light degree per vertex (partitioned rows) or nullptr
+    const unsigned *td;  // tiny-first light parts: tiny entries per vertex (w < tiny), or nullptr
+    float tiny;          // light / G5_TINY_DIV
     uint64_t n;
     unsigned root;
     const uint64_t *roots;  // several sources at once (device array) instead of `root`, or nullptr
@@ -227,6 +229,7 @@ struct PushCtx {
     const float *sub;    // shared: sub-bucket bounds t_0 = b_B .. t_SUB = b_{B+1}
     float sub_hi;        // upper bound of the light frontier's range (t_{j+1}, or b_{B+1})
     bool sub_mode;       // the bucket is processed by sub-buckets
+    bool tiny_rows;      // sub-bucket expansions read only the rows' tiny prefixes
     unsigned *Dl, *DBl;  // expanded set of the open sub-bucket (borrows the idle heavy-set arrays)
     int d_slot;          // its counter slot
     unsigned d_tag;      // its stamp: fine_id(bucket, sub-bucket)
@@ -257,13 +260,16 @@ __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCt
     // In sub mode a vertex entering the frontier joins the sub-bucket's
     // expanded set (once per sub-bucket).
     const bool d = f && x.sub_mode && atomicExch(&a.dstamp[v], x.d_tag) != x.d_tag;
-    uint64_t lb = 0, le = 0, hb = 0, he = 0;
+    uint64_t lb = 0, le = 0, hb = 0, he = 0, dl = 0;
     if (f || s) {
         const uint64_t b = __ldg(&a.rowptr[v]), e = __ldg(&a.rowptr[v + 1]);
         const uint64_t mid = a.ld ? b + __ldg(&a.ld[v]) : e;
         if (f) {
+            // A sub-bucket's frontier rows are their tiny prefixes (the
+            // expansion's row range, which sets the big part's chunks).
             lb = b;
-            le = mid;
+            le = x.sub_mode && x.tiny_rows ? b + __ldg(&a.td[v]) : mid;
+            dl = mid - b;
         }
         if (s) {
             hb = a.ld ? mid : b;
@@ -284,7 +290,7 @@ __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCt
     // Once per vertex and sub-bucket, so the set stays within n entries.
     if (x.sub_mode)
         ok &= frontier_append_staged(x.st.d, x.Dl, x.DBl, a.n, &c->sn.d_small[x.d_slot], &c->sn.d_big[x.d_slot], d, v,
-                                     le - lb, SSSP_BIG_DEG);
+                                     dl, SSSP_BIG_DEG);
     if (!ok) atomicOr(&c->error, DEVERR_CAPACITY);
 }
 
@@ -577,6 +583,7 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
         float du = 0.0f;
         if (valid) {
             part_range(a, u, heavy, rb, re);
+            if (sel == SEL_SAME && x.tiny_rows) re = rb + __ldg(&a.td[u]);
             const unsigned long long pu = __ldcg(&a.pack[u]);
             du = pack_dist(pu);
             if (heavy) settle(a, sparse_out, u, pu);
@@ -631,6 +638,7 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
         const unsigned cfirst = __ldcg(&B[j]);
         uint64_t rb, re;
         part_range(a, u, heavy, rb, re);
+        if (sel == SEL_SAME && x.tiny_rows) re = rb + __ldg(&a.td[u]);
         const unsigned long long pu = __ldcg(&a.pack[u]);
         const float du = pack_dist(pu);
         if (heavy && ch == cfirst && lane == 0) settle(a, sparse_out, u, pu);
@@ -881,6 +889,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
     SsspCtl *c = a.ctl;
     __shared__ float s_bnd[RING + 1];
     __shared__ float s_sub[SUB + 1];
+    __shared__ bool s_tiny_ok;
     constexpr int WARPS = SSSP_THREADS / 32;
     __shared__ unsigned s_fbuf[WARPS][STAGE_F], s_sbuf[WARPS][STAGE_S], s_rbuf[WARPS][RING * STAGE_R];
     __shared__ unsigned s_fcnt[WARPS], s_scnt[WARPS], s_rcnt[WARPS][RING];
@@ -950,6 +959,12 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
             const float wf = a.delta / (float)SUB;
             for (int j = 0; j < SUB; ++j) s_sub[j] = __fadd_rn(blo, (float)j * wf);
             s_sub[SUB] = s_bnd[1];
+            // Tiny prefixes hold every same-sub-bucket relaxation when an
+            // entry of weight >= tiny from anywhere in sub-bucket j reaches
+            // t_{j+1} or beyond (fl(d + w) is monotone in d and w).
+            bool ok = a.td != nullptr;
+            for (int j = 0; j < SUB && ok; ++j) ok = __fadd_rn(s_sub[j], a.tiny) >= s_sub[j + 1];
+            s_tiny_ok = ok;
         }
         __syncthreads();
         PushCtx x;
@@ -959,6 +974,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
         x.sub = s_sub;
         x.sub_hi = s_bnd[1];
         x.sub_mode = false;
+        x.tiny_rows = s_tiny_ok;
         int sj = -1;  // current sub-bucket in sub mode
         const int sb = (int)(nbuckets % 3);
         x.s_slot = sb;
@@ -1465,7 +1481,7 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     SsspWork w;
     int rc = sssp_check(d_rowstarts, d_col, d_w, nverts, root, d_dist, d_pred, d_work, work_bytes, &w, who);
     if (rc) return rc;
-    g5_sssp_params p = {0.1f, 0, 0.0f, 0, 0};
+    g5_sssp_params p = {0.1f, 0, 0.0f, 0, 0, nullptr};
     if (params) p = *params;
     G5_CHECK_ARG(p.delta > 0.0f, "g5_sssp_traverse: delta must be positive");
     int max_blocks = 0;
@@ -1483,6 +1499,8 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     const bool split = d_light_deg && p.delta <= light_delta;
     a.ld = split ? d_light_deg : nullptr;
     a.light = split ? light_delta : p.delta;
+    a.td = split ? p.tiny_deg : nullptr;
+    a.tiny = light_delta / (float)G5_TINY_DIV;
     a.n = nverts;
     a.root = (unsigned)root;
     a.roots = d_roots;

@@ -97,6 +97,19 @@ int g5_csr_fill_kronecker(const uint32_t seed[5], uint32_t log_n, uint64_t nedge
                           float light_delta, void *d_work, uint64_t work_bytes, int32_t *d_col, float *d_w,
                           uint64_t *d_col64, uint32_t *d_light_deg, void *stream);
 
+/* Light entries below light_delta / G5_TINY_DIV ("tiny") are the only ones
+ * whose relaxation can stay inside an SSSP sub-bucket (width delta / 32 <=
+ * light_delta / 32).  g5_csr_split_tiny reorders each row's light part
+ * [rowstart, rowstart + light_deg) in place so that its tiny entries come
+ * first (d_col, d_w and, when given, d_col64 move together; the multiset of
+ * each row is unchanged) and writes their count per vertex to d_tiny_deg.
+ * Idempotent; needs the light counts of g5_csr_fill.  No counterpart in the
+ * reference (its rows are not split at all). */
+#define G5_TINY_DIV 30
+int g5_csr_split_tiny(const uint64_t *d_rowstarts, int32_t *d_col, float *d_w, uint64_t *d_col64,
+                      const uint32_t *d_light_deg, uint64_t nverts, float light_delta, uint32_t *d_tiny_deg,
+                      void *stream);
+
 /* Packs disjoint graphs into one CSR (no counterpart in the reference, which
  * holds one graph): copies one graph's CSR into the destination at vertex
  * offset vbase and entry offset ebase, shifting its column by vbase.  Call
@@ -234,6 +247,11 @@ typedef struct g5_sssp_params {
     int32_t small;   /* 1: the source's component is small (outside the main
                        component): one lean block, label-correcting rounds,
                        same distances and parents; 0 = the bucketed search  */
+    const uint32_t *tiny_deg; /* per-vertex count of the leading light entries
+                       below light_delta / G5_TINY_DIV, rows split by
+                       g5_csr_split_tiny (optional, nullptr = not split).  A
+                       sub-bucket then reads only that prefix of a row while
+                       its distances are still dropping                      */
 } g5_sssp_params;
 
 int g5_sssp_workspace_size(uint64_t nverts, uint64_t *bytes);

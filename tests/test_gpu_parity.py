@@ -87,6 +87,29 @@ def test_csr_light_partition(graphs):
     assert np.array_equal(pos < ld[src], w < np.float32(0.1))
 
 
+def test_csr_tiny_split(cgt, graphs):
+    """g5_csr_split_tiny: every row's light part starts with its entries
+    below light_delta / 30 (tiny_deg of them), the other light entries after
+    them; the rows' multisets stay those of the fill (the canonical-row hash
+    test covers them) and a second split changes nothing."""
+    for scale in (12, 16):
+        g = graphs[scale]["g"]
+        rs = _np(g.rowstarts)
+        w = _np(g.w)
+        ld = _np(g.light_deg).astype(np.int64)
+        td = _np(g.tiny_deg).astype(np.int64)
+        src = np.repeat(np.arange(g.nglobalverts), np.diff(rs))
+        pos = np.arange(rs[-1]) - rs[src]
+        tiny = np.float32(g.light_delta) / np.float32(30)
+        assert np.array_equal(pos < td[src], (pos < ld[src]) & (w < tiny))
+        assert td.sum() > 0 and np.all(td <= ld)
+        assert np.array_equal(_np(g.column), _np(g.col).astype(np.int64))
+        col, ww = _np(g.col).copy(), w.copy()
+        td2 = cgt._split_tiny(g.rowstarts, g.col, g.w, g.column, g.light_deg, g.nglobalverts, g.light_delta, None)
+        assert np.array_equal(_np(td2), td)
+        assert np.array_equal(_np(g.col), col) and np.array_equal(_np(g.w), ww)
+
+
 def test_csr_edge_cases(cgt):
     dev = "cuda"
     # only self loops -> no entries, every vertex isolated
