@@ -43,7 +43,7 @@ __device__ __forceinline__ unsigned long long big_chunks(unsigned long long pack
 // once-per-list invariants rule out.
 __device__ __forceinline__ bool frontier_append(unsigned *L, unsigned *base, uint64_t n, unsigned *n_small,
                                                 unsigned long long *big, bool want, unsigned v, uint64_t deg,
-                                                unsigned big_deg = BIG_DEG) {
+                                                unsigned big_deg = BIG_DEG, unsigned chunk = BIG_CHUNK) {
     const bool sm = want && deg <= big_deg;
     const bool bg = want && deg > big_deg;
     bool ok = true;
@@ -54,7 +54,7 @@ __device__ __forceinline__ bool frontier_append(unsigned *L, unsigned *base, uin
     }
     const unsigned bmask = __ballot_sync(FULL, bg);
     if (bmask) {
-        const unsigned nch = bg ? (unsigned)((deg + BIG_CHUNK - 1) / BIG_CHUNK) : 0u;
+        const unsigned nch = bg ? (unsigned)((deg + chunk - 1) / chunk) : 0u;
         const unsigned incl = warp_incl_scan(nch);
         const unsigned total = __shfl_sync(FULL, incl, 31);
         const unsigned leader = __ffs(bmask) - 1;
@@ -123,9 +123,10 @@ __device__ __forceinline__ bool stage_append(const WarpStage &q, bool want, unsi
 // frontier_append with the small part staged per warp.  All lanes call it.
 __device__ __forceinline__ bool frontier_append_staged(const WarpStage &q, unsigned *L, unsigned *basearr, uint64_t n,
                                                        unsigned *n_small, unsigned long long *big, bool want,
-                                                       unsigned v, uint64_t deg, unsigned big_deg = BIG_DEG) {
+                                                       unsigned v, uint64_t deg, unsigned big_deg = BIG_DEG,
+                                                       unsigned chunk = BIG_CHUNK) {
     bool ok = stage_append(q, want && deg <= big_deg, v, L, n, n_small);
-    ok &= frontier_append(L, basearr, n, n_small, big, want && deg > big_deg, v, deg, big_deg);
+    ok &= frontier_append(L, basearr, n, n_small, big, want && deg > big_deg, v, deg, big_deg, chunk);
     return ok;
 }
 

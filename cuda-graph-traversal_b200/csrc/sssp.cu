@@ -52,10 +52,14 @@ static_assert(STAGE_F >= 32 && STAGE_S >= 32, "staging slices hold one warp step
 static_assert(STAGE_R <= 32 && STAGE_Q <= 32, "stage_push writes a full slice with one lane per entry");
 constexpr int SSSP_TRACE = 256;      // phases recorded in the control block
 // List entries with more edges to expand than this go to the big part (cut
-// into BIG_CHUNK chunks across the grid), and a warp grabs at most SSSP_GRAB
+// into SSSP_CHUNK chunks across the grid), and a warp grabs at most SSSP_GRAB
 // small entries at once: a grab holds at most SSSP_GRAB x SSSP_BIG_DEG edges,
 // so no warp is left with a long tail of relaxations at the end of a phase.
 constexpr unsigned SSSP_BIG_DEG = 128;
+// Chunk of a long row taken by one warp in the frontier, heavy-set and
+// expanded-set lists.  A warp's relaxation steps form a chain of dependent
+// round trips, so the chunk bounds the longest warp of a phase.
+constexpr unsigned SSSP_CHUNK = 256;
 constexpr unsigned SSSP_GRAB = 32;
 // Sub-buckets: once a bucket's light frontier holds SPLIT_MIN light entries,
 // the rest of the bucket is processed in SUB equal sub-buckets in order
@@ -284,13 +288,13 @@ __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCt
     // Each vertex enters a frontier once per phase and a heavy set once per
     // bucket, so no list exceeds n entries.
     bool ok = frontier_append_staged(x.st.f, x.Fout, x.FBout, a.n, &c->sn.f_small[x.f_slot], &c->sn.f_big[x.f_slot], f, v,
-                                     le - lb, SSSP_BIG_DEG);
+                                     le - lb, SSSP_BIG_DEG, SSSP_CHUNK);
     ok &= frontier_append_staged(x.st.s, x.Sl, x.SBl, a.n, &c->sn.s_small[x.s_slot], &c->sn.s_big[x.s_slot], s, v, he - hb,
-                                 SSSP_BIG_DEG);
+                                 SSSP_BIG_DEG, SSSP_CHUNK);
     // Once per vertex and sub-bucket, so the set stays within n entries.
     if (x.sub_mode)
         ok &= frontier_append_staged(x.st.d, x.Dl, x.DBl, a.n, &c->sn.d_small[x.d_slot], &c->sn.d_big[x.d_slot], d, v,
-                                     dl, SSSP_BIG_DEG);
+                                     dl, SSSP_BIG_DEG, SSSP_CHUNK);
     if (!ok) atomicOr(&c->error, DEVERR_CAPACITY);
 }
 
@@ -643,9 +647,9 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
         const float du = pack_dist(pu);
         if (heavy && ch == cfirst && lane == 0) settle(a, sparse_out, u, pu);
         const uint64_t deg = re - rb;
-        const uint64_t cs = (uint64_t)(ch - cfirst) * BIG_CHUNK;
-        const uint64_t ce = min(cs + BIG_CHUNK, deg);
-        for (uint64_t e0 = cs + lane; e0 < cs + BIG_CHUNK; e0 += 32 * SSSP_EDGES) {
+        const uint64_t cs = (uint64_t)(ch - cfirst) * SSSP_CHUNK;
+        const uint64_t ce = min(cs + SSSP_CHUNK, deg);
+        for (uint64_t e0 = cs + lane; e0 < cs + SSSP_CHUNK; e0 += 32 * SSSP_EDGES) {
             EdgeProbe p;
 #pragma unroll
             for (int t = 0; t < SSSP_EDGES; ++t) {
