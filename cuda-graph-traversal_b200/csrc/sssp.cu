@@ -1261,8 +1261,15 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
     __shared__ unsigned s_len[2];
     __shared__ unsigned s_nreach;
     __shared__ unsigned s_err;
+    __shared__ bool s_sparse;
     const unsigned lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     unsigned *R = a.S[0];  // every vertex reached, once (sstamp); entries from SMALL_L on
+    if (threadIdx.x == 32) {
+        // Whether the outputs were pre-filled: loaded by another warp while
+        // the search runs, read after it.
+        s_sparse = __ldcg((const unsigned long long *)&a.prefilled->dist) == (unsigned long long)a.dist &&
+                   __ldcg((const unsigned long long *)&a.prefilled->pred) == (unsigned long long)a.pred;
+    }
     if (threadIdx.x == 0) {
         c->t0 = globaltimer_ns();
         a.pack[a.root] = (unsigned long long)a.root;  // distance 0.0f, parent = root
@@ -1342,9 +1349,7 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
         __syncthreads();
     }
     // Outputs: the reached vertices (pre-filled outputs) or every vertex.
-    const bool sparse_out = __ldcg((const unsigned long long *)&a.prefilled->dist) == (unsigned long long)a.dist &&
-                            __ldcg((const unsigned long long *)&a.prefilled->pred) == (unsigned long long)a.pred;
-    if (sparse_out) {
+    if (s_sparse) {
         const unsigned nr = min(s_nreach, (unsigned)a.n);
         for (unsigned i = threadIdx.x; i < nr; i += blockDim.x) {
             const unsigned v = i < SMALL_L ? s_r[i] : __ldcg(&R[i]);
