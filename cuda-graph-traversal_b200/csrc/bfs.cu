@@ -12,8 +12,9 @@
 // walks the combined edge list 32 edges per step (each lane finds its
 // source by a 5-step shuffle search), so low-degree vertices do not leave
 // lanes idle.  Vertices above BIG_DEG sit at the back of the queue and every
-// warp of the grid takes BIG_CHUNK-edge chunks of them from one counter
-// (g5_frontier.cuh).  A neighbour is claimed with an atomicOr on the visited bitmap;
+// warp of the grid takes BFS_CHUNK-edge chunks of them from one counter
+// (g5_frontier.cuh); a chunk is a chain of BFS_CHUNK / 32 dependent steps of
+// one warp, so it bounds the longest warp of a level.  A neighbour is claimed with an atomicOr on the visited bitmap;
 // the winner writes pred/depth and appends it to the next queue with one
 // atomic per warp.
 //
@@ -39,6 +40,7 @@
 namespace g5 {
 
 constexpr int BFS_THREADS = 256;
+constexpr unsigned BFS_CHUNK = 256;  // edges of a long row taken by one warp
 constexpr unsigned BFS_STAGE = 512;  // per-warp staging of the next queue (16 KiB shared per block)
 constexpr unsigned long long SOLO_EDGES = 4096;  // levels at most this wide run in block 0 alone
 constexpr int BFS_TRACE = 64;                    // levels recorded in the control block
@@ -132,7 +134,7 @@ __device__ __forceinline__ void td_visit(const BfsArgs &a, const WarpStage &bq, 
         deg = __ldg(&a.rowptr[v + 1]) - __ldg(&a.rowptr[v]);
         my_m += deg;
     }
-    if (!frontier_append_staged(bq, qn, basen, a.n, n_small, n_big, disc, v, deg))
+    if (!frontier_append_staged(bq, qn, basen, a.n, n_small, n_big, disc, v, deg, BIG_DEG, BFS_CHUNK))
         atomicOr(&a.ctl->res.error_flags, DEVERR_CAPACITY);
 }
 
@@ -185,9 +187,9 @@ __device__ void td_expand(const BfsArgs &a, const WarpStage &bq, int level, int 
         const unsigned u = __ldcg(&Q[a.n - 1 - j]);
         const uint64_t rb = __ldg(&a.rowptr[u]);
         const uint64_t deg = __ldg(&a.rowptr[u + 1]) - rb;
-        const uint64_t cs = (uint64_t)(ch - __ldcg(&B[j])) * BIG_CHUNK;
-        const uint64_t ce = min(cs + BIG_CHUNK, deg);
-        for (uint64_t e = cs + lane; e < cs + BIG_CHUNK; e += 32) {
+        const uint64_t cs = (uint64_t)(ch - __ldcg(&B[j])) * BFS_CHUNK;
+        const uint64_t ce = min(cs + BFS_CHUNK, deg);
+        for (uint64_t e = cs + lane; e < cs + BFS_CHUNK; e += 32) {
             const bool has = e < ce;
             const unsigned v = has ? (unsigned)__ldg(&a.col[rb + e]) : 0u;
             td_visit(a, bq, has, v, u, level + 1, QN, BN, &c->n_small[s_nxt], &c->big[s_nxt], my_m);
@@ -366,7 +368,7 @@ __device__ void bits_to_queue(const BfsArgs &a, const WarpStage &bq, const unsig
                 m &= m - 1;
                 deg = __ldg(&a.rowptr[v + 1]) - __ldg(&a.rowptr[v]);
             }
-            if (!frontier_append_staged(bq, qn, basen, a.n, n_small, n_big, has, v, deg))
+            if (!frontier_append_staged(bq, qn, basen, a.n, n_small, n_big, has, v, deg, BIG_DEG, BFS_CHUNK))
                 atomicOr(&a.ctl->res.error_flags, DEVERR_CAPACITY);
         }
     }
@@ -522,7 +524,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
                 if (root_deg > BIG_DEG) {
                     a.q[0][a.n - 1] = root;
                     a.base[0][0] = 0;
-                    c->big[0] = (1ull << BIG_SHIFT) | ((root_deg + BIG_CHUNK - 1) / BIG_CHUNK);
+                    c->big[0] = (1ull << BIG_SHIFT) | ((root_deg + BFS_CHUNK - 1) / BFS_CHUNK);
                 } else {
                     a.q[0][0] = root;
                     c->n_small[0] = 1;
@@ -558,7 +560,8 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
                         ++my_n;
                     }
                 }
-                if (!frontier_append_staged(bq, a.q[0], a.base[0], a.n, &c->n_small[0], &c->big[0], mine, r, deg))
+                if (!frontier_append_staged(bq, a.q[0], a.base[0], a.n, &c->n_small[0], &c->big[0], mine, r, deg,
+                                            BIG_DEG, BFS_CHUNK))
                     atomicOr(&c->res.error_flags, DEVERR_CAPACITY);
             }
             if (!stage_flush_warp(bq, a.q[0], a.n, &c->n_small[0])) atomicOr(&c->res.error_flags, DEVERR_CAPACITY);
