@@ -40,3 +40,24 @@ def test_poisson_trace_and_summary(cgt):
            for q in tr]
     s = S.latency_summary(res)
     assert s["queries"] == 2000 and abs(s["p50_ms"] - 5.5) < 1.0 and s["p99_ms"] >= 9.9
+
+
+def test_query_host_pointer_cache_and_sssp_params(cgt):
+    """The query path looks up the host address of the main-component bitmap
+    once per array (a new array gets a new address), and SSSP parameters carry
+    the graph's tiny counts only when the graph has them."""
+    n = 64
+    rs = torch.arange(n + 1, dtype=torch.int64)
+    g = cgt.OnedGraph(n, n, rs, torch.zeros(n, dtype=torch.int32), torch.zeros(n), torch.zeros(n, dtype=torch.int32),
+                      0.1)
+    assert cgt._main_bits_ptr(g) is None
+    g.main_bits = np.full(2, 0xFFFFFFFF, np.uint32)
+    a = cgt._main_bits_ptr(g)
+    assert a == g.main_bits.ctypes.data and cgt._main_bits_ptr(g) == a
+    g.main_bits = np.zeros(2, np.uint32)
+    assert cgt._main_bits_ptr(g) == g.main_bits.ctypes.data
+    p = cgt._sssp_params(g, 0, 0.1, 0, 0.0, 0, None)
+    assert p.tiny_deg is None and p.small == 1 and p.blocks == 1  # root 0 outside the (empty) main component
+    g.tiny_deg = torch.zeros(n, dtype=torch.int32)
+    p = cgt._sssp_params(g, 0, 0.1, 0, 0.0, 0, False)
+    assert p.tiny_deg == g.tiny_deg.data_ptr() and p.small == 0 and p.blocks == 0
