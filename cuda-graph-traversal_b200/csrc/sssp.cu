@@ -1314,6 +1314,11 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
                 uint64_t vb, ve;
                 const unsigned long long old = relax_with_row(a.rowptr, a.pack, v, np, vb, ve);
                 if (!(np < old && (old >> 32) != (np >> 32))) continue;  // distance unchanged
+                // The next round reads v's row: start bringing it into L2 now.
+                if (vb < ve) {
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(a.col + vb));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(a.w + vb));
+                }
                 const unsigned fold = atomicExch(&a.fstamp[v], round);
                 const unsigned sold = atomicExch(&a.sstamp[v], 0u);
                 if (fold != round) {
