@@ -255,15 +255,29 @@ __device__ __forceinline__ int sub_index(const float *t, float d) {
 }
 
 // Appends v to the produced frontier and to the bucket's heavy set (each at
-// most once).  All 32 lanes call it.
+// most once).  All 32 lanes call it.  `unique`: the caller's vertices are
+// distinct and none of them was pushed in this bucket (or sub-bucket) yet --
+// the entries of a bucket's ring queue or a sub-bucket's queue, which hold a
+// vertex at most once and are read by the first phase of their window --
+// so the stamps are set with plain stores instead of being exchanged.
 __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCtx &x, Counts &k, bool want_f,
-                                                 bool want_s, unsigned v) {
+                                                 bool want_s, unsigned v, bool unique = false) {
     SsspCtl *c = a.ctl;
-    bool f = want_f && atomicExch(&a.fstamp[v], x.pid) != x.pid;
-    bool s = want_s && atomicExch(&a.sstamp[v], x.bucket) != x.bucket;
-    // In sub mode a vertex entering the frontier joins the sub-bucket's
-    // expanded set (once per sub-bucket).
-    const bool d = f && x.sub_mode && atomicExch(&a.dstamp[v], x.d_tag) != x.d_tag;
+    bool f, s, d;
+    if (unique) {
+        f = want_f;
+        s = want_s;
+        d = f && x.sub_mode;
+        if (f) a.fstamp[v] = x.pid;
+        if (s) a.sstamp[v] = x.bucket;
+        if (d) a.dstamp[v] = x.d_tag;
+    } else {
+        f = want_f && atomicExch(&a.fstamp[v], x.pid) != x.pid;
+        s = want_s && atomicExch(&a.sstamp[v], x.bucket) != x.bucket;
+        // In sub mode a vertex entering the frontier joins the sub-bucket's
+        // expanded set (once per sub-bucket).
+        d = f && x.sub_mode && atomicExch(&a.dstamp[v], x.d_tag) != x.d_tag;
+    }
     uint64_t lb = 0, le = 0, hb = 0, he = 0, dl = 0;
     if (f || s) {
         const uint64_t b = __ldg(&a.rowptr[v]), e = __ldg(&a.rowptr[v + 1]);
@@ -1017,7 +1031,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
                     const float d = pack_dist(__ldcg(&a.pack[v]));
                     ok = d >= s_bnd[0] && d < s_bnd[1] && !((__ldcg(&a.settled[v >> 5]) >> (v & 31)) & 1u);
                 }
-                push_same_bucket(a, x, cnt, ok, ok, v);
+                push_same_bucket(a, x, cnt, ok, ok, v, true);
             }
             stage_flush(a, x, cnt);
             if (!sssp_sync(a, epoch, sp)) return;
@@ -1101,7 +1115,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
                         const float d = pack_dist(__ldcg(&a.pack[v]));
                         ok = d >= s_sub[sj] && d < s_sub[sj + 1];
                     }
-                    push_same_bucket(a, x, cnt, ok, false, v);
+                    push_same_bucket(a, x, cnt, ok, false, v, true);
                 }
                 stage_flush(a, x, cnt);
                 if (!sssp_sync(a, epoch, sp)) return;
