@@ -563,7 +563,8 @@ def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0):
     build_s = time.time() - t0
     trace = S.poisson_trace(graphs, nqueries, rate, bfs_share=0.7, seed=1)
     warm = S.poisson_trace(graphs, 64, rate, bfs_share=0.5, seed=99)
-    srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots)
+    # A launch that reports a device error is counted in the line, not fatal.
+    srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots, raise_errors=False)
     srv.prewarm()  # workspaces created up front (admission by free HBM)
     srv.run_trace(warm, deadline=600)  # batched copies prepared, kernels loaded
     srv.stats = S.ServerStats()
@@ -575,10 +576,12 @@ def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0):
     low = None
     if low_rate:
         ltrace = S.poisson_trace(graphs, nqueries, low_rate, bfs_share=0.7, seed=2)
-        srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots)
+        srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots, raise_errors=False)
         srv.prewarm()
         srv.run_trace(warm, deadline=600)
-        low = {"rate_qps": low_rate, "ours": S.latency_summary(srv.run_trace(ltrace, deadline=3600))}
+        srv.stats = S.ServerStats()
+        low = {"rate_qps": low_rate, "ours": S.latency_summary(srv.run_trace(ltrace, deadline=3600)),
+               "device_errors": srv.stats.device_errors, "errors": srv.stats.errors}
         del srv
         torch.cuda.empty_cache()
     S.serve_plain(graphs, warm)
@@ -593,6 +596,7 @@ def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0):
             "plain_one_at_a_time": plain, "qps_vs_plain": round(ours["qps"] / plain["qps"], 2),
             "bfs_batches": st.bfs_batches, "bfs_queries_batched": st.bfs_batched_queries,
             "sssp_launches": st.sssp_launches, "max_concurrent_launches": st.max_inflight,
+            "device_errors": st.device_errors, "errors": st.errors,
             "slots": slots, "low_load": low, "build_s": round(build_s, 2),
             "timing": "host clock: latency from a query's arrival time to the host seeing its launch's "
                       "CUDA event complete; BFS results exported as depth arrays"}

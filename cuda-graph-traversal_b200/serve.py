@@ -44,7 +44,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from . import (MSBFS_MAX_ROOTS, BfsParams, BfsState, MsBfsParams, MsBfsState, OnedGraph, SsspState,
+from . import (MSBFS_MAX_ROOTS, BfsParams, BfsState, G5Error, MsBfsParams, MsBfsState, OnedGraph, SsspState,
                bfs_stats, bfs_workspace_bytes, msbfs_depths_u8, msbfs_run, msbfs_stats, oned_graph_bfs_reset,
                oned_graph_bfs_run, oned_graph_bfs_traverse, oned_graph_sssp_reset, oned_graph_sssp_traverse,
                search_grid, sssp_status, sssp_workspace_bytes)
@@ -69,6 +69,7 @@ class Result:
     done: float           # seconds, same clock as arrival
     batch: int            # queries in the launch that answered it
     value: torch.Tensor | None = None  # depth (int32) or distance (float32), when kept
+    ok: bool = True       # False: the launch reported a device error (its result is not valid)
 
     @property
     def latency(self) -> float:
@@ -97,12 +98,14 @@ class ServerStats:
     max_inflight: int = 0
     workspaces: dict = field(default_factory=dict)
     refused_for_memory: int = 0
+    device_errors: int = 0                           # launches whose status reported an error
+    errors: list = field(default_factory=list)       # the first few messages
 
 
 class GraphServer:
     def __init__(self, graphs: list[OnedGraph], slots: int = 4, hbm_reserve: int = 8 << 30,
                  max_batch: int = MSBFS_MAX_ROOTS, keep_results: bool = False, max_sssp_per_graph: int = 4,
-                 bfs_batch_min: int = 8):
+                 bfs_batch_min: int = 8, raise_errors: bool = True):
         if not graphs:
             raise ValueError("GraphServer needs at least one graph")
         self.graphs = graphs
@@ -112,6 +115,7 @@ class GraphServer:
         self.hbm_reserve = int(hbm_reserve)
         self.max_batch = int(max_batch)
         self.keep = keep_results
+        self.raise_errors = raise_errors
         self.max_sssp = int(max_sssp_per_graph)
         self.bfs_batch_min = max(1, int(bfs_batch_min))
         self.bfs_free: list[list[BfsState]] = [[] for _ in graphs]
@@ -290,28 +294,43 @@ class GraphServer:
             return True
         return False
 
+    def _checked(self, status, resource, stream) -> bool:
+        """Reads a finished launch's status.  A device error raises, or with
+        raise_errors=False is counted (the launch's queries are answered with
+        ok=False) and the server goes on: the next reset clears the state."""
+        try:
+            status(resource, stream)
+            return True
+        except G5Error as ex:
+            if self.raise_errors:
+                raise
+            self.stats.device_errors += 1
+            if len(self.stats.errors) < 8:
+                self.stats.errors.append(str(ex))
+            return False
+
     def _complete(self, L: _Launch, t: float) -> list[Result]:
         out = []
         if L.kind == "bfs1":
-            bfs_stats(L.resource, self.streams[L.slot])  # raises on a device error
+            ok = self._checked(bfs_stats, L.resource, self.streams[L.slot])
             q = L.queries[0]
-            v = L.resource.depth.clone() if self.keep else None
-            out.append(Result(q.qid, "bfs", q.graph, q.root, q.arrival, t, 1, v))
+            v = L.resource.depth.clone() if self.keep and ok else None
+            out.append(Result(q.qid, "bfs", q.graph, q.root, q.arrival, t, 1, v, ok))
             self.bfs_free[L.graph].append(L.resource)
         elif L.kind == "bfs":
-            msbfs_stats(L.resource, self.streams[L.slot])  # raises on a device error
+            ok = self._checked(msbfs_stats, L.resource, self.streams[L.slot])
             for i, q in enumerate(L.queries):
                 v = None
-                if self.keep:
+                if self.keep and ok:
                     v = L.out[i].to(torch.int32)
                     v[v == 255] = -1
-                out.append(Result(q.qid, q.kind, q.graph, q.root, q.arrival, t, len(L.queries), v))
+                out.append(Result(q.qid, q.kind, q.graph, q.root, q.arrival, t, len(L.queries), v, ok))
             self.ms_busy[L.graph] = False
         else:
-            sssp_status(L.resource, self.streams[L.slot])
+            ok = self._checked(sssp_status, L.resource, self.streams[L.slot])
             q = L.queries[0]
-            v = L.resource.dist.clone() if self.keep else None
-            out.append(Result(q.qid, q.kind, q.graph, q.root, q.arrival, t, 1, v))
+            v = L.resource.dist.clone() if self.keep and ok else None
+            out.append(Result(q.qid, q.kind, q.graph, q.root, q.arrival, t, 1, v, ok))
             self.sssp_free[L.graph].append(L.resource)
         self.free_slots.append(L.slot)
         self.blocks_in_use -= L.blocks
