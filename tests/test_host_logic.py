@@ -61,3 +61,27 @@ def test_query_host_pointer_cache_and_sssp_params(cgt):
     g.tiny_deg = torch.zeros(n, dtype=torch.int32)
     p = cgt._sssp_params(g, 0, 0.1, 0, 0.0, 0, False)
     assert p.tiny_deg == g.tiny_deg.data_ptr() and p.small == 0 and p.blocks == 0
+
+
+def test_server_status_errors_counted_or_raised(cgt):
+    """A launch whose status reports a device error raises by default; with
+    raise_errors=False it is counted and the server goes on."""
+    from cgt_b200 import serve as S
+
+    def bad(resource, stream):
+        raise cgt.G5Error("libg500b error -5: internal capacity exceeded")
+
+    def good(resource, stream):
+        return None
+
+    srv = object.__new__(S.GraphServer)
+    srv.stats = S.ServerStats()
+    srv.raise_errors = True
+    assert srv._checked(good, None, None)
+    try:
+        srv._checked(bad, None, None)
+        raise AssertionError("expected G5Error")
+    except cgt.G5Error:
+        pass
+    srv.raise_errors = False
+    assert not srv._checked(bad, None, None) and srv.stats.device_errors == 1 and len(srv.stats.errors) == 1
