@@ -124,7 +124,7 @@ class MsBfsStats(C.Structure):
 
 class SsspParams(C.Structure):
     _fields_ = [("delta", C.c_float), ("blocks", C.c_int32), ("pull", C.c_float), ("sub_min", C.c_int32),
-                ("small", C.c_int32), ("tiny_deg", C.c_void_p)]
+                ("small", C.c_int32), ("tiny_deg", C.c_void_p), ("check_opens", C.c_int32)]
 
 
 def _ptr(t: torch.Tensor | None) -> int | None:
@@ -776,19 +776,22 @@ def oned_graph_sssp_create(g: OnedGraph) -> SsspState:
     return SsspState(g)
 
 
-def _sssp_params(g: OnedGraph, root: int, delta, blocks, pull, sub_min, small) -> SsspParams:
+def _sssp_params(g: OnedGraph, root: int, delta, blocks, pull, sub_min, small, check_opens=False) -> SsspParams:
     # small=None: the lean one-block search for a root outside the main
     # component (when the grid is left to the library).
     if small is None:
         small = blocks == 0 and not g.in_main_component(root)
     return SsspParams(delta, 1 if small and blocks == 0 else blocks, pull, sub_min, int(bool(small)),
-                      _ptr(g.tiny_deg))
+                      _ptr(g.tiny_deg), int(bool(check_opens)))
 
 
 def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,
-                        pull: float = 0.0, sub_min: int = 0, small: bool | None = None, stream=None) -> None:
-    """oned_graph_sssp_run (src/traversal.h:52), delta 0.1 as the reference."""
-    p = _sssp_params(g, root, delta, blocks, pull, sub_min, small)
+                        pull: float = 0.0, sub_min: int = 0, small: bool | None = None, stream=None,
+                        check_opens: bool = False) -> None:
+    """oned_graph_sssp_run (src/traversal.h:52), delta 0.1 as the reference.
+    check_opens: the bucket and sub-bucket opens exchange their stamps and
+    fail the search if a queue held a vertex twice (a test aid)."""
+    p = _sssp_params(g, root, delta, blocks, pull, sub_min, small, check_opens)
     _check(lib.g5_sssp_run(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
                            g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                            sssp.work.numel(), C.byref(p), _stream(stream)))
@@ -805,10 +808,10 @@ def oned_graph_sssp_reset(sssp: SsspState, stream=None) -> None:
 
 def oned_graph_sssp_traverse(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,
                              pull: float = 0.0, sub_min: int = 0, small: bool | None = None,
-                             stream=None) -> None:
+                             stream=None, check_opens: bool = False) -> None:
     """The search itself, on a reset state (the lean one-block search for a
     root outside the main component)."""
-    p = _sssp_params(g, root, delta, blocks, pull, sub_min, small)
+    p = _sssp_params(g, root, delta, blocks, pull, sub_min, small, check_opens)
     _check(lib.g5_sssp_traverse(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
                                 g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                                 sssp.work.numel(), C.byref(p), _stream(stream)))

@@ -51,6 +51,9 @@ int deverr_to_status(unsigned flags, const char *what) {
     if (flags & DEVERR_RING)
         return set_error(G5_ERR_INVALID, "%s: an edge weight spans more buckets than the bucket ring holds; "
                          "use a larger delta (flags 0x%x)", what, flags);
+    if (flags & DEVERR_DUPLICATE)
+        return set_error(G5_ERR_DEVICE, "%s: a bucket or sub-bucket queue held a vertex twice (flags 0x%x)", what,
+                         flags);
     if (flags & DEVERR_UNPREPARED)
         return set_error(G5_ERR_INVALID, "%s: workspace not prepared for this graph (flags 0x%x)", what, flags);
     return set_error(G5_ERR_DEVICE, "%s: internal capacity exceeded (flags 0x%x)", what, flags);

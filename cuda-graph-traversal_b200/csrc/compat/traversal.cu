@@ -203,7 +203,7 @@ void oned_graph_sssp_run(Worker_State *ws, const Oned_Graph *g, Sssp_State *sssp
     // A root outside the largest component (host bitmap from the first BFS
     // state) runs on one block: its search touches a handful of vertices.
     const bool small = gx->main_host && !((gx->main_host[root >> 5] >> (root & 31)) & 1u);
-    g5_sssp_params p = {kLightDelta, small ? 1 : 0, 0.0f, 0, small ? 1 : 0, gx->tiny_deg};
+    g5_sssp_params p = {kLightDelta, small ? 1 : 0, 0.0f, 0, small ? 1 : 0, gx->tiny_deg, 0};
     check(ws, g5_sssp_traverse(g->rowstarts, gx->col, g->weights, gx->light_deg, gx->light_delta, g->nglobalverts,
                                root, sssp->dist, sssp->pred, sx->work, sx->work_bytes, &p, 0),
           "oned_graph_sssp_run");

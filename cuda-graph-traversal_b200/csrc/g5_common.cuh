@@ -65,6 +65,7 @@ enum : unsigned {
     DEVERR_DEPTH = 8u,      // a batched search went deeper than its depth planes hold
     DEVERR_UNPREPARED = 16u, // a batched-search workspace was not prepared for this graph
     DEVERR_RING = 32u,      // an SSSP relaxation landed beyond the bucket ring (delta too small for the weights)
+    DEVERR_DUPLICATE = 64u, // an SSSP queue held a vertex twice (reported only by the checked opens)
 };
 int deverr_to_status(unsigned flags, const char *what);
 

@@ -19,9 +19,9 @@
 //     and, among equal distances, the smallest parent -- no locks (the
 //     reference spins on a per-vertex lock, :224).
 //   * a ring of K bucket queues for the next K-1 buckets; a vertex enters a
-//     queue once per bucket (stamp per vertex), stale entries are dropped
-//     when the bucket opens.  No O(N) bucket scans (the reference scans all
-//     vertices per bucket, :297-331).
+//     bucket's queue at most once (its ring stamp only decreases), stale
+//     entries are dropped when the bucket opens.  No O(N) bucket scans (the
+//     reference scans all vertices per bucket, :297-331).
 //   * generation stamps for "already in this frontier" / "already in this
 //     bucket's heavy set", so nothing is cleared per iteration (the
 //     reference clears N visited flags per light iteration, :270-275).
@@ -153,7 +153,13 @@ struct SsspArgs {
     float pull_ratio;  // heavy phase pulls when its rows' entries >= pull_ratio x unsettled rows' entries; <= 0 never
     unsigned long long split_min;  // frontier light entries that start sub-buckets (~0: never)
     unsigned long long *pack;
-    unsigned *fstamp, *sstamp, *qstamp;
+    unsigned *fstamp, *sstamp;
+    // Queue stamps: the lowest bucket (rstamp) and sub-bucket (jstamp,
+    // fine_key) whose queue holds the vertex.  Both only decrease, by
+    // atomicMin, so a queue receives a vertex at most once -- however the
+    // deferred pushes of several warps interleave -- and every open may
+    // take its queue's entries as distinct.
+    unsigned *rstamp, *jstamp;
     unsigned *dstamp;        // expanded-set stamp: fine_id of the sub-bucket that expanded the vertex
     unsigned *settled;
     unsigned *cur;           // bitmap of the bucket being pulled from (heavy pull only)
@@ -167,6 +173,7 @@ struct SsspArgs {
     int64_t *pred;
     unsigned nblocks;
     unsigned long long limit_ns;
+    bool check_opens;  // opens exchange their stamps and flag a vertex met twice (DEVERR_DUPLICATE)
 };
 
 __device__ __forceinline__ float pack_dist(unsigned long long p) { return __uint_as_float((unsigned)(p >> 32)); }
@@ -239,10 +246,17 @@ struct PushCtx {
     unsigned d_tag;      // its stamp: fine_id(bucket, sub-bucket)
 };
 
-// Sub-bucket queue stamp of (bucket, j), kept apart from bucket-ring stamps
-// (bucket numbers) by the top bit.
+// Expanded-set stamp of sub-bucket j of `bucket` (compared for equality).
 __device__ __forceinline__ unsigned fine_id(unsigned bucket, int j) {
     return 0x80000000u | ((bucket * (unsigned)SUB + (unsigned)j) % 0x7fffffffu);
+}
+
+// Sub-bucket queue stamp of (bucket, j), compared by order: a vertex is
+// queued into sub-buckets of one bucket only (the bucket of its distance,
+// which settles it), where the key grows with j and stays below 2^31 - 1, so
+// it never meets the reset value ~0u.
+__device__ __forceinline__ unsigned fine_key(unsigned bucket, int j) {
+    return ((bucket * (unsigned)SUB) & 0x7fffffffu) + (unsigned)j;
 }
 
 // Largest j in [0, SUB) with t_j <= d, for d in [t_0, t_SUB).
@@ -258,19 +272,30 @@ __device__ __forceinline__ int sub_index(const float *t, float d) {
 // most once).  All 32 lanes call it.  `unique`: the caller's vertices are
 // distinct and none of them was pushed in this bucket (or sub-bucket) yet --
 // the entries of a bucket's ring queue or a sub-bucket's queue, which hold a
-// vertex at most once and are read by the first phase of their window --
-// so the stamps are set with plain stores instead of being exchanged.
+// vertex at most once (rstamp / jstamp) and are read by the first phase of
+// their window -- so the stamps are set with plain stores instead of being
+// exchanged.  With a.check_opens they are exchanged all the same, and a
+// vertex whose stamp is already in place is reported (DEVERR_DUPLICATE) and
+// not appended again.
 __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCtx &x, Counts &k, bool want_f,
                                                  bool want_s, unsigned v, bool unique = false) {
     SsspCtl *c = a.ctl;
     bool f, s, d;
-    if (unique) {
+    if (unique && !a.check_opens) {
         f = want_f;
         s = want_s;
         d = f && x.sub_mode;
         if (f) a.fstamp[v] = x.pid;
         if (s) a.sstamp[v] = x.bucket;
         if (d) a.dstamp[v] = x.d_tag;
+    } else if (unique) {
+        const bool df = want_f && atomicExch(&a.fstamp[v], x.pid) == x.pid;
+        const bool ds = want_s && atomicExch(&a.sstamp[v], x.bucket) == x.bucket;
+        const bool dd = want_f && x.sub_mode && atomicExch(&a.dstamp[v], x.d_tag) == x.d_tag;
+        if (df || ds || dd) atomicOr(&c->error, DEVERR_DUPLICATE);
+        f = want_f && !df;
+        s = want_s && !ds;
+        d = f && x.sub_mode && !dd;
     } else {
         f = want_f && atomicExch(&a.fstamp[v], x.pid) != x.pid;
         s = want_s && atomicExch(&a.sstamp[v], x.bucket) != x.bucket;
@@ -344,12 +369,14 @@ __device__ __forceinline__ bool stage_push(const WarpStage &q, bool want, unsign
     return ok;
 }
 
-// Appends v to sub-bucket queue j of the current bucket (lanes with j >= 0),
-// once per (vertex, sub-bucket).  Lanes with the same j append together
-// with one atomicAdd.  All 32 lanes call it.
+// Appends v to sub-bucket queue j of the current bucket (lanes with j >= 0)
+// unless v already sits in queue j or an earlier one (jstamp <= key): its
+// distance, hence its sub-bucket, only decreases, so every queue receives v
+// at most once.  Lanes with the same j append together with one atomicAdd.
+// All 32 lanes call it.
 __device__ __forceinline__ void push_fine(const SsspArgs &a, const PushCtx &x, int j, unsigned v) {
-    const unsigned id = j >= 0 ? fine_id(x.bucket, j) : 0u;
-    const bool r = j >= 0 && atomicExch(&a.qstamp[v], id) != id;
+    const unsigned key = j >= 0 ? fine_key(x.bucket, j) : 0u;
+    const bool r = j >= 0 && atomicMin(&a.jstamp[v], key) > key;
     unsigned todo = __ballot_sync(FULL, r);
     while (todo) {
         const int q = __shfl_sync(FULL, j, __ffs(todo) - 1);
@@ -420,9 +447,11 @@ __device__ __forceinline__ void run_pushes(const SsspArgs &a, const PushCtx &x, 
         push_fine(a, x, fine, v);
         k.front += fine >= 0;
     }
-    // Ring queue of the target bucket, once per (vertex, bucket), staged in
-    // the block's shared memory.
-    const bool r = target >= 0 && atomicExch(&a.qstamp[v], (unsigned)target) != (unsigned)target;
+    // Ring queue of the target bucket unless v already sits in that queue or
+    // an earlier one (rstamp <= target): targets only decrease, so a stale
+    // push that runs late (after a lower one) is dropped here and no queue
+    // receives v twice.  Staged in the block's shared memory.
+    const bool r = target >= 0 && atomicMin(&a.rstamp[v], (unsigned)target) > (unsigned)target;
     k.ring += r;
     k.front += same;
     // Per-slot warp staging: lanes with the same target slot append
@@ -707,6 +736,18 @@ __device__ __forceinline__ bool sssp_sync(const SsspArgs &a, unsigned &epoch, Ss
     return true;
 }
 
+// A list of capacity n keeps its small part at the front and its big part
+// at the back, each append checked against n on its own side only.  The
+// parts hold distinct vertices, so together they stay within n; a consumer
+// checks the sum all the same (every block reads the same snapshot, so all
+// leave together) and reports an overlap instead of reading a list whose
+// parts may have overwritten each other.
+__device__ __forceinline__ bool list_fits(const SsspArgs &a, unsigned ns, unsigned long long bp) {
+    if ((uint64_t)ns + big_count(bp) <= a.n) return true;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+    return false;
+}
+
 // ---- heavy-phase pull -------------------------------------------------------
 // When a bucket's rows hold at least pull_ratio times the CSR entries of the
 // rows of all vertices not settled yet, its heavy phase runs the other way
@@ -941,7 +982,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
         if (gtid == 0) {
             a.pack[a.root] = (unsigned long long)a.root;  // distance 0.0f, parent = root
             a.ring[0] = a.root;
-            a.qstamp[a.root] = 0;
+            a.rstamp[a.root] = 0;
             c->sn.ring_len[0] = 1;
         }
     } else {
@@ -951,7 +992,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
             const uint64_t r = __ldg(&a.roots[i]);
             if (r >= a.n) {
                 atomicOr(&c->error, DEVERR_RANGE);
-            } else if (atomicCAS(&a.qstamp[r], 0xffffffffu, 0u) == 0xffffffffu) {
+            } else if (atomicCAS(&a.rstamp[r], 0xffffffffu, 0u) == 0xffffffffu) {
                 a.pack[r] = r;
                 a.ring[atomicAdd(&c->sn.ring_len[0], 1u)] = (unsigned)r;
             }
@@ -1050,12 +1091,14 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
             const int s_cur = phase % 3, s_nxt = (phase + 1) % 3, s_clr = (phase + 2) % 3;
             const unsigned ns = sp->f_small[s_cur];
             const unsigned long long bp = sp->f_big[s_cur];
+            if (!list_fits(a, ns, bp)) return;
             const unsigned fsize = ns + big_count(bp);
             int nj = -1;
             if (fsize == 0) {
                 if (!x.sub_mode) break;
                 const unsigned dn = sp->d_small[x.d_slot];
                 const unsigned long long dbp = sp->d_big[x.d_slot];
+                if (!list_fits(a, dn, dbp)) return;
                 if (!just_settled && dn + big_count(dbp) > 0) {
                     // Settle pass of sub-bucket sj: every distance in it is
                     // final; its expanded set relaxes the deferred edges.
@@ -1172,6 +1215,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
             x.FBout = a.FB[(phase + 1) & 1];
             const unsigned ns = sp->s_small[sb];
             const unsigned long long bp = sp->s_big[sb];
+            if (!list_fits(a, ns, bp)) return;
             const unsigned long long s_ent = sp->s_entries[sb];
             // Every block reads the same counters after the barrier, so all
             // take the same branch.
@@ -1221,6 +1265,11 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
                 break;
             }
         if (!step) break;
+        // Ring targets are absolute bucket numbers held in an int.
+        if (bucket + (unsigned)step > 0x7fffffffu - RING) {
+            if (gtid == 0) atomicOr(&c->error, DEVERR_RING);
+            return;
+        }
         for (int j = 0; j < step; ++j) blo = __fadd_rn(blo, a.delta);
         bucket += step;
         __syncthreads();  // s_bnd is rewritten at the top of the loop
@@ -1405,7 +1454,7 @@ struct SsspWork {
     SsspCtl *ctl;
     SsspOut *out;
     unsigned long long *pack;
-    unsigned *fstamp, *sstamp, *qstamp, *dstamp, *settled, *cur;
+    unsigned *fstamp, *sstamp, *rstamp, *jstamp, *dstamp, *settled, *cur;
     unsigned *F[2], *FB[2], *S[2], *SB[2];
     unsigned *ring;
     unsigned *fq;
@@ -1420,7 +1469,8 @@ static SsspWork carve_sssp(void *base, uint64_t n) {
     w.pack = c.take<unsigned long long>(n);
     w.fstamp = c.take<unsigned>(n);
     w.sstamp = c.take<unsigned>(n);
-    w.qstamp = c.take<unsigned>(n);
+    w.rstamp = c.take<unsigned>(n);
+    w.jstamp = c.take<unsigned>(n);
     w.dstamp = c.take<unsigned>(n);
     w.settled = c.take<unsigned>((n + 31) / 32);
     w.cur = c.take<unsigned>((n + 31) / 32);
@@ -1493,7 +1543,7 @@ extern "C" int g5_sssp_reset(uint64_t nverts, float *d_dist, int64_t *d_pred, vo
         G5_CUDA_TRY(cudaMemsetAsync(w.out, 0, sizeof(SsspOut), st));
     }
     G5_CUDA_TRY(cudaMemsetAsync(w.pack, 0xff, nverts * sizeof(unsigned long long), st));
-    // fstamp, sstamp, qstamp, dstamp are consecutive carve-outs: one memset.
+    // fstamp, sstamp, rstamp, jstamp, dstamp are consecutive carve-outs: one memset.
     G5_CUDA_TRY(cudaMemsetAsync(w.fstamp, 0xff, (char *)(w.dstamp + nverts) - (char *)w.fstamp, st));
     // settled and cur are consecutive carve-outs: one memset.
     G5_CUDA_TRY(cudaMemsetAsync(w.settled, 0, (char *)(w.cur + (nverts + 31) / 32) - (char *)w.settled, st));
@@ -1509,7 +1559,7 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     SsspWork w;
     int rc = sssp_check(d_rowstarts, d_col, d_w, nverts, root, d_dist, d_pred, d_work, work_bytes, &w, who);
     if (rc) return rc;
-    g5_sssp_params p = {0.1f, 0, 0.0f, 0, 0, nullptr};
+    g5_sssp_params p = {0.1f, 0, 0.0f, 0, 0, nullptr, 0};
     if (params) p = *params;
     G5_CHECK_ARG(p.delta > 0.0f, "g5_sssp_traverse: delta must be positive");
     int max_blocks = 0;
@@ -1539,7 +1589,8 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     a.pack = w.pack;
     a.fstamp = w.fstamp;
     a.sstamp = w.sstamp;
-    a.qstamp = w.qstamp;
+    a.rstamp = w.rstamp;
+    a.jstamp = w.jstamp;
     a.dstamp = w.dstamp;
     a.settled = w.settled;
     a.cur = w.cur;
@@ -1557,6 +1608,7 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     a.pred = d_pred;
     a.nblocks = (unsigned)blocks;
     a.limit_ns = wait_limit_ns();
+    a.check_opens = p.check_opens != 0;
     void *args[] = {&a};
     if (p.small && !d_roots)
         sssp_small_kernel<<<1, SSSP_THREADS, 0, st>>>(a);

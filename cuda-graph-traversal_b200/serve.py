@@ -436,9 +436,19 @@ def poisson_trace(graphs: list[OnedGraph], nqueries: int, rate: float, bfs_share
 
 
 def latency_summary(results: list[Result]) -> dict:
-    lat = np.array([r.latency for r in results])
+    """Throughput and latency over the answered queries (ok); queries whose
+    launch reported a device error are counted apart under "failed" and do
+    not count towards qps or the percentiles.  The makespan runs from the
+    first arrival to the last completion of any query."""
+    good = [r for r in results if r.ok]
     span = max(r.done for r in results) - min(r.arrival for r in results)
-    return {"queries": len(results), "qps": round(len(results) / span, 1),
-            "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
-            "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
-            "mean_ms": round(float(lat.mean()) * 1e3, 3), "makespan_s": round(span, 3)}
+    out = {"queries": len(good), "failed": len(results) - len(good), "qps": round(len(good) / span, 1),
+           "makespan_s": round(span, 3)}
+    if good:
+        lat = np.array([r.latency for r in good])
+        out.update({"p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
+                    "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
+                    "mean_ms": round(float(lat.mean()) * 1e3, 3)})
+    else:
+        out.update({"p50_ms": None, "p99_ms": None, "mean_ms": None})
+    return out

@@ -218,7 +218,9 @@ int g5_bfs_last_trace(const void *d_work, uint64_t work_bytes, int max_levels, i
  * device address, so make it before any stream capture.  All calls share
  * the one array: calls that overlap on the GPU (other streams, other host
  * threads) race, so serialise them.  Each call clears what must start at
- * zero.  No counterpart in the reference. */
+ * zero.  The looked-up address lives as long as the device's context: after
+ * cudaDeviceReset on a device, do not call this entry point there again.
+ * No counterpart in the reference. */
 int g5_bfs_run_static(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
                       int64_t *d_pred, int32_t *d_depth, const g5_bfs_params *params, void *stream);
 
@@ -252,6 +254,10 @@ typedef struct g5_sssp_params {
                        g5_csr_split_tiny (optional, nullptr = not split).  A
                        sub-bucket then reads only that prefix of a row while
                        its distances are still dropping                      */
+    int32_t check_opens; /* 1: bucket and sub-bucket opens exchange their list
+                       stamps atomically and fail the search (G5_ERR_DEVICE,
+                       "held a vertex twice") if a queue held a vertex twice;
+                       a test aid, same results; 0 = plain stores (default) */
 } g5_sssp_params;
 
 int g5_sssp_workspace_size(uint64_t nverts, uint64_t *bytes);

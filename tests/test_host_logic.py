@@ -39,7 +39,12 @@ def test_poisson_trace_and_summary(cgt):
     res = [S.Result(q.qid, q.kind, q.graph, q.root, q.arrival, q.arrival + 0.001 * (1 + q.qid % 10), 1)
            for q in tr]
     s = S.latency_summary(res)
-    assert s["queries"] == 2000 and abs(s["p50_ms"] - 5.5) < 1.0 and s["p99_ms"] >= 9.9
+    assert s["queries"] == 2000 and s["failed"] == 0 and abs(s["p50_ms"] - 5.5) < 1.0 and s["p99_ms"] >= 9.9
+    # failed queries (ok=False) are counted apart, not in qps or the percentiles
+    res[0] = S.Result(0, "bfs", 0, 1, res[0].arrival, res[0].arrival + 100.0, 1, None, False)
+    f = S.latency_summary(res)
+    assert f["queries"] == 1999 and f["failed"] == 1 and f["p99_ms"] < 20.0
+    assert f["qps"] < s["qps"]  # the failed query still spans the makespan
 
 
 def test_query_host_pointer_cache_and_sssp_params(cgt):
