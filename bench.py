@@ -66,6 +66,15 @@ def metric_name(scale, ef):
     return f"harmonic-mean BFS GTEPS at SCALE {scale} ef{ef} (1 B200)"
 
 
+def bench_config(scale, ef, K, world, csr_entries):
+    """The workload, identical in both arms (ours and --impl reference)."""
+    return {"workload": f"graph500 bfs scale{scale} ef{ef}", "scale": scale, "edgefactor": ef,
+            "nverts": 1 << scale, "nedges": ef << scale, "csr_entries": int(csr_entries), "roots_per_rank": K,
+            "roots": "runner root choice (seeds 2, 3): the K roots after the W warm-up roots",
+            "l2": f"inputs larger than L2 (int32 column {csr_entries * 4 / 1e9:.1f} GB)",
+            "parallelism": f"replicas x{world}, roots sharded"}
+
+
 def hmean_gteps(nedge, secs):
     nedge = np.asarray(nedge, np.float64)
     secs = np.asarray(secs, np.float64)
@@ -247,21 +256,20 @@ def run_ours(args):
     sev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
             torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     torch.cuda.synchronize()
-    s_errors: list[str] = []
     nbuckets = nphases = 0
+    s_validated = 0
     for i, r in enumerate(timed):
         sev[i][0].record()
         G.oned_graph_sssp_reset(sssp)
         sev[i][1].record()
         G.oned_graph_sssp_traverse(g, sssp, r)
         sev[i][2].record()
-        # Every search's status is checked; a device error (a bounded wait
-        # that expired, a capacity overflow) is counted and reported.  The
-        # host wait falls outside the events.
-        try:
-            nbuckets, nphases = G.sssp_status(sssp)
-        except G.G5Error as ex:
-            s_errors.append(f"root {r}: {ex}")
+        # Every search's status is read (a device error -- a bounded wait
+        # that expired, a list overflow -- raises) and its result validated
+        # by the Graph500 SSSP rules; both run after the stop event.
+        nbuckets, nphases = G.sssp_status(sssp)
+        assert G.sssp_validate(g, r, sssp.dist, sssp.pred, vw) == 0, f"SSSP validation failed for root {r}"
+        s_validated += 1
     torch.cuda.synchronize()
     s_secs = [b.elapsed_time(c) / 1e3 for _, b, c in sev]
     s_secs_reset = [a.elapsed_time(c) / 1e3 for a, _, c in sev]
@@ -269,8 +277,6 @@ def run_ours(args):
     s_per_root = np.asarray(t_nedge, np.float64) / np.asarray(s_secs) / 1e9
     s_alg_bytes = [2 * nedge[timed[i]] * 8 + reached[timed[i]] * 28 for i in big]
     s_achieved_gbs = float(np.sum(s_alg_bytes) / np.sum([s_secs[i] for i in big]) / 1e9)
-    r_last = timed[-1]
-    assert G.sssp_validate(g, r_last, sssp.dist, sssp.pred, vw) == 0, "SSSP validation failed"
 
     # ---- end to end through the C ABI with host buffers, the runner's
     # protocol: untimed clear, then per step the root goes host->device from
@@ -303,9 +309,22 @@ def run_ours(args):
     if pg:
         max_ms, tot_edges, value = combine_ranks(pg, dev, total_ms, tot_edges, hm)
 
+    # ---- CPU baseline (rank 0, one GPU): the oracle's top-down BFS on the
+    # host cores over the same timed roots; each root's depth array is also
+    # compared with the GPU's (the parity check at this scale).
     cpu = None
+    parity = {"sssp_validated": s_validated, "bfs_trees_validated": 1}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(g, timed[:args.cpu_roots], nedge)
+        def gpu_depth(r):
+            # the GPU's depth array for r, its parent tree validated on the way
+            G.oned_graph_bfs_run(g, bfs, r)
+            d = G.bfs_compute_dist_from_pred(g, bfs, r)
+            assert G.bfs_validate(g, r, bfs.pred, d, vw) == 0, f"BFS validation failed for root {r}"
+            parity["bfs_trees_validated"] += 1
+            return bfs.depth.cpu().numpy()
+        cpu_roots = timed if args.cpu_roots <= 0 else timed[:args.cpu_roots]
+        cpu, checked = cpu_baseline_sample(g, cpu_roots, nedge, gpu_depth)
+        parity[f"s{scale}_depth_roots_checked"] = checked
     if rank == 0:
         line = {
             "metric": metric_name(scale, ef),
@@ -321,10 +340,7 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "int32",
             "data": "synthetic: Graph500 Kronecker generator (A,B,C,D = .57,.19,.19,.05), seeds (2,3), bit-identical to the reference's",
-            "config": {"workload": f"graph500 bfs scale{scale} ef{ef}", "scale": scale, "edgefactor": ef,
-                       "nverts": n, "nedges": m, "csr_entries": g.nlocaledges, "roots_per_rank": K,
-                       "roots": "runner root choice, seeds (2,3)", "l2": "inputs larger than L2 (int32 column "
-                       f"{g.nlocaledges * 4 / 1e9:.1f} GB)", "parallelism": f"replicas x{world}, roots sharded"},
+            "config": bench_config(scale, ef, K, world, g.nlocaledges),
             "aggregate_gteps": round(tot_edges / (max_ms / 1e3) / 1e9, 3),
             "hmean_gteps_with_reset": float(f"{hm_with_reset:.6g}"),
             "median_gteps": round(float(np.median(per_root_gteps)), 3),
@@ -355,7 +371,7 @@ def run_ours(args):
                      "median_gteps": round(float(np.median(s_per_root)), 3),
                      "big_root_ms_mean": round(float(np.mean([s_secs[i] for i in big])) * 1e3, 3),
                      "buckets_last_root": nbuckets, "phases_last_root": nphases, "delta": 0.1,
-                     "device_errors": s_errors,
+                     "validated": s_validated,
                      # The SSSP kernel against the same HBM roofline: algorithmic bytes
                      # per search = 2*nedge*(4 col + 4 w) + reached*(8 rowstarts + 8
                      # packed distance/parent + 12 output).
@@ -373,9 +389,12 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
-        if world == 1 and not (args.no_batched and args.no_packed and args.no_serve):
+        line["parity"] = parity
+        if world == 1:
             del g, bfs, vw, sssp  # the SCALE-26 graph is not needed any more
             torch.cuda.empty_cache()
+        if world == 1 and not args.no_reference_gpu:
+            line["reference_gpu"] = run_reference_gpu(scale, ef, roots_all, W, K, nedge, kern_s, s_secs, e2e_s)
         if world == 1 and not args.no_batched:
             line["batched"] = run_batched(G, dev, args.batched_scale, args.edgefactor, args.batched_roots)
             torch.cuda.empty_cache()
@@ -385,6 +404,7 @@ def run_ours(args):
             torch.cuda.empty_cache()
         if world == 1 and not args.no_serve:
             line["serving"] = run_serving(G, dev, args.serve_queries, args.serve_rate, args.edgefactor, args.serve_slots)
+        line["headline"] = headline(line)
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
@@ -563,8 +583,7 @@ def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0):
     build_s = time.time() - t0
     trace = S.poisson_trace(graphs, nqueries, rate, bfs_share=0.7, seed=1)
     warm = S.poisson_trace(graphs, 64, rate, bfs_share=0.5, seed=99)
-    # A launch that reports a device error is counted in the line, not fatal.
-    srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots, raise_errors=False)
+    srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots)
     srv.prewarm()  # workspaces created up front (admission by free HBM)
     srv.run_trace(warm, deadline=600)  # batched copies prepared, kernels loaded
     srv.stats = S.ServerStats()
@@ -576,7 +595,7 @@ def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0):
     low = None
     if low_rate:
         ltrace = S.poisson_trace(graphs, nqueries, low_rate, bfs_share=0.7, seed=2)
-        srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots, raise_errors=False)
+        srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots)
         srv.prewarm()
         srv.run_trace(warm, deadline=600)
         srv.stats = S.ServerStats()
@@ -618,26 +637,117 @@ def run_batched_only(args):
     print(json.dumps(out), flush=True)
 
 
-def cpu_baseline_sample(g, roots, nedge):
+def cpu_baseline_sample(g, roots, nedge, gpu_depth=None):
     """Oracle BFS (the reference's top-down algorithm, OpenMP on all host
-    cores) on the same CSR, copied to the host, for a few roots."""
+    cores) on the same CSR, copied to the host, for `roots` (the timed roots:
+    the same harmonic mean as `value`).  With gpu_depth(r) -> the GPU's
+    depth array for root r, every root's oracle depth array is compared with
+    it (a mismatch raises).  Returns (baseline dict, roots compared)."""
     from oracle import oracle as O
     rs = g.rowstarts.cpu().numpy().view(np.uint64)
     col = g.col.cpu().numpy().view(np.uint32)
     n = g.nglobalverts
     pred = np.empty(n, np.int64)
     depth = np.empty(n, np.int64)
-    secs = []
+    secs, checked, seen = [], 0, set()
     for r in roots:
         O.bfs_clear(n, pred, depth)
         t = time.perf_counter()
         O.bfs_search(rs, col, n, r, pred, depth)
         secs.append(time.perf_counter() - t)
-    return {"value": float(f"{hmean_gteps([nedge[r] for r in roots], secs):.6g}"), "unit": "GTEPS",
-            "cores": O.num_threads(), "kind": "port",
-            "median_gteps": round(float(np.median(np.asarray([nedge[r] for r in roots]) / np.asarray(secs) / 1e9)), 4),
-            "sample": f"first {len(roots)} timed roots of the same graph, oracle top-down BFS (OpenMP), "
-                      "clear untimed as in the runner"}
+        if gpu_depth is not None and r not in seen:
+            seen.add(r)
+            got = gpu_depth(r)
+            if not np.array_equal(got.astype(np.int64), depth):
+                raise AssertionError(f"GPU depth array of root {r} differs from the oracle's "
+                                     f"({int(np.count_nonzero(got.astype(np.int64) != depth))} vertices)")
+            checked += 1
+    ne = np.asarray([nedge[r] for r in roots], np.float64)
+    big = ne >= 0.5 * ne.max()
+    out = {"value": float(f"{hmean_gteps(ne, secs):.6g}"), "unit": "GTEPS",
+           "cores": O.num_threads(), "kind": "port",
+           "median_gteps": round(float(np.median(ne / np.asarray(secs) / 1e9)), 4),
+           "big_root_median_gteps": round(float(np.median((ne / np.asarray(secs) / 1e9)[big])), 4),
+           "sample": f"the {len(roots)} timed roots of the same graph (the harmonic mean of `value`), oracle "
+                     "top-down BFS (OpenMP), clear untimed as in the runner"}
+    return out, checked
+
+
+REF_BENCH = os.path.join(REPO, "oracle", "_ref", "ref_bench")
+
+
+def run_reference_gpu(scale, ef, roots, W, K, nedge, bfs_secs, sssp_secs, e2e_secs, sssp_big=2):
+    """The reference itself (its library built from its own sources into
+    oracle/_ref/ref_bench by oracle/ref.mk, np=1 through the single-process
+    shims) on this GPU, with its runner's protocol and host wall clock: BFS
+    from the same K timed roots, SSSP from the timed roots outside the main
+    component plus the first `sssp_big` main-component ones (a reference
+    SSSP of the big component takes ~5 s).  TEPS edge counts are this
+    graph's (the same graph, roots and counting rule)."""
+    if not os.path.exists(REF_BENCH):
+        return {"unavailable": "oracle/_ref/ref_bench is not built (the reference sources were absent at build)"}
+    timed = [roots[(W + i) % len(roots)] for i in range(K)]
+    t_ne = np.asarray([nedge[r] for r in timed], np.float64)
+    big = [i for i in range(K) if t_ne[i] >= 0.5 * t_ne.max()]
+    small = [i for i in range(K) if i not in big]
+    s_idx = sorted(set(small + big[:sssp_big]))
+    s_abs = [(W + i) % len(roots) for i in s_idx]
+    cmd = [REF_BENCH, str(scale), str(ef), str(K), "0", str(W), "0"] + [str(j) for j in s_abs]
+    t0 = time.time()
+    try:
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=900, check=True).stdout
+        rb = json.loads(out.strip().splitlines()[-1])
+    except Exception as ex:  # noqa: BLE001 -- a missing or failing reference is reported, not fatal
+        return {"unavailable": f"ref_bench failed: {str(ex)[:200]}"}
+    b_root = [int(x[0]) for x in rb["bfs"]]
+    assert b_root == timed, "reference roots differ from ours"
+    b_t = np.asarray([float(x[1]) for x in rb["bfs"]])
+    s_t = {int(x[0]): float(x[1]) for x in rb["sssp"]}
+    ours_b = np.asarray(bfs_secs)
+    res = {"what": "the reference's own library (np=1, built from its sources), same graph and roots, "
+                   "host wall clock around each synchronous oned_graph_*_run as its runner times it",
+           "generation_s": round(rb["generation_s"], 3), "construction_s": round(rb["construction_s"], 3),
+           "bfs": {"value": float(f"{hmean_gteps(t_ne, b_t):.6g}"), "unit": "GTEPS (harmonic mean, same K roots)",
+                   "median_gteps": round(float(np.median(t_ne / b_t / 1e9)), 4),
+                   "big_root_ms_median": round(float(np.median(b_t[big])) * 1e3, 3),
+                   "small_root_us": round(float(np.min(b_t[small])) * 1e6, 1) if small else None},
+           "sssp": {"roots": [timed[i] for i in s_idx], "ms": [round(s_t[timed[i]] * 1e3, 3) for i in s_idx],
+                    "big_root_ms_median": round(float(np.median([s_t[timed[i]] for i in big[:sssp_big]])) * 1e3, 1),
+                    "small_root_ms": round(min(s_t[timed[i]] for i in small) * 1e3, 3) if small else None},
+           "run_s": round(time.time() - t0, 1)}
+    ours_s = np.asarray(sssp_secs)
+    ref_s_big = np.median([s_t[timed[i]] for i in big[:sssp_big]])
+    res["ours_over_reference"] = {
+        "bfs_hmean": round(hmean_gteps(t_ne, ours_b) / res["bfs"]["value"], 2),
+        "bfs_hmean_e2e": round(hmean_gteps(t_ne, e2e_secs) / res["bfs"]["value"], 2),
+        "bfs_big_root_median": round(float(np.median(b_t[big]) / np.median(ours_b[big])), 1),
+        "sssp_big_root_median": round(float(ref_s_big / np.median(ours_s[big])), 1),
+        "sssp_small_root": round(float(min(s_t[timed[i]] for i in small) / np.min(ours_s[small])), 1)
+        if small else None}
+    return res
+
+
+def headline(line):
+    """A compact summary placed last in the line."""
+    h = {"bfs_hmean_gteps": line["value"], "bfs_median_gteps": line.get("median_gteps"),
+         "bfs_roofline_frac": line["roofline"]["frac"], "e2e_hmean_gteps": line["e2e"]["value"],
+         "sssp_hmean_gteps": line["sssp"]["value"], "sssp_median_gteps": line["sssp"]["median_gteps"],
+         "sssp_roofline_frac": line["sssp"]["roofline"]["frac"], "parity": line.get("parity")}
+    if "cpu_baseline" in line:
+        h["cpu_hmean_gteps"] = line["cpu_baseline"]["value"]
+    rg = line.get("reference_gpu")
+    if rg and "bfs" in rg:
+        h["reference_gpu_bfs_hmean_gteps"] = rg["bfs"]["value"]
+        h["ours_over_reference_gpu"] = rg["ours_over_reference"]
+    if "batched" in line:
+        h["batched_256_speedup"] = line["batched"]["speedup_vs_plain"]
+    if "packed" in line:
+        h["packed_speedup"] = line["packed"]["speedup_vs_plain"]
+    if "serving" in line:
+        sv = line["serving"]
+        h["serving"] = {"qps": sv["qps"], "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"],
+                        "qps_vs_plain": sv["qps_vs_plain"], "device_errors": sv["device_errors"]}
+    return h
 
 
 def run_reference(args):
@@ -682,8 +792,7 @@ def run_reference(args):
         "steps": K, "warmup": W, "ms_per_step": round(total / K * 1e3, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic: Graph500 Kronecker generator, seeds (2,3)",
-        "config": {"workload": f"graph500 bfs scale{scale} ef{ef}", "scale": scale, "edgefactor": ef,
-                   "roots_per_rank": K, "parallelism": "host cores"},
+        "config": bench_config(scale, ef, K, world, int(rs[-1])),
         "impl": "reference",
         "median_gteps": round(float(np.median(np.asarray([nedge[r] for r in timed]) / np.asarray(secs) / 1e9)), 4),
         "cpu_baseline": {"value": float(f"{v:.6g}"), "unit": "GTEPS", "cores": O.num_threads(), "kind": "port",
@@ -703,8 +812,11 @@ def main():
     ap.add_argument("--scale", type=int, default=26)
     ap.add_argument("--edgefactor", type=int, default=16)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-roots", type=int, default=2)
+    ap.add_argument("--cpu-roots", type=int, default=0,
+                    help="timed roots the CPU baseline searches (and compares depth arrays for); 0 = all")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU build (oracle/_ref/ref_bench) on the same roots")
     ap.add_argument("--batched-scale", type=int, default=24, help="SCALE of the batched (multi-source) BFS graph")
     ap.add_argument("--batched-roots", type=int, default=256)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched BFS measurement")

@@ -1132,7 +1132,11 @@ constexpr uint64_t STATIC_BFS_BYTES = 5ull << 20;
 static __device__ __align__(256) unsigned char g5_bfs_static_scratch[STATIC_BFS_BYTES];
 
 // Device address of the array on the current device, looked up once per
-// device (in host code the array's name is only a stand-in).
+// device (in host code the array's name is only a stand-in) and kept for the
+// life of the process.  cudaDeviceReset unloads this library's device image
+// with the device's context, and the next context holds a new copy of the
+// array at another address: a process that resets a device must not call
+// g5_bfs_run_static on it afterwards.
 static int static_bfs_scratch(void **out) {
     static std::mutex mu;
     static void *addr[64] = {};

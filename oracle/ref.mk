@@ -12,7 +12,8 @@
 #                             (jump table included) behind a C ABI
 #   _ref/ref_bench            ref_bench.cu timing the reference library with
 #                             its runner's protocol (selectable root counts)
-REF_ROOT ?= /root/reference
+# make -f ref.mk G5_REF_ROOT=<path to RuanPetrus/cuda-graph-traversal>
+REF_ROOT ?= $(G5_REF_ROOT)
 NVCC     ?= /usr/local/cuda/bin/nvcc
 ARCH     ?= -gencode arch=compute_100a,code=sm_100a
 SHIM     := ../include/compat/shim

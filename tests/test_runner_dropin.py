@@ -15,11 +15,24 @@ import pytest
 
 from tests.conftest import PKG_DIR, REPO, load_golden
 
-REF_RUNNER_SRC = "/root/reference/examples/graph500_runner.cu"
+
+
+def _ref_root() -> str:
+    """The reference checkout: G5_REF_ROOT, else the one the build used
+    (recorded by __graft_entry__.build in oracle/_ref/REF_ROOT)."""
+    root = os.environ.get("G5_REF_ROOT", "")
+    rec = os.path.join(REPO, "oracle", "_ref", "REF_ROOT")
+    if not root and os.path.exists(rec):
+        root = open(rec).read().strip()
+    return root
+
+
+REF_RUNNER_SRC = os.path.join(_ref_root(), "examples", "graph500_runner.cu") if _ref_root() else ""
 RUNNER = os.path.join(PKG_DIR, "lib", "graph500_runner")
 
 
-@pytest.mark.skipif(not os.path.exists(REF_RUNNER_SRC), reason="reference sources not present on this machine")
+@pytest.mark.skipif(not REF_RUNNER_SRC or not os.path.exists(REF_RUNNER_SRC),
+                    reason="reference sources not present on this machine")
 def test_runner_compiles_unchanged(tmp_path):
     out = tmp_path / "runner"
     cmd = ["/usr/local/cuda/bin/nvcc", "-O1", "-Drestrict=__restrict__",
