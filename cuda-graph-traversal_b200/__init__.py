@@ -59,9 +59,13 @@ def _load() -> C.CDLL:
         "g5_bfs_workspace_size": ([u64, p], C.c_int),
         "g5_bfs_run": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_bfs_reset": ([u64, p, p, p, p, u64, p], C.c_int),
+        "g5_bfs_reset_touched": ([u64, p, p, p, p, u64, p], C.c_int),
         "g5_graph_isolated_bitmap": ([p, u64, p, p], C.c_int),
         "g5_bfs_traverse": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_bfs_query": ([p, p, u64, p, p, p, p, p, u64, p, p, p], C.c_int),
+        "g5_bfs_query_plan_create": ([p, p, u64, p, p, p, p, u64, p, p, p, p], C.c_int),
+        "g5_bfs_query_plan_run": ([p, u64], C.c_int),
+        "g5_bfs_query_plan_destroy": ([p], None),
         "g5_bfs_visited_bitmap": ([p, u64, u64, p, p], C.c_int),
         "g5_bfs_last_stats": ([p, u64, p, p], C.c_int),
         "g5_bfs_last_trace": ([p, u64, C.c_int, p, p, p, p, p, p, p], C.c_int),
@@ -70,6 +74,7 @@ def _load() -> C.CDLL:
         "g5_sssp_run": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_sssp_last_status": ([p, u64, p, p, p], C.c_int),
         "g5_sssp_reset": ([u64, p, p, p, u64, p], C.c_int),
+        "g5_sssp_reset_touched": ([u64, p, p, p, u64, p], C.c_int),
         "g5_sssp_last_trace": ([p, u64, p, C.c_int, p, p, p, p, p, p], C.c_int),
         "g5_sssp_traverse": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_validate_workspace_size": ([u64, p], C.c_int),
@@ -96,6 +101,7 @@ def _load() -> C.CDLL:
 
 
 lib = _load()
+_plan_run = lib.g5_bfs_query_plan_run
 
 
 def _check(rc: int) -> None:
@@ -252,8 +258,10 @@ class OnedGraph:
 
 
 def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: float = 0.1,
-                                with_column64: bool = False, stream=None) -> OnedGraph:
-    """oned_graph_from_tuple_graph (src/traversal.h:43)."""
+                                with_column64: bool = False, stream=None, with_main: bool = True) -> OnedGraph:
+    """oned_graph_from_tuple_graph (src/traversal.h:43).  with_main=False
+    skips the main-component search (g.main_bits = None; set it later with
+    main_component_bitmap)."""
     dev = tg.edges.device
     n, m = int(nglobalverts), tg.edges_size
     nb = C.c_uint64()
@@ -276,7 +284,8 @@ def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: 
     _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), n, _ptr(iso), st))
     g = OnedGraph(n, e, rowstarts, col[:e], w[:e], light, light_delta, None if col64 is None else col64[:e], iso)
     g.tiny_deg = tiny
-    g.main_bits = main_component_bitmap(g, stream)
+    if with_main:
+        g.main_bits = main_component_bitmap(g, stream)
     return g
 
 
@@ -558,15 +567,24 @@ class BfsState:
         self.dist: torch.Tensor | None = None
         self.val_work: torch.Tensor | None = None
         self.max_nlocalverts = n
-        self.h_root = torch.zeros(1, dtype=torch.int64).pin_memory()
-        # Pinned too: g5_bfs_query then reads the root and writes the
-        # statistics from the device, with no copy calls.
+        # After its first reset the state undoes only what each search
+        # wrote (g5_bfs_reset_touched); the first one clears everything.
+        self.was_reset = False
+        # Pinned: the query path's kernel writes the statistics here itself.
         self._h_stats_buf = torch.zeros(C.sizeof(BfsStats), dtype=torch.uint8).pin_memory()
         self.h_stats = BfsStats.from_address(self._h_stats_buf.data_ptr())
-        # Raw addresses for the single-call query path.
-        self._root_slot = C.c_uint64.from_address(self.h_root.data_ptr())
-        self._q = (self.h_root.data_ptr(), self.pred.data_ptr(), self.depth.data_ptr(), self.work.data_ptr(),
-                   self.work.numel(), C.byref(self.h_stats))
+        self._plan = None  # (graph, with_depth, stream, g5_bfs_query_plan*, main bitmap) of the query path
+
+    def drop_plan(self) -> None:
+        if self._plan is not None:
+            lib.g5_bfs_query_plan_destroy(self._plan[3])
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.drop_plan()
+        except Exception:  # noqa: BLE001 -- interpreter shutdown
+            pass
 
 
 def oned_graph_bfs_create(g: OnedGraph) -> BfsState:
@@ -585,10 +603,12 @@ def oned_graph_bfs_reset(bfs: BfsState, with_depth: bool = True, g: OnedGraph | 
                          stream=None) -> None:
     """First half of oned_graph_bfs_run (the reference's oned_graph_bfs_clear):
     clear pred/depth and the workspace; with the graph, isolated vertices
-    start out visited."""
-    _check(lib.g5_bfs_reset(bfs.max_nlocalverts, _ptr(bfs.pred), _ptr(bfs.depth) if with_depth else None,
-                            _ptr(g.isolated) if g is not None else None, _ptr(bfs.work), bfs.work.numel(),
-                            _stream(stream)))
+    start out visited.  After the state's first reset only what the last
+    search wrote is undone (O(reached) after a one-block search)."""
+    fn = lib.g5_bfs_reset_touched if bfs.was_reset else lib.g5_bfs_reset
+    _check(fn(bfs.max_nlocalverts, _ptr(bfs.pred), _ptr(bfs.depth) if with_depth else None,
+              _ptr(g.isolated) if g is not None else None, _ptr(bfs.work), bfs.work.numel(), _stream(stream)))
+    bfs.was_reset = True
 
 
 def _right_sized(g: OnedGraph, root: int, params: BfsParams | None) -> BfsParams | None:
@@ -621,17 +641,32 @@ def _main_bits_ptr(g: OnedGraph) -> int | None:
 
 def oned_graph_bfs_query(g: OnedGraph, bfs: BfsState, root: int, with_depth: bool = False,
                          stream=None) -> BfsStats:
-    """One search end to end from the host (g5_bfs_query): the device reads
-    the root from pinned host memory, the search runs on a state reset since
-    its last search, and the device writes its statistics back to pinned
-    host memory; synchronises."""
-    bfs._root_slot.value = root
-    hr, pred, depth, work, nwork, stats = bfs._q
-    rc = lib.g5_bfs_query(g.rowstarts.data_ptr(), g.col.data_ptr(), g.nglobalverts, hr, _main_bits_ptr(g), pred,
-                          depth if with_depth else None, work, nwork, None, stats, _stream(stream))
+    """One search end to end from the host, the reference's synchronous
+    oned_graph_bfs_run on a state reset since its last search: the root goes
+    to the device as a launch argument, the device writes the statistics to
+    pinned host memory, and the host waits on them.  Runs through a
+    g5_bfs_query_plan made on the first query of this state with this graph,
+    depth choice and stream (C ABI: two arguments per query)."""
+    st = _stream(stream)
+    plan = bfs._plan
+    if plan is None or plan[0] is not g or plan[1] != with_depth or plan[2] != st or plan[4] is not g.main_bits:
+        plan = _make_query_plan(g, bfs, with_depth, st)
+    rc = _plan_run(plan[3], root)
     if rc:
         _check(rc)
     return bfs.h_stats
+
+
+def _make_query_plan(g: OnedGraph, bfs: BfsState, with_depth: bool, st):
+    bfs.drop_plan()
+    h = C.c_void_p()
+    _check(lib.g5_bfs_query_plan_create(g.rowstarts.data_ptr(), g.col.data_ptr(), g.nglobalverts, _main_bits_ptr(g),
+                                        bfs.pred.data_ptr(), bfs.depth.data_ptr() if with_depth else None,
+                                        bfs.work.data_ptr(), bfs.work.numel(), None, C.byref(bfs.h_stats), st,
+                                        C.byref(h)))
+    # The graph is held with the plan: the plan keeps its device pointers.
+    bfs._plan = (g, with_depth, st, h.value, g.main_bits)
+    return bfs._plan
 
 
 def bfs_stats(bfs: BfsState, stream=None) -> BfsStats:
@@ -770,6 +805,7 @@ class SsspState:
         self.pred = torch.empty(n, dtype=torch.int64, device=dev)
         self.dist = torch.empty(n, dtype=torch.float32, device=dev)
         self.max_nlocalverts = n
+        self.was_reset = False  # later resets undo only what the last search wrote
 
 
 def oned_graph_sssp_create(g: OnedGraph) -> SsspState:
@@ -795,15 +831,20 @@ def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float =
     _check(lib.g5_sssp_run(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
                            g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                            sssp.work.numel(), C.byref(p), _stream(stream)))
+    sssp.was_reset = True  # g5_sssp_run resets in full first
 
 
 def oned_graph_sssp_reset(sssp: SsspState, stream=None) -> None:
     """The reset half of oned_graph_sssp_run (the reference's
     oned_graph_sssp_clear, which its runner keeps outside the timed region):
     workspace cleared, dist = -1.0f and pred = -1 everywhere, so the search
-    writes only the vertices it reaches."""
-    _check(lib.g5_sssp_reset(sssp.max_nlocalverts, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
-                             sssp.work.numel(), _stream(stream)))
+    writes only the vertices it reaches.  After the state's first reset only
+    what the last search wrote is undone (O(reached) after a one-block
+    search)."""
+    fn = lib.g5_sssp_reset_touched if sssp.was_reset else lib.g5_sssp_reset
+    _check(fn(sssp.max_nlocalverts, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work), sssp.work.numel(),
+              _stream(stream)))
+    sssp.was_reset = True
 
 
 def oned_graph_sssp_traverse(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,

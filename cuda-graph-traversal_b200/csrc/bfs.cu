@@ -34,6 +34,9 @@
 #include <atomic>
 #include <mutex>
 
+#include <chrono>
+#include <new>
+
 #include "g5_common.cuh"
 #include "g5_frontier.cuh"
 
@@ -57,8 +60,8 @@ static_assert(sizeof(LevelState) % 8 == 0, "LevelState is copied in 8-byte words
 
 struct BfsCtl {
     g5_bfs_stats res;     // the search's result (same layout as the C ABI's)
+    const uint32_t *init_used;  // visited bitmap the last reset started from (nullptr: all clear)
     unsigned bar;         // grid barrier arrivals
-    unsigned long long root_in;  // root copied in by g5_bfs_query
     unsigned n_small[3];  // per level slot: queue entries of degree <= BIG_DEG
     unsigned long long big[3];  //           big entries << 40 | their chunks
     unsigned grab[3];     //                 work cursor over the small part
@@ -77,6 +80,20 @@ struct BfsCtl {
     unsigned long long m_level[BFS_TRACE];
     unsigned n_level[BFS_TRACE];
     unsigned char mode_level[BFS_TRACE];
+};
+
+// What the last search on a workspace wrote, for g5_bfs_reset_touched.
+// Only the search kernels write it (every block of the reset reads it): the
+// one-block search lists the vertices it reached (the touched list) and
+// records its outputs and the visited bitmap its reset started from; any
+// other search clears `small`, which makes the next reset a full one.
+struct BfsTouch {
+    unsigned small;
+    unsigned pad;
+    unsigned long long count;  // vertices in the touched list
+    int64_t *pred;
+    int32_t *depth;
+    const uint32_t *init;
 };
 
 struct BfsArgs {
@@ -99,13 +116,12 @@ struct BfsArgs {
     int mode;
     unsigned nblocks;
     unsigned long long limit_ns;
-    // Root source for g5_bfs_query: ctl->root_in (copied in on the stream)
-    // or the caller's mapped pinned host word; nullptr = `root`.
-    const unsigned long long *root_src;
     g5_bfs_stats *stats_out;  // the caller's mapped pinned host statistics, or nullptr
     unsigned long long seq;  // unique per launch: releases only this launch's waiting blocks
     const uint64_t *roots;   // several roots at once (device array) instead of `root`, or nullptr
     unsigned nroots;
+    BfsTouch *touch;
+    unsigned *tlist;  // touched list of the one-block search (n entries)
 };
 
 enum { TOP_DOWN = 0, BOTTOM_UP = 1 };
@@ -461,17 +477,20 @@ __device__ __forceinline__ bool bfs_advance(const BfsArgs &a, LevelState &st, un
 }
 
 // Copies the finished search's statistics to the caller's mapped host
-// memory (g5_bfs_query), visible to the host once the stream is synchronised
-// (the kernel's completion orders them; no fence is needed while the host
-// does not read before that).
+// memory (g5_bfs_query): `levels` last, after a system-scope fence, so a
+// host that set it to -1 before the launch and sees it change knows the
+// search -- its outputs and every other statistic -- is complete, without
+// waiting for the kernel's exit to reach the stream.
 __device__ __forceinline__ void bfs_publish_stats(const BfsArgs &a) {
     if (!a.stats_out) return;
     volatile g5_bfs_stats *r = &a.ctl->res;
-    a.stats_out->levels = r->levels;
-    a.stats_out->bottom_up_levels = r->bottom_up_levels;
-    a.stats_out->reached = r->reached;
-    a.stats_out->error_flags = r->error_flags;
-    a.stats_out->solo_levels = r->solo_levels;
+    volatile g5_bfs_stats *o = a.stats_out;
+    o->bottom_up_levels = r->bottom_up_levels;
+    o->reached = r->reached;
+    o->error_flags = r->error_flags;
+    o->solo_levels = r->solo_levels;
+    __threadfence_system();
+    o->levels = r->levels;
 }
 
 __device__ __forceinline__ void bfs_write_stats(const BfsArgs &a, const LevelState &st) {
@@ -509,13 +528,14 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
             c->t0 = globaltimer_ns();
             c->res = g5_bfs_stats{0, 0, 0, 0, 0};
             c->bar = 0;
+            a.touch->small = 0;  // the next reset clears everything
             for (int k = 0; k < 3; ++k) {
                 c->n_small[k] = c->grab[k] = c->cgrab[k] = c->found[k] = c->ulen[k] = 0;
                 c->big[k] = c->m_next[k] = 0;
             }
         }
         if (!a.roots) {
-            const unsigned root = a.root_src ? (unsigned)ld_volatile(a.root_src) : a.root;
+            const unsigned root = a.root;
             const uint64_t root_deg = __ldg(&a.rowptr[root + 1]) - __ldg(&a.rowptr[root]);
             if (threadIdx.x == 0) {
                 a.visited[root >> 5] |= 1u << (root & 31);
@@ -708,15 +728,16 @@ __global__ void __launch_bounds__(BFS_THREADS) bfs_small_kernel(BfsArgs a) {
     const unsigned lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (threadIdx.x == 0) {
         c->t0 = globaltimer_ns();
-        const unsigned long long root = a.root_src ? ld_volatile(a.root_src) : a.root;
+        const unsigned long long root = a.root;
         if (root >= a.n) {
-            s_err = DEVERR_RANGE;  // the host checks roots; a bad root_in is reported, not used
+            s_err = DEVERR_RANGE;  // the host checks roots; a bad one is reported, not used
             s_len[0] = 0;
         } else {
             uint64_t rb, re;
             claim_with_row(a.rowptr, a.visited, (unsigned)root, rb, re);
             a.pred[root] = (int64_t)root;
             if (a.depth) a.depth[root] = 0;
+            a.tlist[0] = (unsigned)root;
             s_v[0][0] = (unsigned)root;
             s_rb[0][0] = rb;
             s_re[0][0] = re;
@@ -758,6 +779,9 @@ __global__ void __launch_bounds__(BFS_THREADS) bfs_small_kernel(BfsArgs a) {
                 a.pred[v] = u;
                 if (a.depth) a.depth[v] = level + 1;
                 const unsigned pos = atomicAdd(&s_len[nxt], 1u);  // each vertex is claimed once: pos < n
+                // Touched list: vertices in claim order (s_reached counts the
+                // levels before this one), for g5_bfs_reset_touched.
+                if (s_reached + pos < a.n) a.tlist[s_reached + pos] = v;
                 if (pos < SMALL_Q) {
                     s_v[nxt][pos] = v;
                     s_rb[nxt][pos] = vb;
@@ -788,12 +812,16 @@ __global__ void __launch_bounds__(BFS_THREADS) bfs_small_kernel(BfsArgs a) {
         c->res.reached = s_reached;
         c->res.error_flags |= s_err;
         c->res.solo_levels = level;
+        // The touched list holds every vertex this search wrote (a search
+        // that reported an error leaves the next reset a full one).
+        *a.touch = BfsTouch{s_err == 0 && s_reached <= a.n ? 1u : 0u, 0u, s_reached, a.pred, a.depth, c->init_used};
         bfs_publish_stats(a);
     }
 }
 
 struct BfsWork {
     BfsCtl *ctl;
+    BfsTouch *touch;
     unsigned *visited, *fbits, *nbits, *zbits;
     unsigned *q[2], *base[2];
     uint64_t bytes;
@@ -804,6 +832,7 @@ static BfsWork carve_bfs(void *base, uint64_t n) {
     BfsWork w;
     const uint64_t words = (n + 31) / 32;
     w.ctl = c.take<BfsCtl>(1);
+    w.touch = c.take<BfsTouch>(1);
     w.visited = c.take<unsigned>(words);
     w.fbits = c.take<unsigned>(words);
     w.nbits = c.take<unsigned>(words);
@@ -925,33 +954,100 @@ extern "C" int g5_graph_isolated_bitmap(const uint64_t *d_rowstarts, uint64_t nv
     return G5_OK;
 }
 
-extern "C" int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, const uint32_t *d_visited_init,
-                            void *d_work, uint64_t work_bytes, void *stream) {
+struct BfsResetArgs {
+    uint64_t n;
+    int64_t *pred;
+    int32_t *depth;
+    const uint32_t *init;
+    unsigned *visited;
+    BfsCtl *ctl;
+    BfsTouch *touch;
+    const unsigned *tlist;
+    int full;  // 1: clear everything whatever the last search touched
+};
+
+// The reset before a search: pred (and depth) = -1, visited = the initial
+// bitmap (isolated vertices) or zero, a fresh control block.  Each of the
+// three arrays is restored vertex by vertex from the touched list when the
+// last search was a one-block search that wrote this very array (and
+// started from this very bitmap), else cleared in full.  A touched reset
+// reads the touch record in every block and leaves it alone; a full reset
+// reads none of it and records "nothing touched" for these arrays.
+__global__ void bfs_reset_kernel(BfsResetArgs r) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
+    const BfsTouch h = r.full ? BfsTouch{0u, 0u, 0ull, nullptr, nullptr, nullptr} : *r.touch;
+    if (r.full && t == 0) *r.touch = BfsTouch{1u, 0u, 0ull, r.pred, r.depth, r.init};
+    const bool small = !r.full && h.small && h.count <= r.n;
+    const bool pred_t = small && h.pred == r.pred;
+    const bool depth_t = small && h.depth == r.depth;
+    const bool vis_t = small && h.init == r.init;
+    if (blockIdx.x == 0) {
+        constexpr unsigned words = sizeof(BfsCtl) / 4;
+        static_assert(sizeof(BfsCtl) % 4 == 0, "control block cleared in words");
+        for (unsigned i = threadIdx.x; i < words; i += blockDim.x) ((unsigned *)r.ctl)[i] = 0;
+        __syncthreads();
+        if (threadIdx.x == 0) r.ctl->init_used = r.init;
+    }
+    if (pred_t || (r.depth && depth_t) || vis_t) {
+        for (uint64_t i = t; i < h.count; i += T) {
+            const unsigned v = __ldg(&r.tlist[i]);
+            if (v >= r.n) continue;
+            if (pred_t) r.pred[v] = -1;
+            if (r.depth && depth_t) r.depth[v] = -1;
+            if (vis_t) {
+                const unsigned bit = 1u << (v & 31);
+                if (r.init && (__ldg(&r.init[v >> 5]) & bit)) atomicOr(&r.visited[v >> 5], bit);
+                else atomicAnd(&r.visited[v >> 5], ~bit);
+            }
+        }
+    }
+    if (!pred_t) grid_fill<int64_t>(r.pred, r.n, -1, t, T);
+    if (r.depth && !depth_t) grid_fill<int32_t>(r.depth, r.n, -1, t, T);
+    if (!vis_t) {
+        const uint64_t words = (r.n + 31) / 32;
+        if (r.init)
+            for (uint64_t k = t; k < words; k += T) r.visited[k] = __ldg(&r.init[k]);
+        else
+            grid_fill<unsigned>(r.visited, words, 0u, t, T);
+    }
+}
+
+static int bfs_reset_launch(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, const uint32_t *d_visited_init,
+                            void *d_work, uint64_t work_bytes, void *stream, int full, const char *who) {
     clear_error();
-    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31) && d_pred && d_work, "g5_bfs_reset: bad argument");
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31) && d_pred && d_work, "%s: bad argument", who);
     BfsWork w = carve_bfs(d_work, nverts);
-    if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "g5_bfs_reset: workspace too small");
-    cudaStream_t st = (cudaStream_t)stream;
-    G5_CUDA_TRY(cudaMemsetAsync(d_pred, 0xff, nverts * sizeof(int64_t), st));
-    if (d_depth) G5_CUDA_TRY(cudaMemsetAsync(d_depth, 0xff, nverts * sizeof(int32_t), st));
-    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(BfsCtl), st));
-    const uint64_t vbytes = (nverts + 31) / 32 * sizeof(unsigned);
-    if (d_visited_init)
-        G5_CUDA_TRY(cudaMemcpyAsync(w.visited, d_visited_init, vbytes, cudaMemcpyDeviceToDevice, st));
-    else
-        G5_CUDA_TRY(cudaMemsetAsync(w.visited, 0, vbytes, st));
+    if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "%s: workspace too small", who);
+    DeviceInfo di;
+    int rc = device_info(&di);
+    if (rc) return rc;
+    BfsResetArgs r{nverts, d_pred, d_depth, d_visited_init, w.visited, w.ctl, w.touch, w.base[0], full};
+    const uint64_t want = (nverts + 2047) / 2048;  // 2048 vertices a block when the whole array is cleared
+    const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)di.sms * 8, want));
+    bfs_reset_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(r);
+    G5_CUDA_TRY(cudaGetLastError());
     return G5_OK;
 }
 
-// Builds the kernel arguments and launches the persistent BFS.  With h_root
-// the root is read on the device: from h_root itself when it is mapped
-// pinned memory (d_root_map), else from ctl->root_in after a copy on the
-// stream; d_stats_map (mapped pinned memory, or nullptr) receives the
-// statistics at the end of the search.
+extern "C" int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, const uint32_t *d_visited_init,
+                            void *d_work, uint64_t work_bytes, void *stream) {
+    return bfs_reset_launch(nverts, d_pred, d_depth, d_visited_init, d_work, work_bytes, stream, 1, "g5_bfs_reset");
+}
+
+extern "C" int g5_bfs_reset_touched(uint64_t nverts, int64_t *d_pred, int32_t *d_depth,
+                                    const uint32_t *d_visited_init, void *d_work, uint64_t work_bytes, void *stream) {
+    return bfs_reset_launch(nverts, d_pred, d_depth, d_visited_init, d_work, work_bytes, stream, 0,
+                            "g5_bfs_reset_touched");
+}
+
+// Builds the kernel arguments and launches the persistent BFS;
+// d_stats_map (mapped pinned memory, or nullptr) receives the statistics at
+// the end of the search.
 static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
                       uint64_t root, int64_t *d_pred, int32_t *d_depth, const g5_bfs_params *params,
-                      const uint64_t *h_root, cudaStream_t st, const uint64_t *d_roots = nullptr,
-                      unsigned nroots = 0, const uint64_t *d_root_map = nullptr, g5_bfs_stats *d_stats_map = nullptr) {
+                      cudaStream_t st, const uint64_t *d_roots = nullptr, unsigned nroots = 0,
+                      g5_bfs_stats *d_stats_map = nullptr) {
     g5_bfs_params p = {14.0f, 24.0f, 0, 0};
     if (params) p = *params;
     G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= BFS_SMALL, "g5_bfs: bad params");
@@ -982,15 +1078,13 @@ static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32
     a.mode = p.mode;
     a.nblocks = (unsigned)blocks;
     a.limit_ns = wait_limit_ns();
-    a.root_src = d_root_map ? (const unsigned long long *)d_root_map
-                            : h_root ? &w.ctl->root_in : nullptr;
     a.stats_out = d_stats_map;
     a.roots = d_roots;
     a.nroots = nroots;
+    a.touch = w.touch;
+    a.tlist = w.base[0];  // unused by the one-block search, which is the only writer
     static std::atomic<unsigned long long> next_seq{1};
     a.seq = next_seq.fetch_add(1);
-    if (h_root && !d_root_map)
-        G5_CUDA_TRY(cudaMemcpyAsync(&w.ctl->root_in, h_root, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     if (p.mode == BFS_SMALL && !d_roots) {
         bfs_small_kernel<<<1, BFS_THREADS, 0, st>>>(a);
         G5_CUDA_TRY(cudaGetLastError());
@@ -1031,7 +1125,7 @@ extern "C" int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col
     BfsWork w;
     int rc = bfs_check(d_rowstarts, d_col, nverts, root, d_pred, d_work, work_bytes, &w, "g5_bfs_traverse");
     if (rc) return rc;
-    return bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, params, nullptr, (cudaStream_t)stream);
+    return bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, params, (cudaStream_t)stream);
 }
 
 extern "C" int g5_bfs_traverse_multi(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
@@ -1042,8 +1136,8 @@ extern "C" int g5_bfs_traverse_multi(const uint64_t *d_rowstarts, const int32_t 
     BfsWork w;
     int rc = bfs_check(d_rowstarts, d_col, nverts, 0, d_pred, d_work, work_bytes, &w, "g5_bfs_traverse_multi");
     if (rc) return rc;
-    return bfs_launch(w, d_rowstarts, d_col, nverts, 0, d_pred, d_depth, params, nullptr, (cudaStream_t)stream,
-                      d_roots, nroots);
+    return bfs_launch(w, d_rowstarts, d_col, nverts, 0, d_pred, d_depth, params, (cudaStream_t)stream, d_roots,
+                      nroots);
 }
 
 // Device address of pinned host memory `h`, when the device can address it.
@@ -1056,6 +1150,28 @@ static bool host_mapped(const void *h, void **d) {
     if (at.type != cudaMemoryTypeHost || !at.devicePointer) return false;
     *d = at.devicePointer;
     return true;
+}
+
+// Waits for a query launched with mapped statistics: the kernel writes
+// `levels` (set to -1 by the host before the launch) last, after a system
+// fence, so a host spin on it sees the search complete a few microseconds
+// before a stream synchronisation would.  A search still running after
+// QUERY_SPIN_NS (a long one, or one that failed) is waited for with the
+// stream synchronisation, which also reports launch and device faults.
+constexpr double QUERY_SPIN_NS = 200e3;
+
+static int query_wait(g5_bfs_stats *h_stats, cudaStream_t st, const char *who) {
+    volatile int32_t *lv = &h_stats->levels;
+    const auto t0 = std::chrono::steady_clock::now();
+    while (*lv == -1) {
+        if (std::chrono::duration<double, std::nano>(std::chrono::steady_clock::now() - t0).count() > QUERY_SPIN_NS) {
+            G5_CUDA_TRY(cudaStreamSynchronize(st));
+            break;
+        }
+    }
+    std::atomic_thread_fence(std::memory_order_acquire);
+    if (*lv == -1) return set_error(G5_ERR_DEVICE, "%s: the search ended without statistics", who);
+    return deverr_to_status(h_stats->error_flags, who);
 }
 
 extern "C" int g5_bfs_query(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, const uint64_t *h_root,
@@ -1076,22 +1192,80 @@ extern "C" int g5_bfs_query(const uint64_t *d_rowstarts, const int32_t *d_col, u
         p.mode = BFS_SMALL;
     }
     cudaStream_t st = (cudaStream_t)stream;
-    // Pinned host memory that the device can address (mapped; every pinned
-    // allocation is under unified addressing) is read and written by the
-    // kernel itself: no copy calls around the search.
-    void *d_root_map = nullptr, *d_stats_map = nullptr;
-    const bool mapped = host_mapped(h_root, &d_root_map) && host_mapped(h_stats, &d_stats_map);
-    if (mapped) {
-        if ((rc = bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, &p, h_root, st, nullptr, 0,
-                             (const uint64_t *)d_root_map, (g5_bfs_stats *)d_stats_map)))
+    // Pinned host statistics that the device can address are written by the
+    // kernel itself (no copy call), and the host waits on them.
+    void *d_stats_map = nullptr;
+    if (host_mapped(h_stats, &d_stats_map)) {
+        *(volatile int32_t *)&h_stats->levels = -1;
+        if ((rc = bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, &p, st, nullptr, 0,
+                             (g5_bfs_stats *)d_stats_map)))
             return rc;
-    } else {
-        if ((rc = bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, &p, h_root, st))) return rc;
-        G5_CUDA_TRY(cudaMemcpyAsync(h_stats, &w.ctl->res, sizeof(g5_bfs_stats), cudaMemcpyDeviceToHost, st));
+        return query_wait(h_stats, st, "g5_bfs_query");
     }
+    if ((rc = bfs_launch(w, d_rowstarts, d_col, nverts, root, d_pred, d_depth, &p, st))) return rc;
+    G5_CUDA_TRY(cudaMemcpyAsync(h_stats, &w.ctl->res, sizeof(g5_bfs_stats), cudaMemcpyDeviceToHost, st));
     G5_CUDA_TRY(cudaStreamSynchronize(st));
     return deverr_to_status(h_stats->error_flags, "g5_bfs_query");
 }
+
+// A prepared g5_bfs_query: everything but the root checked and resolved
+// once, so a query costs one launch and the wait.
+struct g5_bfs_query_plan {
+    const uint64_t *rowstarts;
+    const int32_t *col;
+    uint64_t nverts;
+    const uint32_t *main_bits;
+    int64_t *pred;
+    int32_t *depth;
+    BfsWork w;
+    g5_bfs_params params;
+    g5_bfs_stats *h_stats, *d_stats;
+    cudaStream_t stream;
+};
+
+extern "C" int g5_bfs_query_plan_create(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
+                                        const uint32_t *h_main_bits, int64_t *d_pred, int32_t *d_depth,
+                                        void *d_work, uint64_t work_bytes, const g5_bfs_params *params,
+                                        g5_bfs_stats *h_stats, void *stream, g5_bfs_query_plan **out) {
+    clear_error();
+    G5_CHECK_ARG(out && h_stats, "g5_bfs_query_plan_create: NULL argument");
+    *out = nullptr;
+    BfsWork w;
+    int rc = bfs_check(d_rowstarts, d_col, nverts, 0, d_pred, d_work, work_bytes, &w, "g5_bfs_query_plan_create");
+    if (rc) return rc;
+    void *d_stats = nullptr;
+    G5_CHECK_ARG(host_mapped(h_stats, &d_stats),
+                 "g5_bfs_query_plan_create: h_stats must be pinned host memory the device can address");
+    g5_bfs_params p = {14.0f, 24.0f, 0, 0};
+    if (params) p = *params;
+    G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= BFS_SMALL, "g5_bfs_query_plan_create: bad params");
+    int max_blocks = 0;
+    if ((rc = bfs_max_blocks(&max_blocks))) return rc;  // resolved (and cached) now, not on the first query
+    auto *q = new (std::nothrow) g5_bfs_query_plan{d_rowstarts, d_col, nverts, h_main_bits, d_pred, d_depth, w, p,
+                                                   h_stats, (g5_bfs_stats *)d_stats, (cudaStream_t)stream};
+    if (!q) return set_error(G5_ERR_INVALID, "g5_bfs_query_plan_create: out of host memory");
+    *out = q;
+    return G5_OK;
+}
+
+extern "C" int g5_bfs_query_plan_run(g5_bfs_query_plan *q, uint64_t root) {
+    clear_error();
+    G5_CHECK_ARG(q, "g5_bfs_query_plan_run: NULL plan");
+    G5_CHECK_ARG(root < q->nverts, "g5_bfs_query_plan_run: root %llu outside [0, %llu)", (unsigned long long)root,
+                 (unsigned long long)q->nverts);
+    g5_bfs_params p = q->params;
+    if (q->main_bits && p.blocks == 0 && !((q->main_bits[root >> 5] >> (root & 31)) & 1u)) {
+        p.blocks = 1;
+        p.mode = BFS_SMALL;
+    }
+    *(volatile int32_t *)&q->h_stats->levels = -1;
+    int rc = bfs_launch(q->w, q->rowstarts, q->col, q->nverts, root, q->pred, q->depth, &p, q->stream, nullptr, 0,
+                        q->d_stats);
+    if (rc) return rc;
+    return query_wait(q->h_stats, q->stream, "g5_bfs_query_plan_run");
+}
+
+extern "C" void g5_bfs_query_plan_destroy(g5_bfs_query_plan *q) { delete q; }
 
 extern "C" int g5_bfs_visited_bitmap(const void *d_work, uint64_t work_bytes, uint64_t nverts, uint32_t *d_bits,
                                      void *stream) {

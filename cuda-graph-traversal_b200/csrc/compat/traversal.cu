@@ -60,6 +60,9 @@ b32 oned_graph_is_vertex_isolated(Worker_State *ws, const Oned_Graph *g, u64 glo
     return r[0] == r[1];
 }
 
+static void bfs_clear(Worker_State *ws, Bfs_State *bfs, bool first);
+static void sssp_clear(Worker_State *ws, Sssp_State *sssp, bool first);
+
 Bfs_State oned_graph_bfs_create(Worker_State *ws, const Oned_Graph *g) {
     Bfs_State bfs;
     memset(&bfs, 0, sizeof bfs);
@@ -95,21 +98,26 @@ Bfs_State oned_graph_bfs_create(Worker_State *ws, const Oned_Graph *g) {
         gx->main_host = (uint32_t *)malloc(words * sizeof(uint32_t));
         CHECK_CUDA(cudaMemcpy(gx->main_host, bits, words * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     }
-    oned_graph_bfs_clear(ws, &bfs);
+    bfs_clear(ws, &bfs, true);
     return bfs;
 }
 
-void oned_graph_bfs_clear(Worker_State *ws, Bfs_State *bfs) {
+// The state's first clear (at creation) resets everything; later ones undo
+// only what the last search wrote (O(reached) after a one-block search).
+static void bfs_clear(Worker_State *ws, Bfs_State *bfs, bool first) {
     const BfsExt *bx = get_bfs(bfs->pred);
     if (!bx) {
         ERROR("Bfs_State was not created by oned_graph_bfs_create of this library");
         worker_abort(ws, 1);
     }
-    check(ws, g5_bfs_reset(bfs->max_nlocalverts, bfs->pred, bx->depth, bx->isolated, bx->work, bx->work_bytes, 0),
+    auto reset = first ? g5_bfs_reset : g5_bfs_reset_touched;
+    check(ws, reset(bfs->max_nlocalverts, bfs->pred, bx->depth, bx->isolated, bx->work, bx->work_bytes, 0),
           "oned_graph_bfs_clear");
     if (bfs->dist) CHECK_CUDA(cudaMemset(bfs->dist, 0xff, bfs->max_nlocalverts * sizeof(i64)));
     CHECK_CUDA(cudaDeviceSynchronize());
 }
+
+void oned_graph_bfs_clear(Worker_State *ws, Bfs_State *bfs) { bfs_clear(ws, bfs, false); }
 
 void oned_graph_bfs_run(Worker_State *ws, const Oned_Graph *g, Bfs_State *bfs, u64 root) {
     if (root >= g->nglobalverts) {
@@ -171,22 +179,27 @@ Sssp_State oned_graph_sssp_create(Worker_State *ws, const Oned_Graph *g) {
     check(ws, g5_sssp_workspace_size(g->nglobalverts, &x.work_bytes), "oned_graph_sssp_create");
     x.work = gpu_push(ws, x.work_bytes, "SSSP workspace");
     put_sssp(s.pred, x);
-    oned_graph_sssp_clear(ws, &s);
+    sssp_clear(ws, &s, true);
     return s;
 }
 
-void oned_graph_sssp_clear(Worker_State *ws, Sssp_State *sssp) {
+// pred = -1 and dist = -1.0f everywhere, the reference's "unreached"
+// (src/traversal.cu:248-249); the search then writes reached vertices only.
+// The first clear (at creation) resets everything; later ones undo only what
+// the last search wrote.
+static void sssp_clear(Worker_State *ws, Sssp_State *sssp, bool first) {
     const SsspExt *sx = get_sssp(sssp->pred);
     if (!sx) {
         ERROR("Sssp_State was not created by oned_graph_sssp_create of this library");
         worker_abort(ws, 1);
     }
-    // pred = -1 and dist = -1.0f everywhere, the reference's "unreached"
-    // (src/traversal.cu:248-249); the search then writes reached vertices only.
-    check(ws, g5_sssp_reset(sssp->max_nlocalverts, sssp->dist, sssp->pred, sx->work, sx->work_bytes, 0),
+    auto reset = first ? g5_sssp_reset : g5_sssp_reset_touched;
+    check(ws, reset(sssp->max_nlocalverts, sssp->dist, sssp->pred, sx->work, sx->work_bytes, 0),
           "oned_graph_sssp_clear");
     CHECK_CUDA(cudaDeviceSynchronize());
 }
+
+void oned_graph_sssp_clear(Worker_State *ws, Sssp_State *sssp) { sssp_clear(ws, sssp, false); }
 
 void oned_graph_sssp_run(Worker_State *ws, const Oned_Graph *g, Sssp_State *sssp, u64 root) {
     if (root >= g->nglobalverts) {

@@ -194,6 +194,24 @@ __device__ __forceinline__ int warp_owner(unsigned excl, unsigned e) {
     return lo;
 }
 
+// p[0 .. n) = x for the calling grid (thread t of T), with 16-byte stores
+// once p is 16-byte aligned (sizeof(T) is 4 or 8).
+template <class T>
+__device__ __forceinline__ void grid_fill(T *p, uint64_t n, T x, uint64_t t, uint64_t T_) {
+    constexpr uint64_t per = 16 / sizeof(T);
+    const uint64_t mis = ((uintptr_t)p & 15) / sizeof(T);
+    const uint64_t head = mis ? (per - mis < n ? per - mis : n) : 0;
+    if (t < head) p[t] = x;
+    const uint64_t nvec = (n - head) / per;
+    T v[per];
+#pragma unroll
+    for (uint64_t k = 0; k < per; ++k) v[k] = x;
+    const uint4 q = *reinterpret_cast<const uint4 *>(v);
+    uint4 *pv = reinterpret_cast<uint4 *>(p + head);
+    for (uint64_t i = t; i < nvec; i += T_) pv[i] = q;
+    for (uint64_t i = head + nvec * per + t; i < n; i += T_) p[i] = x;
+}
+
 __device__ __forceinline__ bool bit_test(const unsigned *bm, unsigned v) { return (bm[v >> 5] >> (v & 31)) & 1u; }
 
 // Sets bit v; true when this call changed it from 0 to 1.

@@ -104,6 +104,19 @@ struct SsspSnap {
 };
 constexpr int SNAP_WORDS = (int)(sizeof(SsspSnap) / 4);
 
+// What the last search on a workspace wrote, for g5_sssp_reset_touched.
+// Only the search kernels write it (every block of the reset reads it): the
+// one-block search lists every vertex it reached in the first heavy-set
+// array and records its outputs; a grid search clears `small`, which makes
+// the next reset a full one.
+struct SsspTouch {
+    unsigned small;
+    unsigned sparse;           // the outputs were pre-filled and only reached vertices written
+    unsigned long long count;  // vertices in the list
+    float *dist;
+    int64_t *pred;
+};
+
 struct SsspCtl {
     SsspSnap sn;  // first: copied as words 0 .. SNAP_WORDS-1
     unsigned bar;
@@ -168,6 +181,7 @@ struct SsspArgs {
     unsigned *ring;
     unsigned *fq;  // SUB sub-bucket queues of n entries
     SsspCtl *ctl;
+    SsspTouch *touch;
     const SsspOut *prefilled;
     float *dist;
     int64_t *pred;
@@ -978,6 +992,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
     const unsigned long long e_total = __ldg(&a.rowptr[a.n]);
     unsigned long long settled_entries = 0;  // CSR entries of the rows of settled vertices
 
+    if (gtid == 0) a.touch->small = 0;  // the next reset clears everything
     if (!a.roots) {
         if (gtid == 0) {
             a.pack[a.root] = (unsigned long long)a.root;  // distance 0.0f, parent = root
@@ -1326,7 +1341,7 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
     __shared__ unsigned s_err;
     __shared__ bool s_sparse;
     const unsigned lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    unsigned *R = a.S[0];  // every vertex reached, once (sstamp); entries from SMALL_L on
+    unsigned *R = a.S[0];  // every vertex reached, once (sstamp): the touched list
     if (threadIdx.x == 32) {
         // Whether the outputs were pre-filled: loaded by another warp while
         // the search runs, read after it.
@@ -1341,6 +1356,7 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
         s_rb[0][0] = __ldg(&a.rowptr[a.root]);
         s_re[0][0] = __ldg(&a.rowptr[a.root + 1]);
         s_r[0] = a.root;
+        R[0] = a.root;
         s_len[0] = 1;
         s_len[1] = 0;
         s_nreach = 1;
@@ -1399,7 +1415,7 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
                 if (sold != 0u) {
                     const unsigned pos = atomicAdd(&s_nreach, 1u);
                     if (pos < SMALL_L) s_r[pos] = v;
-                    else if (pos < a.n) R[pos] = v;
+                    if (pos < a.n) R[pos] = v;
                     else atomicOr(&s_err, DEVERR_CAPACITY);
                 }
             }
@@ -1436,22 +1452,15 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
         c->buckets = 1;
         c->phases = round;
         c->error |= s_err;
+        // R lists every vertex this search wrote (a search that reported an
+        // error leaves the next reset a full one).
+        *a.touch = SsspTouch{s_err == 0 && s_nreach <= a.n ? 1u : 0u, s_sparse ? 1u : 0u, s_nreach, a.dist, a.pred};
     }
-}
-
-// Fills the outputs with "unreached" and records them as pre-filled.
-__global__ void sssp_prefill_kernel(float *__restrict__ dist, int64_t *__restrict__ pred, uint64_t n, SsspOut *hdr) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    for (uint64_t v = t; v < n; v += stride) {
-        dist[v] = -1.0f;
-        pred[v] = -1;
-    }
-    if (t == 0) *hdr = SsspOut{dist, pred};
 }
 
 struct SsspWork {
     SsspCtl *ctl;
+    SsspTouch *touch;
     SsspOut *out;
     unsigned long long *pack;
     unsigned *fstamp, *sstamp, *rstamp, *jstamp, *dstamp, *settled, *cur;
@@ -1465,6 +1474,7 @@ static SsspWork carve_sssp(void *base, uint64_t n) {
     Carver c(base);
     SsspWork w;
     w.ctl = c.take<SsspCtl>(1);
+    w.touch = c.take<SsspTouch>(1);
     w.out = c.take<SsspOut>(1);
     w.pack = c.take<unsigned long long>(n);
     w.fstamp = c.take<unsigned>(n);
@@ -1525,31 +1535,87 @@ static int sssp_check(const uint64_t *d_rowstarts, const int32_t *d_col, const f
     return G5_OK;
 }
 
+struct SsspResetArgs {
+    uint64_t n;
+    float *dist;
+    int64_t *pred;
+    SsspWork w;
+    int full;  // 1: clear everything whatever the last search touched
+};
+
+// The reset before a search: packed distances ~0, the five stamp arrays ~0,
+// settled and pull bitmaps 0, a fresh control block and, with outputs,
+// dist = -1.0f / pred = -1 recorded as pre-filled.  After a one-block search
+// (which touches only the packed distances, two stamp arrays and the
+// outputs of the vertices it reached, all listed) those entries are
+// restored one by one; anything else is cleared in full.  A touched reset
+// reads the touch record in every block and leaves it alone; a full reset
+// reads none of it and records "nothing touched" for these outputs.
+__global__ void sssp_reset_kernel(SsspResetArgs r) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
+    const SsspWork &w = r.w;
+    const SsspTouch h = r.full ? SsspTouch{0u, 0u, 0ull, nullptr, nullptr} : *w.touch;
+    if (r.full && t == 0) *w.touch = SsspTouch{1u, r.dist ? 1u : 0u, 0ull, r.dist, r.pred};
+    const bool small = !r.full && h.small && h.count <= r.n;
+    const bool out_t = small && h.sparse && h.dist == r.dist && h.pred == r.pred;
+    if (blockIdx.x == 0) {
+        constexpr unsigned words = sizeof(SsspCtl) / 4;
+        static_assert(sizeof(SsspCtl) % 4 == 0, "control block cleared in words");
+        for (unsigned i = threadIdx.x; i < words; i += blockDim.x) ((unsigned *)w.ctl)[i] = 0;
+        if (threadIdx.x == 0) *w.out = SsspOut{r.dist, r.pred};
+    }
+    if (small) {
+        const unsigned *L = w.S[0];
+        for (uint64_t i = t; i < h.count; i += T) {
+            const unsigned v = __ldg(&L[i]);
+            if (v >= r.n) continue;
+            w.pack[v] = UNREACHED;
+            w.fstamp[v] = ~0u;
+            w.sstamp[v] = ~0u;
+            if (r.dist && out_t) {
+                r.dist[v] = -1.0f;
+                r.pred[v] = -1;
+            }
+        }
+    } else {
+        grid_fill<unsigned long long>(w.pack, r.n, UNREACHED, t, T);
+        // fstamp .. dstamp are consecutive carve-outs, settled and cur too.
+        grid_fill<unsigned>(w.fstamp, (uint64_t)((w.dstamp + r.n) - w.fstamp), ~0u, t, T);
+        grid_fill<unsigned>(w.settled, (uint64_t)((w.cur + (r.n + 31) / 32) - w.settled), 0u, t, T);
+    }
+    if (r.dist && !out_t) {
+        grid_fill<float>(r.dist, r.n, -1.0f, t, T);
+        grid_fill<int64_t>(r.pred, r.n, -1, t, T);
+    }
+}
+
+static int sssp_reset_launch(uint64_t nverts, float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes,
+                             void *stream, int full, const char *who) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31) && d_work, "%s: bad argument", who);
+    G5_CHECK_ARG((d_dist == nullptr) == (d_pred == nullptr), "%s: give both outputs or neither", who);
+    SsspWork w = carve_sssp(d_work, nverts);
+    if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "%s: workspace too small", who);
+    DeviceInfo di;
+    int rc = device_info(&di);
+    if (rc) return rc;
+    SsspResetArgs r{nverts, d_dist, d_pred, w, full};
+    const uint64_t want = (nverts + 2047) / 2048;  // 2048 vertices a block when everything is cleared
+    const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)di.sms * 8, want));
+    sssp_reset_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(r);
+    G5_CUDA_TRY(cudaGetLastError());
+    return G5_OK;
+}
+
 extern "C" int g5_sssp_reset(uint64_t nverts, float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes,
                              void *stream) {
-    clear_error();
-    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31) && d_work, "g5_sssp_reset: bad argument");
-    G5_CHECK_ARG((d_dist == nullptr) == (d_pred == nullptr), "g5_sssp_reset: give both outputs or neither");
-    SsspWork w = carve_sssp(d_work, nverts);
-    if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "g5_sssp_reset: workspace too small");
-    cudaStream_t st = (cudaStream_t)stream;
-    if (d_dist) {
-        DeviceInfo di;
-        int rc = device_info(&di);
-        if (rc) return rc;
-        sssp_prefill_kernel<<<di.sms * 8, 256, 0, st>>>(d_dist, d_pred, nverts, w.out);
-        G5_CUDA_TRY(cudaGetLastError());
-    } else {
-        G5_CUDA_TRY(cudaMemsetAsync(w.out, 0, sizeof(SsspOut), st));
-    }
-    G5_CUDA_TRY(cudaMemsetAsync(w.pack, 0xff, nverts * sizeof(unsigned long long), st));
-    // fstamp, sstamp, rstamp, jstamp, dstamp are consecutive carve-outs: one memset.
-    G5_CUDA_TRY(cudaMemsetAsync(w.fstamp, 0xff, (char *)(w.dstamp + nverts) - (char *)w.fstamp, st));
-    // settled and cur are consecutive carve-outs: one memset.
-    G5_CUDA_TRY(cudaMemsetAsync(w.settled, 0, (char *)(w.cur + (nverts + 31) / 32) - (char *)w.settled, st));
-    // Fresh control block (counters, cursors, trace) for the next search.
-    G5_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(SsspCtl), st));
-    return G5_OK;
+    return sssp_reset_launch(nverts, d_dist, d_pred, d_work, work_bytes, stream, 1, "g5_sssp_reset");
+}
+
+extern "C" int g5_sssp_reset_touched(uint64_t nverts, float *d_dist, int64_t *d_pred, void *d_work,
+                                     uint64_t work_bytes, void *stream) {
+    return sssp_reset_launch(nverts, d_dist, d_pred, d_work, work_bytes, stream, 0, "g5_sssp_reset_touched");
 }
 
 static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
@@ -1603,6 +1669,7 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     a.ring = w.ring;
     a.fq = w.fq;
     a.ctl = w.ctl;
+    a.touch = w.touch;
     a.prefilled = w.out;
     a.dist = d_dist;
     a.pred = d_pred;

@@ -155,14 +155,28 @@ int g5_bfs_run(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nvert
 /* d_bits[ceil(nverts/32)]: bit v set when vertex v has no CSR entry. */
 int g5_graph_isolated_bitmap(const uint64_t *d_rowstarts, uint64_t nverts, uint32_t *d_bits, void *stream);
 
-/* g5_bfs_run in two steps, like the reference's oned_graph_bfs_clear +
- * oned_graph_bfs_run: g5_bfs_reset clears pred (-1), depth (-1) and the
- * workspace's visited bitmap (O(N) writes) -- to a copy of d_visited_init
- * when given (the isolated-vertex bitmap, so bottom-up levels skip vertices
- * no search can reach); g5_bfs_traverse zeroes the small control block and
- * runs the persistent kernel (on a reset state). */
+/* g5_bfs_run in two steps, like the reference's oned_graph_bfs_clear
+ * (src/traversal.cu:464-477) + oned_graph_bfs_run: g5_bfs_reset clears pred
+ * (-1), depth (-1) and the workspace's visited bitmap (O(N) writes) -- to a
+ * copy of d_visited_init when given (the isolated-vertex bitmap, so
+ * bottom-up levels skip vertices no search can reach) -- and the control
+ * block; g5_bfs_traverse runs the persistent kernel (on a reset state). */
 int g5_bfs_reset(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, const uint32_t *d_visited_init, void *d_work,
                  uint64_t work_bytes, void *stream);
+
+/* g5_bfs_reset that undoes only what the last search on this workspace
+ * wrote, for a workspace that has been reset (by either call) and searched
+ * since: after a search that ran on one block (a root outside the main
+ * component) it restores the vertices that search reached -- O(reached)
+ * instead of O(N) -- in each of pred, depth and the visited bitmap that the
+ * search wrote (the same arrays and initial bitmap as now); anything else
+ * (another array, a grid search, a search that reported an error) is
+ * cleared in full.  The decision is taken on the device, so the call stays
+ * stream-ordered.  Not for a workspace fresh from the allocator: its first
+ * reset must be g5_bfs_reset.  No counterpart in the reference (its clear is
+ * always O(N)). */
+int g5_bfs_reset_touched(uint64_t nverts, int64_t *d_pred, int32_t *d_depth, const uint32_t *d_visited_init,
+                         void *d_work, uint64_t work_bytes, void *stream);
 int g5_bfs_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
                     int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
                     const g5_bfs_params *params, void *stream);
@@ -177,16 +191,34 @@ int g5_bfs_traverse_multi(const uint64_t *d_rowstarts, const int32_t *d_col, uin
                           const g5_bfs_params *params, void *stream);
 
 /* One search end to end from host memory, for callers that issue single
- * queries: reads *h_root, runs the traversal on a workspace reset since its
- * last search, stores the statistics in *h_stats and synchronises.  When
- * both are pinned host memory the kernel itself reads the root and writes
- * the statistics (no copy calls); otherwise they are copied on the stream.  h_main_bits (host bitmap of the
- * main component, optional; see g5_bfs_visited_bitmap) lets a root outside
- * it run on a single block, which a small component needs and which avoids
- * launching and waiting for the whole grid. */
+ * queries (the reference's synchronous oned_graph_bfs_run,
+ * src/traversal.cu:479-503): reads *h_root, runs the traversal on a
+ * workspace reset since its last search, stores the statistics in *h_stats
+ * and returns once the search is complete.  When h_stats is pinned host
+ * memory the kernel writes it itself (no copy call) and the host waits on
+ * it rather than on the stream; otherwise it is copied on the stream, which
+ * is then synchronised.  h_main_bits (host bitmap of the main component,
+ * optional; see g5_bfs_visited_bitmap) lets a root outside it run on a
+ * single block, which a small component needs and which avoids launching
+ * and waiting for the whole grid. */
 int g5_bfs_query(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, const uint64_t *h_root,
                  const uint32_t *h_main_bits, int64_t *d_pred, int32_t *d_depth, void *d_work, uint64_t work_bytes,
                  const g5_bfs_params *params, g5_bfs_stats *h_stats, void *stream);
+
+/* g5_bfs_query prepared once for many queries on one graph, workspace and
+ * set of outputs: the arguments are checked and resolved at creation, so
+ * g5_bfs_query_plan_run(plan, root) costs one launch and the wait.  h_stats
+ * must be pinned host memory the device can address; each run overwrites
+ * it.  Reset the workspace before every run as for g5_bfs_query.  The plan
+ * keeps pointers only; destroy it before freeing what they point to.  No
+ * counterpart in the reference. */
+typedef struct g5_bfs_query_plan g5_bfs_query_plan;
+int g5_bfs_query_plan_create(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
+                             const uint32_t *h_main_bits, int64_t *d_pred, int32_t *d_depth, void *d_work,
+                             uint64_t work_bytes, const g5_bfs_params *params, g5_bfs_stats *h_stats, void *stream,
+                             g5_bfs_query_plan **plan);
+int g5_bfs_query_plan_run(g5_bfs_query_plan *plan, uint64_t root);
+void g5_bfs_query_plan_destroy(g5_bfs_query_plan *plan);
 
 /* Copies the visited bitmap of the last search on this workspace (bit v set
  * when v was reached; ceil(nverts/32) words).  After a search from a
@@ -287,6 +319,18 @@ int g5_sssp_run(const uint64_t *d_rowstarts, const int32_t *d_col, const float *
  * writes only the reached vertices (O(reached) work); otherwise it writes
  * all nverts entries. */
 int g5_sssp_reset(uint64_t nverts, float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes, void *stream);
+
+/* g5_sssp_reset that undoes only what the last search on this workspace
+ * wrote, for a workspace that has been reset (by either call) and searched
+ * since: after a one-block search (a source outside the main component,
+ * g5_sssp_params.small) it restores the packed distances, stamps and -- when
+ * they are the arrays that search wrote sparsely -- the outputs of the
+ * vertices it reached: O(reached) instead of O(N); after any other search
+ * it is g5_sssp_reset.  Decided on the device (stream-ordered).  Not for a
+ * workspace fresh from the allocator: its first reset must be g5_sssp_reset.
+ * No counterpart in the reference (its clear is always O(N)). */
+int g5_sssp_reset_touched(uint64_t nverts, float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes,
+                          void *stream);
 int g5_sssp_traverse(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, const uint32_t *d_light_deg,
                      float light_delta, uint64_t nverts, uint64_t root, float *d_dist, int64_t *d_pred, void *d_work,
                      uint64_t work_bytes, const g5_sssp_params *params, void *stream);
