@@ -88,6 +88,18 @@ int l2_persist_window(uint64_t want, uint64_t *bytes) {
     return G5_OK;
 }
 
+int persistent_kernel_setup(const void *fn) {
+    // G5_SMEM_CARVEOUT (0-100): the preferred shared-memory share of the
+    // SM's unified L1/shared array for every persistent search kernel.
+    static const int carve = [] {
+        const char *s = getenv("G5_SMEM_CARVEOUT");
+        return s && *s ? atoi(s) : -1;
+    }();
+    if (carve >= 0)
+        G5_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, carve > 100 ? 100 : carve));
+    return G5_OK;
+}
+
 unsigned long long wait_limit_ns() {
     static unsigned long long v = [] {
         const char *s = getenv("G5_WAIT_LIMIT_MS");

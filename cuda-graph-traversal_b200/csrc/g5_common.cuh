@@ -80,6 +80,10 @@ int l2_persist_window(uint64_t want, uint64_t *bytes);
 int scan_u32_to_u64(const unsigned *in, uint64_t n, uint64_t *out, uint64_t *scratch, cudaStream_t st);
 inline uint64_t scan_scratch_words(uint64_t n) { return (n + 4095) / 4096 + 1; }
 
+// Function attributes shared by the persistent (cooperative) search kernels,
+// set before their occupancy is first queried.
+int persistent_kernel_setup(const void *fn);
+
 // Wait limit of the persistent kernels' grid barriers, nanoseconds
 // (G5_WAIT_LIMIT_MS overrides; default 2000 ms).
 unsigned long long wait_limit_ns();

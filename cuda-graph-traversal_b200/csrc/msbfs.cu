@@ -968,6 +968,7 @@ static int ms_max_blocks(int *out) {
     int rc = device_info(&di);
     if (rc) return rc;
     if (!cached[di.device]) {
+        if ((rc = persistent_kernel_setup((const void *)ms_persistent_kernel))) return rc;
         int per_sm = 0;
         G5_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ms_persistent_kernel, MS_THREADS, 0));
         cached[di.device] = std::max(1, per_sm) * di.sms;

@@ -33,6 +33,7 @@
 // Algorithmic bytes per search: 2 m_c * (4 col + 4 w) + n_c * (8 rowstarts
 // + 8 packed dist/parent + 4 dist + 8 parent written out).
 #include <algorithm>
+#include <cstring>
 
 #include "g5_common.cuh"
 #include "g5_frontier.cuh"
@@ -83,6 +84,22 @@ constexpr float SSSP_PULL_RATIO = 1.0f;  // default heavy-phase pull threshold
 constexpr double PULL_WALK = 0.25;       // cost of a pull's bitmap walk, in CSR entries per vertex
 constexpr unsigned long long UNREACHED = ~0ull;
 
+// Which capacity check fired: one bit per site above the DEVERR_* flags
+// (bit 16 + site), so a status message names where a list overflowed.
+enum {
+    SITE_PUSH = 0,        // frontier / heavy-set / expanded-set append
+    SITE_FINE = 1,        // sub-bucket queue append
+    SITE_RING = 2,        // bucket ring queue append
+    SITE_HEAVY_SAME = 3,  // a heavy relaxation landed in the open bucket
+    SITE_FLUSH = 4,       // end-of-phase flush of the staging slices
+    SITE_LIST_F = 5,      // frontier parts overlap
+    SITE_LIST_D = 6,      // expanded-set parts overlap
+    SITE_LIST_S = 7,      // heavy-set parts overlap
+    SITE_PULL = 8,        // pull long-row list append
+    SITE_SMALL = 9,       // one-block search list
+};
+__host__ __device__ constexpr unsigned site_bit(int site) { return 1u << (16 + site); }
+
 // List sizes that every block reads after a grid barrier.  They lead the
 // control block, and each block copies them into shared memory once per
 // barrier (a few warps, one load per word) instead of every warp reading
@@ -131,6 +148,11 @@ struct SsspCtl {
     // counters: edges looked at, skipped as settled, atomicMin issued,
     // distances lowered, ring and frontier pushes
     unsigned long long n_edges, n_settled, n_atomic, n_improved, n_ring, n_front;
+    // First relaxation that broke a bucket invariant (site SITE_HEAVY_SAME):
+    // claimed by dbg_claim, then v, the packed candidate (distance, u), u's
+    // packed value when seen, b_B and b_{B+1} bits, the bucket and phase.
+    unsigned dbg_claim;
+    unsigned long long dbg[7];
     // per-phase trace: end time, kind (0 open, 1 light, 2 heavy push, 3
     // heavy pull), input size, edges looked at so far
     unsigned long long t0;
@@ -348,7 +370,7 @@ __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCt
     if (x.sub_mode)
         ok &= frontier_append_staged(x.st.d, x.Dl, x.DBl, a.n, &c->sn.d_small[x.d_slot], &c->sn.d_big[x.d_slot], d, v,
                                      dl, SSSP_BIG_DEG, SSSP_CHUNK);
-    if (!ok) atomicOr(&c->error, DEVERR_CAPACITY);
+    if (!ok) atomicOr(&c->error, DEVERR_CAPACITY | site_bit(SITE_PUSH));
 }
 
 // Appends v for every lane with `want` to a warp's staging slice of any
@@ -400,7 +422,7 @@ __device__ __forceinline__ void push_fine(const SsspArgs &a, const PushCtx &x, i
         // no queue exceeds n entries.
         WarpStage st{x.st.qbuf + q * STAGE_Q, x.st.qcnt + q, STAGE_Q};
         if (!stage_push(st, mine, v, a.fq + (uint64_t)q * a.n, a.n, &a.ctl->sn.fq_len[q]))
-            atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+            atomicOr(&a.ctl->error, DEVERR_CAPACITY | site_bit(SITE_FINE));
         todo &= ~m;
     }
 }
@@ -478,7 +500,7 @@ __device__ __forceinline__ void run_pushes(const SsspArgs &a, const PushCtx &x, 
         const unsigned m = __ballot_sync(FULL, mine);
         WarpStage q{x.st.rbuf + sl * STAGE_R, x.st.rcnt + sl, STAGE_R};
         if (!stage_push(q, mine, v, a.ring + (uint64_t)sl * a.n, a.n, &a.ctl->sn.ring_len[sl]))
-            atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+            atomicOr(&a.ctl->error, DEVERR_CAPACITY | site_bit(SITE_RING));
         todo &= ~m;
     }
 }
@@ -511,7 +533,19 @@ __device__ __forceinline__ void lower(const SsspArgs &a, const PushCtx &x, Count
             if (np < old && (old >> 32) != (np >> 32)) {
                 ++k.improved;
                 if (cand < x.bnd[1]) {
-                    if (heavy_phase) atomicOr(&a.ctl->error, DEVERR_CAPACITY);  // cannot happen: w >= delta
+                    if (heavy_phase) {  // cannot happen: heavy weights are >= delta
+                        atomicOr(&a.ctl->error, DEVERR_CAPACITY | site_bit(SITE_HEAVY_SAME));
+                        if (atomicCAS(&a.ctl->dbg_claim, 0u, 1u) == 0u) {
+                            unsigned long long *d = a.ctl->dbg;
+                            d[0] = v;
+                            d[1] = np;
+                            d[2] = __ldcg(&a.pack[(unsigned)np]);
+                            d[3] = __float_as_uint(x.bnd[0]);
+                            d[4] = __float_as_uint(x.bnd[1]);
+                            d[5] = x.bucket;
+                            d[6] = x.pid;
+                        }
+                    }
                     else if (cand < x.sub_hi) what = P_SAME;
                     else what = P_FINE | (unsigned)sub_index(x.sub, cand);  // a later sub-bucket of this bucket
                 } else {
@@ -603,7 +637,7 @@ __device__ void stage_flush(const SsspArgs &a, const PushCtx &x, Counts &k) {
             ok &= stage_flush_warp(q, a.fq + (uint64_t)j * a.n, a.n, &c->sn.fq_len[j]);
         }
     }
-    if (!ok && lane_id() == 0) atomicOr(&c->error, DEVERR_CAPACITY);
+    if (!ok && lane_id() == 0) atomicOr(&c->error, DEVERR_CAPACITY | site_bit(SITE_FLUSH));
 }
 
 // Which light edges an expansion relaxes: all, only those whose candidate
@@ -756,9 +790,9 @@ __device__ __forceinline__ bool sssp_sync(const SsspArgs &a, unsigned &epoch, Ss
 // checks the sum all the same (every block reads the same snapshot, so all
 // leave together) and reports an overlap instead of reading a list whose
 // parts may have overwritten each other.
-__device__ __forceinline__ bool list_fits(const SsspArgs &a, unsigned ns, unsigned long long bp) {
+__device__ __forceinline__ bool list_fits(const SsspArgs &a, unsigned ns, unsigned long long bp, int site) {
     if ((uint64_t)ns + big_count(bp) <= a.n) return true;
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&a.ctl->error, DEVERR_CAPACITY);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&a.ctl->error, DEVERR_CAPACITY | site_bit(site));
     return false;
 }
 
@@ -846,7 +880,7 @@ __device__ void pull_words(const SsspArgs &a, const PushCtx &x, Counts &k, unsig
         const uint64_t hdeg = he - hb;
         const bool longrow = hdeg > BIG_DEG;
         if (!frontier_append(LL, LB, a.n, &c->pl_small, &c->sn.pl_big, longrow, (unsigned)v, hdeg))
-            atomicOr(&c->error, DEVERR_CAPACITY);
+            atomicOr(&c->error, DEVERR_CAPACITY | site_bit(SITE_PULL));
         const unsigned deg = longrow ? 0u : (unsigned)hdeg;
         const unsigned incl = warp_incl_scan(deg);
         const unsigned total = __shfl_sync(FULL, incl, 31);
@@ -1106,19 +1140,30 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
             const int s_cur = phase % 3, s_nxt = (phase + 1) % 3, s_clr = (phase + 2) % 3;
             const unsigned ns = sp->f_small[s_cur];
             const unsigned long long bp = sp->f_big[s_cur];
-            if (!list_fits(a, ns, bp)) return;
+            if (!list_fits(a, ns, bp, SITE_LIST_F)) return;
             const unsigned fsize = ns + big_count(bp);
             int nj = -1;
             if (fsize == 0) {
                 if (!x.sub_mode) break;
-                const unsigned dn = sp->d_small[x.d_slot];
-                const unsigned long long dbp = sp->d_big[x.d_slot];
-                if (!list_fits(a, dn, dbp)) return;
-                if (!just_settled && dn + big_count(dbp) > 0) {
+                // Every block must take the same branch here, so it may
+                // depend only on counters that no block can change during
+                // this phase.  The expanded set's count is not one of them:
+                // blocks that pass the barrier first and open the next
+                // sub-bucket append to the set while slower blocks are still
+                // copying the snapshot.  So an open sub-bucket whose frontier
+                // has drained always gets its settle pass, even with an
+                // empty expanded set (a sub-bucket whose queue entries were
+                // all stale).
+                if (!just_settled && sj >= 0) {
                     // Settle pass of sub-bucket sj: every distance in it is
                     // final; its expanded set relaxes the deferred edges.
-                    // The other counter slot is cleared for the next set
-                    // (appends to it start after this phase's barrier).
+                    // Nothing appends to the set in this phase, so its
+                    // snapshot count is exact.  The other counter slot is
+                    // cleared for the next set (appends to it start after
+                    // this phase's barrier).
+                    const unsigned dn = sp->d_small[x.d_slot];
+                    const unsigned long long dbp = sp->d_big[x.d_slot];
+                    if (!list_fits(a, dn, dbp, SITE_LIST_D)) return;
                     if (gtid == 0) {
                         c->grab[s_clr] = c->cgrab[s_clr] = c->sn.f_small[s_clr] = 0;
                         c->sn.f_big[s_clr] = c->sn.f_entries[s_clr] = 0;
@@ -1230,7 +1275,7 @@ __global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspAr
             x.FBout = a.FB[(phase + 1) & 1];
             const unsigned ns = sp->s_small[sb];
             const unsigned long long bp = sp->s_big[sb];
-            if (!list_fits(a, ns, bp)) return;
+            if (!list_fits(a, ns, bp, SITE_LIST_S)) return;
             const unsigned long long s_ent = sp->s_entries[sb];
             // Every block reads the same counters after the barrier, so all
             // take the same branch.
@@ -1409,14 +1454,14 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
                     } else if (pos < a.n) {
                         a.F[nxt][pos] = v;
                     } else {
-                        atomicOr(&s_err, DEVERR_CAPACITY);
+                        atomicOr(&s_err, DEVERR_CAPACITY | site_bit(SITE_SMALL));
                     }
                 }
                 if (sold != 0u) {
                     const unsigned pos = atomicAdd(&s_nreach, 1u);
                     if (pos < SMALL_L) s_r[pos] = v;
                     if (pos < a.n) R[pos] = v;
-                    else atomicOr(&s_err, DEVERR_CAPACITY);
+                    else atomicOr(&s_err, DEVERR_CAPACITY | site_bit(SITE_SMALL));
                 }
             }
         }
@@ -1502,6 +1547,7 @@ static int sssp_max_blocks(int *out) {
     int rc = device_info(&di);
     if (rc) return rc;
     if (!cached[di.device]) {
+        if ((rc = persistent_kernel_setup((const void *)sssp_persistent_kernel))) return rc;
         int per_sm = 0;
         G5_CUDA_TRY(
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_persistent_kernel, SSSP_THREADS, 0));
@@ -1764,7 +1810,23 @@ extern "C" int g5_sssp_last_status(const void *d_work, uint64_t work_bytes, uint
     G5_CUDA_TRY(cudaStreamSynchronize(st));
     if (buckets) *buckets = c.buckets;
     if (phases) *phases = c.phases;
-    return deverr_to_status(c.error, "g5_sssp_run");
+    int rc = deverr_to_status(c.error, "g5_sssp_run");
+    if (rc && c.dbg_claim) {
+        auto f = [](unsigned long long b) {
+            float x;
+            unsigned u = (unsigned)b;
+            memcpy(&x, &u, 4);
+            return (double)x;
+        };
+        char extra[320];
+        snprintf(extra, sizeof extra,
+                 "%s; first bad relaxation: v %llu, candidate %.9g from u %llu (u now at %.9g), bucket %llu "
+                 "[%.9g, %.9g), phase %llu",
+                 g5_last_error(), c.dbg[0], f(c.dbg[1] >> 32), c.dbg[1] & 0xffffffffull, f(c.dbg[2] >> 32), c.dbg[5],
+                 f(c.dbg[3]), f(c.dbg[4]), c.dbg[6]);
+        set_error(rc, "%s", extra);
+    }
+    return rc;
 }
 
 extern "C" int g5_sssp_grid(uint64_t nverts, int32_t *blocks, int32_t *max_blocks) {

@@ -294,31 +294,36 @@ class GraphServer:
             return True
         return False
 
-    def _checked(self, status, resource, stream) -> bool:
+    def _checked(self, status, resource, stream, launch=None) -> bool:
         """Reads a finished launch's status.  A device error raises, or with
         raise_errors=False is counted (the launch's queries are answered with
-        ok=False) and the server goes on: the next reset clears the state."""
+        ok=False) and the server goes on: the next reset clears the state.
+        The message names the launch and what else was running."""
         try:
             status(resource, stream)
             return True
         except G5Error as ex:
+            msg = str(ex)
+            if launch is not None:
+                others = [(x.kind, x.graph, x.blocks) for x in self.inflight if x is not launch]
+                msg += f" [{launch.kind} graph {launch.graph} blocks {launch.blocks}; also running {others}]"
             if self.raise_errors:
-                raise
+                raise type(ex)(msg) from ex
             self.stats.device_errors += 1
             if len(self.stats.errors) < 8:
-                self.stats.errors.append(str(ex))
+                self.stats.errors.append(msg)
             return False
 
     def _complete(self, L: _Launch, t: float) -> list[Result]:
         out = []
         if L.kind == "bfs1":
-            ok = self._checked(bfs_stats, L.resource, self.streams[L.slot])
+            ok = self._checked(bfs_stats, L.resource, self.streams[L.slot], L)
             q = L.queries[0]
             v = L.resource.depth.clone() if self.keep and ok else None
             out.append(Result(q.qid, "bfs", q.graph, q.root, q.arrival, t, 1, v, ok))
             self.bfs_free[L.graph].append(L.resource)
         elif L.kind == "bfs":
-            ok = self._checked(msbfs_stats, L.resource, self.streams[L.slot])
+            ok = self._checked(msbfs_stats, L.resource, self.streams[L.slot], L)
             for i, q in enumerate(L.queries):
                 v = None
                 if self.keep and ok:
@@ -327,7 +332,7 @@ class GraphServer:
                 out.append(Result(q.qid, q.kind, q.graph, q.root, q.arrival, t, len(L.queries), v, ok))
             self.ms_busy[L.graph] = False
         else:
-            ok = self._checked(sssp_status, L.resource, self.streams[L.slot])
+            ok = self._checked(sssp_status, L.resource, self.streams[L.slot], L)
             q = L.queries[0]
             v = L.resource.dist.clone() if self.keep and ok else None
             out.append(Result(q.qid, q.kind, q.graph, q.root, q.arrival, t, 1, v, ok))

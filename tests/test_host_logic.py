@@ -90,3 +90,14 @@ def test_server_status_errors_counted_or_raised(cgt):
         pass
     srv.raise_errors = False
     assert not srv._checked(bad, None, None) and srv.stats.device_errors == 1 and len(srv.stats.errors) == 1
+
+    # The library's device errors are G5Error subclasses (and their builtin kinds).
+    def timeout(resource, stream):
+        raise cgt._ERRORS[-4]("libg500b error -4: a bounded grid barrier wait expired")
+
+    def device(resource, stream):
+        raise cgt._ERRORS[-5]("libg500b error -5: internal capacity exceeded")
+
+    assert issubclass(cgt._ERRORS[-4], TimeoutError) and issubclass(cgt._ERRORS[-1], ValueError)
+    assert not srv._checked(timeout, None, None) and not srv._checked(device, None, None)
+    assert srv.stats.device_errors == 3
