@@ -428,7 +428,8 @@ def run_ours(args):
                                         args.edgefactor)
             torch.cuda.empty_cache()
         if world == 1 and not args.no_serve:
-            line["serving"] = run_serving(G, dev, args.serve_queries, args.serve_rate, args.edgefactor, args.serve_slots)
+            line["serving"] = run_serving(G, dev, args.serve_queries, args.serve_rate, args.edgefactor, args.serve_slots,
+                                          args.serve_low_rate, not args.serve_count_errors)
         line["headline"] = headline(line)
         print(json.dumps(line), flush=True)
     if pg:
@@ -592,7 +593,7 @@ def run_packed(G, dev, ngraphs, smin, smax, ef, reps=3):
 SERVE_SCALES = (16, 18, 20, 22, 22, 23, 24, 24)
 
 
-def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0):
+def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0, raise_errors=True):
     """Serving: 8 resident Kronecker graphs (SCALE 16, 18, 20, 22, 22, 23, 24,
     24; seeds (2+i, 3)), a Poisson stream of queries (70% BFS, 30% SSSP,
     uniform graph, uniform non-zero-degree root, seed 1) replayed in real
@@ -608,7 +609,7 @@ def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0):
     build_s = time.time() - t0
     trace = S.poisson_trace(graphs, nqueries, rate, bfs_share=0.7, seed=1)
     warm = S.poisson_trace(graphs, 64, rate, bfs_share=0.5, seed=99)
-    srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots)
+    srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots, raise_errors=raise_errors)
     srv.prewarm()  # workspaces created up front (admission by free HBM)
     srv.run_trace(warm, deadline=600)  # batched copies prepared, kernels loaded
     srv.stats = S.ServerStats()
@@ -620,7 +621,7 @@ def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0):
     low = None
     if low_rate:
         ltrace = S.poisson_trace(graphs, nqueries, low_rate, bfs_share=0.7, seed=2)
-        srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots)
+        srv = S.GraphServer(graphs, slots=slots, hbm_reserve=16 << 30, max_sssp_per_graph=slots, raise_errors=raise_errors)
         srv.prewarm()
         srv.run_trace(warm, deadline=600)
         srv.stats = S.ServerStats()
@@ -658,7 +659,8 @@ def run_batched_only(args):
         out["packed"] = run_packed(G, dev, args.packed_graphs, args.packed_min_scale, args.packed_max_scale,
                                    args.edgefactor)
     if args.only_batched in ("serve", "all"):
-        out["serving"] = run_serving(G, dev, args.serve_queries, args.serve_rate, args.edgefactor, args.serve_slots)
+        out["serving"] = run_serving(G, dev, args.serve_queries, args.serve_rate, args.edgefactor, args.serve_slots,
+                                     args.serve_low_rate, not args.serve_count_errors)
     print(json.dumps(out), flush=True)
 
 
@@ -850,6 +852,10 @@ def main():
     ap.add_argument("--serve-queries", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate, queries per second")
     ap.add_argument("--serve-slots", type=int, default=8, help="concurrent launches (streams) of the server")
+    ap.add_argument("--serve-count-errors", action="store_true",
+                    help="serving: count launches that report a device error instead of raising")
+    ap.add_argument("--serve-low-rate", type=float, default=250.0,
+                    help="rate of the second, below-capacity serving trace (0 = skip it)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     ap.add_argument("--packed-graphs", type=int, default=2000)
     ap.add_argument("--packed-min-scale", type=int, default=10)

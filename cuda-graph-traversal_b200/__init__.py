@@ -27,11 +27,32 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libg500b.so")
 
 G5_OK = 0
-_ERRORS = {-1: ValueError, -2: MemoryError, -3: RuntimeError, -4: TimeoutError, -5: RuntimeError}
-
-
 class G5Error(RuntimeError):
+    """Any error the library returned (also raised as the matching builtin
+    kind below)."""
+
+
+class G5InvalidError(G5Error, ValueError):
     pass
+
+
+class G5WorkspaceError(G5Error, MemoryError):
+    pass
+
+
+class G5CudaError(G5Error):
+    pass
+
+
+class G5TimeoutError(G5Error, TimeoutError):
+    pass
+
+
+class G5DeviceError(G5Error):
+    pass
+
+
+_ERRORS = {-1: G5InvalidError, -2: G5WorkspaceError, -3: G5CudaError, -4: G5TimeoutError, -5: G5DeviceError}
 
 
 def _load() -> C.CDLL:
@@ -54,6 +75,12 @@ def _load() -> C.CDLL:
         "g5_csr_fill_kronecker": ([p, u32, u64, p, f32, p, u64, p, p, p, p, p], C.c_int),
         "g5_csr_pack_append": ([p, p, p, p, u64, u64, u64, u64, p, p, p, p, p], C.c_int),
         "g5_csr_split_tiny": ([p, p, p, p, p, u64, f32, p, p], C.c_int),
+        "g5_csr_sorted_workspace_size": ([u64, u64, p], C.c_int),
+        "g5_csr_fill_sorted": ([p, p, u64, u64, p, u64, p, u64, p, p, p, p], C.c_int),
+        "g5_csr_sort_rows": ([p, u64, u64, p, p, p, p, u64, p], C.c_int),
+        "g5_csr_dedupe_count": ([p, p, u64, u64, p, p, u64, p, p], C.c_int),
+        "g5_csr_dedupe_copy": ([p, p, p, u64, p, p, p, p, p], C.c_int),
+        "g5_csr_split_light": ([p, p, p, u64, u64, f32, p, p, p, p, p, u64, p], C.c_int),
         "g5_bfs_traverse_multi": ([p, p, u64, p, u32, p, p, p, u64, p, p], C.c_int),
         "g5_sssp_traverse_multi": ([p, p, p, p, f32, u64, p, u32, p, p, p, u64, p, p], C.c_int),
         "g5_bfs_workspace_size": ([u64, p], C.c_int),
@@ -239,7 +266,20 @@ class OnedGraph:
     column: torch.Tensor | None = None
     isolated: torch.Tensor | None = None  # int32[ceil(N/32)] bitmap of degree-0 vertices
     main_bits: np.ndarray | None = None   # host uint32 bitmap of the largest component
-    tiny_deg: torch.Tensor | None = None  # int32[N] leading tiny entries of each light part (g5_csr_split_tiny)
+    tiny_deg: torch.Tensor | None = None  # int32[N] leading tiny entries of each light part
+    # The SSSP copy (g5_csr_split_light): rows partitioned tiny | light |
+    # heavy, light_deg / tiny_deg their first parts' sizes.  None: col / w
+    # are in that layout themselves (packed graphs).
+    scol: torch.Tensor | None = None
+    sw: torch.Tensor | None = None
+
+    @property
+    def sssp_col(self) -> torch.Tensor:
+        return self.col if self.scol is None else self.scol
+
+    @property
+    def sssp_w(self) -> torch.Tensor:
+        return self.w if self.sw is None else self.sw
 
     def in_main_component(self, v: int) -> bool:
         """True when v is in the largest component (or unknown / out of
@@ -257,36 +297,77 @@ class OnedGraph:
         return self.rowstarts.device
 
 
+def _sorted_work(n: int, e: int, dev) -> torch.Tensor:
+    nb = C.c_uint64()
+    _check(lib.g5_csr_sorted_workspace_size(n, e, C.byref(nb)))
+    return _workspace(nb.value, dev)
+
+
+def _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, dev, stream,
+                  with_main) -> OnedGraph:
+    """Canonical rows (already sorted) -> optional dedupe -> the SSSP copy
+    (g5_csr_split_light) -> isolated bitmap and main component."""
+    if dedupe:
+        rs2 = torch.empty(n + 1, dtype=torch.int64, device=dev)
+        e2 = C.c_uint64()
+        _check(lib.g5_csr_dedupe_count(_ptr(rowstarts), _ptr(col), n, e, _ptr(rs2), _ptr(work), work.numel(),
+                                       C.byref(e2), st))
+        e2 = e2.value
+        col2 = torch.empty(max(e2, 1), dtype=torch.int32, device=dev)
+        w2 = torch.empty(max(e2, 1), dtype=torch.float32, device=dev)
+        c64 = torch.empty(max(e2, 1), dtype=torch.int64, device=dev) if col64 is not None else None
+        if e:
+            _check(lib.g5_csr_dedupe_copy(_ptr(rowstarts), _ptr(col), _ptr(w), n, _ptr(rs2), _ptr(col2), _ptr(w2),
+                                          _ptr(c64), st))
+        else:
+            rs2.zero_()
+        rowstarts, col, w, col64, e = rs2, col2, w2, c64, e2
+    scol = torch.empty(max(e, 1), dtype=torch.int32, device=dev)
+    sw = torch.empty(max(e, 1), dtype=torch.float32, device=dev)
+    light = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    tiny = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    _check(lib.g5_csr_split_light(_ptr(rowstarts), _ptr(col), _ptr(w), n, e, light_delta, _ptr(scol), _ptr(sw),
+                                  _ptr(light), _ptr(tiny), _ptr(work), work.numel(), st))
+    iso = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
+    _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), n, _ptr(iso), st))
+    g = OnedGraph(n, e, rowstarts, col[:e], w[:e], light[:n], light_delta, None if col64 is None else col64[:e], iso)
+    g.tiny_deg = tiny[:n]
+    g.scol, g.sw = scol[:e], sw[:e]
+    if with_main:
+        g.main_bits = main_component_bitmap(g, stream)
+    return g
+
+
 def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: float = 0.1,
-                                with_column64: bool = False, stream=None, with_main: bool = True) -> OnedGraph:
-    """oned_graph_from_tuple_graph (src/traversal.h:43).  with_main=False
-    skips the main-component search (g.main_bits = None; set it later with
-    main_component_bitmap)."""
+                                with_column64: bool = False, stream=None, with_main: bool = True,
+                                dedupe: bool = False) -> OnedGraph:
+    """oned_graph_from_tuple_graph (src/traversal.h:43): the CSR of both
+    directions of every non-loop edge, duplicates kept, every row in
+    canonical order (sorted by neighbour, then weight bits:
+    g5_csr_fill_sorted), plus the SSSP copy with light-first rows
+    (g.scol / g.sw, g5_csr_split_light).  dedupe=True keeps one entry per
+    (row, neighbour), the lightest (not the reference's CSR: its TEPS edge
+    counts include duplicates).  with_main=False skips the main-component
+    search (g.main_bits = None; set it later with main_component_bitmap)."""
     dev = tg.edges.device
     n, m = int(nglobalverts), tg.edges_size
     nb = C.c_uint64()
     _check(lib.g5_csr_workspace_size(n, m, C.byref(nb)))
-    work = _workspace(nb.value, dev)
+    cwork = _workspace(nb.value, dev)
     rowstarts = torch.empty(n + 1, dtype=torch.int64, device=dev)
     nent = C.c_uint64()
     st = _stream(stream)
-    _check(lib.g5_csr_count(_ptr(tg.edges), m, n, _ptr(rowstarts), _ptr(work), work.numel(),
+    _check(lib.g5_csr_count(_ptr(tg.edges), m, n, _ptr(rowstarts), _ptr(cwork), cwork.numel(),
                             C.byref(nent), st))
+    del cwork
     e = nent.value
     col = torch.empty(max(e, 1), dtype=torch.int32, device=dev)
     w = torch.empty(max(e, 1), dtype=torch.float32, device=dev)
-    light = torch.empty(n, dtype=torch.int32, device=dev)
     col64 = torch.empty(max(e, 1), dtype=torch.int64, device=dev) if with_column64 else None
-    _check(lib.g5_csr_fill(_ptr(tg.edges), _ptr(tg.weights), m, n, _ptr(rowstarts), light_delta,
-                           _ptr(work), work.numel(), _ptr(col), _ptr(w), _ptr(col64), _ptr(light), st))
-    tiny = _split_tiny(rowstarts, col, w, col64, light, n, light_delta, st)
-    iso = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
-    _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), n, _ptr(iso), st))
-    g = OnedGraph(n, e, rowstarts, col[:e], w[:e], light, light_delta, None if col64 is None else col64[:e], iso)
-    g.tiny_deg = tiny
-    if with_main:
-        g.main_bits = main_component_bitmap(g, stream)
-    return g
+    work = _sorted_work(n, e, dev)
+    _check(lib.g5_csr_fill_sorted(_ptr(tg.edges), _ptr(tg.weights), m, n, _ptr(rowstarts), e, _ptr(work),
+                                  work.numel(), _ptr(col), _ptr(w), _ptr(col64), st))
+    return _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, dev, stream, with_main)
 
 
 def _split_tiny(rowstarts, col, w, col64, light, n: int, light_delta: float, st) -> torch.Tensor:
@@ -298,34 +379,36 @@ def _split_tiny(rowstarts, col, w, col64, light, n: int, light_delta: float, st)
 
 
 def oned_graph_from_kronecker(seed, log_n: int, nedges: int, device="cuda", light_delta: float = 0.1,
-                              with_column64: bool = False, stream=None, with_main: bool = True) -> OnedGraph:
+                              with_column64: bool = False, stream=None, with_main: bool = True,
+                              dedupe: bool = False) -> OnedGraph:
     """generate_kronecker_range + oned_graph_from_tuple_graph in one step,
-    with the generator fused into the CSR passes (no edge list in memory).
-    with_main=False skips the main-component search (g.main_bits = None)."""
+    with the generator fused into the CSR passes (no edge list in memory);
+    rows then sorted into canonical order (g5_csr_sort_rows) -- the same
+    graph as the two-step build.  with_main=False skips the main-component
+    search (g.main_bits = None)."""
     n = 1 << log_n
     s = (C.c_uint32 * 5)(*seed)
     nb = C.c_uint64()
     _check(lib.g5_csr_workspace_size(n, nedges, C.byref(nb)))
-    work = _workspace(nb.value, device)
+    cwork = _workspace(nb.value, device)
     rowstarts = torch.empty(n + 1, dtype=torch.int64, device=device)
     nent = C.c_uint64()
     st = _stream(stream)
-    _check(lib.g5_csr_count_kronecker(s, log_n, nedges, _ptr(rowstarts), _ptr(work), work.numel(), C.byref(nent), st))
+    _check(lib.g5_csr_count_kronecker(s, log_n, nedges, _ptr(rowstarts), _ptr(cwork), cwork.numel(), C.byref(nent),
+                                      st))
     e = nent.value
     col = torch.empty(max(e, 1), dtype=torch.int32, device=device)
     w = torch.empty(max(e, 1), dtype=torch.float32, device=device)
     light = torch.empty(n, dtype=torch.int32, device=device)
     col64 = torch.empty(max(e, 1), dtype=torch.int64, device=device) if with_column64 else None
-    _check(lib.g5_csr_fill_kronecker(s, log_n, nedges, _ptr(rowstarts), light_delta, _ptr(work), work.numel(),
-                                     _ptr(col), _ptr(w), _ptr(col64), _ptr(light), st))
-    tiny = _split_tiny(rowstarts, col, w, col64, light, n, light_delta, st)
-    iso = torch.empty((n + 31) // 32, dtype=torch.int32, device=device)
-    _check(lib.g5_graph_isolated_bitmap(_ptr(rowstarts), n, _ptr(iso), st))
-    g = OnedGraph(n, e, rowstarts, col[:e], w[:e], light, light_delta, None if col64 is None else col64[:e], iso)
-    g.tiny_deg = tiny
-    if with_main:
-        g.main_bits = main_component_bitmap(g, stream)
-    return g
+    # every entry "light" (from the row start): the rows are sorted next
+    _check(lib.g5_csr_fill_kronecker(s, log_n, nedges, _ptr(rowstarts), float("inf"), _ptr(cwork), cwork.numel(),
+                                     _ptr(col), _ptr(w), None, _ptr(light), st))
+    del cwork, light
+    work = _sorted_work(n, e, device)
+    _check(lib.g5_csr_sort_rows(_ptr(rowstarts), n, e, _ptr(col), _ptr(w), _ptr(col64), _ptr(work), work.numel(),
+                                st))
+    return _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, device, stream, with_main)
 
 
 # ------------------------------------------------------- packed graphs ----
@@ -397,7 +480,8 @@ def _pack(sizes, graphs, roots, device, light_delta, stream) -> PackedGraphs:
     vb, eb = 0, 0
     nverts, vbase = [], []
     for g in graphs:
-        _check(lib.g5_csr_pack_append(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.nglobalverts,
+        _check(lib.g5_csr_pack_append(_ptr(g.rowstarts), _ptr(g.sssp_col), _ptr(g.sssp_w), _ptr(g.light_deg),
+                                      g.nglobalverts,
                                       g.nlocaledges, vb, eb, _ptr(rowstarts), _ptr(col), _ptr(w), _ptr(light), st))
         nverts.append(g.nglobalverts)
         vbase.append(vb)
@@ -430,7 +514,8 @@ def oned_graph_sssp_traverse_multi(g: OnedGraph, sssp: "SsspState", d_roots: tor
     """SSSP from every source in d_roots at once (g5_sssp_traverse_multi);
     reset sssp first."""
     p = SsspParams(delta, blocks, pull, sub_min, 0, _ptr(g.tiny_deg))
-    _check(lib.g5_sssp_traverse_multi(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
+    _check(lib.g5_sssp_traverse_multi(_ptr(g.rowstarts), _ptr(g.sssp_col), _ptr(g.sssp_w), _ptr(g.light_deg),
+                                      g.light_delta,
                                       g.nglobalverts, _ptr(d_roots), d_roots.numel(), _ptr(sssp.dist),
                                       _ptr(sssp.pred), _ptr(sssp.work), sssp.work.numel(), C.byref(p),
                                       _stream(stream)))
@@ -828,7 +913,7 @@ def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float =
     check_opens: the bucket and sub-bucket opens exchange their stamps and
     fail the search if a queue held a vertex twice (a test aid)."""
     p = _sssp_params(g, root, delta, blocks, pull, sub_min, small, check_opens)
-    _check(lib.g5_sssp_run(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
+    _check(lib.g5_sssp_run(_ptr(g.rowstarts), _ptr(g.sssp_col), _ptr(g.sssp_w), _ptr(g.light_deg), g.light_delta,
                            g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                            sssp.work.numel(), C.byref(p), _stream(stream)))
     sssp.was_reset = True  # g5_sssp_run resets in full first
@@ -853,7 +938,8 @@ def oned_graph_sssp_traverse(g: OnedGraph, sssp: SsspState, root: int, delta: fl
     """The search itself, on a reset state (the lean one-block search for a
     root outside the main component)."""
     p = _sssp_params(g, root, delta, blocks, pull, sub_min, small, check_opens)
-    _check(lib.g5_sssp_traverse(_ptr(g.rowstarts), _ptr(g.col), _ptr(g.w), _ptr(g.light_deg), g.light_delta,
+    _check(lib.g5_sssp_traverse(_ptr(g.rowstarts), _ptr(g.sssp_col), _ptr(g.sssp_w), _ptr(g.light_deg),
+                                g.light_delta,
                                 g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                                 sssp.work.numel(), C.byref(p), _stream(stream)))
 

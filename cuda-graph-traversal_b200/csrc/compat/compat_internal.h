@@ -14,9 +14,11 @@
 namespace g5compat {
 
 struct GraphExt {
-    int32_t *col;        // int32 neighbour ids, light-first rows
+    int32_t *col;        // int32 neighbour ids, rows in canonical order (as Oned_Graph.column)
+    int32_t *scol;       // the SSSP copy (g5_csr_split_light): tiny | light | heavy rows
+    float *sw;           // its weights
     uint32_t *light_deg; // light entries per row
-    uint32_t *tiny_deg;  // leading tiny entries of each light part (g5_csr_split_tiny)
+    uint32_t *tiny_deg;  // leading tiny entries of each light part
     uint32_t *isolated;  // bitmap of degree-0 vertices
     uint32_t *main_host; // host bitmap of the largest component (set by the first BFS state)
     float light_delta;

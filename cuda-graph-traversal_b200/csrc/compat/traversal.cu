@@ -21,28 +21,41 @@ Oned_Graph oned_graph_from_tuple_graph(Worker_State *ws, Tuple_Graph *tg, u64 ng
     g.rowstarts = worker_arena_push_array(ws, g.nlocalverts + 1, u64, &count);
     uint64_t wbytes = 0;
     check(ws, g5_csr_workspace_size(nglobalverts, tg->edges_size, &wbytes), "oned_graph_from_tuple_graph");
+    const Arena before_count = ws->gpu_arena;
     void *work = gpu_push(ws, wbytes, "CSR workspace");
     check(ws,
           g5_csr_count((const uint64_t *)tg->edges, tg->edges_size, nglobalverts, g.rowstarts, work, wbytes,
                        &g.nlocaledges, 0),
           "oned_graph_from_tuple_graph");
+    ws->gpu_arena = before_count;  // the count's scratch is free again (nothing else was pushed since)
     g.column = worker_arena_push_array(ws, g.nlocaledges, u64, &count);
     g.weights = worker_arena_push_array(ws, g.nlocaledges, f32, &count);
     GraphExt x;
-    x.col = (int32_t *)gpu_push(ws, g.nlocaledges * sizeof(int32_t), "int32 column");
+    const uint64_t e = g.nlocaledges;
+    x.col = (int32_t *)gpu_push(ws, e * sizeof(int32_t), "int32 column");
+    x.scol = (int32_t *)gpu_push(ws, e * sizeof(int32_t), "SSSP column");
+    x.sw = (float *)gpu_push(ws, e * sizeof(float), "SSSP weights");
     x.light_deg = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "light degrees");
     x.tiny_deg = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "tiny degrees");
     x.light_delta = kLightDelta;
     x.main_host = nullptr;
     x.isolated = (uint32_t *)gpu_push(ws, (nglobalverts + 31) / 32 * sizeof(uint32_t), "isolated-vertex bitmap");
+    // Rows in canonical order (sorted by neighbour, then weight), and the
+    // SSSP copy; the sorting scratch is the arena's last push, popped after.
+    uint64_t sbytes = 0;
+    check(ws, g5_csr_sorted_workspace_size(nglobalverts, e, &sbytes), "oned_graph_from_tuple_graph");
+    const Arena before_sort = ws->gpu_arena;
+    void *swork = gpu_push(ws, sbytes, "CSR sorting scratch");
     check(ws,
-          g5_csr_fill((const uint64_t *)tg->edges, tg->weights, tg->edges_size, nglobalverts, g.rowstarts,
-                      kLightDelta, work, wbytes, x.col, g.weights, g.column, x.light_deg, 0),
+          g5_csr_fill_sorted((const uint64_t *)tg->edges, tg->weights, tg->edges_size, nglobalverts, g.rowstarts, e,
+                             swork, sbytes, x.col, g.weights, g.column, 0),
           "oned_graph_from_tuple_graph");
     check(ws,
-          g5_csr_split_tiny(g.rowstarts, x.col, g.weights, g.column, x.light_deg, nglobalverts, kLightDelta,
-                            x.tiny_deg, 0),
+          g5_csr_split_light(g.rowstarts, x.col, g.weights, nglobalverts, e, kLightDelta, x.scol, x.sw, x.light_deg,
+                             x.tiny_deg, swork, sbytes, 0),
           "oned_graph_from_tuple_graph");
+    CHECK_CUDA(cudaDeviceSynchronize());
+    ws->gpu_arena = before_sort;
     check(ws, g5_graph_isolated_bitmap(g.rowstarts, nglobalverts, x.isolated, 0), "oned_graph_from_tuple_graph");
     CHECK_CUDA(cudaDeviceSynchronize());
     put_graph(g.rowstarts, x);
@@ -217,7 +230,7 @@ void oned_graph_sssp_run(Worker_State *ws, const Oned_Graph *g, Sssp_State *sssp
     // state) runs on one block: its search touches a handful of vertices.
     const bool small = gx->main_host && !((gx->main_host[root >> 5] >> (root & 31)) & 1u);
     g5_sssp_params p = {kLightDelta, small ? 1 : 0, 0.0f, 0, small ? 1 : 0, gx->tiny_deg, 0};
-    check(ws, g5_sssp_traverse(g->rowstarts, gx->col, g->weights, gx->light_deg, gx->light_delta, g->nglobalverts,
+    check(ws, g5_sssp_traverse(g->rowstarts, gx->scol, gx->sw, gx->light_deg, gx->light_delta, g->nglobalverts,
                                root, sssp->dist, sssp->pred, sx->work, sx->work_bytes, &p, 0),
           "oned_graph_sssp_run");
     check(ws, g5_sssp_last_status(sx->work, sx->work_bytes, nullptr, nullptr, 0), "oned_graph_sssp_run");

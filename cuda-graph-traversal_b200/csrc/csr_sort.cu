@@ -1,0 +1,737 @@
+// csr_sort.cu -- K2 canonical: the CSR with every row sorted by (neighbour,
+// weight bits), built by radix partitioning instead of one scattered atomic
+// fill (the reference's fill_csr_kernel, src/traversal.cu:48-73, leaves rows
+// in atomic order).  Duplicates and their weights are kept unless the
+// caller dedupes; self-loops are dropped as in the reference (:20-21).
+//
+//   partition  each block stages a tile of directed entries (u -> v and
+//              v -> u of every edge) in shared memory by source partition
+//              (the top 8 bits of the source's index range: 256
+//              partitions) and writes each partition's run with one cursor
+//              reservation, into a scratch array laid out like the CSR (a
+//              partition's entries go exactly where its rows will be).
+//   place      one partition at a time across the whole GPU: entries go to
+//              their rows with per-row atomic cursors.  A partition's rows
+//              span E/256 CSR entries (67 MB of column and weight at SCALE
+//              26), so its scattered stores and cursors stay in L2 and reach
+//              DRAM as whole lines.
+//   sort       rows sorted by the 64-bit key (neighbour << 32 | weight
+//              bits): up to 32 entries by a warp in registers (bitonic),
+//              up to 4096 by a block in shared memory (bitonic), longer rows
+//              by a block as sorted 4096-entry chunks merged pairwise (merge
+//              path), ping-ponging with the scratch array.
+//   dedupe     (optional) keeps the first entry of each run of equal
+//              neighbours -- the lightest, rows being sorted -- into new
+//              arrays with new row starts.
+//   split      the SSSP copy of the CSR: each row stably partitioned into
+//              entries below light/G5_TINY_DIV, the other light ones (below
+//              light), and the heavy ones, with per-row counts.
+//
+// Algorithmic bytes per edge (two entries): partition reads 20 and writes
+// 24, place reads 24 and writes 16 (+16 with the u64 column), sort reads and
+// writes 16 per pass over the rows (one pass for rows up to 4096 entries).
+#include <algorithm>
+
+#include "g5_common.cuh"
+
+namespace g5 {
+
+constexpr int PART_BITS = 8;
+constexpr int NPART = 1 << PART_BITS;
+constexpr int P1_THREADS = 512;
+constexpr int P1_EDGES = 4096;  // edges per tile: 8192 staged entries (96 KB of dynamic shared memory)
+constexpr size_t P1_SMEM = (size_t)2 * P1_EDGES * (sizeof(unsigned long long) + sizeof(float));
+constexpr int P1_PER_THREAD = P1_EDGES / P1_THREADS;
+constexpr int SORT_THREADS = 256;
+constexpr unsigned SORT_SMEM_KEYS = 4096;  // rows up to this length sort in shared memory
+constexpr int MERGE_ITEMS = 8;             // outputs per thread per merge step
+
+__host__ __device__ __forceinline__ int part_shift(uint64_t n) {
+    int lg = 0;
+    while ((1ull << lg) < n) ++lg;
+    return lg > PART_BITS ? lg - PART_BITS : 0;
+}
+
+// Scratch: keys (u64) and weights of the partitioned entries, row cursors,
+// partition cursors, the row lists by size class, error flags.
+struct SortWork {
+    unsigned long long *tkey;  // E: partitioned entries (src << 32 | dst), then sort ping-pong buffer
+    float *tw;                 // E: their weights
+    unsigned *rcur;            // N: per-row cursors (place), then dedupe degrees
+    unsigned long long *pcur;  // NPART: partition cursors
+    unsigned *mid, *big;       // N each: rows of 33..4096 and of more than 4096 entries
+    unsigned *cnt;             // [0] mid rows, [1] big rows, [2] errors
+    uint64_t *scan;            // scan scratch
+    uint64_t bytes;
+};
+
+static SortWork carve_sort(void *base, uint64_t n, uint64_t e) {
+    Carver c(base);
+    SortWork w;
+    w.tkey = c.take<unsigned long long>(e ? e : 1);
+    w.tw = c.take<float>(e ? e : 1);
+    w.rcur = c.take<unsigned>(n + 1);
+    w.pcur = c.take<unsigned long long>(NPART + 1);
+    w.mid = c.take<unsigned>(n);
+    w.big = c.take<unsigned>(n);
+    w.cnt = c.take<unsigned>(64);
+    w.scan = c.take<uint64_t>(scan_scratch_words(n));
+    w.bytes = c.used;
+    return w;
+}
+
+enum : unsigned { SORTERR_RANGE = 1u, SORTERR_COUNT = 2u };
+
+// ---------------------------------------------------------------- partition
+
+__global__ void csr_part_init_kernel(const uint64_t *__restrict__ rowstarts, uint64_t n, int pshift,
+                                     unsigned long long *__restrict__ pcur) {
+    const unsigned p = threadIdx.x;
+    if (p <= NPART) {
+        const uint64_t v = min((uint64_t)p << pshift, n);
+        pcur[p] = rowstarts[v];
+    }
+}
+
+__global__ void __launch_bounds__(P1_THREADS) csr_partition_kernel(const ulonglong2 *__restrict__ edges,
+                                                                   const float *__restrict__ weights, uint64_t m,
+                                                                   uint64_t n, int pshift,
+                                                                   const uint64_t *__restrict__ rowstarts,
+                                                                   unsigned long long *__restrict__ pcur,
+                                                                   unsigned long long *__restrict__ tkey,
+                                                                   float *__restrict__ tw, unsigned *__restrict__ err) {
+    extern __shared__ unsigned long long s_key[];  // 2 * P1_EDGES keys, then their weights
+    float *s_w = reinterpret_cast<float *>(s_key + 2 * P1_EDGES);
+    __shared__ unsigned s_cnt[NPART], s_off[NPART], s_wsum[NPART / 32], s_wbase[NPART / 32];
+    __shared__ unsigned long long s_gbase[NPART], s_pend[NPART];
+    __shared__ unsigned s_total;
+    for (int p = threadIdx.x; p < NPART; p += blockDim.x) s_pend[p] = rowstarts[min((uint64_t)(p + 1) << pshift, n)];
+    for (uint64_t tile = blockIdx.x; tile * P1_EDGES < m; tile += gridDim.x) {
+        for (int p = threadIdx.x; p < NPART; p += blockDim.x) s_cnt[p] = 0;
+        __syncthreads();
+        unsigned long long ka[P1_PER_THREAD];
+        float wv[P1_PER_THREAD];
+        unsigned ra[P1_PER_THREAD], rb[P1_PER_THREAD];
+        bool ok[P1_PER_THREAD];
+#pragma unroll
+        for (int k = 0; k < P1_PER_THREAD; ++k) {
+            const uint64_t i = tile * P1_EDGES + (uint64_t)k * P1_THREADS + threadIdx.x;
+            ok[k] = false;
+            ka[k] = 0;
+            wv[k] = 0.0f;
+            if (i < m) {
+                const ulonglong2 e = edges[i];
+                if (e.x >= n || e.y >= n) {
+                    atomicOr(err, SORTERR_RANGE);
+                } else if (e.x != e.y) {
+                    ok[k] = true;
+                    ka[k] = (e.x << 32) | e.y;
+                    wv[k] = weights[i];
+                    ra[k] = atomicAdd(&s_cnt[e.x >> pshift], 1u);
+                    rb[k] = atomicAdd(&s_cnt[e.y >> pshift], 1u);
+                }
+            }
+        }
+        __syncthreads();
+        // Exclusive scan of the partition counts (256 = 8 warps x 32), and
+        // one cursor reservation per partition that has entries in the tile.
+        unsigned c = 0, incl = 0;
+        if (threadIdx.x < NPART) {  // warps 0..7, whole warps
+            c = s_cnt[threadIdx.x];
+            incl = warp_incl_scan(c);
+            if (lane_id() == 31) s_wsum[threadIdx.x >> 5] = incl;
+            if (c) s_gbase[threadIdx.x] = atomicAdd(&pcur[threadIdx.x], (unsigned long long)c);
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            const unsigned ws = threadIdx.x < NPART / 32 ? s_wsum[threadIdx.x] : 0u;
+            const unsigned wi = warp_incl_scan(ws);
+            if (threadIdx.x < NPART / 32) s_wbase[threadIdx.x] = wi - ws;
+            if (threadIdx.x == 31) s_total = wi;
+        }
+        __syncthreads();
+        if (threadIdx.x < NPART) s_off[threadIdx.x] = s_wbase[threadIdx.x >> 5] + incl - c;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < P1_PER_THREAD; ++k) {
+            if (!ok[k]) continue;
+            const unsigned a = (unsigned)(ka[k] >> 32), b = (unsigned)ka[k];
+            const unsigned ja = s_off[a >> pshift] + ra[k], jb = s_off[b >> pshift] + rb[k];
+            s_key[ja] = ka[k];
+            s_w[ja] = wv[k];
+            s_key[jb] = ((unsigned long long)b << 32) | a;
+            s_w[jb] = wv[k];
+        }
+        __syncthreads();
+        const unsigned total = s_total;
+        for (unsigned j = threadIdx.x; j < total; j += blockDim.x) {
+            const unsigned long long key = s_key[j];
+            const unsigned p = (unsigned)(key >> 32) >> pshift;
+            const unsigned long long pos = s_gbase[p] + (j - s_off[p]);
+            if (pos < s_pend[p]) {
+                tkey[pos] = key;
+                tw[pos] = s_w[j];
+            } else {
+                atomicOr(err, SORTERR_COUNT);  // the edges differ from the ones the rows were counted on
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------- place
+
+// Entries of partition p (read from the partition cursors' start values,
+// i.e. rowstarts of its first and last vertex) into their rows.
+__global__ void csr_place_kernel(const unsigned long long *__restrict__ tkey, const float *__restrict__ tw,
+                                 uint64_t n, int pshift, unsigned p, const uint64_t *__restrict__ rowstarts,
+                                 unsigned *__restrict__ rcur, int *__restrict__ col, float *__restrict__ w,
+                                 unsigned *__restrict__ err) {
+    const uint64_t b = rowstarts[min((uint64_t)p << pshift, n)];
+    const uint64_t e = rowstarts[min((uint64_t)(p + 1) << pshift, n)];
+    const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = b + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < e; i += T) {
+        const unsigned long long key = __ldcs(&tkey[i]);
+        const unsigned src = (unsigned)(key >> 32), dst = (unsigned)key;
+        if (src >= n) {  // a slot the partition pass left unwritten (edges that do not match the counts)
+            atomicOr(err, SORTERR_COUNT);
+            continue;
+        }
+        const uint64_t pos = rowstarts[src] + atomicAdd(&rcur[src], 1u);
+        if (pos >= rowstarts[src + 1]) {
+            atomicOr(err, SORTERR_COUNT);
+            continue;
+        }
+        col[pos] = (int)dst;
+        w[pos] = __ldcs(&tw[i]);
+    }
+}
+
+// ---------------------------------------------------------------- row sort
+
+__device__ __forceinline__ unsigned long long row_key(const int *col, const float *w, uint64_t i) {
+    return ((unsigned long long)(unsigned)col[i] << 32) | __float_as_uint(w[i]);
+}
+
+__device__ __forceinline__ void put_key(int *col, float *w, uint64_t *col64, uint64_t i, unsigned long long k) {
+    col[i] = (int)(unsigned)(k >> 32);
+    w[i] = __uint_as_float((unsigned)k);
+    if (col64) col64[i] = k >> 32;
+}
+
+// Rows of 2..256 entries, one warp each: up to 32 entries bitonic in
+// registers, 33..256 bitonic in the warp's shared-memory slice.  Longer rows
+// are listed for the block kernels (mid: up to 4096 entries, big: more).
+constexpr unsigned WARP_SMEM_KEYS = 256;
+
+__global__ void __launch_bounds__(256) csr_sort_warp_kernel(const uint64_t *__restrict__ rowstarts, uint64_t n,
+                                                            int *col, float *w, uint64_t *col64,
+                                                            unsigned *__restrict__ mid, unsigned *__restrict__ big,
+                                                            unsigned *__restrict__ cnt) {
+    __shared__ unsigned long long s_rows[8][WARP_SMEM_KEYS];
+    unsigned long long *sk = s_rows[threadIdx.x >> 5];
+    const unsigned lane = lane_id();
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v0 = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; v0 < n; v0 += nw * 32) {
+        // 32 rows per warp step: each lane reads one row's length and the
+        // long rows are listed with one atomic per list and step.
+        const uint64_t v = v0 + lane;
+        const uint64_t len = v < n ? rowstarts[v + 1] - rowstarts[v] : 0;
+        const bool is_mid = len > WARP_SMEM_KEYS && len <= SORT_SMEM_KEYS, is_big = len > SORT_SMEM_KEYS;
+        const unsigned pm = warp_append(&cnt[0], is_mid);
+        if (is_mid) mid[pm] = (unsigned)v;
+        const unsigned pb = warp_append(&cnt[1], is_big);
+        if (is_big) big[pb] = (unsigned)v;
+        if (col64 && len == 1) col64[rowstarts[v]] = (uint64_t)(unsigned)col[rowstarts[v]];
+        unsigned todo = __ballot_sync(FULL, len >= 2 && len <= WARP_SMEM_KEYS);
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint64_t r = v0 + l;
+            const uint64_t rb = rowstarts[r];
+            const unsigned rl = (unsigned)(rowstarts[r + 1] - rb);
+            if (rl <= 32) {
+                unsigned long long k = lane < rl ? row_key(col, w, rb + lane) : ~0ull;
+#pragma unroll
+                for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+                    for (int j = size >> 1; j > 0; j >>= 1) {
+                        const unsigned long long o = __shfl_xor_sync(FULL, k, j);
+                        const bool up = (lane & size) == 0, lower = (lane & j) == 0;
+                        k = (lower == up) ? min(k, o) : max(k, o);
+                    }
+                }
+                if (lane < rl) put_key(col, w, col64, rb + lane, k);
+                continue;
+            }
+            unsigned P = 64;
+            while (P < rl) P <<= 1;
+            for (unsigned i = lane; i < P; i += 32) sk[i] = i < rl ? row_key(col, w, rb + i) : ~0ull;
+            __syncwarp();
+            for (unsigned size = 2; size <= P; size <<= 1) {
+                for (unsigned j = size >> 1; j > 0; j >>= 1) {
+                    for (unsigned t = lane; t < P / 2; t += 32) {
+                        const unsigned i = 2 * t - (t & (j - 1)), q = i + j;
+                        const unsigned long long a = sk[i], b = sk[q];
+                        if ((a > b) == ((i & size) == 0)) {
+                            sk[i] = b;
+                            sk[q] = a;
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+            for (unsigned i = lane; i < rl; i += 32) put_key(col, w, col64, rb + i, sk[i]);
+            __syncwarp();
+        }
+    }
+}
+
+// Bitonic sort of s[0 .. P) (P a power of two) by the whole block.
+__device__ void block_bitonic(unsigned long long *s, unsigned P) {
+    for (unsigned size = 2; size <= P; size <<= 1) {
+        for (unsigned j = size >> 1; j > 0; j >>= 1) {
+            for (unsigned t = threadIdx.x; t < P / 2; t += blockDim.x) {
+                const unsigned i = 2 * t - (t & (j - 1));
+                const unsigned q = i + j;
+                const bool up = (i & size) == 0;
+                const unsigned long long a = s[i], b = s[q];
+                if ((a > b) == up) {
+                    s[i] = b;
+                    s[q] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned next_pow2(unsigned x) {
+    unsigned p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+// Rows of 257..4096 entries: one block per row, in shared memory.
+__global__ void __launch_bounds__(SORT_THREADS) csr_sort_mid_kernel(const uint64_t *__restrict__ rowstarts,
+                                                                    const unsigned *__restrict__ mid,
+                                                                    const unsigned *__restrict__ cnt, int *col,
+                                                                    float *w, uint64_t *col64) {
+    __shared__ unsigned long long s[SORT_SMEM_KEYS];
+    const unsigned nrows = cnt[0];
+    for (unsigned k = blockIdx.x; k < nrows; k += gridDim.x) {
+        const unsigned v = mid[k];
+        const uint64_t rb = rowstarts[v];
+        const unsigned L = (unsigned)(rowstarts[v + 1] - rb);
+        const unsigned P = next_pow2(L);
+        for (unsigned i = threadIdx.x; i < P; i += blockDim.x) s[i] = i < L ? row_key(col, w, rb + i) : ~0ull;
+        __syncthreads();
+        block_bitonic(s, P);
+        for (unsigned i = threadIdx.x; i < L; i += blockDim.x) put_key(col, w, col64, rb + i, s[i]);
+        __syncthreads();
+    }
+}
+
+// A row's keys live either in the scratch array (u64) or in col/w.
+struct KeyBuf {
+    unsigned long long *key;  // non-null: the scratch array
+    int *col;
+    float *w;
+    __device__ __forceinline__ unsigned long long get(uint64_t i) const {
+        return key ? key[i] : row_key(col, w, i);
+    }
+    __device__ __forceinline__ void set(uint64_t i, unsigned long long k) const {
+        if (key) key[i] = k;
+        else {
+            col[i] = (int)(unsigned)(k >> 32);
+            w[i] = __uint_as_float((unsigned)k);
+        }
+    }
+};
+
+// Merge of the sorted runs A = src[a, a + la) and B = src[b, b + lb) into
+// dst[a, a + la + lb) (b = a + la) by the whole block: each thread takes
+// MERGE_ITEMS consecutive outputs, finds where they start in A and B by a
+// binary search on the cross diagonal (merge path), and merges them.
+__device__ void block_merge(const KeyBuf &src, const KeyBuf &dst, uint64_t a, uint64_t la, uint64_t lb) {
+    const uint64_t b = a + la, total = la + lb;
+    for (uint64_t d0 = (uint64_t)threadIdx.x * MERGE_ITEMS; d0 < total; d0 += (uint64_t)blockDim.x * MERGE_ITEMS) {
+        // i = elements taken from A among the first d0 outputs
+        uint64_t lo = d0 > lb ? d0 - lb : 0, hi = d0 < la ? d0 : la;
+        while (lo < hi) {
+            const uint64_t i = (lo + hi) >> 1;  // A[i] vs B[d0 - 1 - i]
+            if (src.get(a + i) <= src.get(b + d0 - 1 - i)) lo = i + 1;
+            else hi = i;
+        }
+        uint64_t i = lo, j = d0 - lo;
+        const uint64_t dend = min(d0 + MERGE_ITEMS, total);
+        for (uint64_t d = d0; d < dend; ++d) {
+            const bool takeA = j >= lb || (i < la && src.get(a + i) <= src.get(b + j));
+            dst.set(a + d, takeA ? src.get(a + i++) : src.get(b + j++));
+        }
+    }
+}
+
+// Rows of more than 4096 entries: one block per row; 4096-entry chunks are
+// sorted in shared memory into the scratch array, then runs are merged
+// pairwise, the row going back and forth between the scratch array and
+// col/w, and finally copied to col/w (and col64).
+__global__ void __launch_bounds__(SORT_THREADS) csr_sort_big_kernel(const uint64_t *__restrict__ rowstarts,
+                                                                    const unsigned *__restrict__ big,
+                                                                    const unsigned *__restrict__ cnt,
+                                                                    unsigned long long *tkey, int *col, float *w,
+                                                                    uint64_t *col64) {
+    __shared__ unsigned long long s[SORT_SMEM_KEYS];
+    const unsigned nrows = cnt[1];
+    const KeyBuf K{tkey, nullptr, nullptr}, C{nullptr, col, w};
+    for (unsigned k = blockIdx.x; k < nrows; k += gridDim.x) {
+        const unsigned v = big[k];
+        const uint64_t rb = rowstarts[v];
+        const uint64_t L = rowstarts[v + 1] - rb;
+        for (uint64_t c0 = 0; c0 < L; c0 += SORT_SMEM_KEYS) {
+            const unsigned cl = L - c0 < SORT_SMEM_KEYS ? (unsigned)(L - c0) : SORT_SMEM_KEYS;
+            const unsigned P = next_pow2(cl);
+            for (unsigned i = threadIdx.x; i < P; i += blockDim.x) s[i] = i < cl ? row_key(col, w, rb + c0 + i) : ~0ull;
+            __syncthreads();
+            block_bitonic(s, P);
+            for (unsigned i = threadIdx.x; i < cl; i += blockDim.x) tkey[rb + c0 + i] = s[i];
+            __syncthreads();
+        }
+        bool in_scratch = true;
+        for (uint64_t R = SORT_SMEM_KEYS; R < L; R <<= 1) {
+            const KeyBuf &src = in_scratch ? K : C, &dst = in_scratch ? C : K;
+            for (uint64_t a = 0; a < L; a += 2 * R) {
+                const uint64_t la = min(R, L - a), lb = a + R < L ? min(R, L - a - R) : 0;
+                block_merge(KeyBuf{src.key ? src.key + rb : nullptr, src.col ? src.col + rb : nullptr,
+                                   src.w ? src.w + rb : nullptr},
+                            KeyBuf{dst.key ? dst.key + rb : nullptr, dst.col ? dst.col + rb : nullptr,
+                                   dst.w ? dst.w + rb : nullptr},
+                            a, la, lb);
+            }
+            __syncthreads();
+            in_scratch = !in_scratch;
+        }
+        for (uint64_t i = threadIdx.x; i < L; i += blockDim.x) {
+            const unsigned long long key = in_scratch ? tkey[rb + i] : row_key(col, w, rb + i);
+            if (in_scratch) {
+                col[rb + i] = (int)(unsigned)(key >> 32);
+                w[rb + i] = __uint_as_float((unsigned)key);
+            }
+            if (col64) col64[rb + i] = key >> 32;
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ dedupe
+
+// deg[v] = distinct neighbours of sorted row v (one warp per row).
+__global__ void csr_unique_count_kernel(const uint64_t *__restrict__ rowstarts, const int *__restrict__ col,
+                                        uint64_t n, unsigned *__restrict__ deg) {
+    const unsigned lane = lane_id();
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        const uint64_t rb = rowstarts[v], re = rowstarts[v + 1];
+        unsigned c = 0;
+        for (uint64_t i = rb + lane; i < re; i += 32) c += i == rb || col[i] != col[i - 1];
+        c = warp_sum(c);
+        if (lane == 0) deg[v] = c;
+    }
+}
+
+// The first entry of each run of equal neighbours into the new arrays.
+__global__ void csr_unique_copy_kernel(const uint64_t *__restrict__ rowstarts, const int *__restrict__ col,
+                                       const float *__restrict__ w, uint64_t n, const uint64_t *__restrict__ rs2,
+                                       int *__restrict__ col2, float *__restrict__ w2, uint64_t *__restrict__ col64) {
+    const unsigned lane = lane_id();
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        const uint64_t rb = rowstarts[v], re = rowstarts[v + 1];
+        uint64_t out = rs2[v];
+        for (uint64_t i0 = rb; i0 < re; i0 += 32) {
+            const uint64_t i = i0 + lane;
+            const bool first = i < re && (i == rb || col[i] != col[i - 1]);
+            const unsigned m = __ballot_sync(FULL, first);
+            if (first) {
+                const uint64_t o = out + __popc(m & lanemask_lt());
+                col2[o] = col[i];
+                w2[o] = w[i];
+                if (col64) col64[o] = (uint64_t)(unsigned)col[i];
+            }
+            out += __popc(m);
+        }
+    }
+}
+
+// ------------------------------------------------------------- SSSP split
+
+// Stable three-way partition of a row into tiny (w < tiny), other light
+// (w < light) and heavy entries, with the row's light and tiny counts.  The
+// warp version takes rows of up to 4096 entries (one warp each); longer
+// rows, listed, take a block each.
+__device__ __forceinline__ int light_class(float x, float light, float tiny) {
+    return x < tiny ? 0 : x < light ? 1 : 2;
+}
+
+__global__ void csr_split_light_kernel(const uint64_t *__restrict__ rowstarts, const int *__restrict__ col,
+                                       const float *__restrict__ w, uint64_t n, float light, float tiny,
+                                       int *__restrict__ scol, float *__restrict__ sw, unsigned *__restrict__ ld,
+                                       unsigned *__restrict__ td, unsigned *__restrict__ big,
+                                       unsigned *__restrict__ nbig) {
+    const unsigned lane = lane_id();
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        const uint64_t rb = rowstarts[v], re = rowstarts[v + 1];
+        if (re - rb > SORT_SMEM_KEYS) {
+            if (lane == 0) big[atomicAdd(nbig, 1u)] = (unsigned)v;
+            continue;
+        }
+        unsigned nt = 0, nl = 0;
+        for (uint64_t i = rb + lane; i < re; i += 32) {
+            const int k = light_class(w[i], light, tiny);
+            nt += k == 0;
+            nl += k <= 1;
+        }
+        nt = warp_sum(nt);
+        nl = warp_sum(nl);
+        uint64_t o3[3] = {rb, rb + nt, rb + nl};
+        for (uint64_t i0 = rb; i0 < re; i0 += 32) {
+            const uint64_t i = i0 + lane;
+            const bool has = i < re;
+            const float x = has ? w[i] : 0.0f;
+            const int k = has ? light_class(x, light, tiny) : 3;
+            const unsigned lt = lanemask_lt();
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const unsigned m = __ballot_sync(FULL, k == q);
+                if (k == q) {
+                    const uint64_t o = o3[q] + __popc(m & lt);
+                    scol[o] = col[i];
+                    sw[o] = x;
+                }
+                o3[q] += __popc(m);
+            }
+        }
+        if (lane == 0) {
+            ld[v] = nl;
+            td[v] = nt;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) csr_split_light_big_kernel(
+    const uint64_t *__restrict__ rowstarts, const int *__restrict__ col, const float *__restrict__ w, float light,
+    float tiny, int *__restrict__ scol, float *__restrict__ sw, unsigned *__restrict__ ld, unsigned *__restrict__ td,
+    const unsigned *__restrict__ big, const unsigned *__restrict__ nbig) {
+    constexpr int WARPS = SORT_THREADS / 32;
+    __shared__ unsigned s_cnt[3][WARPS];
+    __shared__ unsigned long long s_base[3];
+    const unsigned lane = lane_id(), wid = threadIdx.x >> 5;
+    for (unsigned k = blockIdx.x; k < *nbig; k += gridDim.x) {
+        const unsigned v = big[k];
+        const uint64_t rb = rowstarts[v], re = rowstarts[v + 1];
+        unsigned nt = 0, nl = 0;
+        for (uint64_t i = rb + threadIdx.x; i < re; i += blockDim.x) {
+            const int c = light_class(w[i], light, tiny);
+            nt += c == 0;
+            nl += c <= 1;
+        }
+        nt = warp_sum(nt);
+        nl = warp_sum(nl);
+        if (lane == 0) {
+            s_cnt[0][wid] = nt;
+            s_cnt[1][wid] = nl;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long t = 0, l = 0;
+            for (int q = 0; q < WARPS; ++q) {
+                t += s_cnt[0][q];
+                l += s_cnt[1][q];
+            }
+            s_base[0] = rb;
+            s_base[1] = rb + t;
+            s_base[2] = rb + l;
+            ld[v] = (unsigned)l;
+            td[v] = (unsigned)t;
+        }
+        __syncthreads();
+        // Chunks of blockDim entries in order: per class, the warps' counts
+        // give each warp its offset inside the chunk.
+        for (uint64_t i0 = rb; i0 < re; i0 += blockDim.x) {
+            const uint64_t i = i0 + threadIdx.x;
+            const bool has = i < re;
+            const float x = has ? w[i] : 0.0f;
+            const int c = has ? light_class(x, light, tiny) : 3;
+            unsigned m[3];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                m[q] = __ballot_sync(FULL, c == q);
+                if (lane == 0) s_cnt[q][wid] = __popc(m[q]);
+            }
+            __syncthreads();
+            if (has) {
+                uint64_t o = s_base[c];
+                for (unsigned q = 0; q < wid; ++q) o += s_cnt[c][q];
+                o += __popc(m[c] & lanemask_lt());
+                scol[o] = col[i];
+                sw[o] = x;
+            }
+            __syncthreads();
+            if (threadIdx.x < 3) {
+                unsigned long long t = 0;
+                for (int q = 0; q < WARPS; ++q) t += s_cnt[threadIdx.x][q];
+                s_base[threadIdx.x] += t;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+static int sort_grid(int per_sm) {
+    DeviceInfo di;
+    if (device_info(&di)) return 148 * per_sm;
+    return di.sms * per_sm;
+}
+
+}  // namespace g5
+
+using namespace g5;
+
+extern "C" int g5_csr_sorted_workspace_size(uint64_t nverts, uint64_t nentries, uint64_t *bytes) {
+    G5_CHECK_ARG(bytes, "g5_csr_sorted_workspace_size: bytes is NULL");
+    *bytes = carve_sort(nullptr, nverts, nentries).bytes;
+    return G5_OK;
+}
+
+// Sorts rows in place (any CSR: the rows of g5_csr_fill or of the fused
+// Kronecker fill come out canonical too).
+static int sort_rows(const uint64_t *d_rowstarts, uint64_t nverts, int32_t *d_col, float *d_w, uint64_t *d_col64,
+                     const SortWork &w, cudaStream_t st) {
+    G5_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, 2 * sizeof(unsigned), st));
+    const uint64_t warps = (nverts + 31) / 32;
+    const int wblocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sort_grid(8), (warps + 7) / 8));
+    csr_sort_warp_kernel<<<wblocks, 256, 0, st>>>(d_rowstarts, nverts, d_col, d_w, d_col64, w.mid, w.big, w.cnt);
+    csr_sort_mid_kernel<<<sort_grid(4), SORT_THREADS, 0, st>>>(d_rowstarts, w.mid, w.cnt, d_col, d_w, d_col64);
+    csr_sort_big_kernel<<<sort_grid(4), SORT_THREADS, 0, st>>>(d_rowstarts, w.big, w.cnt, w.tkey, d_col, d_w,
+                                                              d_col64);
+    G5_CUDA_TRY(cudaGetLastError());
+    return G5_OK;
+}
+
+extern "C" int g5_csr_fill_sorted(const uint64_t *d_edges, const float *d_weights, uint64_t nedges, uint64_t nverts,
+                                  const uint64_t *d_rowstarts, uint64_t nentries, void *d_work, uint64_t work_bytes,
+                                  int32_t *d_col, float *d_w, uint64_t *d_col64, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_csr_fill_sorted: nverts outside [1, 2^31]");
+    G5_CHECK_ARG(d_rowstarts && d_work && (nentries == 0 || (d_col && d_w)), "g5_csr_fill_sorted: NULL argument");
+    G5_CHECK_ARG(nedges == 0 || (d_edges && d_weights), "g5_csr_fill_sorted: edges or weights NULL");
+    SortWork w = carve_sort(d_work, nverts, nentries);
+    if (work_bytes < w.bytes)
+        return set_error(G5_ERR_WORKSPACE, "g5_csr_fill_sorted: workspace %llu < %llu bytes",
+                         (unsigned long long)work_bytes, (unsigned long long)w.bytes);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int pshift = part_shift(nverts);
+    G5_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, 64 * sizeof(unsigned), st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.rcur, 0, nverts * sizeof(unsigned), st));
+    if (nedges && nentries) {
+        csr_part_init_kernel<<<1, NPART + 32, 0, st>>>(d_rowstarts, nverts, pshift, w.pcur);
+        const uint64_t tiles = (nedges + P1_EDGES - 1) / P1_EDGES;
+        const int pblocks = (int)std::min<uint64_t>(tiles, (uint64_t)sort_grid(2));
+        static bool smem_set[64] = {};  // the function attribute, once per device
+        int dev = 0;
+        G5_CUDA_TRY(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64 || !smem_set[dev]) {
+            G5_CUDA_TRY(cudaFuncSetAttribute(csr_partition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)P1_SMEM));
+            if (dev >= 0 && dev < 64) smem_set[dev] = true;
+        }
+        csr_partition_kernel<<<pblocks, P1_THREADS, P1_SMEM, st>>>((const ulonglong2 *)d_edges, d_weights, nedges, nverts,
+                                                             pshift, d_rowstarts, w.pcur, w.tkey, w.tw, &w.cnt[2]);
+        const uint64_t nparts = std::min<uint64_t>(NPART, (nverts + (1ull << pshift) - 1) >> pshift);
+        const int gblocks = (int)std::max<uint64_t>(
+            1, std::min<uint64_t>((uint64_t)sort_grid(8), (nentries / nparts + 255) / 256));
+        for (unsigned p = 0; p < nparts; ++p)
+            csr_place_kernel<<<gblocks, 256, 0, st>>>(w.tkey, w.tw, nverts, pshift, p, d_rowstarts, w.rcur, d_col,
+                                                      d_w, &w.cnt[2]);
+        G5_CUDA_TRY(cudaGetLastError());
+    }
+    int rc = sort_rows(d_rowstarts, nverts, d_col, d_w, d_col64, w, st);
+    if (rc) return rc;
+    unsigned err = 0;
+    G5_CUDA_TRY(cudaMemcpyAsync(&err, &w.cnt[2], sizeof err, cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    if (err & SORTERR_RANGE) return set_error(G5_ERR_INVALID, "g5_csr_fill_sorted: an edge endpoint is >= nverts");
+    if (err) return set_error(G5_ERR_INVALID, "g5_csr_fill_sorted: the edges differ from those the rows were counted on");
+    return G5_OK;
+}
+
+extern "C" int g5_csr_sort_rows(const uint64_t *d_rowstarts, uint64_t nverts, uint64_t nentries, int32_t *d_col,
+                                float *d_w, uint64_t *d_col64, void *d_work, uint64_t work_bytes, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_csr_sort_rows: nverts outside [1, 2^31]");
+    G5_CHECK_ARG(d_rowstarts && d_work && (nentries == 0 || (d_col && d_w)), "g5_csr_sort_rows: NULL argument");
+    SortWork w = carve_sort(d_work, nverts, nentries);
+    if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "g5_csr_sort_rows: workspace too small");
+    return sort_rows(d_rowstarts, nverts, d_col, d_w, d_col64, w, (cudaStream_t)stream);
+}
+
+extern "C" int g5_csr_dedupe_count(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
+                                   uint64_t nentries, uint64_t *d_rowstarts_out, void *d_work, uint64_t work_bytes,
+                                   uint64_t *nentries_out, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_csr_dedupe_count: nverts outside [1, 2^31]");
+    G5_CHECK_ARG(d_rowstarts && d_rowstarts_out && d_work && nentries_out && (nentries == 0 || d_col),
+                 "g5_csr_dedupe_count: NULL argument");
+    SortWork w = carve_sort(d_work, nverts, nentries);
+    if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "g5_csr_dedupe_count: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sort_grid(8), (nverts + 7) / 8));
+    csr_unique_count_kernel<<<blocks, 256, 0, st>>>(d_rowstarts, d_col, nverts, w.rcur);
+    G5_CUDA_TRY(cudaGetLastError());
+    int rc = scan_u32_to_u64(w.rcur, nverts, d_rowstarts_out, w.scan, st);
+    if (rc) return rc;
+    G5_CUDA_TRY(cudaMemcpyAsync(nentries_out, d_rowstarts_out + nverts, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    return G5_OK;
+}
+
+extern "C" int g5_csr_dedupe_copy(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
+                                  uint64_t nverts, const uint64_t *d_rowstarts_out, int32_t *d_col_out,
+                                  float *d_w_out, uint64_t *d_col64_out, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_csr_dedupe_copy: nverts outside [1, 2^31]");
+    G5_CHECK_ARG(d_rowstarts && d_col && d_w && d_rowstarts_out && d_col_out && d_w_out,
+                 "g5_csr_dedupe_copy: NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sort_grid(8), (nverts + 7) / 8));
+    csr_unique_copy_kernel<<<blocks, 256, 0, st>>>(d_rowstarts, d_col, d_w, nverts, d_rowstarts_out, d_col_out,
+                                                   d_w_out, d_col64_out);
+    G5_CUDA_TRY(cudaGetLastError());
+    return G5_OK;
+}
+
+extern "C" int g5_csr_split_light(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
+                                  uint64_t nverts, uint64_t nentries, float light_delta, int32_t *d_scol, float *d_sw,
+                                  uint32_t *d_light_deg, uint32_t *d_tiny_deg, void *d_work, uint64_t work_bytes,
+                                  void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_csr_split_light: nverts outside [1, 2^31]");
+    G5_CHECK_ARG(d_rowstarts && d_light_deg && d_tiny_deg && d_work &&
+                     (nentries == 0 || (d_col && d_w && d_scol && d_sw)),
+                 "g5_csr_split_light: NULL argument");
+    G5_CHECK_ARG(light_delta > 0.0f, "g5_csr_split_light: light_delta must be positive");
+    SortWork w = carve_sort(d_work, nverts, nentries);
+    if (work_bytes < w.bytes) return set_error(G5_ERR_WORKSPACE, "g5_csr_split_light: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    const float tiny = light_delta / (float)G5_TINY_DIV;
+    G5_CUDA_TRY(cudaMemsetAsync(&w.cnt[3], 0, sizeof(unsigned), st));
+    const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sort_grid(8), (nverts + 7) / 8));
+    csr_split_light_kernel<<<blocks, 256, 0, st>>>(d_rowstarts, d_col, d_w, nverts, light_delta, tiny, d_scol, d_sw,
+                                                   d_light_deg, d_tiny_deg, w.big, &w.cnt[3]);
+    csr_split_light_big_kernel<<<sort_grid(2), SORT_THREADS, 0, st>>>(d_rowstarts, d_col, d_w, light_delta, tiny,
+                                                                     d_scol, d_sw, d_light_deg, d_tiny_deg, w.big,
+                                                                     &w.cnt[3]);
+    G5_CUDA_TRY(cudaGetLastError());
+    return G5_OK;
+}

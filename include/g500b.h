@@ -110,6 +110,49 @@ int g5_csr_split_tiny(const uint64_t *d_rowstarts, int32_t *d_col, float *d_w, u
                       const uint32_t *d_light_deg, uint64_t nverts, float light_delta, uint32_t *d_tiny_deg,
                       void *stream);
 
+/* ------------------------------------------------- canonical CSR rows --- */
+
+/* Rows in canonical order: every row sorted by (neighbour, weight bits) --
+ * the order the reference's rows have once sorted (its fill leaves them in
+ * atomic order, src/traversal.cu:48-73), so the CSR is the same on every
+ * run.  After g5_csr_count (row starts, entry count), g5_csr_fill_sorted
+ * scatters the edges by radix partitioning (256 source partitions, then
+ * each partition's rows while they are L2-resident) and sorts every row;
+ * d_col64 (optional) receives the u64 column of the reference's Oned_Graph.
+ * Scratch: g5_csr_sorted_workspace_size(nverts, nentries) bytes (12 bytes
+ * per entry, plus 12 per vertex). */
+int g5_csr_sorted_workspace_size(uint64_t nverts, uint64_t nentries, uint64_t *bytes);
+int g5_csr_fill_sorted(const uint64_t *d_edges, const float *d_weights, uint64_t nedges, uint64_t nverts,
+                       const uint64_t *d_rowstarts, uint64_t nentries, void *d_work, uint64_t work_bytes,
+                       int32_t *d_col, float *d_w, uint64_t *d_col64, void *stream);
+
+/* Sorts the rows of any CSR in place into canonical order (e.g. after
+ * g5_csr_fill or g5_csr_fill_kronecker); same scratch as above. */
+int g5_csr_sort_rows(const uint64_t *d_rowstarts, uint64_t nverts, uint64_t nentries, int32_t *d_col, float *d_w,
+                     uint64_t *d_col64, void *d_work, uint64_t work_bytes, void *stream);
+
+/* Opt-in dedupe of a canonical CSR (the reference keeps duplicates; this
+ * changes the TEPS edge count): one entry per (row, neighbour), the one of
+ * least weight.  g5_csr_dedupe_count writes the new row starts
+ * (nverts + 1) and their entry count; g5_csr_dedupe_copy fills new arrays
+ * of that size (d_col64_out optional).  No counterpart in the reference. */
+int g5_csr_dedupe_count(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t nentries,
+                        uint64_t *d_rowstarts_out, void *d_work, uint64_t work_bytes, uint64_t *nentries_out,
+                        void *stream);
+int g5_csr_dedupe_copy(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, uint64_t nverts,
+                       const uint64_t *d_rowstarts_out, int32_t *d_col_out, float *d_w_out, uint64_t *d_col64_out,
+                       void *stream);
+
+/* The SSSP copy of a CSR: each row stably partitioned into entries lighter
+ * than light_delta / G5_TINY_DIV, the other ones lighter than light_delta,
+ * then the rest (so a canonical CSR gives each part in canonical order),
+ * with d_light_deg / d_tiny_deg = the first two parts' sizes per row -- the
+ * layout g5_sssp_run reads (d_scol, d_sw as its column and weights).  Same
+ * scratch as g5_csr_fill_sorted.  No counterpart in the reference. */
+int g5_csr_split_light(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, uint64_t nverts,
+                       uint64_t nentries, float light_delta, int32_t *d_scol, float *d_sw, uint32_t *d_light_deg,
+                       uint32_t *d_tiny_deg, void *d_work, uint64_t work_bytes, void *stream);
+
 /* Packs disjoint graphs into one CSR (no counterpart in the reference, which
  * holds one graph): copies one graph's CSR into the destination at vertex
  * offset vbase and entry offset ebase, shifting its column by vbase.  Call

@@ -80,7 +80,7 @@ def test_csr_matches_reference(graphs, golden_dump):
 def test_csr_light_partition(graphs):
     g = graphs[16]["g"]
     rs = _np(g.rowstarts)
-    w = _np(g.w)
+    w = _np(g.sssp_w)
     ld = _np(g.light_deg).astype(np.int64)
     src = np.repeat(np.arange(g.nglobalverts), np.diff(rs))
     pos = np.arange(rs[-1]) - rs[src]
@@ -95,7 +95,7 @@ def test_csr_tiny_split(cgt, graphs):
     for scale in (12, 16):
         g = graphs[scale]["g"]
         rs = _np(g.rowstarts)
-        w = _np(g.w)
+        w = _np(g.sssp_w)
         ld = _np(g.light_deg).astype(np.int64)
         td = _np(g.tiny_deg).astype(np.int64)
         src = np.repeat(np.arange(g.nglobalverts), np.diff(rs))
@@ -104,10 +104,11 @@ def test_csr_tiny_split(cgt, graphs):
         assert np.array_equal(pos < td[src], (pos < ld[src]) & (w < tiny))
         assert td.sum() > 0 and np.all(td <= ld)
         assert np.array_equal(_np(g.column), _np(g.col).astype(np.int64))
-        col, ww = _np(g.col).copy(), w.copy()
-        td2 = cgt._split_tiny(g.rowstarts, g.col, g.w, g.column, g.light_deg, g.nglobalverts, g.light_delta, None)
+        col, ww = _np(g.sssp_col).copy(), w.copy()
+        td2 = cgt._split_tiny(g.rowstarts, g.sssp_col, g.sssp_w, None, g.light_deg, g.nglobalverts, g.light_delta,
+                              None)
         assert np.array_equal(_np(td2), td)
-        assert np.array_equal(_np(g.col), col) and np.array_equal(_np(g.w), ww)
+        assert np.array_equal(_np(g.sssp_col), col) and np.array_equal(_np(g.sssp_w), ww)
 
 
 def test_csr_edge_cases(cgt):
