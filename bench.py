@@ -524,7 +524,8 @@ def run_packed(G, dev, ngraphs, smin, smax, ef, reps=3):
     tb = T.tune_bfs(pk.g, pk.d_roots, alphas=(10.0, 14.0, 20.0), betas=(24.0,), grids=(0,))
     ts = T.tune_sssp(pk.g, pk.d_roots, deltas=(0.08, 0.1, 0.2, 0.4), grids=(0,))
     batch = G.PackedBatch(pk, delta=ts["delta"], capture=True, bfs_params=T.bfs_params(tb),
-                          sssp_blocks=ts["blocks"], sssp_pull=ts["pull"], sssp_sub_min=ts["sub_min"])
+                          sssp_blocks=ts["blocks"], sssp_pull=ts["pull"], sssp_sub_min=ts["sub_min"],
+                          sssp_big_deg=ts["big_deg"], sssp_chunk=ts["chunk"])
     build_s = time.time() - t0
     bfs_ms, all_ms = [], []
     for _ in range(reps):
@@ -584,8 +585,10 @@ def run_packed(G, dev, ngraphs, smin, smax, ef, reps=3):
             "speedup_vs_plain": round((plain_bfs + plain_sssp) / best, 2),
             "bfs_speedup_vs_plain": round(plain_bfs / best_bfs, 2),
             "graphs_checked_identical": checked, "build_s": round(build_s, 2),
-            "autotuned": {"bfs_alpha": tb["alpha"], "bfs_beta": tb["beta"], "sssp_delta": ts["delta"],
-                          "sssp_pull": ts["pull"], "sssp_sub_min": ts["sub_min"]},
+            "autotuned": {"bfs_alpha": tb["alpha"], "bfs_beta": tb["beta"], "bfs_big_deg": tb["big_deg"],
+                          "bfs_chunk": tb["chunk"], "bfs_lane_entries": tb["lane_entries"],
+                          "sssp_delta": ts["delta"], "sssp_pull": ts["pull"], "sssp_sub_min": ts["sub_min"],
+                          "sssp_big_deg": ts["big_deg"], "sssp_chunk": ts["chunk"]},
             "timing": "device events; batch = replay of the captured CUDA graph (BFS+SSSP resets included), "
                       "min of 3 after a warm-up; plain = per-graph g5_bfs_run + g5_sssp_run, resets included"}
 

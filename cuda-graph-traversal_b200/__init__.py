@@ -138,7 +138,8 @@ def _check(rc: int) -> None:
 
 
 class BfsParams(C.Structure):
-    _fields_ = [("alpha", C.c_float), ("beta", C.c_float), ("mode", C.c_int32), ("blocks", C.c_int32)]
+    _fields_ = [("alpha", C.c_float), ("beta", C.c_float), ("mode", C.c_int32), ("blocks", C.c_int32),
+                ("big_deg", C.c_int32), ("chunk", C.c_int32), ("lane_entries", C.c_int32)]
 
 
 class BfsStats(C.Structure):
@@ -157,7 +158,8 @@ class MsBfsStats(C.Structure):
 
 class SsspParams(C.Structure):
     _fields_ = [("delta", C.c_float), ("blocks", C.c_int32), ("pull", C.c_float), ("sub_min", C.c_int32),
-                ("small", C.c_int32), ("tiny_deg", C.c_void_p), ("check_opens", C.c_int32)]
+                ("small", C.c_int32), ("tiny_deg", C.c_void_p), ("check_opens", C.c_int32), ("big_deg", C.c_int32),
+                ("chunk", C.c_int32)]
 
 
 def _ptr(t: torch.Tensor | None) -> int | None:
@@ -510,10 +512,11 @@ def oned_graph_bfs_traverse_multi(g: OnedGraph, bfs: "BfsState", d_roots: torch.
 
 
 def oned_graph_sssp_traverse_multi(g: OnedGraph, sssp: "SsspState", d_roots: torch.Tensor, delta: float = 0.1,
-                                   blocks: int = 0, pull: float = 0.0, sub_min: int = 0, stream=None) -> None:
+                                   blocks: int = 0, pull: float = 0.0, sub_min: int = 0, stream=None,
+                                   big_deg: int = 0, chunk: int = 0) -> None:
     """SSSP from every source in d_roots at once (g5_sssp_traverse_multi);
     reset sssp first."""
-    p = SsspParams(delta, blocks, pull, sub_min, 0, _ptr(g.tiny_deg))
+    p = SsspParams(delta, blocks, pull, sub_min, 0, _ptr(g.tiny_deg), 0, big_deg, chunk)
     _check(lib.g5_sssp_traverse_multi(_ptr(g.rowstarts), _ptr(g.sssp_col), _ptr(g.sssp_w), _ptr(g.light_deg),
                                       g.light_delta,
                                       g.nglobalverts, _ptr(d_roots), d_roots.numel(), _ptr(sssp.dist),
@@ -529,10 +532,11 @@ class PackedBatch:
 
     def __init__(self, pk: PackedGraphs, delta: float = 0.1, capture: bool = True, with_depth: bool = True,
                  bfs_params: BfsParams | None = None, sssp_blocks: int = 0, sssp_pull: float = 0.0,
-                 sssp_sub_min: int = 0):
+                 sssp_sub_min: int = 0, sssp_big_deg: int = 0, sssp_chunk: int = 0):
         self.pk, self.delta, self.with_depth = pk, delta, with_depth
         self.bfs_params, self.sssp_blocks = bfs_params, sssp_blocks
         self.sssp_pull, self.sssp_sub_min = sssp_pull, sssp_sub_min
+        self.sssp_big_deg, self.sssp_chunk = sssp_big_deg, sssp_chunk
         self.bfs = BfsState(pk.g)
         self.sssp = SsspState(pk.g)
         self.stream = torch.cuda.Stream(device=pk.g.device)
@@ -555,7 +559,8 @@ class PackedBatch:
     def _enqueue_sssp(self):
         oned_graph_sssp_reset(self.sssp)
         oned_graph_sssp_traverse_multi(self.pk.g, self.sssp, self.pk.d_roots, self.delta, self.sssp_blocks,
-                                       self.sssp_pull, self.sssp_sub_min)
+                                       self.sssp_pull, self.sssp_sub_min, big_deg=self.sssp_big_deg,
+                                       chunk=self.sssp_chunk)
 
     def run(self) -> None:
         """Enqueues one batch on self.stream (replaying the graph when captured)."""
@@ -897,22 +902,24 @@ def oned_graph_sssp_create(g: OnedGraph) -> SsspState:
     return SsspState(g)
 
 
-def _sssp_params(g: OnedGraph, root: int, delta, blocks, pull, sub_min, small, check_opens=False) -> SsspParams:
+def _sssp_params(g: OnedGraph, root: int, delta, blocks, pull, sub_min, small, check_opens=False, big_deg=0,
+                 chunk=0) -> SsspParams:
     # small=None: the lean one-block search for a root outside the main
     # component (when the grid is left to the library).
     if small is None:
         small = blocks == 0 and not g.in_main_component(root)
     return SsspParams(delta, 1 if small and blocks == 0 else blocks, pull, sub_min, int(bool(small)),
-                      _ptr(g.tiny_deg), int(bool(check_opens)))
+                      _ptr(g.tiny_deg), int(bool(check_opens)), big_deg, chunk)
 
 
 def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,
                         pull: float = 0.0, sub_min: int = 0, small: bool | None = None, stream=None,
-                        check_opens: bool = False) -> None:
+                        check_opens: bool = False, big_deg: int = 0, chunk: int = 0) -> None:
     """oned_graph_sssp_run (src/traversal.h:52), delta 0.1 as the reference.
     check_opens: the bucket and sub-bucket opens exchange their stamps and
-    fail the search if a queue held a vertex twice (a test aid)."""
-    p = _sssp_params(g, root, delta, blocks, pull, sub_min, small, check_opens)
+    fail the search if a queue held a vertex twice (a test aid).  big_deg /
+    chunk: the work tiles of g5_sssp_params (0 = defaults)."""
+    p = _sssp_params(g, root, delta, blocks, pull, sub_min, small, check_opens, big_deg, chunk)
     _check(lib.g5_sssp_run(_ptr(g.rowstarts), _ptr(g.sssp_col), _ptr(g.sssp_w), _ptr(g.light_deg), g.light_delta,
                            g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                            sssp.work.numel(), C.byref(p), _stream(stream)))
@@ -934,10 +941,10 @@ def oned_graph_sssp_reset(sssp: SsspState, stream=None) -> None:
 
 def oned_graph_sssp_traverse(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,
                              pull: float = 0.0, sub_min: int = 0, small: bool | None = None,
-                             stream=None, check_opens: bool = False) -> None:
+                             stream=None, check_opens: bool = False, big_deg: int = 0, chunk: int = 0) -> None:
     """The search itself, on a reset state (the lean one-block search for a
     root outside the main component)."""
-    p = _sssp_params(g, root, delta, blocks, pull, sub_min, small, check_opens)
+    p = _sssp_params(g, root, delta, blocks, pull, sub_min, small, check_opens, big_deg, chunk)
     _check(lib.g5_sssp_traverse(_ptr(g.rowstarts), _ptr(g.sssp_col), _ptr(g.sssp_w), _ptr(g.light_deg),
                                 g.light_delta,
                                 g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),

@@ -1,8 +1,9 @@
 """Autotuner for the run-time knobs of the persistent searches: the BFS
 direction thresholds (alpha, beta), the batched BFS's switch threshold and
-frontier test, the SSSP bucket width delta, and each kernel's grid size
-(blocks per launch -- the tile of work the persistent grid cuts a level
-into).  No counterpart in the reference, which fixes its launch shape and
+frontier test, the SSSP bucket width delta, each kernel's grid size
+(blocks per launch), and the work tiles: the row length above which a list
+entry is cut into chunks spread over the grid, the chunk size, and the BFS
+bottom-up lane scan length.  No counterpart in the reference, which fixes its launch shape and
 delta (src/traversal.cu:479-503, 638-711).
 
 Every candidate is timed on the device (CUDA events, the search alone, its
@@ -48,16 +49,42 @@ def _searches(roots):
     return [roots] if isinstance(roots, torch.Tensor) else [int(r) for r in roots]
 
 
+def _descend(time_of, base: dict, axes: dict) -> tuple[float, dict, int]:
+    """Coordinate descent over the tile axes: each axis in turn takes the
+    value that times fastest with the others held at their best so far.
+    Returns (ms, settings, candidates timed)."""
+    best = dict(base)
+    best_ms = time_of(best)
+    count = 1
+    for name, values in axes.items():
+        for v in values:
+            if v == best[name]:
+                continue
+            trial = dict(best, **{name: v})
+            ms = time_of(trial)
+            count += 1
+            if ms < best_ms:
+                best_ms, best = ms, trial
+    return best_ms, best, count
+
+
+BFS_TILES = {"chunk": (128, 256, 512, 1024), "big_deg": (256, 1024, 4096), "lane_entries": (4, 8, 16, 32)}
+SSSP_TILES = {"chunk": (128, 256, 512, 1024), "big_deg": (64, 128, 256, 512)}
+
+
 def tune_bfs(g: OnedGraph, roots, alphas=(6.0, 10.0, 14.0, 20.0, 28.0), betas=(12.0, 24.0, 48.0), grids=None,
-             reps: int = 1) -> dict:
+             reps: int = 1, tiles: dict | None = BFS_TILES) -> dict:
     """Best (alpha, beta, blocks) for BFS over `roots`: a list of roots (one
     search each) or a device tensor (one multi-root search, as on packed
-    graphs)."""
+    graphs); then, with those fixed, the work tiles of g5_bfs_params
+    (big_deg, chunk, lane_entries) by coordinate descent over `tiles`
+    (None: the library's defaults)."""
     bfs = BfsState(g)
     grids = _grids("bfs", g.nglobalverts) if grids is None else list(grids)
-    table = []
-    for alpha, beta, blocks in itertools.product(alphas, betas, grids):
-        p = BfsParams(alpha, beta, 0, blocks)
+
+    def time_of(k: dict) -> float:
+        p = BfsParams(k["alpha"], k["beta"], 0, k["blocks"], k.get("big_deg", 0), k.get("chunk", 0),
+                      k.get("lane_entries", 0))
         ms = 0.0
         for _ in range(reps):
             for r in _searches(roots):
@@ -66,34 +93,54 @@ def tune_bfs(g: OnedGraph, roots, alphas=(6.0, 10.0, 14.0, 20.0, 28.0), betas=(1
                 else:
                     run = lambda: oned_graph_bfs_traverse(g, bfs, r, p, with_depth=False)  # noqa: E731
                 ms += _timed(run, lambda: oned_graph_bfs_reset(bfs, False, g))
-        table.append((ms / reps, alpha, beta, blocks))
+        return ms / reps
+
+    table = [(time_of({"alpha": a, "beta": b, "blocks": k}), a, b, k)
+             for a, b, k in itertools.product(alphas, betas, grids)]
     best = min(table)
-    return {"kind": "bfs", "alpha": best[1], "beta": best[2], "blocks": best[3], "ms": round(best[0], 4),
-            "candidates": len(table)}
+    out = {"alpha": best[1], "beta": best[2], "blocks": best[3], "big_deg": 0, "chunk": 0, "lane_entries": 0}
+    ms, count = best[0], len(table)
+    if tiles:
+        out.update(big_deg=1024, chunk=256, lane_entries=8)  # the library's defaults, spelled out
+        ms, out, more = _descend(time_of, out, tiles)
+        count += more
+    return {"kind": "bfs", **out, "ms": round(ms, 4), "candidates": count}
 
 
 def tune_sssp(g: OnedGraph, roots, deltas=(0.08, 0.1, 0.2, 0.4), grids=None, pulls=(0.0, -1.0), subs=(0, -1),
-              reps: int = 1) -> dict:
+              reps: int = 1, tiles: dict | None = SSSP_TILES) -> dict:
     """Best (delta, blocks, pull, sub_min) for SSSP over `roots` (a list: one
     search each; a device tensor: one multi-source search).  pull / sub_min
     are g5_sssp_params' heavy-phase pull threshold and sub-bucket threshold
-    (0 = the library's default, -1 = off)."""
+    (0 = the library's default, -1 = off).  Then the list tiles (big_deg,
+    chunk) by coordinate descent over `tiles`."""
     st = SsspState(g)
     grids = _grids("sssp", g.nglobalverts) if grids is None else list(grids)
-    table = []
-    for delta, blocks, pull, sub in itertools.product(deltas, grids, pulls, subs):
+
+    def time_of(k: dict) -> float:
+        kw = dict(big_deg=k.get("big_deg", 0), chunk=k.get("chunk", 0))
         ms = 0.0
         for _ in range(reps):
             for r in _searches(roots):
                 if isinstance(r, torch.Tensor):
-                    run = lambda: oned_graph_sssp_traverse_multi(g, st, r, delta, blocks, pull, sub)  # noqa: E731
+                    run = lambda: oned_graph_sssp_traverse_multi(g, st, r, k["delta"], k["blocks"], k["pull"],  # noqa: E731
+                                                                 k["sub_min"], **kw)
                 else:
-                    run = lambda: oned_graph_sssp_traverse(g, st, r, delta, blocks, pull, sub)  # noqa: E731
+                    run = lambda: oned_graph_sssp_traverse(g, st, r, k["delta"], k["blocks"], k["pull"],  # noqa: E731
+                                                           k["sub_min"], **kw)
                 ms += _timed(run, lambda: oned_graph_sssp_reset(st))
-        table.append((ms / reps, delta, blocks, pull, sub))
+        return ms / reps
+
+    table = [(time_of({"delta": d, "blocks": b, "pull": p, "sub_min": s}), d, b, p, s)
+             for d, b, p, s in itertools.product(deltas, grids, pulls, subs)]
     best = min(table)
-    return {"kind": "sssp", "delta": best[1], "blocks": best[2], "pull": best[3], "sub_min": best[4],
-            "ms": round(best[0], 4), "candidates": len(table)}
+    out = {"delta": best[1], "blocks": best[2], "pull": best[3], "sub_min": best[4], "big_deg": 0, "chunk": 0}
+    ms, count = best[0], len(table)
+    if tiles:
+        out.update(big_deg=128, chunk=256)
+        ms, out, more = _descend(time_of, out, tiles)
+        count += more
+    return {"kind": "sssp", **out, "ms": round(ms, 4), "candidates": count}
 
 
 def tune_msbfs(g: OnedGraph, roots, alphas=(8.0, 16.0, 32.0, 64.0), checks=(0, 1, 2), grids=None,
@@ -112,7 +159,13 @@ def tune_msbfs(g: OnedGraph, roots, alphas=(8.0, 16.0, 32.0, 64.0), checks=(0, 1
 
 
 def bfs_params(t: dict) -> BfsParams:
-    return BfsParams(t["alpha"], t["beta"], 0, t["blocks"])
+    return BfsParams(t["alpha"], t["beta"], 0, t["blocks"], t.get("big_deg", 0), t.get("chunk", 0),
+                     t.get("lane_entries", 0))
+
+
+def sssp_kwargs(t: dict) -> dict:
+    """Keyword arguments of oned_graph_sssp_run / _traverse for a tune_sssp result."""
+    return {k: t.get(k, 0) for k in ("delta", "blocks", "pull", "sub_min", "big_deg", "chunk")}
 
 
 def msbfs_params(t: dict) -> MsBfsParams:

@@ -14,7 +14,8 @@
 // lanes idle.  Vertices above BIG_DEG sit at the back of the queue and every
 // warp of the grid takes BFS_CHUNK-edge chunks of them from one counter
 // (g5_frontier.cuh); a chunk is a chain of BFS_CHUNK / 32 dependent steps of
-// one warp, so it bounds the longest warp of a level.  A neighbour is claimed with an atomicOr on the visited bitmap;
+// one warp, so it bounds the longest warp of a level.  Both sizes are
+// defaults of g5_bfs_params.big_deg / .chunk, which a tuner may change.  A neighbour is claimed with an atomicOr on the visited bitmap;
 // the winner writes pred/depth and appends it to the next queue with one
 // atomic per warp.
 //
@@ -43,7 +44,8 @@
 namespace g5 {
 
 constexpr int BFS_THREADS = 256;
-constexpr unsigned BFS_CHUNK = 256;  // edges of a long row taken by one warp
+constexpr unsigned BFS_CHUNK = 256;  // default: edges of a long row taken by one warp
+constexpr unsigned BFS_BIG_DEG = BIG_DEG;  // default: longest row expanded by one warp
 constexpr unsigned BFS_STAGE = 512;  // per-warp staging of the next queue (16 KiB shared per block)
 constexpr unsigned long long SOLO_EDGES = 4096;  // levels at most this wide run in block 0 alone
 constexpr int BFS_TRACE = 64;                    // levels recorded in the control block
@@ -122,14 +124,17 @@ struct BfsArgs {
     unsigned nroots;
     BfsTouch *touch;
     unsigned *tlist;  // touched list of the one-block search (n entries)
+    unsigned big_deg;       // queue entries with more edges go to the chunked big part
+    unsigned chunk;         // edges of a big entry per warp grab (a multiple of 32)
+    unsigned lane_entries;  // bottom-up: row head a lane scans alone (a multiple of BU_STEP)
 };
 
 enum { TOP_DOWN = 0, BOTTOM_UP = 1 };
 constexpr int BFS_SMALL = 3;  // g5_bfs_params.mode: one lean block, for a root in a small component
 
 // Bottom-up: entries of a row a lane scans on its own before the rest of
-// the row goes to the whole warp.
-constexpr uint64_t BU_LANE_ENTRIES = 8;
+// the row goes to the whole warp (default of g5_bfs_params.lane_entries).
+constexpr unsigned BU_LANE_ENTRIES = 8;
 constexpr int BU_STEP = 4;  // entries per lane step (loads issued together)
 
 // Claim v for parent u at the next level; appends it to the next queue.
@@ -150,7 +155,7 @@ __device__ __forceinline__ void td_visit(const BfsArgs &a, const WarpStage &bq, 
         deg = __ldg(&a.rowptr[v + 1]) - __ldg(&a.rowptr[v]);
         my_m += deg;
     }
-    if (!frontier_append_staged(bq, qn, basen, a.n, n_small, n_big, disc, v, deg, BIG_DEG, BFS_CHUNK))
+    if (!frontier_append_staged(bq, qn, basen, a.n, n_small, n_big, disc, v, deg, a.big_deg, a.chunk))
         atomicOr(&a.ctl->res.error_flags, DEVERR_CAPACITY);
 }
 
@@ -203,9 +208,9 @@ __device__ void td_expand(const BfsArgs &a, const WarpStage &bq, int level, int 
         const unsigned u = __ldcg(&Q[a.n - 1 - j]);
         const uint64_t rb = __ldg(&a.rowptr[u]);
         const uint64_t deg = __ldg(&a.rowptr[u + 1]) - rb;
-        const uint64_t cs = (uint64_t)(ch - __ldcg(&B[j])) * BFS_CHUNK;
-        const uint64_t ce = min(cs + BFS_CHUNK, deg);
-        for (uint64_t e = cs + lane; e < cs + BFS_CHUNK; e += 32) {
+        const uint64_t cs = (uint64_t)(ch - __ldcg(&B[j])) * a.chunk;
+        const uint64_t ce = min(cs + a.chunk, deg);
+        for (uint64_t e = cs + lane; e < cs + a.chunk; e += 32) {
             const bool has = e < ce;
             const unsigned v = has ? (unsigned)__ldg(&a.col[rb + e]) : 0u;
             td_visit(a, bq, has, v, u, level + 1, QN, BN, &c->n_small[s_nxt], &c->big[s_nxt], my_m);
@@ -267,7 +272,7 @@ __device__ void bu_expand(const BfsArgs &a, const WarpStage &bq, const LevelStat
             // Each lane scans the head of its own row, BU_STEP neighbours per
             // step: their loads and bitmap probes are independent, so a step
             // costs one memory round trip, not BU_STEP.
-            const uint64_t head = min(re, rb + BU_LANE_ENTRIES);
+            const uint64_t head = min(re, rb + a.lane_entries);
             for (e = rb; e < head && found < 0; e += BU_STEP) {
                 unsigned u[BU_STEP], word[BU_STEP];
 #pragma unroll
@@ -384,7 +389,7 @@ __device__ void bits_to_queue(const BfsArgs &a, const WarpStage &bq, const unsig
                 m &= m - 1;
                 deg = __ldg(&a.rowptr[v + 1]) - __ldg(&a.rowptr[v]);
             }
-            if (!frontier_append_staged(bq, qn, basen, a.n, n_small, n_big, has, v, deg, BIG_DEG, BFS_CHUNK))
+            if (!frontier_append_staged(bq, qn, basen, a.n, n_small, n_big, has, v, deg, a.big_deg, a.chunk))
                 atomicOr(&a.ctl->res.error_flags, DEVERR_CAPACITY);
         }
     }
@@ -541,10 +546,10 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
                 a.visited[root >> 5] |= 1u << (root & 31);
                 a.pred[root] = root;
                 if (a.depth) a.depth[root] = 0;
-                if (root_deg > BIG_DEG) {
+                if (root_deg > a.big_deg) {
                     a.q[0][a.n - 1] = root;
                     a.base[0][0] = 0;
-                    c->big[0] = (1ull << BIG_SHIFT) | ((root_deg + BFS_CHUNK - 1) / BFS_CHUNK);
+                    c->big[0] = (1ull << BIG_SHIFT) | ((root_deg + a.chunk - 1) / a.chunk);
                 } else {
                     a.q[0][0] = root;
                     c->n_small[0] = 1;
@@ -581,7 +586,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
                     }
                 }
                 if (!frontier_append_staged(bq, a.q[0], a.base[0], a.n, &c->n_small[0], &c->big[0], mine, r, deg,
-                                            BIG_DEG, BFS_CHUNK))
+                                            a.big_deg, a.chunk))
                     atomicOr(&c->res.error_flags, DEVERR_CAPACITY);
             }
             if (!stage_flush_warp(bq, a.q[0], a.n, &c->n_small[0])) atomicOr(&c->res.error_flags, DEVERR_CAPACITY);
@@ -1042,6 +1047,17 @@ extern "C" int g5_bfs_reset_touched(uint64_t nverts, int64_t *d_pred, int32_t *d
                             "g5_bfs_reset_touched");
 }
 
+// Checks g5_bfs_params (zero tile fields select the defaults).
+static int bfs_params_check(const g5_bfs_params &p, const char *who) {
+    G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= BFS_SMALL, "%s: bad params", who);
+    G5_CHECK_ARG(p.big_deg >= 0 && p.big_deg <= (1 << 20), "%s: big_deg %d outside [0, 2^20]", who, p.big_deg);
+    G5_CHECK_ARG(p.chunk >= 0 && p.chunk <= (1 << 16) && p.chunk % 32 == 0,
+                 "%s: chunk %d is not a multiple of 32 in [0, 65536]", who, p.chunk);
+    G5_CHECK_ARG(p.lane_entries >= 0 && p.lane_entries <= 1024 && p.lane_entries % BU_STEP == 0,
+                 "%s: lane_entries %d is not a multiple of %d in [0, 1024]", who, p.lane_entries, BU_STEP);
+    return G5_OK;
+}
+
 // Builds the kernel arguments and launches the persistent BFS;
 // d_stats_map (mapped pinned memory, or nullptr) receives the statistics at
 // the end of the search.
@@ -1051,9 +1067,10 @@ static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32
                       g5_bfs_stats *d_stats_map = nullptr) {
     g5_bfs_params p = {14.0f, 24.0f, 0, 0};
     if (params) p = *params;
-    G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= BFS_SMALL, "g5_bfs: bad params");
+    int rc = bfs_params_check(p, "g5_bfs");
+    if (rc) return rc;
     int max_blocks = 0;
-    int rc = bfs_max_blocks(&max_blocks);
+    rc = bfs_max_blocks(&max_blocks);
     if (rc) return rc;
     int blocks = p.blocks > 0 ? std::min(p.blocks, max_blocks)
                               : (int)std::min<uint64_t>(max_blocks, std::max<uint64_t>(1, nverts / 2048));
@@ -1084,6 +1101,9 @@ static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32
     a.nroots = nroots;
     a.touch = w.touch;
     a.tlist = w.base[0];  // unused by the one-block search, which is the only writer
+    a.big_deg = p.big_deg ? (unsigned)p.big_deg : BFS_BIG_DEG;
+    a.chunk = p.chunk ? (unsigned)p.chunk : BFS_CHUNK;
+    a.lane_entries = p.lane_entries ? (unsigned)p.lane_entries : BU_LANE_ENTRIES;
     static std::atomic<unsigned long long> next_seq{1};
     a.seq = next_seq.fetch_add(1);
     if (p.mode == BFS_SMALL && !d_roots) {
@@ -1239,7 +1259,7 @@ extern "C" int g5_bfs_query_plan_create(const uint64_t *d_rowstarts, const int32
                  "g5_bfs_query_plan_create: h_stats must be pinned host memory the device can address");
     g5_bfs_params p = {14.0f, 24.0f, 0, 0};
     if (params) p = *params;
-    G5_CHECK_ARG(p.alpha > 0 && p.beta > 0 && p.mode >= 0 && p.mode <= BFS_SMALL, "g5_bfs_query_plan_create: bad params");
+    if ((rc = bfs_params_check(p, "g5_bfs_query_plan_create"))) return rc;
     int max_blocks = 0;
     if ((rc = bfs_max_blocks(&max_blocks))) return rc;  // resolved (and cached) now, not on the first query
     auto *q = new (std::nothrow) g5_bfs_query_plan{d_rowstarts, d_col, nverts, h_main_bits, d_pred, d_depth, w, p,

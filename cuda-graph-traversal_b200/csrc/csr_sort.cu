@@ -18,14 +18,20 @@
 //   sort       rows sorted by the 64-bit key (neighbour << 32 | weight
 //              bits): up to 32 entries by a warp in registers (bitonic),
 //              up to 4096 by a block in shared memory (bitonic), longer rows
-//              by a block as sorted 4096-entry chunks merged pairwise (merge
-//              path), ping-ponging with the scratch array.
+//              cut into 4096-entry tiles spread over the whole grid: every
+//              tile sorted in shared memory, then log2(tiles) merge passes,
+//              each block producing one 4096-entry tile of output (merge
+//              path), ping-ponging with the scratch array.  A hub row of
+//              millions of entries thus takes the whole GPU, not one block.
 //   dedupe     (optional) keeps the first entry of each run of equal
 //              neighbours -- the lightest, rows being sorted -- into new
 //              arrays with new row starts.
 //   split      the SSSP copy of the CSR: each row stably partitioned into
 //              entries below light/G5_TINY_DIV, the other light ones (below
-//              light), and the heavy ones, with per-row counts.
+//              light), and the heavy ones, with per-row counts (a warp per
+//              row up to 4096 entries; longer rows tiled over the grid: per
+//              tile class counts, a scan over tiles, then each tile writes
+//              its entries at their final places).
 //
 // Algorithmic bytes per edge (two entries): partition reads 20 and writes
 // 24, place reads 24 and writes 16 (+16 with the u64 column), sort reads and
@@ -44,7 +50,6 @@ constexpr size_t P1_SMEM = (size_t)2 * P1_EDGES * (sizeof(unsigned long long) + 
 constexpr int P1_PER_THREAD = P1_EDGES / P1_THREADS;
 constexpr int SORT_THREADS = 256;
 constexpr unsigned SORT_SMEM_KEYS = 4096;  // rows up to this length sort in shared memory
-constexpr int MERGE_ITEMS = 8;             // outputs per thread per merge step
 
 __host__ __device__ __forceinline__ int part_shift(uint64_t n) {
     int lg = 0;
@@ -59,15 +64,31 @@ struct SortWork {
     float *tw;                 // E: their weights
     unsigned *rcur;            // N: per-row cursors (place), then dedupe degrees
     unsigned long long *pcur;  // NPART: partition cursors
-    unsigned *mid, *big;       // N each: rows of 33..4096 and of more than 4096 entries
-    unsigned *cnt;             // [0] mid rows, [1] big rows, [2] errors
+    unsigned *mid, *big;       // N each: rows of 257..4096 and of more than 4096 entries
+    unsigned *cnt;             // [0] mid rows, [1] big rows, [2] errors, [3] big rows (split), [4..5] max length
+    // Big rows cut into 4096-entry tiles, spread over the whole grid: per
+    // big row its tile count, then (tp) the exclusive prefix of the counts;
+    // per tile two class counts and their prefixes (the SSSP split).
+    unsigned *tcnt;            // T: per big row tiles, then per tile tiny counts
+    unsigned *tcnt2;           // T: per tile light counts
+    uint64_t *tp;              // N + 1: tile prefix over the big rows
+    uint64_t *tq, *tq2;        // T + 1 each: prefixes of tcnt / tcnt2 over tiles
     uint64_t *scan;            // scan scratch
+    uint64_t tmax;             // T: tiles the per-tile arrays hold
     uint64_t bytes;
 };
+
+constexpr unsigned BIG_TILE = 4096;  // entries of a big row per block step (chunk sort, merge, split)
+
+// Tiles of all big rows: a row of L > BIG_TILE entries has at most
+// L / BIG_TILE + 1, and there are at most e / (BIG_TILE + 1) such rows.
+static uint64_t max_tiles(uint64_t n, uint64_t e) { return e / BIG_TILE + std::min(n, e / (BIG_TILE + 1)) + 1; }
 
 static SortWork carve_sort(void *base, uint64_t n, uint64_t e) {
     Carver c(base);
     SortWork w;
+    const uint64_t T = max_tiles(n, e);
+    w.tmax = T;
     w.tkey = c.take<unsigned long long>(e ? e : 1);
     w.tw = c.take<float>(e ? e : 1);
     w.rcur = c.take<unsigned>(n + 1);
@@ -75,7 +96,12 @@ static SortWork carve_sort(void *base, uint64_t n, uint64_t e) {
     w.mid = c.take<unsigned>(n);
     w.big = c.take<unsigned>(n);
     w.cnt = c.take<unsigned>(64);
-    w.scan = c.take<uint64_t>(scan_scratch_words(n));
+    w.tcnt = c.take<unsigned>(T);
+    w.tcnt2 = c.take<unsigned>(T);
+    w.tp = c.take<uint64_t>(n + 1);
+    w.tq = c.take<uint64_t>(T + 1);
+    w.tq2 = c.take<uint64_t>(T + 1);
+    w.scan = c.take<uint64_t>(scan_scratch_words(T > n ? T : n));
     w.bytes = c.used;
     return w;
 }
@@ -332,7 +358,51 @@ __global__ void __launch_bounds__(SORT_THREADS) csr_sort_mid_kernel(const uint64
     }
 }
 
-// A row's keys live either in the scratch array (u64) or in col/w.
+
+// Per big row its number of BIG_TILE tiles; the longest row's length.
+__global__ void big_tiles_kernel(const uint64_t *__restrict__ rowstarts, const unsigned *__restrict__ big,
+                                 unsigned nbig, unsigned *__restrict__ tcnt, unsigned long long *__restrict__ maxlen) {
+    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < nbig; k += gridDim.x * blockDim.x) {
+        const uint64_t L = rowstarts[big[k] + 1] - rowstarts[big[k]];
+        tcnt[k] = (unsigned)((L + BIG_TILE - 1) / BIG_TILE);
+        atomicMax(maxlen, (unsigned long long)L);
+    }
+}
+
+// Big row k of tile t: largest k with tp[k] <= t.
+__device__ __forceinline__ unsigned tile_row(const uint64_t *tp, unsigned nbig, uint64_t t) {
+    unsigned lo = 0, hi = nbig - 1;
+    while (lo < hi) {
+        const unsigned mid = (lo + hi + 1) >> 1;
+        if (tp[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Sorts every BIG_TILE chunk of every big row in shared memory (one block
+// per chunk, grid-stride over all chunks) into the scratch array.
+__global__ void __launch_bounds__(SORT_THREADS) csr_sort_chunks_kernel(const uint64_t *__restrict__ rowstarts,
+                                                                       const unsigned *__restrict__ big, unsigned nbig,
+                                                                       const uint64_t *__restrict__ tp, uint64_t ntiles,
+                                                                       unsigned long long *tkey, const int *col,
+                                                                       const float *w) {
+    __shared__ unsigned long long s[BIG_TILE];
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const unsigned k = tile_row(tp, nbig, t);
+        const uint64_t rb = rowstarts[big[k]], L = rowstarts[big[k] + 1] - rb;
+        const uint64_t c0 = (t - tp[k]) * BIG_TILE;
+        const unsigned cl = L - c0 < BIG_TILE ? (unsigned)(L - c0) : BIG_TILE;
+        const unsigned P = next_pow2(cl);
+        for (unsigned i = threadIdx.x; i < P; i += blockDim.x) s[i] = i < cl ? row_key(col, w, rb + c0 + i) : ~0ull;
+        __syncthreads();
+        block_bitonic(s, P);
+        for (unsigned i = threadIdx.x; i < cl; i += blockDim.x) tkey[rb + c0 + i] = s[i];
+        __syncthreads();
+    }
+}
+
+// A key array in either form: the scratch array (u64) or col/w.
 struct KeyBuf {
     unsigned long long *key;  // non-null: the scratch array
     int *col;
@@ -349,77 +419,85 @@ struct KeyBuf {
     }
 };
 
-// Merge of the sorted runs A = src[a, a + la) and B = src[b, b + lb) into
-// dst[a, a + la + lb) (b = a + la) by the whole block: each thread takes
-// MERGE_ITEMS consecutive outputs, finds where they start in A and B by a
-// binary search on the cross diagonal (merge path), and merges them.
-__device__ void block_merge(const KeyBuf &src, const KeyBuf &dst, uint64_t a, uint64_t la, uint64_t lb) {
-    const uint64_t b = a + la, total = la + lb;
-    for (uint64_t d0 = (uint64_t)threadIdx.x * MERGE_ITEMS; d0 < total; d0 += (uint64_t)blockDim.x * MERGE_ITEMS) {
-        // i = elements taken from A among the first d0 outputs
-        uint64_t lo = d0 > lb ? d0 - lb : 0, hi = d0 < la ? d0 : la;
-        while (lo < hi) {
-            const uint64_t i = (lo + hi) >> 1;  // A[i] vs B[d0 - 1 - i]
-            if (src.get(a + i) <= src.get(b + d0 - 1 - i)) lo = i + 1;
-            else hi = i;
+// Elements of A taken among the first d outputs of merging A[0, la) and
+// B[0, lb) (merge path; ties to A): the diagonal's crossing point.
+template <class GetA, class GetB>
+__device__ __forceinline__ uint64_t co_rank(uint64_t d, uint64_t la, uint64_t lb, GetA getA, GetB getB) {
+    uint64_t lo = d > lb ? d - lb : 0, hi = d < la ? d : la;
+    while (lo < hi) {
+        const uint64_t i = (lo + hi) >> 1;  // A[i] vs B[d - 1 - i]
+        if (getA(i) <= getB(d - 1 - i)) lo = i + 1;
+        else hi = i;
+    }
+    return lo;
+}
+
+// One merge pass over all big rows: sorted runs of R entries are merged
+// pairwise (a last run without a partner is copied).  Each block takes a
+// tile of BIG_TILE outputs of some row: it finds where the tile's outputs
+// start and end in the two runs (merge path on the row in memory), stages
+// those input ranges in shared memory and merges them there, each thread
+// placing 16 outputs after a merge-path search of its own in shared memory.
+__global__ void __launch_bounds__(SORT_THREADS) csr_merge_pass_kernel(const uint64_t *__restrict__ rowstarts,
+                                                                      const unsigned *__restrict__ big, unsigned nbig,
+                                                                      const uint64_t *__restrict__ tp, uint64_t ntiles,
+                                                                      uint64_t R, KeyBuf src, KeyBuf dst) {
+    __shared__ unsigned long long s[BIG_TILE];
+    __shared__ uint64_t s_i[2];
+    constexpr unsigned PER = BIG_TILE / SORT_THREADS;
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const unsigned k = tile_row(tp, nbig, t);
+        const uint64_t rb = rowstarts[big[k]], L = rowstarts[big[k] + 1] - rb;
+        const uint64_t o = (t - tp[k]) * BIG_TILE;
+        const uint64_t a0 = o / (2 * R) * (2 * R);
+        const uint64_t la = min(R, L - a0), b0 = a0 + la, lb = b0 < L ? min(R, L - b0) : 0;
+        const uint64_t d0 = o - a0, d1 = min(d0 + BIG_TILE, la + lb);
+        if (threadIdx.x < 2) {
+            const uint64_t d = threadIdx.x ? d1 : d0;
+            s_i[threadIdx.x] = co_rank(
+                d, la, lb, [&](uint64_t i) { return src.get(rb + a0 + i); },
+                [&](uint64_t j) { return src.get(rb + b0 + j); });
         }
-        uint64_t i = lo, j = d0 - lo;
-        const uint64_t dend = min(d0 + MERGE_ITEMS, total);
-        for (uint64_t d = d0; d < dend; ++d) {
-            const bool takeA = j >= lb || (i < la && src.get(a + i) <= src.get(b + j));
-            dst.set(a + d, takeA ? src.get(a + i++) : src.get(b + j++));
+        __syncthreads();
+        const uint64_t i0 = s_i[0], i1 = s_i[1], j0 = d0 - i0, j1 = d1 - i1;
+        const unsigned na = (unsigned)(i1 - i0), nb = (unsigned)(j1 - j0);
+        for (unsigned q = threadIdx.x; q < na + nb; q += blockDim.x)
+            s[q] = q < na ? src.get(rb + a0 + i0 + q) : src.get(rb + b0 + j0 + (q - na));
+        __syncthreads();
+        const unsigned q0 = threadIdx.x * PER;
+        if (q0 < na + nb) {
+            const unsigned long long *A = s, *B = s + na;
+            unsigned i = (unsigned)co_rank(
+                q0, na, nb, [&](uint64_t x) { return A[x]; }, [&](uint64_t y) { return B[y]; });
+            unsigned j = q0 - i;
+            const unsigned qe = min(q0 + PER, na + nb);
+            for (unsigned q = q0; q < qe; ++q) {
+                const bool takeA = j >= nb || (i < na && A[i] <= B[j]);
+                dst.set(rb + a0 + d0 + q, takeA ? A[i++] : B[j++]);
+            }
         }
+        __syncthreads();
     }
 }
 
-// Rows of more than 4096 entries: one block per row; 4096-entry chunks are
-// sorted in shared memory into the scratch array, then runs are merged
-// pairwise, the row going back and forth between the scratch array and
-// col/w, and finally copied to col/w (and col64).
-__global__ void __launch_bounds__(SORT_THREADS) csr_sort_big_kernel(const uint64_t *__restrict__ rowstarts,
-                                                                    const unsigned *__restrict__ big,
-                                                                    const unsigned *__restrict__ cnt,
-                                                                    unsigned long long *tkey, int *col, float *w,
-                                                                    uint64_t *col64) {
-    __shared__ unsigned long long s[SORT_SMEM_KEYS];
-    const unsigned nrows = cnt[1];
-    const KeyBuf K{tkey, nullptr, nullptr}, C{nullptr, col, w};
-    for (unsigned k = blockIdx.x; k < nrows; k += gridDim.x) {
-        const unsigned v = big[k];
-        const uint64_t rb = rowstarts[v];
-        const uint64_t L = rowstarts[v + 1] - rb;
-        for (uint64_t c0 = 0; c0 < L; c0 += SORT_SMEM_KEYS) {
-            const unsigned cl = L - c0 < SORT_SMEM_KEYS ? (unsigned)(L - c0) : SORT_SMEM_KEYS;
-            const unsigned P = next_pow2(cl);
-            for (unsigned i = threadIdx.x; i < P; i += blockDim.x) s[i] = i < cl ? row_key(col, w, rb + c0 + i) : ~0ull;
-            __syncthreads();
-            block_bitonic(s, P);
-            for (unsigned i = threadIdx.x; i < cl; i += blockDim.x) tkey[rb + c0 + i] = s[i];
-            __syncthreads();
-        }
-        bool in_scratch = true;
-        for (uint64_t R = SORT_SMEM_KEYS; R < L; R <<= 1) {
-            const KeyBuf &src = in_scratch ? K : C, &dst = in_scratch ? C : K;
-            for (uint64_t a = 0; a < L; a += 2 * R) {
-                const uint64_t la = min(R, L - a), lb = a + R < L ? min(R, L - a - R) : 0;
-                block_merge(KeyBuf{src.key ? src.key + rb : nullptr, src.col ? src.col + rb : nullptr,
-                                   src.w ? src.w + rb : nullptr},
-                            KeyBuf{dst.key ? dst.key + rb : nullptr, dst.col ? dst.col + rb : nullptr,
-                                   dst.w ? dst.w + rb : nullptr},
-                            a, la, lb);
-            }
-            __syncthreads();
-            in_scratch = !in_scratch;
-        }
-        for (uint64_t i = threadIdx.x; i < L; i += blockDim.x) {
-            const unsigned long long key = in_scratch ? tkey[rb + i] : row_key(col, w, rb + i);
-            if (in_scratch) {
+// Big rows back into col/w from the scratch array (after an odd number of
+// buffer swaps) and/or into col64.
+__global__ void csr_big_finish_kernel(const uint64_t *__restrict__ rowstarts, const unsigned *__restrict__ big,
+                                      unsigned nbig, const uint64_t *__restrict__ tp, uint64_t ntiles,
+                                      const unsigned long long *__restrict__ tkey, bool from_scratch, int *col,
+                                      float *w, uint64_t *col64) {
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const unsigned k = tile_row(tp, nbig, t);
+        const uint64_t rb = rowstarts[big[k]], L = rowstarts[big[k] + 1] - rb;
+        const uint64_t c0 = (t - tp[k]) * BIG_TILE, c1 = min(c0 + BIG_TILE, L);
+        for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+            const unsigned long long key = from_scratch ? tkey[rb + i] : row_key(col, w, rb + i);
+            if (from_scratch) {
                 col[rb + i] = (int)(unsigned)(key >> 32);
                 w[rb + i] = __uint_as_float((unsigned)key);
             }
             if (col64) col64[rb + i] = key >> 32;
         }
-        __syncthreads();
     }
 }
 
@@ -519,49 +597,76 @@ __global__ void csr_split_light_kernel(const uint64_t *__restrict__ rowstarts, c
     }
 }
 
-__global__ void __launch_bounds__(SORT_THREADS) csr_split_light_big_kernel(
-    const uint64_t *__restrict__ rowstarts, const int *__restrict__ col, const float *__restrict__ w, float light,
-    float tiny, int *__restrict__ scol, float *__restrict__ sw, unsigned *__restrict__ ld, unsigned *__restrict__ td,
-    const unsigned *__restrict__ big, const unsigned *__restrict__ nbig) {
-    constexpr int WARPS = SORT_THREADS / 32;
-    __shared__ unsigned s_cnt[3][WARPS];
-    __shared__ unsigned long long s_base[3];
-    const unsigned lane = lane_id(), wid = threadIdx.x >> 5;
-    for (unsigned k = blockIdx.x; k < *nbig; k += gridDim.x) {
-        const unsigned v = big[k];
-        const uint64_t rb = rowstarts[v], re = rowstarts[v + 1];
+// Big rows of the split, tiled as for the sort: per tile its tiny and light
+// entry counts (one block per tile) ...
+__global__ void __launch_bounds__(SORT_THREADS) csr_split_count_kernel(
+    const uint64_t *__restrict__ rowstarts, const float *__restrict__ w, const unsigned *__restrict__ big,
+    unsigned nbig, const uint64_t *__restrict__ tp, uint64_t ntiles, float light, float tiny,
+    unsigned *__restrict__ ct, unsigned *__restrict__ cl) {
+    __shared__ unsigned s_t, s_l;
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        if (threadIdx.x == 0) s_t = s_l = 0;
+        __syncthreads();
+        const unsigned k = tile_row(tp, nbig, t);
+        const uint64_t rb = rowstarts[big[k]], L = rowstarts[big[k] + 1] - rb;
+        const uint64_t c0 = (t - tp[k]) * BIG_TILE, c1 = min(c0 + BIG_TILE, L);
         unsigned nt = 0, nl = 0;
-        for (uint64_t i = rb + threadIdx.x; i < re; i += blockDim.x) {
-            const int c = light_class(w[i], light, tiny);
+        for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+            const int c = light_class(w[rb + i], light, tiny);
             nt += c == 0;
             nl += c <= 1;
         }
         nt = warp_sum(nt);
         nl = warp_sum(nl);
-        if (lane == 0) {
-            s_cnt[0][wid] = nt;
-            s_cnt[1][wid] = nl;
+        if (lane_id() == 0) {
+            atomicAdd(&s_t, nt);
+            atomicAdd(&s_l, nl);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            unsigned long long t = 0, l = 0;
-            for (int q = 0; q < WARPS; ++q) {
-                t += s_cnt[0][q];
-                l += s_cnt[1][q];
-            }
-            s_base[0] = rb;
-            s_base[1] = rb + t;
-            s_base[2] = rb + l;
-            ld[v] = (unsigned)l;
-            td[v] = (unsigned)t;
+            ct[t] = s_t;
+            cl[t] = s_l;
         }
         __syncthreads();
-        // Chunks of blockDim entries in order: per class, the warps' counts
-        // give each warp its offset inside the chunk.
-        for (uint64_t i0 = rb; i0 < re; i0 += blockDim.x) {
+    }
+}
+
+// ... then, with those counts scanned over all tiles (qt, ql), every tile
+// writes its entries of each class in order: tiny ones after the row's
+// earlier tiny ones, the other light ones after all the row's tiny ones,
+// heavy ones after all its light ones.  The block of a row's first tile also
+// writes the row's counts.
+__global__ void __launch_bounds__(SORT_THREADS) csr_split_write_kernel(
+    const uint64_t *__restrict__ rowstarts, const int *__restrict__ col, const float *__restrict__ w,
+    const unsigned *__restrict__ big, unsigned nbig, const uint64_t *__restrict__ tp, uint64_t ntiles, float light,
+    float tiny, const uint64_t *__restrict__ qt, const uint64_t *__restrict__ ql, int *__restrict__ scol,
+    float *__restrict__ sw, unsigned *__restrict__ ld, unsigned *__restrict__ td) {
+    constexpr int WARPS = SORT_THREADS / 32;
+    __shared__ unsigned s_cnt[3][WARPS];
+    __shared__ unsigned long long s_base[3];
+    const unsigned lane = lane_id(), wid = threadIdx.x >> 5;
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const unsigned k = tile_row(tp, nbig, t);
+        const unsigned v = big[k];
+        const uint64_t rb = rowstarts[v], L = rowstarts[v + 1] - rb;
+        const uint64_t f = tp[k], l = tp[k + 1];  // the row's tiles [f, l)
+        const uint64_t c0 = (t - f) * BIG_TILE, c1 = min(c0 + BIG_TILE, L);
+        const uint64_t T_row = qt[l] - qt[f], L_row = ql[l] - ql[f];
+        const uint64_t t_before = qt[t] - qt[f], l_before = ql[t] - ql[f];
+        if (threadIdx.x == 0) {
+            s_base[0] = rb + t_before;
+            s_base[1] = rb + T_row + (l_before - t_before);
+            s_base[2] = rb + L_row + (c0 - l_before);
+            if (t == f) {
+                ld[v] = (unsigned)L_row;
+                td[v] = (unsigned)T_row;
+            }
+        }
+        __syncthreads();
+        for (uint64_t i0 = c0; i0 < c1; i0 += blockDim.x) {
             const uint64_t i = i0 + threadIdx.x;
-            const bool has = i < re;
-            const float x = has ? w[i] : 0.0f;
+            const bool has = i < c1;
+            const float x = has ? w[rb + i] : 0.0f;
             const int c = has ? light_class(x, light, tiny) : 3;
             unsigned m[3];
 #pragma unroll
@@ -574,14 +679,14 @@ __global__ void __launch_bounds__(SORT_THREADS) csr_split_light_big_kernel(
                 uint64_t o = s_base[c];
                 for (unsigned q = 0; q < wid; ++q) o += s_cnt[c][q];
                 o += __popc(m[c] & lanemask_lt());
-                scol[o] = col[i];
+                scol[o] = col[rb + i];
                 sw[o] = x;
             }
             __syncthreads();
             if (threadIdx.x < 3) {
-                unsigned long long t = 0;
-                for (int q = 0; q < WARPS; ++q) t += s_cnt[threadIdx.x][q];
-                s_base[threadIdx.x] += t;
+                unsigned long long sum = 0;
+                for (int q = 0; q < WARPS; ++q) sum += s_cnt[threadIdx.x][q];
+                s_base[threadIdx.x] += sum;
             }
             __syncthreads();
         }
@@ -604,6 +709,32 @@ extern "C" int g5_csr_sorted_workspace_size(uint64_t nverts, uint64_t nentries, 
     return G5_OK;
 }
 
+// Tile prefix over the big rows listed in w.big (count in w.cnt[cidx]):
+// returns their number, their tiles and the longest row's length (one
+// synchronisation).
+static int big_rows_prepare(const uint64_t *d_rowstarts, const SortWork &w, int cidx, cudaStream_t st,
+                            unsigned *nbig, uint64_t *ntiles, unsigned long long *maxlen) {
+    G5_CUDA_TRY(cudaMemsetAsync(&w.cnt[4], 0, 2 * sizeof(unsigned), st));
+    unsigned nb = 0;
+    G5_CUDA_TRY(cudaMemcpyAsync(&nb, &w.cnt[cidx], sizeof nb, cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    *nbig = nb;
+    *ntiles = 0;
+    *maxlen = 0;
+    if (!nb) return G5_OK;
+    big_tiles_kernel<<<std::max(1u, std::min(nb / 256 + 1, 1024u)), 256, 0, st>>>(
+        d_rowstarts, w.big, nb, w.tcnt, (unsigned long long *)&w.cnt[4]);
+    int rc = scan_u32_to_u64(w.tcnt, nb, w.tp, w.scan, st);
+    if (rc) return rc;
+    G5_CUDA_TRY(cudaMemcpyAsync(ntiles, w.tp + nb, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaMemcpyAsync(maxlen, &w.cnt[4], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    if (*ntiles > w.tmax)
+        return set_error(G5_ERR_INVALID, "canonical CSR: rows hold more entries than nentries (%llu tiles > %llu)",
+                         (unsigned long long)*ntiles, (unsigned long long)w.tmax);
+    return G5_OK;
+}
+
 // Sorts rows in place (any CSR: the rows of g5_csr_fill or of the fused
 // Kronecker fill come out canonical too).
 static int sort_rows(const uint64_t *d_rowstarts, uint64_t nverts, int32_t *d_col, float *d_w, uint64_t *d_col64,
@@ -613,8 +744,24 @@ static int sort_rows(const uint64_t *d_rowstarts, uint64_t nverts, int32_t *d_co
     const int wblocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sort_grid(8), (warps + 7) / 8));
     csr_sort_warp_kernel<<<wblocks, 256, 0, st>>>(d_rowstarts, nverts, d_col, d_w, d_col64, w.mid, w.big, w.cnt);
     csr_sort_mid_kernel<<<sort_grid(4), SORT_THREADS, 0, st>>>(d_rowstarts, w.mid, w.cnt, d_col, d_w, d_col64);
-    csr_sort_big_kernel<<<sort_grid(4), SORT_THREADS, 0, st>>>(d_rowstarts, w.big, w.cnt, w.tkey, d_col, d_w,
-                                                              d_col64);
+    G5_CUDA_TRY(cudaGetLastError());
+    unsigned nbig = 0;
+    uint64_t ntiles = 0;
+    unsigned long long maxlen = 0;
+    int rc = big_rows_prepare(d_rowstarts, w, 1, st, &nbig, &ntiles, &maxlen);
+    if (rc || !nbig) return rc;
+    const int grid = (int)std::min<uint64_t>(ntiles, (uint64_t)sort_grid(4));
+    csr_sort_chunks_kernel<<<grid, SORT_THREADS, 0, st>>>(d_rowstarts, w.big, nbig, w.tp, ntiles, w.tkey, d_col, d_w);
+    const KeyBuf K{w.tkey, nullptr, nullptr}, C{nullptr, d_col, d_w};
+    bool in_scratch = true;
+    for (uint64_t R = BIG_TILE; R < maxlen; R <<= 1) {
+        csr_merge_pass_kernel<<<grid, SORT_THREADS, 0, st>>>(d_rowstarts, w.big, nbig, w.tp, ntiles, R,
+                                                             in_scratch ? K : C, in_scratch ? C : K);
+        in_scratch = !in_scratch;
+    }
+    if (in_scratch || d_col64)
+        csr_big_finish_kernel<<<grid, 256, 0, st>>>(d_rowstarts, w.big, nbig, w.tp, ntiles, w.tkey, in_scratch, d_col,
+                                                    d_w, d_col64);
     G5_CUDA_TRY(cudaGetLastError());
     return G5_OK;
 }
@@ -729,9 +876,20 @@ extern "C" int g5_csr_split_light(const uint64_t *d_rowstarts, const int32_t *d_
     const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sort_grid(8), (nverts + 7) / 8));
     csr_split_light_kernel<<<blocks, 256, 0, st>>>(d_rowstarts, d_col, d_w, nverts, light_delta, tiny, d_scol, d_sw,
                                                    d_light_deg, d_tiny_deg, w.big, &w.cnt[3]);
-    csr_split_light_big_kernel<<<sort_grid(2), SORT_THREADS, 0, st>>>(d_rowstarts, d_col, d_w, light_delta, tiny,
-                                                                     d_scol, d_sw, d_light_deg, d_tiny_deg, w.big,
-                                                                     &w.cnt[3]);
+    G5_CUDA_TRY(cudaGetLastError());
+    unsigned nbig = 0;
+    uint64_t ntiles = 0;
+    unsigned long long maxlen = 0;
+    int rc = big_rows_prepare(d_rowstarts, w, 3, st, &nbig, &ntiles, &maxlen);
+    if (rc || !nbig) return rc;
+    const int grid = (int)std::min<uint64_t>(ntiles, (uint64_t)sort_grid(4));
+    csr_split_count_kernel<<<grid, SORT_THREADS, 0, st>>>(d_rowstarts, d_w, w.big, nbig, w.tp, ntiles, light_delta,
+                                                          tiny, w.tcnt, w.tcnt2);
+    if ((rc = scan_u32_to_u64(w.tcnt, ntiles, w.tq, w.scan, st))) return rc;
+    if ((rc = scan_u32_to_u64(w.tcnt2, ntiles, w.tq2, w.scan, st))) return rc;
+    csr_split_write_kernel<<<grid, SORT_THREADS, 0, st>>>(d_rowstarts, d_col, d_w, w.big, nbig, w.tp, ntiles,
+                                                          light_delta, tiny, w.tq, w.tq2, d_scol, d_sw, d_light_deg,
+                                                          d_tiny_deg);
     G5_CUDA_TRY(cudaGetLastError());
     return G5_OK;
 }

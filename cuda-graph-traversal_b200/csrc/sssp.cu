@@ -56,10 +56,12 @@ constexpr int SSSP_TRACE = 256;      // phases recorded in the control block
 // into SSSP_CHUNK chunks across the grid), and a warp grabs at most SSSP_GRAB
 // small entries at once: a grab holds at most SSSP_GRAB x SSSP_BIG_DEG edges,
 // so no warp is left with a long tail of relaxations at the end of a phase.
+// Both are defaults of g5_sssp_params.big_deg / .chunk.
 constexpr unsigned SSSP_BIG_DEG = 128;
 // Chunk of a long row taken by one warp in the frontier, heavy-set and
 // expanded-set lists.  A warp's relaxation steps form a chain of dependent
-// round trips, so the chunk bounds the longest warp of a phase.
+// round trips, so the chunk bounds the longest warp of a phase.  A multiple
+// of 32 x SSSP_EDGES (the entries a warp step covers).
 constexpr unsigned SSSP_CHUNK = 256;
 constexpr unsigned SSSP_GRAB = 32;
 // Sub-buckets: once a bucket's light frontier holds SPLIT_MIN light entries,
@@ -210,6 +212,8 @@ struct SsspArgs {
     unsigned nblocks;
     unsigned long long limit_ns;
     bool check_opens;  // opens exchange their stamps and flag a vertex met twice (DEVERR_DUPLICATE)
+    unsigned big_deg;  // list entries with more edges to expand go to the chunked big part
+    unsigned chunk;    // edges of a big entry per warp grab
 };
 
 __device__ __forceinline__ float pack_dist(unsigned long long p) { return __uint_as_float((unsigned)(p >> 32)); }
@@ -363,13 +367,13 @@ __device__ __forceinline__ void push_same_bucket(const SsspArgs &a, const PushCt
     // Each vertex enters a frontier once per phase and a heavy set once per
     // bucket, so no list exceeds n entries.
     bool ok = frontier_append_staged(x.st.f, x.Fout, x.FBout, a.n, &c->sn.f_small[x.f_slot], &c->sn.f_big[x.f_slot], f, v,
-                                     le - lb, SSSP_BIG_DEG, SSSP_CHUNK);
+                                     le - lb, a.big_deg, a.chunk);
     ok &= frontier_append_staged(x.st.s, x.Sl, x.SBl, a.n, &c->sn.s_small[x.s_slot], &c->sn.s_big[x.s_slot], s, v, he - hb,
-                                 SSSP_BIG_DEG, SSSP_CHUNK);
+                                 a.big_deg, a.chunk);
     // Once per vertex and sub-bucket, so the set stays within n entries.
     if (x.sub_mode)
         ok &= frontier_append_staged(x.st.d, x.Dl, x.DBl, a.n, &c->sn.d_small[x.d_slot], &c->sn.d_big[x.d_slot], d, v,
-                                     dl, SSSP_BIG_DEG, SSSP_CHUNK);
+                                     dl, a.big_deg, a.chunk);
     if (!ok) atomicOr(&c->error, DEVERR_CAPACITY | site_bit(SITE_PUSH));
 }
 
@@ -738,9 +742,9 @@ __device__ void expand_list(const SsspArgs &a, const PushCtx &x, Counts &k, cons
         const float du = pack_dist(pu);
         if (heavy && ch == cfirst && lane == 0) settle(a, sparse_out, u, pu);
         const uint64_t deg = re - rb;
-        const uint64_t cs = (uint64_t)(ch - cfirst) * SSSP_CHUNK;
-        const uint64_t ce = min(cs + SSSP_CHUNK, deg);
-        for (uint64_t e0 = cs + lane; e0 < cs + SSSP_CHUNK; e0 += 32 * SSSP_EDGES) {
+        const uint64_t cs = (uint64_t)(ch - cfirst) * a.chunk;
+        const uint64_t ce = min(cs + a.chunk, deg);
+        for (uint64_t e0 = cs + lane; e0 < cs + a.chunk; e0 += 32 * SSSP_EDGES) {
             EdgeProbe p;
 #pragma unroll
             for (int t = 0; t < SSSP_EDGES; ++t) {
@@ -992,7 +996,12 @@ __device__ __forceinline__ void trace_phase(SsspCtl *c, unsigned phase, int kind
     }
 }
 
-__global__ void __launch_bounds__(SSSP_THREADS, 4) sssp_persistent_kernel(SsspArgs a) {
+// Blocks per SM the register allocation is sized for (64 registers a thread
+// at 4).
+#ifndef SSSP_MIN_BLOCKS
+#define SSSP_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(SSSP_THREADS, SSSP_MIN_BLOCKS) sssp_persistent_kernel(SsspArgs a) {
     SsspCtl *c = a.ctl;
     __shared__ float s_bnd[RING + 1];
     __shared__ float s_sub[SUB + 1];
@@ -1674,6 +1683,9 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     g5_sssp_params p = {0.1f, 0, 0.0f, 0, 0, nullptr, 0};
     if (params) p = *params;
     G5_CHECK_ARG(p.delta > 0.0f, "g5_sssp_traverse: delta must be positive");
+    G5_CHECK_ARG(p.big_deg >= 0 && p.big_deg <= (1 << 20), "%s: big_deg %d outside [0, 2^20]", who, p.big_deg);
+    G5_CHECK_ARG(p.chunk >= 0 && p.chunk <= (1 << 16) && p.chunk % (32 * SSSP_EDGES) == 0,
+                 "%s: chunk %d is not a multiple of %d in [0, 65536]", who, p.chunk, 32 * SSSP_EDGES);
     int max_blocks = 0;
     if ((rc = sssp_max_blocks(&max_blocks))) return rc;
     int blocks = p.blocks > 0 ? std::min(p.blocks, max_blocks)
@@ -1722,6 +1734,8 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     a.nblocks = (unsigned)blocks;
     a.limit_ns = wait_limit_ns();
     a.check_opens = p.check_opens != 0;
+    a.big_deg = p.big_deg ? (unsigned)p.big_deg : SSSP_BIG_DEG;
+    a.chunk = p.chunk ? (unsigned)p.chunk : SSSP_CHUNK;
     void *args[] = {&a};
     if (p.small && !d_roots)
         sssp_small_kernel<<<1, SSSP_THREADS, 0, st>>>(a);

@@ -173,6 +173,11 @@ typedef struct g5_bfs_params {
                        3 = one lean block, top-down (a root in a small component; g5_bfs_query picks
                        it from the main-component bitmap)                                             */
     int32_t blocks; /* persistent grid size; 0 = fill the device                                          */
+    /* Work tiles (0 = default; none changes a result, only the speed):                                  */
+    int32_t big_deg;      /* queue entries with more edges are cut into chunks across the grid (1024)     */
+    int32_t chunk;        /* edges per chunk, a multiple of 32 up to 65536 (256)                          */
+    int32_t lane_entries; /* bottom-up: entries of a row one lane scans before its warp joins, a multiple
+                             of 4 up to 1024 (8)                                                          */
 } g5_bfs_params;
 
 typedef struct g5_bfs_stats {
@@ -333,6 +338,10 @@ typedef struct g5_sssp_params {
                        stamps atomically and fail the search (G5_ERR_DEVICE,
                        "held a vertex twice") if a queue held a vertex twice;
                        a test aid, same results; 0 = plain stores (default) */
+    int32_t big_deg; /* list entries with more edges to expand are cut into
+                       chunks across the grid; 0 = default (128)            */
+    int32_t chunk;   /* edges per chunk, a multiple of 64 up to 65536; 0 =
+                       default (256).  Neither tile changes a result        */
 } g5_sssp_params;
 
 int g5_sssp_workspace_size(uint64_t nverts, uint64_t *bytes);
