@@ -172,18 +172,20 @@ def run_ours(args):
     # ---- setup (untimed): generation + CSR build on the GPU, as the runner.
     t0 = time.time()
     seed = G.make_mrg_seed(2, 3)
-    ev0, ev1, ev2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    ev0, ev1, ev2, ev3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
     ev0.record()
     tg = G.generate_kronecker_range(seed, scale, 0, m, device=dev)
     ev1.record()
-    g = G.oned_graph_from_tuple_graph(tg, n, with_main=False)
+    g = G.oned_graph_from_tuple_graph(tg, n, with_main=False, bfs_order=False)
     ev2.record()
+    del tg
+    G.oned_graph_bfs_order(g)  # the BFS's copy of the column, rows by decreasing neighbour degree
+    ev3.record()
     torch.cuda.synchronize()
-    gen_s, csr_s = ev0.elapsed_time(ev1) / 1e3, ev1.elapsed_time(ev2) / 1e3
+    gen_s, csr_s, order_s = ev0.elapsed_time(ev1) / 1e3, ev1.elapsed_time(ev2) / 1e3, ev2.elapsed_time(ev3) / 1e3
     t_main = time.perf_counter()
     g.main_bits = G.main_component_bitmap(g)  # one BFS from the hub: routes small-component roots
     main_s = time.perf_counter() - t_main
-    del tg
     torch.cuda.empty_cache()
     roots_all = G.generate_bfs_roots(g, 2, 3, 64)
     my_roots = rank_roots(roots_all, rank, world)
@@ -197,6 +199,31 @@ def run_ours(args):
     G.oned_graph_bfs_reset(bfs_s, with_depth=False, g=g)
     state = lambda r: bfs if g.in_main_component(r) else bfs_s  # noqa: E731
     vw = G._val_work(g)
+
+    # Knobs of the main-component searches (alpha, beta and the work tiles
+    # for BFS; the list tiles for SSSP at the reference's delta 0.1), tuned
+    # on roots that are not timed (another root seed: 8 for BFS, 2 for SSSP)
+    # or taken from the cache; the grid stays the library's (roots outside
+    # the main component keep their one-block searches).
+    tuned, bparams, skw = None, None, {}
+    if not args.no_tune:
+        import cgt_b200.autotune as T
+        t_tune = time.time()
+        cache = T.TuningCache(args.tune_cache)
+        hits = (cache.get("bfs", g) is not None, cache.get("sssp", g) is not None)
+        troots = [r for r in G.generate_bfs_roots(g, 5, 7, 64) if g.in_main_component(r)][:8]
+        tb = cache.get("bfs", g) or T.tune_bfs(g, troots, alphas=(10.0, 14.0, 20.0), betas=(24.0,), grids=(0,), reps=2)
+        ts = cache.get("sssp", g) or T.tune_sssp(g, troots[:2], deltas=(0.1,), grids=(0,), pulls=(0.0,), subs=(0,))
+        if rank == 0:
+            cache.put("bfs", g, tb)
+            cache.put("sssp", g, ts)
+        bparams = T.bfs_params(tb)
+        skw = {"big_deg": ts["big_deg"], "chunk": ts["chunk"]}
+        tuned = {"bfs": {k: tb[k] for k in ("alpha", "beta", "big_deg", "chunk", "lane_entries")},
+                 "sssp": {k: ts[k] for k in ("delta", "big_deg", "chunk")}, "from_cache": list(hits),
+                 "tune_s": round(time.time() - t_tune, 2), "tuning_roots": [int(r) for r in troots]}
+    bp = lambda r: bparams if g.in_main_component(r) else None  # noqa: E731
+
     nedge, reached = {}, {}
     for r in set(seq):
         G.oned_graph_bfs_run(g, bfs, r, with_depth=False)
@@ -222,7 +249,7 @@ def run_ours(args):
     # them, so the reset time is reported too.
     for r in seq[:W]:
         G.oned_graph_bfs_reset(state(r), with_depth=False, g=g)
-        G.oned_graph_bfs_traverse(g, state(r), r, with_depth=False)
+        G.oned_graph_bfs_traverse(g, state(r), r, bp(r), with_depth=False)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
             torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     if pg:
@@ -240,7 +267,7 @@ def run_ours(args):
             a.record()
             G.oned_graph_bfs_reset(bs, with_depth=False, g=g)
             b.record()
-            G.oned_graph_bfs_traverse(g, bs, r, with_depth=False)
+            G.oned_graph_bfs_traverse(g, bs, r, bp(r), with_depth=False)
             c.record()
         stop.record()
         torch.cuda.synchronize()
@@ -273,7 +300,7 @@ def run_ours(args):
     sstate = lambda r: sssp if g.in_main_component(r) else sssp_s  # noqa: E731
     for r in seq[:W]:
         G.oned_graph_sssp_reset(sstate(r))
-        G.oned_graph_sssp_traverse(g, sstate(r), r)
+        G.oned_graph_sssp_traverse(g, sstate(r), r, **skw)
     sev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
             torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     torch.cuda.synchronize()
@@ -285,7 +312,7 @@ def run_ours(args):
         sev[i][0].record()
         G.oned_graph_sssp_reset(ss)
         sev[i][1].record()
-        G.oned_graph_sssp_traverse(g, ss, r)
+        G.oned_graph_sssp_traverse(g, ss, r, **skw)
         sev[i][2].record()
         # Every search's status is read (a device error -- a bounded wait
         # that expired, a list overflow -- raises) and its result validated
@@ -317,7 +344,7 @@ def run_ours(args):
             t = time.perf_counter()
             # one public call: the device reads the root from pinned host
             # memory, searches, and writes the statistics back to it
-            res = G.oned_graph_bfs_query(g, state(r), int(r))
+            res = G.oned_graph_bfs_query(g, state(r), int(r), params=bparams)
             reps.append(time.perf_counter() - t)
             assert res.reached == reached[r]
         e2e_s.append(float(np.median(reps)))
@@ -405,6 +432,7 @@ def run_ours(args):
                                   "bytes_per_launch": int(np.mean(s_alg_bytes)),
                                   "bytes_model": "2*nedge*8 (col + w) + reached*(8 rowstarts + 8 packed + 12 out)"}},
             "construction": {"generation_s": round(gen_s, 4), "csr_build_s": round(csr_s, 4),
+                             "bfs_degree_order_s": round(order_s, 4),
                              "main_component_s": round(main_s, 4), "setup_total_s": round(setup_s, 2),
                              "note": "device events; the CSR build includes its first-use allocations"},
             "nedge_per_root": int(np.median(t_nedge)),
@@ -415,6 +443,7 @@ def run_ours(args):
         if cpu:
             line["cpu_baseline"] = cpu
         line["parity"] = parity
+        line["autotuned"] = tuned
         if world == 1:
             del g, bfs, bfs_s, vw, sssp, sssp_s, state, sstate  # the SCALE-26 graph is not needed any more
             torch.cuda.empty_cache()
@@ -763,6 +792,9 @@ def headline(line):
          "bfs_roofline_frac": line["roofline"]["frac"], "e2e_hmean_gteps": line["e2e"]["value"],
          "sssp_hmean_gteps": line["sssp"]["value"], "sssp_median_gteps": line["sssp"]["median_gteps"],
          "sssp_roofline_frac": line["sssp"]["roofline"]["frac"], "parity": line.get("parity")}
+    t = line.get("autotuned")
+    if t:
+        h["tuned"] = {"bfs": t["bfs"], "sssp": t["sssp"]}
     if "cpu_baseline" in line:
         h["cpu_hmean_gteps"] = line["cpu_baseline"]["value"]
     rg = line.get("reference_gpu")
@@ -864,6 +896,9 @@ def main():
     ap.add_argument("--packed-min-scale", type=int, default=10)
     ap.add_argument("--packed-max-scale", type=int, default=18)
     ap.add_argument("--no-packed", action="store_true", help="skip the packed many-graph measurement")
+    ap.add_argument("--no-tune", action="store_true", help="headline searches on the library's default knobs")
+    ap.add_argument("--tune-cache", default=os.path.join(REPO, "cuda-graph-traversal_b200", "tuned.json"),
+                    help="JSON cache of the headline searches' tuned knobs (keyed by device and graph size)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per BFS launch (read+write) to report beside the roofline")
     args = ap.parse_args()

@@ -78,6 +78,8 @@ def _load() -> C.CDLL:
         "g5_csr_sorted_workspace_size": ([u64, u64, p], C.c_int),
         "g5_csr_fill_sorted": ([p, p, u64, u64, p, u64, p, u64, p, p, p, p], C.c_int),
         "g5_csr_sort_rows": ([p, u64, u64, p, p, p, p, u64, p], C.c_int),
+        "g5_csr_degree_order_workspace_size": ([u64, u64, p], C.c_int),
+        "g5_csr_degree_order": ([p, p, u64, u64, p, p, u64, p], C.c_int),
         "g5_csr_dedupe_count": ([p, p, u64, u64, p, p, u64, p, p], C.c_int),
         "g5_csr_dedupe_copy": ([p, p, p, u64, p, p, p, p, p], C.c_int),
         "g5_csr_split_light": ([p, p, p, u64, u64, f32, p, p, p, p, p, u64, p], C.c_int),
@@ -274,6 +276,13 @@ class OnedGraph:
     # are in that layout themselves (packed graphs).
     scol: torch.Tensor | None = None
     sw: torch.Tensor | None = None
+    # The BFS copy of the column (g5_csr_degree_order): each row's
+    # neighbours by decreasing degree.  None: the BFS reads col.
+    bcol: torch.Tensor | None = None
+
+    @property
+    def bfs_col(self) -> torch.Tensor:
+        return self.col if self.bcol is None else self.bcol
 
     @property
     def sssp_col(self) -> torch.Tensor:
@@ -299,16 +308,39 @@ class OnedGraph:
         return self.rowstarts.device
 
 
-def _sorted_work(n: int, e: int, dev) -> torch.Tensor:
+def _sorted_work(n: int, e: int, dev, bfs_order: bool = False) -> torch.Tensor:
+    """Scratch of the canonical build (and of g5_csr_degree_order, which
+    needs a little more, when bfs_order)."""
     nb = C.c_uint64()
-    _check(lib.g5_csr_sorted_workspace_size(n, e, C.byref(nb)))
+    _check((lib.g5_csr_degree_order_workspace_size if bfs_order else lib.g5_csr_sorted_workspace_size)(
+        n, e, C.byref(nb)))
     return _workspace(nb.value, dev)
 
 
+def oned_graph_bfs_order(g: OnedGraph, stream=None, work: torch.Tensor | None = None) -> OnedGraph:
+    """Gives the BFS its own copy of the column with every row's neighbours
+    by decreasing degree (g5_csr_degree_order; col itself, the CSR the
+    validators and the reference API see, keeps its canonical order).
+    Costs 4 bytes per CSR entry; BFS depths are unchanged (the parents are
+    other tree edges of the same graph).  `work`: scratch of at least
+    g5_csr_degree_order_workspace_size bytes, else one is allocated."""
+    n, e = g.nglobalverts, g.nlocaledges
+    nb = C.c_uint64()
+    _check(lib.g5_csr_degree_order_workspace_size(n, e, C.byref(nb)))
+    if work is None or work.numel() < nb.value:
+        work = _workspace(nb.value, g.device)
+    bcol = torch.empty(max(e, 1), dtype=torch.int32, device=g.device)
+    _check(lib.g5_csr_degree_order(_ptr(g.rowstarts), _ptr(g.col), n, e, _ptr(bcol), _ptr(work), work.numel(),
+                                   _stream(stream)))
+    g.bcol = bcol
+    return g
+
+
 def _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, dev, stream,
-                  with_main) -> OnedGraph:
+                  with_main, bfs_order) -> OnedGraph:
     """Canonical rows (already sorted) -> optional dedupe -> the SSSP copy
-    (g5_csr_split_light) -> isolated bitmap and main component."""
+    (g5_csr_split_light) -> the BFS copy (g5_csr_degree_order, when
+    bfs_order) -> isolated bitmap and main component."""
     if dedupe:
         rs2 = torch.empty(n + 1, dtype=torch.int64, device=dev)
         e2 = C.c_uint64()
@@ -335,6 +367,8 @@ def _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st,
     g = OnedGraph(n, e, rowstarts, col[:e], w[:e], light[:n], light_delta, None if col64 is None else col64[:e], iso)
     g.tiny_deg = tiny[:n]
     g.scol, g.sw = scol[:e], sw[:e]
+    if bfs_order:
+        oned_graph_bfs_order(g, stream, work)
     if with_main:
         g.main_bits = main_component_bitmap(g, stream)
     return g
@@ -342,7 +376,7 @@ def _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st,
 
 def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: float = 0.1,
                                 with_column64: bool = False, stream=None, with_main: bool = True,
-                                dedupe: bool = False) -> OnedGraph:
+                                dedupe: bool = False, bfs_order: bool = True) -> OnedGraph:
     """oned_graph_from_tuple_graph (src/traversal.h:43): the CSR of both
     directions of every non-loop edge, duplicates kept, every row in
     canonical order (sorted by neighbour, then weight bits:
@@ -350,7 +384,9 @@ def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: 
     (g.scol / g.sw, g5_csr_split_light).  dedupe=True keeps one entry per
     (row, neighbour), the lightest (not the reference's CSR: its TEPS edge
     counts include duplicates).  with_main=False skips the main-component
-    search (g.main_bits = None; set it later with main_component_bitmap)."""
+    search (g.main_bits = None; set it later with main_component_bitmap).
+    bfs_order=False skips the BFS's degree-ordered copy of the column
+    (g.bcol; oned_graph_bfs_order makes it later)."""
     dev = tg.edges.device
     n, m = int(nglobalverts), tg.edges_size
     nb = C.c_uint64()
@@ -366,10 +402,11 @@ def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: 
     col = torch.empty(max(e, 1), dtype=torch.int32, device=dev)
     w = torch.empty(max(e, 1), dtype=torch.float32, device=dev)
     col64 = torch.empty(max(e, 1), dtype=torch.int64, device=dev) if with_column64 else None
-    work = _sorted_work(n, e, dev)
+    work = _sorted_work(n, e, dev, bfs_order)
     _check(lib.g5_csr_fill_sorted(_ptr(tg.edges), _ptr(tg.weights), m, n, _ptr(rowstarts), e, _ptr(work),
                                   work.numel(), _ptr(col), _ptr(w), _ptr(col64), st))
-    return _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, dev, stream, with_main)
+    return _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, dev, stream, with_main,
+                         bfs_order)
 
 
 def _split_tiny(rowstarts, col, w, col64, light, n: int, light_delta: float, st) -> torch.Tensor:
@@ -382,7 +419,7 @@ def _split_tiny(rowstarts, col, w, col64, light, n: int, light_delta: float, st)
 
 def oned_graph_from_kronecker(seed, log_n: int, nedges: int, device="cuda", light_delta: float = 0.1,
                               with_column64: bool = False, stream=None, with_main: bool = True,
-                              dedupe: bool = False) -> OnedGraph:
+                              dedupe: bool = False, bfs_order: bool = True) -> OnedGraph:
     """generate_kronecker_range + oned_graph_from_tuple_graph in one step,
     with the generator fused into the CSR passes (no edge list in memory);
     rows then sorted into canonical order (g5_csr_sort_rows) -- the same
@@ -407,10 +444,11 @@ def oned_graph_from_kronecker(seed, log_n: int, nedges: int, device="cuda", ligh
     _check(lib.g5_csr_fill_kronecker(s, log_n, nedges, _ptr(rowstarts), float("inf"), _ptr(cwork), cwork.numel(),
                                      _ptr(col), _ptr(w), None, _ptr(light), st))
     del cwork, light
-    work = _sorted_work(n, e, device)
+    work = _sorted_work(n, e, device, bfs_order)
     _check(lib.g5_csr_sort_rows(_ptr(rowstarts), n, e, _ptr(col), _ptr(w), _ptr(col64), _ptr(work), work.numel(),
                                 st))
-    return _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, device, stream, with_main)
+    return _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, device, stream, with_main,
+                         bfs_order)
 
 
 # ------------------------------------------------------- packed graphs ----
@@ -461,7 +499,7 @@ def pack_kronecker(scales, edgefactor: int = 16, seed1_base: int = 2, seed2: int
     def gen():
         for i, s in enumerate(scales):
             g = oned_graph_from_kronecker(make_mrg_seed(seed1_base + i, seed2), s, edgefactor << s, device=device,
-                                          light_delta=light_delta, stream=stream, with_main=False)
+                                          light_delta=light_delta, stream=stream, with_main=False, bfs_order=False)
             r = generate_bfs_roots(g, 2, 3, 1)
             roots.append(r[0] if r else 0)
             yield g
@@ -505,7 +543,7 @@ def oned_graph_bfs_traverse_multi(g: OnedGraph, bfs: "BfsState", d_roots: torch.
                                   with_depth: bool = True, stream=None) -> None:
     """BFS from every root in d_roots (device int64) at once
     (g5_bfs_traverse_multi); reset bfs first."""
-    _check(lib.g5_bfs_traverse_multi(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, _ptr(d_roots), d_roots.numel(),
+    _check(lib.g5_bfs_traverse_multi(_ptr(g.rowstarts), _ptr(g.bfs_col), g.nglobalverts, _ptr(d_roots), d_roots.numel(),
                                      _ptr(bfs.pred), _ptr(bfs.depth) if with_depth else None, _ptr(bfs.work),
                                      bfs.work.numel(), C.byref(params) if params is not None else None,
                                      _stream(stream)))
@@ -587,7 +625,7 @@ def main_component_bitmap(g: OnedGraph, stream=None) -> np.ndarray:
     bfs = BfsState(g)
     _check(lib.g5_bfs_reset(g.nglobalverts, _ptr(bfs.pred), None, None, _ptr(bfs.work), bfs.work.numel(),
                             _stream(stream)))
-    _check(lib.g5_bfs_traverse(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, hub, _ptr(bfs.pred), None,
+    _check(lib.g5_bfs_traverse(_ptr(g.rowstarts), _ptr(g.bfs_col), g.nglobalverts, hub, _ptr(bfs.pred), None,
                                _ptr(bfs.work), bfs.work.numel(), None, _stream(stream)))
     bits = torch.empty((g.nglobalverts + 31) // 32, dtype=torch.int32, device=g.device)
     _check(lib.g5_bfs_visited_bitmap(_ptr(bfs.work), bfs.work.numel(), g.nglobalverts, _ptr(bits),
@@ -712,7 +750,7 @@ def oned_graph_bfs_traverse(g: OnedGraph, bfs: BfsState, root: int, params: BfsP
     """Second half of oned_graph_bfs_run: the persistent BFS kernel alone
     (one block for a root outside the main component)."""
     params = _right_sized(g, root, params)
-    _check(lib.g5_bfs_traverse(_ptr(g.rowstarts), _ptr(g.col), g.nglobalverts, root, _ptr(bfs.pred),
+    _check(lib.g5_bfs_traverse(_ptr(g.rowstarts), _ptr(g.bfs_col), g.nglobalverts, root, _ptr(bfs.pred),
                                _ptr(bfs.depth) if with_depth else None, _ptr(bfs.work), bfs.work.numel(),
                                C.byref(params) if params is not None else None, _stream(stream)))
 
@@ -730,32 +768,36 @@ def _main_bits_ptr(g: OnedGraph) -> int | None:
 
 
 def oned_graph_bfs_query(g: OnedGraph, bfs: BfsState, root: int, with_depth: bool = False,
-                         stream=None) -> BfsStats:
+                         stream=None, params: BfsParams | None = None) -> BfsStats:
     """One search end to end from the host, the reference's synchronous
     oned_graph_bfs_run on a state reset since its last search: the root goes
     to the device as a launch argument, the device writes the statistics to
     pinned host memory, and the host waits on them.  Runs through a
     g5_bfs_query_plan made on the first query of this state with this graph,
-    depth choice and stream (C ABI: two arguments per query)."""
+    depth choice, stream and params (C ABI: two arguments per query); with
+    params.blocks == 0 a root outside the main component still gets the
+    one-block search."""
     st = _stream(stream)
     plan = bfs._plan
-    if plan is None or plan[0] is not g or plan[1] != with_depth or plan[2] != st or plan[4] is not g.main_bits:
-        plan = _make_query_plan(g, bfs, with_depth, st)
+    if (plan is None or plan[0] is not g or plan[1] != with_depth or plan[2] != st or plan[4] is not g.main_bits
+            or plan[5] is not params or plan[6] is not g.bfs_col):
+        plan = _make_query_plan(g, bfs, with_depth, st, params)
     rc = _plan_run(plan[3], root)
     if rc:
         _check(rc)
     return bfs.h_stats
 
 
-def _make_query_plan(g: OnedGraph, bfs: BfsState, with_depth: bool, st):
+def _make_query_plan(g: OnedGraph, bfs: BfsState, with_depth: bool, st, params: BfsParams | None = None):
     bfs.drop_plan()
     h = C.c_void_p()
-    _check(lib.g5_bfs_query_plan_create(g.rowstarts.data_ptr(), g.col.data_ptr(), g.nglobalverts, _main_bits_ptr(g),
+    _check(lib.g5_bfs_query_plan_create(g.rowstarts.data_ptr(), g.bfs_col.data_ptr(), g.nglobalverts, _main_bits_ptr(g),
                                         bfs.pred.data_ptr(), bfs.depth.data_ptr() if with_depth else None,
-                                        bfs.work.data_ptr(), bfs.work.numel(), None, C.byref(bfs.h_stats), st,
+                                        bfs.work.data_ptr(), bfs.work.numel(),
+                                        C.byref(params) if params is not None else None, C.byref(bfs.h_stats), st,
                                         C.byref(h)))
-    # The graph is held with the plan: the plan keeps its device pointers.
-    bfs._plan = (g, with_depth, st, h.value, g.main_bits)
+    # The graph (and params) are held with the plan: the plan keeps its device pointers.
+    bfs._plan = (g, with_depth, st, h.value, g.main_bits, params, g.bfs_col)
     return bfs._plan
 
 

@@ -57,9 +57,11 @@ def _descend(time_of, base: dict, axes: dict) -> tuple[float, dict, int]:
     best_ms = time_of(best)
     count = 1
     for name, values in axes.items():
+        tried = {best[name]}  # timed already, as part of best
         for v in values:
-            if v == best[name]:
+            if v in tried:
                 continue
+            tried.add(v)
             trial = dict(best, **{name: v})
             ms = time_of(trial)
             count += 1
@@ -70,6 +72,9 @@ def _descend(time_of, base: dict, axes: dict) -> tuple[float, dict, int]:
 
 BFS_TILES = {"chunk": (128, 256, 512, 1024), "big_deg": (256, 1024, 4096), "lane_entries": (4, 8, 16, 32)}
 SSSP_TILES = {"chunk": (128, 256, 512, 1024), "big_deg": (64, 128, 256, 512)}
+# The library's defaults (what 0 in g5_bfs_params / g5_sssp_params selects).
+BFS_DEFAULT_TILES = {"big_deg": 1024, "chunk": 256, "lane_entries": 8}
+SSSP_DEFAULT_TILES = {"big_deg": 256, "chunk": 256}
 
 
 def tune_bfs(g: OnedGraph, roots, alphas=(6.0, 10.0, 14.0, 20.0, 28.0), betas=(12.0, 24.0, 48.0), grids=None,
@@ -101,7 +106,7 @@ def tune_bfs(g: OnedGraph, roots, alphas=(6.0, 10.0, 14.0, 20.0, 28.0), betas=(1
     out = {"alpha": best[1], "beta": best[2], "blocks": best[3], "big_deg": 0, "chunk": 0, "lane_entries": 0}
     ms, count = best[0], len(table)
     if tiles:
-        out.update(big_deg=1024, chunk=256, lane_entries=8)  # the library's defaults, spelled out
+        out.update(**BFS_DEFAULT_TILES)  # the library's defaults, spelled out
         ms, out, more = _descend(time_of, out, tiles)
         count += more
     return {"kind": "bfs", **out, "ms": round(ms, 4), "candidates": count}
@@ -137,7 +142,7 @@ def tune_sssp(g: OnedGraph, roots, deltas=(0.08, 0.1, 0.2, 0.4), grids=None, pul
     out = {"delta": best[1], "blocks": best[2], "pull": best[3], "sub_min": best[4], "big_deg": 0, "chunk": 0}
     ms, count = best[0], len(table)
     if tiles:
-        out.update(big_deg=128, chunk=256)
+        out.update(**SSSP_DEFAULT_TILES)
         ms, out, more = _descend(time_of, out, tiles)
         count += more
     return {"kind": "sssp", **out, "ms": round(ms, 4), "candidates": count}

@@ -15,6 +15,7 @@ namespace g5compat {
 
 struct GraphExt {
     int32_t *col;        // int32 neighbour ids, rows in canonical order (as Oned_Graph.column)
+    int32_t *bcol;       // the BFS copy (g5_csr_degree_order): rows by decreasing neighbour degree
     int32_t *scol;       // the SSSP copy (g5_csr_split_light): tiny | light | heavy rows
     float *sw;           // its weights
     uint32_t *light_deg; // light entries per row

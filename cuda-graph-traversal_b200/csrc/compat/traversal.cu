@@ -33,6 +33,7 @@ Oned_Graph oned_graph_from_tuple_graph(Worker_State *ws, Tuple_Graph *tg, u64 ng
     GraphExt x;
     const uint64_t e = g.nlocaledges;
     x.col = (int32_t *)gpu_push(ws, e * sizeof(int32_t), "int32 column");
+    x.bcol = (int32_t *)gpu_push(ws, e * sizeof(int32_t), "BFS column");
     x.scol = (int32_t *)gpu_push(ws, e * sizeof(int32_t), "SSSP column");
     x.sw = (float *)gpu_push(ws, e * sizeof(float), "SSSP weights");
     x.light_deg = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "light degrees");
@@ -40,10 +41,11 @@ Oned_Graph oned_graph_from_tuple_graph(Worker_State *ws, Tuple_Graph *tg, u64 ng
     x.light_delta = kLightDelta;
     x.main_host = nullptr;
     x.isolated = (uint32_t *)gpu_push(ws, (nglobalverts + 31) / 32 * sizeof(uint32_t), "isolated-vertex bitmap");
-    // Rows in canonical order (sorted by neighbour, then weight), and the
-    // SSSP copy; the sorting scratch is the arena's last push, popped after.
+    // Rows in canonical order (sorted by neighbour, then weight), the SSSP
+    // copy and the BFS copy; the sorting scratch (sized for the degree
+    // order, the largest of the three) is the arena's last push, popped after.
     uint64_t sbytes = 0;
-    check(ws, g5_csr_sorted_workspace_size(nglobalverts, e, &sbytes), "oned_graph_from_tuple_graph");
+    check(ws, g5_csr_degree_order_workspace_size(nglobalverts, e, &sbytes), "oned_graph_from_tuple_graph");
     const Arena before_sort = ws->gpu_arena;
     void *swork = gpu_push(ws, sbytes, "CSR sorting scratch");
     check(ws,
@@ -53,6 +55,8 @@ Oned_Graph oned_graph_from_tuple_graph(Worker_State *ws, Tuple_Graph *tg, u64 ng
     check(ws,
           g5_csr_split_light(g.rowstarts, x.col, g.weights, nglobalverts, e, kLightDelta, x.scol, x.sw, x.light_deg,
                              x.tiny_deg, swork, sbytes, 0),
+          "oned_graph_from_tuple_graph");
+    check(ws, g5_csr_degree_order(g.rowstarts, x.col, nglobalverts, e, x.bcol, swork, sbytes, 0),
           "oned_graph_from_tuple_graph");
     CHECK_CUDA(cudaDeviceSynchronize());
     ws->gpu_arena = before_sort;
@@ -103,7 +107,7 @@ Bfs_State oned_graph_bfs_create(Worker_State *ws, const Oned_Graph *g) {
         const u64 words = (g->nglobalverts + 31) / 32;
         check(ws, g5_bfs_reset(g->nglobalverts, bfs.pred, nullptr, nullptr, x.work, x.work_bytes, 0),
               "oned_graph_bfs_create");
-        check(ws, g5_bfs_traverse(g->rowstarts, gx->col, g->nglobalverts, hub, bfs.pred, nullptr, x.work, x.work_bytes,
+        check(ws, g5_bfs_traverse(g->rowstarts, gx->bcol, g->nglobalverts, hub, bfs.pred, nullptr, x.work, x.work_bytes,
                                   nullptr, 0),
               "oned_graph_bfs_create");
         uint32_t *bits = (uint32_t *)gpu_push(ws, words * sizeof(uint32_t), "component bitmap");
@@ -148,7 +152,7 @@ void oned_graph_bfs_run(Worker_State *ws, const Oned_Graph *g, Bfs_State *bfs, u
     // protocol calls before every search (examples/graph500_runner.cu:309).
     *bx->root_host = root;
     g5_bfs_stats *st = (g5_bfs_stats *)(bx->root_host + 1);
-    check(ws, g5_bfs_query(g->rowstarts, gx->col, g->nglobalverts, bx->root_host, gx->main_host, bfs->pred, bx->depth,
+    check(ws, g5_bfs_query(g->rowstarts, gx->bcol, g->nglobalverts, bx->root_host, gx->main_host, bfs->pred, bx->depth,
                            bx->work, bx->work_bytes, nullptr, st, 0),
           "oned_graph_bfs_run");
 }

@@ -432,8 +432,20 @@ __device__ __forceinline__ uint64_t co_rank(uint64_t d, uint64_t la, uint64_t lb
     return lo;
 }
 
-// One merge pass over all big rows: sorted runs of R entries are merged
-// pairwise (a last run without a partner is copied).  Each block takes a
+// Merge passes a big row of L entries goes through: one per run length
+// R = BIG_TILE * 2^i below L.  Pass 1 writes col/w from the scratch array,
+// pass 2 the scratch array, and so on, so after its passes a row sits in
+// col/w when their number is odd.
+__device__ __forceinline__ int merge_passes(uint64_t L) {
+    const uint64_t tiles = (L + BIG_TILE - 1) / BIG_TILE;
+    int p = 0;
+    while ((1ull << p) < tiles) ++p;
+    return p;
+}
+
+// One merge pass over the big rows longer than R: sorted runs of R entries
+// are merged pairwise (a last run without a partner is copied); shorter
+// rows are sorted already and stay where they are.  Each block takes a
 // tile of BIG_TILE outputs of some row: it finds where the tile's outputs
 // start and end in the two runs (merge path on the row in memory), stages
 // those input ranges in shared memory and merges them there, each thread
@@ -448,6 +460,7 @@ __global__ void __launch_bounds__(SORT_THREADS) csr_merge_pass_kernel(const uint
     for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const unsigned k = tile_row(tp, nbig, t);
         const uint64_t rb = rowstarts[big[k]], L = rowstarts[big[k] + 1] - rb;
+        if (L <= R) continue;  // the same t for the whole block
         const uint64_t o = (t - tp[k]) * BIG_TILE;
         const uint64_t a0 = o / (2 * R) * (2 * R);
         const uint64_t la = min(R, L - a0), b0 = a0 + la, lb = b0 < L ? min(R, L - b0) : 0;
@@ -480,15 +493,17 @@ __global__ void __launch_bounds__(SORT_THREADS) csr_merge_pass_kernel(const uint
     }
 }
 
-// Big rows back into col/w from the scratch array (after an odd number of
-// buffer swaps) and/or into col64.
+// Big rows whose passes left them in the scratch array (an even number)
+// back into col/w, and every big row into col64 when it is wanted.
 __global__ void csr_big_finish_kernel(const uint64_t *__restrict__ rowstarts, const unsigned *__restrict__ big,
                                       unsigned nbig, const uint64_t *__restrict__ tp, uint64_t ntiles,
-                                      const unsigned long long *__restrict__ tkey, bool from_scratch, int *col,
-                                      float *w, uint64_t *col64) {
+                                      const unsigned long long *__restrict__ tkey, int *col, float *w,
+                                      uint64_t *col64) {
     for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const unsigned k = tile_row(tp, nbig, t);
         const uint64_t rb = rowstarts[big[k]], L = rowstarts[big[k] + 1] - rb;
+        const bool from_scratch = merge_passes(L) % 2 == 0;
+        if (!from_scratch && !col64) continue;
         const uint64_t c0 = (t - tp[k]) * BIG_TILE, c1 = min(c0 + BIG_TILE, L);
         for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
             const unsigned long long key = from_scratch ? tkey[rb + i] : row_key(col, w, rb + i);
@@ -538,6 +553,32 @@ __global__ void csr_unique_copy_kernel(const uint64_t *__restrict__ rowstarts, c
             }
             out += __popc(m);
         }
+    }
+}
+
+// ------------------------------------------------------- BFS degree order
+
+// deg[v] = entries of row v (saturated at 2^32 - 1).
+__global__ void row_lengths_kernel(const uint64_t *__restrict__ rowstarts, uint64_t n, unsigned *__restrict__ deg) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        const uint64_t d = rowstarts[v + 1] - rowstarts[v];
+        deg[v] = d > 0xffffffffull ? 0xffffffffu : (unsigned)d;
+    }
+}
+
+// Sort keys of every entry: (~deg(neighbour), neighbour) in the (col, w)
+// slots the row sort orders by, so sorted rows list their neighbours by
+// decreasing degree, ties by index.
+__global__ void degree_keys_kernel(const int *__restrict__ col, uint64_t e, const unsigned *__restrict__ deg,
+                                   uint64_t n, int *__restrict__ ka, float *__restrict__ kb,
+                                   unsigned *__restrict__ err) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < e; i += stride) {
+        const unsigned v = (unsigned)__ldg(&col[i]);
+        if (v >= n) atomicOr(err, SORTERR_RANGE);
+        ka[i] = (int)(0xffffffffu - (v < n ? __ldg(&deg[v]) : 0u));
+        kb[i] = __uint_as_float(v);
     }
 }
 
@@ -759,9 +800,7 @@ static int sort_rows(const uint64_t *d_rowstarts, uint64_t nverts, int32_t *d_co
                                                              in_scratch ? K : C, in_scratch ? C : K);
         in_scratch = !in_scratch;
     }
-    if (in_scratch || d_col64)
-        csr_big_finish_kernel<<<grid, 256, 0, st>>>(d_rowstarts, w.big, nbig, w.tp, ntiles, w.tkey, in_scratch, d_col,
-                                                    d_w, d_col64);
+    csr_big_finish_kernel<<<grid, 256, 0, st>>>(d_rowstarts, w.big, nbig, w.tp, ntiles, w.tkey, d_col, d_w, d_col64);
     G5_CUDA_TRY(cudaGetLastError());
     return G5_OK;
 }
@@ -855,6 +894,41 @@ extern "C" int g5_csr_dedupe_copy(const uint64_t *d_rowstarts, const int32_t *d_
     csr_unique_copy_kernel<<<blocks, 256, 0, st>>>(d_rowstarts, d_col, d_w, nverts, d_rowstarts_out, d_col_out,
                                                    d_w_out, d_col64_out);
     G5_CUDA_TRY(cudaGetLastError());
+    return G5_OK;
+}
+
+extern "C" int g5_csr_degree_order_workspace_size(uint64_t nverts, uint64_t nentries, uint64_t *bytes) {
+    G5_CHECK_ARG(bytes, "g5_csr_degree_order_workspace_size: bytes is NULL");
+    *bytes = carve_sort(nullptr, nverts, nentries).bytes + align_up(nentries * 4, 256) + align_up(nverts * 4, 256);
+    return G5_OK;
+}
+
+extern "C" int g5_csr_degree_order(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
+                                   uint64_t nentries, int32_t *d_out_col, void *d_work, uint64_t work_bytes,
+                                   void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_csr_degree_order: nverts outside [1, 2^31]");
+    G5_CHECK_ARG(d_rowstarts && d_work && (nentries == 0 || (d_col && d_out_col)),
+                 "g5_csr_degree_order: NULL argument");
+    G5_CHECK_ARG(nentries == 0 || d_out_col != d_col, "g5_csr_degree_order: d_out_col must not be d_col");
+    uint64_t need = 0;
+    g5_csr_degree_order_workspace_size(nverts, nentries, &need);
+    if (work_bytes < need) return set_error(G5_ERR_WORKSPACE, "g5_csr_degree_order: workspace too small");
+    if (nentries == 0) return G5_OK;
+    SortWork w = carve_sort(d_work, nverts, nentries);
+    int *ka = (int *)((char *)d_work + w.bytes);
+    unsigned *deg = (unsigned *)((char *)ka + align_up(nentries * 4, 256));
+    cudaStream_t st = (cudaStream_t)stream;
+    G5_CUDA_TRY(cudaMemsetAsync(&w.cnt[2], 0, sizeof(unsigned), st));
+    row_lengths_kernel<<<sort_grid(8), 256, 0, st>>>(d_rowstarts, nverts, deg);
+    degree_keys_kernel<<<sort_grid(8), 256, 0, st>>>(d_col, nentries, deg, nverts, ka, (float *)d_out_col, &w.cnt[2]);
+    G5_CUDA_TRY(cudaGetLastError());
+    int rc = sort_rows(d_rowstarts, nverts, ka, (float *)d_out_col, nullptr, w, st);
+    if (rc) return rc;
+    unsigned errs = 0;
+    G5_CUDA_TRY(cudaMemcpyAsync(&errs, &w.cnt[2], sizeof errs, cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    if (errs) return set_error(G5_ERR_INVALID, "g5_csr_degree_order: a column entry is not a vertex");
     return G5_OK;
 }
 

@@ -57,7 +57,7 @@ constexpr int SSSP_TRACE = 256;      // phases recorded in the control block
 // small entries at once: a grab holds at most SSSP_GRAB x SSSP_BIG_DEG edges,
 // so no warp is left with a long tail of relaxations at the end of a phase.
 // Both are defaults of g5_sssp_params.big_deg / .chunk.
-constexpr unsigned SSSP_BIG_DEG = 128;
+constexpr unsigned SSSP_BIG_DEG = 256;
 // Chunk of a long row taken by one warp in the frontier, heavy-set and
 // expanded-set lists.  A warp's relaxation steps form a chain of dependent
 // round trips, so the chunk bounds the longest warp of a phase.  A multiple
@@ -434,7 +434,10 @@ __device__ __forceinline__ void push_fine(const SsspArgs &a, const PushCtx &x, i
 // Edges of one warp step, E per lane: their target vertices' settled bits
 // and packed distances are loaded together before any is used, so the
 // step costs one chain of memory round trips, not E.
-constexpr int SSSP_EDGES = 2;
+#ifndef SSSP_EDGES_PER_LANE
+#define SSSP_EDGES_PER_LANE 2
+#endif
+constexpr int SSSP_EDGES = SSSP_EDGES_PER_LANE;
 
 struct EdgeProbe {
     unsigned v[SSSP_EDGES];
@@ -996,10 +999,12 @@ __device__ __forceinline__ void trace_phase(SsspCtl *c, unsigned phase, int kind
     }
 }
 
-// Blocks per SM the register allocation is sized for (64 registers a thread
-// at 4).
+// Blocks per SM the register allocation is sized for: 3 (80 registers a
+// thread) spills 48 bytes a thread where 4 (64 registers) spilled 250, at
+// the same S26 search time; 2 (128 registers, no spills) leaves too few
+// warps to hide the relaxations' latency (5 % slower).
 #ifndef SSSP_MIN_BLOCKS
-#define SSSP_MIN_BLOCKS 4
+#define SSSP_MIN_BLOCKS 3
 #endif
 __global__ void __launch_bounds__(SSSP_THREADS, SSSP_MIN_BLOCKS) sssp_persistent_kernel(SsspArgs a) {
     SsspCtl *c = a.ctl;

@@ -153,6 +153,17 @@ int g5_csr_split_light(const uint64_t *d_rowstarts, const int32_t *d_col, const 
                        uint64_t nentries, float light_delta, int32_t *d_scol, float *d_sw, uint32_t *d_light_deg,
                        uint32_t *d_tiny_deg, void *d_work, uint64_t work_bytes, void *stream);
 
+/* The BFS copy of a CSR's column: every row's neighbours ordered by
+ * decreasing degree, ties by index (d_out_col, nentries entries, distinct
+ * from d_col).  A bottom-up level then probes a vertex's best-connected
+ * neighbours first, the ones most likely to be in the frontier.  Any
+ * order of a row gives the same BFS depths; the parents chosen may differ
+ * (every one is valid).  Scratch: g5_csr_degree_order_workspace_size.  No
+ * counterpart in the reference. */
+int g5_csr_degree_order_workspace_size(uint64_t nverts, uint64_t nentries, uint64_t *bytes);
+int g5_csr_degree_order(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t nentries,
+                        int32_t *d_out_col, void *d_work, uint64_t work_bytes, void *stream);
+
 /* Packs disjoint graphs into one CSR (no counterpart in the reference, which
  * holds one graph): copies one graph's CSR into the destination at vertex
  * offset vbase and entry offset ebase, shifting its column by vbase.  Call
@@ -339,7 +350,7 @@ typedef struct g5_sssp_params {
                        "held a vertex twice") if a queue held a vertex twice;
                        a test aid, same results; 0 = plain stores (default) */
     int32_t big_deg; /* list entries with more edges to expand are cut into
-                       chunks across the grid; 0 = default (128)            */
+                       chunks across the grid; 0 = default (256)            */
     int32_t chunk;   /* edges per chunk, a multiple of 64 up to 65536; 0 =
                        default (256).  Neither tile changes a result        */
 } g5_sssp_params;

@@ -26,6 +26,14 @@ def test_exports_every_declared_symbol(cgt):
     assert not missing, missing
 
 
+def test_python_mirror_binds_every_function(cgt):
+    """Every declared function has a ctypes signature in the Python mirror
+    (an unbound one would pass 64-bit pointers and sizes as C ints).
+    g5_bfs_run_static is bound by its own test."""
+    unbound = [n for n in header_functions() if n != "g5_bfs_run_static" and getattr(cgt.lib, n).argtypes is None]
+    assert not unbound, unbound
+
+
 def test_host_functions_match_reference(cgt, golden_host):
     for k in golden_host["make_mrg_seed"]:
         assert cgt.make_mrg_seed(k["s1"], k["s2"]) == k["seed"]

@@ -20,7 +20,10 @@ def test_tuned_settings_keep_results(cgt, g, tmp_path):
     _, maxb = cgt.search_grid("bfs", g.nglobalverts)
     tb = T.tune_bfs(g, roots, alphas=(10.0, 14.0), betas=(24.0,), grids=(0, maxb),
                     tiles={"chunk": (64, 256), "big_deg": (32, 1024), "lane_entries": (4, 8)})
-    assert tb["candidates"] == 4 + 3 and tb["ms"] > 0  # the grid, then one new value per tile axis
+    # the 4 direction/grid settings, then the defaults' tiles and every other value of each axis
+    tiles = {"chunk": (64, 256), "big_deg": (32, 1024), "lane_entries": (4, 8)}
+    others = sum(len(set(v) - {T.BFS_DEFAULT_TILES[k]}) for k, v in tiles.items())
+    assert tb["candidates"] == 4 + 1 + others and tb["ms"] > 0
     assert tb["chunk"] in (64, 256) and tb["big_deg"] in (32, 1024) and tb["lane_entries"] in (4, 8)
     bfs = cgt.BfsState(g)
     cgt.oned_graph_bfs_run(g, bfs, roots[0])

@@ -148,3 +148,37 @@ def test_fill_sorted_rejects_changed_edges(cgt):
                                     g.nlocaledges, work.data_ptr(), work.numel(), col.data_ptr(), w.data_ptr(), None,
                                     None)
     assert rc == -1 and b"differ" in cgt.lib.g5_last_error()
+
+
+def test_degree_order_copy(cgt):
+    """g5_csr_degree_order: every row of the BFS copy holds the row's
+    entries by decreasing neighbour degree, ties by index (rows of every
+    size class, a hub of 150k included); BFS depths on it equal those on
+    the canonical column and its parent trees validate."""
+    rng = np.random.default_rng(4)
+    n = 1 << 18
+    lens = [3, 40, 300, 5000, 150_000]
+    e = [np.stack([np.full(L, 7 + i), rng.integers(0, n, L)], 1) for i, L in enumerate(lens)]
+    e.append(rng.integers(0, n, size=(400_000, 2)))
+    e = np.concatenate(e).astype(np.int64)
+    e = e[e[:, 0] != e[:, 1]]
+    tg = cgt.TupleGraph(torch.from_numpy(e).cuda(), torch.ones(e.shape[0], device="cuda"), e.shape[0])
+    g = cgt.oned_graph_from_tuple_graph(tg, n)
+    cgt.oned_graph_bfs_order(g)
+    rs = _np(g.rowstarts).astype(np.int64)
+    col, bcol = _np(g.col).astype(np.int64), _np(g.bcol).astype(np.int64)
+    deg = np.diff(rs)
+    src = np.repeat(np.arange(n), deg)
+    order = np.lexsort((col, -deg[col], src))  # numpy: rows by (-degree, index)
+    assert np.array_equal(bcol, col[order])
+    vw = cgt._val_work(g)
+    bfs = cgt.BfsState(g)
+    for r in (7, 11, int(e[-1, 0])):
+        bcol_t, g.bcol = g.bcol, None
+        cgt.oned_graph_bfs_run(g, bfs, r)
+        want = bfs.depth.clone()
+        g.bcol = bcol_t
+        cgt.oned_graph_bfs_run(g, bfs, r)
+        assert torch.equal(bfs.depth, want)
+        d = cgt.bfs_compute_dist_from_pred(g, bfs, r)
+        assert cgt.bfs_validate(g, r, bfs.pred, d, vw) == 0

@@ -444,3 +444,47 @@ def test_sssp_delta_too_small_is_an_error(cgt, graphs):
         cgt.sssp_status(ss)
     cgt.oned_graph_sssp_run(g, ss, r)
     assert cgt.sssp_status(ss)[0] > 0
+
+
+@pytest.mark.parametrize("shape", ["dense", "sparse_runs"])
+def test_validation_tile_table_edge_cases(cgt, oracle, shape):
+    """The validators and the edge count find each entry's row from a
+    per-tile table (built by a pre-pass) or, for graphs denser than the
+    table allows, by searching rowptr; tiles whose span includes long runs
+    of empty rows fall back to a per-entry search.  Every path gives the
+    oracle's counts, with and without planted mistakes."""
+    rng = np.random.default_rng(11)
+    if shape == "dense":  # 400 entries per vertex on average: more tiles than the table holds
+        n = 96
+        e = rng.integers(0, 64, size=(19_200, 2))  # vertices 64..95 stay unreached
+    else:  # a few busy vertices separated by thousands of isolated ones
+        n = 1 << 16
+        busy = rng.choice(n, 40, replace=False)
+        e = np.stack([rng.choice(busy, 60_000), rng.choice(busy, 60_000)], 1)
+    e = e[e[:, 0] != e[:, 1]].astype(np.int64)
+    wt = rng.random(e.shape[0], dtype=np.float32)
+    tg = cgt.TupleGraph(torch.from_numpy(e).cuda(), torch.from_numpy(wt).cuda(), e.shape[0])
+    g = cgt.oned_graph_from_tuple_graph(tg, n)
+    ors, ocol, ocw = _np(g.rowstarts).view(np.uint64), _np(g.col), _np(g.w)
+    vw = cgt._val_work(g)
+    bfs, s = cgt.BfsState(g), cgt.SsspState(g)
+    r = int(e[0, 0])
+    cgt.oned_graph_bfs_run(g, bfs, r)
+    dist = cgt.bfs_compute_dist_from_pred(g, bfs, r)
+    pred = _np(bfs.pred)
+    assert cgt.bfs_validate(g, r, bfs.pred, dist, vw) == 0
+    assert cgt.edge_count(g, bfs.pred, vw) == oracle.edge_count(ors, ocol, n, pred) > 0
+    for bad in _corruptions(pred, n, r, rng):
+        bfs.pred.copy_(torch.from_numpy(bad))
+        odist = oracle.bfs_dist_from_pred(ors, ocol, n, bad, r)
+        gd = cgt.bfs_compute_dist_from_pred(g, bfs, r)
+        assert np.array_equal(_np(gd), odist)
+        assert cgt.bfs_validate(g, r, bfs.pred, gd, vw) == oracle.bfs_validate(ors, ocol, n, r, bad, odist)
+        assert cgt.edge_count(g, bfs.pred, vw) == oracle.edge_count(ors, ocol, n, bad)
+    cgt.oned_graph_sssp_run(g, s, r)
+    assert cgt.sssp_validate(g, r, s.dist, s.pred, vw) == 0
+    cd = _np(s.dist).copy()
+    cd[np.nonzero(cd > 0)[0][:3]] *= np.float32(1.5)
+    cp = _np(s.pred)
+    want = oracle.sssp_validate(ors, ocol, ocw, n, r, cd, cp)
+    assert cgt.sssp_validate(g, r, torch.from_numpy(cd).cuda(), s.pred, vw) == want > 0
