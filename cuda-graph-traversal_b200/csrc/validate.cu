@@ -4,19 +4,17 @@
 // The BFS rules and the edge count are the runner's
 // (examples/graph500_runner.cu:84-201): same rules, same error count.  The
 // reference walks each row with one thread (a hub row of millions of entries
-// serialises on that thread); here every edge pass is edge-parallel: a block
-// takes a tile of 4096 CSR entries, caches the row starts of the rows the
-// tile spans in shared memory, and each thread walks 16 consecutive entries,
-// finding its first row by a binary search in shared memory and the next
-// ones by stepping forward -- no per-entry search through rowptr in memory.
-// (A tile spanning more rows than the cache holds -- many empty rows --
-// searches rowptr per entry instead.)  The first row of every tile comes
-// from a pre-pass (one thread per tile, all searches in parallel), so no
-// block waits on a 26-step dependent search through rowptr per tile.  A
-// neighbour's two values the rules compare (BFS: dist and pred; SSSP: dist
-// and pred) are packed by a pre-pass into one 16-byte record, so each entry
-// reads one sector of it; a thread issues the record loads of its 16
-// entries before it tests any of them.
+// serialises on that thread); here every edge pass is edge-parallel and
+// free of block barriers: a warp takes a tile of 512 consecutive CSR
+// entries, each lane 16 of them.  The rows the warp tile spans come from a
+// pre-pass table (the row of every tile's first entry, all searched in
+// parallel); a lane finds the row of its first entry by a binary search
+// inside that span (a few row starts, cached) and steps forward from row to
+// row.  The column is read 16 bytes at a time.  A neighbour's two values
+// the rules compare (BFS: dist and pred; SSSP: dist and pred) are packed by
+// a pre-pass into one 16-byte record, so each entry reads one sector of
+// it; a lane issues the record loads of its 16 entries before it tests any
+// of them.
 //
 // HBM bytes per pass: E * 4 (col) [+ E * 4 w] + one random 16-byte record
 // per entry (a 32-byte sector).
@@ -25,9 +23,9 @@
 namespace g5 {
 
 constexpr int VAL_THREADS = 256;
-constexpr int VAL_ITEMS = 16;                       // consecutive entries a thread walks
-constexpr int VAL_TILE = VAL_THREADS * VAL_ITEMS;   // entries per tile
-constexpr unsigned VAL_SPAN = 4096;                 // row starts cached per tile
+constexpr int VAL_WTILE = 512;  // entries per warp tile (the tile table's unit)
+constexpr int COUNT_ITEMS = 16; // consecutive entries a lane takes per step: edge count
+constexpr int RULE_ITEMS = 8;   //   the validators (their neighbour records held in registers)
 
 // Largest v in [lo, hi] with rowptr[v] <= e.
 __device__ __forceinline__ uint64_t row_of(const uint64_t *__restrict__ rowptr, uint64_t lo, uint64_t hi, uint64_t e) {
@@ -39,101 +37,100 @@ __device__ __forceinline__ uint64_t row_of(const uint64_t *__restrict__ rowptr, 
     return lo;
 }
 
-// Tile table: trow[t] = row of entry t * VAL_TILE for every tile t, and
-// trow[ntiles] = row of the last entry, when the table has room (the
-// pre-pass sets ok[0]).
+// Tile table: trow[t] = row of entry t * VAL_WTILE for every warp tile t,
+// and trow[ntiles] = row of the last entry, when the table has room (the
+// pre-pass then sets ok[0]).
 __global__ void val_tile_rows_kernel(const uint64_t *__restrict__ rowptr, uint64_t n, unsigned *__restrict__ trow,
                                      uint64_t cap, unsigned long long *__restrict__ ok) {
     const uint64_t E = rowptr[n];
-    const uint64_t ntiles = (E + VAL_TILE - 1) / VAL_TILE;
-    if (E == 0 || ntiles + 1 > cap) return;  // ok stays 0: tiles search rowptr themselves
+    const uint64_t ntiles = (E + VAL_WTILE - 1) / VAL_WTILE;
+    if (E == 0 || ntiles + 1 > cap) return;  // ok stays 0: lanes search all of rowptr themselves
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t <= ntiles; t += stride)
-        trow[t] = (unsigned)row_of(rowptr, 0, n - 1, t < ntiles ? t * VAL_TILE : E - 1);
+        trow[t] = (unsigned)row_of(rowptr, 0, n - 1, t < ntiles ? t * VAL_WTILE : E - 1);
     if (blockIdx.x == 0 && threadIdx.x == 0) *ok = 1;
 }
 
-// Row span of the tile [e0, e1) of the CSR, into shared memory: from the
-// tile table when it is there (the row of the next tile's first entry
-// bounds the span; rows beyond the tile's last entry start after it and are
-// never stepped into), else by two searches.
-__device__ __forceinline__ void tile_rows(const uint64_t *__restrict__ rowptr, uint64_t n, uint64_t e0, uint64_t e1,
-                                          const unsigned *__restrict__ trow, bool table, uint64_t *s_lo,
-                                          uint64_t *s_hi) {
-    if (threadIdx.x == 0) {
+// Every CSR entry, warp tile by warp tile: calls visit(u, eb, ne, c) per
+// lane and step with the lane's ne <= ITEMS consecutive entries eb.. (u[k]
+// the row of entry eb + k, c[k] its column entry; lanes past the last
+// entry have ne = 0).  A warp tile of VAL_WTILE entries takes
+// VAL_WTILE / (32 ITEMS) steps.  No block barrier: each warp runs on its
+// own.  With the table, the rows a warp tile spans are known (the row of
+// the next tile's first entry bounds them; rows after a lane's entries
+// start beyond them and are never stepped into).  When they are fewer
+// than 32, lane j holds the start of the tile's j-th row (one coalesced
+// load) and each lane finds the row of its first entry by a 5-step binary
+// search over the lanes (shuffles); otherwise it searches rowptr.  From
+// there a lane steps forward with one compare per entry.  All 32 lanes
+// call it.
+template <int ITEMS, class Visit>
+__device__ __forceinline__ void warp_walk(const uint64_t *__restrict__ rowptr, const int *__restrict__ col, uint64_t n,
+                                          uint64_t E, const unsigned *__restrict__ trow, bool table, Visit visit) {
+    static_assert(ITEMS % 4 == 0 && VAL_WTILE % (32 * ITEMS) == 0, "whole int4 loads, whole steps");
+    const unsigned lane = lane_id();
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t * VAL_WTILE < E; t += nwarps) {
+        uint64_t lo = 0, hi = n - 1;
         if (table) {
-            const uint64_t t = e0 / VAL_TILE;
-            *s_lo = __ldg(&trow[t]);
-            *s_hi = __ldg(&trow[t + 1]);
-        } else {
-            *s_lo = row_of(rowptr, 0, n - 1, e0);
-            *s_hi = row_of(rowptr, *s_lo, n - 1, e1 - 1);
+            lo = __ldg(&trow[t]);
+            hi = __ldg(&trow[t + 1]);
         }
-    }
-    __syncthreads();
-}
-
-// Entries of tile [e0, e1): calls visit(u, eb, ne, c) once per thread with
-// the thread's ne <= 16 consecutive entries eb.. (u[k] the row of entry
-// eb + k, c[k] its column entry).  Thread t takes [e0 + 16 t, e0 + 16 t +
-// 16).  The tile's row starts are cached in s_rp (when its rows fit) and
-// each thread steps from row to row; the column is read 16 bytes at a time
-// where it is aligned.  Every thread of the block calls it.
-template <class Visit>
-__device__ __forceinline__ void tile_walk(const uint64_t *__restrict__ rowptr, const int *__restrict__ col, uint64_t n,
-                                          uint64_t e0, uint64_t e1, const unsigned *__restrict__ trow, bool table,
-                                          uint64_t *s_rp, uint64_t *s_lo, uint64_t *s_hi, Visit visit) {
-    tile_rows(rowptr, n, e0, e1, trow, table, s_lo, s_hi);
-    const uint64_t lo = *s_lo, span64 = *s_hi - lo + 1;
-    const unsigned span = span64 <= VAL_SPAN ? (unsigned)span64 : 0u;
-    for (unsigned r = threadIdx.x; span && r <= span; r += blockDim.x) s_rp[r] = __ldg(&rowptr[lo + r]);
-    __syncthreads();
-    const uint64_t eb = e0 + (uint64_t)threadIdx.x * VAL_ITEMS;
-    if (eb < e1) {
-        const uint64_t ee = min(eb + VAL_ITEMS, e1);
-        int c[VAL_ITEMS];
-        if (ee - eb == VAL_ITEMS && ((uintptr_t)(col + eb) & 15) == 0) {
-            const int4 *p = reinterpret_cast<const int4 *>(col + eb);
+        // the window: starts of rows lo .. lo + 31 (those past n are never reached)
+        const bool win = table && hi - lo < 31;
+        uint64_t rp = ~0ull;
+        if (win && lo + lane <= n) rp = __ldg(&rowptr[lo + lane]);
+#pragma unroll 1
+        for (int step = 0; step < VAL_WTILE / (32 * ITEMS); ++step) {
+            const uint64_t eb = t * VAL_WTILE + (uint64_t)step * 32 * ITEMS + (uint64_t)lane * ITEMS;
+            const uint64_t ee = eb < E ? min(eb + (uint64_t)ITEMS, E) : eb;
+            const unsigned ne = (unsigned)(ee - eb);
+            int c[ITEMS];
+            if (ne == ITEMS && ((uintptr_t)(col + eb) & 15) == 0) {
+                const int4 *p = reinterpret_cast<const int4 *>(col + eb);
 #pragma unroll
-            for (int k = 0; k < VAL_ITEMS / 4; ++k) {
-                const int4 q = __ldg(p + k);
-                c[4 * k] = q.x;
-                c[4 * k + 1] = q.y;
-                c[4 * k + 2] = q.z;
-                c[4 * k + 3] = q.w;
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k < VAL_ITEMS; ++k) c[k] = eb + k < ee ? __ldg(&col[eb + k]) : 0;
-        }
-        unsigned r = 0;
-        if (span) {
-            unsigned a = 0, b = span - 1;  // largest r with s_rp[r] <= eb
-            while (a < b) {
-                const unsigned mid = (a + b + 1) >> 1;
-                if (s_rp[mid] <= eb) a = mid;
-                else b = mid - 1;
-            }
-            r = a;
-        }
-        const unsigned ne = (unsigned)(ee - eb);
-        unsigned u[VAL_ITEMS];
-#pragma unroll
-        for (int k = 0; k < VAL_ITEMS; ++k) {
-            const uint64_t e = eb + k;
-            u[k] = 0;
-            if (k < ne) {
-                if (span) {
-                    while (s_rp[r + 1] <= e) ++r;
-                    u[k] = (unsigned)(lo + r);
-                } else {
-                    u[k] = (unsigned)row_of(rowptr, lo, *s_hi, e);
+                for (int k = 0; k < ITEMS / 4; ++k) {
+                    const int4 q = __ldg(p + k);
+                    c[4 * k] = q.x;
+                    c[4 * k + 1] = q.y;
+                    c[4 * k + 2] = q.z;
+                    c[4 * k + 3] = q.w;
                 }
+            } else {
+#pragma unroll
+                for (int k = 0; k < ITEMS; ++k) c[k] = k < ne ? __ldg(&col[eb + k]) : 0;
             }
+            uint64_t r, next;
+            if (win) {
+                unsigned j = 0;  // largest window row starting at or before eb
+#pragma unroll
+                for (unsigned s = 16; s >= 1; s >>= 1) {
+                    const uint64_t x = __shfl_sync(FULL, rp, j + s);  // j + s <= 31
+                    if (x <= eb) j += s;
+                }
+                r = lo + j;
+                next = __shfl_sync(FULL, rp, min(j + 1, 31u));
+            } else {
+                r = ne ? row_of(rowptr, lo, hi, eb) : 0;
+                next = ne ? __ldg(&rowptr[r + 1]) : ~0ull;
+            }
+            unsigned u[ITEMS];
+#pragma unroll
+            for (int k = 0; k < ITEMS; ++k) {
+                const uint64_t e = eb + k;
+                if (k < ne && e >= next) {  // into a later row: the next one, or past empty rows a search
+                    ++r;
+                    next = __ldg(&rowptr[r + 1]);
+                    if (next <= e) {
+                        r = row_of(rowptr, r + 1, hi, e);
+                        next = __ldg(&rowptr[r + 1]);
+                    }
+                }
+                u[k] = (unsigned)r;
+            }
+            visit(u, eb, ne, c);
         }
-        visit(u, eb, ne, c);
     }
-    __syncthreads();
 }
 
 __device__ __forceinline__ void block_add(unsigned long long *dst, unsigned long long v) {
@@ -147,28 +144,24 @@ __global__ void __launch_bounds__(VAL_THREADS) edge_count_kernel(const uint64_t 
                                                                  const unsigned *__restrict__ trow,
                                                                  const unsigned long long *__restrict__ table,
                                                                  unsigned long long *__restrict__ out) {
-    __shared__ uint64_t s_lo, s_hi;
-    __shared__ uint64_t s_rp[VAL_SPAN + 1];
     const uint64_t E = rowptr[n];
     const bool tab = *table != 0;
     unsigned long long cnt = 0;
-    for (uint64_t e0 = (uint64_t)blockIdx.x * VAL_TILE; e0 < E; e0 += (uint64_t)gridDim.x * VAL_TILE) {
-        tile_walk(rowptr, col, n, e0, min(e0 + VAL_TILE, E), trow, tab, s_rp, &s_lo, &s_hi,
-                  [&](const unsigned *u, uint64_t, unsigned ne, const int *c) {
-                      // rows change rarely within 16 entries: one pred load per row
-                      unsigned ur = ~0u;
-                      bool reached = false;
+    warp_walk<COUNT_ITEMS>(rowptr, col, n, E, trow, tab,
+              [&](const unsigned *u, uint64_t, unsigned ne, const int *c) {
+                  // rows change rarely within 16 entries: one pred load per row
+                  unsigned ur = ~0u;
+                  bool reached = false;
 #pragma unroll
-                      for (int k = 0; k < VAL_ITEMS; ++k) {
-                          if (k >= ne) break;
-                          if (u[k] != ur) {
-                              ur = u[k];
-                              reached = __ldg(&pred[ur]) != -1;
-                          }
-                          if (reached && (unsigned)c[k] <= u[k]) ++cnt;
+                  for (int k = 0; k < COUNT_ITEMS; ++k) {
+                      if (k >= ne) break;
+                      if (u[k] != ur) {
+                          ur = u[k];
+                          reached = __ldg(&pred[ur]) != -1;
                       }
-                  });
-    }
+                      if (reached && (unsigned)c[k] <= u[k]) ++cnt;
+                  }
+              });
     block_add(out, cnt);
 }
 
@@ -215,45 +208,41 @@ __global__ void __launch_bounds__(VAL_THREADS, 2) bfs_val_edge_kernel(const uint
                                                                    const unsigned long long *__restrict__ table,
                                                                    unsigned *__restrict__ confirmed,
                                                                    unsigned long long *__restrict__ errors) {
-    __shared__ uint64_t s_lo, s_hi;
-    __shared__ uint64_t s_rp[VAL_SPAN + 1];
     const uint64_t E = rowptr[n];
     const bool tab = *table != 0;
     unsigned long long err = 0;
-    for (uint64_t e0 = (uint64_t)blockIdx.x * VAL_TILE; e0 < E; e0 += (uint64_t)gridDim.x * VAL_TILE) {
-        tile_walk(rowptr, col, n, e0, min(e0 + VAL_TILE, E), trow, tab, s_rp, &s_lo, &s_hi,
-                  [&](const unsigned *u, uint64_t, unsigned ne, const int *c) {
-                      // every neighbour record in flight before the first test
-                      longlong2 xv[VAL_ITEMS];
+    warp_walk<RULE_ITEMS>(rowptr, col, n, E, trow, tab,
+              [&](const unsigned *u, uint64_t, unsigned ne, const int *c) {
+                  // every neighbour record in flight before the first test
+                  longlong2 xv[RULE_ITEMS];
 #pragma unroll
-                      for (int k = 0; k < VAL_ITEMS; ++k) {
-                          const unsigned x = (unsigned)c[k];
-                          xv[k] = k < ne && x < n ? __ldg(&vx[x]) : make_longlong2(0, 0);
-                      }
-                      unsigned ur = ~0u;
-                      int64_t ud = 0, up = 0;
+                  for (int k = 0; k < RULE_ITEMS; ++k) {
+                      const unsigned x = (unsigned)c[k];
+                      xv[k] = k < ne && x < n ? __ldg(&vx[x]) : make_longlong2(0, 0);
+                  }
+                  unsigned ur = ~0u;
+                  int64_t ud = 0, up = 0;
 #pragma unroll
-                      for (int k = 0; k < VAL_ITEMS; ++k) {
-                          if (k >= ne) break;
-                          const unsigned uu = u[k];
-                          const uint64_t x = (unsigned)c[k];
-                          if (x == uu || x >= n) {  // a self-loop entry, or not a vertex (counted once, nothing else compared)
-                              ++err;
-                              continue;
-                          }
-                          if (uu != ur) {
-                              ur = uu;
-                              ud = __ldg(&dist[uu]);
-                              up = __ldg(&pred[uu]);
-                          }
-                          const int64_t xd = xv[k].x, xp = xv[k].y;
-                          if ((ud == -1) != (xd == -1)) ++err;
-                          if (ud >= 0 && xd >= 0 && (ud + 1 < xd || xd + 1 < ud)) ++err;
-                          if (up == (int64_t)x) atomicOr(&confirmed[uu >> 5], 1u << (uu & 31));
-                          if (xp == (int64_t)uu) atomicOr(&confirmed[x >> 5], 1u << (x & 31));
+                  for (int k = 0; k < RULE_ITEMS; ++k) {
+                      if (k >= ne) break;
+                      const unsigned uu = u[k];
+                      const uint64_t x = (unsigned)c[k];
+                      if (x == uu || x >= n) {  // a self-loop entry, or not a vertex (counted once, nothing else compared)
+                          ++err;
+                          continue;
                       }
-                  });
-    }
+                      if (uu != ur) {
+                          ur = uu;
+                          ud = __ldg(&dist[uu]);
+                          up = __ldg(&pred[uu]);
+                      }
+                      const int64_t xd = xv[k].x, xp = xv[k].y;
+                      if ((ud == -1) != (xd == -1)) ++err;
+                      if (ud >= 0 && xd >= 0 && (ud + 1 < xd || xd + 1 < ud)) ++err;
+                      if (up == (int64_t)x) atomicOr(&confirmed[uu >> 5], 1u << (uu & 31));
+                      if (xp == (int64_t)uu) atomicOr(&confirmed[x >> 5], 1u << (x & 31));
+                  }
+              });
     block_add(errors, err);
 }
 
@@ -289,7 +278,7 @@ __global__ void sssp_val_vertex_kernel(const float *__restrict__ dist, const int
     block_add(errors, err);
 }
 
-__global__ void __launch_bounds__(VAL_THREADS, 2) sssp_val_edge_kernel(const uint64_t *__restrict__ rowptr,
+__global__ void __launch_bounds__(VAL_THREADS, 3) sssp_val_edge_kernel(const uint64_t *__restrict__ rowptr,
                                                                     const int *__restrict__ col,
                                                                     const float *__restrict__ w, uint64_t n,
                                                                     const float *__restrict__ dist,
@@ -298,51 +287,47 @@ __global__ void __launch_bounds__(VAL_THREADS, 2) sssp_val_edge_kernel(const uin
                                                                     const unsigned long long *__restrict__ table,
                                                                     unsigned *__restrict__ confirmed,
                                                                     unsigned long long *__restrict__ errors) {
-    __shared__ uint64_t s_lo, s_hi;
-    __shared__ uint64_t s_rp[VAL_SPAN + 1];
     const uint64_t E = rowptr[n];
     const bool tab = *table != 0;
     unsigned long long err = 0;
-    for (uint64_t e0 = (uint64_t)blockIdx.x * VAL_TILE; e0 < E; e0 += (uint64_t)gridDim.x * VAL_TILE) {
-        tile_walk(rowptr, col, n, e0, min(e0 + VAL_TILE, E), trow, tab, s_rp, &s_lo, &s_hi,
-                  [&](const unsigned *u, uint64_t eb, unsigned ne, const int *c) {
-                      // the rows' distances first (one load per row), then every
-                      // record of a reached row in flight before the first test
-                      float du[VAL_ITEMS];
-                      unsigned ur = ~0u;
-                      float d = -1.0f;
+    warp_walk<RULE_ITEMS>(rowptr, col, n, E, trow, tab,
+              [&](const unsigned *u, uint64_t eb, unsigned ne, const int *c) {
+                  // the rows' distances first (one load per row), then every
+                  // record of a reached row in flight before the first test
+                  float du[RULE_ITEMS];
+                  unsigned ur = ~0u;
+                  float d = -1.0f;
 #pragma unroll
-                      for (int k = 0; k < VAL_ITEMS; ++k) {
-                          if (k < ne && u[k] != ur) {
-                              ur = u[k];
-                              d = __ldg(&dist[ur]);
-                          }
-                          du[k] = k < ne ? d : -1.0f;
+                  for (int k = 0; k < RULE_ITEMS; ++k) {
+                      if (k < ne && u[k] != ur) {
+                          ur = u[k];
+                          d = __ldg(&dist[ur]);
                       }
-                      longlong2 xv[VAL_ITEMS];
-                      float wk[VAL_ITEMS];
+                      du[k] = k < ne ? d : -1.0f;
+                  }
+                  longlong2 xv[RULE_ITEMS];
+                  float wk[RULE_ITEMS];
 #pragma unroll
-                      for (int k = 0; k < VAL_ITEMS; ++k) {
-                          const unsigned x = (unsigned)c[k];
-                          const bool live = du[k] != -1.0f && x < n;
-                          xv[k] = live ? __ldg(&vx[x]) : make_longlong2(0, 0);
-                          wk[k] = live ? __ldg(&w[eb + k]) : 0.0f;
-                      }
+                  for (int k = 0; k < RULE_ITEMS; ++k) {
+                      const unsigned x = (unsigned)c[k];
+                      const bool live = du[k] != -1.0f && x < n;
+                      xv[k] = live ? __ldg(&vx[x]) : make_longlong2(0, 0);
+                      wk[k] = live ? __ldg(&w[eb + k]) : 0.0f;
+                  }
 #pragma unroll
-                      for (int k = 0; k < VAL_ITEMS; ++k) {
-                          if (du[k] == -1.0f) continue;
-                          const uint64_t x = (unsigned)c[k];
-                          if (x >= n) {
-                              ++err;
-                              continue;
-                          }
-                          const float dx = __uint_as_float((unsigned)xv[k].x);
-                          const float cand = __fadd_rn(du[k], wk[k]);
-                          if (dx == -1.0f || cand < dx) ++err;
-                          if (xv[k].y == (int64_t)u[k] && cand == dx) atomicOr(&confirmed[x >> 5], 1u << (x & 31));
+                  for (int k = 0; k < RULE_ITEMS; ++k) {
+                      if (du[k] == -1.0f) continue;
+                      const uint64_t x = (unsigned)c[k];
+                      if (x >= n) {
+                          ++err;
+                          continue;
                       }
-                  });
-    }
+                      const float dx = __uint_as_float((unsigned)xv[k].x);
+                      const float cand = __fadd_rn(du[k], wk[k]);
+                      if (dx == -1.0f || cand < dx) ++err;
+                      if (xv[k].y == (int64_t)u[k] && cand == dx) atomicOr(&confirmed[x >> 5], 1u << (x & 31));
+                  }
+              });
     block_add(errors, err);
 }
 
@@ -361,7 +346,7 @@ struct ValWork {
     unsigned long long *counter;  // [0] the result, [1] the tile table is valid
     longlong2 *vx;  // packed neighbour records (16 bytes per vertex)
     unsigned *trow;  // tile table (val_tile_rows_kernel)
-    uint64_t tcap;   // its entries: room for graphs of up to 256 entries per vertex on average
+    uint64_t tcap;   // its entries: room for graphs of up to 128 entries per vertex on average
     uint64_t bytes;
 };
 
@@ -371,7 +356,7 @@ static ValWork carve_val(void *base, uint64_t n) {
     w.confirmed = c.take<unsigned>((n + 31) / 32);
     w.counter = c.take<unsigned long long>(32);
     w.vx = c.take<longlong2>(n);
-    w.tcap = n / 16 + 2;
+    w.tcap = n / 4 + 2;
     w.trow = c.take<unsigned>(w.tcap);
     w.bytes = c.used;
     return w;
