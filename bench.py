@@ -38,7 +38,7 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per traversed input edge of bfs_persistent_kernel on a
 # main-component root, from an ncu capture at SCALE 23 (610.4 MB for 134,213,828 edges,
 # profiles/bfs_persistent_kernel_scale23.md); scaled to the bench's roots by their edges.
-TRAFFIC_BYTES_PER_EDGE = 4.55
+TRAFFIC_BYTES_PER_EDGE = 4.53
 E2E_REPS = 3  # end-to-end calls per root (median kept)
 GATE_CYCLES = 200_000  # ~0.1 ms device-side spin queued before each timed root
 
@@ -409,7 +409,7 @@ def run_ours(args):
                          "traffic": int(args.traffic if args.traffic is not None
                                         else TRAFFIC_BYTES_PER_EDGE * np.mean([nedge[timed[i]] for i in big])),
                          "traffic_source": "ncu dram__bytes_read+write given by --traffic" if args.traffic
-                         is not None else "ncu capture at SCALE 23: 4.55 B per traversed edge, scaled by edges"},
+                         is not None else "ncu capture at SCALE 23: 4.53 B per traversed edge, scaled by edges"},
             "e2e": {"value": float(f"{(e2e_hm if world == 1 else e2e_hm * world):.6g}"), "unit": "GTEPS",
                     "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 24,
                     "small_root_us": round(min(e2e_s) * 1e6, 1) if e2e_s else None,
@@ -679,6 +679,33 @@ def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0, raise_er
                       "CUDA event complete; BFS results exported as depth arrays"}
 
 
+def run_kernels_once(scale, ef):
+    """Every kernel of the path once, through the public API, checked: the
+    command that the per-kernel ncu summaries capture."""
+    import torch
+    G = load_package()
+    torch.cuda.set_device(0)
+    seed = G.make_mrg_seed(2, 3)
+    tg = G.generate_kronecker_range(seed, scale, 0, ef << scale)  # kron_generate_kernel
+    g = G.oned_graph_from_tuple_graph(tg, 1 << scale)  # count, partition, place, row sorts, split, degree order
+    del tg
+    r = next(x for x in G.generate_bfs_roots(g, 2, 3, 8) if g.in_main_component(x))
+    bfs, vw = G.BfsState(g), G._val_work(g)
+    G.oned_graph_bfs_run(g, bfs, r)
+    d = G.bfs_compute_dist_from_pred(g, bfs, r)
+    ne = G.edge_count(g, bfs.pred, vw)  # edge_count_kernel
+    err = G.bfs_validate(g, r, bfs.pred, d, vw)  # bfs_val_edge_kernel
+    s = G.SsspState(g)
+    G.oned_graph_sssp_run(g, s, r)
+    G.sssp_status(s)
+    serr = G.sssp_validate(g, r, s.dist, s.pred, vw)  # sssp_val_edge_kernel
+    torch.cuda.synchronize()
+    print(json.dumps({"scale": scale, "root": int(r), "nedge": int(ne), "bfs_errors": int(err),
+                      "sssp_errors": int(serr)}), flush=True)
+    if err or serr:
+        raise SystemExit("validation failed")
+
+
 def run_batched_only(args):
     import torch
     torch.cuda.set_device(0)
@@ -901,11 +928,17 @@ def main():
                     help="JSON cache of the headline searches' tuned knobs (keyed by device and graph size)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per BFS launch (read+write) to report beside the roofline")
+    ap.add_argument("--kernels-once", type=int, default=0, metavar="SCALE",
+                    help="one pass of every kernel of the path at SCALE (the command the ncu summaries profile): "
+                         "generation, canonical CSR, SSSP and BFS copies, one BFS and SSSP from a main-component "
+                         "root, the edge count and both validations")
     args = ap.parse_args()
     if args.warmup < 1 or args.steps < 1:
         ap.error("steps and warmup must be positive")
     if args.impl == "reference":
         run_reference(args)
+    elif args.kernels_once:
+        run_kernels_once(args.kernels_once, args.edgefactor)
     elif args.only_batched:
         run_batched_only(args)
     else:

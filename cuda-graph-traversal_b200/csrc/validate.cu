@@ -68,6 +68,8 @@ template <int ITEMS, class Visit>
 __device__ __forceinline__ void warp_walk(const uint64_t *__restrict__ rowptr, const int *__restrict__ col, uint64_t n,
                                           uint64_t E, const unsigned *__restrict__ trow, bool table, Visit visit) {
     static_assert(ITEMS % 4 == 0 && VAL_WTILE % (32 * ITEMS) == 0, "whole int4 loads, whole steps");
+    __shared__ int s_win[VAL_THREADS / 32][32];
+    int *wrp = s_win[threadIdx.x >> 5];
     const unsigned lane = lane_id();
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t * VAL_WTILE < E; t += nwarps) {
@@ -76,10 +78,20 @@ __device__ __forceinline__ void warp_walk(const uint64_t *__restrict__ rowptr, c
             lo = __ldg(&trow[t]);
             hi = __ldg(&trow[t + 1]);
         }
-        // the window: starts of rows lo .. lo + 31 (those past n are never reached)
+        // The window: starts of rows lo .. lo + 31 (those past n are never
+        // reached), as 32-bit offsets from the tile's first entry (starts
+        // before it clamp to -1, far ones to 2^30), so the lookups below
+        // compare 32-bit numbers.
+        const uint64_t t0 = t * VAL_WTILE;
         const bool win = table && hi - lo < 31;
-        uint64_t rp = ~0ull;
-        if (win && lo + lane <= n) rp = __ldg(&rowptr[lo + lane]);
+        int rp = 1 << 30;
+        if (win && lo + lane <= n) {
+            const uint64_t x = __ldg(&rowptr[lo + lane]);
+            rp = x < t0 ? -1 : x - t0 > (1u << 30) ? 1 << 30 : (int)(x - t0);
+        }
+        __syncwarp();  // the last tile's window is read
+        wrp[lane] = rp;
+        __syncwarp();
 #pragma unroll 1
         for (int step = 0; step < VAL_WTILE / (32 * ITEMS); ++step) {
             const uint64_t eb = t * VAL_WTILE + (uint64_t)step * 32 * ITEMS + (uint64_t)lane * ITEMS;
@@ -100,33 +112,40 @@ __device__ __forceinline__ void warp_walk(const uint64_t *__restrict__ rowptr, c
 #pragma unroll
                 for (int k = 0; k < ITEMS; ++k) c[k] = k < ne ? __ldg(&col[eb + k]) : 0;
             }
-            uint64_t r, next;
+            unsigned u[ITEMS];
             if (win) {
+                const int el = (int)(eb - t0);  // < VAL_WTILE
                 unsigned j = 0;  // largest window row starting at or before eb
 #pragma unroll
-                for (unsigned s = 16; s >= 1; s >>= 1) {
-                    const uint64_t x = __shfl_sync(FULL, rp, j + s);  // j + s <= 31
-                    if (x <= eb) j += s;
-                }
-                r = lo + j;
-                next = __shfl_sync(FULL, rp, min(j + 1, 31u));
-            } else {
-                r = ne ? row_of(rowptr, lo, hi, eb) : 0;
-                next = ne ? __ldg(&rowptr[r + 1]) : ~0ull;
-            }
-            unsigned u[ITEMS];
+                for (unsigned s = 16; s >= 1; s >>= 1)
+                    if (wrp[j + s] <= el) j += s;  // j + s <= 31
+                const unsigned ul = (unsigned)lo;
 #pragma unroll
-            for (int k = 0; k < ITEMS; ++k) {
-                const uint64_t e = eb + k;
-                if (k < ne && e >= next) {  // into a later row: the next one, or past empty rows a search
-                    ++r;
-                    next = __ldg(&rowptr[r + 1]);
-                    if (next <= e) {
-                        r = row_of(rowptr, r + 1, hi, e);
-                        next = __ldg(&rowptr[r + 1]);
-                    }
+                for (int k = 0; k < ITEMS; ++k) {
+                    // Later rows start at or before this entry: step (past
+                    // empty rows too).  The row of a real entry is at most
+                    // hi - lo <= 30, and window row hi - lo + 1 starts after
+                    // the tile's last entry, so the loop stops by itself.
+                    if (k < (int)ne)
+                        while (j < 31 && wrp[j + 1] <= el + k) ++j;
+                    u[k] = ul + j;
                 }
-                u[k] = (unsigned)r;
+            } else {
+                uint64_t r = ne ? row_of(rowptr, lo, hi, eb) : 0;
+                uint64_t next = ne ? __ldg(&rowptr[r + 1]) : ~0ull;
+#pragma unroll
+                for (int k = 0; k < ITEMS; ++k) {
+                    const uint64_t e = eb + k;
+                    if (k < ne && e >= next) {  // into a later row: the next one, or past empty rows a search
+                        ++r;
+                        next = __ldg(&rowptr[r + 1]);
+                        if (next <= e) {
+                            r = row_of(rowptr, r + 1, hi, e);
+                            next = __ldg(&rowptr[r + 1]);
+                        }
+                    }
+                    u[k] = (unsigned)r;
+                }
             }
             visit(u, eb, ne, c);
         }
