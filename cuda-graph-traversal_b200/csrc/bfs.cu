@@ -1326,27 +1326,17 @@ constexpr uint64_t STATIC_BFS_MAX_VERTS = 1ull << 18;
 constexpr uint64_t STATIC_BFS_BYTES = 5ull << 20;
 static __device__ __align__(256) unsigned char g5_bfs_static_scratch[STATIC_BFS_BYTES];
 
-// Device address of the array on the current device, looked up once per
-// device (in host code the array's name is only a stand-in) and kept for the
-// life of the process.  cudaDeviceReset unloads this library's device image
-// with the device's context, and the next context holds a new copy of the
-// array at another address: a process that resets a device must not call
-// g5_bfs_run_static on it afterwards.
+// Device address of the array in the current context, looked up on every
+// call (in host code the array's name is only a stand-in; the lookup is
+// cheap once the module is loaded).  Nothing is cached: after a
+// cudaDeviceReset the next context holds a new copy of the array at
+// another address, and the next call finds that one.
 static int static_bfs_scratch(void **out) {
-    static std::mutex mu;
-    static void *addr[64] = {};
-    int dev = 0;
-    G5_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return set_error(G5_ERR_INVALID, "device ordinal %d out of range", dev);
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g5_bfs_static_scratch);
-        if (e != cudaSuccess || !p)
-            return set_error(G5_ERR_CUDA, "g5_bfs_run_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-        addr[dev] = p;
-    }
-    *out = addr[dev];
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g5_bfs_static_scratch);
+    if (e != cudaSuccess || !p)
+        return set_error(G5_ERR_CUDA, "g5_bfs_run_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+    *out = p;
     return G5_OK;
 }
 

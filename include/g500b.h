@@ -305,13 +305,13 @@ int g5_bfs_last_trace(const void *d_work, uint64_t work_bytes, int max_levels, i
  * for.  The scratch is a fixed 5 MiB array inside the library, present on
  * every GPU that loads it until the process exits; graphs are limited to
  * 2^18 vertices (G5_ERR_INVALID beyond).  The caller still provides the
- * graph and the outputs.  The first call on a device looks up the array's
- * device address, so make it before any stream capture.  All calls share
- * the one array: calls that overlap on the GPU (other streams, other host
- * threads) race, so serialise them.  Each call clears what must start at
- * zero.  The looked-up address lives as long as the device's context: after
- * cudaDeviceReset on a device, do not call this entry point there again.
- * No counterpart in the reference. */
+ * graph and the outputs.  Every call looks up the array's device address in
+ * the current context (cheap; after cudaDeviceReset it finds the new
+ * context's copy); make one call before any stream capture, so that the
+ * library's device code is loaded.  All calls share the one array: calls
+ * that overlap on the GPU (other streams, other host threads) race, so
+ * serialise them.  Each call clears what must start at zero.  No
+ * counterpart in the reference. */
 int g5_bfs_run_static(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
                       int64_t *d_pred, int32_t *d_depth, const g5_bfs_params *params, void *stream);
 
