@@ -25,6 +25,38 @@ def test_tuning_cache_round_trip(cgt, tmp_path):
     assert T.bfs_params(c2.get("bfs", fake)).alpha == 10.0
 
 
+def test_tile_descent_and_committed_cache(cgt):
+    """Coordinate descent over the tile axes: each axis keeps its fastest
+    value with the others at their best so far, and no setting is timed
+    twice.  The committed cache holds a B200 SCALE 26 result whose knobs
+    form valid parameters."""
+    import json
+    import os
+    from cgt_b200 import autotune as T
+    timed = []
+
+    def time_of(k):  # a bowl: best at chunk 512, big_deg 256, lane_entries 8
+        timed.append(tuple(sorted(k.items())))
+        return abs(k["chunk"] - 512) + abs(k["big_deg"] - 256) / 4 + abs(k["lane_entries"] - 8) * 10
+
+    base = dict(T.BFS_DEFAULT_TILES)
+    ms, best, count = T._descend(time_of, base, T.BFS_TILES)
+    assert (best["chunk"], best["big_deg"], best["lane_entries"]) == (512, 256, 8) and ms == 0
+    assert count == len(timed) == len(set(timed))
+    assert count == 1 + sum(len(set(v) - {base[k]}) for k, v in T.BFS_TILES.items())
+    path = os.path.join(os.path.dirname(cgt.__file__), "tuned.json")
+    data = json.load(open(path))
+    kinds = {k.split("|")[1] for k in data}
+    assert kinds == {"bfs", "sssp"} and all(k.startswith("NVIDIA B200|") for k in data)
+    for key, t in data.items():
+        if "|bfs|" in key:
+            p = T.bfs_params(t)
+            assert p.chunk % 32 == 0 and 0 < p.alpha and p.lane_entries % 4 == 0
+        else:
+            kw = T.sssp_kwargs(t)
+            assert kw["delta"] == 0.1 and kw["chunk"] % 64 == 0
+
+
 def test_poisson_trace_and_summary(cgt):
     from cgt_b200 import serve as S
     # graph 1 has isolated vertices 0 and 2: roots never land there
