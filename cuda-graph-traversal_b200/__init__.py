@@ -80,6 +80,8 @@ def _load() -> C.CDLL:
         "g5_csr_sort_rows": ([p, u64, u64, p, p, p, p, u64, p], C.c_int),
         "g5_csr_degree_order_workspace_size": ([u64, u64, p], C.c_int),
         "g5_csr_degree_order": ([p, p, u64, u64, p, p, u64, p], C.c_int),
+        "g5_csr_sssp_renumber_workspace_size": ([u64, p], C.c_int),
+        "g5_csr_sssp_renumber": ([p, p, p, p, p, u64, u64, p, p, p, p, p, p, p, p, u64, p], C.c_int),
         "g5_csr_dedupe_count": ([p, p, u64, u64, p, p, u64, p, p], C.c_int),
         "g5_csr_dedupe_copy": ([p, p, p, u64, p, p, p, p, p], C.c_int),
         "g5_csr_split_light": ([p, p, p, u64, u64, f32, p, p, p, p, p, u64, p], C.c_int),
@@ -161,7 +163,7 @@ class MsBfsStats(C.Structure):
 class SsspParams(C.Structure):
     _fields_ = [("delta", C.c_float), ("blocks", C.c_int32), ("pull", C.c_float), ("sub_min", C.c_int32),
                 ("small", C.c_int32), ("tiny_deg", C.c_void_p), ("check_opens", C.c_int32), ("big_deg", C.c_int32),
-                ("chunk", C.c_int32)]
+                ("chunk", C.c_int32), ("perm", C.c_void_p), ("inv", C.c_void_p)]
 
 
 def _ptr(t: torch.Tensor | None) -> int | None:
@@ -279,6 +281,10 @@ class OnedGraph:
     # The BFS copy of the column (g5_csr_degree_order): each row's
     # neighbours by decreasing degree.  None: the BFS reads col.
     bcol: torch.Tensor | None = None
+    # The SSSP copy renumbered by decreasing degree (g5_csr_sssp_renumber),
+    # which the SSSP entry points use when present; None: the split copy
+    # above in the caller's numbering.
+    sr: "SsspCopy | None" = None
 
     @property
     def bfs_col(self) -> torch.Tensor:
@@ -306,6 +312,52 @@ class OnedGraph:
     @property
     def device(self):
         return self.rowstarts.device
+
+
+@dataclass
+class SsspCopy:
+    """The SSSP's CSR in its own vertex numbering (decreasing degree): row
+    starts, column, weights, light and tiny counts, perm (caller's vertex ->
+    search's) and inv (back)."""
+    rowstarts: torch.Tensor
+    col: torch.Tensor
+    w: torch.Tensor
+    light_deg: torch.Tensor
+    tiny_deg: torch.Tensor
+    perm: torch.Tensor
+    inv: torch.Tensor
+
+
+def oned_graph_sssp_renumber(g: OnedGraph, stream=None) -> OnedGraph:
+    """Gives the SSSP a copy of its split CSR renumbered by decreasing
+    degree (g5_csr_sssp_renumber): the vertices most relaxations target
+    then have their per-vertex state side by side, where it stays in L2.
+    Distances are unchanged; parents are still tight edges' sources.  Costs
+    12 bytes per CSR entry and 24 per vertex."""
+    n, e = g.nglobalverts, g.nlocaledges
+    dev = g.device
+    nb = C.c_uint64()
+    _check(lib.g5_csr_sssp_renumber_workspace_size(n, C.byref(nb)))
+    work = _workspace(nb.value, dev)
+    i32 = dict(dtype=torch.int32, device=dev)
+    sr = SsspCopy(torch.empty(n + 1, dtype=torch.int64, device=dev), torch.empty(max(e, 1), **i32),
+                  torch.empty(max(e, 1), dtype=torch.float32, device=dev), torch.empty(n, **i32), torch.empty(n, **i32),
+                  torch.empty(n, **i32), torch.empty(n, **i32))
+    _check(lib.g5_csr_sssp_renumber(_ptr(g.rowstarts), _ptr(g.sssp_col), _ptr(g.sssp_w), _ptr(g.light_deg),
+                                    _ptr(g.tiny_deg), n, e, _ptr(sr.perm), _ptr(sr.inv), _ptr(sr.rowstarts),
+                                    _ptr(sr.col), _ptr(sr.w), _ptr(sr.light_deg), _ptr(sr.tiny_deg), _ptr(work),
+                                    work.numel(), _stream(stream)))
+    g.sr = sr
+    return g
+
+
+def _sssp_csr(g: OnedGraph):
+    """(row starts, column, weights, light counts, tiny counts, perm, inv)
+    the SSSP entry points are given."""
+    if g.sr is not None:
+        r = g.sr
+        return r.rowstarts, r.col, r.w, r.light_deg, r.tiny_deg, r.perm, r.inv
+    return g.rowstarts, g.sssp_col, g.sssp_w, g.light_deg, g.tiny_deg, None, None
 
 
 def _sorted_work(n: int, e: int, dev, bfs_order: bool = False) -> torch.Tensor:
@@ -337,7 +389,7 @@ def oned_graph_bfs_order(g: OnedGraph, stream=None, work: torch.Tensor | None = 
 
 
 def _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, dev, stream,
-                  with_main, bfs_order) -> OnedGraph:
+                  with_main, bfs_order, sssp_renumber=True) -> OnedGraph:
     """Canonical rows (already sorted) -> optional dedupe -> the SSSP copy
     (g5_csr_split_light) -> the BFS copy (g5_csr_degree_order, when
     bfs_order) -> isolated bitmap and main component."""
@@ -369,6 +421,9 @@ def _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st,
     g.scol, g.sw = scol[:e], sw[:e]
     if bfs_order:
         oned_graph_bfs_order(g, stream, work)
+    if sssp_renumber:
+        del work
+        oned_graph_sssp_renumber(g, stream)
     if with_main:
         g.main_bits = main_component_bitmap(g, stream)
     return g
@@ -376,7 +431,7 @@ def _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st,
 
 def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: float = 0.1,
                                 with_column64: bool = False, stream=None, with_main: bool = True,
-                                dedupe: bool = False, bfs_order: bool = True) -> OnedGraph:
+                                dedupe: bool = False, bfs_order: bool = True, sssp_renumber: bool = True) -> OnedGraph:
     """oned_graph_from_tuple_graph (src/traversal.h:43): the CSR of both
     directions of every non-loop edge, duplicates kept, every row in
     canonical order (sorted by neighbour, then weight bits:
@@ -386,7 +441,8 @@ def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: 
     counts include duplicates).  with_main=False skips the main-component
     search (g.main_bits = None; set it later with main_component_bitmap).
     bfs_order=False skips the BFS's degree-ordered copy of the column
-    (g.bcol; oned_graph_bfs_order makes it later)."""
+    (g.bcol; oned_graph_bfs_order makes it later), sssp_renumber=False the
+    SSSP's renumbered copy (g.sr; oned_graph_sssp_renumber)."""
     dev = tg.edges.device
     n, m = int(nglobalverts), tg.edges_size
     nb = C.c_uint64()
@@ -406,7 +462,7 @@ def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: 
     _check(lib.g5_csr_fill_sorted(_ptr(tg.edges), _ptr(tg.weights), m, n, _ptr(rowstarts), e, _ptr(work),
                                   work.numel(), _ptr(col), _ptr(w), _ptr(col64), st))
     return _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, dev, stream, with_main,
-                         bfs_order)
+                         bfs_order, sssp_renumber)
 
 
 def _split_tiny(rowstarts, col, w, col64, light, n: int, light_delta: float, st) -> torch.Tensor:
@@ -419,7 +475,7 @@ def _split_tiny(rowstarts, col, w, col64, light, n: int, light_delta: float, st)
 
 def oned_graph_from_kronecker(seed, log_n: int, nedges: int, device="cuda", light_delta: float = 0.1,
                               with_column64: bool = False, stream=None, with_main: bool = True,
-                              dedupe: bool = False, bfs_order: bool = True) -> OnedGraph:
+                              dedupe: bool = False, bfs_order: bool = True, sssp_renumber: bool = True) -> OnedGraph:
     """generate_kronecker_range + oned_graph_from_tuple_graph in one step,
     with the generator fused into the CSR passes (no edge list in memory);
     rows then sorted into canonical order (g5_csr_sort_rows) -- the same
@@ -448,7 +504,7 @@ def oned_graph_from_kronecker(seed, log_n: int, nedges: int, device="cuda", ligh
     _check(lib.g5_csr_sort_rows(_ptr(rowstarts), n, e, _ptr(col), _ptr(w), _ptr(col64), _ptr(work), work.numel(),
                                 st))
     return _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, device, stream, with_main,
-                         bfs_order)
+                         bfs_order, sssp_renumber)
 
 
 # ------------------------------------------------------- packed graphs ----
@@ -499,7 +555,8 @@ def pack_kronecker(scales, edgefactor: int = 16, seed1_base: int = 2, seed2: int
     def gen():
         for i, s in enumerate(scales):
             g = oned_graph_from_kronecker(make_mrg_seed(seed1_base + i, seed2), s, edgefactor << s, device=device,
-                                          light_delta=light_delta, stream=stream, with_main=False, bfs_order=False)
+                                          light_delta=light_delta, stream=stream, with_main=False, bfs_order=False,
+                                          sssp_renumber=False)
             r = generate_bfs_roots(g, 2, 3, 1)
             roots.append(r[0] if r else 0)
             yield g
@@ -554,8 +611,9 @@ def oned_graph_sssp_traverse_multi(g: OnedGraph, sssp: "SsspState", d_roots: tor
                                    big_deg: int = 0, chunk: int = 0) -> None:
     """SSSP from every source in d_roots at once (g5_sssp_traverse_multi);
     reset sssp first."""
-    p = SsspParams(delta, blocks, pull, sub_min, 0, _ptr(g.tiny_deg), 0, big_deg, chunk)
-    _check(lib.g5_sssp_traverse_multi(_ptr(g.rowstarts), _ptr(g.sssp_col), _ptr(g.sssp_w), _ptr(g.light_deg),
+    rs, col, w, light, tiny, perm, inv = _sssp_csr(g)
+    p = SsspParams(delta, blocks, pull, sub_min, 0, _ptr(tiny), 0, big_deg, chunk, _ptr(perm), _ptr(inv))
+    _check(lib.g5_sssp_traverse_multi(_ptr(rs), _ptr(col), _ptr(w), _ptr(light),
                                       g.light_delta,
                                       g.nglobalverts, _ptr(d_roots), d_roots.numel(), _ptr(sssp.dist),
                                       _ptr(sssp.pred), _ptr(sssp.work), sssp.work.numel(), C.byref(p),
@@ -950,8 +1008,9 @@ def _sssp_params(g: OnedGraph, root: int, delta, blocks, pull, sub_min, small, c
     # component (when the grid is left to the library).
     if small is None:
         small = blocks == 0 and not g.in_main_component(root)
+    _, _, _, _, tiny, perm, inv = _sssp_csr(g)
     return SsspParams(delta, 1 if small and blocks == 0 else blocks, pull, sub_min, int(bool(small)),
-                      _ptr(g.tiny_deg), int(bool(check_opens)), big_deg, chunk)
+                      _ptr(tiny), int(bool(check_opens)), big_deg, chunk, _ptr(perm), _ptr(inv))
 
 
 def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float = 0.1, blocks: int = 0,
@@ -962,7 +1021,8 @@ def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float =
     fail the search if a queue held a vertex twice (a test aid).  big_deg /
     chunk: the work tiles of g5_sssp_params (0 = defaults)."""
     p = _sssp_params(g, root, delta, blocks, pull, sub_min, small, check_opens, big_deg, chunk)
-    _check(lib.g5_sssp_run(_ptr(g.rowstarts), _ptr(g.sssp_col), _ptr(g.sssp_w), _ptr(g.light_deg), g.light_delta,
+    rs, col, w, light = _sssp_csr(g)[:4]
+    _check(lib.g5_sssp_run(_ptr(rs), _ptr(col), _ptr(w), _ptr(light), g.light_delta,
                            g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                            sssp.work.numel(), C.byref(p), _stream(stream)))
     sssp.was_reset = True  # g5_sssp_run resets in full first
@@ -987,7 +1047,8 @@ def oned_graph_sssp_traverse(g: OnedGraph, sssp: SsspState, root: int, delta: fl
     """The search itself, on a reset state (the lean one-block search for a
     root outside the main component)."""
     p = _sssp_params(g, root, delta, blocks, pull, sub_min, small, check_opens, big_deg, chunk)
-    _check(lib.g5_sssp_traverse(_ptr(g.rowstarts), _ptr(g.sssp_col), _ptr(g.sssp_w), _ptr(g.light_deg),
+    rs, col, w, light = _sssp_csr(g)[:4]
+    _check(lib.g5_sssp_traverse(_ptr(rs), _ptr(col), _ptr(w), _ptr(light),
                                 g.light_delta,
                                 g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                                 sssp.work.numel(), C.byref(p), _stream(stream)))

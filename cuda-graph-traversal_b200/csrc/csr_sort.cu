@@ -582,6 +582,60 @@ __global__ void degree_keys_kernel(const int *__restrict__ col, uint64_t e, cons
     }
 }
 
+// --------------------------------------------------- SSSP vertex numbering
+
+// Sort keys of the vertex order: (~degree, index) in the (col, w) slots of
+// one row of n entries.
+__global__ void vertex_order_keys_kernel(const unsigned *__restrict__ deg, uint64_t n, int *__restrict__ ka,
+                                         float *__restrict__ kb) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        ka[v] = (int)(0xffffffffu - __ldg(&deg[v]));
+        kb[v] = __uint_as_float((unsigned)v);
+    }
+}
+
+// perm[inv[i]] = i, and the new rows' lengths.
+__global__ void vertex_perm_kernel(const unsigned *__restrict__ inv, const unsigned *__restrict__ deg, uint64_t n,
+                                   unsigned *__restrict__ perm, unsigned *__restrict__ len2) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const unsigned o = __ldg(&inv[i]);
+        perm[o] = (unsigned)i;
+        len2[i] = __ldg(&deg[o]);
+    }
+}
+
+// Row i of the renumbered copy = row inv[i] of the source, in the same
+// order, its neighbours renamed by perm (one warp per row).
+__global__ void renumber_rows_kernel(const uint64_t *__restrict__ rs, const int *__restrict__ col,
+                                     const float *__restrict__ w, const unsigned *__restrict__ light,
+                                     const unsigned *__restrict__ tiny, uint64_t n, const unsigned *__restrict__ perm,
+                                     const unsigned *__restrict__ inv, const uint64_t *__restrict__ rs2,
+                                     int *__restrict__ col2, float *__restrict__ w2, unsigned *__restrict__ light2,
+                                     unsigned *__restrict__ tiny2, unsigned *__restrict__ err) {
+    const unsigned lane = lane_id();
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        const unsigned o = __ldg(&inv[i]);
+        const uint64_t b = __ldg(&rs[o]), len = __ldg(&rs[o + 1]) - b, b2 = __ldg(&rs2[i]);
+        if (lane == 0) {
+            light2[i] = __ldg(&light[o]);
+            tiny2[i] = __ldg(&tiny[o]);
+        }
+        for (uint64_t k = lane; k < len; k += 32) {
+            const unsigned v = (unsigned)__ldg(&col[b + k]);
+            if (v >= n) {
+                atomicOr(err, SORTERR_RANGE);
+                col2[b2 + k] = (int)v;  // kept out of range: the search reports it
+            } else {
+                col2[b2 + k] = (int)__ldg(&perm[v]);
+            }
+            w2[b2 + k] = __ldg(&w[b + k]);
+        }
+    }
+}
+
 // ------------------------------------------------------------- SSSP split
 
 // Stable three-way partition of a row into tiny (w < tiny), other light
@@ -929,6 +983,75 @@ extern "C" int g5_csr_degree_order(const uint64_t *d_rowstarts, const int32_t *d
     G5_CUDA_TRY(cudaMemcpyAsync(&errs, &w.cnt[2], sizeof errs, cudaMemcpyDeviceToHost, st));
     G5_CUDA_TRY(cudaStreamSynchronize(st));
     if (errs) return set_error(G5_ERR_INVALID, "g5_csr_degree_order: a column entry is not a vertex");
+    return G5_OK;
+}
+
+// Scratch of g5_csr_sssp_renumber: the row sort's for one row of n
+// entries, the degrees and new lengths, the sort keys, a scan's scratch.
+static uint64_t renumber_bytes(uint64_t n, uint64_t *off_deg, uint64_t *off_len, uint64_t *off_ka,
+                               uint64_t *off_rs, uint64_t *off_scan) {
+    uint64_t b = align_up(carve_sort(nullptr, 1, n).bytes, 256);
+    *off_deg = b;
+    b += align_up(n * 4, 256);
+    *off_len = b;
+    b += align_up(n * 4, 256);
+    *off_ka = b;
+    b += align_up(n * 4, 256);
+    *off_rs = b;
+    b += 256;
+    *off_scan = b;
+    b += align_up(scan_scratch_words(n) * 8, 256);
+    return b;
+}
+
+extern "C" int g5_csr_sssp_renumber_workspace_size(uint64_t nverts, uint64_t *bytes) {
+    G5_CHECK_ARG(bytes, "g5_csr_sssp_renumber_workspace_size: bytes is NULL");
+    uint64_t a, b, c, d, e;
+    *bytes = renumber_bytes(nverts, &a, &b, &c, &d, &e);
+    return G5_OK;
+}
+
+extern "C" int g5_csr_sssp_renumber(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
+                                    const uint32_t *d_light_deg, const uint32_t *d_tiny_deg, uint64_t nverts,
+                                    uint64_t nentries, uint32_t *d_perm, uint32_t *d_inv, uint64_t *d_rowstarts_out,
+                                    int32_t *d_col_out, float *d_w_out, uint32_t *d_light_out, uint32_t *d_tiny_out,
+                                    void *d_work, uint64_t work_bytes, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_csr_sssp_renumber: nverts outside [1, 2^31]");
+    G5_CHECK_ARG(d_rowstarts && d_light_deg && d_tiny_deg && d_perm && d_inv && d_rowstarts_out && d_light_out &&
+                     d_tiny_out && d_work && (nentries == 0 || (d_col && d_w && d_col_out && d_w_out)),
+                 "g5_csr_sssp_renumber: NULL argument");
+    uint64_t off_deg, off_len, off_ka, off_rs, off_scan;
+    if (work_bytes < renumber_bytes(nverts, &off_deg, &off_len, &off_ka, &off_rs, &off_scan))
+        return set_error(G5_ERR_WORKSPACE, "g5_csr_sssp_renumber: workspace too small");
+    char *base = (char *)d_work;
+    SortWork w = carve_sort(d_work, 1, nverts);
+    unsigned *deg = (unsigned *)(base + off_deg), *len2 = (unsigned *)(base + off_len);
+    int *ka = (int *)(base + off_ka);
+    uint64_t *rs1 = (uint64_t *)(base + off_rs), *scan = (uint64_t *)(base + off_scan);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int grid = sort_grid(8);
+    // The vertex order: decreasing degree, ties by index (a row sort of one
+    // row of n keys); inv = the order, perm its inverse.
+    const uint64_t one_row[2] = {0, nverts};
+    G5_CUDA_TRY(cudaMemcpyAsync(rs1, one_row, sizeof one_row, cudaMemcpyHostToDevice, st));
+    G5_CUDA_TRY(cudaMemsetAsync(&w.cnt[2], 0, sizeof(unsigned), st));
+    row_lengths_kernel<<<grid, 256, 0, st>>>(d_rowstarts, nverts, deg);
+    vertex_order_keys_kernel<<<grid, 256, 0, st>>>(deg, nverts, ka, (float *)d_inv);
+    G5_CUDA_TRY(cudaGetLastError());
+    int rc = sort_rows(rs1, 1, ka, (float *)d_inv, nullptr, w, st);
+    if (rc) return rc;
+    vertex_perm_kernel<<<grid, 256, 0, st>>>(d_inv, deg, nverts, d_perm, len2);
+    G5_CUDA_TRY(cudaGetLastError());
+    if ((rc = scan_u32_to_u64(len2, nverts, d_rowstarts_out, scan, st))) return rc;
+    renumber_rows_kernel<<<grid, 256, 0, st>>>(d_rowstarts, d_col, d_w, d_light_deg, d_tiny_deg, nverts, d_perm, d_inv,
+                                               d_rowstarts_out, d_col_out, d_w_out, d_light_out, d_tiny_out,
+                                               &w.cnt[2]);
+    G5_CUDA_TRY(cudaGetLastError());
+    unsigned errs = 0;
+    G5_CUDA_TRY(cudaMemcpyAsync(&errs, &w.cnt[2], sizeof errs, cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    if (errs) return set_error(G5_ERR_INVALID, "g5_csr_sssp_renumber: a column entry is not a vertex");
     return G5_OK;
 }
 

@@ -134,6 +134,7 @@ struct SsspTouch {
     unsigned long long count;  // vertices in the list
     float *dist;
     int64_t *pred;
+    const unsigned *inv;  // the search's vertex numbering: output index of listed vertex v (nullptr: v)
 };
 
 struct SsspCtl {
@@ -214,9 +215,27 @@ struct SsspArgs {
     bool check_opens;  // opens exchange their stamps and flag a vertex met twice (DEVERR_DUPLICATE)
     unsigned big_deg;  // list entries with more edges to expand go to the chunked big part
     unsigned chunk;    // edges of a big entry per warp grab
+    // Renumbered search (both set) or not (both nullptr): the CSR is in the
+    // search's numbering, roots and outputs in the caller's; perm maps a
+    // caller's vertex to the search's, inv back.  Parents in pack are the
+    // search's numbers (mapped through inv when written out).
+    const unsigned *perm, *inv;
 };
 
 __device__ __forceinline__ float pack_dist(unsigned long long p) { return __uint_as_float((unsigned)(p >> 32)); }
+
+// The caller's number of the search's vertex v, and back.
+__device__ __forceinline__ unsigned out_id(const SsspArgs &a, unsigned v) { return a.inv ? __ldg(&a.inv[v]) : v; }
+__device__ __forceinline__ unsigned in_id(const SsspArgs &a, uint64_t v) {
+    return a.perm ? __ldg(&a.perm[v]) : (unsigned)v;
+}
+
+// Writes vertex v's final packed value p to the caller's outputs.
+__device__ __forceinline__ void write_out(const SsspArgs &a, unsigned v, unsigned long long p) {
+    const unsigned o = out_id(a, v);
+    a.dist[o] = p == UNREACHED ? -1.0f : pack_dist(p);
+    a.pred[o] = p == UNREACHED ? -1 : (int64_t)out_id(a, (unsigned)p);
+}
 
 // Row range [b, e) of u's light (heavy = false) or heavy part.  Without
 // partition data the whole row is returned and the caller filters by weight.
@@ -1035,24 +1054,30 @@ __global__ void __launch_bounds__(SSSP_THREADS, SSSP_MIN_BLOCKS) sssp_persistent
     unsigned epoch = 0;
     const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
-    const bool sparse_out = __ldcg((const unsigned long long *)&a.prefilled->dist) == (unsigned long long)a.dist &&
-                            __ldcg((const unsigned long long *)&a.prefilled->pred) == (unsigned long long)a.pred;
+    const bool prefilled = __ldcg((const unsigned long long *)&a.prefilled->dist) == (unsigned long long)a.dist &&
+                           __ldcg((const unsigned long long *)&a.prefilled->pred) == (unsigned long long)a.pred;
+    // Pre-filled outputs are written as vertices settle, unless the search
+    // is renumbered: then one pass at the end writes them (in the caller's
+    // numbering), which costs less than mapping every settle's writes.
+    const bool sparse_out = prefilled && !a.inv;
     const unsigned long long e_total = __ldg(&a.rowptr[a.n]);
     unsigned long long settled_entries = 0;  // CSR entries of the rows of settled vertices
 
     if (gtid == 0) a.touch->small = 0;  // the next reset clears everything
     if (!a.roots) {
         if (gtid == 0) {
-            a.pack[a.root] = (unsigned long long)a.root;  // distance 0.0f, parent = root
-            a.ring[0] = a.root;
-            a.rstamp[a.root] = 0;
+            const unsigned root = in_id(a, a.root);
+            a.pack[root] = (unsigned long long)root;  // distance 0.0f, parent = root
+            a.ring[0] = root;
+            a.rstamp[root] = 0;
             c->sn.ring_len[0] = 1;
         }
     } else {
         // Several sources (disjoint graphs packed into one CSR, one source
         // each) all start in bucket 0; a repeated source is queued once.
         for (uint64_t i = gtid; i < a.nroots; i += nthreads) {
-            const uint64_t r = __ldg(&a.roots[i]);
+            const uint64_t r0 = __ldg(&a.roots[i]);
+            const uint64_t r = r0 < a.n ? in_id(a, r0) : r0;
             if (r >= a.n) {
                 atomicOr(&c->error, DEVERR_RANGE);
             } else if (atomicCAS(&a.rstamp[r], 0xffffffffu, 0u) == 0xffffffffu) {
@@ -1353,12 +1378,12 @@ __global__ void __launch_bounds__(SSSP_THREADS, SSSP_MIN_BLOCKS) sssp_persistent
         c->phases = phase;
     }
     // Every distance is final (the last heavy phase ended at a grid barrier).
-    // Outputs not pre-filled by the reset are written here in full.
+    // Outputs not written as vertices settled are written here: every
+    // vertex, or with pre-filled outputs the reached ones.
     if (!sparse_out) {
         for (uint64_t v = gtid; v < a.n; v += nthreads) {
             const unsigned long long p = __ldcg(&a.pack[v]);
-            a.dist[v] = p == UNREACHED ? -1.0f : pack_dist(p);
-            a.pred[v] = p == UNREACHED ? -1 : (int64_t)(unsigned)p;
+            if (p != UNREACHED || !prefilled) write_out(a, (unsigned)v, p);
         }
     }
 }
@@ -1409,13 +1434,14 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
     }
     if (threadIdx.x == 0) {
         c->t0 = globaltimer_ns();
-        a.pack[a.root] = (unsigned long long)a.root;  // distance 0.0f, parent = root
-        a.sstamp[a.root] = 0;
-        s_v[0][0] = a.root;
-        s_rb[0][0] = __ldg(&a.rowptr[a.root]);
-        s_re[0][0] = __ldg(&a.rowptr[a.root + 1]);
-        s_r[0] = a.root;
-        R[0] = a.root;
+        const unsigned root = in_id(a, a.root);
+        a.pack[root] = (unsigned long long)root;  // distance 0.0f, parent = root
+        a.sstamp[root] = 0;
+        s_v[0][0] = root;
+        s_rb[0][0] = __ldg(&a.rowptr[root]);
+        s_re[0][0] = __ldg(&a.rowptr[root + 1]);
+        s_r[0] = root;
+        R[0] = root;
         s_len[0] = 1;
         s_len[1] = 0;
         s_nreach = 1;
@@ -1496,16 +1522,10 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
         const unsigned nr = min(s_nreach, (unsigned)a.n);
         for (unsigned i = threadIdx.x; i < nr; i += blockDim.x) {
             const unsigned v = i < SMALL_L ? s_r[i] : __ldcg(&R[i]);
-            const unsigned long long p = __ldcg(&a.pack[v]);
-            a.dist[v] = pack_dist(p);
-            a.pred[v] = (int64_t)(unsigned)p;
+            write_out(a, v, __ldcg(&a.pack[v]));
         }
     } else {
-        for (uint64_t v = threadIdx.x; v < a.n; v += blockDim.x) {
-            const unsigned long long p = __ldcg(&a.pack[v]);
-            a.dist[v] = p == UNREACHED ? -1.0f : pack_dist(p);
-            a.pred[v] = p == UNREACHED ? -1 : (int64_t)(unsigned)p;
-        }
+        for (uint64_t v = threadIdx.x; v < a.n; v += blockDim.x) write_out(a, (unsigned)v, __ldcg(&a.pack[v]));
     }
     if (threadIdx.x == 0) {
         c->buckets = 1;
@@ -1513,7 +1533,8 @@ __global__ void __launch_bounds__(SSSP_THREADS) sssp_small_kernel(SsspArgs a) {
         c->error |= s_err;
         // R lists every vertex this search wrote (a search that reported an
         // error leaves the next reset a full one).
-        *a.touch = SsspTouch{s_err == 0 && s_nreach <= a.n ? 1u : 0u, s_sparse ? 1u : 0u, s_nreach, a.dist, a.pred};
+        *a.touch = SsspTouch{s_err == 0 && s_nreach <= a.n ? 1u : 0u, s_sparse ? 1u : 0u, s_nreach, a.dist, a.pred,
+                             a.inv};
     }
 }
 
@@ -1615,8 +1636,8 @@ __global__ void sssp_reset_kernel(SsspResetArgs r) {
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
     const SsspWork &w = r.w;
-    const SsspTouch h = r.full ? SsspTouch{0u, 0u, 0ull, nullptr, nullptr} : *w.touch;
-    if (r.full && t == 0) *w.touch = SsspTouch{1u, r.dist ? 1u : 0u, 0ull, r.dist, r.pred};
+    const SsspTouch h = r.full ? SsspTouch{0u, 0u, 0ull, nullptr, nullptr, nullptr} : *w.touch;
+    if (r.full && t == 0) *w.touch = SsspTouch{1u, r.dist ? 1u : 0u, 0ull, r.dist, r.pred, nullptr};
     const bool small = !r.full && h.small && h.count <= r.n;
     const bool out_t = small && h.sparse && h.dist == r.dist && h.pred == r.pred;
     if (blockIdx.x == 0) {
@@ -1633,9 +1654,10 @@ __global__ void sssp_reset_kernel(SsspResetArgs r) {
             w.pack[v] = UNREACHED;
             w.fstamp[v] = ~0u;
             w.sstamp[v] = ~0u;
-            if (r.dist && out_t) {
-                r.dist[v] = -1.0f;
-                r.pred[v] = -1;
+            if (r.dist && out_t) {  // the outputs of a renumbered search are in the caller's numbering
+                const unsigned o = h.inv ? __ldg(&h.inv[v]) : v;
+                r.dist[o] = -1.0f;
+                r.pred[o] = -1;
             }
         }
     } else {
@@ -1692,6 +1714,7 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     G5_CHECK_ARG(p.big_deg >= 0 && p.big_deg <= (1 << 20), "%s: big_deg %d outside [0, 2^20]", who, p.big_deg);
     G5_CHECK_ARG(p.chunk >= 0 && p.chunk <= (1 << 16) && p.chunk % (32 * SSSP_EDGES) == 0,
                  "%s: chunk %d is not a multiple of %d in [0, 65536]", who, p.chunk, 32 * SSSP_EDGES);
+    G5_CHECK_ARG((p.perm == nullptr) == (p.inv == nullptr), "%s: give both perm and inv or neither", who);
     int max_blocks = 0;
     if ((rc = sssp_max_blocks(&max_blocks))) return rc;
     int blocks = p.blocks > 0 ? std::min(p.blocks, max_blocks)
@@ -1742,6 +1765,8 @@ static int sssp_launch(const uint64_t *d_rowstarts, const int32_t *d_col, const 
     a.check_opens = p.check_opens != 0;
     a.big_deg = p.big_deg ? (unsigned)p.big_deg : SSSP_BIG_DEG;
     a.chunk = p.chunk ? (unsigned)p.chunk : SSSP_CHUNK;
+    a.perm = p.perm;
+    a.inv = p.inv;
     if (p.small && !d_roots) {
         sssp_small_kernel<<<1, SSSP_THREADS, 0, st>>>(a);
     } else if (blocks == 1) {  // nothing to co-schedule: a plain launch

@@ -164,6 +164,23 @@ int g5_csr_degree_order_workspace_size(uint64_t nverts, uint64_t nentries, uint6
 int g5_csr_degree_order(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t nentries,
                         int32_t *d_out_col, void *d_work, uint64_t work_bytes, void *stream);
 
+/* The SSSP copy renumbered for locality: vertices ordered by decreasing
+ * degree (ties by index), so the few vertices most relaxations target have
+ * their distances, stamps and bits side by side at the front of every
+ * per-vertex array, where they stay in L2.  In: the split copy from
+ * g5_csr_split_light with its row starts and counts.  Out: perm (caller's
+ * vertex -> search's), inv (back), and the copy in the new numbering (rows
+ * in the new order, each row's entries in the same order, neighbours
+ * renamed); pass them to g5_sssp_* with g5_sssp_params.perm / inv.
+ * Scratch: g5_csr_sssp_renumber_workspace_size(nverts).  No counterpart in
+ * the reference. */
+int g5_csr_sssp_renumber_workspace_size(uint64_t nverts, uint64_t *bytes);
+int g5_csr_sssp_renumber(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
+                         const uint32_t *d_light_deg, const uint32_t *d_tiny_deg, uint64_t nverts, uint64_t nentries,
+                         uint32_t *d_perm, uint32_t *d_inv, uint64_t *d_rowstarts_out, int32_t *d_col_out,
+                         float *d_w_out, uint32_t *d_light_out, uint32_t *d_tiny_out, void *d_work,
+                         uint64_t work_bytes, void *stream);
+
 /* Packs disjoint graphs into one CSR (no counterpart in the reference, which
  * holds one graph): copies one graph's CSR into the destination at vertex
  * offset vbase and entry offset ebase, shifting its column by vbase.  Call
@@ -353,6 +370,14 @@ typedef struct g5_sssp_params {
                        chunks across the grid; 0 = default (256)            */
     int32_t chunk;   /* edges per chunk, a multiple of 64 up to 65536; 0 =
                        default (256).  Neither tile changes a result        */
+    const uint32_t *perm; /* renumbered search (both set, from
+                       g5_csr_sssp_renumber) or not (both NULL): the CSR
+                       arguments (row starts, column, weights, light and
+                       tiny counts) are the renumbered copy, the root(s) and
+                       the outputs stay in the caller's numbering.  Same
+                       distances; each parent is still a tight edge's
+                       source (the smallest in the search's numbering)     */
+    const uint32_t *inv;
 } g5_sssp_params;
 
 int g5_sssp_workspace_size(uint64_t nverts, uint64_t *bytes);
