@@ -16,10 +16,14 @@ namespace g5compat {
 struct GraphExt {
     int32_t *col;        // int32 neighbour ids, rows in canonical order (as Oned_Graph.column)
     int32_t *bcol;       // the BFS copy (g5_csr_degree_order): rows by decreasing neighbour degree
-    int32_t *scol;       // the SSSP copy (g5_csr_split_light): tiny | light | heavy rows
+    // The SSSP copy: rows split tiny | light | heavy (g5_csr_split_light),
+    // renumbered by decreasing degree (g5_csr_sssp_renumber).
+    uint64_t *srowstarts;
+    int32_t *scol;
     float *sw;           // its weights
     uint32_t *light_deg; // light entries per row
     uint32_t *tiny_deg;  // leading tiny entries of each light part
+    uint32_t *perm, *inv;  // caller's vertex -> the copy's, and back
     uint32_t *isolated;  // bitmap of degree-0 vertices
     uint32_t *main_host; // host bitmap of the largest component (set by the first BFS state)
     float light_delta;

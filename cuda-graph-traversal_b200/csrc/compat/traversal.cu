@@ -34,27 +34,42 @@ Oned_Graph oned_graph_from_tuple_graph(Worker_State *ws, Tuple_Graph *tg, u64 ng
     const uint64_t e = g.nlocaledges;
     x.col = (int32_t *)gpu_push(ws, e * sizeof(int32_t), "int32 column");
     x.bcol = (int32_t *)gpu_push(ws, e * sizeof(int32_t), "BFS column");
+    x.srowstarts = (uint64_t *)gpu_push(ws, (nglobalverts + 1) * sizeof(uint64_t), "SSSP row starts");
     x.scol = (int32_t *)gpu_push(ws, e * sizeof(int32_t), "SSSP column");
     x.sw = (float *)gpu_push(ws, e * sizeof(float), "SSSP weights");
     x.light_deg = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "light degrees");
     x.tiny_deg = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "tiny degrees");
+    x.perm = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "SSSP numbering");
+    x.inv = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "SSSP numbering, inverse");
     x.light_delta = kLightDelta;
     x.main_host = nullptr;
     x.isolated = (uint32_t *)gpu_push(ws, (nglobalverts + 31) / 32 * sizeof(uint32_t), "isolated-vertex bitmap");
     // Rows in canonical order (sorted by neighbour, then weight), the SSSP
-    // copy and the BFS copy; the sorting scratch (sized for the degree
-    // order, the largest of the three) is the arena's last push, popped after.
-    uint64_t sbytes = 0;
+    // copy (split, then renumbered by decreasing degree) and the BFS copy;
+    // the scratch (the split copy in the caller's numbering and the sorting
+    // scratch, sized for the largest step) is the arena's last push, popped
+    // after.
+    uint64_t sbytes = 0, rbytes = 0;
     check(ws, g5_csr_degree_order_workspace_size(nglobalverts, e, &sbytes), "oned_graph_from_tuple_graph");
+    check(ws, g5_csr_sssp_renumber_workspace_size(nglobalverts, &rbytes), "oned_graph_from_tuple_graph");
+    sbytes = sbytes > rbytes ? sbytes : rbytes;
     const Arena before_sort = ws->gpu_arena;
+    int32_t *tcol = (int32_t *)gpu_push(ws, e * sizeof(int32_t), "split SSSP column (scratch)");
+    float *tw = (float *)gpu_push(ws, e * sizeof(float), "split SSSP weights (scratch)");
+    uint32_t *tlight = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "light degrees (scratch)");
+    uint32_t *ttiny = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "tiny degrees (scratch)");
     void *swork = gpu_push(ws, sbytes, "CSR sorting scratch");
     check(ws,
           g5_csr_fill_sorted((const uint64_t *)tg->edges, tg->weights, tg->edges_size, nglobalverts, g.rowstarts, e,
                              swork, sbytes, x.col, g.weights, g.column, 0),
           "oned_graph_from_tuple_graph");
     check(ws,
-          g5_csr_split_light(g.rowstarts, x.col, g.weights, nglobalverts, e, kLightDelta, x.scol, x.sw, x.light_deg,
-                             x.tiny_deg, swork, sbytes, 0),
+          g5_csr_split_light(g.rowstarts, x.col, g.weights, nglobalverts, e, kLightDelta, tcol, tw, tlight, ttiny,
+                             swork, sbytes, 0),
+          "oned_graph_from_tuple_graph");
+    check(ws,
+          g5_csr_sssp_renumber(g.rowstarts, tcol, tw, tlight, ttiny, nglobalverts, e, x.perm, x.inv, x.srowstarts,
+                               x.scol, x.sw, x.light_deg, x.tiny_deg, swork, sbytes, 0),
           "oned_graph_from_tuple_graph");
     check(ws, g5_csr_degree_order(g.rowstarts, x.col, nglobalverts, e, x.bcol, swork, sbytes, 0),
           "oned_graph_from_tuple_graph");
@@ -234,7 +249,9 @@ void oned_graph_sssp_run(Worker_State *ws, const Oned_Graph *g, Sssp_State *sssp
     // state) runs on one block: its search touches a handful of vertices.
     const bool small = gx->main_host && !((gx->main_host[root >> 5] >> (root & 31)) & 1u);
     g5_sssp_params p = {kLightDelta, small ? 1 : 0, 0.0f, 0, small ? 1 : 0, gx->tiny_deg, 0};
-    check(ws, g5_sssp_traverse(g->rowstarts, gx->scol, gx->sw, gx->light_deg, gx->light_delta, g->nglobalverts,
+    p.perm = gx->perm;  // the SSSP copy is renumbered; root and outputs stay the caller's
+    p.inv = gx->inv;
+    check(ws, g5_sssp_traverse(gx->srowstarts, gx->scol, gx->sw, gx->light_deg, gx->light_delta, g->nglobalverts,
                                root, sssp->dist, sssp->pred, sx->work, sx->work_bytes, &p, 0),
           "oned_graph_sssp_run");
     check(ws, g5_sssp_last_status(sx->work, sx->work_bytes, nullptr, nullptr, 0), "oned_graph_sssp_run");
