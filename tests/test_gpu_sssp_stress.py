@@ -112,3 +112,47 @@ def test_sssp_checked_opens_small_graph_dense_buckets(cgt, oracle, delta):
                                         small=False, check_opens=True)
                 cgt.sssp_status(s)
                 assert np.array_equal(_np(s.dist).view(np.uint32), od.view(np.uint32)), (r, blocks, pull, sub_min)
+
+
+def test_renumbered_copy_same_distances(cgt, oracle):
+    """The SSSP on its degree-renumbered copy (the default) and on the split
+    copy in the caller's numbering give bit-identical distances and valid
+    parents, for main-component and small-component roots, with and without
+    pre-filled outputs; the copy holds each row's entries renamed, in order;
+    perm and inv are inverse permutations; perm without inv is refused."""
+    scale = 16
+    g = cgt.oned_graph_from_kronecker(cgt.make_mrg_seed(2, 3), scale, 16 << scale)
+    assert g.sr is not None
+    n = g.nglobalverts
+    perm, inv = _np(g.sr.perm).astype(np.int64), _np(g.sr.inv).astype(np.int64)
+    assert np.array_equal(perm[inv], np.arange(n)) and np.array_equal(np.sort(perm), np.arange(n))
+    deg = np.diff(_np(g.rowstarts))
+    assert (np.diff(deg[inv]) <= 0).all()  # decreasing degree
+    rs, rs2 = _np(g.rowstarts), _np(g.sr.rowstarts)
+    scol, scol2 = _np(g.scol).astype(np.int64), _np(g.sr.col).astype(np.int64)
+    for i in (0, 1, 2, n // 2, n - 1):
+        o = inv[i]
+        assert np.array_equal(perm[scol[rs[o]:rs[o + 1]]], scol2[rs2[i]:rs2[i + 1]])
+        assert _np(g.sr.light_deg)[i] == _np(g.light_deg)[o] and _np(g.sr.tiny_deg)[i] == _np(g.tiny_deg)[o]
+    roots = cgt.generate_bfs_roots(g, 2, 3, 64)
+    small = [r for r in roots if not g.in_main_component(r)]
+    plain = cgt.oned_graph_from_kronecker(cgt.make_mrg_seed(2, 3), scale, 16 << scale, sssp_renumber=False)
+    a, b, vw = cgt.SsspState(g), cgt.SsspState(plain), cgt._val_work(g)
+    for r in roots[:4] + small[:2]:
+        for prefill in (True, False):
+            if prefill:
+                cgt.oned_graph_sssp_run(g, a, r)
+            else:
+                cgt.oned_graph_sssp_reset(a)
+                cgt.lib.g5_sssp_reset(n, None, None, cgt._ptr(a.work), a.work.numel(), None)
+                a.was_reset = True
+                cgt.oned_graph_sssp_traverse(g, a, r)
+            cgt.sssp_status(a)
+            cgt.oned_graph_sssp_run(plain, b, r)
+            assert torch.equal(a.dist.view(torch.int32), b.dist.view(torch.int32)), (r, prefill)
+            assert cgt.sssp_validate(g, r, a.dist, a.pred, vw) == 0, (r, prefill)
+    p = cgt.SsspParams(0.1, 0, 0.0, 0, 0, None, 0, 0, 0, cgt._ptr(g.sr.perm), None)
+    rc = cgt.lib.g5_sssp_traverse(cgt._ptr(g.sr.rowstarts), cgt._ptr(g.sr.col), cgt._ptr(g.sr.w), cgt._ptr(g.sr.light_deg),
+                                  g.light_delta, n, int(roots[0]), cgt._ptr(a.dist), cgt._ptr(a.pred), cgt._ptr(a.work),
+                                  a.work.numel(), cgt.C.byref(p), None)
+    assert rc == -1 and b"perm and inv" in cgt.lib.g5_last_error()
