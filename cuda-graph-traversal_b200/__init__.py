@@ -533,17 +533,18 @@ class PackedGraphs:
         return slice(int(self.vbase[i]), int(self.vbase[i] + self.nverts[i]))
 
 
-def pack_graphs(graphs, roots, device="cuda", stream=None) -> PackedGraphs:
+def pack_graphs(graphs, roots, device="cuda", stream=None, sssp_renumber: bool = True) -> PackedGraphs:
     """Packs the OnedGraphs in `graphs`; roots[i] is graph i's root (its own
     vertex number).  pack_kronecker builds and packs generated graphs one
-    at a time instead, without holding them all unpacked."""
+    at a time instead, without holding them all unpacked.  sssp_renumber:
+    the union also gets the SSSP's renumbered copy (oned_graph_sssp_renumber)."""
     graphs = list(graphs)
     sizes = [(g.nglobalverts, g.nlocaledges) for g in graphs]
-    return _pack(sizes, iter(graphs), roots, device, graphs[0].light_delta if graphs else 0.1, stream)
+    return _pack(sizes, iter(graphs), roots, device, graphs[0].light_delta if graphs else 0.1, stream, sssp_renumber)
 
 
 def pack_kronecker(scales, edgefactor: int = 16, seed1_base: int = 2, seed2: int = 3, device="cuda",
-                   light_delta: float = 0.1, stream=None) -> PackedGraphs:
+                   light_delta: float = 0.1, stream=None, sssp_renumber: bool = True) -> PackedGraphs:
     """Generates Kronecker graph i (SCALE scales[i], seeds (seed1_base + i,
     seed2)) with the fused generator -> CSR path and packs it at once; each
     graph's root is its first Graph500 root (the runner's choice)."""
@@ -561,10 +562,10 @@ def pack_kronecker(scales, edgefactor: int = 16, seed1_base: int = 2, seed2: int
             roots.append(r[0] if r else 0)
             yield g
 
-    return _pack(sizes, gen(), roots, device, light_delta, stream)
+    return _pack(sizes, gen(), roots, device, light_delta, stream, sssp_renumber)
 
 
-def _pack(sizes, graphs, roots, device, light_delta, stream) -> PackedGraphs:
+def _pack(sizes, graphs, roots, device, light_delta, stream, sssp_renumber=True) -> PackedGraphs:
     N = sum(n for n, _ in sizes)
     Emax = sum(e for _, e in sizes)
     if N > (1 << 31):
@@ -593,6 +594,8 @@ def _pack(sizes, graphs, roots, device, light_delta, stream) -> PackedGraphs:
     # Packed rows keep their order; the split (a no-op on split rows) yields
     # the packed graph's tiny counts.
     u.tiny_deg = _split_tiny(u.rowstarts, u.col, u.w, None, u.light_deg, vb, light_delta, st)
+    if sssp_renumber:
+        oned_graph_sssp_renumber(u, stream)
     return PackedGraphs(nverts, vbase, u, list(roots))
 
 
