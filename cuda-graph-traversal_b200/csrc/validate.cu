@@ -184,26 +184,41 @@ __global__ void __launch_bounds__(VAL_THREADS) edge_count_kernel(const uint64_t 
     block_add(out, cnt);
 }
 
-// A neighbour's values for the edge rules, packed into one 16-byte record:
-// BFS {dist, pred}; SSSP {dist bits, pred}.
+// A vertex's values for the edge rules, packed into one 16-byte record in
+// the CSR's numbering: BFS {dist, pred}; SSSP {dist bits, pred}.  With a
+// renumbered CSR (perm: caller's vertex -> CSR's, inv back) record v holds
+// caller's vertex inv[v], its parent renamed by perm (-1 kept; a parent
+// that is not a vertex becomes -2, which equals no vertex, as the raw value
+// did).
+__device__ __forceinline__ int64_t val_parent(int64_t p, uint64_t n, const unsigned *perm) {
+    if (!perm || p == -1) return p;
+    return p >= 0 && (uint64_t)p < n ? (int64_t)__ldg(&perm[p]) : -2;
+}
+
 __global__ void val_pack_bfs_kernel(const int64_t *__restrict__ dist, const int64_t *__restrict__ pred, uint64_t n,
+                                    const unsigned *__restrict__ perm, const unsigned *__restrict__ inv,
                                     longlong2 *__restrict__ vx) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
-        vx[v] = make_longlong2(dist[v], pred[v]);
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        const uint64_t o = inv ? __ldg(&inv[v]) : v;
+        vx[v] = make_longlong2(dist[o], val_parent(pred[o], n, perm));
+    }
 }
 
 __global__ void val_pack_sssp_kernel(const float *__restrict__ dist, const int64_t *__restrict__ pred, uint64_t n,
+                                     const unsigned *__restrict__ perm, const unsigned *__restrict__ inv,
                                      longlong2 *__restrict__ vx) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
-        vx[v] = make_longlong2((long long)__float_as_uint(dist[v]), pred[v]);
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        const uint64_t o = inv ? __ldg(&inv[v]) : v;
+        vx[v] = make_longlong2((long long)__float_as_uint(dist[o]), val_parent(pred[o], n, perm));
+    }
 }
 
 // Rules 1-2 (examples/graph500_runner.cu:84-109).
 __global__ void bfs_val_vertex_kernel(const int64_t *__restrict__ pred, const int64_t *__restrict__ dist, uint64_t n,
-                                      uint64_t root, unsigned *__restrict__ confirmed,
-                                      unsigned long long *__restrict__ errors) {
+                                      uint64_t root, const unsigned *__restrict__ perm,
+                                      unsigned *__restrict__ confirmed, unsigned long long *__restrict__ errors) {
     unsigned long long err = 0;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
@@ -211,7 +226,10 @@ __global__ void bfs_val_vertex_kernel(const int64_t *__restrict__ pred, const in
         if (p != -1 && (p < 0 || (uint64_t)p >= n)) ++err;
         if (v == root) {
             if (p != (int64_t)root || dist[v] != 0) ++err;
-            else atomicOr(&confirmed[v >> 5], 1u << (v & 31));
+            else {
+                const uint64_t r = perm ? __ldg(&perm[v]) : v;  // the bitmap is in the CSR's numbering
+                atomicOr(&confirmed[r >> 5], 1u << (r & 31));
+            }
         }
     }
     block_add(errors, err);
@@ -220,8 +238,6 @@ __global__ void bfs_val_vertex_kernel(const int64_t *__restrict__ pred, const in
 // Rules 3-6 (examples/graph500_runner.cu:111-153), one thread per CSR entry.
 __global__ void __launch_bounds__(VAL_THREADS, 2) bfs_val_edge_kernel(const uint64_t *__restrict__ rowptr,
                                                                    const int *__restrict__ col, uint64_t n,
-                                                                   const int64_t *__restrict__ pred,
-                                                                   const int64_t *__restrict__ dist,
                                                                    const longlong2 *__restrict__ vx,
                                                                    const unsigned *__restrict__ trow,
                                                                    const unsigned long long *__restrict__ table,
@@ -250,10 +266,11 @@ __global__ void __launch_bounds__(VAL_THREADS, 2) bfs_val_edge_kernel(const uint
                           ++err;
                           continue;
                       }
-                      if (uu != ur) {
+                      if (uu != ur) {  // the row's own record
                           ur = uu;
-                          ud = __ldg(&dist[uu]);
-                          up = __ldg(&pred[uu]);
+                          const longlong2 uv = __ldg(&vx[uu]);
+                          ud = uv.x;
+                          up = uv.y;
                       }
                       const int64_t xd = xv[k].x, xp = xv[k].y;
                       if ((ud == -1) != (xd == -1)) ++err;
@@ -265,23 +282,25 @@ __global__ void __launch_bounds__(VAL_THREADS, 2) bfs_val_edge_kernel(const uint
     block_add(errors, err);
 }
 
-// Rule 7 (examples/graph500_runner.cu:155-169).
-__global__ void bfs_val_confirm_kernel(const int64_t *__restrict__ pred, const int64_t *__restrict__ dist, uint64_t n,
-                                       uint64_t root, const unsigned *__restrict__ confirmed,
+// Rule 7 (examples/graph500_runner.cu:155-169), over the records (the
+// CSR's numbering; root = the root's number there).
+__global__ void bfs_val_confirm_kernel(const longlong2 *__restrict__ vx, uint64_t n, uint64_t root,
+                                       const unsigned *__restrict__ confirmed,
                                        unsigned long long *__restrict__ errors) {
     unsigned long long err = 0;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
-        if (pred[v] == -1) continue;
+        const longlong2 r = vx[v];
+        if (r.y == -1) continue;
         const bool conf = (confirmed[v >> 5] >> (v & 31)) & 1u;
-        if (dist[v] == INT64_MAX || (v != root && !conf)) ++err;
+        if (r.x == INT64_MAX || (v != root && !conf)) ++err;
     }
     block_add(errors, err);
 }
 
 __global__ void sssp_val_vertex_kernel(const float *__restrict__ dist, const int64_t *__restrict__ pred, uint64_t n,
-                                       uint64_t root, unsigned *__restrict__ confirmed,
-                                       unsigned long long *__restrict__ errors) {
+                                       uint64_t root, const unsigned *__restrict__ perm,
+                                       unsigned *__restrict__ confirmed, unsigned long long *__restrict__ errors) {
     unsigned long long err = 0;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
@@ -289,7 +308,8 @@ __global__ void sssp_val_vertex_kernel(const float *__restrict__ dist, const int
         const float d = dist[v];
         if (v == root) {
             if (d != 0.0f || p != (int64_t)root) ++err;
-            atomicOr(&confirmed[v >> 5], 1u << (v & 31));
+            const uint64_t r = perm ? __ldg(&perm[v]) : v;  // the bitmap is in the CSR's numbering
+            atomicOr(&confirmed[r >> 5], 1u << (r & 31));
         }
         if ((p == -1) != (d == -1.0f)) ++err;
         if (p != -1 && (p < 0 || (uint64_t)p >= n)) ++err;
@@ -300,7 +320,6 @@ __global__ void sssp_val_vertex_kernel(const float *__restrict__ dist, const int
 __global__ void __launch_bounds__(VAL_THREADS, 3) sssp_val_edge_kernel(const uint64_t *__restrict__ rowptr,
                                                                     const int *__restrict__ col,
                                                                     const float *__restrict__ w, uint64_t n,
-                                                                    const float *__restrict__ dist,
                                                                     const longlong2 *__restrict__ vx,
                                                                     const unsigned *__restrict__ trow,
                                                                     const unsigned long long *__restrict__ table,
@@ -318,9 +337,9 @@ __global__ void __launch_bounds__(VAL_THREADS, 3) sssp_val_edge_kernel(const uin
                   float d = -1.0f;
 #pragma unroll
                   for (int k = 0; k < RULE_ITEMS; ++k) {
-                      if (k < ne && u[k] != ur) {
+                      if (k < ne && u[k] != ur) {  // the row's own record
                           ur = u[k];
-                          d = __ldg(&dist[ur]);
+                          d = __uint_as_float((unsigned)__ldg(&vx[ur]).x);
                       }
                       du[k] = k < ne ? d : -1.0f;
                   }
@@ -350,13 +369,13 @@ __global__ void __launch_bounds__(VAL_THREADS, 3) sssp_val_edge_kernel(const uin
     block_add(errors, err);
 }
 
-__global__ void sssp_val_confirm_kernel(const float *__restrict__ dist, uint64_t n,
+__global__ void sssp_val_confirm_kernel(const longlong2 *__restrict__ vx, uint64_t n,
                                         const unsigned *__restrict__ confirmed,
                                         unsigned long long *__restrict__ errors) {
     unsigned long long err = 0;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
-        if (dist[v] != -1.0f && !((confirmed[v >> 5] >> (v & 31)) & 1u)) ++err;
+        if (__uint_as_float((unsigned)vx[v].x) != -1.0f && !((confirmed[v >> 5] >> (v & 31)) & 1u)) ++err;
     block_add(errors, err);
 }
 
@@ -435,12 +454,14 @@ extern "C" int g5_edge_count(const uint64_t *d_rowstarts, const int32_t *d_col, 
     return val_finish(w, count, st);
 }
 
-extern "C" int g5_bfs_validate(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
-                               const int64_t *d_pred, const int64_t *d_dist, void *d_work, uint64_t work_bytes,
-                               uint64_t *errors, void *stream) {
+extern "C" int g5_bfs_validate_renumbered(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
+                                          uint64_t root, const int64_t *d_pred, const int64_t *d_dist,
+                                          const uint32_t *d_perm, const uint32_t *d_inv, void *d_work,
+                                          uint64_t work_bytes, uint64_t *errors, void *stream) {
     clear_error();
     G5_CHECK_ARG(d_rowstarts && d_col && d_pred && d_dist && errors, "g5_bfs_validate: NULL argument");
     G5_CHECK_ARG(root < nverts, "g5_bfs_validate: root out of range");
+    G5_CHECK_ARG((d_perm == nullptr) == (d_inv == nullptr), "g5_bfs_validate: give both perm and inv or neither");
     ValWork w;
     int grid = 0;
     int rc = val_prepare(nverts, d_work, work_bytes, &w, &grid, "g5_bfs_validate");
@@ -448,20 +469,37 @@ extern "C" int g5_bfs_validate(const uint64_t *d_rowstarts, const int32_t *d_col
     cudaStream_t st = (cudaStream_t)stream;
     G5_CUDA_TRY(cudaMemsetAsync(w.confirmed, 0, (nverts + 31) / 32 * sizeof(unsigned), st));
     if ((rc = val_tiles(d_rowstarts, nverts, w, grid, st))) return rc;
-    bfs_val_vertex_kernel<<<grid, VAL_THREADS, 0, st>>>(d_pred, d_dist, nverts, root, w.confirmed, w.counter);
-    val_pack_bfs_kernel<<<grid, VAL_THREADS, 0, st>>>(d_dist, d_pred, nverts, w.vx);
-    bfs_val_edge_kernel<<<grid, VAL_THREADS, 0, st>>>(d_rowstarts, d_col, nverts, d_pred, d_dist, w.vx, w.trow,
-                                                      &w.counter[1], w.confirmed, w.counter);
-    bfs_val_confirm_kernel<<<grid, VAL_THREADS, 0, st>>>(d_pred, d_dist, nverts, root, w.confirmed, w.counter);
+    uint64_t root_csr = root;
+    if (d_perm) {
+        uint32_t r = 0;
+        G5_CUDA_TRY(cudaMemcpyAsync(&r, d_perm + root, sizeof r, cudaMemcpyDeviceToHost, st));
+        G5_CUDA_TRY(cudaStreamSynchronize(st));
+        root_csr = r;
+    }
+    bfs_val_vertex_kernel<<<grid, VAL_THREADS, 0, st>>>(d_pred, d_dist, nverts, root, d_perm, w.confirmed,
+                                                        w.counter);
+    val_pack_bfs_kernel<<<grid, VAL_THREADS, 0, st>>>(d_dist, d_pred, nverts, d_perm, d_inv, w.vx);
+    bfs_val_edge_kernel<<<grid, VAL_THREADS, 0, st>>>(d_rowstarts, d_col, nverts, w.vx, w.trow, &w.counter[1],
+                                                      w.confirmed, w.counter);
+    bfs_val_confirm_kernel<<<grid, VAL_THREADS, 0, st>>>(w.vx, nverts, root_csr, w.confirmed, w.counter);
     return val_finish(w, errors, st);
 }
 
-extern "C" int g5_sssp_validate(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, uint64_t nverts,
-                                uint64_t root, const float *d_dist, const int64_t *d_pred, void *d_work,
-                                uint64_t work_bytes, uint64_t *errors, void *stream) {
+extern "C" int g5_bfs_validate(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
+                               const int64_t *d_pred, const int64_t *d_dist, void *d_work, uint64_t work_bytes,
+                               uint64_t *errors, void *stream) {
+    return g5_bfs_validate_renumbered(d_rowstarts, d_col, nverts, root, d_pred, d_dist, nullptr, nullptr, d_work,
+                                      work_bytes, errors, stream);
+}
+
+extern "C" int g5_sssp_validate_renumbered(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w,
+                                           uint64_t nverts, uint64_t root, const float *d_dist,
+                                           const int64_t *d_pred, const uint32_t *d_perm, const uint32_t *d_inv,
+                                           void *d_work, uint64_t work_bytes, uint64_t *errors, void *stream) {
     clear_error();
     G5_CHECK_ARG(d_rowstarts && d_col && d_w && d_pred && d_dist && errors, "g5_sssp_validate: NULL argument");
     G5_CHECK_ARG(root < nverts, "g5_sssp_validate: root out of range");
+    G5_CHECK_ARG((d_perm == nullptr) == (d_inv == nullptr), "g5_sssp_validate: give both perm and inv or neither");
     ValWork w;
     int grid = 0;
     int rc = val_prepare(nverts, d_work, work_bytes, &w, &grid, "g5_sssp_validate");
@@ -469,10 +507,18 @@ extern "C" int g5_sssp_validate(const uint64_t *d_rowstarts, const int32_t *d_co
     cudaStream_t st = (cudaStream_t)stream;
     G5_CUDA_TRY(cudaMemsetAsync(w.confirmed, 0, (nverts + 31) / 32 * sizeof(unsigned), st));
     if ((rc = val_tiles(d_rowstarts, nverts, w, grid, st))) return rc;
-    sssp_val_vertex_kernel<<<grid, VAL_THREADS, 0, st>>>(d_dist, d_pred, nverts, root, w.confirmed, w.counter);
-    val_pack_sssp_kernel<<<grid, VAL_THREADS, 0, st>>>(d_dist, d_pred, nverts, w.vx);
-    sssp_val_edge_kernel<<<grid, VAL_THREADS, 0, st>>>(d_rowstarts, d_col, d_w, nverts, d_dist, w.vx, w.trow,
-                                                       &w.counter[1], w.confirmed, w.counter);
-    sssp_val_confirm_kernel<<<grid, VAL_THREADS, 0, st>>>(d_dist, nverts, w.confirmed, w.counter);
+    sssp_val_vertex_kernel<<<grid, VAL_THREADS, 0, st>>>(d_dist, d_pred, nverts, root, d_perm, w.confirmed,
+                                                         w.counter);
+    val_pack_sssp_kernel<<<grid, VAL_THREADS, 0, st>>>(d_dist, d_pred, nverts, d_perm, d_inv, w.vx);
+    sssp_val_edge_kernel<<<grid, VAL_THREADS, 0, st>>>(d_rowstarts, d_col, d_w, nverts, w.vx, w.trow, &w.counter[1],
+                                                       w.confirmed, w.counter);
+    sssp_val_confirm_kernel<<<grid, VAL_THREADS, 0, st>>>(w.vx, nverts, w.confirmed, w.counter);
     return val_finish(w, errors, st);
+}
+
+extern "C" int g5_sssp_validate(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, uint64_t nverts,
+                                uint64_t root, const float *d_dist, const int64_t *d_pred, void *d_work,
+                                uint64_t work_bytes, uint64_t *errors, void *stream) {
+    return g5_sssp_validate_renumbered(d_rowstarts, d_col, d_w, nverts, root, d_dist, d_pred, nullptr, nullptr,
+                                       d_work, work_bytes, errors, stream);
 }

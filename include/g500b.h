@@ -472,6 +472,22 @@ int g5_sssp_validate(const uint64_t *d_rowstarts, const int32_t *d_col, const fl
                      uint64_t root, const float *d_dist, const int64_t *d_pred, void *d_work, uint64_t work_bytes,
                      uint64_t *errors, void *stream);
 
+/* The two validators on a renumbered CSR (perm: caller's vertex -> the CSR's,
+ * inv back, e.g. the copy from g5_csr_sssp_renumber, whose rows hold every
+ * entry of the graph): pred, dist and root stay in the caller's numbering;
+ * the same error counts as on the graph in the caller's numbering.  The
+ * records the rules read (a vertex's depth or distance and parent) then lie
+ * in degree order, so the neighbours most entries point at share a few L2
+ * lines.  NULL perm and inv: g5_bfs_validate / g5_sssp_validate. */
+int g5_bfs_validate_renumbered(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint64_t root,
+                               const int64_t *d_pred, const int64_t *d_dist, const uint32_t *d_perm,
+                               const uint32_t *d_inv, void *d_work, uint64_t work_bytes, uint64_t *errors,
+                               void *stream);
+int g5_sssp_validate_renumbered(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, uint64_t nverts,
+                                uint64_t root, const float *d_dist, const int64_t *d_pred, const uint32_t *d_perm,
+                                const uint32_t *d_inv, void *d_work, uint64_t work_bytes, uint64_t *errors,
+                                void *stream);
+
 /* ------------------------------------------------------- batched BFS --- */
 /*
  * Multi-source BFS: up to 256 roots searched together in one persistent

@@ -150,7 +150,21 @@ def test_renumbered_copy_same_distances(cgt, oracle):
             cgt.sssp_status(a)
             cgt.oned_graph_sssp_run(plain, b, r)
             assert torch.equal(a.dist.view(torch.int32), b.dist.view(torch.int32)), (r, prefill)
-            assert cgt.sssp_validate(g, r, a.dist, a.pred, vw) == 0, (r, prefill)
+            assert cgt.sssp_validate(g, r, a.dist, a.pred, vw) == 0, (r, prefill)  # on the renumbered copy
+            assert cgt.sssp_validate(plain, r, a.dist, a.pred, vw) == 0, (r, prefill)  # in the caller's numbering
+    # planted mistakes: both validators count the same errors
+    bad = a.dist.clone()
+    bad[torch.nonzero(bad > 0)[:5, 0]] *= 1.25
+    assert cgt.sssp_validate(g, roots[0], bad, a.pred, vw) == cgt.sssp_validate(plain, roots[0], bad, a.pred, vw) > 0
+    bfs = cgt.BfsState(g)
+    cgt.oned_graph_bfs_run(g, bfs, roots[0])
+    d = cgt.bfs_compute_dist_from_pred(g, bfs, roots[0])
+    assert cgt.bfs_validate(g, roots[0], bfs.pred, d, vw) == cgt.bfs_validate(plain, roots[0], bfs.pred, d, vw) == 0
+    badp = bfs.pred.clone()
+    reached = torch.nonzero(badp >= 0)[:, 0]
+    badp[reached[1:6]] = reached[10:15]
+    badp[reached[6]] = n + 7
+    assert cgt.bfs_validate(g, roots[0], badp, d, vw) == cgt.bfs_validate(plain, roots[0], badp, d, vw) > 0
     p = cgt.SsspParams(0.1, 0, 0.0, 0, 0, None, 0, 0, 0, cgt._ptr(g.sr.perm), None)
     rc = cgt.lib.g5_sssp_traverse(cgt._ptr(g.sr.rowstarts), cgt._ptr(g.sr.col), cgt._ptr(g.sr.w), cgt._ptr(g.sr.light_deg),
                                   g.light_delta, n, int(roots[0]), cgt._ptr(a.dist), cgt._ptr(a.pred), cgt._ptr(a.work),
