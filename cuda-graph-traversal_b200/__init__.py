@@ -353,10 +353,14 @@ def oned_graph_sssp_renumber(g: OnedGraph, stream=None) -> OnedGraph:
     return g
 
 
-def _sssp_csr(g: OnedGraph):
+def _sssp_csr(g: OnedGraph, small: bool = False):
     """(row starts, column, weights, light counts, tiny counts, perm, inv)
-    the SSSP entry points are given."""
-    if g.sr is not None:
+    the SSSP entry points are given: the renumbered copy for the grid
+    search, the split copy in the caller's numbering for the one-block
+    search of a small component (it touches a handful of vertices, so the
+    numbering buys nothing there and its mapping would add dependent loads
+    to a search that takes microseconds)."""
+    if g.sr is not None and not small:
         r = g.sr
         return r.rowstarts, r.col, r.w, r.light_deg, r.tiny_deg, r.perm, r.inv
     return g.rowstarts, g.sssp_col, g.sssp_w, g.light_deg, g.tiny_deg, None, None
@@ -1013,7 +1017,7 @@ def _sssp_params(g: OnedGraph, root: int, delta, blocks, pull, sub_min, small, c
     # component (when the grid is left to the library).
     if small is None:
         small = blocks == 0 and not g.in_main_component(root)
-    _, _, _, _, tiny, perm, inv = _sssp_csr(g)
+    _, _, _, _, tiny, perm, inv = _sssp_csr(g, bool(small))
     return SsspParams(delta, 1 if small and blocks == 0 else blocks, pull, sub_min, int(bool(small)),
                       _ptr(tiny), int(bool(check_opens)), big_deg, chunk, _ptr(perm), _ptr(inv))
 
@@ -1026,7 +1030,7 @@ def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float =
     fail the search if a queue held a vertex twice (a test aid).  big_deg /
     chunk: the work tiles of g5_sssp_params (0 = defaults)."""
     p = _sssp_params(g, root, delta, blocks, pull, sub_min, small, check_opens, big_deg, chunk)
-    rs, col, w, light = _sssp_csr(g)[:4]
+    rs, col, w, light = _sssp_csr(g, bool(p.small))[:4]
     _check(lib.g5_sssp_run(_ptr(rs), _ptr(col), _ptr(w), _ptr(light), g.light_delta,
                            g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                            sssp.work.numel(), C.byref(p), _stream(stream)))
@@ -1052,7 +1056,7 @@ def oned_graph_sssp_traverse(g: OnedGraph, sssp: SsspState, root: int, delta: fl
     """The search itself, on a reset state (the lean one-block search for a
     root outside the main component)."""
     p = _sssp_params(g, root, delta, blocks, pull, sub_min, small, check_opens, big_deg, chunk)
-    rs, col, w, light = _sssp_csr(g)[:4]
+    rs, col, w, light = _sssp_csr(g, bool(p.small))[:4]
     _check(lib.g5_sssp_traverse(_ptr(rs), _ptr(col), _ptr(w), _ptr(light),
                                 g.light_delta,
                                 g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),

@@ -607,7 +607,28 @@ __global__ void vertex_perm_kernel(const unsigned *__restrict__ inv, const unsig
 }
 
 // Row i of the renumbered copy = row inv[i] of the source, in the same
-// order, its neighbours renamed by perm (one warp per row).
+// order, its neighbours renamed by perm.  Rows of at most RENUM_LONG entries
+// take a warp each; the longer ones -- a prefix of the new order, which is
+// by decreasing length -- a block each (renumber_long_rows_kernel).
+constexpr unsigned RENUM_LONG = 2048;
+
+template <int STEP>
+__device__ __forceinline__ void renumber_copy(const int *__restrict__ col, const float *__restrict__ w, uint64_t b,
+                                              uint64_t len, uint64_t b2, uint64_t n, const unsigned *__restrict__ perm,
+                                              int *__restrict__ col2, float *__restrict__ w2, unsigned *err,
+                                              unsigned t) {
+    for (uint64_t k = t; k < len; k += STEP) {
+        const unsigned v = (unsigned)__ldg(&col[b + k]);
+        if (v >= n) {
+            atomicOr(err, SORTERR_RANGE);
+            col2[b2 + k] = (int)v;  // kept out of range: the search reports it
+        } else {
+            col2[b2 + k] = (int)__ldg(&perm[v]);
+        }
+        w2[b2 + k] = __ldg(&w[b + k]);
+    }
+}
+
 __global__ void renumber_rows_kernel(const uint64_t *__restrict__ rs, const int *__restrict__ col,
                                      const float *__restrict__ w, const unsigned *__restrict__ light,
                                      const unsigned *__restrict__ tiny, uint64_t n, const unsigned *__restrict__ perm,
@@ -623,16 +644,19 @@ __global__ void renumber_rows_kernel(const uint64_t *__restrict__ rs, const int 
             light2[i] = __ldg(&light[o]);
             tiny2[i] = __ldg(&tiny[o]);
         }
-        for (uint64_t k = lane; k < len; k += 32) {
-            const unsigned v = (unsigned)__ldg(&col[b + k]);
-            if (v >= n) {
-                atomicOr(err, SORTERR_RANGE);
-                col2[b2 + k] = (int)v;  // kept out of range: the search reports it
-            } else {
-                col2[b2 + k] = (int)__ldg(&perm[v]);
-            }
-            w2[b2 + k] = __ldg(&w[b + k]);
-        }
+        if (len <= RENUM_LONG) renumber_copy<32>(col, w, b, len, b2, n, perm, col2, w2, err, lane);
+    }
+}
+
+__global__ void renumber_long_rows_kernel(const uint64_t *__restrict__ rs, const int *__restrict__ col,
+                                          const float *__restrict__ w, uint64_t n, const unsigned *__restrict__ perm,
+                                          const unsigned *__restrict__ inv, const uint64_t *__restrict__ rs2,
+                                          int *__restrict__ col2, float *__restrict__ w2, unsigned *__restrict__ err) {
+    for (uint64_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const uint64_t b2 = __ldg(&rs2[i]), len = __ldg(&rs2[i + 1]) - b2;
+        if (len <= RENUM_LONG) break;  // the rest of the new order is shorter still (block-uniform)
+        const uint64_t b = __ldg(&rs[__ldg(&inv[i])]);
+        renumber_copy<256>(col, w, b, len, b2, n, perm, col2, w2, err, threadIdx.x);
     }
 }
 
@@ -1047,6 +1071,8 @@ extern "C" int g5_csr_sssp_renumber(const uint64_t *d_rowstarts, const int32_t *
     renumber_rows_kernel<<<grid, 256, 0, st>>>(d_rowstarts, d_col, d_w, d_light_deg, d_tiny_deg, nverts, d_perm, d_inv,
                                                d_rowstarts_out, d_col_out, d_w_out, d_light_out, d_tiny_out,
                                                &w.cnt[2]);
+    renumber_long_rows_kernel<<<grid, 256, 0, st>>>(d_rowstarts, d_col, d_w, nverts, d_perm, d_inv, d_rowstarts_out,
+                                                    d_col_out, d_w_out, &w.cnt[2]);
     G5_CUDA_TRY(cudaGetLastError());
     unsigned errs = 0;
     G5_CUDA_TRY(cudaMemcpyAsync(&errs, &w.cnt[2], sizeof errs, cudaMemcpyDeviceToHost, st));

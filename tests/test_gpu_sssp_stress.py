@@ -165,6 +165,22 @@ def test_renumbered_copy_same_distances(cgt, oracle):
     badp[reached[1:6]] = reached[10:15]
     badp[reached[6]] = n + 7
     assert cgt.bfs_validate(g, roots[0], badp, d, vw) == cgt.bfs_validate(plain, roots[0], badp, d, vw) > 0
+    # the one-block search on the renumbered copy (the Python API runs small
+    # components on the caller-numbered copy; the C ABI and the reference
+    # API can run them on either)
+    for r in small[:2]:
+        cgt.oned_graph_sssp_run(plain, b, r)
+        for rep in range(2):  # the second reset undoes only this search's vertices
+            cgt.oned_graph_sssp_reset(a)
+            ps = cgt.SsspParams(0.1, 1, 0.0, 0, 1, cgt._ptr(g.sr.tiny_deg), 0, 0, 0, cgt._ptr(g.sr.perm),
+                                cgt._ptr(g.sr.inv))
+            assert cgt.lib.g5_sssp_traverse(cgt._ptr(g.sr.rowstarts), cgt._ptr(g.sr.col), cgt._ptr(g.sr.w),
+                                            cgt._ptr(g.sr.light_deg), g.light_delta, n, int(r), cgt._ptr(a.dist),
+                                            cgt._ptr(a.pred), cgt._ptr(a.work), a.work.numel(), cgt.C.byref(ps),
+                                            None) == 0
+            cgt.sssp_status(a)
+            assert torch.equal(a.dist.view(torch.int32), b.dist.view(torch.int32)), (r, rep)
+            assert cgt.sssp_validate(g, r, a.dist, a.pred, vw) == 0, (r, rep)
     p = cgt.SsspParams(0.1, 0, 0.0, 0, 0, None, 0, 0, 0, cgt._ptr(g.sr.perm), None)
     rc = cgt.lib.g5_sssp_traverse(cgt._ptr(g.sr.rowstarts), cgt._ptr(g.sr.col), cgt._ptr(g.sr.w), cgt._ptr(g.sr.light_deg),
                                   g.light_delta, n, int(roots[0]), cgt._ptr(a.dist), cgt._ptr(a.pred), cgt._ptr(a.work),
