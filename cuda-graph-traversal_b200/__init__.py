@@ -77,6 +77,9 @@ def _load() -> C.CDLL:
         "g5_csr_split_tiny": ([p, p, p, p, p, u64, f32, p, p], C.c_int),
         "g5_csr_sorted_workspace_size": ([u64, u64, p], C.c_int),
         "g5_csr_fill_sorted": ([p, p, u64, u64, p, u64, p, u64, p, p, p, p], C.c_int),
+        "g5_csr_radix_workspace_size": ([u64, u64, p], C.c_int),
+        "g5_csr_radix_count": ([p, u64, u64, p, u64, p, p], C.c_int),
+        "g5_csr_radix_fill": ([p, p, u64, u64, u64, p, u64, p, p, p, p, p], C.c_int),
         "g5_csr_sort_rows": ([p, u64, u64, p, p, p, p, u64, p], C.c_int),
         "g5_csr_degree_order_workspace_size": ([u64, u64, p], C.c_int),
         "g5_csr_degree_order": ([p, p, u64, u64, p, p, u64, p], C.c_int),
@@ -437,36 +440,52 @@ def _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st,
 
 def oned_graph_from_tuple_graph(tg: TupleGraph, nglobalverts: int, light_delta: float = 0.1,
                                 with_column64: bool = False, stream=None, with_main: bool = True,
-                                dedupe: bool = False, bfs_order: bool = True, sssp_renumber: bool = True) -> OnedGraph:
+                                dedupe: bool = False, bfs_order: bool = True, sssp_renumber: bool = True,
+                                radix: bool = True) -> OnedGraph:
     """oned_graph_from_tuple_graph (src/traversal.h:43): the CSR of both
     directions of every non-loop edge, duplicates kept, every row in
-    canonical order (sorted by neighbour, then weight bits:
-    g5_csr_fill_sorted), plus the SSSP copy with light-first rows
-    (g.scol / g.sw, g5_csr_split_light).  dedupe=True keeps one entry per
-    (row, neighbour), the lightest (not the reference's CSR: its TEPS edge
-    counts include duplicates).  with_main=False skips the main-component
-    search (g.main_bits = None; set it later with main_component_bitmap).
+    canonical order (sorted by neighbour, then weight bits), plus the SSSP
+    copy with light-first rows (g.scol / g.sw, g5_csr_split_light).  The
+    rows come from one LSD radix sort of all entries (g5_csr_radix_count +
+    g5_csr_radix_fill); radix=False builds the same CSR by degree count,
+    source partitioning and row sorts (g5_csr_count + g5_csr_fill_sorted),
+    which needs half the scratch.  dedupe=True keeps one entry per (row,
+    neighbour), the lightest (not the reference's CSR: its TEPS edge counts
+    include duplicates).  with_main=False skips the main-component search
+    (g.main_bits = None; set it later with main_component_bitmap).
     bfs_order=False skips the BFS's degree-ordered copy of the column
     (g.bcol; oned_graph_bfs_order makes it later), sssp_renumber=False the
     SSSP's renumbered copy (g.sr; oned_graph_sssp_renumber)."""
     dev = tg.edges.device
     n, m = int(nglobalverts), tg.edges_size
-    nb = C.c_uint64()
-    _check(lib.g5_csr_workspace_size(n, m, C.byref(nb)))
-    cwork = _workspace(nb.value, dev)
+    st = _stream(stream)
     rowstarts = torch.empty(n + 1, dtype=torch.int64, device=dev)
     nent = C.c_uint64()
-    st = _stream(stream)
-    _check(lib.g5_csr_count(_ptr(tg.edges), m, n, _ptr(rowstarts), _ptr(cwork), cwork.numel(),
-                            C.byref(nent), st))
-    del cwork
+    if radix:
+        nb, ns = C.c_uint64(), C.c_uint64()
+        _check(lib.g5_csr_radix_workspace_size(n, m, C.byref(nb)))
+        _check((lib.g5_csr_degree_order_workspace_size if bfs_order else lib.g5_csr_sorted_workspace_size)(
+            n, 2 * m, C.byref(ns)))
+        work = _workspace(max(nb.value, ns.value), dev)
+        _check(lib.g5_csr_radix_count(_ptr(tg.edges), m, n, _ptr(work), work.numel(), C.byref(nent), st))
+    else:
+        nb = C.c_uint64()
+        _check(lib.g5_csr_workspace_size(n, m, C.byref(nb)))
+        cwork = _workspace(nb.value, dev)
+        _check(lib.g5_csr_count(_ptr(tg.edges), m, n, _ptr(rowstarts), _ptr(cwork), cwork.numel(),
+                                C.byref(nent), st))
+        del cwork
     e = nent.value
     col = torch.empty(max(e, 1), dtype=torch.int32, device=dev)
     w = torch.empty(max(e, 1), dtype=torch.float32, device=dev)
     col64 = torch.empty(max(e, 1), dtype=torch.int64, device=dev) if with_column64 else None
-    work = _sorted_work(n, e, dev, bfs_order)
-    _check(lib.g5_csr_fill_sorted(_ptr(tg.edges), _ptr(tg.weights), m, n, _ptr(rowstarts), e, _ptr(work),
-                                  work.numel(), _ptr(col), _ptr(w), _ptr(col64), st))
+    if radix:
+        _check(lib.g5_csr_radix_fill(_ptr(tg.edges), _ptr(tg.weights), m, n, e, _ptr(work), work.numel(),
+                                     _ptr(rowstarts), _ptr(col), _ptr(w), _ptr(col64), st))
+    else:
+        work = _sorted_work(n, e, dev, bfs_order)
+        _check(lib.g5_csr_fill_sorted(_ptr(tg.edges), _ptr(tg.weights), m, n, _ptr(rowstarts), e, _ptr(work),
+                                      work.numel(), _ptr(col), _ptr(w), _ptr(col64), st))
     return _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, dev, stream, with_main,
                          bfs_order, sssp_renumber)
 

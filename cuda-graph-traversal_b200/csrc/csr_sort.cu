@@ -106,7 +106,13 @@ static SortWork carve_sort(void *base, uint64_t n, uint64_t e) {
     return w;
 }
 
-enum : unsigned { SORTERR_RANGE = 1u, SORTERR_COUNT = 2u };
+enum : unsigned {
+    SORTERR_RANGE = 1u,     // an edge endpoint >= nverts
+    SORTERR_COUNT = 2u,     // the edges differ from the ones counted
+    SORTERR_WAIT = 4u,      // a radix look-back wait gave up
+    SORTERR_ORDER = 8u,     // radix output out of order (the edges changed after counting)
+    SORTERR_CAPACITY = 16u, // a radix list (gaps, long runs) would have overflowed
+};
 
 // ---------------------------------------------------------------- partition
 
@@ -812,6 +818,459 @@ __global__ void __launch_bounds__(SORT_THREADS) csr_split_write_kernel(
     }
 }
 
+
+// ------------------------------------------------------------ radix build
+//
+// The canonical CSR as one LSD radix sort of every directed entry by the key
+// (src << lg | dst), lg = bits of a vertex index, 8 bits a pass
+// (ceil(2 lg / 8) passes: 7 at SCALE 26).  Each pass is one "one-sweep"
+// kernel: a block takes the next tile of 4096 entries (tile numbers handed
+// out in launch order by an atomic counter, so every earlier tile is held by
+// a running block), ranks it by digit in shared memory (warp match plus
+// per-warp digit counters: stable), publishes the tile's digit counts, adds
+// up the preceding tiles' published counts for its global offsets
+// (decoupled look-back with a bounded wait) and writes each digit's run of
+// the tile with consecutive stores.  The first pass reads the edge list
+// (both directions of each non-loop edge); every pass's digit totals come
+// from one counting pass over the edges before it, which also gives the
+// entry count before the caller allocates the CSR.  A finish pass writes
+// col / w / row starts from the sorted keys and orders each run of equal
+// (src, dst) by weight bits: runs of up to 32 by one thread, longer ones
+// listed and sorted by the row-sort kernels.
+//
+// HBM bytes per entry: the counting pass reads 8 (16 per edge), the first
+// pass 10 and writes 12, each further pass reads and writes 12, the finish
+// reads 12 and writes 8 (16 with the u64 column).
+
+constexpr int RX_BITS = 8;
+constexpr int RX_BINS = 1 << RX_BITS;
+constexpr int RX_THREADS = 256;  // one thread per digit in the look-back
+constexpr int RX_WARPS = RX_THREADS / 32;
+#ifndef G5_RX_ITEMS
+#define G5_RX_ITEMS 16  // entries a thread takes per tile (even: the first pass takes both directions of ITEMS / 2 edges)
+#endif
+#ifndef G5_RX_MIN_BLOCKS
+#define G5_RX_MIN_BLOCKS 3  // 3 blocks of 256 threads an SM (a few spilled registers; 2 blocks: 18 % slower)
+#endif
+#ifndef G5_RX_LOOKBACK
+#define G5_RX_LOOKBACK 4  // predecessor tiles a look-back step reads at once (8 and 16: slower at SCALE 26)
+#endif
+constexpr int RX_ITEMS = G5_RX_ITEMS;
+constexpr int RX_LOOKBACK = G5_RX_LOOKBACK;
+constexpr int RX_TILE = RX_THREADS * RX_ITEMS;  // 4096 entries
+constexpr int RX_EDGE_TILE = RX_TILE / 2;       // first pass: 2048 edges, both directions
+static_assert(RX_ITEMS % 2 == 0 && RX_ITEMS <= 32, "items: even, at most the valid mask's 32 bits");
+constexpr int RX_MAXPASS = 8;                   // 2 lg <= 62 bits
+constexpr size_t RX_SMEM = (size_t)RX_TILE * (sizeof(unsigned long long) + sizeof(unsigned));
+constexpr unsigned RX_RUN_INLINE = 32;  // duplicate runs up to this long are sorted by one thread
+constexpr uint64_t RX_GAP_INLINE = 64;  // empty-row gaps up to this long are filled by one thread
+
+// Look-back status word of (tile, digit): pass epoch (8 bits), flag
+// (1 = the tile's own count, 2 = inclusive prefix over tiles 0..t), count.
+constexpr int RX_EPOCH_SHIFT = 56, RX_FLAG_SHIFT = 54;
+constexpr unsigned long long RX_COUNT_MASK = (1ull << RX_FLAG_SHIFT) - 1;
+constexpr unsigned long long RX_AGG = 1, RX_PREFIX = 2;
+
+enum : unsigned { RXC_ERR = 0, RXC_RUNS = 1, RXC_GAPS = 2, RXC_TILES = 8 };  // RadixWork::cnt slots
+
+struct RadixWork {
+    unsigned long long *hist;   // RX_MAXPASS x RX_BINS: digit totals per pass
+    unsigned long long *base;   // RX_MAXPASS x RX_BINS: their exclusive prefixes
+    unsigned long long *total;  // [0] entries counted, [1] edges counted over
+    unsigned *cnt;              // 64 counters (RXC_*)
+    unsigned *scnt;             // 64: the row sort's list counts ([0] mid runs, [1] big runs, [4..5] longest)
+    uint64_t *gaps;             // 3 x gcap: empty-row gaps (first row, end row, start value)
+    uint64_t gcap;
+    uint64_t *runs;             // 2 x rcap: long duplicate runs as [start, end) "rows" for the row sort
+    unsigned *rmid, *rbig;      // rcap each: run numbers 2k by length class
+    uint64_t rcap;
+    unsigned long long *status; // tmax x RX_BINS
+    uint64_t tmax;
+    unsigned long long *ka, *kb;  // entry keys, ping-pong (emax each)
+    unsigned *va, *vb;            // their weight bits
+    uint64_t region;              // bytes from ka to the end (the long-run sort's scratch)
+    uint64_t bytes;
+};
+
+static int vertex_bits(uint64_t n) {
+    int lg = 0;
+    while ((1ull << lg) < n) ++lg;
+    return lg;
+}
+
+static RadixWork carve_radix(void *base, uint64_t n, uint64_t m) {
+    Carver c(base);
+    RadixWork w;
+    const uint64_t emax = 2 * m;
+    w.hist = c.take<unsigned long long>(RX_MAXPASS * RX_BINS);
+    w.base = c.take<unsigned long long>(RX_MAXPASS * RX_BINS);
+    w.total = c.take<unsigned long long>(2);
+    w.cnt = c.take<unsigned>(64);
+    w.scnt = c.take<unsigned>(64);
+    w.gcap = (n + 1) / (RX_GAP_INLINE + 1) + 2;
+    w.gaps = c.take<uint64_t>(3 * w.gcap);
+    w.rcap = emax / (RX_RUN_INLINE + 1) + 1;
+    w.runs = c.take<uint64_t>(2 * w.rcap);
+    w.rmid = c.take<unsigned>(w.rcap);
+    w.rbig = c.take<unsigned>(w.rcap);
+    w.tmax = (m + RX_EDGE_TILE - 1) / RX_EDGE_TILE + 1;
+    w.status = c.take<unsigned long long>(w.tmax * RX_BINS);
+    const uint64_t before = align_up(c.used, 256);
+    w.ka = c.take<unsigned long long>(emax ? emax : 1);
+    w.kb = c.take<unsigned long long>(emax ? emax : 1);
+    w.va = c.take<unsigned>(emax ? emax : 1);
+    w.vb = c.take<unsigned>(emax ? emax : 1);
+    w.region = c.used - before;
+    w.bytes = c.used;
+    return w;
+}
+
+// Digit totals of every pass over both directions of every non-loop edge.
+__global__ void __launch_bounds__(256) csr_radix_hist_kernel(const ulonglong2 *__restrict__ edges, uint64_t m,
+                                                             uint64_t n, int lg, int passes,
+                                                             unsigned long long *__restrict__ hist,
+                                                             unsigned *__restrict__ err) {
+    __shared__ unsigned s_h[RX_MAXPASS * RX_BINS];
+    for (int i = threadIdx.x; i < passes * RX_BINS; i += blockDim.x) s_h[i] = 0;
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        const ulonglong2 e = __ldcs(&edges[i]);
+        if (e.x >= n || e.y >= n) {
+            atomicOr(err, SORTERR_RANGE);
+            continue;
+        }
+        if (e.x == e.y) continue;
+        const unsigned long long k1 = (e.x << lg) | e.y, k2 = (e.y << lg) | e.x;
+        for (int p = 0; p < passes; ++p) {
+            atomicAdd(&s_h[p * RX_BINS + ((k1 >> (RX_BITS * p)) & (RX_BINS - 1))], 1u);
+            atomicAdd(&s_h[p * RX_BINS + ((k2 >> (RX_BITS * p)) & (RX_BINS - 1))], 1u);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * RX_BINS; i += blockDim.x)
+        if (s_h[i]) atomicAdd(&hist[i], (unsigned long long)s_h[i]);
+}
+
+// base[p][d] = exclusive prefix of hist[p][*]; total[0] = entries.  One block
+// of RX_BINS threads.
+__global__ void csr_radix_scan_kernel(const unsigned long long *__restrict__ hist, int passes,
+                                      unsigned long long *__restrict__ base, unsigned long long *__restrict__ total) {
+    __shared__ unsigned long long s_ws[RX_WARPS];
+    const unsigned d = threadIdx.x, lane = lane_id(), wid = d >> 5;
+    for (int p = 0; p < passes; ++p) {
+        const unsigned long long x = hist[p * RX_BINS + d];
+        const unsigned long long incl = warp_incl_scan(x);
+        if (lane == 31) s_ws[wid] = incl;
+        __syncthreads();
+        unsigned long long wb = 0, all = 0;
+        for (int q = 0; q < RX_WARPS; ++q) {
+            if (q < (int)wid) wb += s_ws[q];
+            all += s_ws[q];
+        }
+        base[p * RX_BINS + d] = wb + incl - x;
+        if (p == 0 && d == 0) total[0] = all;
+        __syncthreads();
+    }
+}
+
+struct RxPass {
+    const ulonglong2 *edges;  // first pass: the edge list and its weights
+    const float *weights;
+    uint64_t m;
+    const unsigned long long *kin;  // later passes: the previous pass's output
+    const unsigned *vin;
+    unsigned long long *kout;
+    unsigned *vout;
+    uint64_t n, E, ntiles;
+    int lg, shift;
+    unsigned long long epoch;
+    const unsigned long long *base, *hist;  // this pass's digit starts and totals
+    unsigned long long *status;
+    unsigned *tilectr, *err;
+    unsigned long long limit_ns;
+};
+
+__device__ __forceinline__ void st_status(unsigned long long *p, unsigned long long x) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(x) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+template <bool FIRST>
+__global__ void __launch_bounds__(RX_THREADS, G5_RX_MIN_BLOCKS) csr_radix_pass_kernel(RxPass a) {
+    extern __shared__ unsigned long long s_key[];  // RX_TILE keys, then their values
+    unsigned *s_val = reinterpret_cast<unsigned *>(s_key + RX_TILE);
+    __shared__ unsigned s_wcnt[RX_WARPS][RX_BINS];
+    __shared__ unsigned s_wsum[RX_WARPS];
+    __shared__ unsigned long long s_gdelta[RX_BINS];
+    __shared__ unsigned s_tile, s_total;
+    const unsigned tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(a.tilectr, 1u);
+    for (int i = tid; i < RX_WARPS * RX_BINS; i += RX_THREADS) (&s_wcnt[0][0])[i] = 0;
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    if (tile >= a.ntiles) return;  // block-uniform (the grid has ntiles blocks)
+
+    // The tile's items, warp-striped (item k of lane l of warp w is entry
+    // w * 512 + k * 32 + l of the tile): coalesced loads, and that order is
+    // the ranking's, which keeps the pass stable.
+    unsigned long long key[RX_ITEMS];
+    unsigned val[RX_ITEMS];
+    unsigned valid = 0;
+    if (FIRST) {
+        const uint64_t e0 = tile * RX_EDGE_TILE + wid * (RX_EDGE_TILE / RX_WARPS) + lane;
+#pragma unroll
+        for (int k = 0; k < RX_ITEMS / 2; ++k) {
+            const uint64_t i = e0 + (uint64_t)k * 32;
+            unsigned long long u = 0, v = 0;
+            unsigned wb = 0;
+            if (i < a.m) {
+                const ulonglong2 e = __ldcs(&a.edges[i]);
+                u = e.x;
+                v = e.y;
+                if (u >= a.n || v >= a.n) {
+                    atomicOr(a.err, SORTERR_RANGE);
+                } else if (u != v) {
+                    valid |= 1u << k | 1u << (k + RX_ITEMS / 2);
+                    wb = __float_as_uint(__ldcs(&a.weights[i]));
+                }
+            }
+            key[k] = (u << a.lg) | v;
+            key[k + RX_ITEMS / 2] = (v << a.lg) | u;
+            val[k] = val[k + RX_ITEMS / 2] = wb;
+        }
+    } else {
+        const uint64_t p0 = tile * RX_TILE + wid * (RX_TILE / RX_WARPS) + lane;
+#pragma unroll
+        for (int k = 0; k < RX_ITEMS; ++k) {
+            const uint64_t i = p0 + (uint64_t)k * 32;
+            key[k] = 0;
+            val[k] = 0;
+            if (i < a.E) {
+                key[k] = __ldcs(&a.kin[i]);
+                val[k] = __ldcs(&a.vin[i]);
+                valid |= 1u << k;
+            }
+        }
+    }
+
+    // Rank: per warp, items in order k = 0, 1, ...; lanes of one digit
+    // (match) take consecutive slots after the warp's earlier items of it.
+    unsigned rank[RX_ITEMS / 2];  // two 16-bit ranks a register (a rank is below 32 * RX_ITEMS)
+    unsigned *wc = s_wcnt[wid];
+#pragma unroll
+    for (int k = 0; k < RX_ITEMS; ++k) {
+        const bool ok = (valid >> k) & 1u;
+        const unsigned d = ok ? (unsigned)(key[k] >> a.shift) & (RX_BINS - 1) : RX_BINS;
+        const unsigned peers = __match_any_sync(FULL, d);
+        const unsigned leader = __ffs(peers) - 1;
+        unsigned c = 0;
+        if (ok && lane == leader) {
+            c = wc[d];
+            wc[d] = c + __popc(peers);
+        }
+        c = __shfl_sync(FULL, c, leader);
+        const unsigned r = c + __popc(peers & lanemask_lt());
+        rank[k / 2] = (k & 1) ? rank[k / 2] | r << 16 : r;
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // Thread d: digit d's warp offsets, tile count, tile offset, look-back.
+    const unsigned d = tid;
+    unsigned tot = 0;
+#pragma unroll
+    for (int q = 0; q < RX_WARPS; ++q) {
+        const unsigned c = s_wcnt[q][d];
+        s_wcnt[q][d] = tot;
+        tot += c;
+    }
+    unsigned long long *my = a.status + tile * RX_BINS + d;
+    const unsigned long long ep = a.epoch << RX_EPOCH_SHIFT;
+    st_status(my, ep | ((tile == 0 ? RX_PREFIX : RX_AGG) << RX_FLAG_SHIFT) | tot);
+    const unsigned incl = warp_incl_scan(tot);
+    if (lane == 31) s_wsum[wid] = incl;
+    __syncthreads();
+    unsigned wb = 0, all = 0;
+#pragma unroll
+    for (int q = 0; q < RX_WARPS; ++q) {
+        const unsigned x = s_wsum[q];
+        if (q < (int)wid) wb += x;
+        all += x;
+    }
+    // Tile offsets folded into the warp offsets: s_wcnt[w][d] = where warp
+    // w's digit-d items start in the tile.
+    const unsigned toff = wb + incl - tot;
+#pragma unroll
+    for (int q = 0; q < RX_WARPS; ++q) s_wcnt[q][d] += toff;
+    if (tid == 0) s_total = all;
+    __syncthreads();
+
+    // Into shared memory in tile order by digit (the items' registers are
+    // free from here on).
+#pragma unroll
+    for (int k = 0; k < RX_ITEMS; ++k) {
+        if ((valid >> k) & 1u) {
+            const unsigned dk = (unsigned)(key[k] >> a.shift) & (RX_BINS - 1);
+            const unsigned pos = s_wcnt[wid][dk] + ((rank[k / 2] >> (16 * (k & 1))) & 0xffffu);
+            s_key[pos] = key[k];
+            s_val[pos] = val[k];
+        }
+    }
+
+    // Look-back for digit d, after the scatter (read later, the status
+    // words are further along): RX_LOOKBACK predecessors' words in flight at
+    // once, taken in order from the nearest; a predecessor that has not
+    // published yet is waited for (bounded), a prefix ends the walk.
+    unsigned long long excl = 0;
+    if (tile > 0) {
+        int64_t j = (int64_t)tile - 1;
+        const unsigned long long t0 = globaltimer_ns();
+        unsigned spins = 0;
+        bool done = false;
+        while (!done) {
+            unsigned long long sw[RX_LOOKBACK];
+#pragma unroll
+            for (int q = 0; q < RX_LOOKBACK; ++q)
+                sw[q] = j - q >= 0 ? ld_relaxed64(a.status + (uint64_t)(j - q) * RX_BINS + d) : 0ull;
+#pragma unroll
+            for (int q = 0; q < RX_LOOKBACK; ++q) {
+                if (done) break;
+                if (j - q < 0) {  // tile 0 publishes a prefix: a walk past it means a broken status
+                    atomicOr(a.err, SORTERR_WAIT);
+                    done = true;
+                    break;
+                }
+                unsigned long long x = sw[q];
+                while ((x >> RX_EPOCH_SHIFT) != a.epoch || ((x >> RX_FLAG_SHIFT) & 3ull) == 0) {
+                    if (++spins > 64) {
+                        if (ld_volatile(a.err) & SORTERR_WAIT) break;  // another tile gave up: so do the rest
+                        if (globaltimer_ns() - t0 > a.limit_ns) {
+                            atomicOr(a.err, SORTERR_WAIT);
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                    x = ld_relaxed64(a.status + (uint64_t)(j - q) * RX_BINS + d);
+                }
+                if ((x >> RX_EPOCH_SHIFT) != a.epoch || ((x >> RX_FLAG_SHIFT) & 3ull) == 0) {  // gave up
+                    done = true;
+                    break;
+                }
+                excl += x & RX_COUNT_MASK;
+                if (((x >> RX_FLAG_SHIFT) & 3ull) == RX_PREFIX) done = true;
+            }
+            j -= RX_LOOKBACK;
+        }
+        st_status(my, ep | (RX_PREFIX << RX_FLAG_SHIFT) | ((excl + tot) & RX_COUNT_MASK));
+    }
+    // Entry i of the tile (digit d) goes to s_gdelta[d] + i (mod 2^64).
+    s_gdelta[d] = a.base[d] + excl - toff;
+    if (tile + 1 == a.ntiles && excl + tot != a.hist[d]) atomicOr(a.err, SORTERR_COUNT);
+    __syncthreads();
+
+    // Out, run by run.
+    const unsigned total = s_total;
+    for (unsigned i = tid; i < total; i += RX_THREADS) {
+        const unsigned long long k = s_key[i];
+        const unsigned dk = (unsigned)(k >> a.shift) & (RX_BINS - 1);
+        const unsigned long long pos = s_gdelta[dk] + i;
+        if (pos < a.E) {
+            a.kout[pos] = k;
+            a.vout[pos] = s_val[i];
+        } else {
+            atomicOr(a.err, SORTERR_COUNT);
+        }
+    }
+}
+
+// rowstarts[r] = x for rows [r0, r1): short gaps here, long ones listed.
+__device__ __forceinline__ void rx_gap(uint64_t *rowstarts, uint64_t r0, uint64_t r1, uint64_t x, uint64_t *gaps,
+                                       uint64_t gcap, unsigned *cnt, unsigned *err) {
+    if (r1 - r0 <= RX_GAP_INLINE) {
+        for (uint64_t r = r0; r < r1; ++r) rowstarts[r] = x;
+        return;
+    }
+    const unsigned g = atomicAdd(&cnt[RXC_GAPS], 1u);
+    if (g >= gcap) {
+        atomicOr(err, SORTERR_CAPACITY);
+        return;
+    }
+    gaps[3 * g] = r0;
+    gaps[3 * g + 1] = r1;
+    gaps[3 * g + 2] = x;
+}
+
+// Sorted keys -> col / w / row starts; runs of equal (src, dst) by weight.
+__global__ void csr_radix_finish_kernel(const unsigned long long *__restrict__ K, const unsigned *__restrict__ V,
+                                        uint64_t E, uint64_t n, int lg, uint64_t *__restrict__ rowstarts,
+                                        int *__restrict__ col, float *__restrict__ w, uint64_t *__restrict__ col64,
+                                        RadixWork rw) {
+    const unsigned long long dmask = (1ull << lg) - 1;
+    unsigned *err = &rw.cnt[RXC_ERR];
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += stride) {
+        const unsigned long long k = K[i];
+        const unsigned long long kp = i ? K[i - 1] : ~0ull, kn = i + 1 < E ? K[i + 1] : ~0ull;
+        const uint64_t src = k >> lg, dst = k & dmask;
+        if ((i && kp > k) || src >= n) {
+            atomicOr(err, SORTERR_ORDER);
+            continue;
+        }
+        col[i] = (int)dst;
+        if (col64) col64[i] = dst;
+        if (i == 0) rx_gap(rowstarts, 0, src + 1, 0, rw.gaps, rw.gcap, rw.cnt, err);
+        else if ((kp >> lg) != src) rx_gap(rowstarts, (kp >> lg) + 1, src + 1, i, rw.gaps, rw.gcap, rw.cnt, err);
+        if (i + 1 == E) rx_gap(rowstarts, src + 1, n + 1, E, rw.gaps, rw.gcap, rw.cnt, err);
+        if (kp != k && kn != k) {
+            w[i] = __uint_as_float(V[i]);
+        } else if (kp != k) {  // the first of a run of equal keys: the run's weights, sorted
+            uint64_t j = i + 1;
+            while (j < E && K[j] == k) ++j;
+            const uint64_t L = j - i;
+            if (L <= RX_RUN_INLINE) {
+                unsigned x[RX_RUN_INLINE];
+                for (unsigned q = 0; q < (unsigned)L; ++q) {
+                    const unsigned y = V[i + q];
+                    unsigned b = q;
+                    while (b > 0 && x[b - 1] > y) {
+                        x[b] = x[b - 1];
+                        --b;
+                    }
+                    x[b] = y;
+                }
+                for (unsigned q = 0; q < (unsigned)L; ++q) w[i + q] = __uint_as_float(x[q]);
+            } else {
+                for (uint64_t q = i; q < j; ++q) w[q] = __uint_as_float(V[q]);
+                const unsigned r = atomicAdd(&rw.cnt[RXC_RUNS], 1u);
+                if (r >= rw.rcap) {
+                    atomicOr(err, SORTERR_CAPACITY);
+                } else {
+                    rw.runs[2 * r] = i;
+                    rw.runs[2 * r + 1] = j;
+                    if (L <= SORT_SMEM_KEYS) rw.rmid[atomicAdd(&rw.scnt[0], 1u)] = 2 * r;
+                    else rw.rbig[atomicAdd(&rw.scnt[1], 1u)] = 2 * r;
+                }
+            }
+        }
+    }
+}
+
+// The listed long gaps of empty rows, a block each.
+__global__ void csr_radix_gaps_kernel(const uint64_t *__restrict__ gaps, const unsigned *__restrict__ cnt,
+                                      uint64_t gcap, uint64_t *__restrict__ rowstarts) {
+    const uint64_t ng = min((uint64_t)cnt[RXC_GAPS], gcap);
+    for (uint64_t g = blockIdx.x; g < ng; g += gridDim.x) {
+        const uint64_t r0 = gaps[3 * g], r1 = gaps[3 * g + 1], x = gaps[3 * g + 2];
+        for (uint64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) rowstarts[r] = x;
+    }
+}
+
 static int sort_grid(int per_sm) {
     DeviceInfo di;
     if (device_info(&di)) return 148 * per_sm;
@@ -854,20 +1313,14 @@ static int big_rows_prepare(const uint64_t *d_rowstarts, const SortWork &w, int 
     return G5_OK;
 }
 
-// Sorts rows in place (any CSR: the rows of g5_csr_fill or of the fused
-// Kronecker fill come out canonical too).
-static int sort_rows(const uint64_t *d_rowstarts, uint64_t nverts, int32_t *d_col, float *d_w, uint64_t *d_col64,
-                     const SortWork &w, cudaStream_t st) {
-    G5_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, 2 * sizeof(unsigned), st));
-    const uint64_t warps = (nverts + 31) / 32;
-    const int wblocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sort_grid(8), (warps + 7) / 8));
-    csr_sort_warp_kernel<<<wblocks, 256, 0, st>>>(d_rowstarts, nverts, d_col, d_w, d_col64, w.mid, w.big, w.cnt);
-    csr_sort_mid_kernel<<<sort_grid(4), SORT_THREADS, 0, st>>>(d_rowstarts, w.mid, w.cnt, d_col, d_w, d_col64);
-    G5_CUDA_TRY(cudaGetLastError());
+// The listed big rows (w.big, count w.cnt[cidx]) sorted in place: every
+// BIG_TILE chunk in shared memory, then merge passes over the whole grid.
+static int sort_big_rows(const uint64_t *d_rowstarts, int32_t *d_col, float *d_w, uint64_t *d_col64,
+                         const SortWork &w, int cidx, cudaStream_t st) {
     unsigned nbig = 0;
     uint64_t ntiles = 0;
     unsigned long long maxlen = 0;
-    int rc = big_rows_prepare(d_rowstarts, w, 1, st, &nbig, &ntiles, &maxlen);
+    int rc = big_rows_prepare(d_rowstarts, w, cidx, st, &nbig, &ntiles, &maxlen);
     if (rc || !nbig) return rc;
     const int grid = (int)std::min<uint64_t>(ntiles, (uint64_t)sort_grid(4));
     csr_sort_chunks_kernel<<<grid, SORT_THREADS, 0, st>>>(d_rowstarts, w.big, nbig, w.tp, ntiles, w.tkey, d_col, d_w);
@@ -881,6 +1334,19 @@ static int sort_rows(const uint64_t *d_rowstarts, uint64_t nverts, int32_t *d_co
     csr_big_finish_kernel<<<grid, 256, 0, st>>>(d_rowstarts, w.big, nbig, w.tp, ntiles, w.tkey, d_col, d_w, d_col64);
     G5_CUDA_TRY(cudaGetLastError());
     return G5_OK;
+}
+
+// Sorts rows in place (any CSR: the rows of g5_csr_fill or of the fused
+// Kronecker fill come out canonical too).
+static int sort_rows(const uint64_t *d_rowstarts, uint64_t nverts, int32_t *d_col, float *d_w, uint64_t *d_col64,
+                     const SortWork &w, cudaStream_t st) {
+    G5_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, 2 * sizeof(unsigned), st));
+    const uint64_t warps = (nverts + 31) / 32;
+    const int wblocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sort_grid(8), (warps + 7) / 8));
+    csr_sort_warp_kernel<<<wblocks, 256, 0, st>>>(d_rowstarts, nverts, d_col, d_w, d_col64, w.mid, w.big, w.cnt);
+    csr_sort_mid_kernel<<<sort_grid(4), SORT_THREADS, 0, st>>>(d_rowstarts, w.mid, w.cnt, d_col, d_w, d_col64);
+    G5_CUDA_TRY(cudaGetLastError());
+    return sort_big_rows(d_rowstarts, d_col, d_w, d_col64, w, 1, st);
 }
 
 extern "C" int g5_csr_fill_sorted(const uint64_t *d_edges, const float *d_weights, uint64_t nedges, uint64_t nverts,
@@ -927,6 +1393,152 @@ extern "C" int g5_csr_fill_sorted(const uint64_t *d_edges, const float *d_weight
     G5_CUDA_TRY(cudaStreamSynchronize(st));
     if (err & SORTERR_RANGE) return set_error(G5_ERR_INVALID, "g5_csr_fill_sorted: an edge endpoint is >= nverts");
     if (err) return set_error(G5_ERR_INVALID, "g5_csr_fill_sorted: the edges differ from those the rows were counted on");
+    return G5_OK;
+}
+
+// ------------------------------------------------------------ radix build
+
+static int radix_passes(uint64_t n) { return (2 * vertex_bits(n) + RX_BITS - 1) / RX_BITS; }
+
+extern "C" int g5_csr_radix_workspace_size(uint64_t nverts, uint64_t nedges, uint64_t *bytes) {
+    G5_CHECK_ARG(bytes, "g5_csr_radix_workspace_size: bytes is NULL");
+    *bytes = carve_radix(nullptr, nverts, nedges).bytes;
+    return G5_OK;
+}
+
+extern "C" int g5_csr_radix_count(const uint64_t *d_edges, uint64_t nedges, uint64_t nverts, void *d_work,
+                                  uint64_t work_bytes, uint64_t *nentries, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_csr_radix_count: nverts outside [1, 2^31]");
+    G5_CHECK_ARG(d_work && nentries && (nedges == 0 || d_edges), "g5_csr_radix_count: NULL argument");
+    RadixWork w = carve_radix(d_work, nverts, nedges);
+    if (work_bytes < w.bytes)
+        return set_error(G5_ERR_WORKSPACE, "g5_csr_radix_count: workspace %llu < %llu bytes",
+                         (unsigned long long)work_bytes, (unsigned long long)w.bytes);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int lg = vertex_bits(nverts), passes = radix_passes(nverts);
+    G5_CUDA_TRY(cudaMemsetAsync(w.hist, 0, 2 * RX_MAXPASS * RX_BINS * sizeof(unsigned long long), st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.total, 0, 2 * sizeof(unsigned long long), st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, 64 * sizeof(unsigned), st));
+    if (nedges) {  // (with one vertex there are no passes, but the endpoints are still checked)
+        const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((nedges + 255) / 256, (uint64_t)sort_grid(8)));
+        csr_radix_hist_kernel<<<grid, 256, 0, st>>>((const ulonglong2 *)d_edges, nedges, nverts, lg, passes, w.hist,
+                                                    &w.cnt[RXC_ERR]);
+        if (passes) csr_radix_scan_kernel<<<1, RX_BINS, 0, st>>>(w.hist, passes, w.base, w.total);
+        G5_CUDA_TRY(cudaGetLastError());
+    }
+    const unsigned long long m = nedges;
+    G5_CUDA_TRY(cudaMemcpyAsync(&w.total[1], &m, sizeof m, cudaMemcpyHostToDevice, st));
+    unsigned long long total = 0;
+    unsigned err = 0;
+    G5_CUDA_TRY(cudaMemcpyAsync(&total, w.total, sizeof total, cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaMemcpyAsync(&err, &w.cnt[RXC_ERR], sizeof err, cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    if (err & SORTERR_RANGE) return set_error(G5_ERR_INVALID, "g5_csr_radix_count: an edge endpoint is >= nverts");
+    *nentries = total;
+    return G5_OK;
+}
+
+extern "C" int g5_csr_radix_fill(const uint64_t *d_edges, const float *d_weights, uint64_t nedges, uint64_t nverts,
+                                 uint64_t nentries, void *d_work, uint64_t work_bytes, uint64_t *d_rowstarts,
+                                 int32_t *d_col, float *d_w, uint64_t *d_col64, void *stream) {
+    clear_error();
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_csr_radix_fill: nverts outside [1, 2^31]");
+    G5_CHECK_ARG(d_work && d_rowstarts && (nentries == 0 || (d_col && d_w)), "g5_csr_radix_fill: NULL argument");
+    G5_CHECK_ARG(nedges == 0 || (d_edges && d_weights), "g5_csr_radix_fill: edges or weights NULL");
+    G5_CHECK_ARG(nentries <= 2 * nedges, "g5_csr_radix_fill: nentries > 2 * nedges");
+    RadixWork w = carve_radix(d_work, nverts, nedges);
+    if (work_bytes < w.bytes)
+        return set_error(G5_ERR_WORKSPACE, "g5_csr_radix_fill: workspace %llu < %llu bytes",
+                         (unsigned long long)work_bytes, (unsigned long long)w.bytes);
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned long long counted[2] = {0, 0};
+    G5_CUDA_TRY(cudaMemcpyAsync(counted, w.total, sizeof counted, cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    if (counted[0] != nentries || counted[1] != nedges)
+        return set_error(G5_ERR_INVALID, "g5_csr_radix_fill: run g5_csr_radix_count on the same edges first "
+                         "(counted %llu entries of %llu edges, given %llu of %llu)", counted[0], counted[1],
+                         (unsigned long long)nentries, (unsigned long long)nedges);
+    const int lg = vertex_bits(nverts), passes = radix_passes(nverts);
+    const uint64_t E = nentries;
+    G5_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, 64 * sizeof(unsigned), st));
+    G5_CUDA_TRY(cudaMemsetAsync(w.scnt, 0, 64 * sizeof(unsigned), st));
+    if (E == 0) {
+        G5_CUDA_TRY(cudaMemsetAsync(d_rowstarts, 0, (nverts + 1) * sizeof(uint64_t), st));
+        G5_CUDA_TRY(cudaStreamSynchronize(st));
+        return G5_OK;
+    }
+    static bool smem_set[64][2] = {};  // the function attributes, once per device
+    int dev = 0;
+    G5_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || !smem_set[dev][0]) {
+        G5_CUDA_TRY(cudaFuncSetAttribute(csr_radix_pass_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)RX_SMEM));
+        G5_CUDA_TRY(cudaFuncSetAttribute(csr_radix_pass_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)RX_SMEM));
+        if (dev >= 0 && dev < 64) smem_set[dev][0] = true;
+    }
+    const uint64_t t_first = (nedges + RX_EDGE_TILE - 1) / RX_EDGE_TILE, t_rest = (E + RX_TILE - 1) / RX_TILE;
+    G5_CUDA_TRY(cudaMemsetAsync(w.status, 0, t_first * RX_BINS * sizeof(unsigned long long), st));
+    RxPass a{};
+    a.edges = (const ulonglong2 *)d_edges;
+    a.weights = d_weights;
+    a.m = nedges;
+    a.n = nverts;
+    a.E = E;
+    a.lg = lg;
+    a.status = w.status;
+    a.err = &w.cnt[RXC_ERR];
+    a.limit_ns = wait_limit_ns();
+    unsigned long long *kin = nullptr, *kout = w.ka;
+    unsigned *vin = nullptr, *vout = w.va;
+    for (int p = 0; p < passes; ++p) {
+        a.kin = kin;
+        a.vin = vin;
+        a.kout = kout;
+        a.vout = vout;
+        a.shift = RX_BITS * p;
+        a.epoch = (unsigned long long)(p + 1);
+        a.base = w.base + p * RX_BINS;
+        a.hist = w.hist + p * RX_BINS;
+        a.tilectr = &w.cnt[RXC_TILES + p];
+        a.ntiles = p == 0 ? t_first : t_rest;
+        if (a.ntiles > 0x7fffffffull) return set_error(G5_ERR_INVALID, "g5_csr_radix_fill: too many tiles");
+        if (p == 0) csr_radix_pass_kernel<true><<<(unsigned)a.ntiles, RX_THREADS, RX_SMEM, st>>>(a);
+        else csr_radix_pass_kernel<false><<<(unsigned)a.ntiles, RX_THREADS, RX_SMEM, st>>>(a);
+        G5_CUDA_TRY(cudaGetLastError());
+        kin = kout;
+        vin = vout;
+        kout = kout == w.ka ? w.kb : w.ka;
+        vout = vout == w.va ? w.vb : w.va;
+    }
+    const int fgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((E + 255) / 256, (uint64_t)sort_grid(8)));
+    csr_radix_finish_kernel<<<fgrid, 256, 0, st>>>(kin, vin, E, nverts, lg, d_rowstarts, d_col, d_w, d_col64, w);
+    csr_radix_gaps_kernel<<<sort_grid(2), 256, 0, st>>>(w.gaps, w.cnt, w.gcap, d_rowstarts);
+    G5_CUDA_TRY(cudaGetLastError());
+    unsigned c[3] = {0, 0, 0};
+    G5_CUDA_TRY(cudaMemcpyAsync(c, w.cnt, sizeof c, cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    const unsigned err = c[RXC_ERR];
+    if (err & SORTERR_RANGE) return set_error(G5_ERR_INVALID, "g5_csr_radix_fill: an edge endpoint is >= nverts");
+    if (err & SORTERR_WAIT) return set_error(G5_ERR_TIMEOUT, "g5_csr_radix_fill: a look-back wait gave up");
+    if (err & SORTERR_CAPACITY) return set_error(G5_ERR_DEVICE, "g5_csr_radix_fill: internal list overflow");
+    if (err) return set_error(G5_ERR_INVALID, "g5_csr_radix_fill: the edges differ from the ones counted");
+    if (c[RXC_RUNS]) {
+        // Long runs of one (row, neighbour): sorted as "rows" [start, end)
+        // by the row-sort kernels, with the key buffers as their scratch.
+        const uint64_t nruns = std::min<uint64_t>(c[RXC_RUNS], w.rcap);
+        SortWork sw = carve_sort(w.ka, 2 * nruns + 1, E);
+        if (sw.bytes > w.region) return set_error(G5_ERR_DEVICE, "g5_csr_radix_fill: run-sort scratch too small");
+        sw.mid = w.rmid;
+        sw.big = w.rbig;
+        sw.cnt = w.scnt;
+        csr_sort_mid_kernel<<<sort_grid(4), SORT_THREADS, 0, st>>>(w.runs, w.rmid, w.scnt, d_col, d_w, d_col64);
+        G5_CUDA_TRY(cudaGetLastError());
+        int rc = sort_big_rows(w.runs, d_col, d_w, d_col64, sw, 1, st);
+        if (rc) return rc;
+        G5_CUDA_TRY(cudaStreamSynchronize(st));
+    }
     return G5_OK;
 }
 

@@ -26,6 +26,7 @@ constexpr int VAL_THREADS = 256;
 constexpr int VAL_WTILE = 512;  // entries per warp tile (the tile table's unit)
 constexpr int COUNT_ITEMS = 16; // consecutive entries a lane takes per step: edge count
 constexpr int RULE_ITEMS = 8;   //   the validators (their neighbour records held in registers)
+constexpr int VAL_WIN = 128;    // rows a warp tile's shared window holds
 
 // Largest v in [lo, hi] with rowptr[v] <= e.
 __device__ __forceinline__ uint64_t row_of(const uint64_t *__restrict__ rowptr, uint64_t lo, uint64_t hi, uint64_t e) {
@@ -59,16 +60,17 @@ __global__ void val_tile_rows_kernel(const uint64_t *__restrict__ rowptr, uint64
 // own.  With the table, the rows a warp tile spans are known (the row of
 // the next tile's first entry bounds them; rows after a lane's entries
 // start beyond them and are never stepped into).  When they are fewer
-// than 32, lane j holds the start of the tile's j-th row (one coalesced
-// load) and each lane finds the row of its first entry by a 5-step binary
-// search over the lanes (shuffles); otherwise it searches rowptr.  From
-// there a lane steps forward with one compare per entry.  All 32 lanes
-// call it.
+// than VAL_WIN - 1, the warp's shared window holds the starts of the
+// tile's rows (coalesced loads of just those rows) and each lane finds the
+// row of its first entry by a binary search of the window; otherwise it
+// searches rowptr.  From there a lane keeps the next row's start in a
+// register: an entry costs one compare unless a row ends there.  All 32
+// lanes call it.
 template <int ITEMS, class Visit>
 __device__ __forceinline__ void warp_walk(const uint64_t *__restrict__ rowptr, const int *__restrict__ col, uint64_t n,
                                           uint64_t E, const unsigned *__restrict__ trow, bool table, Visit visit) {
     static_assert(ITEMS % 4 == 0 && VAL_WTILE % (32 * ITEMS) == 0, "whole int4 loads, whole steps");
-    __shared__ int s_win[VAL_THREADS / 32][32];
+    __shared__ int s_win[VAL_THREADS / 32][VAL_WIN];
     int *wrp = s_win[threadIdx.x >> 5];
     const unsigned lane = lane_id();
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -78,19 +80,24 @@ __device__ __forceinline__ void warp_walk(const uint64_t *__restrict__ rowptr, c
             lo = __ldg(&trow[t]);
             hi = __ldg(&trow[t + 1]);
         }
-        // The window: starts of rows lo .. lo + 31 (those past n are never
-        // reached), as 32-bit offsets from the tile's first entry (starts
-        // before it clamp to -1, far ones to 2^30), so the lookups below
-        // compare 32-bit numbers.
+        // The window: starts of rows lo .. lo + hi - lo + 1 (the last one
+        // starts after the tile's last entry), as 32-bit offsets from the
+        // tile's first entry (starts before it clamp to -1, far ones and the
+        // unused slots to 2^30), so the lookups below compare 32-bit
+        // numbers.
         const uint64_t t0 = t * VAL_WTILE;
-        const bool win = table && hi - lo < 31;
-        int rp = 1 << 30;
-        if (win && lo + lane <= n) {
-            const uint64_t x = __ldg(&rowptr[lo + lane]);
-            rp = x < t0 ? -1 : x - t0 > (1u << 30) ? 1 << 30 : (int)(x - t0);
-        }
+        const bool win = table && hi - lo < VAL_WIN - 1;
         __syncwarp();  // the last tile's window is read
-        wrp[lane] = rp;
+        if (win) {
+            for (unsigned i = lane; i < VAL_WIN; i += 32) {
+                int rp = 1 << 30;
+                if (i <= hi - lo + 1 && lo + i <= n) {
+                    const uint64_t x = __ldg(&rowptr[lo + i]);
+                    rp = x < t0 ? -1 : x - t0 > (1u << 30) ? 1 << 30 : (int)(x - t0);
+                }
+                wrp[i] = rp;
+            }
+        }
         __syncwarp();
 #pragma unroll 1
         for (int step = 0; step < VAL_WTILE / (32 * ITEMS); ++step) {
@@ -117,17 +124,22 @@ __device__ __forceinline__ void warp_walk(const uint64_t *__restrict__ rowptr, c
                 const int el = (int)(eb - t0);  // < VAL_WTILE
                 unsigned j = 0;  // largest window row starting at or before eb
 #pragma unroll
-                for (unsigned s = 16; s >= 1; s >>= 1)
-                    if (wrp[j + s] <= el) j += s;  // j + s <= 31
+                for (unsigned s = VAL_WIN / 2; s >= 1; s >>= 1)
+                    if (wrp[j + s] <= el) j += s;  // j + s <= VAL_WIN - 1
+                // d: this lane's entries before row j + 1 starts.  The row of
+                // a real entry is at most hi - lo <= VAL_WIN - 2, and window
+                // row hi - lo + 1 starts after the tile's last entry, so the
+                // stepping stops by itself (the guard only bounds the index).
+                int d = (j + 1 < VAL_WIN ? wrp[j + 1] : 1 << 30) - el;
                 const unsigned ul = (unsigned)lo;
 #pragma unroll
                 for (int k = 0; k < ITEMS; ++k) {
-                    // Later rows start at or before this entry: step (past
-                    // empty rows too).  The row of a real entry is at most
-                    // hi - lo <= 30, and window row hi - lo + 1 starts after
-                    // the tile's last entry, so the loop stops by itself.
-                    if (k < (int)ne)
-                        while (j < 31 && wrp[j + 1] <= el + k) ++j;
+                    if (k < (int)ne) {
+                        while (k >= d) {  // a later row starts at or before this entry (past empty rows too)
+                            ++j;
+                            d = (j + 1 < VAL_WIN ? wrp[j + 1] : 1 << 30) - el;
+                        }
+                    }
                     u[k] = ul + j;
                 }
             } else {

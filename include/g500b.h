@@ -126,6 +126,29 @@ int g5_csr_fill_sorted(const uint64_t *d_edges, const float *d_weights, uint64_t
                        const uint64_t *d_rowstarts, uint64_t nentries, void *d_work, uint64_t work_bytes,
                        int32_t *d_col, float *d_w, uint64_t *d_col64, void *stream);
 
+/* The same canonical CSR by one LSD radix sort of every directed entry by
+ * (source, neighbour), the reference's two steps (src/traversal.cu:342-389:
+ * count_degrees + rowstarts scan, then fill_csr_kernel) recast:
+ * g5_csr_radix_count counts, in one pass over the edges, the entries and
+ * every sort pass's digit totals (kept in the workspace) and returns the
+ * entry count (synchronises); the caller allocates the CSR and calls
+ * g5_csr_radix_fill with the same edges, which sorts (8-bit digits,
+ * ceil(2 * ceil(log2 nverts) / 8) one-sweep passes, the first reading the
+ * edge list), then writes d_rowstarts (nverts + 1), d_col, d_w and d_col64
+ * (optional), runs of one (row, neighbour) ordered by weight bits.  Output
+ * identical to g5_csr_count + g5_csr_fill_sorted; no per-row atomics.
+ * Self-loops are dropped, duplicates kept.  Scratch:
+ * g5_csr_radix_workspace_size(nverts, nedges) bytes (24 bytes per possible
+ * entry, 2 * nedges, plus 1 per edge and 12 per vertex).  Fails with
+ * G5_ERR_INVALID when an endpoint is >= nverts or the edges changed between
+ * the calls, G5_ERR_TIMEOUT when a pass's bounded look-back wait gives up. */
+int g5_csr_radix_workspace_size(uint64_t nverts, uint64_t nedges, uint64_t *bytes);
+int g5_csr_radix_count(const uint64_t *d_edges, uint64_t nedges, uint64_t nverts, void *d_work, uint64_t work_bytes,
+                       uint64_t *nentries, void *stream);
+int g5_csr_radix_fill(const uint64_t *d_edges, const float *d_weights, uint64_t nedges, uint64_t nverts,
+                      uint64_t nentries, void *d_work, uint64_t work_bytes, uint64_t *d_rowstarts, int32_t *d_col,
+                      float *d_w, uint64_t *d_col64, void *stream);
+
 /* Sorts the rows of any CSR in place into canonical order (e.g. after
  * g5_csr_fill or g5_csr_fill_kronecker); same scratch as above. */
 int g5_csr_sort_rows(const uint64_t *d_rowstarts, uint64_t nverts, uint64_t nentries, int32_t *d_col, float *d_w,
