@@ -1206,58 +1206,98 @@ __device__ __forceinline__ void rx_gap(uint64_t *rowstarts, uint64_t r0, uint64_
     gaps[3 * g + 2] = x;
 }
 
-// Sorted keys -> col / w / row starts; runs of equal (src, dst) by weight.
+// Entry i of the sorted keys (kp, k, kn: keys i - 1, i, i + 1, ~0 past
+// the ends) -> col / w / row starts; a run of equal (src, dst) is ordered by
+// weight bits by its first entry's thread.
+__device__ __forceinline__ void rx_finish_entry(uint64_t i, unsigned long long kp, unsigned long long k,
+                                                unsigned long long kn, const unsigned long long *__restrict__ K,
+                                                const unsigned *__restrict__ V, unsigned v, uint64_t E, uint64_t n,
+                                                int lg, uint64_t *__restrict__ rowstarts, int *__restrict__ col,
+                                                float *__restrict__ w, uint64_t *__restrict__ col64,
+                                                const RadixWork &rw) {
+    unsigned *err = &rw.cnt[RXC_ERR];
+    const uint64_t src = k >> lg, dst = k & ((1ull << lg) - 1);
+    if ((i && kp > k) || src >= n) {
+        atomicOr(err, SORTERR_ORDER);
+        return;
+    }
+    col[i] = (int)dst;
+    if (col64) col64[i] = dst;
+    if (i == 0) rx_gap(rowstarts, 0, src + 1, 0, rw.gaps, rw.gcap, rw.cnt, err);
+    else if ((kp >> lg) != src) rx_gap(rowstarts, (kp >> lg) + 1, src + 1, i, rw.gaps, rw.gcap, rw.cnt, err);
+    if (i + 1 == E) rx_gap(rowstarts, src + 1, n + 1, E, rw.gaps, rw.gcap, rw.cnt, err);
+    if (kp != k && kn != k) {
+        w[i] = __uint_as_float(v);
+    } else if (kp != k) {  // the first of a run of equal keys: the run's weights, sorted
+        uint64_t j = i + 1;
+        while (j < E && K[j] == k) ++j;
+        const uint64_t L = j - i;
+        if (L <= RX_RUN_INLINE) {
+            unsigned x[RX_RUN_INLINE];
+            for (unsigned q = 0; q < (unsigned)L; ++q) {
+                const unsigned y = V[i + q];
+                unsigned b = q;
+                while (b > 0 && x[b - 1] > y) {
+                    x[b] = x[b - 1];
+                    --b;
+                }
+                x[b] = y;
+            }
+            for (unsigned q = 0; q < (unsigned)L; ++q) w[i + q] = __uint_as_float(x[q]);
+        } else {
+            for (uint64_t q = i; q < j; ++q) w[q] = __uint_as_float(V[q]);
+            const unsigned r = atomicAdd(&rw.cnt[RXC_RUNS], 1u);
+            if (r >= rw.rcap) {
+                atomicOr(err, SORTERR_CAPACITY);
+            } else {
+                rw.runs[2 * r] = i;
+                rw.runs[2 * r + 1] = j;
+                if (L <= SORT_SMEM_KEYS) rw.rmid[atomicAdd(&rw.scnt[0], 1u)] = 2 * r;
+                else rw.rbig[atomicAdd(&rw.scnt[1], 1u)] = 2 * r;
+            }
+        }
+    }
+}
+
+// Sorted keys -> col / w / row starts, RX_FIN consecutive entries a thread
+// (16-byte loads of the keys and weights; the neighbours' keys from L1).
+constexpr int RX_FIN = 4;  // the loads below are written for 4
+
 __global__ void csr_radix_finish_kernel(const unsigned long long *__restrict__ K, const unsigned *__restrict__ V,
                                         uint64_t E, uint64_t n, int lg, uint64_t *__restrict__ rowstarts,
                                         int *__restrict__ col, float *__restrict__ w, uint64_t *__restrict__ col64,
                                         RadixWork rw) {
-    const unsigned long long dmask = (1ull << lg) - 1;
-    unsigned *err = &rw.cnt[RXC_ERR];
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += stride) {
-        const unsigned long long k = K[i];
-        const unsigned long long kp = i ? K[i - 1] : ~0ull, kn = i + 1 < E ? K[i + 1] : ~0ull;
-        const uint64_t src = k >> lg, dst = k & dmask;
-        if ((i && kp > k) || src >= n) {
-            atomicOr(err, SORTERR_ORDER);
-            continue;
-        }
-        col[i] = (int)dst;
-        if (col64) col64[i] = dst;
-        if (i == 0) rx_gap(rowstarts, 0, src + 1, 0, rw.gaps, rw.gcap, rw.cnt, err);
-        else if ((kp >> lg) != src) rx_gap(rowstarts, (kp >> lg) + 1, src + 1, i, rw.gaps, rw.gcap, rw.cnt, err);
-        if (i + 1 == E) rx_gap(rowstarts, src + 1, n + 1, E, rw.gaps, rw.gcap, rw.cnt, err);
-        if (kp != k && kn != k) {
-            w[i] = __uint_as_float(V[i]);
-        } else if (kp != k) {  // the first of a run of equal keys: the run's weights, sorted
-            uint64_t j = i + 1;
-            while (j < E && K[j] == k) ++j;
-            const uint64_t L = j - i;
-            if (L <= RX_RUN_INLINE) {
-                unsigned x[RX_RUN_INLINE];
-                for (unsigned q = 0; q < (unsigned)L; ++q) {
-                    const unsigned y = V[i + q];
-                    unsigned b = q;
-                    while (b > 0 && x[b - 1] > y) {
-                        x[b] = x[b - 1];
-                        --b;
-                    }
-                    x[b] = y;
-                }
-                for (unsigned q = 0; q < (unsigned)L; ++q) w[i + q] = __uint_as_float(x[q]);
-            } else {
-                for (uint64_t q = i; q < j; ++q) w[q] = __uint_as_float(V[q]);
-                const unsigned r = atomicAdd(&rw.cnt[RXC_RUNS], 1u);
-                if (r >= rw.rcap) {
-                    atomicOr(err, SORTERR_CAPACITY);
-                } else {
-                    rw.runs[2 * r] = i;
-                    rw.runs[2 * r + 1] = j;
-                    if (L <= SORT_SMEM_KEYS) rw.rmid[atomicAdd(&rw.scnt[0], 1u)] = 2 * r;
-                    else rw.rbig[atomicAdd(&rw.scnt[1], 1u)] = 2 * r;
-                }
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g * RX_FIN < E; g += stride) {
+        const uint64_t i0 = g * RX_FIN;
+        unsigned long long k[RX_FIN + 2];  // keys i0 - 1 .. i0 + RX_FIN
+        unsigned v[RX_FIN];
+        k[0] = i0 ? K[i0 - 1] : ~0ull;
+        if (i0 + RX_FIN <= E) {  // K and V are 256-byte aligned, i0 a multiple of 4: 16-byte aligned
+            const ulonglong2 a = *reinterpret_cast<const ulonglong2 *>(K + i0);
+            const ulonglong2 b = *reinterpret_cast<const ulonglong2 *>(K + i0 + 2);
+            const uint4 c = *reinterpret_cast<const uint4 *>(V + i0);
+            k[1] = a.x;
+            k[2] = a.y;
+            k[3] = b.x;
+            k[4] = b.y;
+            v[0] = c.x;
+            v[1] = c.y;
+            v[2] = c.z;
+            v[3] = c.w;
+            k[RX_FIN + 1] = i0 + RX_FIN < E ? K[i0 + RX_FIN] : ~0ull;
+        } else {
+#pragma unroll
+            for (int q = 0; q < RX_FIN; ++q) {
+                k[q + 1] = i0 + q < E ? K[i0 + q] : ~0ull;
+                v[q] = i0 + q < E ? V[i0 + q] : 0u;
             }
+            k[RX_FIN + 1] = ~0ull;
         }
+#pragma unroll
+        for (int q = 0; q < RX_FIN; ++q)
+            if (i0 + q < E) rx_finish_entry(i0 + q, k[q], k[q + 1], k[q + 2], K, V, v[q], E, n, lg, rowstarts, col, w,
+                                            col64, rw);
     }
 }
 
@@ -1512,7 +1552,7 @@ extern "C" int g5_csr_radix_fill(const uint64_t *d_edges, const float *d_weights
         kout = kout == w.ka ? w.kb : w.ka;
         vout = vout == w.va ? w.vb : w.va;
     }
-    const int fgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((E + 255) / 256, (uint64_t)sort_grid(8)));
+    const int fgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((E / RX_FIN + 256) / 256, (uint64_t)sort_grid(8)));
     csr_radix_finish_kernel<<<fgrid, 256, 0, st>>>(kin, vin, E, nverts, lg, d_rowstarts, d_col, d_w, d_col64, w);
     csr_radix_gaps_kernel<<<sort_grid(2), 256, 0, st>>>(w.gaps, w.cnt, w.gcap, d_rowstarts);
     G5_CUDA_TRY(cudaGetLastError());
