@@ -354,6 +354,34 @@ def run_ours(args):
         e2e_s.append(float(np.median(reps)))
     e2e_hm = hmean_gteps(t_nedge, e2e_s)
 
+    # The same calls with the search's result brought to the host as well:
+    # right behind the search, g5_bfs_export's kernel writes one 16-byte
+    # record (vertex, depth, parent) per reached vertex straight into pinned
+    # host memory; one C call (g5_bfs_query_plan_export), one wait.
+    xbuf = torch.empty(16 * n, dtype=torch.uint8).pin_memory()
+    first_root = {}
+    for r in timed:
+        first_root.setdefault(id(state(r)), r)
+    for r in first_root.values():  # each state's with-depth query plan made before timing
+        G.oned_graph_bfs_reset(state(r), with_depth=True, g=g)
+        G.oned_graph_bfs_query_export(g, state(r), int(r), with_depth=True, out=xbuf, params=bparams)
+    e2e_res_s, e2e_res_bytes = [], []
+    for r in timed:
+        reps = []
+        for _ in range(E2E_REPS):
+            G.oned_graph_bfs_reset(state(r), with_depth=True, g=g)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            _, rec = G.oned_graph_bfs_query_export(g, state(r), int(r), with_depth=True, out=xbuf, params=bparams)
+            reps.append(time.perf_counter() - t)
+            assert len(rec) == reached[r]
+        root_rec = rec[rec["vertex"] == r]
+        assert len(root_rec) == 1 and root_rec["parent"][0] == r and root_rec["depth"][0] == 0
+        e2e_res_s.append(float(np.median(reps)))
+        e2e_res_bytes.append(24 + 8 + 16 * len(rec))
+    e2e_res_hm = hmean_gteps(t_nedge, e2e_res_s)
+    del xbuf
+
     # Whole-job numbers across ranks: slowest rank's time, all ranks' edges.
     tot_edges = float(np.sum(t_nedge))
     max_ms = total_ms
@@ -420,7 +448,18 @@ def run_ours(args):
                     "timing": f"median of {E2E_REPS} calls per root (reset untimed before each)",
                     "path": "oned_graph_bfs_query -> C ABI g5_bfs_query after an untimed reset: the kernel "
                             "reads the 8-byte root from pinned host memory and writes the 24-byte stats back "
-                            "to pinned host memory (over PCIe, inside the timed call), host wall clock"},
+                            "to pinned host memory (over PCIe, inside the timed call), host wall clock",
+                    "with_result": {
+                        "value": float(f"{(e2e_res_hm if world == 1 else e2e_res_hm * world):.6g}"),
+                        "unit": "GTEPS", "h2d_bytes_per_step": 8,
+                        "d2h_bytes_per_step": int(np.mean(e2e_res_bytes)) if e2e_res_bytes else 0,
+                        "small_root_us": round(min(e2e_res_s) * 1e6, 1) if e2e_res_s else None,
+                        "big_root_ms_mean": round(float(np.mean([e2e_res_s[i] for i in big])) * 1e3, 3)
+                        if big else None,
+                        "path": "oned_graph_bfs_query_export -> C ABI g5_bfs_query_plan_export after an "
+                                "untimed reset: the search, then one 16-byte record (vertex, depth, parent) per "
+                                "reached vertex written by a kernel into pinned host memory, one host wait, "
+                                "median of 3 calls per root"}},
             "sssp": {"value": float(f"{s_hm:.6g}"), "unit": "GTEPS (harmonic mean)",
                      "hmean_gteps_with_reset": float(f"{hmean_gteps(t_nedge, s_secs_reset):.6g}"),
                      "median_gteps": round(float(np.median(s_per_root)), 3),

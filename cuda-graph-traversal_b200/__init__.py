@@ -97,8 +97,10 @@ def _load() -> C.CDLL:
         "g5_graph_isolated_bitmap": ([p, u64, p, p], C.c_int),
         "g5_bfs_traverse": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_bfs_query": ([p, p, u64, p, p, p, p, p, u64, p, p, p], C.c_int),
+        "g5_bfs_export": ([p, p, u64, p, u64, p, u64, p, p], C.c_int),
         "g5_bfs_query_plan_create": ([p, p, u64, p, p, p, p, u64, p, p, p, p], C.c_int),
         "g5_bfs_query_plan_run": ([p, u64], C.c_int),
+        "g5_bfs_query_plan_export": ([p, u64, p, u64, p], C.c_int),
         "g5_bfs_query_plan_destroy": ([p], None),
         "g5_bfs_visited_bitmap": ([p, u64, u64, p, p], C.c_int),
         "g5_bfs_last_stats": ([p, u64, p, p], C.c_int),
@@ -138,6 +140,7 @@ def _load() -> C.CDLL:
 
 lib = _load()
 _plan_run = lib.g5_bfs_query_plan_run
+_plan_export = lib.g5_bfs_query_plan_export
 
 
 def _check(rc: int) -> None:
@@ -853,6 +856,38 @@ def _main_bits_ptr(g: OnedGraph) -> int | None:
     return c[1]
 
 
+# One record of g5_bfs_export.
+REACHED_DTYPE = np.dtype([("vertex", "<u4"), ("depth", "<i4"), ("parent", "<i8")])
+
+
+def oned_graph_bfs_export(g: OnedGraph, bfs: BfsState, with_depth: bool = False, stream=None,
+                          out: torch.Tensor | None = None) -> np.ndarray | torch.Tensor:
+    """The last search's result for the host (g5_bfs_export): one record
+    (vertex, depth, parent) per reached vertex, root included -- depth -1
+    unless with_depth (the search must have kept depths: a query or run
+    with_depth).  `out`: a uint8 tensor of at least 16 bytes per record, in
+    pinned host memory (the kernel writes the records there itself; the
+    result is a numpy structured view of REACHED_DTYPE) or on the device (a
+    byte tensor of the records); by default a pinned buffer of the state,
+    overwritten by its next export.  After a one-block search the records
+    come from its touched list, in the order reached (the cost follows the
+    result); otherwise in no particular order."""
+    n = g.nglobalverts
+    if out is None:
+        if getattr(bfs, "_xbuf", None) is None or bfs._xbuf.numel() < 16 * n:
+            bfs._xbuf = torch.empty(16 * n, dtype=torch.uint8).pin_memory()
+        out = bfs._xbuf
+    if getattr(bfs, "_xcnt", None) is None:
+        bfs._xcnt = torch.zeros(8, dtype=torch.uint8).pin_memory()
+    cap = out.numel() // 16
+    _check(lib.g5_bfs_export(_ptr(bfs.pred), _ptr(bfs.depth) if with_depth else None, n, _ptr(bfs.work),
+                             bfs.work.numel(), _ptr(out), cap, bfs._xcnt.data_ptr(), _stream(stream)))
+    cnt = int(C.c_uint64.from_address(bfs._xcnt.data_ptr()).value)
+    if out.device.type == "cpu":
+        return out.numpy()[: 16 * cnt].view(REACHED_DTYPE)
+    return out[: 16 * cnt]
+
+
 def oned_graph_bfs_query(g: OnedGraph, bfs: BfsState, root: int, with_depth: bool = False,
                          stream=None, params: BfsParams | None = None) -> BfsStats:
     """One search end to end from the host, the reference's synchronous
@@ -872,6 +907,33 @@ def oned_graph_bfs_query(g: OnedGraph, bfs: BfsState, root: int, with_depth: boo
     if rc:
         _check(rc)
     return bfs.h_stats
+
+
+def oned_graph_bfs_query_export(g: OnedGraph, bfs: BfsState, root: int, with_depth: bool = True,
+                                out: torch.Tensor | None = None, stream=None,
+                                params: BfsParams | None = None) -> tuple[BfsStats, np.ndarray]:
+    """oned_graph_bfs_query and oned_graph_bfs_export in one C call
+    (g5_bfs_query_plan_export): the search, then right behind it in the
+    stream the export of its result into pinned host memory (`out`, a
+    pinned uint8 tensor of 16 bytes a record; by default the state's own
+    buffer), with one wait on the host.  Returns the statistics and the
+    records (REACHED_DTYPE, a view of `out`)."""
+    st = _stream(stream)
+    plan = bfs._plan
+    if (plan is None or plan[0] is not g or plan[1] != with_depth or plan[2] != st or plan[4] is not g.main_bits
+            or plan[5] is not params or plan[6] is not g.bfs_col):
+        plan = _make_query_plan(g, bfs, with_depth, st, params)
+    if out is None:
+        if getattr(bfs, "_xbuf", None) is None or bfs._xbuf.numel() < 16 * g.nglobalverts:
+            bfs._xbuf = torch.empty(16 * g.nglobalverts, dtype=torch.uint8).pin_memory()
+        out = bfs._xbuf
+    if getattr(bfs, "_xcnt", None) is None:
+        bfs._xcnt = torch.zeros(8, dtype=torch.uint8).pin_memory()
+    rc = _plan_export(plan[3], root, out.data_ptr(), out.numel() // 16, bfs._xcnt.data_ptr())
+    if rc:
+        _check(rc)
+    cnt = int(C.c_uint64.from_address(bfs._xcnt.data_ptr()).value)
+    return bfs.h_stats, out.numpy()[: 16 * cnt].view(REACHED_DTYPE)
 
 
 def _make_query_plan(g: OnedGraph, bfs: BfsState, with_depth: bool, st, params: BfsParams | None = None):

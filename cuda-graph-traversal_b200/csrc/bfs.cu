@@ -82,6 +82,9 @@ struct BfsCtl {
     unsigned long long m_level[BFS_TRACE];
     unsigned n_level[BFS_TRACE];
     unsigned char mode_level[BFS_TRACE];
+    // g5_bfs_export: records appended, blocks finished, the final count
+    unsigned long long xcount, xresult;
+    unsigned xdone;
 };
 
 // What the last search on a workspace wrote, for g5_bfs_reset_touched.
@@ -124,6 +127,12 @@ struct BfsArgs {
     unsigned nroots;
     BfsTouch *touch;
     unsigned *tlist;  // touched list of the one-block search (n entries)
+    // The one-block search's own export of its result (g5_bfs_query_plan_export):
+    // records into xout (device-addressable, xcap of them), then the count to
+    // pinned host memory (xcount_map).  nullptr: no export.
+    g5_bfs_reached *xout;
+    uint64_t xcap;
+    unsigned long long *xcount_map;
     unsigned big_deg;       // queue entries with more edges go to the chunked big part
     unsigned chunk;         // edges of a big entry per warp grab (a multiple of 32)
     unsigned lane_entries;  // bottom-up: row head a lane scans alone (a multiple of BU_STEP)
@@ -131,6 +140,16 @@ struct BfsArgs {
 
 enum { TOP_DOWN = 0, BOTTOM_UP = 1 };
 constexpr int BFS_SMALL = 3;  // g5_bfs_params.mode: one lean block, for a root in a small component
+
+static_assert(sizeof(g5_bfs_reached) == 16, "one 16-byte store a record");
+
+// One record as one 16-byte store (a single bus write when `out` is host
+// memory): {vertex, depth} then the parent, the g5_bfs_reached layout.
+__device__ __forceinline__ void put_reached(g5_bfs_reached *out, uint64_t i, unsigned v, int d, int64_t p) {
+    reinterpret_cast<ulonglong2 *>(out)[i] =
+        make_ulonglong2((unsigned long long)v | (unsigned long long)(unsigned)d << 32, (unsigned long long)p);
+}
+
 
 // Bottom-up: entries of a row a lane scans on its own before the rest of
 // the row goes to the whole warp (default of g5_bfs_params.lane_entries).
@@ -532,6 +551,8 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(BfsArgs 
             // earlier search on the workspace can release them.
             c->t0 = globaltimer_ns();
             c->res = g5_bfs_stats{0, 0, 0, 0, 0};
+            c->xcount = 0;
+            c->xdone = 0;
             c->bar = 0;
             a.touch->small = 0;  // the next reset clears everything
             for (int k = 0; k < 3; ++k) {
@@ -733,6 +754,8 @@ __global__ void __launch_bounds__(BFS_THREADS) bfs_small_kernel(BfsArgs a) {
     const unsigned lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (threadIdx.x == 0) {
         c->t0 = globaltimer_ns();
+        c->xcount = 0;
+        c->xdone = 0;
         const unsigned long long root = a.root;
         if (root >= a.n) {
             s_err = DEVERR_RANGE;  // the host checks roots; a bad one is reported, not used
@@ -821,6 +844,22 @@ __global__ void __launch_bounds__(BFS_THREADS) bfs_small_kernel(BfsArgs a) {
         // that reported an error leaves the next reset a full one).
         *a.touch = BfsTouch{s_err == 0 && s_reached <= a.n ? 1u : 0u, 0u, s_reached, a.pred, a.depth, c->init_used};
         bfs_publish_stats(a);
+    }
+    if (a.xout) {
+        // The result for the host: a record per touched vertex, then the
+        // count (after the statistics above and a system fence).
+        __syncthreads();
+        const unsigned long long cnt = s_reached < a.n ? s_reached : a.n;
+        for (uint64_t i = threadIdx.x; i < cnt && i < a.xcap; i += blockDim.x) {
+            const unsigned v = a.tlist[i];
+            put_reached(a.xout, i, v, a.depth ? a.depth[v] : -1, a.pred[v]);
+        }
+        __threadfence_system();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            c->xresult = cnt;
+            *(volatile unsigned long long *)a.xcount_map = cnt;
+        }
     }
 }
 
@@ -1064,7 +1103,8 @@ static int bfs_params_check(const g5_bfs_params &p, const char *who) {
 static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
                       uint64_t root, int64_t *d_pred, int32_t *d_depth, const g5_bfs_params *params,
                       cudaStream_t st, const uint64_t *d_roots = nullptr, unsigned nroots = 0,
-                      g5_bfs_stats *d_stats_map = nullptr) {
+                      g5_bfs_stats *d_stats_map = nullptr, g5_bfs_reached *xout = nullptr, uint64_t xcap = 0,
+                      unsigned long long *xcount_map = nullptr) {
     g5_bfs_params p = {14.0f, 24.0f, 0, 0};
     if (params) p = *params;
     int rc = bfs_params_check(p, "g5_bfs");
@@ -1101,6 +1141,9 @@ static int bfs_launch(const BfsWork &w, const uint64_t *d_rowstarts, const int32
     a.nroots = nroots;
     a.touch = w.touch;
     a.tlist = w.base[0];  // unused by the one-block search, which is the only writer
+    a.xout = xout;  // only the one-block search exports by itself
+    a.xcap = xcap;
+    a.xcount_map = xcount_map;
     a.big_deg = p.big_deg ? (unsigned)p.big_deg : BFS_BIG_DEG;
     a.chunk = p.chunk ? (unsigned)p.chunk : BFS_CHUNK;
     a.lane_entries = p.lane_entries ? (unsigned)p.lane_entries : BU_LANE_ENTRIES;
@@ -1162,6 +1205,66 @@ extern "C" int g5_bfs_traverse_multi(const uint64_t *d_rowstarts, const int32_t 
 }
 
 // Device address of pinned host memory `h`, when the device can address it.
+// g5_bfs_export: records of the reached vertices.  After a one-block
+// search, from its touched list by block 0; otherwise a scan of the parents
+// with warp-aggregated appends, the last block to finish publishing the
+// count.  A host-mapped count is written after a system fence that follows
+// every record.
+__global__ void __launch_bounds__(256) bfs_export_kernel(const int64_t *__restrict__ pred,
+                                                          const int *__restrict__ depth, uint64_t n,
+                                                          const BfsTouch *__restrict__ touch,
+                                                          const unsigned *__restrict__ tlist, BfsCtl *c,
+                                                          g5_bfs_reached *out, uint64_t cap,
+                                                          unsigned long long *count_map) {
+    __shared__ unsigned s_last;
+    if (touch->small) {
+        // The touched list: block 0 alone (it is short), the others leave.
+        if (blockIdx.x != 0) return;
+        const uint64_t cnt = touch->count;
+        for (uint64_t i = threadIdx.x; i < cnt && i < cap; i += blockDim.x) {
+            const unsigned v = tlist[i];
+            put_reached(out, i, v, depth ? depth[v] : -1, pred[v]);
+        }
+        __threadfence_system();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            c->xresult = cnt;
+            if (count_map) *(volatile unsigned long long *)count_map = cnt;
+        }
+        return;
+    }
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const unsigned lane = lane_id();
+    for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x - lane; b < n; b += stride) {  // warp-uniform
+        const uint64_t v = b + lane;
+        const int64_t p = v < n ? pred[v] : -1;
+        const bool reached = p != -1;
+        const unsigned m = __ballot_sync(FULL, reached);
+        if (!m) continue;
+        const unsigned leader = __ffs(m) - 1;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(&c->xcount, (unsigned long long)__popc(m));
+        base = __shfl_sync(FULL, base, leader);
+        const unsigned long long pos = base + __popc(m & lanemask_lt());
+        if (reached && pos < cap) put_reached(out, pos, (unsigned)v, depth ? depth[v] : -1, p);
+    }
+    __threadfence_system();  // this thread's records before the count
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&c->xdone, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        const unsigned long long cnt = atomicAdd(&c->xcount, 0ull);
+        c->xresult = cnt;
+        c->xcount = 0;  // ready for another export of the same search
+        c->xdone = 0;
+        if (count_map) {
+            __threadfence_system();
+            *(volatile unsigned long long *)count_map = cnt;
+        }
+    }
+}
+
 static bool host_mapped(const void *h, void **d) {
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, h) != cudaSuccess) {
@@ -1229,6 +1332,52 @@ extern "C" int g5_bfs_query(const uint64_t *d_rowstarts, const int32_t *d_col, u
     return deverr_to_status(h_stats->error_flags, "g5_bfs_query");
 }
 
+extern "C" int g5_bfs_export(const int64_t *d_pred, const int32_t *d_depth, uint64_t nverts, void *d_work,
+                             uint64_t work_bytes, g5_bfs_reached *out, uint64_t capacity, uint64_t *h_count,
+                             void *stream) {
+    clear_error();
+    G5_CHECK_ARG(h_count && out && d_pred, "g5_bfs_export: NULL argument");
+    G5_CHECK_ARG(((uintptr_t)out & 15) == 0, "g5_bfs_export: out is not 16-byte aligned");
+    G5_CHECK_ARG(nverts >= 1 && nverts <= (1ull << 31), "g5_bfs_export: nverts outside [1, 2^31]");
+    G5_CHECK_ARG(d_work, "g5_bfs_export: workspace is NULL");
+    const BfsWork w = carve_bfs(d_work, nverts);
+    if (work_bytes < w.bytes)
+        return set_error(G5_ERR_WORKSPACE, "g5_bfs_export: workspace %llu < %llu bytes",
+                         (unsigned long long)work_bytes, (unsigned long long)w.bytes);
+    void *out_dev = out, *cnt_dev = nullptr;
+    host_mapped(out, &out_dev);  // pinned host records: the kernel writes them itself
+    const bool mapped_count = host_mapped(h_count, &cnt_dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    DeviceInfo di;
+    const int sms = device_info(&di) ? 148 : di.sms;
+    const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((nverts + 255) / 256, (uint64_t)sms * 2));
+    if (mapped_count) *(volatile uint64_t *)h_count = ~0ull;
+    bfs_export_kernel<<<grid, 256, 0, st>>>(d_pred, d_depth, nverts, w.touch, w.base[0], w.ctl,
+                                            (g5_bfs_reached *)out_dev, capacity,
+                                            mapped_count ? (unsigned long long *)cnt_dev : nullptr);
+    G5_CUDA_TRY(cudaGetLastError());
+    if (mapped_count) {
+        volatile uint64_t *hc = h_count;
+        const auto t0 = std::chrono::steady_clock::now();
+        while (*hc == ~0ull) {
+            if (std::chrono::duration<double, std::nano>(std::chrono::steady_clock::now() - t0).count() >
+                QUERY_SPIN_NS) {
+                G5_CUDA_TRY(cudaStreamSynchronize(st));
+                break;
+            }
+        }
+        std::atomic_thread_fence(std::memory_order_acquire);
+        if (*hc == ~0ull) return set_error(G5_ERR_DEVICE, "g5_bfs_export: the export ended without a count");
+    } else {
+        G5_CUDA_TRY(cudaMemcpyAsync(h_count, &w.ctl->xresult, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+        G5_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    if (*h_count > capacity)
+        return set_error(G5_ERR_INVALID, "g5_bfs_export: %llu reached vertices, capacity %llu",
+                         (unsigned long long)*h_count, (unsigned long long)capacity);
+    return G5_OK;
+}
+
 // A prepared g5_bfs_query: everything but the root checked and resolved
 // once, so a query costs one launch and the wait.
 struct g5_bfs_query_plan {
@@ -1242,6 +1391,12 @@ struct g5_bfs_query_plan {
     g5_bfs_params params;
     g5_bfs_stats *h_stats, *d_stats;
     cudaStream_t stream;
+    // g5_bfs_query_plan_export: the export buffers last resolved
+    g5_bfs_reached *x_out = nullptr;
+    void *x_out_dev = nullptr;
+    uint64_t *x_count = nullptr;
+    void *x_count_dev = nullptr;
+    int sms = 148;
 };
 
 extern "C" int g5_bfs_query_plan_create(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts,
@@ -1265,6 +1420,8 @@ extern "C" int g5_bfs_query_plan_create(const uint64_t *d_rowstarts, const int32
     auto *q = new (std::nothrow) g5_bfs_query_plan{d_rowstarts, d_col, nverts, h_main_bits, d_pred, d_depth, w, p,
                                                    h_stats, (g5_bfs_stats *)d_stats, (cudaStream_t)stream};
     if (!q) return set_error(G5_ERR_INVALID, "g5_bfs_query_plan_create: out of host memory");
+    DeviceInfo di;
+    if (!device_info(&di)) q->sms = di.sms;
     *out = q;
     return G5_OK;
 }
@@ -1284,6 +1441,74 @@ extern "C" int g5_bfs_query_plan_run(g5_bfs_query_plan *q, uint64_t root) {
                         q->d_stats);
     if (rc) return rc;
     return query_wait(q->h_stats, q->stream, "g5_bfs_query_plan_run");
+}
+
+extern "C" int g5_bfs_query_plan_export(g5_bfs_query_plan *q, uint64_t root, g5_bfs_reached *out,
+                                        uint64_t capacity, uint64_t *h_count) {
+    clear_error();
+    G5_CHECK_ARG(q && out && h_count, "g5_bfs_query_plan_export: NULL argument");
+    G5_CHECK_ARG(((uintptr_t)out & 15) == 0, "g5_bfs_query_plan_export: out is not 16-byte aligned");
+    G5_CHECK_ARG(root < q->nverts, "g5_bfs_query_plan_export: root %llu outside [0, %llu)",
+                 (unsigned long long)root, (unsigned long long)q->nverts);
+    if (out != q->x_out) {
+        q->x_out_dev = out;
+        host_mapped(out, &q->x_out_dev);
+        q->x_out = out;
+    }
+    if (h_count != q->x_count) {
+        q->x_count_dev = nullptr;
+        host_mapped(h_count, &q->x_count_dev);
+        q->x_count = h_count;
+    }
+    g5_bfs_params p = q->params;
+    const bool small = q->main_bits && p.blocks == 0 && !((q->main_bits[root >> 5] >> (root & 31)) & 1u);
+    if (small) {
+        p.blocks = 1;
+        p.mode = BFS_SMALL;
+    }
+    *(volatile int32_t *)&q->h_stats->levels = -1;
+    if (q->x_count_dev) *(volatile uint64_t *)h_count = ~0ull;
+    // A small search with a host-mapped count writes its records itself at
+    // its end; otherwise the export kernel runs right behind the search in
+    // the stream (a grid scan of the parents).  The host waits once, on the
+    // count.
+    const bool fused = small && q->x_count_dev;
+    int rc = bfs_launch(q->w, q->rowstarts, q->col, q->nverts, root, q->pred, q->depth, &p, q->stream, nullptr, 0,
+                        q->d_stats, fused ? (g5_bfs_reached *)q->x_out_dev : nullptr, capacity,
+                        fused ? (unsigned long long *)q->x_count_dev : nullptr);
+    if (rc) return rc;
+    if (!fused) {
+        const int grid = small ? 1 : (int)std::max<uint64_t>(1, std::min<uint64_t>((q->nverts + 255) / 256,
+                                                                                  (uint64_t)q->sms * 2));
+        bfs_export_kernel<<<grid, 256, 0, q->stream>>>(q->pred, q->depth, q->nverts, q->w.touch, q->w.base[0],
+                                                       q->w.ctl, (g5_bfs_reached *)q->x_out_dev, capacity,
+                                                       (unsigned long long *)q->x_count_dev);
+        G5_CUDA_TRY(cudaGetLastError());
+    }
+    if (q->x_count_dev) {
+        volatile uint64_t *hc = h_count;
+        const auto t0 = std::chrono::steady_clock::now();
+        while (*hc == ~0ull) {
+            if (std::chrono::duration<double, std::nano>(std::chrono::steady_clock::now() - t0).count() >
+                QUERY_SPIN_NS) {
+                G5_CUDA_TRY(cudaStreamSynchronize(q->stream));
+                break;
+            }
+        }
+        std::atomic_thread_fence(std::memory_order_acquire);
+        if (*hc == ~0ull) return set_error(G5_ERR_DEVICE, "g5_bfs_query_plan_export: the export ended without a count");
+    } else {
+        G5_CUDA_TRY(cudaMemcpyAsync(h_count, &q->w.ctl->xresult, sizeof(uint64_t), cudaMemcpyDeviceToHost, q->stream));
+        G5_CUDA_TRY(cudaStreamSynchronize(q->stream));
+    }
+    // The search's statistics landed before the export began (stream order).
+    if (*(volatile int32_t *)&q->h_stats->levels == -1)
+        return set_error(G5_ERR_DEVICE, "g5_bfs_query_plan_export: the search ended without statistics");
+    if ((rc = deverr_to_status(q->h_stats->error_flags, "g5_bfs_query_plan_export"))) return rc;
+    if (*h_count > capacity)
+        return set_error(G5_ERR_INVALID, "g5_bfs_query_plan_export: %llu reached vertices, capacity %llu",
+                         (unsigned long long)*h_count, (unsigned long long)capacity);
+    return G5_OK;
 }
 
 extern "C" void g5_bfs_query_plan_destroy(g5_bfs_query_plan *q) { delete q; }

@@ -239,6 +239,13 @@ typedef struct g5_bfs_stats {
     int32_t solo_levels;      /* levels run by one block before the grid       */
 } g5_bfs_stats;
 
+/* One reached vertex of a search, for the host (g5_bfs_export). */
+typedef struct g5_bfs_reached {
+    uint32_t vertex;
+    int32_t depth;
+    int64_t parent;
+} g5_bfs_reached;
+
 int g5_bfs_workspace_size(uint64_t nverts, uint64_t *bytes);
 
 /* oned_graph_bfs_run, src/traversal.h:47 (src/traversal.cu:479-503): BFS
@@ -317,6 +324,12 @@ int g5_bfs_query_plan_create(const uint64_t *d_rowstarts, const int32_t *d_col, 
                              uint64_t work_bytes, const g5_bfs_params *params, g5_bfs_stats *h_stats, void *stream,
                              g5_bfs_query_plan **plan);
 int g5_bfs_query_plan_run(g5_bfs_query_plan *plan, uint64_t root);
+/* g5_bfs_query_plan_run followed by g5_bfs_export of its result into `out`
+ * (capacity records, *h_count the reached count), with one wait on the
+ * host: the export kernel runs right behind the search in the stream (one
+ * block after a search of a small component). */
+int g5_bfs_query_plan_export(g5_bfs_query_plan *plan, uint64_t root, g5_bfs_reached *out, uint64_t capacity,
+                             uint64_t *h_count);
 void g5_bfs_query_plan_destroy(g5_bfs_query_plan *plan);
 
 /* Copies the visited bitmap of the last search on this workspace (bit v set
@@ -324,6 +337,23 @@ void g5_bfs_query_plan_destroy(g5_bfs_query_plan *plan);
  * vertex of the largest component, reset without an initial bitmap, this
  * is the main-component bitmap g5_bfs_query takes. */
 int g5_bfs_visited_bitmap(const void *d_work, uint64_t work_bytes, uint64_t nverts, uint32_t *d_bits, void *stream);
+
+/* The result of the last search on this workspace, for the host: one
+ * record per reached vertex (root included) -- its index, depth (-1 when the
+ * search kept no depth array) and parent -- written to `out` (device memory,
+ * or pinned host memory mapped into the device: then the kernel writes it
+ * over the bus itself, no copy call), with *h_count = the number of reached
+ * vertices.  After a one-block search (a root in a small component) it reads
+ * that search's list of touched vertices, records in the order reached, so
+ * its cost follows the result, not nverts; otherwise it scans the parents,
+ * records in no particular order.  Same d_pred / d_depth as the search.
+ * More reached vertices than `capacity`: the first `capacity` records are
+ * written, *h_count holds the full count and G5_ERR_INVALID is returned.
+ * `out` must be 16-byte aligned.  Synchronises (returns once the records
+ * are in place).  The reference
+ * leaves Bfs_State.pred on the device (src/traversal.h:59-66). */
+int g5_bfs_export(const int64_t *d_pred, const int32_t *d_depth, uint64_t nverts, void *d_work, uint64_t work_bytes,
+                  g5_bfs_reached *out, uint64_t capacity, uint64_t *h_count, void *stream);
 
 /* Statistics of the last g5_bfs_run that used this workspace (synchronises). */
 int g5_bfs_last_stats(const void *d_work, uint64_t work_bytes, g5_bfs_stats *stats, void *stream);
