@@ -108,6 +108,9 @@ def _load() -> C.CDLL:
         "g5_bfs_dist_from_pred": ([p, p, u64, p, u64, p, p, u64, p], C.c_int),
         "g5_sssp_workspace_size": ([u64, p], C.c_int),
         "g5_sssp_run": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
+        "g5_sssp_multi_workspace_size": ([u64, p], C.c_int),
+        "g5_sssp_multi_run": ([p, p, p, u64, p, p, p, C.c_uint32, p, p, p, u64, C.c_float, C.c_int32, p, p],
+                              C.c_int),
         "g5_sssp_last_status": ([p, u64, p, p, p], C.c_int),
         "g5_sssp_reset": ([u64, p, p, p, u64, p], C.c_int),
         "g5_sssp_reset_touched": ([u64, p, p, p, u64, p], C.c_int),
@@ -166,6 +169,11 @@ class MsBfsParams(C.Structure):
 class MsBfsStats(C.Structure):
     _fields_ = [("levels", C.c_int32), ("pull_levels", C.c_int32), ("error_flags", C.c_uint32),
                 ("nroots", C.c_uint32), ("pairs_reached", C.c_uint64), ("frontier_edges", C.c_uint64)]
+
+
+class SsspMultiStats(C.Structure):
+    _fields_ = [("rounds", C.c_int32), ("error_flags", C.c_uint32), ("frontier_entries", C.c_uint64),
+                ("entries_scanned", C.c_uint64)]
 
 
 class SsspParams(C.Structure):
@@ -1116,6 +1124,40 @@ def oned_graph_sssp_run(g: OnedGraph, sssp: SsspState, root: int, delta: float =
                            g.nglobalverts, root, _ptr(sssp.dist), _ptr(sssp.pred), _ptr(sssp.work),
                            sssp.work.numel(), C.byref(p), _stream(stream)))
     sssp.was_reset = True  # g5_sssp_run resets in full first
+
+
+def sssp_multi_workspace(g: OnedGraph) -> torch.Tensor:
+    """Scratch of oned_graph_sssp_multi (about 276 bytes per vertex)."""
+    nb = C.c_uint64()
+    _check(lib.g5_sssp_multi_workspace_size(g.nglobalverts, C.byref(nb)))
+    return _workspace(nb.value, g.device)
+
+
+def oned_graph_sssp_multi(g: OnedGraph, sources, work: torch.Tensor | None = None, with_pred: bool = True,
+                          blocks: int = 0, stream=None, delta: float = 0.0, dist: torch.Tensor | None = None,
+                          pred: torch.Tensor | None = None) -> tuple[torch.Tensor, torch.Tensor | None, SsspMultiStats]:
+    """SSSP from up to 32 sources of g in one launch (g5_sssp_multi_run):
+    dist[s] / pred[s] equal oned_graph_sssp_run's outputs from sources[s]
+    bit for bit (float32 distances, -1.0 / -1 where unreached).  Runs on the
+    graph's renumbered SSSP copy when it has one (sources and outputs stay
+    in the caller's numbering).  delta: the shared bucket width (0 = 0.1;
+    results never depend on it).  `work`: sssp_multi_workspace(g), else one
+    is allocated; `dist` / `pred`: [len(sources), N] outputs to reuse."""
+    src = [int(x) for x in sources]
+    k, n = len(src), g.nglobalverts
+    if work is None:
+        work = sssp_multi_workspace(g)
+    if dist is None:
+        dist = torch.empty((k, n), dtype=torch.float32, device=g.device)
+    if with_pred and pred is None:
+        pred = torch.empty((k, n), dtype=torch.int64, device=g.device)
+    rs, col, w, _, _, perm, inv = _sssp_csr(g)
+    h_src = (C.c_uint64 * max(k, 1))(*src)
+    st = SsspMultiStats()
+    _check(lib.g5_sssp_multi_run(_ptr(rs), _ptr(col), _ptr(w), n, _ptr(perm), _ptr(inv), h_src, k, _ptr(dist),
+                                 _ptr(pred) if with_pred else None, _ptr(work), work.numel(), delta, blocks,
+                                 C.byref(st), _stream(stream)))
+    return dist, (pred if with_pred else None), st
 
 
 def oned_graph_sssp_reset(sssp: SsspState, stream=None) -> None:

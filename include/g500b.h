@@ -609,6 +609,34 @@ int g5_msbfs_last_trace(const void *d_work, uint64_t work_bytes, int max_levels,
                         uint64_t *frontier_vertices, uint64_t *frontier_edges, double *level_ms, int32_t *nlevels,
                         void *stream);
 
+/* ------------------------------------------------------ batched SSSP --- */
+
+/* SSSP from up to 32 sources of one graph in one persistent launch (the
+ * reference runs one source at a time, src/traversal.cu:638-711): one warp
+ * lane per source, each vertex's 32 packed (distance, parent) words side by
+ * side, so an edge's column entry and weight are read once for every
+ * source; label-correcting rounds over the vertices whose words dropped, in
+ * buckets of width delta shared by the sources (0 = 0.1), as delta-stepping
+ * takes them.
+ * Distances and parents equal g5_sssp_run's for each source bit for bit.
+ * Any row order of the CSR will do (the renumbered SSSP copy: pass its
+ * perm / inv, sources and outputs stay in the caller's numbering).
+ * d_dist / d_pred (optional, nsources x nverts, source-major: entry
+ * s * nverts + v) receive -1.0f / -1 where unreached.  Synchronises when
+ * h_stats is given.  Scratch: g5_sssp_multi_workspace_size (about 276 bytes
+ * per vertex). */
+typedef struct g5_sssp_multi_stats {
+    int32_t rounds;            /* relaxation rounds                                   */
+    uint32_t error_flags;      /* device-side error bits, 0 when none                 */
+    uint64_t frontier_entries; /* queued vertices over all rounds                     */
+    uint64_t entries_scanned;  /* CSR entries relaxed (each for every changed source) */
+} g5_sssp_multi_stats;
+int g5_sssp_multi_workspace_size(uint64_t nverts, uint64_t *bytes);
+int g5_sssp_multi_run(const uint64_t *d_rowstarts, const int32_t *d_col, const float *d_w, uint64_t nverts,
+                      const uint32_t *d_perm, const uint32_t *d_inv, const uint64_t *h_sources, uint32_t nsources,
+                      float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes, float delta,
+                      int32_t blocks, g5_sssp_multi_stats *h_stats, void *stream);
+
 /* ------------------------------------------------------------- grids ----- */
 /* Grid (blocks) sized for a graph of nverts vertices -- what g5_bfs_* and
  * g5_sssp_* launch with params.blocks = 0 (g5_msbfs_run then takes every
