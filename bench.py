@@ -501,6 +501,9 @@ def run_ours(args):
         if world == 1 and not args.no_batched:
             line["batched"] = run_batched(G, dev, args.batched_scale, args.edgefactor, args.batched_roots)
             torch.cuda.empty_cache()
+        if world == 1 and not args.no_batched:
+            line["sssp_batched"] = run_sssp_batched(G, dev, args.sssp_batched_scale, args.edgefactor)
+            torch.cuda.empty_cache()
         if world == 1 and not args.no_packed:
             line["packed"] = run_packed(G, dev, args.packed_graphs, args.packed_min_scale, args.packed_max_scale,
                                         args.edgefactor)
@@ -583,6 +586,59 @@ def run_batched(G, dev, scale, ef, nroots, reps=3):
             "autotuned": {k: tuned[k] for k in ("alpha", "check_frontier", "blocks", "candidates")},
             "timing": "device events, min of 3 after one warm-up; plain = single-root traverse with depth, "
                       "reset untimed"}
+
+
+def run_sssp_batched(G, dev, scale, ef, nsources=32, reps=3):
+    """Batched SSSP: `nsources` Graph500 roots of the SCALE-`scale` Kronecker
+    graph in one g5_sssp_multi_run, against the same sources one at a time
+    with the single-source search (reset untimed).  Every source's distance
+    and parent arrays are compared bit for bit; aggregate GTEPS = sum of the
+    sources' TEPS edge counts / device time."""
+    import torch
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    t0 = time.time()
+    g = G.oned_graph_from_kronecker(G.make_mrg_seed(2, 3), scale, ef << scale, device=dev)
+    roots = G.generate_bfs_roots(g, 2, 3, nsources)
+    work = G.sssp_multi_workspace(g)
+    G.oned_graph_sssp_multi(g, roots, work=work)  # warm-up
+    times = []
+    for _ in range(reps):
+        a, b = ev(), ev()
+        a.record()
+        dist, pred, st = G.oned_graph_sssp_multi(g, roots, work=work)
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    ss = G.SsspState(g)
+    vw = G._val_work(g)
+    plain_ms, nedge, checked = 0.0, [], 0
+    for i, r in enumerate(roots):
+        G.oned_graph_sssp_reset(ss)
+        torch.cuda.synchronize()
+        a, b = ev(), ev()
+        a.record()
+        G.oned_graph_sssp_traverse(g, ss, int(r))
+        b.record()
+        torch.cuda.synchronize()
+        G.sssp_status(ss)
+        plain_ms += a.elapsed_time(b)
+        assert torch.equal(dist[i].view(torch.int32), ss.dist.view(torch.int32)) and torch.equal(pred[i], ss.pred), \
+            f"batched SSSP of source {r} differs from the single-source search"
+        checked += 1
+        nedge.append(G.edge_count(g, ss.pred, vw))
+    assert G.sssp_validate(g, int(roots[0]), dist[0], pred[0], vw) == 0
+    E = float(sum(nedge))
+    best = min(times)
+    return {"workload": f"batched sssp scale{scale} ef{ef}, {len(roots)} sources in one launch",
+            "value": round(E / best / 1e6, 2), "unit": "GTEPS (aggregate over the batch)",
+            "ms_per_batch": round(best, 3), "plain_ms_total": round(plain_ms, 3),
+            "plain_gteps": round(E / plain_ms / 1e6, 2), "speedup_vs_plain": round(plain_ms / best, 2),
+            "sources_checked_identical": checked, "rounds": st.rounds,
+            "entries_scanned_per_entry": round(st.entries_scanned / max(1, g.nlocaledges), 2),
+            "setup_s": round(time.time() - t0, 2),
+            "timing": "device events, min of 3 after one warm-up; plain = single-source traverse, reset untimed",
+            "note": "a win up to about 2^20 vertices (SCALE 14: 10-13x, 18: 3.6-3.9x, 20: 1.5-1.7x); from SCALE 22 "
+                    "the single-source delta-stepping search is faster (0.7x at 22, 0.27x at 26)"}
 
 
 def run_packed(G, dev, ngraphs, smin, smax, ef, reps=3):
@@ -763,6 +819,8 @@ def run_batched_only(args):
     out = {}
     if args.only_batched in ("msbfs", "all"):
         out["batched"] = run_batched(G, dev, args.batched_scale, args.edgefactor, args.batched_roots)
+    if args.only_batched in ("sssp", "all"):
+        out["sssp_batched"] = run_sssp_batched(G, dev, args.sssp_batched_scale, args.edgefactor)
     if args.only_batched in ("packed", "all"):
         out["packed"] = run_packed(G, dev, args.packed_graphs, args.packed_min_scale, args.packed_max_scale,
                                    args.edgefactor)
@@ -879,6 +937,8 @@ def headline(line):
         h["ours_over_reference_gpu"] = rg["ours_over_reference"]
     if "batched" in line:
         h["batched_256_speedup"] = line["batched"]["speedup_vs_plain"]
+    if "sssp_batched" in line:
+        h["sssp_batched_32_speedup"] = line["sssp_batched"]["speedup_vs_plain"]
     if "packed" in line:
         h["packed_speedup"] = line["packed"]["speedup_vs_plain"]
     if "serving" in line:
@@ -956,9 +1016,11 @@ def main():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own GPU build (oracle/_ref/ref_bench) on the same roots")
     ap.add_argument("--batched-scale", type=int, default=24, help="SCALE of the batched (multi-source) BFS graph")
+    ap.add_argument("--sssp-batched-scale", type=int, default=18,
+                    help="SCALE of the batched SSSP graph (32 sources in one launch)")
     ap.add_argument("--batched-roots", type=int, default=256)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched BFS measurement")
-    ap.add_argument("--only-batched", nargs="?", const="msbfs", choices=["msbfs", "packed", "serve", "all"],
+    ap.add_argument("--only-batched", nargs="?", const="msbfs", choices=["msbfs", "sssp", "packed", "serve", "all"],
                     help="run only the batched measurements (multi-source BFS, packed graphs, serving or all)")
     ap.add_argument("--serve-queries", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate, queries per second")
