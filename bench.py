@@ -799,11 +799,16 @@ def run_kernels_once(scale, ef):
     G.oned_graph_bfs_run(g, bfs, r)
     d = G.bfs_compute_dist_from_pred(g, bfs, r)
     ne = G.edge_count(g, bfs.pred, vw)  # edge_count_kernel
+    rec = G.oned_graph_bfs_export(g, bfs)  # bfs_export_kernel (a grid search's result: a scan of the parents)
+    assert len(rec) == G.bfs_stats(bfs).reached
     err = G.bfs_validate(g, r, bfs.pred, d, vw)  # bfs_val_edge_kernel
     s = G.SsspState(g)
     G.oned_graph_sssp_run(g, s, r)
     G.sssp_status(s)
     serr = G.sssp_validate(g, r, s.dist, s.pred, vw)  # sssp_val_edge_kernel
+    roots32 = [x for x in G.generate_bfs_roots(g, 2, 3, 64) if g.in_main_component(x)][:32]
+    md, _, _ = G.oned_graph_sssp_multi(g, roots32, with_pred=False)  # mss_persistent_kernel
+    assert torch.equal(md[roots32.index(r)].view(torch.int32), s.dist.view(torch.int32)) if r in roots32 else True
     torch.cuda.synchronize()
     print(json.dumps({"scale": scale, "root": int(r), "nedge": int(ne), "bfs_errors": int(err),
                       "sssp_errors": int(serr)}), flush=True)
