@@ -777,7 +777,8 @@ def run_serving(G, dev, nqueries, rate, ef=16, slots=8, low_rate=250.0, raise_er
             "makespan_s": ours["makespan_s"], "by_kind": kinds,
             "plain_one_at_a_time": plain, "qps_vs_plain": round(ours["qps"] / plain["qps"], 2),
             "bfs_batches": st.bfs_batches, "bfs_queries_batched": st.bfs_batched_queries,
-            "sssp_launches": st.sssp_launches, "max_concurrent_launches": st.max_inflight,
+            "sssp_launches": st.sssp_launches, "sssp_batches": st.sssp_batches,
+            "sssp_queries_batched": st.sssp_batched_queries, "max_concurrent_launches": st.max_inflight,
             "device_errors": st.device_errors, "errors": st.errors,
             "slots": slots, "low_load": low, "build_s": round(build_s, 2),
             "timing": "host clock: latency from a query's arrival time to the host seeing its launch's "

@@ -109,6 +109,8 @@ def _load() -> C.CDLL:
         "g5_sssp_workspace_size": ([u64, p], C.c_int),
         "g5_sssp_run": ([p, p, p, p, f32, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_sssp_multi_workspace_size": ([u64, p], C.c_int),
+        "g5_sssp_multi_last_stats": ([p, u64, p, p], C.c_int),
+        "g5_sssp_multi_grid": ([u64, p, p], C.c_int),
         "g5_sssp_multi_run": ([p, p, p, u64, p, p, p, C.c_uint32, p, p, p, u64, C.c_float, C.c_int32, p, p],
                               C.c_int),
         "g5_sssp_last_status": ([p, u64, p, p, p], C.c_int),
@@ -204,7 +206,7 @@ def _workspace(nbytes: int, device) -> torch.Tensor:
 
 def search_grid(kind: str, nverts: int) -> tuple[int, int]:
     """(blocks, max co-resident blocks) of the persistent kernel of `kind`
-    ("bfs", "sssp", "msbfs") for a graph of nverts vertices."""
+    ("bfs", "sssp", "msbfs", "sssp_multi") for a graph of nverts vertices."""
     b, m = C.c_int32(), C.c_int32()
     _check(getattr(lib, f"g5_{kind}_grid")(nverts, C.byref(b), C.byref(m)))
     return b.value, m.value
@@ -1133,16 +1135,36 @@ def sssp_multi_workspace(g: OnedGraph) -> torch.Tensor:
     return _workspace(nb.value, g.device)
 
 
+class SsspMultiState:
+    """A batched-SSSP workspace of one graph with its distance outputs for
+    up to 32 sources (dist[s] for source s of the last run)."""
+
+    def __init__(self, g: OnedGraph, max_sources: int = 32):
+        self.work = sssp_multi_workspace(g)
+        self.dist = torch.empty((max_sources, g.nglobalverts), dtype=torch.float32, device=g.device)
+        self.max_sources = max_sources
+
+
+def sssp_multi_status(state: SsspMultiState, stream=None) -> SsspMultiStats:
+    """Statistics of the state's last batched run; raises on a device error
+    (synchronises the stream)."""
+    st = SsspMultiStats()
+    _check(lib.g5_sssp_multi_last_stats(_ptr(state.work), state.work.numel(), C.byref(st), _stream(stream)))
+    return st
+
+
 def oned_graph_sssp_multi(g: OnedGraph, sources, work: torch.Tensor | None = None, with_pred: bool = True,
                           blocks: int = 0, stream=None, delta: float = 0.0, dist: torch.Tensor | None = None,
-                          pred: torch.Tensor | None = None) -> tuple[torch.Tensor, torch.Tensor | None, SsspMultiStats]:
+                          pred: torch.Tensor | None = None,
+                          sync: bool = True) -> tuple[torch.Tensor, torch.Tensor | None, SsspMultiStats | None]:
     """SSSP from up to 32 sources of g in one launch (g5_sssp_multi_run):
     dist[s] / pred[s] equal oned_graph_sssp_run's outputs from sources[s]
     bit for bit (float32 distances, -1.0 / -1 where unreached).  Runs on the
     graph's renumbered SSSP copy when it has one (sources and outputs stay
     in the caller's numbering).  delta: the shared bucket width (0 = 0.1;
     results never depend on it).  `work`: sssp_multi_workspace(g), else one
-    is allocated; `dist` / `pred`: [len(sources), N] outputs to reuse."""
+    is allocated; `dist` / `pred`: [len(sources), N] outputs to reuse.
+    sync=False: no wait (statistics None; sssp_multi_status reads them)."""
     src = [int(x) for x in sources]
     k, n = len(src), g.nglobalverts
     if work is None:
@@ -1153,10 +1175,10 @@ def oned_graph_sssp_multi(g: OnedGraph, sources, work: torch.Tensor | None = Non
         pred = torch.empty((k, n), dtype=torch.int64, device=g.device)
     rs, col, w, _, _, perm, inv = _sssp_csr(g)
     h_src = (C.c_uint64 * max(k, 1))(*src)
-    st = SsspMultiStats()
+    st = SsspMultiStats() if sync else None
     _check(lib.g5_sssp_multi_run(_ptr(rs), _ptr(col), _ptr(w), n, _ptr(perm), _ptr(inv), h_src, k, _ptr(dist),
                                  _ptr(pred) if with_pred else None, _ptr(work), work.numel(), delta, blocks,
-                                 C.byref(st), _stream(stream)))
+                                 C.byref(st) if sync else None, _stream(stream)))
     return dist, (pred if with_pred else None), st
 
 

@@ -428,3 +428,27 @@ extern "C" int g5_sssp_multi_run(const uint64_t *d_rowstarts, const int32_t *d_c
     G5_CUDA_TRY(cudaStreamSynchronize(st));
     return deverr_to_status(h_stats->error_flags, "g5_sssp_multi_run");
 }
+
+extern "C" int g5_sssp_multi_grid(uint64_t nverts, int32_t *blocks, int32_t *max_blocks) {
+    clear_error();
+    G5_CHECK_ARG(blocks && max_blocks, "g5_sssp_multi_grid: NULL argument");
+    int mb = 0;
+    int rc = mss_max_blocks(&mb);
+    if (rc) return rc;
+    *max_blocks = mb;
+    *blocks = (int)std::min<uint64_t>(mb, std::max<uint64_t>(1, nverts / 2048));
+    return G5_OK;
+}
+
+extern "C" int g5_sssp_multi_last_stats(const void *d_work, uint64_t work_bytes, g5_sssp_multi_stats *stats,
+                                        void *stream) {
+    clear_error();
+    G5_CHECK_ARG(d_work && stats, "g5_sssp_multi_last_stats: NULL argument");
+    G5_CHECK_ARG(work_bytes >= sizeof(MssCtl), "g5_sssp_multi_last_stats: workspace too small");
+    const MssCtl *ctl = (const MssCtl *)d_work;  // the workspace starts with the control block
+    cudaStream_t st = (cudaStream_t)stream;
+    G5_CUDA_TRY(cudaMemcpyAsync(stats, &ctl->res, sizeof(g5_sssp_multi_stats), cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaMemcpyAsync(&stats->error_flags, &ctl->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    G5_CUDA_TRY(cudaStreamSynchronize(st));
+    return deverr_to_status(stats->error_flags, "g5_sssp_multi_run");
+}

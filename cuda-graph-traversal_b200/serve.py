@@ -13,8 +13,13 @@ free it launches the oldest waiting work:
   time by the plain search on a pooled BFS workspace, which costs less than
   a batched search below about 8 roots (SCALE 16-24: a batch of one root
   takes 4-6x a plain search, a batch of 16 about 1.1x two plain searches);
-* an SSSP query runs on its own (distances differ per source) on a pooled
-  SSSP workspace of that graph.
+* pending SSSP queries of a graph of at most `sssp_batch_max_vertices`
+  (2^20) vertices, when at least `sssp_batch_min` (2) wait, become one
+  batched search of up to 32 sources (g5_sssp_multi_run) on that graph's
+  batched-SSSP workspace, which answers 32 sources 1.5-13x faster than 32
+  single searches on graphs of 2^20 down to 2^14 vertices; otherwise (and on
+  larger graphs, where the single search is the faster one) an SSSP query
+  runs on its own on a pooled SSSP workspace of that graph.
 
 Every search is a persistent cooperative kernel whose grid is sized to its
 graph (g5_*_grid); launches run concurrently only while the sum of their
@@ -44,10 +49,13 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from . import (MSBFS_MAX_ROOTS, BfsParams, BfsState, G5Error, MsBfsParams, MsBfsState, OnedGraph, SsspState,
-               bfs_stats, bfs_workspace_bytes, msbfs_depths_u8, msbfs_run, msbfs_stats, oned_graph_bfs_reset,
-               oned_graph_bfs_run, oned_graph_bfs_traverse, oned_graph_sssp_reset, oned_graph_sssp_traverse,
-               search_grid, sssp_status, sssp_workspace_bytes)
+from . import (MSBFS_MAX_ROOTS, BfsParams, BfsState, G5Error, MsBfsParams, MsBfsState, OnedGraph,
+               SsspMultiState, SsspState, bfs_stats, bfs_workspace_bytes, msbfs_depths_u8, msbfs_run, msbfs_stats,
+               oned_graph_bfs_reset, oned_graph_bfs_run, oned_graph_bfs_traverse, oned_graph_sssp_multi,
+               oned_graph_sssp_reset, oned_graph_sssp_traverse, search_grid, sssp_multi_status, sssp_status,
+               sssp_workspace_bytes)
+
+SSSP_BATCH_MAX = 32  # sources of one batched SSSP launch
 
 
 @dataclass
@@ -95,6 +103,8 @@ class ServerStats:
     bfs_batched_queries: int = 0
     bfs_single: int = 0
     sssp_launches: int = 0
+    sssp_batches: int = 0
+    sssp_batched_queries: int = 0
     max_inflight: int = 0
     workspaces: dict = field(default_factory=dict)
     refused_for_memory: int = 0
@@ -105,7 +115,8 @@ class ServerStats:
 class GraphServer:
     def __init__(self, graphs: list[OnedGraph], slots: int = 4, hbm_reserve: int = 8 << 30,
                  max_batch: int = MSBFS_MAX_ROOTS, keep_results: bool = False, max_sssp_per_graph: int = 4,
-                 bfs_batch_min: int = 8, raise_errors: bool = True):
+                 bfs_batch_min: int = 8, raise_errors: bool = True, sssp_batch_min: int = 2,
+                 sssp_batch_max_vertices: int = 1 << 20):
         if not graphs:
             raise ValueError("GraphServer needs at least one graph")
         self.graphs = graphs
@@ -125,9 +136,14 @@ class GraphServer:
         self.ms_busy = [False] * len(graphs)
         self.sssp_free: list[list[SsspState]] = [[] for _ in graphs]
         self.sssp_count = [0] * len(graphs)
+        self.sssp_batch_min = max(2, int(sssp_batch_min))
+        self.sssp_batch_max_vertices = int(sssp_batch_max_vertices)
+        self.mss: list[SsspMultiState | None] = [None] * len(graphs)
+        self.mss_busy = [False] * len(graphs)
         self.inflight: list[_Launch] = []
-        self.grid = {k: [search_grid(k, g.nglobalverts)[0] for g in graphs] for k in ("bfs", "msbfs", "sssp")}
-        self.max_blocks = min(search_grid(k, 1)[1] for k in ("bfs", "msbfs", "sssp"))
+        kinds = ("bfs", "msbfs", "sssp", "sssp_multi")
+        self.grid = {k: [search_grid(k, g.nglobalverts)[0] for g in graphs] for k in kinds}
+        self.max_blocks = min(search_grid(k, 1)[1] for k in kinds)
         self.blocks_in_use = 0
         self.stats = ServerStats()
         self.clock0 = time.perf_counter()
@@ -149,6 +165,19 @@ class GraphServer:
             self.ms[gi] = MsBfsState(g)
             self.stats.workspaces[f"msbfs{gi}"] = self.ms[gi].work.numel()
         return self.ms[gi]
+
+    def _mss_state(self, gi: int) -> SsspMultiState | None:
+        """The graph's batched-SSSP workspace (graphs up to
+        sssp_batch_max_vertices only)."""
+        g = self.graphs[gi]
+        if g.nglobalverts > self.sssp_batch_max_vertices:
+            return None
+        if self.mss[gi] is None:
+            if not self._fits(404 * g.nglobalverts):  # workspace + 32 distance rows
+                return None
+            self.mss[gi] = SsspMultiState(g, SSSP_BATCH_MAX)
+            self.stats.workspaces[f"sssp_multi{gi}"] = self.mss[gi].work.numel()
+        return self.mss[gi]
 
     def _bfs_state(self, gi: int) -> BfsState | None:
         if self.bfs_free[gi]:
@@ -187,6 +216,7 @@ class GraphServer:
         that no query waits on a first-use allocation."""
         for gi in range(len(self.graphs)):
             self._ms_state(gi)
+            self._mss_state(gi)
         for _ in range(self.max_sssp):
             grew = False
             for gi in range(len(self.graphs)):
@@ -236,7 +266,9 @@ class GraphServer:
         share = max(1, self.max_blocks // max(1, k))
         for _, kind, gi in cands:
             single = kind == "bfs" and len(self.pending["bfs"][gi]) < self.bfs_batch_min
-            gk = ("bfs" if single else "msbfs") if kind == "bfs" else "sssp"
+            sbatch = (kind == "sssp" and len(self.pending["sssp"][gi]) >= self.sssp_batch_min and not self.mss_busy[gi]
+                      and self._mss_state(gi) is not None)
+            gk = ("bfs" if single else "msbfs") if kind == "bfs" else ("sssp_multi" if sbatch else "sssp")
             blocks = min(self.grid[gk][gi], share)
             if self.blocks_in_use + blocks > self.max_blocks:
                 # Oldest first: younger work may not take the SMs this
@@ -274,6 +306,21 @@ class GraphServer:
                 self.inflight.append(_Launch(ev, qs, "bfs", gi, slot, ms, blocks, out))
                 self.stats.bfs_batches += 1
                 self.stats.bfs_batched_queries += len(qs)
+            elif sbatch:
+                ms = self.mss[gi]
+                slot = self.free_slots.pop()
+                d = self.pending["sssp"][gi]
+                qs = [d.popleft() for _ in range(min(len(d), SSSP_BATCH_MAX))]
+                s = self.streams[slot]
+                with torch.cuda.stream(s):
+                    oned_graph_sssp_multi(g, [q.root for q in qs], work=ms.work, with_pred=False, blocks=blocks,
+                                          stream=s, dist=ms.dist[:len(qs)], sync=False)
+                    ev = torch.cuda.Event()
+                    ev.record(s)
+                self.mss_busy[gi] = True
+                self.inflight.append(_Launch(ev, qs, "sssp_b", gi, slot, ms, blocks))
+                self.stats.sssp_batches += 1
+                self.stats.sssp_batched_queries += len(qs)
             else:
                 st = self._sssp_state(gi)
                 if st is None:
@@ -331,6 +378,12 @@ class GraphServer:
                     v[v == 255] = -1
                 out.append(Result(q.qid, q.kind, q.graph, q.root, q.arrival, t, len(L.queries), v, ok))
             self.ms_busy[L.graph] = False
+        elif L.kind == "sssp_b":
+            ok = self._checked(sssp_multi_status, L.resource, self.streams[L.slot], L)
+            for i, q in enumerate(L.queries):
+                v = L.resource.dist[i].clone() if self.keep and ok else None
+                out.append(Result(q.qid, q.kind, q.graph, q.root, q.arrival, t, len(L.queries), v, ok))
+            self.mss_busy[L.graph] = False
         else:
             ok = self._checked(sssp_status, L.resource, self.streams[L.slot], L)
             q = L.queries[0]

@@ -636,6 +636,11 @@ int g5_sssp_multi_run(const uint64_t *d_rowstarts, const int32_t *d_col, const f
                       const uint32_t *d_perm, const uint32_t *d_inv, const uint64_t *h_sources, uint32_t nsources,
                       float *d_dist, int64_t *d_pred, void *d_work, uint64_t work_bytes, float delta,
                       int32_t blocks, g5_sssp_multi_stats *h_stats, void *stream);
+/* Statistics and status of the last g5_sssp_multi_run on this workspace
+ * (synchronises `stream`); its grid: blocks for a graph of nverts vertices
+ * and the largest co-resident grid. */
+int g5_sssp_multi_last_stats(const void *d_work, uint64_t work_bytes, g5_sssp_multi_stats *stats, void *stream);
+int g5_sssp_multi_grid(uint64_t nverts, int32_t *blocks, int32_t *max_blocks);
 
 /* ------------------------------------------------------------- grids ----- */
 /* Grid (blocks) sized for a graph of nverts vertices -- what g5_bfs_* and

@@ -24,6 +24,7 @@ def test_batched_results_equal_alone(cgt, graphs):
     res = srv.run_trace(trace, deadline=120.0)
     assert sorted(r.qid for r in res) == list(range(300))
     assert srv.stats.bfs_batches < sum(1 for q in trace if q.kind == "bfs")  # queries were batched
+    assert srv.stats.sssp_batches > 0 and srv.stats.sssp_batched_queries > srv.stats.sssp_batches  # SSSP too
     assert max(r.batch for r in res) > 1
     alone = {r.qid: r for r in serve.serve_plain(graphs, trace, keep_results=True)}
     for r in res:
