@@ -169,30 +169,119 @@ __device__ __forceinline__ void block_add(unsigned long long *dst, unsigned long
     if (lane_id() == 0 && v) atomicAdd(dst, v);
 }
 
+// The TEPS edge count walks the CSR as warp_walk does, with two changes for
+// its one cheap test per entry: the window also holds each row's reached
+// flag (pred != -1, loaded with the row starts, coalesced), and a lane keeps
+// its current row, its flag and where the next row starts in registers, so
+// an entry costs a compare and an add unless a row ends at it.
 __global__ void __launch_bounds__(VAL_THREADS) edge_count_kernel(const uint64_t *__restrict__ rowptr,
                                                                  const int *__restrict__ col, uint64_t n,
                                                                  const int64_t *__restrict__ pred,
                                                                  const unsigned *__restrict__ trow,
                                                                  const unsigned long long *__restrict__ table,
                                                                  unsigned long long *__restrict__ out) {
+    constexpr int ITEMS = COUNT_ITEMS;
+    __shared__ int s_win[VAL_THREADS / 32][VAL_WIN];
+    __shared__ unsigned char s_reach[VAL_THREADS / 32][VAL_WIN];
     const uint64_t E = rowptr[n];
     const bool tab = *table != 0;
+    int *wrp = s_win[threadIdx.x >> 5];
+    unsigned char *wrc = s_reach[threadIdx.x >> 5];
+    const unsigned lane = lane_id();
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long cnt = 0;
-    warp_walk<COUNT_ITEMS>(rowptr, col, n, E, trow, tab,
-              [&](const unsigned *u, uint64_t, unsigned ne, const int *c) {
-                  // rows change rarely within 16 entries: one pred load per row
-                  unsigned ur = ~0u;
-                  bool reached = false;
+    for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t * VAL_WTILE < E; t += nwarps) {
+        uint64_t lo = 0, hi = n - 1;
+        if (tab) {
+            lo = __ldg(&trow[t]);
+            hi = __ldg(&trow[t + 1]);
+        }
+        const uint64_t t0 = t * VAL_WTILE;
+        const bool win = tab && hi - lo < VAL_WIN - 1;
+        __syncwarp();  // the last tile's window is read
+        if (win) {
+            for (unsigned i = lane; i < VAL_WIN; i += 32) {
+                int rp = 1 << 30;
+                unsigned char rc = 0;
+                if (i <= hi - lo + 1 && lo + i <= n) {
+                    const uint64_t x = __ldg(&rowptr[lo + i]);
+                    rp = x < t0 ? -1 : x - t0 > (1u << 30) ? 1 << 30 : (int)(x - t0);
+                    rc = lo + i < n && __ldg(&pred[lo + i]) != -1;
+                }
+                wrp[i] = rp;
+                wrc[i] = rc;
+            }
+        }
+        __syncwarp();
+#pragma unroll 1
+        for (int step = 0; step < VAL_WTILE / (32 * ITEMS); ++step) {
+            const uint64_t eb = t0 + (uint64_t)step * 32 * ITEMS + (uint64_t)lane * ITEMS;
+            const uint64_t ee = eb < E ? min(eb + (uint64_t)ITEMS, E) : eb;
+            const unsigned ne = (unsigned)(ee - eb);
+            if (!ne) continue;
+            int c[ITEMS];
+            if (ne == ITEMS && ((uintptr_t)(col + eb) & 15) == 0) {
+                const int4 *p = reinterpret_cast<const int4 *>(col + eb);
 #pragma unroll
-                  for (int k = 0; k < COUNT_ITEMS; ++k) {
-                      if (k >= ne) break;
-                      if (u[k] != ur) {
-                          ur = u[k];
-                          reached = __ldg(&pred[ur]) != -1;
-                      }
-                      if (reached && (unsigned)c[k] <= u[k]) ++cnt;
-                  }
-              });
+                for (int k = 0; k < ITEMS / 4; ++k) {
+                    const int4 q = __ldg(p + k);
+                    c[4 * k] = q.x;
+                    c[4 * k + 1] = q.y;
+                    c[4 * k + 2] = q.z;
+                    c[4 * k + 3] = q.w;
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < ITEMS; ++k) c[k] = k < ne ? __ldg(&col[eb + k]) : 0;
+            }
+            unsigned local = 0;
+            if (win) {
+                const int el = (int)(eb - t0);
+                unsigned j = 0;  // largest window row starting at or before eb
+#pragma unroll
+                for (unsigned s2 = VAL_WIN / 2; s2 >= 1; s2 >>= 1)
+                    if (wrp[j + s2] <= el) j += s2;
+                int d = (j + 1 < VAL_WIN ? wrp[j + 1] : 1 << 30) - el;
+                unsigned u = (unsigned)lo + j;
+                bool reached = wrc[j];
+#pragma unroll
+                for (int k = 0; k < ITEMS; ++k) {
+                    if (k < (int)ne) {
+                        if (k >= d) {  // a later row starts at or before this entry (past empty rows too)
+                            do {
+                                ++j;
+                                d = (j + 1 < VAL_WIN ? wrp[j + 1] : 1 << 30) - el;
+                            } while (k >= d);
+                            u = (unsigned)lo + j;
+                            reached = wrc[j];
+                        }
+                        local += reached && (unsigned)c[k] <= u;
+                    }
+                }
+            } else {
+                uint64_t r = row_of(rowptr, lo, hi, eb);
+                uint64_t next = __ldg(&rowptr[r + 1]);
+                bool reached = __ldg(&pred[r]) != -1;
+#pragma unroll
+                for (int k = 0; k < ITEMS; ++k) {
+                    const uint64_t e = eb + k;
+                    if (k < (int)ne) {
+                        if (e >= next) {  // into a later row: the next one, or past empty rows a search
+                            ++r;
+                            next = __ldg(&rowptr[r + 1]);
+                            if (next <= e) {
+                                r = row_of(rowptr, r + 1, hi, e);
+                                next = __ldg(&rowptr[r + 1]);
+                            }
+                            reached = __ldg(&pred[r]) != -1;
+                        }
+                        local += reached && (unsigned)c[k] <= (unsigned)r;
+                    }
+                }
+            }
+            cnt += local;
+        }
+    }
     block_add(out, cnt);
 }
 
