@@ -683,41 +683,69 @@ __global__ void csr_split_light_kernel(const uint64_t *__restrict__ rowstarts, c
                                        unsigned *__restrict__ nbig) {
     const unsigned lane = lane_id();
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
-        const uint64_t rb = rowstarts[v], re = rowstarts[v + 1];
-        if (re - rb > SORT_SMEM_KEYS) {
-            if (lane == 0) big[atomicAdd(nbig, 1u)] = (unsigned)v;
-            continue;
-        }
-        unsigned nt = 0, nl = 0;
-        for (uint64_t i = rb + lane; i < re; i += 32) {
-            const int k = light_class(w[i], light, tiny);
-            nt += k == 0;
-            nl += k <= 1;
-        }
-        nt = warp_sum(nt);
-        nl = warp_sum(nl);
-        uint64_t o3[3] = {rb, rb + nt, rb + nl};
-        for (uint64_t i0 = rb; i0 < re; i0 += 32) {
-            const uint64_t i = i0 + lane;
-            const bool has = i < re;
-            const float x = has ? w[i] : 0.0f;
-            const int k = has ? light_class(x, light, tiny) : 3;
-            const unsigned lt = lanemask_lt();
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                const unsigned m = __ballot_sync(FULL, k == q);
-                if (k == q) {
-                    const uint64_t o = o3[q] + __popc(m & lt);
-                    scol[o] = col[i];
-                    sw[o] = x;
-                }
-                o3[q] += __popc(m);
+    for (uint64_t v0 = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; v0 < n; v0 += nw * 32) {
+        // 32 rows per warp step (coalesced row starts): a row of up to 32
+        // entries is split by its own lane (most rows of a Kronecker graph
+        // are short: a warp each left most lanes idle), longer ones by the
+        // whole warp, rows beyond SORT_SMEM_KEYS listed for the tiled kernels.
+        const uint64_t v = v0 + lane;
+        const uint64_t rb = v < n ? rowstarts[v] : 0, re = v < n ? rowstarts[v + 1] : 0;
+        const uint64_t len = re - rb;
+        if (len > SORT_SMEM_KEYS) big[atomicAdd(nbig, 1u)] = (unsigned)v;
+        if (v < n && len <= 32) {
+            unsigned nt = 0, nl = 0;
+            for (uint64_t i = rb; i < re; ++i) {
+                const int k = light_class(w[i], light, tiny);
+                nt += k == 0;
+                nl += k <= 1;
             }
-        }
-        if (lane == 0) {
+            uint64_t o0 = rb, o1 = rb + nt, o2 = rb + nl;
+            for (uint64_t i = rb; i < re; ++i) {
+                const float x = w[i];
+                const int k = light_class(x, light, tiny);
+                const uint64_t o = k == 0 ? o0++ : k == 1 ? o1++ : o2++;
+                scol[o] = col[i];
+                sw[o] = x;
+            }
             ld[v] = nl;
             td[v] = nt;
+        }
+        unsigned todo = __ballot_sync(FULL, len > 32 && len <= SORT_SMEM_KEYS);
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint64_t r = v0 + l;
+            const uint64_t b = __shfl_sync(FULL, rb, l), e = __shfl_sync(FULL, re, l);
+            unsigned nt = 0, nl = 0;
+            for (uint64_t i = b + lane; i < e; i += 32) {
+                const int k = light_class(w[i], light, tiny);
+                nt += k == 0;
+                nl += k <= 1;
+            }
+            nt = warp_sum(nt);
+            nl = warp_sum(nl);
+            uint64_t o3[3] = {b, b + nt, b + nl};
+            for (uint64_t i0 = b; i0 < e; i0 += 32) {
+                const uint64_t i = i0 + lane;
+                const bool has = i < e;
+                const float x = has ? w[i] : 0.0f;
+                const int k = has ? light_class(x, light, tiny) : 3;
+                const unsigned lt = lanemask_lt();
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    const unsigned m = __ballot_sync(FULL, k == q);
+                    if (k == q) {
+                        const uint64_t o = o3[q] + __popc(m & lt);
+                        scol[o] = col[i];
+                        sw[o] = x;
+                    }
+                    o3[q] += __popc(m);
+                }
+            }
+            if (lane == 0) {
+                ld[r] = nl;
+                td[r] = nt;
+            }
         }
     }
 }
