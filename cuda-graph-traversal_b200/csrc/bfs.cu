@@ -1220,10 +1220,13 @@ __global__ void __launch_bounds__(256) bfs_export_kernel(const int64_t *__restri
     if (touch->small) {
         // The touched list: block 0 alone (it is short), the others leave.
         if (blockIdx.x != 0) return;
-        const uint64_t cnt = touch->count;
+        // (clamped and checked: on a workspace no search has written yet the
+        // record is whatever the memory held)
+        const uint64_t cnt = min((uint64_t)touch->count, n);
         for (uint64_t i = threadIdx.x; i < cnt && i < cap; i += blockDim.x) {
             const unsigned v = tlist[i];
-            put_reached(out, i, v, depth ? depth[v] : -1, pred[v]);
+            if (v < n) put_reached(out, i, v, depth ? depth[v] : -1, pred[v]);
+            else put_reached(out, i, v, -1, -1);
         }
         __threadfence_system();
         __syncthreads();
