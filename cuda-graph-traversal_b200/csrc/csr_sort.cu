@@ -641,16 +641,30 @@ __global__ void renumber_rows_kernel(const uint64_t *__restrict__ rs, const int 
                                      const unsigned *__restrict__ inv, const uint64_t *__restrict__ rs2,
                                      int *__restrict__ col2, float *__restrict__ w2, unsigned *__restrict__ light2,
                                      unsigned *__restrict__ tiny2, unsigned *__restrict__ err) {
+    // 32 consecutive new rows per warp step (similar lengths: the new order
+    // is by decreasing length).  A row of up to 32 entries is copied by its
+    // own lane, longer ones up to RENUM_LONG by the whole warp.
     const unsigned lane = lane_id();
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
-        const unsigned o = __ldg(&inv[i]);
-        const uint64_t b = __ldg(&rs[o]), len = __ldg(&rs[o + 1]) - b, b2 = __ldg(&rs2[i]);
-        if (lane == 0) {
+    for (uint64_t i0 = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; i0 < n; i0 += nw * 32) {
+        const uint64_t i = i0 + lane;
+        uint64_t b = 0, len = 0, b2 = 0;
+        if (i < n) {
+            const unsigned o = __ldg(&inv[i]);
+            b = __ldg(&rs[o]);
+            len = __ldg(&rs[o + 1]) - b;
+            b2 = __ldg(&rs2[i]);
             light2[i] = __ldg(&light[o]);
             tiny2[i] = __ldg(&tiny[o]);
+            if (len <= 32) renumber_copy<1>(col, w, b, len, b2, n, perm, col2, w2, err, 0);
         }
-        if (len <= RENUM_LONG) renumber_copy<32>(col, w, b, len, b2, n, perm, col2, w2, err, lane);
+        unsigned todo = __ballot_sync(FULL, len > 32 && len <= RENUM_LONG);
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            renumber_copy<32>(col, w, __shfl_sync(FULL, b, l), __shfl_sync(FULL, len, l), __shfl_sync(FULL, b2, l), n,
+                              perm, col2, w2, err, lane);
+        }
     }
 }
 
