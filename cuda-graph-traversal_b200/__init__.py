@@ -98,6 +98,7 @@ def _load() -> C.CDLL:
         "g5_bfs_traverse": ([p, p, u64, u64, p, p, p, u64, p, p], C.c_int),
         "g5_bfs_query": ([p, p, u64, p, p, p, p, p, u64, p, p, p], C.c_int),
         "g5_bfs_export": ([p, p, u64, p, u64, p, u64, p, p], C.c_int),
+        "g5_bfs_first_neighbours": ([p, p, u64, p, p], C.c_int),
         "g5_bfs_query_plan_create": ([p, p, u64, p, p, p, p, u64, p, p, p, p], C.c_int),
         "g5_bfs_query_plan_run": ([p, u64], C.c_int),
         "g5_bfs_query_plan_export": ([p, u64, p, u64, p], C.c_int),
@@ -156,7 +157,7 @@ def _check(rc: int) -> None:
 
 class BfsParams(C.Structure):
     _fields_ = [("alpha", C.c_float), ("beta", C.c_float), ("mode", C.c_int32), ("blocks", C.c_int32),
-                ("big_deg", C.c_int32), ("chunk", C.c_int32), ("lane_entries", C.c_int32)]
+                ("big_deg", C.c_int32), ("chunk", C.c_int32), ("lane_entries", C.c_int32), ("top", C.c_void_p)]
 
 
 class BfsStats(C.Structure):
@@ -299,6 +300,9 @@ class OnedGraph:
     # The BFS copy of the column (g5_csr_degree_order): each row's
     # neighbours by decreasing degree.  None: the BFS reads col.
     bcol: torch.Tensor | None = None
+    # Each vertex's first entry of bcol (g5_bfs_first_neighbours): what a
+    # bottom-up level probes before reading the row.
+    btop: torch.Tensor | None = None
     # The SSSP copy renumbered by decreasing degree (g5_csr_sssp_renumber),
     # which the SSSP entry points use when present; None: the split copy
     # above in the caller's numbering.
@@ -406,8 +410,20 @@ def oned_graph_bfs_order(g: OnedGraph, stream=None, work: torch.Tensor | None = 
     bcol = torch.empty(max(e, 1), dtype=torch.int32, device=g.device)
     _check(lib.g5_csr_degree_order(_ptr(g.rowstarts), _ptr(g.col), n, e, _ptr(bcol), _ptr(work), work.numel(),
                                    _stream(stream)))
-    g.bcol = bcol
+    btop = torch.empty(max(n, 1), dtype=torch.int32, device=g.device)
+    _check(lib.g5_bfs_first_neighbours(_ptr(g.rowstarts), _ptr(bcol), n, _ptr(btop), _stream(stream)))
+    g.bcol, g.btop = bcol, btop
     return g
+
+
+def _bfs_p(g: OnedGraph, params: "BfsParams | None") -> "BfsParams | None":
+    """params for a search on g.bfs_col, with the graph's first-neighbour
+    array when it has one (a copy: the caller's struct is left alone)."""
+    if g.btop is None or g.bcol is None:
+        return params
+    q = BfsParams(14.0, 24.0, 0, 0) if params is None else BfsParams.from_buffer_copy(params)
+    q.top = g.btop.data_ptr()
+    return q
 
 
 def _finish_graph(n, e, rowstarts, col, w, col64, light_delta, work, dedupe, st, dev, stream,
@@ -641,6 +657,7 @@ def oned_graph_bfs_traverse_multi(g: OnedGraph, bfs: "BfsState", d_roots: torch.
                                   with_depth: bool = True, stream=None) -> None:
     """BFS from every root in d_roots (device int64) at once
     (g5_bfs_traverse_multi); reset bfs first."""
+    params = _bfs_p(g, params)
     _check(lib.g5_bfs_traverse_multi(_ptr(g.rowstarts), _ptr(g.bfs_col), g.nglobalverts, _ptr(d_roots), d_roots.numel(),
                                      _ptr(bfs.pred), _ptr(bfs.depth) if with_depth else None, _ptr(bfs.work),
                                      bfs.work.numel(), C.byref(params) if params is not None else None,
@@ -724,8 +741,10 @@ def main_component_bitmap(g: OnedGraph, stream=None) -> np.ndarray:
     bfs = BfsState(g)
     _check(lib.g5_bfs_reset(g.nglobalverts, _ptr(bfs.pred), None, None, _ptr(bfs.work), bfs.work.numel(),
                             _stream(stream)))
+    hp = _bfs_p(g, None)
     _check(lib.g5_bfs_traverse(_ptr(g.rowstarts), _ptr(g.bfs_col), g.nglobalverts, hub, _ptr(bfs.pred), None,
-                               _ptr(bfs.work), bfs.work.numel(), None, _stream(stream)))
+                               _ptr(bfs.work), bfs.work.numel(), C.byref(hp) if hp is not None else None,
+                               _stream(stream)))
     bits = torch.empty((g.nglobalverts + 31) // 32, dtype=torch.int32, device=g.device)
     _check(lib.g5_bfs_visited_bitmap(_ptr(bfs.work), bfs.work.numel(), g.nglobalverts, _ptr(bits),
                                      _stream(stream)))
@@ -848,7 +867,7 @@ def oned_graph_bfs_traverse(g: OnedGraph, bfs: BfsState, root: int, params: BfsP
                             with_depth: bool = True, stream=None) -> None:
     """Second half of oned_graph_bfs_run: the persistent BFS kernel alone
     (one block for a root outside the main component)."""
-    params = _right_sized(g, root, params)
+    params = _bfs_p(g, _right_sized(g, root, params))
     _check(lib.g5_bfs_traverse(_ptr(g.rowstarts), _ptr(g.bfs_col), g.nglobalverts, root, _ptr(bfs.pred),
                                _ptr(bfs.depth) if with_depth else None, _ptr(bfs.work), bfs.work.numel(),
                                C.byref(params) if params is not None else None, _stream(stream)))
@@ -949,10 +968,11 @@ def oned_graph_bfs_query_export(g: OnedGraph, bfs: BfsState, root: int, with_dep
 def _make_query_plan(g: OnedGraph, bfs: BfsState, with_depth: bool, st, params: BfsParams | None = None):
     bfs.drop_plan()
     h = C.c_void_p()
+    cp = _bfs_p(g, params)  # the plan copies it
     _check(lib.g5_bfs_query_plan_create(g.rowstarts.data_ptr(), g.bfs_col.data_ptr(), g.nglobalverts, _main_bits_ptr(g),
                                         bfs.pred.data_ptr(), bfs.depth.data_ptr() if with_depth else None,
                                         bfs.work.data_ptr(), bfs.work.numel(),
-                                        C.byref(params) if params is not None else None, C.byref(bfs.h_stats), st,
+                                        C.byref(cp) if cp is not None else None, C.byref(bfs.h_stats), st,
                                         C.byref(h)))
     # The graph (and params) are held with the plan: the plan keeps its device pointers.
     bfs._plan = (g, with_depth, st, h.value, g.main_bits, params, g.bfs_col)

@@ -16,6 +16,7 @@ namespace g5compat {
 struct GraphExt {
     int32_t *col;        // int32 neighbour ids, rows in canonical order (as Oned_Graph.column)
     int32_t *bcol;       // the BFS copy (g5_csr_degree_order): rows by decreasing neighbour degree
+    uint32_t *btop;      // each row's first entry of bcol (g5_bfs_first_neighbours)
     // The SSSP copy: rows split tiny | light | heavy (g5_csr_split_light),
     // renumbered by decreasing degree (g5_csr_sssp_renumber).
     uint64_t *srowstarts;

@@ -44,6 +44,7 @@ Oned_Graph oned_graph_from_tuple_graph(Worker_State *ws, Tuple_Graph *tg, u64 ng
     x.light_delta = kLightDelta;
     x.main_host = nullptr;
     x.isolated = (uint32_t *)gpu_push(ws, (nglobalverts + 31) / 32 * sizeof(uint32_t), "isolated-vertex bitmap");
+    x.btop = (uint32_t *)gpu_push(ws, nglobalverts * sizeof(uint32_t), "BFS first neighbours");
     // Rows in canonical order (sorted by neighbour, then weight), the SSSP
     // copy (split, then renumbered by decreasing degree) and the BFS copy;
     // the scratch (the split copy in the caller's numbering and the sorting
@@ -73,6 +74,7 @@ Oned_Graph oned_graph_from_tuple_graph(Worker_State *ws, Tuple_Graph *tg, u64 ng
           "oned_graph_from_tuple_graph");
     check(ws, g5_csr_degree_order(g.rowstarts, x.col, nglobalverts, e, x.bcol, swork, sbytes, 0),
           "oned_graph_from_tuple_graph");
+    check(ws, g5_bfs_first_neighbours(g.rowstarts, x.bcol, nglobalverts, x.btop, 0), "oned_graph_from_tuple_graph");
     CHECK_CUDA(cudaDeviceSynchronize());
     ws->gpu_arena = before_sort;
     check(ws, g5_graph_isolated_bitmap(g.rowstarts, nglobalverts, x.isolated, 0), "oned_graph_from_tuple_graph");
@@ -122,8 +124,10 @@ Bfs_State oned_graph_bfs_create(Worker_State *ws, const Oned_Graph *g) {
         const u64 words = (g->nglobalverts + 31) / 32;
         check(ws, g5_bfs_reset(g->nglobalverts, bfs.pred, nullptr, nullptr, x.work, x.work_bytes, 0),
               "oned_graph_bfs_create");
+        g5_bfs_params hp = {14.0f, 24.0f, 0, 0};
+        hp.top = gx->btop;
         check(ws, g5_bfs_traverse(g->rowstarts, gx->bcol, g->nglobalverts, hub, bfs.pred, nullptr, x.work, x.work_bytes,
-                                  nullptr, 0),
+                                  &hp, 0),
               "oned_graph_bfs_create");
         uint32_t *bits = (uint32_t *)gpu_push(ws, words * sizeof(uint32_t), "component bitmap");
         check(ws, g5_bfs_visited_bitmap(x.work, x.work_bytes, g->nglobalverts, bits, 0), "oned_graph_bfs_create");
@@ -167,8 +171,10 @@ void oned_graph_bfs_run(Worker_State *ws, const Oned_Graph *g, Bfs_State *bfs, u
     // protocol calls before every search (examples/graph500_runner.cu:309).
     *bx->root_host = root;
     g5_bfs_stats *st = (g5_bfs_stats *)(bx->root_host + 1);
+    g5_bfs_params bp = {14.0f, 24.0f, 0, 0};  // the library's defaults, with the first-neighbour probe
+    bp.top = gx->btop;
     check(ws, g5_bfs_query(g->rowstarts, gx->bcol, g->nglobalverts, bx->root_host, gx->main_host, bfs->pred, bx->depth,
-                           bx->work, bx->work_bytes, nullptr, st, 0),
+                           bx->work, bx->work_bytes, &bp, st, 0),
           "oned_graph_bfs_run");
 }
 

@@ -229,6 +229,11 @@ typedef struct g5_bfs_params {
     int32_t chunk;        /* edges per chunk, a multiple of 32 up to 65536 (256)                          */
     int32_t lane_entries; /* bottom-up: entries of a row one lane scans before its warp joins, a multiple
                              of 4 up to 1024 (8)                                                          */
+    /* Optional (NULL = none): top[v] = col[rowstarts[v]], the first entry of v's row in the column the
+       search is given (nverts for an empty row), from g5_bfs_first_neighbours.  A bottom-up level then
+       probes each unvisited vertex's first neighbour from this dense array before reading its row: with
+       rows by decreasing neighbour degree (g5_csr_degree_order) most hits are there.  Same parents. */
+    const uint32_t *top;
 } g5_bfs_params;
 
 typedef struct g5_bfs_stats {
@@ -354,6 +359,10 @@ int g5_bfs_visited_bitmap(const void *d_work, uint64_t work_bytes, uint64_t nver
  * leaves Bfs_State.pred on the device (src/traversal.h:59-66). */
 int g5_bfs_export(const int64_t *d_pred, const int32_t *d_depth, uint64_t nverts, void *d_work, uint64_t work_bytes,
                   g5_bfs_reached *out, uint64_t capacity, uint64_t *h_count, void *stream);
+
+/* top[v] = d_col[d_rowstarts[v]] (nverts when row v is empty), for g5_bfs_params.top. */
+int g5_bfs_first_neighbours(const uint64_t *d_rowstarts, const int32_t *d_col, uint64_t nverts, uint32_t *d_top,
+                            void *stream);
 
 /* Statistics of the last g5_bfs_run that used this workspace (synchronises). */
 int g5_bfs_last_stats(const void *d_work, uint64_t work_bytes, g5_bfs_stats *stats, void *stream);
