@@ -37,9 +37,9 @@ sys.path.insert(0, REPO)
 PEAKS = os.path.join(REPO, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per traversed input edge of bfs_persistent_kernel on a
-# main-component root, from an ncu capture at SCALE 23 (610.4 MB for 134,213,828 edges,
-# profiles/bfs_persistent_kernel_scale23.md); scaled to the bench's roots by their edges.
-TRAFFIC_BYTES_PER_EDGE = 4.53
+# main-component root, from an ncu capture at SCALE 23 (479.8 MB for 134,213,828 edges,
+# with the bottom-up first-neighbour probe); scaled to the bench's roots by their edges.
+TRAFFIC_BYTES_PER_EDGE = 3.57
 E2E_REPS = 3  # end-to-end calls per root (median kept)
 GATE_CYCLES = 200_000  # ~0.1 ms device-side spin queued before each timed root
 
@@ -441,7 +441,7 @@ def run_ours(args):
                          "traffic": int(args.traffic if args.traffic is not None
                                         else TRAFFIC_BYTES_PER_EDGE * np.mean([nedge[timed[i]] for i in big])),
                          "traffic_source": "ncu dram__bytes_read+write given by --traffic" if args.traffic
-                         is not None else "ncu capture at SCALE 23: 4.53 B per traversed edge, scaled by edges"},
+                         is not None else "ncu capture at SCALE 23: 3.57 B per traversed edge, scaled by edges"},
             "e2e": {"value": float(f"{(e2e_hm if world == 1 else e2e_hm * world):.6g}"), "unit": "GTEPS",
                     "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 24,
                     "small_root_us": round(min(e2e_s) * 1e6, 1) if e2e_s else None,
